@@ -1,0 +1,47 @@
+// ORACLE — test infrastructure only.  Plain-argument entry points around the reference's own
+// host audio library (built from the reference sources by oracle/build_ref.sh), so that
+// Python's ctypes can drive it: handle creation with an explicit thread count and the resample
+// call, whose RpptResamplingWindow& argument (api/rppdefs.h:751-790) holds a std::vector and
+// __m128 members that ctypes cannot build.  Compiled against the reference headers.
+#include <vector>
+
+#include "rpp.h"
+#include "rppdefs.h"
+#include "rppt_tensor_audio_augmentations.h"
+
+extern "C" {
+
+// rppCreate with the host backend (api/rpp.h:132).  numThreads must be explicit: 0 means
+// "batch size" threads in the reference (src/modules/handle_host.cpp:57-59).
+__attribute__((visibility("default"))) void* ref_create(size_t batchSlots, unsigned numThreads)
+{
+    rppHandle_t h = nullptr;
+    if (rppCreate(&h, batchSlots, numThreads, nullptr, RPP_HOST_BACKEND) != rppStatusSuccess) return nullptr;
+    return h;
+}
+
+__attribute__((visibility("default"))) int ref_destroy(void* h)
+{
+    return rppDestroy(static_cast<rppHandle_t>(h), RPP_HOST_BACKEND);
+}
+
+// rppt_resample_host (api/rppt_tensor_audio_augmentations.h:292) with the window given as its
+// lookup table and the scale/center/lobes/coeffs fields the reference's windowed_sinc sets
+// (utilities/test_suite/rpp_test_suite_audio.h:401-430).
+__attribute__((visibility("default"))) int ref_resample(float* src, RpptDesc* srcDesc, float* dst, RpptDesc* dstDesc,
+                                                        float* inRate, float* outRate, int* srcDims, const float* lut,
+                                                        int lutSize, float scale, float center, int lobes, int coeffs,
+                                                        void* h)
+{
+    RpptResamplingWindow w;
+    w.lookup.assign(lut, lut + lutSize);
+    w.lookupSize = lutSize;
+    w.scale = scale;
+    w.center = center;
+    w.lobes = lobes;
+    w.coeffs = coeffs;
+    w.pCenter = _mm_set1_ps(center);
+    w.pScale = _mm_set1_ps(scale);
+    return rppt_resample_host(src, srcDesc, dst, dstDesc, inRate, outRate, srcDims, w, static_cast<rppHandle_t>(h));
+}
+}

@@ -1,0 +1,677 @@
+/*
+ * ORACLE — test infrastructure only.  This file is a CPU restatement of the reference's host
+ * audio path (ROCm/rpp src/modules/tensor/cpu/kernel/*.cpp), used by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker.  It is never
+ * linked into the product library and never runs on the product path.
+ *
+ * Two kinds of functions:
+ *  - float restatements that repeat the reference's float operations in the reference's order
+ *    (compiled with -ffp-contract=off, no fast-math, like the reference's -mno-fma build), so
+ *    they agree bit for bit with the reference where the reference is deterministic float
+ *    arithmetic (pre-emphasis, down-mixing, resampling, mel filter bank, decibels, NSR);
+ *  - FP64 forms (spectrogram, mel, decibels, the whole front-end chain) that evaluate the same
+ *    definitions in double precision: the "FP64 oracle" against which errors are reported.
+ *    The reference's FP32 spectrogram runs ffts (a prebuilt third-party binary), whose
+ *    operation order is not restated; its FP32 results are checked against the reference
+ *    library itself and the shipped goldens, within a per-frame relative tolerance.
+ *
+ * Parity is pinned by tests/test_oracle_golden.py: against the shipped golden outputs
+ * (utilities/test_suite/REFERENCE_OUTPUTS_AUDIO/*.bin, captured under tests/golden/) and
+ * against the reference host library built by oracle/build_ref.sh.
+ *
+ * Strides are in elements, as in RpptDesc.strides.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+
+#define EXPORT __attribute__((visibility("default")))
+
+/* ---------------------------------------------------------------- pre-emphasis
+ * cpu/kernel/pre_emphasis_filter.cpp:39-71: y[0] = x[0] - c*border, y[i] = x[i] - c*x[i-1]. */
+EXPORT void oracle_pre_emphasis(const float *src, long srcStride, float *dst, long dstStride, int n,
+                                const int *len, const float *coeff, int border)
+{
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < n; b++)
+    {
+        const float *x = src + (long)b * srcStride;
+        float *y = dst + (long)b * dstStride;
+        float c = coeff[b];
+        float bv = (border == 1) ? x[0] : (border == 2) ? x[1] : 0.f;   /* CLAMP=1, REFLECT=2 */
+        y[0] = x[0] - c * bv;
+        for (int i = 1; i < len[b]; i++)
+            y[i] = x[i] - c * x[i - 1];
+    }
+}
+
+/* ---------------------------------------------------------------- down-mixing
+ * cpu/kernel/down_mixing.cpp:42-117.  Lane sums and horizontal sums in the SSE/AVX order of
+ * rpp_hsum_ps (src/include/common/cpu/rpp_cpu_simd_math.hpp:846-867). */
+static float hsum4(const float p[4]) { return (p[0] + p[1]) + (p[2] + p[3]); }
+static float hsum8(const float p[8]) { return ((p[0] + p[4]) + (p[2] + p[6])) + ((p[1] + p[5]) + (p[3] + p[7])); }
+
+EXPORT void oracle_down_mixing(const float *src, long srcStride, float *dst, long dstStride, int n,
+                               const int *dims, int normalize)
+{
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < n; b++)
+    {
+        const float *x = src + (long)b * srcStride;
+        float *y = dst + (long)b * dstStride;
+        int samples = dims[2 * b], ch = dims[2 * b + 1];
+        if (ch == 1)
+        {
+            memcpy(y, x, (size_t)samples * sizeof(float));
+            continue;
+        }
+        float w[64];
+        for (int c = 0; c < ch; c++) w[c] = 1.f / ch;
+        if (normalize)
+        {
+            float sum = 0.0f;
+            for (int c = 0; c < ch; c++) sum += w[c];
+            float inv = (float)(1.0 / sum);
+            for (int c = 0; c < ch; c++) w[c] *= inv;
+        }
+        int lanes = ch > 7 ? 8 : 4;
+        int aligned = (ch / lanes) * lanes;
+        for (long t = 0; t < samples; t++)
+        {
+            const float *xs = x + t * ch;
+            float p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int g = 0; g < aligned; g += lanes)
+                for (int l = 0; l < lanes; l++) p[l] = p[l] + xs[g + l] * w[g + l];
+            float acc = (lanes == 8) ? hsum8(p) : hsum4(p);
+            for (int c = aligned; c < ch; c++) acc += xs[c] * w[c];
+            y[t] = acc;
+        }
+    }
+}
+
+/* ---------------------------------------------------------------- resample
+ * cpu/kernel/resample.cpp:46-141 with the window of api/rppdefs.h:751-790: LUT interpolation,
+ * 256-output blocks with an FP64 block origin and an FP32 running phase, 4-lane partial sums
+ * for mono input, per-channel sequential sums for multi-channel input. */
+typedef struct
+{
+    const float *lut;
+    int lutSize;
+    float scale, center;
+    int lobes;
+} oracle_window;
+
+static float win_scalar(const oracle_window *w, float x)        /* rppdefs.h:760-769 */
+{
+    float locRaw = x * w->scale + w->center;
+    int locFloor = (int)floorf(locRaw);
+    float weight = locRaw - locFloor;
+    if (locFloor > w->lutSize - 2) locFloor = w->lutSize - 2;
+    if (locFloor < 0) locFloor = 0;
+    float cur = w->lut[locFloor], nxt = w->lut[locFloor + 1];
+    return cur + weight * (nxt - cur);
+}
+
+static float win_lane(const oracle_window *w, float x)          /* rppdefs.h:771-782 (truncating) */
+{
+    float locRaw = x * w->scale + w->center;
+    int idx = (int)locRaw;
+    float weight = locRaw - (float)idx;
+    float cur = w->lut[idx], nxt = w->lut[idx + 1];
+    return cur + weight * (nxt - cur);
+}
+
+EXPORT void oracle_resample(const float *src, long srcStride, float *dst, long dstStride, int n,
+                            const float *inRate, const float *outRate, const int *dims,
+                            const float *lut, int lutSize, float wscale, float wcenter, int lobes)
+{
+    oracle_window W = {lut, lutSize, wscale, wcenter, lobes};
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < n; b++)
+    {
+        const float *x = src + (long)b * srcStride;
+        float *y = dst + (long)b * dstStride;
+        float ir = inRate[b], orate = outRate[b];
+        int len = dims[2 * b], ch = dims[2 * b + 1];
+        if (orate == ir)
+        {
+            memcpy(y, x, (size_t)len * ch * sizeof(float));
+            continue;
+        }
+        int outEnd = (int)ceilf((float)len * orate / ir);
+        double scale = (double)ir / orate;
+        float fscale = (float)scale;
+        float tmp[64];
+        for (int outBlock = 0; outBlock < outEnd; outBlock += 256)
+        {
+            int blockEnd = outBlock + 256 < outEnd ? outBlock + 256 : outEnd;
+            double inBlockRaw = outBlock * scale;
+            int inBlockRounded = (int)inBlockRaw;
+            float inPos = (float)(inBlockRaw - inBlockRounded);
+            const float *in = x + (long)inBlockRounded * ch;
+            for (int outPos = outBlock; outPos < blockEnd; outPos++, inPos += fscale)
+            {
+                int xc = (int)ceilf(inPos);
+                int loc0 = xc - lobes, loc1 = xc + lobes;
+                if (loc0 + inBlockRounded < 0) loc0 = -inBlockRounded;
+                if (loc1 + inBlockRounded > len) loc1 = len - inBlockRounded;
+                if (ch == 1)
+                {
+                    int l = loc0;
+                    float locBegin = l - inPos;
+                    float lane[4] = {locBegin + 0.f, locBegin + 1.f, locBegin + 2.f, locBegin + 3.f};
+                    float acc4[4] = {0, 0, 0, 0};
+                    for (; l + 3 < loc1; l += 4)
+                        for (int j = 0; j < 4; j++)
+                        {
+                            acc4[j] = acc4[j] + in[l + j] * win_lane(&W, lane[j]);
+                            lane[j] = lane[j] + 4.f;
+                        }
+                    float accum = (acc4[0] + acc4[2]) + (acc4[1] + acc4[3]);
+                    float xx = l - inPos;
+                    for (; l < loc1; l++, xx++)
+                        accum += in[l] * win_scalar(&W, xx);
+                    y[outPos] = accum;
+                }
+                else
+                {
+                    for (int c = 0; c < ch; c++) tmp[c] = 0.f;
+                    float xx = loc0 - inPos;
+                    for (int l = loc0; l < loc1; l++, xx++)
+                    {
+                        float wv = win_scalar(&W, xx);
+                        for (int c = 0; c < ch; c++) tmp[c] += in[(long)l * ch + c] * wv;
+                    }
+                    for (int c = 0; c < ch; c++) y[(long)outPos * ch + c] = tmp[c];
+                }
+            }
+        }
+    }
+}
+
+/* ---------------------------------------------------------------- spectrogram (FP64)
+ * cpu/kernel/spectrogram.cpp:36-69 (Hann with the t+0.5 phase, frame count, reflect rule) and
+ * :116-242 (frames, window centred in the nfft buffer, power 2 -> re^2+im^2, else |X|),
+ * evaluated in double with an exact-twiddle FFT (radix-2 for powers of two, direct DFT
+ * otherwise). */
+static int reflect_idx(int loc, int minLoc, int maxLoc)          /* spectrogram.cpp:55-69 */
+{
+    if (maxLoc - minLoc < 2) return maxLoc - 1;
+    for (;;)
+    {
+        if (loc < minLoc) loc = 2 * minLoc - loc;
+        else if (loc >= maxLoc) loc = 2 * maxLoc - 2 - loc;
+        else break;
+    }
+    return loc;
+}
+
+EXPORT int oracle_num_windows(int len, int windowLength, int windowStep, int center)   /* :47-52 */
+{
+    if (!center) len -= windowLength;
+    return len / windowStep + 1;
+}
+
+static void fft_d(double *re, double *im, int N)    /* in-place, forward, natural order */
+{
+    for (int i = 1, j = 0; i < N; i++)
+    {
+        int bit = N >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j)
+        {
+            double t = re[i]; re[i] = re[j]; re[j] = t;
+            t = im[i]; im[i] = im[j]; im[j] = t;
+        }
+    }
+    for (int len = 2; len <= N; len <<= 1)
+    {
+        int half = len >> 1;
+        for (int k = 0; k < half; k++)
+        {
+            double ang = -2.0 * M_PI * (double)k / (double)len;
+            double wr = cos(ang), wi = sin(ang);
+            for (int i = 0; i < N; i += len)
+            {
+                double ur = re[i + k], ui = im[i + k];
+                double vr = re[i + k + half] * wr - im[i + k + half] * wi;
+                double vi = re[i + k + half] * wi + im[i + k + half] * wr;
+                re[i + k] = ur + vr; im[i + k] = ui + vi;
+                re[i + k + half] = ur - vr; im[i + k + half] = ui - vi;
+            }
+        }
+    }
+}
+
+/* Power spectrum of one prepared nfft buffer v (double) into out[bin] (bins = nfft/2+1). */
+static void spectrum_d(const double *v, int nfft, int power, double *out, double *re, double *im)
+{
+    int bins = nfft / 2 + 1;
+    int pow2 = (nfft & (nfft - 1)) == 0;
+    if (pow2)
+    {
+        for (int i = 0; i < nfft; i++) { re[i] = v[i]; im[i] = 0.0; }
+        fft_d(re, im, nfft);
+    }
+    else
+    {
+        for (int k = 0; k < bins; k++)
+        {
+            double sr = 0, si = 0;
+            for (int t = 0; t < nfft; t++)
+            {
+                long e = ((long)t * k) % nfft;
+                double ang = -2.0 * M_PI * (double)e / (double)nfft;
+                sr += v[t] * cos(ang);
+                si += v[t] * sin(ang);
+            }
+            re[k] = sr; im[k] = si;
+        }
+    }
+    for (int k = 0; k < bins; k++)
+        out[k] = (power == 1) ? sqrt(re[k] * re[k] + im[k] * im[k]) : re[k] * re[k] + im[k] * im[k];
+}
+
+/* Hann window as the reference builds it: FP64 then rounded to float (spectrogram.cpp:36-44). */
+EXPORT void oracle_hann_window(float *w, int W)
+{
+    double a = (2.0 * M_PI) / W;
+    for (int t = 0; t < W; t++) w[t] = (float)(0.5 * (1.0 - cos(a * (t + 0.5))));
+}
+
+/* dst (double) gets NFT [bins][hStride] (layoutNFT=1) or NTF [frames][hStride] per sample.
+ * `preemph` != 0 applies pre-emphasis (coefficient coeff[b], border ZERO/CLAMP/REFLECT) in
+ * double before framing, so the same function is the FP64 front of the fused chain. */
+EXPORT void oracle_spectrogram_f64(const float *src, long srcStride, double *dst, long dstNStride, long dstHStride,
+                                   int n, const int *len, int center, int reflect, const float *window, int nfft,
+                                   int power, int W, int hop, int layoutNFT, int preemph, const float *coeff,
+                                   int border)
+{
+    if (nfft == 0) nfft = W;
+    int bins = nfft / 2 + 1;
+    int off = center ? W / 2 : 0;
+    float *wf = (float *)malloc(sizeof(float) * W);
+    if (window) memcpy(wf, window, sizeof(float) * W);
+    else oracle_hann_window(wf, W);
+    int start0 = W < nfft ? (nfft - W) / 2 : 0;
+#pragma omp parallel
+    {
+        double *v = (double *)malloc(sizeof(double) * nfft);
+        double *re = (double *)malloc(sizeof(double) * nfft);
+        double *im = (double *)malloc(sizeof(double) * nfft);
+        double *pw = (double *)malloc(sizeof(double) * bins);
+#pragma omp for schedule(dynamic)
+        for (int b = 0; b < n; b++)
+        {
+            const float *x = src + (long)b * srcStride;
+            int L = len[b];
+            int F = oracle_num_windows(L, W, hop, center);
+            double c = preemph ? (double)coeff[b] : 0.0;
+            for (int f = 0; f < F; f++)
+            {
+                int ws = f * hop - off;
+                for (int i = 0; i < nfft; i++) v[i] = 0.0;
+                for (int t = 0; t < W; t++)
+                {
+                    int idx = ws + t;
+                    double xv = 0.0;
+                    int valid = 1;
+                    if (idx < 0 || idx >= L)
+                    {
+                        if (reflect) idx = reflect_idx(idx, 0, L);
+                        else valid = 0;
+                    }
+                    if (!valid || idx < 0 || idx >= L) xv = 0.0;
+                    else if (preemph)
+                    {
+                        double prev = idx > 0 ? (double)x[idx - 1]
+                                              : (border == 1 ? (double)x[0] : border == 2 ? (double)x[1] : 0.0);
+                        xv = (double)x[idx] - c * prev;
+                    }
+                    else xv = (double)x[idx];
+                    v[start0 + t] = (double)wf[t] * xv;
+                }
+                spectrum_d(v, nfft, power, pw, re, im);
+                double *o = dst + (long)b * dstNStride;
+                for (int k = 0; k < bins; k++)
+                {
+                    if (layoutNFT) o[(long)k * dstHStride + f] = pw[k];
+                    else o[(long)f * dstHStride + k] = pw[k];
+                }
+            }
+        }
+        free(v); free(re); free(im); free(pw);
+    }
+    free(wf);
+}
+
+/* ---------------------------------------------------------------- mel filter bank
+ * cpu/kernel/mel_filter_bank.cpp:40-193 with the scales of api/rppdefs.h:806-851.  The scale
+ * functions are float functions (float log/exp), the filter edges FP64, the per-bin weights
+ * rounded to float, and the output accumulated in float bin by bin. */
+static float hz_to_mel_f(int htk, float hz)
+{
+    if (htk) return 1127.0f * logf(1.0f + (hz / 700.0f));
+    const float fsp = 66.666667f, minLogHz = 1000.0f, minLogMel = (1000.0f - 0.0f) / fsp;
+    const float stepLog = 0.068751777f, invMinLogHz = 0.001f, invStepLog = 1.0f / stepLog, invFsp = 1.0f / fsp;
+    if (hz >= minLogHz) return minLogMel + logf(hz * invMinLogHz) * invStepLog;
+    return (hz - 0.0f) * invFsp;
+}
+
+static float mel_to_hz_f(int htk, float mel)
+{
+    if (htk) return 700.0f * (expf(mel / 1127.0f) - 1.0f);
+    const float fsp = 66.666667f, minLogHz = 1000.0f, minLogMel = (1000.0f - 0.0f) / fsp;
+    const float stepLog = 0.068751777f;
+    if (mel >= minLogMel) return minLogHz * expf(stepLog * (mel - minLogMel));
+    return 0.0f + mel * fsp;
+}
+
+/* Table of one sample: interval[bin] (-1 = none), weightsDown[bin] (float), norm[filter]. */
+typedef struct
+{
+    int start, end;     /* fftBinStart, fftBinEnd */
+} mel_range;
+
+static mel_range mel_tables(int htk, float minFreq, float maxFreq, int numFilter, float sampleRate, int normalize,
+                            int nfft, int *interval, float *weightsDown, float *norm, double *weightsDownD,
+                            double *normD)
+{
+    int numBins = nfft / 2 + 1;
+    double melLow = hz_to_mel_f(htk, minFreq), melHigh = hz_to_mel_f(htk, maxFreq);
+    double melStep = (melHigh - melLow) / (numFilter + 1);
+    double hzStep = (double)sampleRate / nfft, invHzStep = 1.0 / hzStep;
+    int binStart = (int)ceil(minFreq * invHzStep);
+    int binEnd = (int)ceil(maxFreq * invHzStep);
+    if (binEnd > numBins) binEnd = numBins;
+    for (int i = 0; i < numFilter; i++) { norm[i] = 1.f; if (normD) normD[i] = 1.0; }
+    for (int k = 0; k < numBins; k++) { interval[k] = -1; weightsDown[k] = 0.f; if (weightsDownD) weightsDownD[k] = 0.0; }
+    int bin = binStart;
+    double mel0 = melLow, mel1 = melLow + melStep;
+    double fIter = bin * hzStep;
+    for (int it = 0; it < numFilter + 1; it++, mel0 = mel1, mel1 += melStep)
+    {
+        double f0 = mel_to_hz_f(htk, (float)mel0);
+        double f1 = mel_to_hz_f(htk, (float)(it == numFilter ? melHigh : mel1));
+        double slope = 1. / (f1 - f0);
+        if (normalize && it < numFilter)
+        {
+            double f2 = mel_to_hz_f(htk, (float)(mel1 + melStep));
+            norm[it] = (float)(2.0 / (f2 - f0));
+            if (normD) normD[it] = 2.0 / (f2 - f0);
+        }
+        for (; bin < binEnd && fIter < f1; bin++, fIter = bin * hzStep)
+        {
+            weightsDown[bin] = (float)((f1 - fIter) * slope);
+            if (weightsDownD) weightsDownD[bin] = (f1 - fIter) * slope;
+            interval[bin] = it;
+        }
+    }
+    mel_range r = {binStart, binEnd};
+    return r;
+}
+
+EXPORT void oracle_mel_filter_bank(const float *src, long srcNStride, long srcHStride, float *dst, long dstNStride,
+                                   long dstHStride, int n, const int *dims, float maxFreqVal, float minFreq, int htk,
+                                   int numFilter, float sampleRate, int normalize)
+{
+    float maxFreq = (maxFreqVal == 0) ? sampleRate / 2 : maxFreqVal;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < n; b++)
+    {
+        int nfft = (dims[2 * b] - 1) * 2, numBins = nfft / 2 + 1, frames = dims[2 * b + 1];
+        int *interval = (int *)malloc(sizeof(int) * (numBins + 1));
+        float *wd = (float *)malloc(sizeof(float) * (numBins + 1));
+        float *norm = (float *)malloc(sizeof(float) * (numFilter + 1));
+        mel_range r = mel_tables(htk, minFreq, maxFreq, numFilter, sampleRate, normalize, nfft, interval, wd, norm,
+                                 NULL, NULL);
+        const float *x = src + (long)b * srcNStride;
+        float *y = dst + (long)b * dstNStride;
+        long zc = frames + 8 < dstHStride ? frames + 8 : dstHStride;
+        for (int m = 0; m < numFilter; m++)
+            for (long t = 0; t < zc; t++) y[m * dstHStride + t] = 0.f;
+        for (int bin = r.start; bin < r.end; bin++)
+        {
+            const float *row = x + (long)bin * srcHStride;
+            int up = interval[bin], down = up - 1;
+            float wDown = wd[bin], wUp = 1.0f - wd[bin];
+            if (down >= 0)
+            {
+                float w = normalize ? wDown * norm[down] : wDown;
+                float *o = y + (long)down * dstHStride;
+                for (int t = 0; t < frames; t++) o[t] = o[t] + row[t] * w;
+            }
+            if (up >= 0 && up < numFilter)
+            {
+                float w = normalize ? wUp * norm[up] : wUp;
+                float *o = y + (long)up * dstHStride;
+                for (int t = 0; t < frames; t++) o[t] = o[t] + row[t] * w;
+            }
+        }
+        free(interval); free(wd); free(norm);
+    }
+}
+
+/* FP64 mel of an FP64 spectrum: same filter placement, weights kept in double. */
+EXPORT void oracle_mel_filter_bank_f64(const double *src, long srcNStride, long srcHStride, double *dst,
+                                       long dstNStride, long dstHStride, int n, const int *dims, float maxFreqVal,
+                                       float minFreq, int htk, int numFilter, float sampleRate, int normalize)
+{
+    float maxFreq = (maxFreqVal == 0) ? sampleRate / 2 : maxFreqVal;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < n; b++)
+    {
+        int nfft = (dims[2 * b] - 1) * 2, numBins = nfft / 2 + 1, frames = dims[2 * b + 1];
+        int *interval = (int *)malloc(sizeof(int) * (numBins + 1));
+        float *wd = (float *)malloc(sizeof(float) * (numBins + 1));
+        float *norm = (float *)malloc(sizeof(float) * (numFilter + 1));
+        double *wdD = (double *)malloc(sizeof(double) * (numBins + 1));
+        double *normD = (double *)malloc(sizeof(double) * (numFilter + 1));
+        mel_range r = mel_tables(htk, minFreq, maxFreq, numFilter, sampleRate, normalize, nfft, interval, wd, norm,
+                                 wdD, normD);
+        const double *x = src + (long)b * srcNStride;
+        double *y = dst + (long)b * dstNStride;
+        for (int m = 0; m < numFilter; m++)
+            for (long t = 0; t < frames; t++) y[m * dstHStride + t] = 0.0;
+        for (int bin = r.start; bin < r.end; bin++)
+        {
+            const double *row = x + (long)bin * srcHStride;
+            int up = interval[bin], down = up - 1;
+            if (down >= 0)
+            {
+                double w = normalize ? wdD[bin] * normD[down] : wdD[bin];
+                for (int t = 0; t < frames; t++) y[(long)down * dstHStride + t] += row[t] * w;
+            }
+            if (up >= 0 && up < numFilter)
+            {
+                double w = normalize ? (1.0 - wdD[bin]) * normD[up] : (1.0 - wdD[bin]);
+                for (int t = 0; t < frames; t++) y[(long)up * dstHStride + t] += row[t] * w;
+            }
+        }
+        free(interval); free(wd); free(norm); free(wdD); free(normD);
+    }
+}
+
+/* Exposes the per-sample filter placement (tests compare the GPU-built tables with it). */
+EXPORT void oracle_mel_tables(int htk, float minFreq, float maxFreqVal, int numFilter, float sampleRate,
+                              int normalize, int nfft, int *interval, float *weightsDown, float *norm, int *range)
+{
+    float maxFreq = (maxFreqVal == 0) ? sampleRate / 2 : maxFreqVal;
+    mel_range r = mel_tables(htk, minFreq, maxFreq, numFilter, sampleRate, normalize, nfft, interval, weightsDown,
+                             norm, NULL, NULL);
+    range[0] = r.start;
+    range[1] = r.end;
+}
+
+/* ---------------------------------------------------------------- to_decibels
+ * cpu/kernel/to_decibels.cpp:39-95: minRatio = pow(10, cutOff/mult) (denorm-min if 0),
+ * mult *= log10(2), reference = per-sample max over the ROI when 0, y = mult*log2(max(minRatio,
+ * x*inv)). */
+EXPORT void oracle_to_decibels(const float *src, long srcNStride, long srcHStride, float *dst, long dstNStride,
+                               long dstHStride, int n, const unsigned *dims /* {width,height} pairs */,
+                               float cutOffDB, float multiplier, float referenceMagnitude)
+{
+    float minRatio = (float)pow(10, cutOffDB / multiplier);
+    if (minRatio == 0.0f) minRatio = nextafterf(0.0f, 1.0f);
+    const float log10Factor = 0.3010299956639812;
+    multiplier *= log10Factor;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < n; b++)
+    {
+        const float *x = src + (long)b * srcNStride;
+        float *y = dst + (long)b * dstNStride;
+        unsigned width = dims[2 * b], height = dims[2 * b + 1];
+        float ref = referenceMagnitude;
+        if (!referenceMagnitude)
+        {
+            ref = -FLT_MAX;
+            if (width == 1)
+            {
+                for (unsigned i = 0; i < height; i++) if (x[i] > ref) ref = x[i];
+            }
+            else
+                for (unsigned r = 0; r < height; r++)
+                    for (unsigned c = 0; c < width; c++)
+                        if (x[(long)r * srcHStride + c] > ref) ref = x[(long)r * srcHStride + c];
+        }
+        float inv = ref ? (1.f / ref) : 1.0f;
+        if (width == 1)
+        {
+            for (unsigned i = 0; i < height; i++)
+            {
+                float v = x[i] * inv;
+                y[i] = multiplier * log2f(minRatio < v ? v : minRatio);
+            }
+        }
+        else
+            for (unsigned r = 0; r < height; r++)
+                for (unsigned c = 0; c < width; c++)
+                {
+                    float v = x[(long)r * srcHStride + c] * inv;
+                    y[(long)r * dstHStride + c] = multiplier * log2f(minRatio < v ? v : minRatio);
+                }
+    }
+}
+
+/* FP64 decibels of a 2-D FP64 array per sample ([rows][hStride], rows x cols valid). */
+EXPORT void oracle_to_decibels_f64(const double *src, long nStride, long hStride, double *dst, int n, const int *rows,
+                                   const int *cols, double cutOffDB, double multiplier, double referenceMagnitude)
+{
+    double minRatio = pow(10.0, cutOffDB / multiplier);
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < n; b++)
+    {
+        const double *x = src + (long)b * nStride;
+        double *y = dst + (long)b * nStride;
+        double ref = referenceMagnitude;
+        if (ref == 0.0)
+        {
+            ref = -DBL_MAX;
+            for (int r = 0; r < rows[b]; r++)
+                for (int c = 0; c < cols[b]; c++)
+                    if (x[(long)r * hStride + c] > ref) ref = x[(long)r * hStride + c];
+        }
+        double inv = ref != 0.0 ? 1.0 / ref : 1.0;
+        for (int r = 0; r < rows[b]; r++)
+            for (int c = 0; c < cols[b]; c++)
+            {
+                double v = x[(long)r * hStride + c] * inv;
+                y[(long)r * hStride + c] = multiplier * log10(v > minRatio ? v : minRatio);
+            }
+    }
+}
+
+/* ---------------------------------------------------------------- non-silent region
+ * cpu/kernel/non_silent_region_detection.cpp:105-184: float moving sum of squares restarted
+ * every resetInterval samples, cutoff, first/last index at or above it, begin moved back by
+ * windowLength-1.  `mms` (optional, n x srcStride) receives the moving mean square. */
+EXPORT void oracle_nsr(const float *src, long srcStride, int n, const int *len, int *begin, int *length,
+                       float cutOffDB, int windowLength, float referencePower, int resetInterval, float *mms,
+                       float *cutoffOut)
+{
+    const float cutOff = powf(10.0f, cutOffDB * 0.1f);
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < n; b++)
+    {
+        const float *x = src + (long)b * srcStride;
+        int L = len[b];
+        float *m = (float *)calloc(L > 0 ? L : 1, sizeof(float));
+        int resetLength = (resetInterval == -1) ? L : resetInterval;
+        float meanFactor = 1.0f / windowLength;
+        int windowBegin = -windowLength + 1;
+        for (int outPos = 0; outPos < L;)
+        {
+            float sum = 0.0f;
+            for (int i = windowBegin > 0 ? windowBegin : 0; i < outPos; i++) sum += x[i] * x[i];
+            int end = outPos + resetLength < L ? outPos + resetLength : L;
+            for (; outPos < end; outPos++, windowBegin++)
+            {
+                sum += x[outPos] * x[outPos];
+                m[outPos] = sum * meanFactor;
+                if (windowBegin >= 0) sum -= x[windowBegin] * x[windowBegin];
+            }
+        }
+        float base = referencePower;
+        if (referencePower == 0.0f)
+        {
+            base = L > 0 ? m[0] : 0.f;
+            for (int i = 1; i < L; i++) if (base < m[i]) base = m[i];
+        }
+        float cutOffMag = base * cutOff;
+        int endIdx = L, beginIdx = L, db, de;
+        for (int i = 0; i < endIdx; i++) if (m[i] >= cutOffMag) { beginIdx = i; break; }
+        if (beginIdx == endIdx) { db = 0; de = 0; }
+        else
+        {
+            for (int i = endIdx - 1; i >= beginIdx; i--) if (m[i] >= cutOffMag) { endIdx = i; break; }
+            db = beginIdx;
+            de = endIdx - beginIdx + 1;
+        }
+        if (db != 0 && de != 0)
+        {
+            int nb = db - (windowLength - 1);
+            if (nb < 0) nb = 0;
+            de += db - nb;
+            db = nb;
+        }
+        begin[b] = db;
+        length[b] = de;
+        if (mms) memcpy(mms + (long)b * srcStride, m, sizeof(float) * (size_t)L);
+        if (cutoffOut) cutoffOut[b] = cutOffMag;
+        free(m);
+    }
+}
+
+/* ---------------------------------------------------------------- resampling window
+ * The test suite's caller-side LUT builder, utilities/test_suite/rpp_test_suite_audio.h:390-430
+ * (Hann-windowed sinc, float arithmetic as written there).  lut must hold coeffs + 5 floats;
+ * out[0..2] = scale, center, lobes of the resulting RpptResamplingWindow. */
+static float ts_sinc(float x)
+{
+    x *= M_PI;
+    return (fabsf(x) < 1e-5f) ? (1.f - (x * x * 0.16666667)) : sinf(x) / x;
+}
+
+static double ts_hann(double x) { return 0.5 * (1 + cos(x * M_PI)); }
+
+EXPORT void oracle_windowed_sinc(int coeffs, int lobes, float *lut, float *out)
+{
+    float scale = 2.0f * lobes / (coeffs - 1);
+    float scale_envelope = 2.0f / coeffs;
+    int lookupSize = coeffs + 5;
+    int center = (coeffs - 1) * 0.5f;
+    for (int i = 0; i < lookupSize; i++) lut[i] = 0.f;
+    for (int i = 0; i < coeffs; i++)
+    {
+        float x = (i - center) * scale;
+        float y = (i - center) * scale_envelope;
+        float w = ts_sinc(x) * ts_hann(y);
+        lut[i + 1] = w;
+    }
+    out[0] = 1 / scale;
+    out[1] = center + 1;
+    out[2] = (float)lobes;
+}

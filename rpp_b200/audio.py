@@ -1,0 +1,113 @@
+"""Python front of the B200 audio path, mirroring the reference's rppt_* audio interface.
+
+Each function takes the same arguments as the reference's C entry point (descriptors, per-sample
+tensors, scalars, handle) and returns its RppStatus; tensors are torch CUDA tensors (or pinned /
+host tensors for the per-sample arguments, as the C API allows) or raw integer addresses.  The
+call goes straight through the C ABI of librppb.so (rpp_b200/lib.py); nothing here computes.
+"""
+import ctypes
+
+from . import lib as _lib
+from .types import RpptImagePatch, RpptResamplingWindow, RppStatus
+
+
+def _addr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if isinstance(t, ctypes.Array):
+        return ctypes.addressof(t)
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    if hasattr(t, "ctypes"):
+        return t.ctypes.data
+    raise TypeError(f"cannot take the address of {type(t)}")
+
+
+def _h(handle):
+    return handle.value if hasattr(handle, "value") else handle
+
+
+def _status(v):
+    try:
+        return RppStatus(v)
+    except ValueError:
+        return v
+
+
+def non_silent_region_detection(src, src_desc, src_length, detected_index, detection_length, cut_off_db,
+                                window_length, reference_power, reset_interval, handle):
+    L = _lib.load()
+    return _status(L.rppt_non_silent_region_detection_gpu(
+        _addr(src), ctypes.byref(src_desc), _addr(src_length), _addr(detected_index), _addr(detection_length),
+        float(cut_off_db), int(window_length), float(reference_power), int(reset_interval), _h(handle)))
+
+
+def to_decibels(src, src_desc, dst, dst_desc, src_dims, cut_off_db, multiplier, reference_magnitude, handle):
+    L = _lib.load()
+    return _status(L.rppt_to_decibels_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                          _addr(src_dims), float(cut_off_db), float(multiplier),
+                                          float(reference_magnitude), _h(handle)))
+
+
+def pre_emphasis_filter(src, src_desc, dst, dst_desc, src_length, coeff, border_type, handle):
+    L = _lib.load()
+    return _status(L.rppt_pre_emphasis_filter_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst),
+                                                  ctypes.byref(dst_desc), _addr(src_length), _addr(coeff),
+                                                  int(border_type), _h(handle)))
+
+
+def down_mixing(src, src_desc, dst, dst_desc, src_dims, normalize_weights, handle):
+    L = _lib.load()
+    return _status(L.rppt_down_mixing_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                          _addr(src_dims), bool(normalize_weights), _h(handle)))
+
+
+def spectrogram(src, src_desc, dst, dst_desc, src_length, center_windows, reflect_padding, window_function, nfft,
+                power, window_length, window_step, handle):
+    L = _lib.load()
+    return _status(L.rppt_spectrogram_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                          _addr(src_length), bool(center_windows), bool(reflect_padding),
+                                          _addr(window_function), int(nfft), int(power), int(window_length),
+                                          int(window_step), _h(handle)))
+
+
+def mel_filter_bank(src, src_desc, dst, dst_desc, src_dims, max_freq, min_freq, mel_formula, num_filter,
+                    sample_rate, normalize, handle):
+    L = _lib.load()
+    return _status(L.rppt_mel_filter_bank_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                              _addr(src_dims), float(max_freq), float(min_freq), int(mel_formula),
+                                              int(num_filter), float(sample_rate), bool(normalize), _h(handle)))
+
+
+def resampling_window(lut, scale, center, lobes, coeffs=None):
+    """RpptResamplingWindow whose lookupPinned points at `lut` (a torch tensor, pinned or device,
+    or a host array kept alive by the caller)."""
+    w = RpptResamplingWindow()
+    w.scale = float(scale)
+    w.center = float(center)
+    w.lobes = int(lobes)
+    w.coeffs = int(coeffs if coeffs is not None else len(lut) - 5)
+    w.lookupSize = int(len(lut))
+    w.lookupPinned = _addr(lut)
+    for i in range(4):
+        w.pCenter[i] = w.center
+        w.pScale[i] = w.scale
+    return w
+
+
+def resample(src, src_desc, dst, dst_desc, in_rate, out_rate, src_dims, window, handle):
+    L = _lib.load()
+    return _status(L.rppt_resample_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                       _addr(in_rate), _addr(out_rate), _addr(src_dims), ctypes.byref(window),
+                                       _h(handle)))
+
+
+def image_patches(widths, heights):
+    """Host array of RpptImagePatch {width, height} (keep it alive during the call)."""
+    arr = (RpptImagePatch * len(widths))()
+    for i, (w, h) in enumerate(zip(widths, heights)):
+        arr[i].width = int(w)
+        arr[i].height = int(h)
+    return arr

@@ -1,0 +1,105 @@
+// Device helpers shared by the audio kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace rppb {
+
+// ---------------------------------------------------------------- ragged batches
+// A batch of uneven samples is addressed as one flat list of work units (chunks, frame tiles,
+// reset blocks ...).  prefix[b] is the number of units of samples 0..b-1 (prefix[n] = total),
+// computed on the device from the per-sample tensors, so no call reads lengths on the host.
+
+// Largest b in [0, n) with prefix[b] <= w (w < prefix[n]); empty samples are skipped.
+__device__ __forceinline__ int ragged_find(const long long* __restrict__ prefix, int n, long long w)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One CTA of 1024 threads: prefix[0..n] = exclusive scan of count(b).
+template <class Count>
+__global__ void __launch_bounds__(1024) ragged_prefix_kernel(Count count, int n, long long* __restrict__ prefix)
+{
+    __shared__ long long part[1024];
+    const int t = threadIdx.x;
+    const int per = (n + 1023) / 1024;
+    const int b0 = t * per, b1 = min(n, b0 + per);
+    long long s = 0;
+    for (int b = b0; b < b1; ++b) s += count(b);
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1)
+    {
+        long long v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    long long run = t ? part[t - 1] : 0;
+    for (int b = b0; b < b1; ++b)
+    {
+        prefix[b] = run;
+        run += count(b);
+    }
+    if (t == 1023) prefix[n] = part[1023];
+}
+
+template <class Count>
+inline void launch_ragged_prefix(Count count, int n, long long* prefix, cudaStream_t s)
+{
+    ragged_prefix_kernel<Count><<<1, 1024, 0, s>>>(count, n, prefix);
+}
+
+// ---------------------------------------------------------------- float helpers
+// Monotone map of float to uint32 so that atomicMax on the key is a float max (NaN excluded).
+__device__ __forceinline__ unsigned float_key(float f)
+{
+    unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(unsigned k)
+{
+    unsigned u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+__device__ __forceinline__ float warp_max(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Reflect an out-of-range index into [minLoc, maxLoc) the way the reference does
+// (src/modules/tensor/cpu/kernel/spectrogram.cpp:55-69): mirror without repeating the edge,
+// repeatedly for short signals; a signal shorter than 2 maps everything to its last sample.
+__device__ __forceinline__ int reflect_index(int loc, int minLoc, int maxLoc)
+{
+    if (maxLoc - minLoc < 2) return maxLoc - 1;
+    for (int guard = 0; guard < 64; ++guard)
+    {
+        if (loc < minLoc) loc = 2 * minLoc - loc;
+        else if (loc >= maxLoc) loc = 2 * maxLoc - 2 - loc;
+        else break;
+    }
+    return loc;
+}
+
+// Frames of a sample (spectrogram.cpp:47-52), never negative.
+__host__ __device__ __forceinline__ int num_windows(int length, int windowLength, int windowStep, bool center)
+{
+    if (!center) length -= windowLength;
+    int f = length / windowStep + 1;
+    return f < 0 ? 0 : f;
+}
+
+}  // namespace rppb

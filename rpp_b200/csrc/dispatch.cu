@@ -1,0 +1,383 @@
+// The seven rppt_*_gpu entry points of include/rppt_tensor_audio_augmentations.h.
+//
+// Argument checks follow the reference's GPU dispatch
+// (src/modules/tensor/rppt_tensor_audio_augmentations.cpp:332-629) in the same order and with
+// the same status codes.  Beyond those, inputs on which the reference would crash, hang or write
+// out of bounds return RPP_ERROR_INVALID_ARGUMENTS (null pointers, non-positive window or step,
+// resetInterval 0, nfft smaller than the window).  Scalars the reference derives on the host
+// (decibel minRatio and log10 factor, NSR cutoff) are derived here with the same float/double
+// expressions.  Per-sample tensors are resolved to device addresses (device and pinned pointers
+// are used in place; pageable ones are staged into the workspace), then the launchers of
+// rpp_b200/csrc/*.cu enqueue the kernels on the handle stream.  Nothing here synchronizes the
+// stream except a pageable NSR output, whose device-to-host copy is stream-ordered.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "../../include/rppt_tensor_audio_augmentations.h"
+#include "handle.hpp"
+#include "ops.hpp"
+
+namespace rppb {
+const float2* spectrogram_twiddles(Handle& h, int nfft);
+}
+
+using namespace rppb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+RppStatus guarded(rppHandle_t handle, F&& body)
+{
+    try
+    {
+        Handle& h = deref(handle);
+        h.begin_call();
+        RppStatus st = body(h);
+        if (st == RPP_SUCCESS) h.end_call();
+        return st;
+    }
+    catch (const Error& e)
+    {
+        g_last_error = e.what;
+        return e.status;
+    }
+    catch (const std::bad_alloc&)
+    {
+        g_last_error = "host allocation failed";
+        return RPP_ERROR_NOT_ENOUGH_MEMORY;
+    }
+    catch (...)
+    {
+        g_last_error = "unknown error";
+        return RPP_ERROR;
+    }
+}
+
+inline bool is_f32(const RpptDesc* d) { return d->dataType == F32; }
+
+void require(bool cond, const char* what)
+{
+    if (!cond) fail(RPP_ERROR_INVALID_ARGUMENTS, what);
+}
+
+void build_hann(float* out, size_t count, const void*)
+{
+    // spectrogram.cpp:36-44: 0.5 * (1 - cos(2*pi*(t + 0.5) / W)) in FP64, rounded to float
+    const double a = (2.0 * M_PI) / double(count);
+    for (size_t t = 0; t < count; ++t) out[t] = float(0.5 * (1.0 - std::cos(a * (double(t) + 0.5))));
+}
+
+}  // namespace
+
+extern "C" SHARED_PUBLIC const char* rppbGetLastError() { return g_last_error.c_str(); }
+
+extern "C" SHARED_PUBLIC RppStatus rppt_pre_emphasis_filter_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                                RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor,
+                                                                Rpp32f* coeffTensor, RpptAudioBorderType borderType,
+                                                                rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        if (srcDescPtr->numDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr, "null tensor");
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        Carver m(nullptr);
+        m.take<int>(n);
+        m.take<float>(n);
+        m.take<char>(prefix_bytes(n));
+        Carver cv(h.workspace(m.used()));
+        int* lenStage = cv.take<int>(n);
+        float* coeffStage = cv.take<float>(n);
+        void* scratch = cv.take<char>(prefix_bytes(n));
+        const int* len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
+        const float* coeff = static_cast<const float*>(h.device_view(coeffTensor, n * sizeof(float), coeffStage));
+        launch_pre_emphasis(h, scratch, static_cast<const float*>(srcPtr), srcDescPtr->strides.nStride,
+                            static_cast<float*>(dstPtr), dstDescPtr->strides.nStride, n, len, coeff, int(borderType),
+                            size_t(n) * srcDescPtr->strides.nStride);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppt_down_mixing_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                        RpptDescPtr dstDescPtr, Rpp32s* srcDimsTensor,
+                                                        bool normalizeWeights, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        const Rpp32u tensorDims = Rpp32u(srcDescPtr->numDims - 1);
+        if (tensorDims != 1 && tensorDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr, "null tensor");
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        Carver m(nullptr);
+        m.take<int>(2 * n);
+        m.take<char>(prefix_bytes(n));
+        Carver cv(h.workspace(m.used()));
+        int* dimsStage = cv.take<int>(2 * n);
+        void* scratch = cv.take<char>(prefix_bytes(n));
+        const int* dims = static_cast<const int*>(h.device_view(srcDimsTensor, 2 * n * sizeof(int), dimsStage));
+        launch_down_mixing(h, scratch, static_cast<const float*>(srcPtr), srcDescPtr->strides.nStride,
+                           static_cast<float*>(dstPtr), dstDescPtr->strides.nStride, n, dims, normalizeWeights);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppt_to_decibels_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                        RpptDescPtr dstDescPtr, RpptImagePatchPtr srcDims,
+                                                        Rpp32f cutOffDB, Rpp32f multiplier,
+                                                        Rpp32f referenceMagnitude, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        const Rpp32u tensorDims = Rpp32u(srcDescPtr->numDims - 1);
+        if (tensorDims != 1 && tensorDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (!multiplier) return RPP_ERROR_ZERO_DIVISION;
+        if (!is_f32(srcDescPtr)) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr, "null tensor");
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        // to_decibels.cpp:40-45
+        float minRatio = float(std::pow(10, cutOffDB / multiplier));
+        if (minRatio == 0.0f) minRatio = std::nextafter(0.0f, 1.0f);
+        const Rpp32f log10Factor = 0.3010299956639812;
+        multiplier *= log10Factor;
+        Carver m(nullptr);
+        m.take<uint32_t>(2 * n);
+        m.take<char>(to_decibels_scratch_bytes(n));
+        Carver cv(h.workspace(m.used()));
+        uint32_t* dimsStage = cv.take<uint32_t>(2 * n);
+        void* scratch = cv.take<char>(to_decibels_scratch_bytes(n));
+        DecibelArgs a;
+        a.src = static_cast<const float*>(srcPtr);
+        a.srcNStride = srcDescPtr->strides.nStride;
+        a.srcHStride = srcDescPtr->strides.hStride;
+        a.dst = static_cast<float*>(dstPtr);
+        a.dstNStride = dstDescPtr->strides.nStride;
+        a.dstHStride = dstDescPtr->strides.hStride;
+        a.n = n;
+        a.dims = static_cast<const uint32_t*>(h.device_view(srcDims, 2 * n * sizeof(uint32_t), dimsStage));
+        a.minRatio = minRatio;
+        a.multiplier = multiplier;
+        a.referenceMagnitude = referenceMagnitude;
+        launch_to_decibels(h, scratch, a);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppt_non_silent_region_detection_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr,
+                                                                        Rpp32s* srcLengthTensor,
+                                                                        Rpp32s* detectedIndexTensor,
+                                                                        Rpp32s* detectionLengthTensor, Rpp32f cutOffDB,
+                                                                        Rpp32s windowLength, Rpp32f referencePower,
+                                                                        Rpp32s resetInterval, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr != nullptr, "null descriptor");
+        const Rpp32u tensorDims = Rpp32u(srcDescPtr->numDims - 1);
+        if (tensorDims != 1) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (!is_f32(srcDescPtr)) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && detectedIndexTensor && detectionLengthTensor, "null tensor");
+        require(windowLength > 0, "windowLength must be positive");
+        require(resetInterval == -1 || resetInterval > 0, "resetInterval must be -1 or positive");
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        const uint32_t stride = srcDescPtr->strides.nStride;
+        const size_t scratchBytes = nsr_scratch_bytes(n, stride, resetInterval);
+        Carver m(nullptr);
+        m.take<int>(n);
+        m.take<int>(2 * n);
+        m.take<char>(scratchBytes);
+        Carver cv(h.workspace(m.used()));
+        int* lenStage = cv.take<int>(n);
+        int* outStage = cv.take<int>(2 * n);
+        void* scratch = cv.take<char>(scratchBytes);
+        NsrArgs a;
+        a.src = static_cast<const float*>(srcPtr);
+        a.srcStride = stride;
+        a.n = n;
+        a.len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
+        void* dBegin = nullptr;
+        void* dLength = nullptr;
+        const bool directBegin = h.device_writable(detectedIndexTensor, &dBegin);
+        const bool directLength = h.device_writable(detectionLengthTensor, &dLength);
+        a.begin = directBegin ? static_cast<int*>(dBegin) : outStage;
+        a.length = directLength ? static_cast<int*>(dLength) : outStage + n;
+        a.cutOff = std::pow(10.0f, cutOffDB * 0.1f);   // non_silent_region_detection.cpp:105
+        a.windowLength = windowLength;
+        a.referencePower = referencePower;
+        a.resetInterval = resetInterval;
+        launch_nsr(h, scratch, a);
+        if (!directBegin)
+            check_cuda(cudaMemcpyAsync(detectedIndexTensor, outStage, n * sizeof(int), cudaMemcpyDeviceToHost,
+                                       h.stream()),
+                       "copy NSR begin");
+        if (!directLength)
+            check_cuda(cudaMemcpyAsync(detectionLengthTensor, outStage + n, n * sizeof(int), cudaMemcpyDeviceToHost,
+                                       h.stream()),
+                       "copy NSR length");
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppt_spectrogram_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                        RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor,
+                                                        bool centerWindows, bool reflectPadding,
+                                                        Rpp32f* windowFunction, Rpp32s nfft, Rpp32s power,
+                                                        Rpp32s windowLength, Rpp32s windowStep, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        if ((dstDescPtr->layout != NFT) && (dstDescPtr->layout != NTF)) return RPP_ERROR_INVALID_DST_LAYOUT;
+        const Rpp32u srcTensorDims = Rpp32u(srcDescPtr->numDims - 1);
+        const Rpp32u dstTensorDims = Rpp32u(dstDescPtr->numDims - 1);
+        if (srcTensorDims != 1) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (dstTensorDims != 2) return RPP_ERROR_INVALID_DST_DIMS;
+        if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr, "null tensor");
+        require(windowLength > 0 && windowStep > 0, "windowLength and windowStep must be positive");
+        if (nfft == 0) nfft = windowLength;   // spectrogram.cpp:88
+        require(nfft >= windowLength, "nfft must be at least windowLength");
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        // bins must fit the destination (the reference writes them unchecked)
+        const Rpp32u binsCap = dstDescPtr->layout == NFT ? dstDescPtr->h : dstDescPtr->w;
+        if (binsCap < Rpp32u(nfft / 2 + 1) || dstDescPtr->strides.hStride < (dstDescPtr->layout == NFT ? dstDescPtr->w : Rpp32u(nfft / 2 + 1)))
+            return RPP_ERROR_INVALID_DST_DIMS;
+        Carver m(nullptr);
+        m.take<int>(n);
+        m.take<float>(windowFunction ? windowLength : 0);
+        m.take<char>(prefix_bytes(n));
+        Carver cv(h.workspace(m.used()));
+        int* lenStage = cv.take<int>(n);
+        float* winStage = cv.take<float>(windowFunction ? windowLength : 0);
+        void* scratch = cv.take<char>(prefix_bytes(n));
+        SpectrogramArgs a;
+        a.src = static_cast<const float*>(srcPtr);
+        a.srcStride = srcDescPtr->strides.nStride;
+        a.dst = static_cast<float*>(dstPtr);
+        a.dstNStride = dstDescPtr->strides.nStride;
+        a.dstHStride = dstDescPtr->strides.hStride;
+        a.nft = dstDescPtr->layout == NFT;
+        a.n = n;
+        a.len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
+        a.center = centerWindows;
+        a.reflect = reflectPadding;
+        if (windowFunction)
+        {
+            // the reference reads the window on the host and copies it (hip/kernel/spectrogram.cpp:264-277)
+            h.upload(winStage, windowFunction, windowLength * sizeof(float));
+            a.window = winStage;
+        }
+        else
+        {
+            a.window = h.table("hann" + std::to_string(windowLength), size_t(windowLength), build_hann, nullptr);
+        }
+        a.nfft = nfft;
+        a.power = power;
+        a.windowLength = windowLength;
+        a.windowStep = windowStep;
+        a.maxFrames = int(a.nft ? dstDescPtr->w : dstDescPtr->h);
+        launch_spectrogram(h, scratch, a);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppt_mel_filter_bank_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                            RpptDescPtr dstDescPtr, Rpp32s* srcDimsTensor,
+                                                            Rpp32f maxFreq, Rpp32f minFreq,
+                                                            RpptMelScaleFormula melFormula, Rpp32s numFilter,
+                                                            Rpp32f sampleRate, bool normalize, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        const Rpp32u tensorDims = Rpp32u(srcDescPtr->numDims - 1);
+        if (tensorDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (srcDescPtr->layout != NFT) return RPP_ERROR_INVALID_SRC_LAYOUT;
+        if (dstDescPtr->layout != NFT) return RPP_ERROR_INVALID_DST_LAYOUT;
+        if (maxFreq < 0 || maxFreq > sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
+        if (minFreq < 0 || minFreq > sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
+        if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr, "null tensor");
+        require(numFilter > 0, "numFilter must be positive");
+        if (dstDescPtr->h < Rpp32u(numFilter)) return RPP_ERROR_INVALID_DST_DIMS;
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        Carver m(nullptr);
+        m.take<int>(2 * n);
+        m.take<char>(prefix_bytes(n));
+        Carver cv(h.workspace(m.used()));
+        int* dimsStage = cv.take<int>(2 * n);
+        void* scratch = cv.take<char>(prefix_bytes(n));
+        MelArgs a;
+        a.src = static_cast<const float*>(srcPtr);
+        a.srcNStride = srcDescPtr->strides.nStride;
+        a.srcHStride = srcDescPtr->strides.hStride;
+        a.dst = static_cast<float*>(dstPtr);
+        a.dstNStride = dstDescPtr->strides.nStride;
+        a.dstHStride = dstDescPtr->strides.hStride;
+        a.n = n;
+        a.dims = static_cast<const int*>(h.device_view(srcDimsTensor, 2 * n * sizeof(int), dimsStage));
+        a.srcRows = srcDescPtr->h;
+        a.maxFreq = maxFreq;
+        a.minFreq = minFreq;
+        a.htk = melFormula == HTK ? 1 : 0;
+        a.numFilter = numFilter;
+        a.sampleRate = sampleRate;
+        a.normalize = normalize;
+        launch_mel_filter_bank(h, scratch, a);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppt_resample_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                     RpptDescPtr dstDescPtr, Rpp32f* inRateTensor,
+                                                     Rpp32f* outRateTensor, Rpp32s* srcDimsTensor,
+                                                     RpptResamplingWindow& window, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        const Rpp32u tensorDims = Rpp32u(srcDescPtr->numDims - 1);
+        if (tensorDims != 1 && tensorDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (!is_f32(srcDescPtr)) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr, "null tensor");
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        const float* lutHost = window.lookupPinned ? window.lookupPinned : window.lookup.data();
+        const int lutSize = window.lookupSize;
+        require(lutHost != nullptr && lutSize >= 2, "resampling window has no lookup table");
+        require(window.lookupPinned != nullptr || int(window.lookup.size()) >= lutSize, "lookup shorter than lookupSize");
+        require(window.lobes >= 0, "negative lobes");
+        require(size_t(lutSize) * sizeof(float) <= 200 * 1024, "lookup table above 200 KB");
+        Carver m(nullptr);
+        m.take<float>(n);
+        m.take<float>(n);
+        m.take<int>(2 * n);
+        m.take<float>(lutSize);
+        m.take<char>(prefix_bytes(n));
+        Carver cv(h.workspace(m.used()));
+        float* inStage = cv.take<float>(n);
+        float* outStage = cv.take<float>(n);
+        int* dimsStage = cv.take<int>(2 * n);
+        float* lutStage = cv.take<float>(lutSize);
+        void* scratch = cv.take<char>(prefix_bytes(n));
+        ResampleWindowDev win;
+        win.lut = static_cast<const float*>(h.device_view(lutHost, lutSize * sizeof(float), lutStage));
+        win.lutSize = lutSize;
+        win.scale = window.scale;
+        win.center = window.center;
+        win.lobes = window.lobes;
+        launch_resample(h, scratch, static_cast<const float*>(srcPtr), srcDescPtr->strides.nStride,
+                        static_cast<float*>(dstPtr), dstDescPtr->strides.nStride, n,
+                        static_cast<const float*>(h.device_view(inRateTensor, n * sizeof(float), inStage)),
+                        static_cast<const float*>(h.device_view(outRateTensor, n * sizeof(float), outStage)),
+                        static_cast<const int*>(h.device_view(srcDimsTensor, 2 * n * sizeof(int), dimsStage)), win);
+        return RPP_SUCCESS;
+    });
+}

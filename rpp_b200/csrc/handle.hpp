@@ -1,0 +1,127 @@
+// Internal handle of the B200 audio path (behind the opaque rppHandle_t of include/rpp.h).
+//
+// Plays the role of the reference's rpp::Handle (src/include/common/handle.hpp:63-180,
+// src/modules/handle_hip.cpp:100-240) with a different memory model: instead of a fixed
+// 1.49 GB device scratch and an 8.3 M-float pinned scratch allocated at creation
+// (handle_hip.cpp:216-234), the workspace is sized from each call and grows on demand, so
+// there is no scratch cap and no RPP_ERROR_OUT_OF_BOUND_SCRATCH_MEMORY_SIZE.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rpp.h"
+
+namespace rppb {
+
+// Thrown inside the library and converted to a status code at the C boundary.
+struct Error
+{
+    RppStatus status;
+    std::string what;
+};
+
+[[noreturn]] void fail(RppStatus status, const std::string& what);
+void check_cuda(cudaError_t err, const char* what);
+
+// Bump allocator over one workspace block: measure with base == nullptr, then carve.
+class Carver
+{
+  public:
+    explicit Carver(void* base) : base_(static_cast<char*>(base)) {}
+    template <class T>
+    T* take(size_t count)
+    {
+        size_t off = (used_ + 255) & ~size_t(255);
+        used_ = off + count * sizeof(T);
+        return base_ ? reinterpret_cast<T*>(base_ + off) : nullptr;
+    }
+    size_t used() const { return (used_ + 255) & ~size_t(255); }
+
+  private:
+    char* base_;
+    size_t used_ = 0;
+};
+
+class Handle
+{
+  public:
+    Handle(size_t batchSize, cudaStream_t stream);
+    ~Handle();
+
+    cudaStream_t stream() const { return stream_; }
+    void set_stream(cudaStream_t s) { stream_ = s; }
+    size_t batch_size() const { return batch_; }
+    void set_batch_size(size_t b) { batch_ = b; }
+    int device() const { return device_; }
+    int num_sms() const { return num_sms_; }
+
+    // Device workspace valid for the current call; contents are undefined on entry.
+    void* workspace(size_t bytes);
+
+    // Makes a per-sample tensor readable by kernels.  Device, managed and pinned pointers are
+    // returned as device addresses; pageable host memory is copied through pinned staging into
+    // the workspace region `dst` (which must hold `bytes`).
+    const void* device_view(const void* p, size_t bytes, void* dst);
+    // True when the device can write `p` directly (device, managed or pinned memory).
+    bool device_writable(const void* p, void** devicePtr);
+
+    // Cached device tables keyed by a string (window functions, twiddles).  The host builder
+    // fills `host` once; the table is uploaded and kept until the handle is destroyed.
+    const float* table(const std::string& key, size_t count, void (*build)(float*, size_t, const void*),
+                       const void* ctx);
+    // Uploads `bytes` of host data to a device region that stays valid for this call.
+    void upload(void* dDst, const void* hSrc, size_t bytes);
+
+    void set_allocator(rppAllocatorFunction a, rppDeallocatorFunction d, void* ctx);
+
+    // Profiling (rppEnableProfiling / rppGetKernelTime).
+    void enable_profiling(bool on);
+    void begin_call();
+    void end_call();
+    float last_call_ms();
+
+    // Scratch of size `bytes` in pinned host memory, reused after the previous user's copy ended.
+    void* staging(size_t bytes);
+    void staging_done();
+
+  private:
+    void* dev_alloc(size_t bytes);
+    void dev_free(void* p);
+
+    int device_ = 0;
+    int num_sms_ = 148;
+    cudaStream_t stream_ = nullptr;
+    size_t batch_ = 1;
+
+    void* ws_ = nullptr;
+    size_t ws_bytes_ = 0;
+
+    void* pinned_ = nullptr;
+    size_t pinned_bytes_ = 0;
+    cudaEvent_t pinned_free_ = nullptr;
+    bool pinned_pending_ = false;
+
+    std::map<std::string, void*> tables_;
+
+    rppAllocatorFunction alloc_fn_ = nullptr;
+    rppDeallocatorFunction free_fn_ = nullptr;
+    void* alloc_ctx_ = nullptr;
+
+    bool profiling_ = false;
+    cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
+    bool timed_ = false;
+};
+
+Handle& deref(rppHandle_t h);
+
+// Number of CTAs for a persistent launch of `kernel` with `threads` threads and `smem` bytes.
+int persistent_grid(const Handle& h, const void* kernel, int threads, size_t smem);
+
+}  // namespace rppb

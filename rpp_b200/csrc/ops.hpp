@@ -1,0 +1,94 @@
+// Launchers of the audio kernels.  Every pointer is a device address (per-sample tensors are
+// already resolved by the dispatch layer); every launch goes on h.stream().  Each launcher takes
+// a device `scratch` region of at least <op>_scratch_bytes(...) bytes, carved by the dispatch
+// layer out of the handle workspace.
+#pragma once
+
+#include "handle.hpp"
+
+namespace rppb {
+
+inline size_t prefix_bytes(int n) { return size_t(n + 1) * sizeof(long long); }
+
+void launch_pre_emphasis(Handle& h, void* scratch, const float* src, uint32_t srcStride, float* dst,
+                         uint32_t dstStride, int n, const int* len, const float* coeff, int border, size_t srcElems);
+
+void launch_down_mixing(Handle& h, void* scratch, const float* src, uint32_t srcStride, float* dst,
+                        uint32_t dstStride, int n, const int* dims, bool normalize);
+
+struct ResampleWindowDev
+{
+    const float* lut;
+    int lutSize;
+    float scale, center;
+    int lobes;
+};
+void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStride, float* dst, uint32_t dstStride, int n,
+                     const float* inRate, const float* outRate, const int* dims, const ResampleWindowDev& win);
+
+struct SpectrogramArgs
+{
+    const float* src;
+    uint32_t srcStride;
+    float* dst;
+    uint32_t dstNStride, dstHStride;
+    bool nft;
+    int n;
+    const int* len;
+    bool center, reflect;
+    const float* window;   // device, windowLength floats
+    int nfft, power, windowLength, windowStep;
+    int maxFrames;         // frames the dst descriptor holds per sample
+};
+void launch_spectrogram(Handle& h, void* scratch, const SpectrogramArgs& a);
+
+struct MelArgs
+{
+    const float* src;
+    uint32_t srcNStride, srcHStride;
+    float* dst;
+    uint32_t dstNStride, dstHStride;
+    int n;
+    const int* dims;       // {bins, frames} per sample
+    uint32_t srcRows;      // bins the src descriptor holds per sample
+    float maxFreq, minFreq;
+    int htk;
+    int numFilter;
+    float sampleRate;
+    bool normalize;
+};
+void launch_mel_filter_bank(Handle& h, void* scratch, const MelArgs& a);
+
+struct DecibelArgs
+{
+    const float* src;
+    uint32_t srcNStride, srcHStride;
+    float* dst;
+    uint32_t dstNStride, dstHStride;
+    int n;
+    const uint32_t* dims;  // {width, height} per sample
+    float minRatio;        // pow(10, cutOffDB / multiplier), denorm-min when 0
+    float multiplier;      // multiplier * log10(2)
+    float referenceMagnitude;
+};
+inline size_t to_decibels_scratch_bytes(int n) { return prefix_bytes(n) + 256 + size_t(n) * sizeof(unsigned); }
+void launch_to_decibels(Handle& h, void* scratch, const DecibelArgs& a);
+
+struct NsrArgs
+{
+    const float* src;
+    uint32_t srcStride;
+    int n;
+    const int* len;
+    int* begin;            // device-writable
+    int* length;
+    float cutOff;          // powf(10, cutOffDB * 0.1f)
+    int windowLength;
+    float referencePower;
+    int resetInterval;
+};
+// Moving-mean-square buffer (srcStride floats per sample), per-reset-block maxima and the prefix.
+size_t nsr_scratch_bytes(int n, uint32_t srcStride, int resetInterval);
+void launch_nsr(Handle& h, void* scratch, const NsrArgs& a);
+
+}  // namespace rppb

@@ -1,0 +1,192 @@
+// resample: band-limited interpolation with the caller's windowed-sinc lookup table.
+//
+// Reference: src/modules/tensor/cpu/kernel/resample.cpp:46-141 and RpptResamplingWindow
+// (api/rppdefs.h:751-790).  Output length ceil(length * outRate / inRate) (float arithmetic);
+// equal rates copy.  Outputs go in blocks of 256: a block's origin in the input is FP64
+// (outBlock * inRate/outRate), split into an integer sample and a float phase, and the phase
+// advances by the float ratio once per output — a sequential float sum the GPU replays in the
+// same order.  Output j sums input samples [ceil(phase) - lobes, ceil(phase) + lobes) clipped to
+// the signal, each weighted by linear interpolation in the table at x * scale + center.  For
+// mono input the reference sums 4 lanes (SSE; truncating table index) and folds them as
+// (l0 + l2) + (l1 + l3) before a scalar tail (flooring, clamped index); multi-channel input is
+// summed per channel in order.  Every product and sum is explicitly rounded, so outputs are
+// bit-identical to the host path.
+//
+// One CTA per 256-output block: thread 0 replays the phase sum into shared memory while the
+// others stage the table; then one output per thread.  Inputs are read through L1 (neighbouring
+// outputs share taps).  Compute-bound: 2 * lobes taps of ~10 float operations per output.
+#include "common.cuh"
+#include "ops.hpp"
+
+namespace rppb {
+namespace {
+
+constexpr int kBlock = 256;        // outputs per block (the reference's block size)
+constexpr int kCopyChunk = 4096;   // floats per unit of an equal-rate copy
+
+__device__ __forceinline__ int out_length(int L, float inRate, float outRate)
+{
+    return int(ceilf(__fdiv_rn(__fmul_rn(float(L), outRate), inRate)));
+}
+
+struct ResampleCount
+{
+    const float* inRate;
+    const float* outRate;
+    const int* dims;
+    __device__ long long operator()(int b) const
+    {
+        const int L = dims[2 * b], C = dims[2 * b + 1];
+        if (L <= 0 || C <= 0) return 0;
+        if (inRate[b] == outRate[b]) return ((long long)L * C + kCopyChunk - 1) / kCopyChunk;
+        const int outEnd = out_length(L, inRate[b], outRate[b]);
+        return outEnd <= 0 ? 0 : (outEnd + kBlock - 1) / kBlock;
+    }
+};
+
+struct Win
+{
+    const float* lut;   // shared memory
+    int lutSize;
+    float scale, center;
+
+    // rppdefs.h:771-782: truncating index (the SSE lanes)
+    __device__ __forceinline__ float lane(float x) const
+    {
+        const float locRaw = __fadd_rn(__fmul_rn(x, scale), center);
+        int idx = int(locRaw);
+        const float weight = __fsub_rn(locRaw, float(idx));
+        idx = min(max(idx, 0), lutSize - 2);
+        const float cur = lut[idx], nxt = lut[idx + 1];
+        return __fadd_rn(cur, __fmul_rn(weight, __fsub_rn(nxt, cur)));
+    }
+    // rppdefs.h:760-769: floor, clamped index (the scalar tail and the multi-channel path)
+    __device__ __forceinline__ float scalar(float x) const
+    {
+        const float locRaw = __fadd_rn(__fmul_rn(x, scale), center);
+        int idx = int(floorf(locRaw));
+        const float weight = __fsub_rn(locRaw, float(idx));
+        idx = min(max(idx, 0), lutSize - 2);
+        const float cur = lut[idx], nxt = lut[idx + 1];
+        return __fadd_rn(cur, __fmul_rn(weight, __fsub_rn(nxt, cur)));
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restrict__ src, uint32_t srcStride,
+                                                          float* __restrict__ dst, uint32_t dstStride,
+                                                          const float* __restrict__ inRateT,
+                                                          const float* __restrict__ outRateT,
+                                                          const int* __restrict__ dims, ResampleWindowDev wd,
+                                                          const long long* __restrict__ prefix, int n)
+{
+    extern __shared__ float s_lut[];
+    __shared__ float s_phase[kBlock];
+    for (int i = threadIdx.x; i < wd.lutSize; i += blockDim.x) s_lut[i] = wd.lut[i];
+    __syncthreads();
+    const Win win{s_lut, wd.lutSize, wd.scale, wd.center};
+    const int lobes = wd.lobes;
+    const long long total = prefix[n];
+    for (long long w = blockIdx.x; w < total; w += gridDim.x)
+    {
+        const int b = ragged_find(prefix, n, w);
+        const int unit = int(w - prefix[b]);
+        const int L = dims[2 * b], C = dims[2 * b + 1];
+        const float inRate = inRateT[b], outRate = outRateT[b];
+        const float* x = src + size_t(b) * srcStride;
+        float* y = dst + size_t(b) * dstStride;
+        if (inRate == outRate)
+        {
+            const long long count = min((long long)L * C, (long long)min(srcStride, dstStride));
+            for (long long i = (long long)unit * kCopyChunk + threadIdx.x; i < min(count, (long long)(unit + 1) * kCopyChunk);
+                 i += blockDim.x)
+                y[i] = x[i];
+            continue;
+        }
+        const int outEnd = min(out_length(L, inRate, outRate), int(dstStride / uint32_t(C)));   // stay inside dst
+        const double scale = __ddiv_rn(double(inRate), double(outRate));
+        const float fscale = __double2float_rn(scale);
+        const int outBlock = unit * kBlock;
+        const double inBlockRaw = __dmul_rn(double(outBlock), scale);
+        const int inBlockRounded = int(inBlockRaw);
+        if (threadIdx.x == 0)
+        {
+            float p = __double2float_rn(__dsub_rn(inBlockRaw, double(inBlockRounded)));
+            for (int k = 0; k < kBlock; ++k)
+            {
+                s_phase[k] = p;
+                p = __fadd_rn(p, fscale);
+            }
+        }
+        __syncthreads();
+        const int outPos = outBlock + threadIdx.x;
+        if (outPos < outEnd)
+        {
+            const float inPos = s_phase[threadIdx.x];
+            const int xc = int(ceilf(inPos));
+            int loc0 = xc - lobes, loc1 = xc + lobes;
+            if (loc0 + inBlockRounded < 0) loc0 = -inBlockRounded;
+            if (loc1 + inBlockRounded > L) loc1 = L - inBlockRounded;
+            const float* in = x + (long long)inBlockRounded * C;
+            if (C == 1)
+            {
+                int l = loc0;
+                const float locBegin = __fsub_rn(float(l), inPos);
+                float lane[4] = {__fadd_rn(locBegin, 0.f), __fadd_rn(locBegin, 1.f), __fadd_rn(locBegin, 2.f),
+                                 __fadd_rn(locBegin, 3.f)};
+                float acc4[4] = {0.f, 0.f, 0.f, 0.f};
+                for (; l + 3 < loc1; l += 4)
+                {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                    {
+                        acc4[j] = __fadd_rn(acc4[j], __fmul_rn(__ldg(in + l + j), win.lane(lane[j])));
+                        lane[j] = __fadd_rn(lane[j], 4.f);
+                    }
+                }
+                float accum = __fadd_rn(__fadd_rn(acc4[0], acc4[2]), __fadd_rn(acc4[1], acc4[3]));
+                float xx = __fsub_rn(float(l), inPos);
+                for (; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
+                    accum = __fadd_rn(accum, __fmul_rn(__ldg(in + l), win.scalar(xx)));
+                y[outPos] = accum;
+            }
+            else
+            {
+                constexpr int kMaxC = 16;
+                float acc[kMaxC];
+#pragma unroll
+                for (int c = 0; c < kMaxC; ++c) acc[c] = 0.f;
+                float xx = __fsub_rn(float(loc0), inPos);
+                for (int l = loc0; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
+                {
+                    const float wv = win.scalar(xx);
+#pragma unroll
+                    for (int c = 0; c < kMaxC; ++c)
+                        if (c < C) acc[c] = __fadd_rn(acc[c], __fmul_rn(__ldg(in + (long long)l * C + c), wv));
+                }
+#pragma unroll
+                for (int c = 0; c < kMaxC; ++c)
+                    if (c < C) y[(long long)outPos * C + c] = acc[c];
+            }
+        }
+        __syncthreads();   // s_phase is rewritten by the next unit
+    }
+}
+
+}  // namespace
+
+void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStride, float* dst, uint32_t dstStride,
+                     int n, const float* inRate, const float* outRate, const int* dims, const ResampleWindowDev& win)
+{
+    if (n <= 0) return;
+    long long* prefix = static_cast<long long*>(scratch);
+    launch_ragged_prefix(ResampleCount{inRate, outRate, dims}, n, prefix, h.stream());
+    const size_t smem = size_t(win.lutSize) * sizeof(float);
+    check_cuda(cudaFuncSetAttribute(resample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "smem attr");
+    int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel), kBlock, smem);
+    resample_kernel<<<grid, kBlock, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate, outRate, dims, win,
+                                                        prefix, n);
+    check_cuda(cudaGetLastError(), "resample_kernel");
+}
+
+}  // namespace rppb

@@ -1,0 +1,101 @@
+"""ctypes binding of rpp_b200/librppb.so — the same C ABI a C/C++ caller of the reference links.
+
+Loading fails loudly when the library is missing: there is no CPU fallback.  Build it with
+``python -m rpp_b200.build`` (or ``__graft_entry__.build()``).
+"""
+import ctypes
+import os
+
+from .types import RpptDesc, RpptImagePatch, RpptResamplingWindow, RppBackend
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "librppb.so")
+
+# Every symbol the public headers (include/*.h) declare.
+EXPORTED = (
+    "rppCreate", "rppDestroy", "rppSetBatchSize", "rppGetBatchSize", "rppSetStream", "rppGetStream",
+    "rppSetAllocator", "rppGetKernelTime", "rppEnableProfiling",
+    "rppt_non_silent_region_detection_gpu", "rppt_to_decibels_gpu", "rppt_pre_emphasis_filter_gpu",
+    "rppt_down_mixing_gpu", "rppt_spectrogram_gpu", "rppt_mel_filter_bank_gpu", "rppt_resample_gpu",
+    "rppbGetLastError",
+)
+
+_lib = None
+
+_V = ctypes.c_void_p
+_D = ctypes.POINTER(RpptDesc)
+_I = ctypes.c_int
+_F = ctypes.c_float
+_B = ctypes.c_bool
+
+
+def load(path=None):
+    """Loads the library once and declares every entry point's signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.isfile(p):
+        raise FileNotFoundError(f"{p} is missing: build it with `python -m rpp_b200.build` (no CPU fallback)")
+    L = ctypes.CDLL(p)
+    L.rppCreate.argtypes = [ctypes.POINTER(_V), ctypes.c_size_t, ctypes.c_uint, _V, _I]
+    L.rppDestroy.argtypes = [_V, _I]
+    L.rppSetBatchSize.argtypes = [_V, ctypes.c_size_t]
+    L.rppGetBatchSize.argtypes = [_V, ctypes.POINTER(ctypes.c_size_t)]
+    L.rppSetStream.argtypes = [_V, _V]
+    L.rppGetStream.argtypes = [_V, ctypes.POINTER(_V)]
+    L.rppSetAllocator.argtypes = [_V, _V, _V, _V]
+    L.rppGetKernelTime.argtypes = [_V, ctypes.POINTER(_F)]
+    L.rppEnableProfiling.argtypes = [_V, _B]
+    for f in ("rppCreate", "rppDestroy", "rppSetBatchSize", "rppGetBatchSize", "rppSetStream", "rppGetStream",
+              "rppSetAllocator", "rppGetKernelTime", "rppEnableProfiling"):
+        getattr(L, f).restype = _I
+    L.rppt_non_silent_region_detection_gpu.argtypes = [_V, _D, _V, _V, _V, _F, _I, _F, _I, _V]
+    L.rppt_to_decibels_gpu.argtypes = [_V, _D, _V, _D, _V, _F, _F, _F, _V]
+    L.rppt_pre_emphasis_filter_gpu.argtypes = [_V, _D, _V, _D, _V, _V, _I, _V]
+    L.rppt_down_mixing_gpu.argtypes = [_V, _D, _V, _D, _V, _B, _V]
+    L.rppt_spectrogram_gpu.argtypes = [_V, _D, _V, _D, _V, _B, _B, _V, _I, _I, _I, _I, _V]
+    L.rppt_mel_filter_bank_gpu.argtypes = [_V, _D, _V, _D, _V, _F, _F, _I, _I, _F, _B, _V]
+    L.rppt_resample_gpu.argtypes = [_V, _D, _V, _D, _V, _V, _V, ctypes.POINTER(RpptResamplingWindow), _V]
+    for f in ("rppt_non_silent_region_detection_gpu", "rppt_to_decibels_gpu", "rppt_pre_emphasis_filter_gpu",
+              "rppt_down_mixing_gpu", "rppt_spectrogram_gpu", "rppt_mel_filter_bank_gpu", "rppt_resample_gpu"):
+        getattr(L, f).restype = _I
+    L.rppbGetLastError.argtypes = []
+    L.rppbGetLastError.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def last_error():
+    return load().rppbGetLastError().decode()
+
+
+class Handle:
+    """rppCreate/rppDestroy around a CUDA stream (an int handle, e.g. torch's stream.cuda_stream)."""
+
+    def __init__(self, batch_size=1, stream=0):
+        L = load()
+        h = _V()
+        st = L.rppCreate(ctypes.byref(h), batch_size, 0, _V(stream), int(RppBackend.RPP_HIP_BACKEND))
+        if st != 0:
+            raise RuntimeError(f"rppCreate failed with status {st}")
+        self.ptr = h
+
+    def set_stream(self, stream):
+        st = load().rppSetStream(self.ptr, _V(stream))
+        if st != 0:
+            raise RuntimeError(f"rppSetStream failed with status {st}")
+
+    @property
+    def value(self):
+        return self.ptr
+
+    def close(self):
+        if self.ptr:
+            load().rppDestroy(self.ptr, int(RppBackend.RPP_HIP_BACKEND))
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,159 @@
+"""ctypes mirrors of the audio path's ABI types (include/rppdefs.h).
+
+Layouts follow the reference's api/rppdefs.h: RpptDesc (:581-589), RpptStrides (:570-576),
+RpptImagePatch (:645-649) and RpptResamplingWindow (:751-790); enum values follow
+RppStatus (:121-176), RppBackend (:181-186), RpptDataType (:397-405), RpptLayout (:410-419),
+RpptAudioBorderType (:464-469) and RpptMelScaleFormula (:474-478).
+"""
+import ctypes
+import enum
+
+
+class RppStatus(enum.IntEnum):
+    RPP_SUCCESS = 0
+    RPP_ERROR = -1
+    RPP_ERROR_INVALID_ARGUMENTS = -2
+    RPP_ERROR_LOW_OFFSET = -3
+    RPP_ERROR_ZERO_DIVISION = -4
+    RPP_ERROR_HIGH_SRC_DIMENSION = -5
+    RPP_ERROR_NOT_IMPLEMENTED = -6
+    RPP_ERROR_INVALID_SRC_CHANNELS = -7
+    RPP_ERROR_INVALID_DST_CHANNELS = -8
+    RPP_ERROR_INVALID_SRC_LAYOUT = -9
+    RPP_ERROR_INVALID_DST_LAYOUT = -10
+    RPP_ERROR_INVALID_SRC_DATATYPE = -11
+    RPP_ERROR_INVALID_DST_DATATYPE = -12
+    RPP_ERROR_INVALID_SRC_OR_DST_DATATYPE = -13
+    RPP_ERROR_INSUFFICIENT_DST_BUFFER_LENGTH = -14
+    RPP_ERROR_INVALID_PARAMETER_DATATYPE = -15
+    RPP_ERROR_NOT_ENOUGH_MEMORY = -16
+    RPP_ERROR_OUT_OF_BOUND_SRC_ROI = -17
+    RPP_ERROR_LAYOUT_MISMATCH = -18
+    RPP_ERROR_INVALID_CHANNELS = -19
+    RPP_ERROR_INVALID_OUTPUT_TILE_LENGTH = -20
+    RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE = -21
+    RPP_ERROR_OUT_OF_BOUND_SCRATCH_MEMORY_SIZE = -22
+    RPP_ERROR_INVALID_SRC_DIMS = -23
+    RPP_ERROR_INVALID_DST_DIMS = -24
+    RPP_ERROR_INVALID_DIM_LENGTHS = -25
+    RPP_ERROR_INVALID_AXIS = -26
+
+
+class RppHandleStatus(enum.IntEnum):
+    rppStatusSuccess = 0
+    rppStatusBadParm = -1
+    rppStatusUnknownError = -2
+    rppStatusNotInitialized = -3
+    rppStatusInvalidValue = -4
+    rppStatusAllocFailed = -5
+    rppStatusInternalError = -6
+    rppStatusNotImplemented = -7
+    rppStatusUnsupportedOp = -8
+
+
+class RppBackend(enum.IntEnum):
+    RPP_HOST_BACKEND = 0
+    RPP_HIP_BACKEND = 1
+    RPP_OCL_BACKEND = 2
+
+
+class RpptDataType(enum.IntEnum):
+    U8 = 0
+    F32 = 1
+    F16 = 2
+    I8 = 3
+    I16 = 4
+
+
+class RpptLayout(enum.IntEnum):
+    NCHW = 0
+    NHWC = 1
+    NCDHW = 2
+    NDHWC = 3
+    NHW = 4
+    NFT = 5
+    NTF = 6
+
+
+class RpptAudioBorderType(enum.IntEnum):
+    ZERO = 0
+    CLAMP = 1
+    REFLECT = 2
+
+
+class RpptMelScaleFormula(enum.IntEnum):
+    SLANEY = 0
+    HTK = 1
+
+
+class RpptStrides(ctypes.Structure):
+    _fields_ = [("nStride", ctypes.c_uint32), ("cStride", ctypes.c_uint32),
+                ("hStride", ctypes.c_uint32), ("wStride", ctypes.c_uint32)]
+
+
+class RpptDesc(ctypes.Structure):
+    _fields_ = [("numDims", ctypes.c_size_t), ("offsetInBytes", ctypes.c_uint32),
+                ("dataType", ctypes.c_int), ("n", ctypes.c_uint32), ("c", ctypes.c_uint32),
+                ("h", ctypes.c_uint32), ("w", ctypes.c_uint32), ("strides", RpptStrides),
+                ("layout", ctypes.c_int)]
+
+
+class RpptImagePatch(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
+
+
+class _StdVectorFloat(ctypes.Structure):
+    # libstdc++ std::vector<float>: begin, end, end-of-storage pointers
+    _fields_ = [("begin", ctypes.c_void_p), ("end", ctypes.c_void_p), ("cap", ctypes.c_void_p)]
+
+
+class RpptResamplingWindow(ctypes.Structure):
+    """Byte image of the reference's RpptResamplingWindow (96 bytes on x86-64).
+
+    Only `lookupPinned` is used to pass the table from Python (the vector stays empty, so
+    nothing on the C++ side ever frees Python memory)."""
+    _fields_ = [("scale", ctypes.c_float), ("center", ctypes.c_float),
+                ("lobes", ctypes.c_int32), ("coeffs", ctypes.c_int32),
+                ("lookupSize", ctypes.c_int32), ("_pad0", ctypes.c_int32),
+                ("lookupPinned", ctypes.c_void_p), ("lookup", _StdVectorFloat),
+                ("_pad1", ctypes.c_uint8 * 8),
+                ("pCenter", ctypes.c_float * 4), ("pScale", ctypes.c_float * 4)]
+
+
+assert ctypes.sizeof(RpptDesc) == 56
+assert ctypes.sizeof(RpptResamplingWindow) == 96
+assert RpptResamplingWindow.pCenter.offset == 64
+
+
+def audio_desc(n, max_len, channels=1, num_dims=2, pad_to_8=False):
+    """Descriptor of a batch of 1-D (optionally interleaved multi-channel) signals.
+
+    pad_to_8 reproduces the test suite's stride choice, w = (w/8)*8 + 8
+    (utilities/test_suite/rpp_test_suite_audio.h:84-99)."""
+    d = RpptDesc()
+    d.numDims = num_dims
+    d.offsetInBytes = 0
+    d.dataType = RpptDataType.F32
+    d.n, d.h, d.c = n, 1, channels
+    d.w = (max_len // 8) * 8 + 8 if pad_to_8 else max_len
+    d.strides.nStride = d.c * d.w * d.h
+    d.strides.hStride = d.c * d.w
+    d.strides.wStride = d.c
+    d.strides.cStride = 1
+    d.layout = RpptLayout.NFT
+    return d
+
+
+def spectra_desc(n, height, width, layout=RpptLayout.NFT):
+    """Descriptor of a batch of 2-D spectra [height][width] per sample (numDims 3)."""
+    d = RpptDesc()
+    d.numDims = 3
+    d.offsetInBytes = 0
+    d.dataType = RpptDataType.F32
+    d.n, d.c, d.h, d.w = n, 1, height, width
+    d.strides.nStride = height * width
+    d.strides.hStride = width
+    d.strides.wStride = 1
+    d.strides.cStride = 1
+    d.layout = layout
+    return d

@@ -1,0 +1,104 @@
+"""The C-ABI boundary without a GPU: the library loads, exports every symbol the public headers
+declare, and the headers keep the reference's type layouts and enum values."""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from rpp_b200 import lib
+from rpp_b200 import types as T
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INCLUDE = os.path.join(ROOT, "include")
+REF = os.environ.get("RPP_REF", "/root/reference")
+
+
+def declared_symbols():
+    names = set()
+    for h in os.listdir(INCLUDE):
+        if h.endswith(".h"):
+            text = open(os.path.join(INCLUDE, h)).read()
+            names |= set(re.findall(r"SHARED_PUBLIC\s+[\w\s\*]+?\b(\w+)\s*\(", text))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = lib.load()
+    declared = declared_symbols()
+    assert {"rppCreate", "rppt_spectrogram_gpu", "rppt_resample_gpu"} <= declared
+    for name in sorted(declared | set(lib.EXPORTED)):
+        assert hasattr(L, name), name
+
+
+def test_no_host_backend():
+    h = ctypes.c_void_p()
+    st = lib.load().rppCreate(ctypes.byref(h), 1, 0, None, int(T.RppBackend.RPP_HOST_BACKEND))
+    assert st == T.RppHandleStatus.rppStatusNotImplemented
+
+
+def test_create_without_device_fails_cleanly():
+    """With no usable GPU rppCreate returns an error status instead of aborting."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = ctypes.c_void_p()
+    st = lib.load().rppCreate(ctypes.byref(h), 1, 0, None, int(T.RppBackend.RPP_HIP_BACKEND))
+    assert st != 0
+
+
+def test_null_handle_status():
+    d = T.audio_desc(1, 16)
+    st = lib.load().rppt_pre_emphasis_filter_gpu(None, ctypes.byref(d), None, ctypes.byref(d), None, None, 0, None)
+    assert st == T.RppStatus.RPP_ERROR_INVALID_ARGUMENTS
+
+
+LAYOUT_PROBE = r"""
+#include <cstdio>
+#include <cstddef>
+#include "rppdefs.h"
+int main() {
+  std::printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(RpptDesc), offsetof(RpptDesc, strides), offsetof(RpptDesc, layout),
+              sizeof(RpptImagePatch), sizeof(RpptResamplingWindow), offsetof(RpptResamplingWindow, lookup),
+              offsetof(RpptResamplingWindow, pCenter));
+  std::printf("%d %d %d %d %d %d %d %d\n", (int)RPP_ERROR_INVALID_AXIS, (int)RPP_ERROR_OUT_OF_BOUND_SCRATCH_MEMORY_SIZE,
+              (int)NFT, (int)NTF, (int)REFLECT, (int)HTK, (int)F32, (int)RPP_HIP_BACKEND);
+  return 0;
+}
+"""
+
+
+def _probe(include_dirs, extra=()):
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "p.cpp")
+        exe = os.path.join(d, "p")
+        open(src, "w").write(LAYOUT_PROBE)
+        cmd = ["g++", "-std=c++17", "-w", src, "-o", exe] + [f"-I{i}" for i in include_dirs] + list(extra)
+        subprocess.run(cmd, check=True, capture_output=True)
+        return subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+
+
+def test_header_layout_matches_ctypes():
+    out = _probe([INCLUDE]).split("\n")
+    sizes = [int(v) for v in out[0].split()]
+    assert sizes[0] == ctypes.sizeof(T.RpptDesc)
+    assert sizes[1] == T.RpptDesc.strides.offset
+    assert sizes[2] == T.RpptDesc.layout.offset
+    assert sizes[3] == ctypes.sizeof(T.RpptImagePatch)
+    assert sizes[4] == ctypes.sizeof(T.RpptResamplingWindow)
+    assert sizes[5] == T.RpptResamplingWindow.lookup.offset
+    assert sizes[6] == T.RpptResamplingWindow.pCenter.offset
+
+
+def test_header_layout_matches_reference():
+    """Same probe compiled against the reference's api/rppdefs.h (where the sources exist)."""
+    if not os.path.isdir(os.path.join(REF, "api")):
+        pytest.skip("reference headers absent")
+    gen = os.path.join(ROOT, "oracle", "_ref", "gen")
+    if not os.path.isdir(gen):
+        pytest.skip("oracle/_ref/gen missing (run oracle/build_ref.sh)")
+    ours = _probe([INCLUDE])
+    theirs = _probe([gen, os.path.join(REF, "api")], extra=["-mavx2", "-mf16c"])
+    assert ours == theirs

@@ -1,0 +1,404 @@
+"""GPU parity of the seven rppt_*_gpu entry points, called through the C ABI (librppb.so),
+against the oracle (C restatement, itself pinned bit-exact to the reference's host library and
+goldens) on seeded inputs, plus the shipped golden outputs, edge cases and status codes.
+
+Bars: bit-exact for pre-emphasis, down-mixing, resampling and NSR begin/length (NSR may differ
+only where a moving mean square is within 1 ulp of the cutoff); mel bit-exact in > 99.9% of
+values and within 1e-5 of each frame's maximum everywhere; spectrogram within 1e-5 of each
+frame's maximum bin (SPEC_FRAME_REL); decibels within 1e-3 dB (DB_ABS).
+"""
+import numpy as np
+import pytest
+import torch
+
+from rpp_b200 import audio, synth
+from rpp_b200.types import RppStatus, RpptLayout, audio_desc, spectra_desc, RpptDataType
+from gpu_util import dev, pinned, host, canvas, frame_rel_err, SPEC_FRAME_REL, DB_ABS
+
+pytestmark = pytest.mark.gpu
+OK = RppStatus.RPP_SUCCESS
+
+
+def rng(k):
+    return np.random.Generator(np.random.PCG64(5000 + k))
+
+
+def batch(n=7, hi=20000, seed=0, lens=None):
+    r = rng(seed)
+    if lens is None:
+        lens = r.integers(1, hi, n)
+        lens[0] = hi
+    return synth.mono_batch(len(lens), np.asarray(lens, np.int32), r, gaps=True)
+
+
+# ---------------------------------------------------------------- pre-emphasis
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+@pytest.mark.parametrize("stride_pad", [0, 3])
+def test_pre_emphasis(gpu, oracle, border, stride_pad):
+    x, lens = batch(seed=border)
+    lens[1] = 0
+    lens[2] = 1
+    n, L = x.shape
+    xs = np.zeros((n, L + stride_pad), np.float32)
+    xs[:, :L] = x
+    d = audio_desc(n, L + stride_pad)
+    coeff = rng(3).uniform(0.5, 0.99, n).astype(np.float32)
+    ref = np.full_like(xs, -12345.0)
+    oracle.pre_emphasis(xs, ref, lens, coeff, border)
+    out = canvas(xs.shape)
+    st = audio.pre_emphasis_filter(dev(xs), d, out, d, dev(lens), dev(coeff), border, gpu)
+    assert st == OK
+    np.testing.assert_array_equal(host(out), ref)
+
+
+def test_pre_emphasis_golden(gpu, golden):
+    lens = golden["lengths"].astype(np.int32)
+    d = audio_desc(3, int(lens.max()), pad_to_8=True)
+    x = np.zeros((3, d.w), np.float32)
+    for i in range(3):
+        x[i, :lens[i]] = golden[f"pcm{i}"].astype(np.float32) / 32768.0
+    out = canvas(x.shape, 0.0)
+    coeff = pinned(np.full(3, 0.97, np.float32))
+    assert audio.pre_emphasis_filter(dev(x), d, out, d, pinned(lens), coeff, 1, gpu) == OK
+    g = golden["pre_emphasis_filter"].reshape(3, d.w)
+    o = host(out)
+    for i in range(3):
+        np.testing.assert_array_equal(o[i, :lens[i]], g[i, :lens[i]])
+
+
+def test_pre_emphasis_pageable_tensors(gpu, oracle):
+    """Per-sample tensors in pageable host memory are staged by the library."""
+    x, lens = batch(n=3, seed=11)
+    d = audio_desc(3, x.shape[1])
+    coeff = np.full(3, 0.9, np.float32)
+    ref = np.full_like(x, -12345.0)
+    oracle.pre_emphasis(x, ref, lens, coeff, 0)
+    out = canvas(x.shape)
+    assert audio.pre_emphasis_filter(dev(x), d, out, d, lens, coeff, 0, gpu) == OK
+    np.testing.assert_array_equal(host(out), ref)
+
+
+# ---------------------------------------------------------------- down-mixing
+
+@pytest.mark.parametrize("channels", [1, 2, 3, 4, 6, 8, 13])
+@pytest.mark.parametrize("normalize", [False, True])
+def test_down_mixing(gpu, oracle, channels, normalize):
+    r = rng(channels)
+    n, L = 5, 7001
+    lens = r.integers(0, L + 1, n).astype(np.int32)
+    lens[0] = L
+    x = r.normal(0, 0.3, (n, L * channels)).astype(np.float32)
+    dims = np.stack([lens, np.full(n, channels, np.int32)], 1).astype(np.int32)
+    ref = np.full((n, L), -12345.0, np.float32)
+    oracle.down_mixing(x, ref, dims.ravel(), normalize)
+    out = canvas((n, L))
+    st = audio.down_mixing(dev(x), audio_desc(n, L, channels=channels, num_dims=3), out, audio_desc(n, L),
+                           dev(dims), normalize, gpu)
+    assert st == OK
+    np.testing.assert_array_equal(host(out), ref)
+
+
+# ---------------------------------------------------------------- resample
+
+@pytest.mark.parametrize("rates,channels", [((16000, 18400), 1), ((48000, 16000), 1), ((44100, 16000), 1),
+                                            ((22050, 16000), 1), ((16000, 16000), 1), ((8000, 44100), 1),
+                                            ((48000, 16000), 2), ((22050, 16000), 3)])
+def test_resample(gpu, oracle, rates, channels):
+    r = rng(17)
+    n, L = 4, 9000
+    lens = np.array([L, 3001, 1, 0], np.int32)
+    x = r.normal(0, 0.3, (n, L * channels)).astype(np.float32)
+    lut, scale, center, lobes = oracle.windowed_sinc(16 * 64 + 1, 16)
+    ir = np.full(n, rates[0], np.float32)
+    orr = np.full(n, rates[1], np.float32)
+    out_len = int(np.ceil(L * rates[1] / rates[0])) + 8
+    dims = np.stack([lens, np.full(n, channels, np.int32)], 1).astype(np.int32)
+    ref = np.full((n, out_len * channels), -12345.0, np.float32)
+    oracle.resample(x, ref, ir, orr, dims.ravel(), lut, scale, center, lobes)
+    out = canvas(ref.shape)
+    lut_d = dev(lut)
+    win = audio.resampling_window(lut_d, scale, center, lobes)
+    st = audio.resample(dev(x), audio_desc(n, L, channels=channels), out, audio_desc(n, out_len, channels=channels),
+                        dev(ir), dev(orr), dev(dims), win, gpu)
+    assert st == OK
+    np.testing.assert_array_equal(host(out), ref)
+
+
+def test_resample_golden(gpu, oracle, golden):
+    lens = golden["lengths"].astype(np.int32)
+    d = audio_desc(3, int(lens.max()), pad_to_8=True)
+    x = np.zeros((3, d.w), np.float32)
+    for i in range(3):
+        x[i, :lens[i]] = golden[f"pcm{i}"].astype(np.float32) / 32768.0
+    lut, scale, center, lobes = oracle.windowed_sinc(16 * 64 + 1, 16)
+    out_rate = np.float32(16000 * np.float32(1.15))
+    g = golden["resample"].reshape(3, -1)
+    out = canvas(g.shape, 0.0)
+    dims = np.stack([lens, np.ones(3, np.int32)], 1).astype(np.int32)
+    lut_p = pinned(lut)
+    win = audio.resampling_window(lut_p, scale, center, lobes)
+    st = audio.resample(dev(x), d, out, audio_desc(3, g.shape[1]), pinned(np.full(3, 16000, np.float32)),
+                        pinned(np.full(3, out_rate, np.float32)), pinned(dims), win, gpu)
+    assert st == OK
+    o = host(out)
+    for i in range(3):
+        ol = int(np.ceil(np.float32(np.float32(lens[i]) * out_rate) / np.float32(16000)))
+        np.testing.assert_array_equal(o[i, :ol], g[i, :ol])
+
+
+# ---------------------------------------------------------------- spectrogram
+
+SPEC_CASES = [
+    (512, 400, 160, True, True, RpptLayout.NFT, 2),
+    (512, 320, 160, True, True, RpptLayout.NTF, 2),
+    (512, 512, 128, False, True, RpptLayout.NFT, 1),
+    (256, 200, 80, True, False, RpptLayout.NFT, 2),
+    (128, 128, 64, True, True, RpptLayout.NTF, 2),
+    (1024, 1024, 256, True, True, RpptLayout.NFT, 2),
+    (2048, 1600, 512, True, True, RpptLayout.NTF, 2),
+    (400, 400, 160, True, True, RpptLayout.NFT, 2),     # non-power-of-two: direct DFT
+]
+
+
+@pytest.mark.parametrize("nfft,W,hop,center,reflect,layout,power", SPEC_CASES)
+def test_spectrogram(gpu, oracle, nfft, W, hop, center, reflect, layout, power):
+    x, lens = batch(n=6, hi=24000, seed=nfft + W)
+    lens[1], lens[2], lens[3] = 1, 2, W - 1
+    n = len(lens)
+    nft = layout == RpptLayout.NFT
+    F = [oracle.num_windows(l, W, hop, center) for l in lens]
+    mf = max(F)
+    bins = nfft // 2 + 1
+    shape = (n, bins, mf) if nft else (n, mf, bins)
+    dd = spectra_desc(n, bins, mf, layout) if nft else spectra_desc(n, mf, bins, layout)
+    out = canvas(shape)
+    st = audio.spectrogram(dev(x), audio_desc(n, x.shape[1]), out, dd, pinned(lens), center, reflect, None, nfft,
+                           power, W, hop, gpu)
+    assert st == OK
+    o = host(out)
+    ref = oracle.spectrogram_f64(x, lens, center, reflect, None, nfft, power, W, hop, nft, max_frames=mf)
+    for i in range(n):
+        if F[i] <= 0:
+            assert (o[i] == -12345.0).all()
+            continue
+        got = o[i, :, :F[i]] if nft else o[i, :F[i], :].T
+        exp = ref[i, :, :F[i]] if nft else ref[i, :F[i], :].T
+        assert frame_rel_err(got, exp) < SPEC_FRAME_REL, (i, frame_rel_err(got, exp))
+        tail = o[i, :, F[i]:] if nft else o[i, F[i]:, :]
+        assert (tail == -12345.0).all()
+
+
+def test_spectrogram_vs_reference_library(gpu, reference):
+    """Against the reference's own FP32 host spectrogram (ffts), per-frame relative 1e-5."""
+    x, lens = batch(n=5, hi=30000, seed=77)
+    n = len(lens)
+    F = [l // 160 + 1 for l in lens]
+    mf = max(F)
+    dd = spectra_desc(n, 257, mf)
+    ref = np.zeros((n, 257, mf), np.float32)
+    sd = audio_desc(n, x.shape[1])
+    assert reference.spectrogram(x, sd, ref, dd, lens, True, True, None, 512, 2, 400, 160) == 0
+    out = canvas((n, 257, mf))
+    assert audio.spectrogram(dev(x), sd, out, dd, dev(lens), True, True, None, 512, 2, 400, 160, gpu) == OK
+    o = host(out)
+    for i in range(n):
+        assert frame_rel_err(o[i, :, :F[i]], ref[i, :, :F[i]]) < SPEC_FRAME_REL
+
+
+def test_spectrogram_golden(gpu, golden):
+    lens = golden["lengths"].astype(np.int32)
+    d = audio_desc(3, int(lens.max()), pad_to_8=True)
+    x = np.zeros((3, d.w), np.float32)
+    for i in range(3):
+        x[i, :lens[i]] = golden[f"pcm{i}"].astype(np.float32) / 32768.0
+    F = [225, 211, 214]
+    dd = spectra_desc(3, 257, 225)
+    out = canvas((3, 257, 225), 0.0)
+    assert audio.spectrogram(dev(x), d, out, dd, pinned(lens), True, True, None, 512, 2, 320, 160, gpu) == OK
+    o = host(out)
+    g = golden["spectrogram"].reshape(3, 257, 225)
+    for i in range(3):
+        assert frame_rel_err(o[i, :, :F[i]], g[i, :, :F[i]]) < SPEC_FRAME_REL
+
+
+def test_spectrogram_custom_window(gpu, oracle):
+    x, lens = batch(n=3, hi=8000, seed=5)
+    W = 300
+    win = np.hamming(W).astype(np.float32)
+    F = [oracle.num_windows(l, W, 100, True) for l in lens]
+    mf = max(F)
+    out = canvas((3, 257, mf))
+    st = audio.spectrogram(dev(x), audio_desc(3, x.shape[1]), out, spectra_desc(3, 257, mf), dev(lens), True, True,
+                           win, 512, 2, W, 100, gpu)
+    assert st == OK
+    ref = oracle.spectrogram_f64(x, lens, 1, 1, win, 512, 2, W, 100, 1, max_frames=mf)
+    o = host(out)
+    for i in range(3):
+        assert frame_rel_err(o[i, :, :F[i]], ref[i, :, :F[i]]) < SPEC_FRAME_REL
+
+
+# ---------------------------------------------------------------- mel filter bank
+
+@pytest.mark.parametrize("htk,normalize,nfft,nmel,fmin,fmax", [
+    (0, 1, 512, 128, 0.0, 8000.0), (1, 1, 512, 80, 0.0, 0.0), (0, 0, 1024, 64, 60.0, 7600.0),
+    (1, 0, 256, 40, 20.0, 4000.0), (0, 1, 2048, 256, 0.0, 8000.0)])
+def test_mel_filter_bank(gpu, oracle, htk, normalize, nfft, nmel, fmin, fmax):
+    r = rng(nfft + nmel)
+    n, bins, T = 4, nfft // 2 + 1, 150
+    frames = np.array([T, 70, 1, 0], np.int32)
+    spec = (r.random((n, bins, T)) ** 4).astype(np.float32)
+    dims = np.stack([np.full(n, bins, np.int32), frames], 1).astype(np.int32)
+    ref = np.full((n, nmel, T), -12345.0, np.float32)
+    oracle.mel_filter_bank(spec, ref, dims.ravel(), fmax, fmin, htk, nmel, 16000, normalize)
+    out = canvas((n, nmel, T))
+    st = audio.mel_filter_bank(dev(spec), spectra_desc(n, bins, T), out, spectra_desc(n, nmel, T), pinned(dims),
+                               fmax, fmin, htk, nmel, 16000, normalize, gpu)
+    assert st == OK
+    o = host(out)
+    exact = (o == ref).mean()
+    assert exact > 0.999, exact
+    for i in range(n):
+        zc = min(frames[i] + 8, T)
+        assert (o[i, :, zc:] == -12345.0).all()
+        if frames[i]:
+            assert frame_rel_err(o[i, :, :frames[i]], ref[i, :, :frames[i]]) < 1e-6
+
+
+def test_mel_filter_bank_golden(gpu, golden):
+    dims = np.array([[257, 225], [257, 211], [257, 214]], np.int32)
+    spec = golden["spectrogram"].reshape(3, 257, 225).copy()
+    out = canvas((3, 80, 225), 0.0)
+    st = audio.mel_filter_bank(dev(spec), spectra_desc(3, 257, 225), out, spectra_desc(3, 80, 225), dev(dims), 8000,
+                               0, 0, 80, 16000, True, gpu)
+    assert st == OK
+    o = host(out)
+    g = golden["mel_filter_bank"].reshape(3, 80, 225)
+    for i in range(3):
+        np.testing.assert_array_equal(o[i, :, :dims[i, 1]], g[i, :, :dims[i, 1]])
+
+
+# ---------------------------------------------------------------- to_decibels
+
+@pytest.mark.parametrize("two_d,ref_mag", [(False, 0.0), (True, 0.0), (True, 2.5), (False, 1.0)])
+def test_to_decibels(gpu, oracle, two_d, ref_mag):
+    r = rng(21)
+    n, H, Wd = 4, 128, 1601
+    if two_d:
+        x = (r.random((n, H, Wd)) ** 3).astype(np.float32)
+        wh = [(Wd, H), (700, 100), (1, 1), (0, 0)]
+        desc = spectra_desc(n, H, Wd)
+    else:
+        x = (r.normal(0, 1, (n, H * Wd)) ** 2).astype(np.float32)
+        wh = [(1, H * Wd), (1, 10001), (1, 1), (1, 0)]
+        desc = audio_desc(n, H * Wd)
+    dims = np.array(wh, np.uint32)
+    ref = np.full_like(x, -12345.0)
+    oracle.to_decibels(x, ref, dims, -80.0, 10.0, ref_mag)
+    out = canvas(x.shape)
+    st = audio.to_decibels(dev(x), desc, out, desc, audio.image_patches(*zip(*wh)), -80.0, 10.0, ref_mag, gpu)
+    assert st == OK
+    o = host(out)
+    untouched = ref == -12345.0
+    assert (o[untouched] == -12345.0).all()
+    assert np.abs(o[~untouched] - ref[~untouched]).max() <= DB_ABS / 10
+
+
+def test_to_decibels_golden(gpu, golden):
+    lens = golden["lengths"].astype(np.int32)
+    d = audio_desc(3, int(lens.max()), pad_to_8=True)
+    x = np.zeros((3, d.w), np.float32)
+    for i in range(3):
+        x[i, :lens[i]] = golden[f"pcm{i}"].astype(np.float32) / 32768.0
+    dims = np.stack([np.ones(3, np.uint32), lens.astype(np.uint32)], 1)
+    out = canvas(x.shape, 0.0)
+    st = audio.to_decibels(dev(x), d, out, d, pinned(dims), np.float32(np.log(1e-20)), np.float32(np.log(10)), 1.0,
+                           gpu)
+    assert st == OK
+    o = host(out)
+    g = golden["to_decibels"].reshape(3, d.w)
+    for i in range(3):
+        assert np.abs(o[i, :lens[i]] - g[i, :lens[i]]).max() <= DB_ABS / 10
+
+
+# ---------------------------------------------------------------- non-silent region
+
+@pytest.mark.parametrize("reset,window,ref,cut", [(8192, 2048, 0.0, -60.0), (-1, 2048, 0.0, -60.0),
+                                                  (1000, 333, 0.0, -40.0), (8192, 2048, 0.05, -20.0),
+                                                  (4096, 1, 0.0, -3.0)])
+def test_nsr(gpu, oracle, reset, window, ref, cut):
+    x, lens = batch(n=9, hi=70000, seed=31)
+    lens[1], lens[2] = 0, 1
+    x[3] = 0.0          # a silent sample
+    b_ref, l_ref, mms, cutoff = oracle.nsr(x, lens, cut, window, ref, reset, want_mms=True)
+    begin = torch.full((len(lens),), -7, dtype=torch.int32, device="cuda")
+    length = torch.full((len(lens),), -7, dtype=torch.int32, device="cuda")
+    st = audio.non_silent_region_detection(dev(x), audio_desc(len(lens), x.shape[1]), dev(lens), begin, length, cut,
+                                           window, ref, reset, gpu)
+    assert st == OK
+    np.testing.assert_array_equal(host(begin), b_ref)
+    np.testing.assert_array_equal(host(length), l_ref)
+
+
+def test_nsr_golden_pinned_outputs(gpu, golden):
+    lens = golden["lengths"].astype(np.int32)
+    d = audio_desc(3, int(lens.max()), pad_to_8=True)
+    x = np.zeros((3, d.w), np.float32)
+    for i in range(3):
+        x[i, :lens[i]] = golden[f"pcm{i}"].astype(np.float32) / 32768.0
+    begin = pinned(np.full(3, -1, np.int32))
+    length = pinned(np.full(3, -1, np.int32))
+    assert audio.non_silent_region_detection(dev(x), d, pinned(lens), begin, length, -60.0, 2048, 0.0, 8192,
+                                             gpu) == OK
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(begin.numpy(), golden["nsr_begin"])
+    np.testing.assert_array_equal(length.numpy(), golden["nsr_length"])
+
+
+def test_nsr_pageable_outputs(gpu, oracle):
+    x, lens = batch(n=4, hi=30000, seed=41)
+    b_ref, l_ref = oracle.nsr(x, lens, -50, 1024, 0.0, 4096)
+    begin = np.full(4, -1, np.int32)
+    length = np.full(4, -1, np.int32)
+    assert audio.non_silent_region_detection(dev(x), audio_desc(4, x.shape[1]), lens, begin, length, -50, 1024, 0.0,
+                                             4096, gpu) == OK
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(begin, b_ref)
+    np.testing.assert_array_equal(length, l_ref)
+
+
+# ---------------------------------------------------------------- status codes (reference GPU dispatch)
+
+def test_status_codes(gpu):
+    x = dev(np.zeros((2, 64), np.float32))
+    y = canvas((2, 64))
+    lens = dev(np.array([64, 64], np.int32))
+    coeff = dev(np.array([0.9, 0.9], np.float32))
+    d1 = audio_desc(2, 64)
+    d3 = audio_desc(2, 64, num_dims=3)
+    assert audio.pre_emphasis_filter(x, d3, y, d1, lens, coeff, 0, gpu) == RppStatus.RPP_ERROR_INVALID_SRC_DIMS
+    du8 = audio_desc(2, 64)
+    du8.dataType = RpptDataType.U8
+    assert audio.pre_emphasis_filter(x, du8, y, d1, lens, coeff, 0, gpu) == RppStatus.RPP_ERROR_NOT_IMPLEMENTED
+    patches = audio.image_patches([1, 1], [64, 64])
+    assert audio.to_decibels(x, d1, y, d1, patches, -80, 0.0, 0, gpu) == RppStatus.RPP_ERROR_ZERO_DIVISION
+    sd = spectra_desc(2, 257, 8)
+    sd.layout = RpptLayout.NCHW
+    assert audio.spectrogram(x, d1, y, sd, lens, True, True, None, 512, 2, 400, 160,
+                             gpu) == RppStatus.RPP_ERROR_INVALID_DST_LAYOUT
+    assert audio.spectrogram(x, d3, y, spectra_desc(2, 257, 8), lens, True, True, None, 512, 2, 400, 160,
+                             gpu) == RppStatus.RPP_ERROR_INVALID_SRC_DIMS
+    assert audio.spectrogram(x, d1, y, spectra_desc(2, 257, 8), lens, True, True, None, 256, 2, 400, 160,
+                             gpu) == RppStatus.RPP_ERROR_INVALID_ARGUMENTS
+    ms = spectra_desc(2, 257, 8)
+    assert audio.mel_filter_bank(x, ms, y, ms, lens, 9000, 0, 0, 16, 16000, True,
+                                 gpu) == RppStatus.RPP_ERROR_INVALID_ARGUMENTS
+    ms_t = spectra_desc(2, 257, 8, RpptLayout.NTF)
+    assert audio.mel_filter_bank(x, ms_t, y, ms, lens, 8000, 0, 0, 16, 16000, True,
+                                 gpu) == RppStatus.RPP_ERROR_INVALID_SRC_LAYOUT
+    b = torch.zeros(2, dtype=torch.int32, device="cuda")
+    assert audio.non_silent_region_detection(x, d1, lens, b, b, -60, 2048, 0.0, 0,
+                                             gpu) == RppStatus.RPP_ERROR_INVALID_ARGUMENTS
+    assert audio.non_silent_region_detection(x, d3, lens, b, b, -60, 2048, 0.0, 8192,
+                                             gpu) == RppStatus.RPP_ERROR_INVALID_SRC_DIMS
+    torch.cuda.synchronize()

@@ -1,0 +1,126 @@
+"""Pins the oracle: the C restatement (and, where built, the reference's own host library)
+against the reference's shipped golden outputs for the audio QA suite.
+
+Fixture: tests/golden/reference_audio_qa.npz (made by tests/golden/make_fixtures.py from
+utilities/test_suite/{TEST_AUDIO_FILES,REFERENCE_OUTPUTS_AUDIO} and the NSR triples of
+utilities/test_suite/rpp_test_suite_audio.h:64-69).  QA parameters follow
+utilities/test_suite/HOST/Tensor_audio_host.cpp:189-375.
+"""
+import numpy as np
+import pytest
+
+from rpp_b200.types import audio_desc, spectra_desc, RpptImagePatch
+
+N = 3
+
+
+def qa_inputs(golden):
+    lens = golden["lengths"].astype(np.int32)
+    d = audio_desc(N, int(lens.max()), pad_to_8=True)
+    src = np.zeros((N, d.w), np.float32)
+    for i in range(N):
+        src[i, :lens[i]] = golden[f"pcm{i}"].astype(np.float32) / 32768.0
+    return src, lens, d
+
+
+def test_pre_emphasis_golden(oracle, golden):
+    src, lens, d = qa_inputs(golden)
+    dst = np.zeros_like(src)
+    oracle.pre_emphasis(src, dst, lens, np.full(N, 0.97, np.float32), 1)   # CLAMP
+    gold = golden["pre_emphasis_filter"].reshape(N, d.w)
+    for i in range(N):
+        np.testing.assert_array_equal(dst[i, :lens[i]], gold[i, :lens[i]])
+
+
+def test_to_decibels_golden(oracle, golden):
+    src, lens, d = qa_inputs(golden)
+    dims = np.stack([np.ones(N, np.uint32), lens.astype(np.uint32)], 1)
+    dst = np.zeros_like(src)
+    oracle.to_decibels(src, dst, dims, np.float32(np.log(1e-20)), np.float32(np.log(10)), 1.0)
+    gold = golden["to_decibels"].reshape(N, d.w)
+    for i in range(N):
+        np.testing.assert_array_equal(dst[i, :lens[i]], gold[i, :lens[i]])
+
+
+def test_spectrogram_f64_golden(oracle, golden):
+    """FP64 restatement vs the reference's FP32 (ffts) golden: within 1e-6 of each frame's max."""
+    src, lens, _ = qa_inputs(golden)
+    frames = [oracle.num_windows(l, 320, 160, True) for l in lens]
+    assert frames == [225, 211, 214]
+    mf = max(frames)
+    gold = golden["spectrogram"].reshape(N, 257, mf)
+    o = oracle.spectrogram_f64(src, lens, 1, 1, None, 512, 2, 320, 160, 1, max_frames=mf)
+    for i in range(N):
+        g = gold[i, :, :frames[i]].astype(np.float64)
+        err = np.abs(o[i, :, :frames[i]] - g) / g.max(axis=0, keepdims=True)
+        assert err.max() < 1e-6
+
+
+def test_mel_filter_bank_golden(oracle, golden):
+    dims = np.array([257, 225, 257, 211, 257, 214], np.int32)
+    spec = golden["spectrogram"].reshape(N, 257, 225).copy()
+    out = np.zeros((N, 80, 225), np.float32)
+    oracle.mel_filter_bank(spec, out, dims, 8000, 0, 0, 80, 16000, 1)
+    gold = golden["mel_filter_bank"].reshape(N, 80, 225)
+    for i in range(N):
+        np.testing.assert_array_equal(out[i, :, :dims[2 * i + 1]], gold[i, :, :dims[2 * i + 1]])
+
+
+def qa_resample_window(oracle):
+    quality = 50.0
+    lobes = int(round(0.007 * quality * quality - 0.09 * quality + 3))
+    return oracle.windowed_sinc(lobes * 64 + 1, lobes)
+
+
+def test_resample_golden(oracle, golden):
+    src, lens, _ = qa_inputs(golden)
+    lut, scale, center, lobes = qa_resample_window(oracle)
+    assert (lobes, scale, center) == (16, 32.0, 513.0)
+    out_rate = np.float32(16000 * np.float32(1.15))
+    gold = golden["resample"].reshape(N, -1)
+    dst = np.zeros((N, gold.shape[1]), np.float32)
+    dims = np.stack([lens, np.ones(N, np.int32)], 1).ravel()
+    oracle.resample(src, dst, np.full(N, 16000, np.float32), np.full(N, out_rate, np.float32), dims, lut, scale,
+                    center, lobes)
+    for i in range(N):
+        ol = int(np.ceil(np.float32(np.float32(lens[i]) * out_rate) / np.float32(16000)))
+        np.testing.assert_array_equal(dst[i, :ol], gold[i, :ol])
+
+
+def test_nsr_golden(oracle, golden):
+    src, lens, _ = qa_inputs(golden)
+    b, l = oracle.nsr(src, lens, -60, 2048, 0.0, 8192)
+    np.testing.assert_array_equal(b, golden["nsr_begin"])
+    np.testing.assert_array_equal(l, golden["nsr_length"])
+
+
+# ---- the reference's own host library against the same goldens (where it is built)
+
+def test_reference_library_golden(reference, golden):
+    src, lens, d = qa_inputs(golden)
+    dst = np.zeros_like(src)
+    assert reference.pre_emphasis_filter(src, d, dst, d, lens, np.full(N, 0.97, np.float32), 1) == 0
+    gold = golden["pre_emphasis_filter"].reshape(N, d.w)
+    for i in range(N):
+        np.testing.assert_array_equal(dst[i, :lens[i]], gold[i, :lens[i]])
+    frames = [l // 160 + 1 for l in lens]
+    mf = max(frames)
+    dd = spectra_desc(N, 257, mf)
+    spec = np.zeros((N, 257, mf), np.float32)
+    assert reference.spectrogram(src, d, spec, dd, lens, True, True, None, 512, 2, 320, 160) == 0
+    gold = golden["spectrogram"].reshape(N, 257, mf)
+    for i in range(N):
+        np.testing.assert_array_equal(spec[i, :, :frames[i]], gold[i, :, :frames[i]])
+    begin = np.zeros(N, np.int32)
+    length = np.zeros(N, np.int32)
+    assert reference.nsr(src, d, lens, begin, length, -60, 2048, 0.0, 8192) == 0
+    np.testing.assert_array_equal(begin, golden["nsr_begin"])
+    np.testing.assert_array_equal(length, golden["nsr_length"])
+    patches = (RpptImagePatch * N)()
+    for i in range(N):
+        patches[i].width, patches[i].height = 1, int(lens[i])
+    db = np.zeros_like(src)
+    assert reference.to_decibels(src, d, db, d, patches, np.float32(np.log(1e-20)), np.float32(np.log(10)), 1.0) == 0
+    gold = golden["to_decibels"].reshape(N, d.w)
+    for i in range(N):
+        np.testing.assert_array_equal(db[i, :lens[i]], gold[i, :lens[i]])

@@ -1,0 +1,151 @@
+"""Cross-checks the C restatement against the reference's own host library on seeded synthetic
+batches, op by op, across the parameter space the reference supports (border types, channel
+counts, rate pairs, mel formulas, ROI shapes, reset intervals).  The float restatements must
+agree bit for bit; this is what lets the GPU tests use the restatement as the oracle on a box
+where the reference sources are absent.
+"""
+import numpy as np
+import pytest
+
+from rpp_b200 import synth
+from rpp_b200.types import audio_desc, spectra_desc, RpptImagePatch, RpptLayout
+
+
+def rng(k):
+    return np.random.Generator(np.random.PCG64(1000 + k))
+
+
+def small_batch(n=6, lo=1, hi=9000, seed=0):
+    r = rng(seed)
+    lens = r.integers(lo, hi, n).astype(np.int32)
+    lens[0] = hi   # one full-stride sample
+    x, lens = synth.mono_batch(n, lens, r, gaps=True)
+    return x, lens
+
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_pre_emphasis(oracle, reference, border):
+    x, lens = small_batch(seed=border)
+    d = audio_desc(len(lens), x.shape[1])
+    coeff = rng(7).uniform(0.5, 0.99, len(lens)).astype(np.float32)
+    a = np.zeros_like(x)
+    b = np.zeros_like(x)
+    oracle.pre_emphasis(x, a, lens, coeff, border)
+    assert reference.pre_emphasis_filter(x, d, b, d, lens, coeff, border) == 0
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("channels", [1, 2, 3, 5, 8, 11])
+@pytest.mark.parametrize("normalize", [False, True])
+def test_down_mixing(oracle, reference, channels, normalize):
+    r = rng(channels)
+    n, L = 4, 3001
+    lens = r.integers(1, L + 1, n).astype(np.int32)
+    x = r.normal(0, 0.3, (n, L * channels)).astype(np.float32)
+    dims = np.stack([lens, np.full(n, channels, np.int32)], 1).ravel().astype(np.int32)
+    sd = audio_desc(n, L, channels=channels, num_dims=3)
+    dd = audio_desc(n, L)
+    a = np.zeros((n, L), np.float32)
+    b = np.zeros((n, L), np.float32)
+    oracle.down_mixing(x, a, dims, normalize)
+    assert reference.down_mixing(x, sd, b, dd, dims, normalize) == 0
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("rates,channels", [((16000, 18400), 1), ((48000, 16000), 1), ((44100, 16000), 1),
+                                            ((22050, 16000), 2), ((16000, 16000), 1), ((8000, 44100), 1)])
+def test_resample(oracle, reference, rates, channels):
+    r = rng(3)
+    n, L = 3, 4000
+    lens = np.array([L, 1777, 1], np.int32)
+    x = r.normal(0, 0.3, (n, L * channels)).astype(np.float32)
+    lut, scale, center, lobes = oracle.windowed_sinc(16 * 64 + 1, 16)
+    ir = np.full(n, rates[0], np.float32)
+    orr = np.full(n, rates[1], np.float32)
+    out_len = int(np.ceil(L * rates[1] / rates[0])) + 8
+    dims = np.stack([lens, np.full(n, channels, np.int32)], 1).ravel().astype(np.int32)
+    sd = audio_desc(n, L, channels=channels)
+    dd = audio_desc(n, out_len, channels=channels)
+    a = np.zeros((n, out_len * channels), np.float32)
+    b = np.zeros((n, out_len * channels), np.float32)
+    oracle.resample(x, a, ir, orr, dims, lut, scale, center, lobes)
+    assert reference.resample(x, sd, b, dd, ir, orr, dims, lut, scale, center, lobes, 16 * 64 + 1) == 0
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("htk,normalize,nfft,nmel,fmin,fmax", [
+    (0, 1, 512, 128, 0.0, 8000.0), (1, 1, 512, 80, 0.0, 0.0), (0, 0, 1024, 64, 60.0, 7600.0),
+    (1, 0, 256, 40, 20.0, 4000.0)])
+def test_mel_filter_bank(oracle, reference, htk, normalize, nfft, nmel, fmin, fmax):
+    r = rng(nfft + nmel)
+    n, bins, T = 3, nfft // 2 + 1, 97
+    frames = np.array([T, 50, 1], np.int32)
+    spec = (r.random((n, bins, T)) ** 4).astype(np.float32)
+    dims = np.stack([np.full(n, bins, np.int32), frames], 1).ravel().astype(np.int32)
+    sd = spectra_desc(n, bins, T)
+    dd = spectra_desc(n, nmel, T)
+    a = np.full((n, nmel, T), -7.0, np.float32)
+    b = np.full((n, nmel, T), -7.0, np.float32)
+    oracle.mel_filter_bank(spec, a, dims, fmax, fmin, htk, nmel, 16000, normalize)
+    assert reference.mel_filter_bank(spec, sd, b, dd, dims, fmax, fmin, htk, nmel, 16000, normalize) == 0
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("two_d,ref", [(False, 0.0), (True, 0.0), (True, 2.5), (False, 1.0)])
+def test_to_decibels(oracle, reference, two_d, ref):
+    r = rng(11)
+    n, H, Wd = 3, 40, 77
+    if two_d:
+        x = (r.random((n, H, Wd)) ** 3).astype(np.float32)
+        wh = [(Wd, H), (30, 12), (1, 1)]
+        sd = spectra_desc(n, H, Wd)
+    else:
+        x = r.normal(0, 1, (n, H * Wd)).astype(np.float32) ** 2
+        wh = [(1, H * Wd), (1, 100), (1, 1)]
+        sd = audio_desc(n, H * Wd)
+    dims = np.array(wh, np.uint32)
+    patches = (RpptImagePatch * n)()
+    for i, (w, h) in enumerate(wh):
+        patches[i].width, patches[i].height = w, h
+    a = np.zeros_like(x)
+    b = np.zeros_like(x)
+    oracle.to_decibels(x, a, dims, -80.0, 10.0, ref)
+    assert reference.to_decibels(x, sd, b, sd, patches, -80.0, 10.0, ref) == 0
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("reset,window,ref,cut", [(8192, 2048, 0.0, -60.0), (-1, 2048, 0.0, -60.0),
+                                                  (1000, 333, 0.0, -40.0), (8192, 2048, 0.05, -20.0)])
+def test_nsr(oracle, reference, reset, window, ref, cut):
+    x, lens = small_batch(n=5, lo=1, hi=20000, seed=5)
+    d = audio_desc(len(lens), x.shape[1])
+    b1, l1 = oracle.nsr(x, lens, cut, window, ref, reset)
+    b2 = np.zeros(len(lens), np.int32)
+    l2 = np.zeros(len(lens), np.int32)
+    assert reference.nsr(x, d, lens, b2, l2, cut, window, ref, reset) == 0
+    np.testing.assert_array_equal(b1, b2)
+    np.testing.assert_array_equal(l1, l2)
+
+
+@pytest.mark.parametrize("nfft,W,hop,center,reflect,layout", [
+    (512, 400, 160, True, True, RpptLayout.NFT), (512, 320, 160, True, False, RpptLayout.NTF),
+    (256, 256, 100, False, True, RpptLayout.NFT), (400, 400, 160, True, True, RpptLayout.NFT)])
+def test_spectrogram_f64_vs_reference(oracle, reference, nfft, W, hop, center, reflect, layout):
+    x, lens = small_batch(n=4, lo=1, hi=6000, seed=9)
+    n = len(lens)
+    F = [oracle.num_windows(l, W, hop, center) for l in lens]
+    mf = max(F)
+    bins = nfft // 2 + 1
+    nft = layout == RpptLayout.NFT
+    dd = spectra_desc(n, bins, mf, layout) if nft else spectra_desc(n, mf, bins, layout)
+    out = np.zeros((n, bins, mf) if nft else (n, mf, bins), np.float32)
+    assert reference.spectrogram(x, audio_desc(n, x.shape[1]), out, dd, lens, center, reflect, None, nfft, 2, W,
+                                 hop) == 0
+    o = oracle.spectrogram_f64(x, lens, center, reflect, None, nfft, 2, W, hop, nft, max_frames=mf)
+    for i in range(n):
+        if F[i] <= 0 or lens[i] < 2:
+            continue
+        g = out[i, :, :F[i]] if nft else out[i, :F[i], :].T
+        e = o[i, :, :F[i]] if nft else o[i, :F[i], :].T
+        scale = np.maximum(g.max(axis=0, keepdims=True), 1e-30)
+        assert (np.abs(e - g) / scale).max() < 2e-6
