@@ -1,0 +1,479 @@
+"""Benchmark of the batched audio front end: clip-seconds per second of
+pre-emphasis -> spectrogram -> mel filter bank -> decibels on the 256-clip ragged batch
+(16 kHz mono clips of 1-16 s; nfft 512, window 400, hop 160, Hann, centred, reflect padding,
+power 2, 128 Slaney mel filters 0-8 kHz normalized, decibels x10 with -80 dB cutoff against the
+per-clip maximum).  Synthetic seeded input with the benchmark's signal model (rpp_b200/synth.py).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One process per GPU (torchrun for N > 1); each rank runs its own batch (weak scaling, no
+collective on the data path).  Rank 0 prints one JSON line.  `--impl reference` times the
+reference's own host (OpenMP) implementation of the same chain on the host cores instead.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from rpp_b200 import synth  # noqa: E402
+from rpp_b200.types import RpptLayout, audio_desc, spectra_desc  # noqa: E402
+
+METRIC = "clip-sec/s for preemph→STFT→mel→dB at stated err vs FP64; p50/p99 serve latency"
+RATE = 16000
+NFFT, WIN, HOP, NMEL = 512, 400, 160, 128
+COEFF, CUTOFF_DB, MULT = 0.97, -80.0, 10.0
+WORKLOAD = ("configs[1]: 256 mono f32 clips @16 kHz, lengths U[1 s, 16 s] with silent gaps; "
+            "pre_emphasis(0.97, ZERO) -> spectrogram(nfft 512, win 400, hop 160, Hann, centred, reflect, power 2, NFT) "
+            "-> mel_filter_bank(128, 0-8 kHz, Slaney, normalized) -> to_decibels(x10, -80 dB, ref = per-clip max)")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--clips", type=int, default=256)
+    return p.parse_args()
+
+
+def frames_of(lengths):
+    return (np.asarray(lengths) // HOP + 1).astype(np.int32)
+
+
+def algorithmic_bytes(lengths):
+    """Compulsory HBM bytes of each op of the unfused chain for the batch (inputs + outputs,
+    valid regions only; the decibel max pass re-reads the mel output)."""
+    L = np.asarray(lengths, np.int64)
+    F = L // HOP + 1
+    return {
+        "pre_emphasis": int((8 * L).sum()),
+        "spectrogram": int((4 * L + 4 * (NFFT // 2 + 1) * F).sum()),
+        "mel_filter_bank": int((4 * (NFFT // 2 + 1) * F + 4 * NMEL * F).sum()),
+        "to_decibels": int((3 * 4 * NMEL * F).sum()),
+    }
+
+
+# ---------------------------------------------------------------- clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([v.strip() for v in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(s[0]) for s in self.samples if len(s) >= 8 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 8 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) >= 8:
+                for k, v in zip(names, s[4:8]):
+                    if v.lower() == "active":
+                        reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- distributed plumbing
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------- the reference arm
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import Reference
+    from rpp_b200.types import RpptImagePatch
+    threads = os.cpu_count() or 1
+    ref = Reference(threads=threads)
+    x, lens = synth.config1(n=args.clips)
+    n, L = x.shape
+    F = frames_of(lens)
+    mf = int(F.max())
+    sd = audio_desc(n, L)
+    pre = np.zeros_like(x)
+    spec = np.zeros((n, NFFT // 2 + 1, mf), np.float32)
+    mel = np.zeros((n, NMEL, mf), np.float32)
+    db = np.zeros_like(mel)
+    coeff = np.full(n, COEFF, np.float32)
+    dims = np.stack([np.full(n, NFFT // 2 + 1, np.int32), F], 1).astype(np.int32).ravel()
+    patches = (RpptImagePatch * n)()
+    for i in range(n):
+        patches[i].width, patches[i].height = int(F[i]), NMEL
+    spd = spectra_desc(n, NFFT // 2 + 1, mf)
+    md = spectra_desc(n, NMEL, mf)
+
+    def step():
+        t0 = time.perf_counter()
+        assert ref.pre_emphasis_filter(x, sd, pre, sd, lens, coeff, 0) == 0
+        assert ref.spectrogram(pre, sd, spec, spd, lens, True, True, None, NFFT, 2, WIN, HOP) == 0
+        assert ref.mel_filter_bank(spec, spd, mel, md, dims, 8000.0, 0.0, 0, NMEL, float(RATE), True) == 0
+        assert ref.to_decibels(mel, md, db, md, patches, CUTOFF_DB, MULT, 0.0) == 0
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    clip_s = float(lens.sum()) / RATE
+    med = statistics.median(times)
+    value = clip_s / med
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "clip-s/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": med * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, configs[1] signal model)",
+        "config": {"workload": WORKLOAD, "clips": n, "clip_seconds": clip_s},
+        "cpu_baseline": {"value": value, "unit": "clip-s/s", "cores": threads, "kind": "reference",
+                         "sample": f"the full {n}-clip batch per step, median of {args.steps} steps"},
+        "e2e": {"value": value, "unit": "clip-s/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+    ref.close()
+
+
+def cpu_baseline_sample(x, lens, sample_clips=256, repeats=5):
+    """The reference's host chain on the same batch (all host threads), median of `repeats`."""
+    from oracle import Reference
+    from rpp_b200.types import RpptImagePatch
+    threads = os.cpu_count() or 1
+    ref = Reference(threads=threads)
+    x = np.ascontiguousarray(x[:sample_clips])
+    lens = np.ascontiguousarray(lens[:sample_clips])
+    n, L = x.shape
+    F = frames_of(lens)
+    mf = int(F.max())
+    sd = audio_desc(n, L)
+    pre = np.zeros_like(x)
+    spec = np.zeros((n, NFFT // 2 + 1, mf), np.float32)
+    mel = np.zeros((n, NMEL, mf), np.float32)
+    db = np.zeros_like(mel)
+    coeff = np.full(n, COEFF, np.float32)
+    dims = np.stack([np.full(n, NFFT // 2 + 1, np.int32), F], 1).astype(np.int32).ravel()
+    patches = (RpptImagePatch * n)()
+    for i in range(n):
+        patches[i].width, patches[i].height = int(F[i]), NMEL
+    spd = spectra_desc(n, NFFT // 2 + 1, mf)
+    md = spectra_desc(n, NMEL, mf)
+    times = []
+    for r in range(repeats + 1):
+        t0 = time.perf_counter()
+        ref.pre_emphasis_filter(x, sd, pre, sd, lens, coeff, 0)
+        ref.spectrogram(pre, sd, spec, spd, lens, True, True, None, NFFT, 2, WIN, HOP)
+        ref.mel_filter_bank(spec, spd, mel, md, dims, 8000.0, 0.0, 0, NMEL, float(RATE), True)
+        ref.to_decibels(mel, md, db, md, patches, CUTOFF_DB, MULT, 0.0)
+        if r:
+            times.append(time.perf_counter() - t0)
+    ref.close()
+    clip_s = float(lens.sum()) / RATE
+    return {"value": clip_s / statistics.median(times), "unit": "clip-s/s", "cores": threads, "kind": "reference",
+            "sample": f"{n} clips ({clip_s:.0f} clip-s) of the same batch, median of {repeats} runs"}
+
+
+# ---------------------------------------------------------------- the B200 arm
+
+class Chain:
+    """The four rppt_*_gpu calls of the plain path on device-resident buffers."""
+
+    def __init__(self, torch, handle, lens_np, n, L):
+        from rpp_b200 import audio
+        self.audio = audio
+        self.torch = torch
+        self.h = handle
+        dev = torch.device("cuda")
+        self.n, self.L = n, L
+        F = frames_of(lens_np)
+        self.F = F
+        self.mf = mf = int(F.max())
+        self.sd = audio_desc(n, L)
+        self.spd = spectra_desc(n, NFFT // 2 + 1, mf)
+        self.md = spectra_desc(n, NMEL, mf)
+        self.lens = torch.from_numpy(lens_np).to(dev)
+        self.coeff = torch.full((n,), COEFF, device=dev)
+        self.dims = torch.from_numpy(np.stack([np.full(n, NFFT // 2 + 1, np.int32), F], 1).astype(np.int32)).to(dev)
+        self.patches = torch.from_numpy(np.stack([F, np.full(n, NMEL, np.int32)], 1).astype(np.int32)).to(dev)
+        self.pre = torch.empty((n, L), device=dev)
+        self.spec = torch.empty((n, NFFT // 2 + 1, mf), device=dev)
+        self.mel = torch.empty((n, NMEL, mf), device=dev)
+        self.db = torch.empty((n, NMEL, mf), device=dev)
+
+    def run(self, x, events=None):
+        a, ok = self.audio, 0
+        ev = events or [None] * 5
+        if ev[0] is not None:
+            ev[0].record()
+        assert a.pre_emphasis_filter(x, self.sd, self.pre, self.sd, self.lens, self.coeff, 0, self.h) == ok
+        if ev[1] is not None:
+            ev[1].record()
+        assert a.spectrogram(self.pre, self.sd, self.spec, self.spd, self.lens, True, True, None, NFFT, 2, WIN, HOP,
+                             self.h) == ok
+        if ev[2] is not None:
+            ev[2].record()
+        assert a.mel_filter_bank(self.spec, self.spd, self.mel, self.md, self.dims, 8000.0, 0.0, 0, NMEL, float(RATE),
+                                 True, self.h) == ok
+        if ev[3] is not None:
+            ev[3].record()
+        assert a.to_decibels(self.mel, self.md, self.db, self.md, self.patches, CUTOFF_DB, MULT, 0.0, self.h) == ok
+        if ev[4] is not None:
+            ev[4].record()
+        return self.db
+
+
+class Fused:
+    """The same chain as one rppb_frontend_gpu call (include/rppb_frontend.h)."""
+
+    def __init__(self, torch, handle, chain):
+        from rpp_b200 import audio
+        from rpp_b200.types import frontend_params
+        self.audio = audio
+        self.h = handle
+        self.c = chain
+        self.params = frontend_params(nfft=NFFT, window_length=WIN, window_step=HOP, num_filter=NMEL,
+                                      sample_rate=float(RATE), min_freq=0.0, max_freq=8000.0, cut_off_db=CUTOFF_DB,
+                                      multiplier=MULT, reference_magnitude=0.0, border=0)
+        self.out = torch.empty_like(chain.db)
+
+    def run(self, x):
+        c = self.c
+        assert self.audio.frontend(x, c.sd, self.out, c.md, c.lens, c.coeff, self.params, self.h) == 0
+        return self.out
+
+
+def error_vs_fp64(chain, x_np, lens_np, clips=8, db_out=None):
+    """Max errors of the GPU chain against the FP64 oracle chain on the first `clips` clips."""
+    from oracle import Oracle
+    orc = Oracle()
+    xs = np.ascontiguousarray(x_np[:clips])
+    ls = np.ascontiguousarray(lens_np[:clips])
+    F = frames_of(ls)
+    mf = int(F.max())
+    spec64 = orc.spectrogram_f64(xs, ls, 1, 1, None, NFFT, 2, WIN, HOP, 1, max_frames=mf,
+                                 preemph_coeff=np.full(clips, COEFF, np.float32), border=0)
+    dims = np.stack([np.full(clips, NFFT // 2 + 1, np.int32), F], 1).astype(np.int32).ravel()
+    mel64 = orc.mel_filter_bank_f64(spec64, dims, 8000.0, 0.0, 0, NMEL, float(RATE), 1)
+    db64 = orc.to_decibels_f64(mel64, np.full(clips, NMEL, np.int32), F, CUTOFF_DB, MULT, 0.0)
+    mel = chain.mel[:clips, :, :mf].cpu().numpy().astype(np.float64)
+    db = (db_out if db_out is not None else chain.db)[:clips, :, :mf].cpu().numpy().astype(np.float64)
+    mel_rel, db_abs = 0.0, 0.0
+    for i in range(clips):
+        m64 = mel64[i, :, :F[i]]
+        scale = np.maximum(m64.max(axis=0, keepdims=True), 1e-30)
+        mel_rel = max(mel_rel, float((np.abs(mel[i, :, :F[i]] - m64) / scale).max()))
+        db_abs = max(db_abs, float(np.abs(db[i, :, :F[i]] - db64[i, :, :F[i]]).max()))
+    return {"mel_power_max_rel_err_per_frame": mel_rel, "db_max_abs_err": db_abs, "clips_checked": clips,
+            "oracle": "FP64 restatement (oracle/rppb_oracle.c)"}
+
+
+def read_traffic(kernel):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    if not os.path.isfile(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from rpp_b200 import lib
+    L_ = lib.load()
+    L_.rppbGetLaunchCount.restype = ctypes.c_longlong
+    x_np, lens_np = synth.config1(n=args.clips)
+    n, L = x_np.shape
+    clip_s = float(lens_np.sum()) / RATE
+    stream = torch.cuda.current_stream()
+    h = lib.Handle(batch_size=n, stream=stream.cuda_stream)
+    chain = Chain(torch, h, lens_np, n, L)
+    x = torch.from_numpy(x_np).cuda()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    fused = Fused(torch, h, chain)
+
+    def timed(fn, steps, per_op=False):
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(steps)] if per_op else None
+        barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for k in range(steps):
+            if per_op:
+                fn(x, evs[k])
+            else:
+                fn(x)
+        end.record()
+        barrier()
+        t = torch.tensor([start.elapsed_time(end)], device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ops = None
+        if per_op:
+            ops = np.zeros(4)
+            for k in range(steps):
+                for o in range(4):
+                    ops[o] += evs[k][o].elapsed_time(evs[k][o + 1])
+            ops /= steps
+        return float(t.item()) / steps, ops
+
+    # ---- device-resident throughput: plain four-call chain, then the fused call (the headline)
+    for _ in range(max(args.warmup, 3)):
+        chain.run(x)
+        fused.run(x)
+    plain_ms, op_ms = timed(chain.run, args.steps, per_op=True)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    launches0 = L_.rppbGetLaunchCount()
+    ms_step, _ = timed(fused.run, args.steps)
+    launches = L_.rppbGetLaunchCount() - launches0
+    clocks = sampler.stop() if sampler else None
+    value = world * clip_s / (ms_step / 1e3)
+    plain_value = world * clip_s / (plain_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers: H2D input, chain, D2H decibels
+    x_host = torch.from_numpy(x_np).pin_memory()
+    out_host = torch.empty(chain.db.shape, dtype=torch.float32).pin_memory()
+    x_dev = torch.empty_like(x)
+    for _ in range(2):
+        x_dev.copy_(x_host, non_blocking=True)
+        out_host.copy_(fused.run(x_dev), non_blocking=True)
+    barrier()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_steps = max(3, args.steps // 2)
+    e_start.record()
+    for _ in range(e_steps):
+        x_dev.copy_(x_host, non_blocking=True)
+        out_host.copy_(fused.run(x_dev), non_blocking=True)
+    e_end.record()
+    barrier()
+    te = torch.tensor([e_start.elapsed_time(e_end)], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(te.item()) / e_steps
+    e2e = {"value": world * clip_s / (e2e_ms / 1e3), "unit": "clip-s/s",
+           "h2d_bytes_per_step": int(x_host.numel() * 4), "d2h_bytes_per_step": int(out_host.numel() * 4),
+           "ms_per_step": e2e_ms,
+           "path": "pinned host input -> rppb_frontend_gpu (C ABI) -> pinned host output, one stream"}
+
+    if rank == 0:
+        peaks = {}
+        pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.isfile(pk):
+            peaks = json.load(open(pk))
+        hbm = peaks.get("hbm_gbs")
+        peak_src = "measured" if hbm else "fallback"
+        hbm = hbm or 6650.0
+        ab = algorithmic_bytes(lens_np)
+        ops = ["pre_emphasis", "spectrogram", "mel_filter_bank", "to_decibels"]
+        per_op = {o: {"ms": float(op_ms[i]), "gbs": ab[o] / (op_ms[i] / 1e3) / 1e9,
+                      "frac_of_" + peak_src + "_hbm": ab[o] / (op_ms[i] / 1e3) / 1e9 / hbm}
+                  for i, o in enumerate(ops)}
+        L64 = lens_np.astype(np.int64)
+        F64 = L64 // HOP + 1
+        fused_bytes = int((4 * L64 + 3 * 4 * NMEL * F64).sum())
+        fused_gbs = fused_bytes / (ms_step / 1e3) / 1e9
+        traffic = read_traffic("frontend_kernel<512>")
+        err = error_vs_fp64(chain, x_np, lens_np, db_out=fused.out)
+        try:
+            cpu = cpu_baseline_sample(x_np, lens_np)
+        except Exception as exc:  # the reference host library is optional on a box without it
+            cpu = {"value": None, "unit": "clip-s/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+        total_bytes = sum(ab.values())
+        line = {
+            "metric": METRIC, "value": value, "unit": "clip-s/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, configs[1] signal model)",
+            "config": {"workload": WORKLOAD,
+                       "path": "fused: one rppb_frontend_gpu call per step (pre-emphasis, STFT, mel, dB in one "
+                               "persistent launch); bit-identical to the four rppt_*_gpu calls",
+                       "clips_per_gpu": n, "clip_seconds_per_gpu": clip_s,
+                       "l2": "inputs larger than L2 (input 262 MB, output 210 MB per step); no flush"},
+            "roofline": {"bound": "hbm", "kernel": "frontend_kernel<512> (rppb_frontend_gpu)", "achieved": fused_gbs,
+                         "peak": hbm, "unit": "GB/s", "frac": fused_gbs / hbm, "peak_source": peak_src + " hbm_gbs",
+                         "traffic": traffic, "algorithmic_bytes_per_launch": fused_bytes, "launch_ms": ms_step,
+                         "algorithmic_bytes": "4 B x samples read + (mel write, mel re-read, dB write) 12 B x 128 x frames"},
+            "plain_chain": {"value": plain_value, "unit": "clip-s/s", "ms_per_step": plain_ms,
+                            "path": "four rppt_*_gpu C-ABI calls per step",
+                            "algorithmic_bytes_per_step": sum(ab.values()),
+                            "frac_of_hbm": sum(ab.values()) / (plain_ms / 1e3) / 1e9 / hbm, "per_op": per_op},
+            "fused_over_plain": plain_ms / ms_step,
+            "err_vs_fp64": err,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    h.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_b200(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,73 @@
+/*
+ * rppb — fused audio front end (extension; no single counterpart in the reference).
+ *
+ * rppb_frontend_gpu computes, in one persistent launch, exactly what this sequence of the
+ * reference's entry points computes (api/rppt_tensor_audio_augmentations.h:156, :232, :274, :122):
+ *
+ *   rppt_pre_emphasis_filter_gpu(src -> pre, srcLength, coeff, borderType)
+ *   rppt_spectrogram_gpu(pre -> spec NFT, srcLength, centerWindows, reflectPadding, windowFunction,
+ *                        nfft, power, windowLength, windowStep)
+ *   rppt_mel_filter_bank_gpu(spec -> mel NFT, {nfft/2+1, frames}, maxFreq, minFreq, melFormula,
+ *                            numFilter, sampleRate, normalize)
+ *   rppt_to_decibels_gpu(mel -> dst, {frames, numFilter}, cutOffDB, multiplier, referenceMagnitude)
+ *
+ * and its outputs are bit-identical to that sequence run through this library.  The
+ * intermediate pre-emphasized signal, spectrum and mel tensors never reach memory except the mel
+ * power, which is written into dst and converted to decibels in place once the clip's maximum is
+ * known.  dst is NFT [numFilter][frames] per sample (hStride >= frames); only the valid frames
+ * are written.  nfft must be a power of two from 128 to 2048.  Asynchronous on the handle stream;
+ * capturable in a CUDA graph after one uncaptured call has sized the handle workspace.
+ */
+#ifndef RPPB_FRONTEND_H
+#define RPPB_FRONTEND_H
+
+#include "rpp.h"
+#include "rppdefs.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct
+{
+    /* pre_emphasis_filter */
+    RpptAudioBorderType borderType;
+    /* spectrogram */
+    bool centerWindows;
+    bool reflectPadding;
+    Rpp32f* windowFunction; /* host pointer, windowLength floats; nullptr = Hann */
+    Rpp32s nfft;
+    Rpp32s power;           /* 2: power, 1: magnitude */
+    Rpp32s windowLength;
+    Rpp32s windowStep;
+    /* mel_filter_bank */
+    Rpp32f maxFreq;         /* 0: sampleRate / 2 */
+    Rpp32f minFreq;
+    RpptMelScaleFormula melFormula;
+    Rpp32s numFilter;
+    Rpp32f sampleRate;
+    bool normalize;
+    /* to_decibels */
+    Rpp32f cutOffDB;
+    Rpp32f multiplier;
+    Rpp32f referenceMagnitude; /* 0: per-sample maximum */
+    /* schedule: clips by which the decibel tiles trail the spectrum tiles (0 = default 8) */
+    Rpp32s lookahead;
+} RppbFrontendParams;
+
+/* srcDesc numDims = 2 (F32 1-D signals); dstDesc numDims = 3, layout NFT, F32.
+ * srcLengthTensor and coeffTensor as for rppt_pre_emphasis_filter_gpu. */
+SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr, RpptDescPtr dstDescPtr,
+                                          Rpp32s* srcLengthTensor, Rpp32f* coeffTensor, const RppbFrontendParams* params,
+                                          rppHandle_t rppHandle);
+
+/* Reads (and clears) the handle's device error word: nonzero when a fused launch gave up
+ * waiting for a clip's spectrum tiles (a bounded wait; the affected tiles are left unconverted).
+ * Synchronizes the handle stream. */
+SHARED_PUBLIC RppStatus rppb_get_device_error(rppHandle_t rppHandle, Rpp32s* errorCode);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RPPB_FRONTEND_H */

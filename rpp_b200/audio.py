@@ -111,3 +111,20 @@ def image_patches(widths, heights):
         arr[i].width = int(w)
         arr[i].height = int(h)
     return arr
+
+
+def frontend(src, src_desc, dst, dst_desc, src_length, coeff, params, handle):
+    """rppb_frontend_gpu: the fused pre-emphasis -> spectrogram -> mel -> decibels chain."""
+    L = _lib.load()
+    return _status(L.rppb_frontend_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                       _addr(src_length), _addr(coeff), ctypes.byref(params), _h(handle)))
+
+
+def device_error(handle):
+    """Reads and clears the handle's device error word (synchronizes the handle stream)."""
+    L = _lib.load()
+    v = ctypes.c_int32(0)
+    st = L.rppb_get_device_error(_h(handle), ctypes.byref(v))
+    if st != 0:
+        raise RuntimeError(f"rppb_get_device_error failed with status {st}")
+    return v.value

@@ -7,6 +7,8 @@
 
 namespace rppb {
 
+void count_launch(int kernels);
+
 // ---------------------------------------------------------------- ragged batches
 // A batch of uneven samples is addressed as one flat list of work units (chunks, frame tiles,
 // reset blocks ...).  prefix[b] is the number of units of samples 0..b-1 (prefix[n] = total),
@@ -57,6 +59,7 @@ template <class Count>
 inline void launch_ragged_prefix(Count count, int n, long long* prefix, cudaStream_t s)
 {
     ragged_prefix_kernel<Count><<<1, 1024, 0, s>>>(count, n, prefix);
+    count_launch(1);
 }
 
 // ---------------------------------------------------------------- float helpers
@@ -82,16 +85,16 @@ __device__ __forceinline__ float warp_max(float v)
 // Reflect an out-of-range index into [minLoc, maxLoc) the way the reference does
 // (src/modules/tensor/cpu/kernel/spectrogram.cpp:55-69): mirror without repeating the edge,
 // repeatedly for short signals; a signal shorter than 2 maps everything to its last sample.
+// The reference's repeated mirroring is periodic with period 2 * (len - 1), so it is evaluated
+// in closed form; the result is always inside [minLoc, maxLoc).
 __device__ __forceinline__ int reflect_index(int loc, int minLoc, int maxLoc)
 {
-    if (maxLoc - minLoc < 2) return maxLoc - 1;
-    for (int guard = 0; guard < 64; ++guard)
-    {
-        if (loc < minLoc) loc = 2 * minLoc - loc;
-        else if (loc >= maxLoc) loc = 2 * maxLoc - 2 - loc;
-        else break;
-    }
-    return loc;
+    const int len = maxLoc - minLoc;
+    if (len < 2) return maxLoc - 1;
+    const int period = 2 * (len - 1);
+    int r = (loc - minLoc) % period;
+    if (r < 0) r += period;
+    return minLoc + (r < len ? r : period - r);
 }
 
 // Frames of a sample (spectrogram.cpp:47-52), never negative.

@@ -15,13 +15,10 @@
 #include <cstring>
 #include <string>
 
+#include "../../include/rppb_frontend.h"
 #include "../../include/rppt_tensor_audio_augmentations.h"
 #include "handle.hpp"
 #include "ops.hpp"
-
-namespace rppb {
-const float2* spectrogram_twiddles(Handle& h, int nfft);
-}
 
 using namespace rppb;
 
@@ -378,6 +375,102 @@ extern "C" SHARED_PUBLIC RppStatus rppt_resample_gpu(RppPtr_t srcPtr, RpptDescPt
                         static_cast<const float*>(h.device_view(inRateTensor, n * sizeof(float), inStage)),
                         static_cast<const float*>(h.device_view(outRateTensor, n * sizeof(float), outStage)),
                         static_cast<const int*>(h.device_view(srcDimsTensor, 2 * n * sizeof(int), dimsStage)), win);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                     RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor,
+                                                     Rpp32f* coeffTensor, const RppbFrontendParams* params,
+                                                     rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr && params, "null descriptor or parameters");
+        const RppbFrontendParams& p = *params;
+        if (srcDescPtr->numDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (dstDescPtr->numDims != 3) return RPP_ERROR_INVALID_DST_DIMS;
+        if (dstDescPtr->layout != NFT) return RPP_ERROR_INVALID_DST_LAYOUT;
+        if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
+        if (!p.multiplier) return RPP_ERROR_ZERO_DIVISION;
+        if (p.maxFreq < 0 || p.maxFreq > p.sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
+        if (p.minFreq < 0 || p.minFreq > p.sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
+        require(srcPtr && dstPtr, "null tensor");
+        require(p.windowLength > 0 && p.windowStep > 0, "windowLength and windowStep must be positive");
+        const int nfft = p.nfft == 0 ? p.windowLength : p.nfft;
+        require(nfft >= p.windowLength, "nfft must be at least windowLength");
+        require(p.numFilter > 0, "numFilter must be positive");
+        if (dstDescPtr->h < Rpp32u(p.numFilter) || dstDescPtr->strides.hStride < dstDescPtr->w)
+            return RPP_ERROR_INVALID_DST_DIMS;
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        const int lookahead = p.lookahead > 0 ? p.lookahead : 8;
+        const size_t scratchBytes = frontend_scratch_bytes(n, lookahead);
+        Carver m(nullptr);
+        m.take<int>(n);
+        m.take<float>(n);
+        m.take<float>(p.windowFunction ? p.windowLength : 0);
+        m.take<char>(scratchBytes);
+        Carver cv(h.workspace(m.used()));
+        int* lenStage = cv.take<int>(n);
+        float* coeffStage = cv.take<float>(n);
+        float* winStage = cv.take<float>(p.windowFunction ? p.windowLength : 0);
+        void* scratch = cv.take<char>(scratchBytes);
+        FrontendArgs a;
+        a.src = static_cast<const float*>(srcPtr);
+        a.srcStride = srcDescPtr->strides.nStride;
+        a.srcElems = size_t(n) * srcDescPtr->strides.nStride;
+        a.dst = static_cast<float*>(dstPtr);
+        a.dstNStride = dstDescPtr->strides.nStride;
+        a.dstHStride = dstDescPtr->strides.hStride;
+        a.n = n;
+        a.len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
+        a.coeff = static_cast<const float*>(h.device_view(coeffTensor, n * sizeof(float), coeffStage));
+        a.border = int(p.borderType);
+        a.center = p.centerWindows;
+        a.reflect = p.reflectPadding;
+        if (p.windowFunction)
+        {
+            h.upload(winStage, p.windowFunction, p.windowLength * sizeof(float));
+            a.window = winStage;
+        }
+        else
+        {
+            a.window = h.table("hann" + std::to_string(p.windowLength), size_t(p.windowLength), build_hann, nullptr);
+        }
+        a.nfft = nfft;
+        a.W = p.windowLength;
+        a.hop = p.windowStep;
+        a.maxFrames = int(dstDescPtr->w);
+        a.power = p.power;
+        a.mel.minFreq = p.minFreq;
+        a.mel.maxFreq = (p.maxFreq == 0) ? p.sampleRate / 2 : p.maxFreq;
+        a.mel.sampleRate = p.sampleRate;
+        a.mel.htk = p.melFormula == HTK ? 1 : 0;
+        a.mel.numFilter = p.numFilter;
+        a.mel.normalize = p.normalize;
+        // to_decibels.cpp:40-45
+        float minRatio = float(std::pow(10, p.cutOffDB / p.multiplier));
+        if (minRatio == 0.0f) minRatio = std::nextafter(0.0f, 1.0f);
+        const Rpp32f log10Factor = 0.3010299956639812;
+        a.minRatio = minRatio;
+        a.multiplier = p.multiplier * log10Factor;
+        a.refMag = p.referenceMagnitude;
+        a.lookahead = lookahead;
+        launch_frontend(h, scratch, a);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppb_get_device_error(rppHandle_t rppHandle, Rpp32s* errorCode)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(errorCode != nullptr, "null errorCode");
+        int* flags = h.device_flags();
+        int v = 0;
+        check_cuda(cudaMemcpyAsync(&v, flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream()), "read device error");
+        check_cuda(cudaMemsetAsync(flags, 0, sizeof(int), h.stream()), "clear device error");
+        check_cuda(cudaStreamSynchronize(h.stream()), "sync");
+        *errorCode = v;
         return RPP_SUCCESS;
     });
 }

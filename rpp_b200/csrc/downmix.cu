@@ -103,6 +103,7 @@ void launch_down_mixing(Handle& h, void* scratch, const float* src, uint32_t src
     launch_ragged_prefix(DownmixCount{dims}, n, prefix, h.stream());
     int grid = persistent_grid(h, reinterpret_cast<const void*>(down_mixing_kernel), kThreads, 0);
     down_mixing_kernel<<<grid, kThreads, 0, h.stream()>>>(src, srcStride, dst, dstStride, dims, normalize, prefix, n);
+    count_launch();
     check_cuda(cudaGetLastError(), "down_mixing_kernel");
 }
 

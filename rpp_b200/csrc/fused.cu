@@ -1,0 +1,304 @@
+// Fused front end: pre-emphasis -> STFT power -> mel filter bank -> decibels in one persistent
+// launch (include/rppb_frontend.h).
+//
+// Work items of two kinds walk one queue, claimed in order with an atomic counter:
+//   spectrum tile (clip b, frames f0..f0+TF): gather the pre-emphasized, reflected, windowed
+//     frames straight from the raw signal (stft.cuh, PreemphSource), FFT them into a shared
+//     power tile, project onto the mel filters from a shared CSR weight table (same weights and
+//     the same ascending-bin float accumulation as the mel_filter_bank kernel), write the mel
+//     power into dst, fold the tile maximum into the clip's float-ordered atomicMax, then count
+//     the tile done;
+//   decibel tile (clip b, same frames): wait until every spectrum tile of clip b is counted (a
+//     bounded wait: a timeout sets the handle's device error word and skips the tile), then
+//     convert the tile in place with the clip's maximum.
+// The queue interleaves them per clip slot: [spectrum tiles of clip s][decibel tiles of clip
+// s - D], so a clip's mel power is re-read D clips after it was written, while it is still in
+// L2.  Claiming items in order makes the waits deadlock-free at any residency: a decibel item's
+// spectrum items have lower indices and were claimed by running CTAs.
+//
+// HBM traffic per clip: the raw signal once, the mel power written, re-read (mostly from L2) and
+// overwritten with decibels: 4 L + (4 + 4 + 4) * numFilter * frames bytes at most, against
+// 8 L + 4 L + 2*4*bins*frames + ... for the four separate calls.
+#include <cfloat>
+
+#include "common.cuh"
+#include "mel_tables.cuh"
+#include "ops.hpp"
+#include "stft.cuh"
+
+namespace rppb {
+
+constexpr int kFusedThreads = 256;
+constexpr long long kWaitLimit = 1ll << 24;   // x ~128 ns sleeps: a few seconds
+
+namespace {
+
+template <int TF>
+struct SlotCount
+{
+    const int* len;
+    int n, D, W, hop, maxFrames;
+    bool center;
+    __device__ int tiles(int b) const
+    {
+        const int F = min(num_windows(len[b], W, hop, center), maxFrames);
+        return F <= 0 ? 0 : (F + TF - 1) / TF;
+    }
+    __device__ long long operator()(int s) const
+    {
+        long long c = 0;
+        if (s < n) c += tiles(s);
+        if (s - D >= 0 && s - D < n) c += tiles(s - D);
+        return c;
+    }
+};
+
+// Shared memory plan (bytes), computed identically on host and device.
+template <int NFFT>
+struct FusedLayout
+{
+    using S = StftShape<NFFT, kFusedThreads>;
+    int nmel;
+    size_t tw, win, work, csrRow, csrBin, csrW, total;
+    __host__ __device__ FusedLayout(int numFilter) : nmel(numFilter)
+    {
+        const int bins = S::BINS;
+        tw = 0;
+        win = tw + size_t(NFFT) * 8;
+        work = win + size_t(NFFT) * 4;
+        // the FFT slots + power tile, or (before the loop) the mel table build
+        size_t fftOut = S::fft_bytes + S::out_bytes;
+        size_t tables = 2 * size_t(numFilter + 2) * 4 + size_t(numFilter) * 4 + 2 * size_t(numFilter + 1) * 8 +
+                        size_t(bins) * 4 + 64;
+        size_t workBytes = (fftOut > tables ? fftOut : tables);
+        csrRow = (work + workBytes + 15) & ~size_t(15);
+        csrBin = (csrRow + size_t(numFilter + 1) * 4 + 15) & ~size_t(15);
+        csrW = (csrBin + size_t(2 * bins + 2) * 4 + 15) & ~size_t(15);
+        total = (csrW + size_t(2 * bins + 2) * 4 + 15) & ~size_t(15);
+    }
+};
+
+template <int NFFT>
+__global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a, const float2* __restrict__ twiddle,
+                                                                 const long long* __restrict__ prefix,
+                                                                 unsigned long long* __restrict__ workCounter,
+                                                                 int* __restrict__ done, unsigned* __restrict__ maxKey,
+                                                                 int* __restrict__ errorWord)
+{
+    using S = StftShape<NFFT, kFusedThreads>;
+    constexpr int TF = S::TF, BINS = S::BINS, LD = S::OUT_LD;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const FusedLayout<NFFT> lay(a.mel.numFilter);
+    float2* s_tw = reinterpret_cast<float2*>(smem + lay.tw);
+    float* s_win = reinterpret_cast<float*>(smem + lay.win);
+    float2* s_fft = reinterpret_cast<float2*>(smem + lay.work);
+    float* s_out = reinterpret_cast<float*>(smem + lay.work + S::fft_bytes);
+    int* csrRow = reinterpret_cast<int*>(smem + lay.csrRow);
+    int* csrBin = reinterpret_cast<int*>(smem + lay.csrBin);
+    float* csrW = reinterpret_cast<float*>(smem + lay.csrW);
+    __shared__ long long s_item;
+    __shared__ float s_warpMax[kFusedThreads / 32];
+    const int nmel = a.mel.numFilter;
+
+    for (int i = threadIdx.x; i < NFFT; i += kFusedThreads) s_tw[i] = twiddle[i];
+    for (int i = threadIdx.x; i < a.W; i += kFusedThreads) s_win[i] = a.window[i];
+
+    // ---- mel weights as CSR rows (filter m: bins of interval m with (1 - wd) * norm, then bins of
+    //      interval m + 1 with wd * norm), built in the work region before it holds FFT data
+    {
+        unsigned char* t = smem + lay.work;
+        MelTableView v;
+        v.first = reinterpret_cast<int*>(t);
+        v.last = v.first + (nmel + 2);
+        v.norm = reinterpret_cast<float*>(v.last + (nmel + 2));
+        size_t o = (size_t(reinterpret_cast<unsigned char*>(v.norm + nmel) - t) + 7) & ~size_t(7);
+        v.f0 = reinterpret_cast<double*>(t + o);
+        v.f1 = v.f0 + (nmel + 1);
+        v.weightsDown = reinterpret_cast<float*>(v.f1 + (nmel + 1));
+        v.range = reinterpret_cast<int*>(v.weightsDown + BINS);
+        build_mel_tables(v, a.mel, NFFT);   // ends with __syncthreads
+        if (threadIdx.x == 0)
+        {
+            int acc = 0;
+            for (int m = 0; m < nmel; ++m)
+            {
+                csrRow[m] = acc;
+                if (v.last[m] > v.first[m]) acc += v.last[m] - v.first[m];
+                if (v.last[m + 1] > v.first[m + 1]) acc += v.last[m + 1] - v.first[m + 1];
+            }
+            csrRow[nmel] = acc;
+        }
+        __syncthreads();
+        for (int m = threadIdx.x; m < nmel; m += kFusedThreads)
+        {
+            int e = csrRow[m];
+            const float nm = v.norm[m];
+            for (int k = v.first[m]; k < v.last[m]; ++k, ++e)
+            {
+                float w = __fsub_rn(1.0f, v.weightsDown[k]);
+                csrBin[e] = k;
+                csrW[e] = a.mel.normalize ? __fmul_rn(w, nm) : w;
+            }
+            for (int k = v.first[m + 1]; k < v.last[m + 1]; ++k, ++e)
+            {
+                const float w = v.weightsDown[k];
+                csrBin[e] = k;
+                csrW[e] = a.mel.normalize ? __fmul_rn(w, nm) : w;
+            }
+        }
+        __syncthreads();
+    }
+
+    const int centerOffset = a.center ? a.W / 2 : 0;
+    const int nslots = a.n + a.lookahead;
+    const long long total = prefix[nslots];
+    const SlotCount<TF> cnt{a.len, a.n, a.lookahead, a.W, a.hop, a.maxFrames, a.center};
+    const int f = threadIdx.x % TF;      // frame column this thread owns in mel / decibel tiles
+    const int g = threadIdx.x / TF;
+    constexpr int kGroups = kFusedThreads / TF;
+
+    for (;;)
+    {
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(workCounter, 1ull);
+        __syncthreads();
+        const long long w = s_item;
+        if (w >= total) break;
+        const int s = ragged_find(prefix, nslots, w);
+        const int local = int(w - prefix[s]);
+        const int c1 = s < a.n ? cnt.tiles(s) : 0;
+        const bool spectrumItem = local < c1;
+        const int b = spectrumItem ? s : s - a.lookahead;
+        const int tile = spectrumItem ? local : local - c1;
+        const int L = a.len[b];
+        const int F = min(num_windows(L, a.W, a.hop, a.center), a.maxFrames);
+        const int f0 = tile * TF;
+        const int Tv = min(TF, F - f0);
+        float* y = a.dst + size_t(b) * a.dstNStride + f0;
+
+        if (spectrumItem)
+        {
+            const float* x = a.src + size_t(b) * a.srcStride;
+            const size_t base = size_t(b) * a.srcStride;
+            const float bval = a.border == 1 ? x[0] : a.border == 2 ? (base + 1 < a.srcElems ? x[1] : 0.f) : 0.f;
+            const PreemphSource src{x, L, a.reflect, a.coeff[b], bval};
+            stft_tile<NFFT, kFusedThreads>(src, f0, F, a.W, a.hop, centerOffset, a.power, s_win, s_tw, s_fft, s_out);
+            __syncthreads();
+            float tmax = -FLT_MAX;
+            if (f < Tv)
+            {
+                for (int m = g; m < nmel; m += kGroups)
+                {
+                    float acc = 0.0f;
+                    for (int e = csrRow[m]; e < csrRow[m + 1]; ++e)
+                        acc = __fadd_rn(acc, __fmul_rn(s_out[csrBin[e] * LD + f], csrW[e]));
+                    y[size_t(m) * a.dstHStride + f] = acc;
+                    tmax = fmaxf(tmax, acc);
+                }
+            }
+            tmax = warp_max(tmax);
+            if ((threadIdx.x & 31) == 0) s_warpMax[threadIdx.x >> 5] = tmax;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                float v = s_warpMax[0];
+                for (int i = 1; i < kFusedThreads / 32; ++i) v = fmaxf(v, s_warpMax[i]);
+                atomicMax(maxKey + b, float_key(v));
+                __threadfence();
+                atomicAdd(done + b, 1);
+            }
+        }
+        else
+        {
+            if (threadIdx.x == 0)
+            {
+                const int need = cnt.tiles(b);
+                long long spins = 0;
+                while (atomicAdd(done + b, 0) < need)
+                {
+                    if (++spins > kWaitLimit)
+                    {
+                        atomicOr(errorWord, 1);
+                        break;
+                    }
+                    __nanosleep(128);
+                }
+                __threadfence();
+                s_item = spins > kWaitLimit ? -1 : w;
+            }
+            __syncthreads();
+            if (s_item >= 0)
+            {
+                float ref = a.refMag;
+                if (a.refMag == 0.f)
+                {
+                    const unsigned k = __ldcg(maxKey + b);
+                    ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
+                }
+                const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
+                if (f < Tv)
+                {
+                    for (int m = g; m < nmel; m += kGroups)
+                    {
+                        float* p = y + size_t(m) * a.dstHStride + f;
+                        float v = __fmul_rn(__ldcg(p), inv);
+                        v = a.minRatio < v ? v : a.minRatio;
+                        *p = __fmul_rn(a.multiplier, log2f(v));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int NFFT>
+void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
+{
+    using S = StftShape<NFFT, kFusedThreads>;
+    const int nslots = a.n + a.lookahead;
+    Carver cv(scratch);
+    long long* prefix = cv.take<long long>(nslots + 1);
+    unsigned long long* counter = cv.take<unsigned long long>(1);
+    int* done = cv.take<int>(a.n);
+    unsigned* maxKey = cv.take<unsigned>(a.n);
+    const size_t clear = reinterpret_cast<char*>(maxKey + a.n) - reinterpret_cast<char*>(counter);
+    check_cuda(cudaMemsetAsync(counter, 0, clear, h.stream()), "memset(frontend state)");
+    launch_ragged_prefix(SlotCount<S::TF>{a.len, a.n, a.lookahead, a.W, a.hop, a.maxFrames, a.center}, nslots, prefix,
+                         h.stream());
+    const FusedLayout<NFFT> lay(a.mel.numFilter);
+    if (lay.total > 200 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
+    const float2* tw = spectrogram_twiddles(h, NFFT);
+    const int grid = persistent_grid(h, reinterpret_cast<const void*>(frontend_kernel<NFFT>), kFusedThreads, lay.total);
+    frontend_kernel<NFFT><<<grid, kFusedThreads, lay.total, h.stream()>>>(a, tw, prefix, counter, done, maxKey,
+                                                                          h.device_flags());
+    count_launch();
+    check_cuda(cudaGetLastError(), "frontend_kernel");
+}
+
+}  // namespace
+
+size_t frontend_scratch_bytes(int n, int lookahead)
+{
+    Carver cv(nullptr);
+    cv.take<long long>(n + lookahead + 1);
+    cv.take<unsigned long long>(1);
+    cv.take<int>(n);
+    cv.take<unsigned>(n);
+    return cv.used();
+}
+
+void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a)
+{
+    if (a.n <= 0) return;
+    switch (a.nfft)
+    {
+        case 128: launch_fused<128>(h, a, scratch); return;
+        case 256: launch_fused<256>(h, a, scratch); return;
+        case 512: launch_fused<512>(h, a, scratch); return;
+        case 1024: launch_fused<1024>(h, a, scratch); return;
+        case 2048: launch_fused<2048>(h, a, scratch); return;
+        default: fail(RPP_ERROR_NOT_IMPLEMENTED, "fused front end needs a power-of-two nfft from 128 to 2048");
+    }
+}
+
+}  // namespace rppb

@@ -2,6 +2,8 @@
 // profiling (reference: api/rpp.h:132-280, src/modules/handle_api.cpp:29-101).
 #include "handle.hpp"
 
+#include <atomic>
+#include <tuple>
 #include <cstring>
 #include <stdexcept>
 
@@ -28,6 +30,7 @@ Handle::~Handle()
     cudaStreamSynchronize(stream_);
     if (ws_) dev_free(ws_);
     for (auto& kv : tables_) cudaFree(kv.second);
+    if (flags_) cudaFree(flags_);
     if (pinned_) cudaFreeHost(pinned_);
     if (pinned_free_) cudaEventDestroy(pinned_free_);
     if (ev_begin_) cudaEventDestroy(ev_begin_);
@@ -165,6 +168,16 @@ const float* Handle::table(const std::string& key, size_t count, void (*build)(f
     return static_cast<const float*>(d);
 }
 
+int* Handle::device_flags()
+{
+    if (!flags_)
+    {
+        check_cuda(cudaMalloc(&flags_, 64 * sizeof(int)), "cudaMalloc(flags)");
+        check_cuda(cudaMemset(flags_, 0, 64 * sizeof(int)), "cudaMemset(flags)");
+    }
+    return flags_;
+}
+
 void Handle::set_allocator(rppAllocatorFunction a, rppDeallocatorFunction d, void* ctx)
 {
     check_cuda(cudaStreamSynchronize(stream_), "cudaStreamSynchronize(set allocator)");
@@ -215,12 +228,33 @@ Handle& deref(rppHandle_t h)
     return *reinterpret_cast<Handle*>(h);
 }
 
+static std::atomic<long long> g_launches{0};
+
+void count_launch(int kernels) { g_launches.fetch_add(kernels, std::memory_order_relaxed); }
+
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
 int persistent_grid(const Handle& h, const void* kernel, int threads, size_t smem)
 {
+    // Cached per (kernel, device, threads, smem) so that repeated calls, including calls made while
+    // a stream is being captured into a CUDA graph, make no further non-stream CUDA API calls.
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
+    const auto key = std::make_tuple(kernel, h.device(), threads, smem);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    if (smem > 48 * 1024)
+        check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem attr");
     int per_sm = 0;
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem), "occupancy");
     if (per_sm < 1) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "kernel does not fit on an SM");
-    return per_sm * h.num_sms();
+    const int grid = per_sm * h.num_sms();
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = grid;
+    return grid;
 }
 
 }  // namespace rppb
@@ -306,6 +340,9 @@ extern "C" SHARED_PUBLIC rppStatus_t rppGetKernelTime(rppHandle_t handle, float*
     if (time == nullptr) return rppStatusBadParm;
     return handle_try([&] { *time = rppb::deref(handle).last_call_ms(); });
 }
+
+// Kernels launched by this library in this process so far.
+extern "C" SHARED_PUBLIC long long rppbGetLaunchCount() { return rppb::launch_count(); }
 
 extern "C" SHARED_PUBLIC rppStatus_t rppEnableProfiling(rppHandle_t handle, bool enable)
 {

@@ -87,6 +87,9 @@ class Handle
     void end_call();
     float last_call_ms();
 
+    // A small zeroed device word array that kernels set on bounded-wait timeouts.
+    int* device_flags();
+
     // Scratch of size `bytes` in pinned host memory, reused after the previous user's copy ended.
     void* staging(size_t bytes);
     void staging_done();
@@ -109,6 +112,7 @@ class Handle
     bool pinned_pending_ = false;
 
     std::map<std::string, void*> tables_;
+    int* flags_ = nullptr;
 
     rppAllocatorFunction alloc_fn_ = nullptr;
     rppDeallocatorFunction free_fn_ = nullptr;
@@ -120,6 +124,10 @@ class Handle
 };
 
 Handle& deref(rppHandle_t h);
+
+// Counts kernel launches made by this library (reported by rppbGetLaunchCount).
+void count_launch(int kernels = 1);
+long long launch_count();
 
 // Number of CTAs for a persistent launch of `kernel` with `threads` threads and `smem` bytes.
 int persistent_grid(const Handle& h, const void* kernel, int threads, size_t smem);

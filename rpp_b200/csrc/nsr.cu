@@ -185,11 +185,13 @@ void launch_nsr(Handle& h, void* scratch, const NsrArgs& a)
     int grid = persistent_grid(h, reinterpret_cast<const void*>(mms_kernel), 128, 0);
     mms_kernel<<<grid, 128, 0, h.stream()>>>(a.src, a.srcStride, a.len, a.windowLength, a.resetInterval, mms,
                                              blockMax, prefix, a.n);
+    count_launch();
     check_cuda(cudaGetLastError(), "mms_kernel");
     const int rgrid = (a.n + kRegionThreads / 32 - 1) / (kRegionThreads / 32);
     region_kernel<<<rgrid, kRegionThreads, 0, h.stream()>>>(mms, a.srcStride, a.len, a.windowLength, a.resetInterval,
                                                             a.referencePower, a.cutOff, blockMax, a.begin, a.length,
                                                             prefix, a.n);
+    count_launch();
     check_cuda(cudaGetLastError(), "region_kernel");
 }
 

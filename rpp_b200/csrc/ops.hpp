@@ -91,4 +91,38 @@ struct NsrArgs
 size_t nsr_scratch_bytes(int n, uint32_t srcStride, int resetInterval);
 void launch_nsr(Handle& h, void* scratch, const NsrArgs& a);
 
+// Mel filter placement parameters (maxFreq already resolved: 0 -> sampleRate / 2).
+struct MelParams
+{
+    float minFreq, maxFreq;
+    float sampleRate;
+    int htk;
+    int numFilter;
+    bool normalize;
+};
+
+// Twiddle table W_nfft^e = (cos, sin)(2*pi*e/nfft), e < nfft, cached on the handle.
+const float2* spectrogram_twiddles(Handle& h, int nfft);
+
+struct FrontendArgs
+{
+    const float* src;
+    uint32_t srcStride;
+    size_t srcElems;
+    float* dst;
+    uint32_t dstNStride, dstHStride;
+    int n;
+    const int* len;
+    const float* coeff;
+    int border;
+    bool center, reflect;
+    const float* window;     // device, W floats
+    int nfft, W, hop, maxFrames, power;
+    MelParams mel;
+    float minRatio, multiplier, refMag;
+    int lookahead;
+};
+size_t frontend_scratch_bytes(int n, int lookahead);
+void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);
+
 }  // namespace rppb

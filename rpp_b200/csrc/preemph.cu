@@ -107,12 +107,14 @@ void launch_pre_emphasis(Handle& h, void* scratch, const float* src, uint32_t sr
         int grid = persistent_grid(h, reinterpret_cast<const void*>(pre_emphasis_kernel<true>), kThreads, 0);
         pre_emphasis_kernel<true><<<grid, kThreads, 0, h.stream()>>>(src, srcStride, dst, dstStride, len, coeff,
                                                                      border, srcElems, prefix, n);
+        count_launch();
     }
     else
     {
         int grid = persistent_grid(h, reinterpret_cast<const void*>(pre_emphasis_kernel<false>), kThreads, 0);
         pre_emphasis_kernel<false><<<grid, kThreads, 0, h.stream()>>>(src, srcStride, dst, dstStride, len, coeff,
                                                                       border, srcElems, prefix, n);
+        count_launch();
     }
     check_cuda(cudaGetLastError(), "pre_emphasis_kernel");
 }

@@ -181,11 +181,10 @@ void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStr
     long long* prefix = static_cast<long long*>(scratch);
     launch_ragged_prefix(ResampleCount{inRate, outRate, dims}, n, prefix, h.stream());
     const size_t smem = size_t(win.lutSize) * sizeof(float);
-    check_cuda(cudaFuncSetAttribute(resample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-               "smem attr");
     int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel), kBlock, smem);
     resample_kernel<<<grid, kBlock, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate, outRate, dims, win,
                                                         prefix, n);
+    count_launch();
     check_cuda(cudaGetLastError(), "resample_kernel");
 }
 

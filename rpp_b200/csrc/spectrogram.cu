@@ -22,28 +22,13 @@
 // FP32 arithmetic in a different order than the reference's third-party FFT: results match the
 // host path within 1e-5 of each frame's largest bin (ffts' own FP32 error is of the same order).
 #include "common.cuh"
-#include "fft.cuh"
 #include "ops.hpp"
+#include "stft.cuh"
 
 namespace rppb {
 namespace {
 
-using fft::Dft;
-
 constexpr int kThreads = 256;
-
-template <int NFFT>
-struct Plan;
-template <>
-struct Plan<128> { static constexpr int R1 = 8, R2 = 8, TF = 32; };
-template <>
-struct Plan<256> { static constexpr int R1 = 16, R2 = 8, TF = 32; };
-template <>
-struct Plan<512> { static constexpr int R1 = 16, R2 = 16, TF = 32; };
-template <>
-struct Plan<1024> { static constexpr int R1 = 32, R2 = 16, TF = 16; };
-template <>
-struct Plan<2048> { static constexpr int R1 = 32, R2 = 32, TF = 16; };
 
 struct SpecCount
 {
@@ -57,27 +42,14 @@ struct SpecCount
     }
 };
 
-// Sample of the (padded) signal at index i.
-__device__ __forceinline__ float padded_sample(const float* __restrict__ x, int L, int i, bool reflect)
-{
-    if (i >= 0 && i < L) return __ldg(x + i);
-    if (!reflect || L <= 0) return 0.f;
-    return __ldg(x + reflect_index(i, 0, L));
-}
-
 template <int NFFT>
 struct SmemLayout
 {
-    static constexpr int M = NFFT / 2;
-    static constexpr int R1 = Plan<NFFT>::R1, R2 = Plan<NFFT>::R2, TF = Plan<NFFT>::TF;
-    static constexpr int G = R2;
-    static constexpr int FPP = kThreads / G;                 // frames per pass
-    static constexpr int BINS = M + 1;
-    static constexpr int FFT_SLOT = R1 * (R2 + 1);           // float2 per frame slot
-    static constexpr size_t tw = 0;                                   // NFFT float2
-    static constexpr size_t fftBuf = tw + size_t(NFFT) * 8;          // FPP * FFT_SLOT float2
-    static constexpr size_t out = fftBuf + size_t(FPP) * FFT_SLOT * 8;   // BINS * (TF+1) float
-    static constexpr size_t win = out + size_t(BINS) * (TF + 1) * 4;     // NFFT floats (window <= nfft)
+    using S = StftShape<NFFT, kThreads>;
+    static constexpr size_t tw = 0;                          // NFFT float2
+    static constexpr size_t fftBuf = tw + size_t(NFFT) * 8;  // FPP frame slots
+    static constexpr size_t out = fftBuf + S::fft_bytes;     // [BINS][TF+1] floats
+    static constexpr size_t win = out + S::out_bytes;        // NFFT floats (window <= nfft)
     static constexpr size_t bytes = win + size_t(NFFT) * 4;
 };
 
@@ -85,25 +57,19 @@ template <int NFFT>
 __global__ void __launch_bounds__(kThreads) spectrogram_fft_kernel(SpectrogramArgs a, const float2* __restrict__ twiddle,
                                                                    const long long* __restrict__ prefix)
 {
-    using S = SmemLayout<NFFT>;
-    constexpr int M = S::M, R1 = S::R1, R2 = S::R2, TF = S::TF, G = S::G, FPP = S::FPP, BINS = S::BINS;
-    static_assert(R1 * R2 == M, "plan");
-    static_assert(R1 % G == 0 || G % R1 == 0, "plan");
+    using L_ = SmemLayout<NFFT>;
+    using S = StftShape<NFFT, kThreads>;
+    constexpr int TF = S::TF, BINS = S::BINS;
     extern __shared__ __align__(16) unsigned char smem[];
-    float2* s_tw = reinterpret_cast<float2*>(smem + S::tw);
-    float2* s_fft = reinterpret_cast<float2*>(smem + S::fftBuf);
-    float* s_out = reinterpret_cast<float*>(smem + S::out);
-    float* s_win = reinterpret_cast<float*>(smem + S::win);
+    float2* s_tw = reinterpret_cast<float2*>(smem + L_::tw);
+    float2* s_fft = reinterpret_cast<float2*>(smem + L_::fftBuf);
+    float* s_out = reinterpret_cast<float*>(smem + L_::out);
+    float* s_win = reinterpret_cast<float*>(smem + L_::win);
 
     const int W = a.windowLength;
     for (int i = threadIdx.x; i < NFFT; i += kThreads) s_tw[i] = twiddle[i];
     for (int i = threadIdx.x; i < W; i += kThreads) s_win[i] = a.window[i];
     __syncthreads();
-
-    const int j = threadIdx.x % G;          // thread within the frame group
-    const int slot = threadIdx.x / G;       // frame slot within a pass
-    float2* buf = s_fft + slot * S::FFT_SLOT;
-    const int off = (W < NFFT) ? (NFFT - W) / 2 : 0;
     const int centerOffset = a.center ? W / 2 : 0;
     const long long total = prefix[a.n];
 
@@ -113,81 +79,10 @@ __global__ void __launch_bounds__(kThreads) spectrogram_fft_kernel(SpectrogramAr
         const int f0 = int(w - prefix[b]) * TF;
         const int L = a.len[b];
         const int F = min(num_windows(L, W, a.windowStep, a.center), a.maxFrames);
-        const float* x = a.src + size_t(b) * a.srcStride;
-
-        for (int pass = 0; pass < TF / FPP + (TF % FPP ? 1 : 0); ++pass)
-        {
-            const int fl = pass * FPP + slot;        // frame within the tile
-            const int frame = f0 + fl;
-            const int ws = frame * a.windowStep - centerOffset;
-            // ---- gather the windowed frame: z[n] = v[2n] + i v[2n+1], thread holds n = j + R2*m
-            float2 z[R1];
-#pragma unroll
-            for (int m = 0; m < R1; ++m)
-            {
-                const int t0 = 2 * (j + R2 * m) - off;   // window index of the real part
-                float re = 0.f, im = 0.f;
-                if (fl < TF && frame < F)
-                {
-                    if (t0 >= 0 && t0 < W) re = s_win[t0] * padded_sample(x, L, ws + t0, a.reflect);
-                    if (t0 + 1 >= 0 && t0 + 1 < W) im = s_win[t0 + 1] * padded_sample(x, L, ws + t0 + 1, a.reflect);
-                }
-                z[m] = make_float2(re, im);
-            }
-            // ---- stage 1: R1-point DFT over m, twiddle W_M^(j*k1) = W_nfft^(2*j*k1)
-            Dft<R1>::run(z);
-#pragma unroll
-            for (int k1 = 0; k1 < R1; ++k1)
-            {
-                const float2 t = s_tw[(2 * j * k1) & (NFFT - 1)];
-                buf[k1 * (R2 + 1) + j] = fft::cmul_conj(z[k1], t.x, t.y);
-            }
-            __syncwarp();
-            // ---- stage 2: R2-point DFTs over j for k1 = j, j+G, ...
-            constexpr int ROWS = R1 / G > 0 ? R1 / G : 1;
-            float2 y[ROWS][R2];
-#pragma unroll
-            for (int r = 0; r < ROWS; ++r)
-            {
-                const int k1 = j + G * r;
-#pragma unroll
-                for (int jj = 0; jj < R2; ++jj) y[r][jj] = (k1 < R1) ? buf[k1 * (R2 + 1) + jj] : make_float2(0.f, 0.f);
-            }
-            __syncwarp();
-#pragma unroll
-            for (int r = 0; r < ROWS; ++r)
-            {
-                const int k1 = j + G * r;
-                Dft<R2>::run(y[r]);
-                if (k1 < R1)
-                {
-#pragma unroll
-                    for (int k2 = 0; k2 < R2; ++k2) buf[k1 + R1 * k2] = y[r][k2];   // Z in natural order
-                }
-            }
-            __syncwarp();
-            // ---- unpack the real spectrum: X[k] = E[k] + W_nfft^k O[k]
-            if (fl < TF)
-            {
-                for (int k = j; k < BINS; k += G)
-                {
-                    const float2 A = buf[k & (M - 1)];
-                    const float2 Bc = buf[(M - k) & (M - 1)];
-                    // E = (A + conj(B)) / 2,  O = (A - conj(B)) / (2i)
-                    const float er = 0.5f * (A.x + Bc.x), ei = 0.5f * (A.y - Bc.y);
-                    const float orr = 0.5f * (A.y + Bc.y), oi = -0.5f * (A.x - Bc.x);
-                    const float2 t = s_tw[k & (NFFT - 1)];
-                    // X = E + (orr + i oi)(c - i s)
-                    const float xr = er + fmaf(orr, t.x, oi * t.y);
-                    const float xi = ei + fmaf(oi, t.x, -orr * t.y);
-                    const float p = fmaf(xr, xr, xi * xi);
-                    s_out[k * (TF + 1) + fl] = (a.power == 1) ? sqrtf(p) : p;
-                }
-            }
-            __syncwarp();
-        }
+        const PlainSource src{a.src + size_t(b) * a.srcStride, L, a.reflect};
+        stft_tile<NFFT, kThreads>(src, f0, F, W, a.windowStep, centerOffset, a.power, s_win, s_tw, s_fft, s_out);
         __syncthreads();
-        // ---- store the tile
+        // store the tile: a warp writes 32 consecutive frames of one bin (NFT) or bins of one frame (NTF)
         const int Tv = min(TF, F - f0);
         float* y = a.dst + size_t(b) * a.dstNStride;
         if (a.nft)
@@ -195,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) spectrogram_fft_kernel(SpectrogramAr
             for (int idx = threadIdx.x; idx < BINS * TF; idx += kThreads)
             {
                 const int k = idx / TF, f = idx % TF;
-                if (f < Tv) y[size_t(k) * a.dstHStride + f0 + f] = s_out[k * (TF + 1) + f];
+                if (f < Tv) y[size_t(k) * a.dstHStride + f0 + f] = s_out[k * S::OUT_LD + f];
             }
         }
         else
@@ -203,7 +98,7 @@ __global__ void __launch_bounds__(kThreads) spectrogram_fft_kernel(SpectrogramAr
             for (int idx = threadIdx.x; idx < BINS * TF; idx += kThreads)
             {
                 const int f = idx / BINS, k = idx % BINS;
-                if (f < Tv) y[size_t(f0 + f) * a.dstHStride + k] = s_out[k * (TF + 1) + f];
+                if (f < Tv) y[size_t(f0 + f) * a.dstHStride + k] = s_out[k * S::OUT_LD + f];
             }
         }
         __syncthreads();
@@ -247,7 +142,7 @@ __global__ void __launch_bounds__(kThreads) spectrogram_dft_kernel(SpectrogramAr
         for (int t = threadIdx.x; t < N; t += kThreads)
         {
             const int u = t - off;
-            s_v[t] = (u >= 0 && u < W) ? a.window[u] * padded_sample(x, L, ws + u, a.reflect) : 0.f;
+            s_v[t] = (u >= 0 && u < W) ? a.window[u] * PlainSource{x, L, a.reflect}(ws + u) : 0.f;
         }
         __syncthreads();
         float* y = a.dst + size_t(b) * a.dstNStride;
@@ -276,14 +171,12 @@ template <int NFFT>
 void launch_fft(Handle& h, long long* prefix, const SpectrogramArgs& a, const float2* tw)
 {
     using S = SmemLayout<NFFT>;
-    launch_ragged_prefix(SpecCount{a.len, a.windowLength, a.windowStep, a.maxFrames, S::TF, a.center}, a.n, prefix,
+    launch_ragged_prefix(SpecCount{a.len, a.windowLength, a.windowStep, a.maxFrames, Plan<NFFT>::TF, a.center}, a.n, prefix,
                          h.stream());
     const size_t smem = S::bytes;
-    check_cuda(cudaFuncSetAttribute(spectrogram_fft_kernel<NFFT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(smem)),
-               "smem attr");
     int grid = persistent_grid(h, reinterpret_cast<const void*>(spectrogram_fft_kernel<NFFT>), kThreads, smem);
     spectrogram_fft_kernel<NFFT><<<grid, kThreads, smem, h.stream()>>>(a, tw, prefix);
+    count_launch();
     check_cuda(cudaGetLastError(), "spectrogram_fft_kernel");
 }
 
@@ -325,10 +218,9 @@ void launch_spectrogram(Handle& h, void* scratch, const SpectrogramArgs& a)
                          h.stream());
     const size_t smem = size_t(a.nfft) * 12;
     if (smem > 200 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "nfft too large for the direct DFT");
-    check_cuda(cudaFuncSetAttribute(spectrogram_dft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-               "smem attr");
     int grid = persistent_grid(h, reinterpret_cast<const void*>(spectrogram_dft_kernel), kThreads, smem);
     spectrogram_dft_kernel<<<grid, kThreads, smem, h.stream()>>>(a, tw, prefix);
+    count_launch();
     check_cuda(cudaGetLastError(), "spectrogram_dft_kernel");
 }
 

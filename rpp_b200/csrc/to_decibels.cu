@@ -136,11 +136,13 @@ void launch_to_decibels(Handle& h, void* scratch, const DecibelArgs& a)
         int grid = persistent_grid(h, reinterpret_cast<const void*>(decibel_max_kernel), kThreads, 0);
         decibel_max_kernel<<<grid, kThreads, 0, h.stream()>>>(a.src, a.srcNStride, a.srcHStride, a.dims, maxKey,
                                                               prefix, a.n);
+        count_launch();
         check_cuda(cudaGetLastError(), "decibel_max_kernel");
         grid = persistent_grid(h, reinterpret_cast<const void*>(decibel_kernel<true>), kThreads, 0);
         decibel_kernel<true><<<grid, kThreads, 0, h.stream()>>>(a.src, a.srcNStride, a.srcHStride, a.dst, a.dstNStride,
                                                                 a.dstHStride, a.dims, maxKey, 0.f, a.minRatio,
                                                                 a.multiplier, prefix, a.n);
+        count_launch();
     }
     else
     {
@@ -149,6 +151,7 @@ void launch_to_decibels(Handle& h, void* scratch, const DecibelArgs& a)
                                                                  a.dstNStride, a.dstHStride, a.dims, nullptr,
                                                                  a.referenceMagnitude, a.minRatio, a.multiplier,
                                                                  prefix, a.n);
+        count_launch();
     }
     check_cuda(cudaGetLastError(), "decibel_kernel");
 }

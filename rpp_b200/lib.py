@@ -6,7 +6,7 @@ Loading fails loudly when the library is missing: there is no CPU fallback.  Bui
 import ctypes
 import os
 
-from .types import RpptDesc, RpptImagePatch, RpptResamplingWindow, RppBackend
+from .types import RpptDesc, RpptImagePatch, RpptResamplingWindow, RppBackend, RppbFrontendParams
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "librppb.so")
 
@@ -16,7 +16,7 @@ EXPORTED = (
     "rppSetAllocator", "rppGetKernelTime", "rppEnableProfiling",
     "rppt_non_silent_region_detection_gpu", "rppt_to_decibels_gpu", "rppt_pre_emphasis_filter_gpu",
     "rppt_down_mixing_gpu", "rppt_spectrogram_gpu", "rppt_mel_filter_bank_gpu", "rppt_resample_gpu",
-    "rppbGetLastError",
+    "rppbGetLastError", "rppbGetLaunchCount", "rppb_frontend_gpu", "rppb_get_device_error",
 )
 
 _lib = None
@@ -59,6 +59,12 @@ def load(path=None):
     for f in ("rppt_non_silent_region_detection_gpu", "rppt_to_decibels_gpu", "rppt_pre_emphasis_filter_gpu",
               "rppt_down_mixing_gpu", "rppt_spectrogram_gpu", "rppt_mel_filter_bank_gpu", "rppt_resample_gpu"):
         getattr(L, f).restype = _I
+    L.rppb_frontend_gpu.argtypes = [_V, _D, _V, _D, _V, _V, ctypes.POINTER(RppbFrontendParams), _V]
+    L.rppb_frontend_gpu.restype = _I
+    L.rppb_get_device_error.argtypes = [_V, ctypes.POINTER(ctypes.c_int32)]
+    L.rppb_get_device_error.restype = _I
+    L.rppbGetLaunchCount.argtypes = []
+    L.rppbGetLaunchCount.restype = ctypes.c_longlong
     L.rppbGetLastError.argtypes = []
     L.rppbGetLastError.restype = ctypes.c_char_p
     _lib = L

@@ -157,3 +157,35 @@ def spectra_desc(n, height, width, layout=RpptLayout.NFT):
     d.strides.cStride = 1
     d.layout = layout
     return d
+
+
+class RppbFrontendParams(ctypes.Structure):
+    """include/rppb_frontend.h: parameters of the fused pre-emphasis -> spectrogram -> mel -> dB call."""
+    _fields_ = [("borderType", ctypes.c_int), ("centerWindows", ctypes.c_bool), ("reflectPadding", ctypes.c_bool),
+                ("windowFunction", ctypes.c_void_p), ("nfft", ctypes.c_int32), ("power", ctypes.c_int32),
+                ("windowLength", ctypes.c_int32), ("windowStep", ctypes.c_int32), ("maxFreq", ctypes.c_float),
+                ("minFreq", ctypes.c_float), ("melFormula", ctypes.c_int), ("numFilter", ctypes.c_int32),
+                ("sampleRate", ctypes.c_float), ("normalize", ctypes.c_bool), ("cutOffDB", ctypes.c_float),
+                ("multiplier", ctypes.c_float), ("referenceMagnitude", ctypes.c_float),
+                ("lookahead", ctypes.c_int32)]
+
+
+assert ctypes.sizeof(RppbFrontendParams) == 72
+
+
+def frontend_params(nfft=512, window_length=400, window_step=160, num_filter=128, sample_rate=16000.0,
+                    min_freq=0.0, max_freq=8000.0, mel_formula=0, normalize=True, cut_off_db=-80.0,
+                    multiplier=10.0, reference_magnitude=0.0, border=0, center=True, reflect=True, power=2,
+                    window=None, lookahead=0):
+    p = RppbFrontendParams()
+    p.borderType = int(border)
+    p.centerWindows = bool(center)
+    p.reflectPadding = bool(reflect)
+    p.windowFunction = window
+    p.nfft, p.power, p.windowLength, p.windowStep = int(nfft), int(power), int(window_length), int(window_step)
+    p.maxFreq, p.minFreq = float(max_freq), float(min_freq)
+    p.melFormula, p.numFilter, p.sampleRate, p.normalize = int(mel_formula), int(num_filter), float(sample_rate), \
+        bool(normalize)
+    p.cutOffDB, p.multiplier, p.referenceMagnitude = float(cut_off_db), float(multiplier), float(reference_magnitude)
+    p.lookahead = int(lookahead)
+    return p

@@ -1,0 +1,116 @@
+"""The fused front end (rppb_frontend_gpu) against the plain four-call chain through the same
+C ABI — bit-identical by construction — and against the FP64 oracle chain."""
+import numpy as np
+import pytest
+import torch
+
+from rpp_b200 import audio, synth
+from rpp_b200.types import RppStatus, audio_desc, spectra_desc, frontend_params
+from gpu_util import dev, host, canvas, frame_rel_err
+
+pytestmark = pytest.mark.gpu
+OK = RppStatus.RPP_SUCCESS
+
+
+def plain_chain(h, x, lens, coeff, p, maxf):
+    n, L = x.shape
+    bins = p.nfft // 2 + 1
+    d = audio_desc(n, L)
+    xd, ld, cd = dev(x), dev(lens), dev(coeff)
+    pre = torch.zeros_like(xd)
+    assert audio.pre_emphasis_filter(xd, d, pre, d, ld, cd, p.borderType, h) == OK
+    spec = torch.zeros((n, bins, maxf), device="cuda")
+    sdsc = spectra_desc(n, bins, maxf)
+    assert audio.spectrogram(pre, d, spec, sdsc, ld, p.centerWindows, p.reflectPadding, None, p.nfft, p.power,
+                             p.windowLength, p.windowStep, h) == OK
+    F = [max(0, min(maxf, (int(l) - (0 if p.centerWindows else p.windowLength)) // p.windowStep + 1)) for l in lens]
+    dims = dev(np.array([[bins, f] for f in F], np.int32))
+    mel = torch.zeros((n, p.numFilter, maxf), device="cuda")
+    mdsc = spectra_desc(n, p.numFilter, maxf)
+    assert audio.mel_filter_bank(spec, sdsc, mel, mdsc, dims, p.maxFreq, p.minFreq, p.melFormula, p.numFilter,
+                                 p.sampleRate, p.normalize, h) == OK
+    db = canvas((n, p.numFilter, maxf))
+    patches = dev(np.array([[f, p.numFilter] for f in F], np.int32))
+    assert audio.to_decibels(mel, mdsc, db, mdsc, patches, p.cutOffDB, p.multiplier, p.referenceMagnitude, h) == OK
+    return host(db), F
+
+
+CASES = [
+    dict(nfft=512, window_length=400, window_step=160, num_filter=128),
+    dict(nfft=512, window_length=320, window_step=160, num_filter=80, border=1, lookahead=1),
+    dict(nfft=256, window_length=256, window_step=100, num_filter=40, mel_formula=1, normalize=False, border=2),
+    dict(nfft=1024, window_length=1024, window_step=256, num_filter=64, reference_magnitude=1.0, lookahead=64),
+    dict(nfft=512, window_length=400, window_step=160, num_filter=128, center=False, reflect=False,
+         cut_off_db=-60.0),
+]
+
+
+@pytest.mark.parametrize("kw", CASES)
+def test_frontend_equals_plain_chain(gpu, kw):
+    r = np.random.Generator(np.random.PCG64(99))
+    lens = r.integers(1, 48000, 11)
+    lens[0], lens[1], lens[2] = 48000, 1, 2
+    x, lens = synth.mono_batch(len(lens), lens.astype(np.int32), r, gaps=True)
+    n, L = x.shape
+    coeff = r.uniform(0.9, 0.99, n).astype(np.float32)
+    p = frontend_params(**kw)
+    maxf = 48000 // p.windowStep + 1
+    ref, F = plain_chain(gpu, x, lens, coeff, p, maxf)
+    out = canvas((n, p.numFilter, maxf))
+    st = audio.frontend(dev(x), audio_desc(n, L), out, spectra_desc(n, p.numFilter, maxf), dev(lens), dev(coeff), p,
+                        gpu)
+    assert st == OK
+    o = host(out)
+    for i in range(n):
+        np.testing.assert_array_equal(o[i, :, :F[i]], ref[i, :, :F[i]])
+        assert (o[i, :, F[i]:] == -12345.0).all()
+    assert audio.device_error(gpu) == 0
+
+
+def test_frontend_vs_fp64_oracle(gpu, oracle):
+    """Error of the fused chain against the FP64 chain: mel power within 1e-5 of each frame's
+    maximum, decibels within 1e-3 dB."""
+    x, lens = synth.config1(n=12, max_len=64000)
+    n, L = x.shape
+    coeff = np.full(n, 0.97, np.float32)
+    p = frontend_params()
+    F = (lens // 160 + 1).astype(np.int32)
+    mf = int(F.max())
+    out = canvas((n, 128, mf))
+    assert audio.frontend(dev(x), audio_desc(n, L), out, spectra_desc(n, 128, mf), dev(lens), dev(coeff), p,
+                          gpu) == OK
+    o = host(out)
+    spec64 = oracle.spectrogram_f64(x, lens, 1, 1, None, 512, 2, 400, 160, 1, max_frames=mf, preemph_coeff=coeff)
+    dims = np.stack([np.full(n, 257, np.int32), F], 1).ravel()
+    mel64 = oracle.mel_filter_bank_f64(spec64, dims, 8000.0, 0.0, 0, 128, 16000.0, 1)
+    db64 = oracle.to_decibels_f64(mel64, np.full(n, 128, np.int32), F, -80.0, 10.0, 0.0)
+    for i in range(n):
+        assert np.abs(o[i, :, :F[i]] - db64[i, :, :F[i]]).max() < 1e-3
+
+
+def test_frontend_graph_capture(gpu):
+    """After one uncaptured call sized the workspace, the fused call captures into a CUDA graph
+    and replays to the same result."""
+    x, lens = synth.config1(n=16, max_len=48000)
+    n, L = x.shape
+    p = frontend_params()
+    mf = 48000 // 160 + 1
+    xd, ld, cd = dev(x), dev(lens), dev(np.full(n, 0.97, np.float32))
+    out = canvas((n, 128, mf))
+    sd, dd = audio_desc(n, L), spectra_desc(n, 128, mf)
+    assert audio.frontend(xd, sd, out, dd, ld, cd, p, gpu) == OK
+    first = host(out).copy()
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    gpu.set_stream(s.cuda_stream)
+    try:
+        with torch.cuda.stream(s):
+            out.fill_(0.0)
+            torch.cuda.synchronize()
+            with torch.cuda.graph(g, stream=s):
+                assert audio.frontend(xd, sd, out, dd, ld, cd, p, gpu) == OK
+        g.replay()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(host(out), first)
+    finally:
+        gpu.set_stream(torch.cuda.current_stream().cuda_stream)
