@@ -296,14 +296,20 @@ def error_vs_fp64(chain, x_np, lens_np, clips=8, db_out=None):
     db64 = orc.to_decibels_f64(mel64, np.full(clips, NMEL, np.int32), F, CUTOFF_DB, MULT, 0.0)
     mel = chain.mel[:clips, :, :mf].cpu().numpy().astype(np.float64)
     db = (db_out if db_out is not None else chain.db)[:clips, :, :mf].cpu().numpy().astype(np.float64)
-    mel_rel, db_abs = 0.0, 0.0
+    mel_rel, db_abs, db_near = 0.0, 0.0, 0.0
     for i in range(clips):
         m64 = mel64[i, :, :F[i]]
         scale = np.maximum(m64.max(axis=0, keepdims=True), 1e-30)
         mel_rel = max(mel_rel, float((np.abs(mel[i, :, :F[i]] - m64) / scale).max()))
-        db_abs = max(db_abs, float(np.abs(db[i, :, :F[i]] - db64[i, :, :F[i]]).max()))
-    return {"mel_power_max_rel_err_per_frame": mel_rel, "db_max_abs_err": db_abs, "clips_checked": clips,
-            "oracle": "FP64 restatement (oracle/rppb_oracle.c)"}
+        d64 = db64[i, :, :F[i]]
+        err = np.abs(db[i, :, :F[i]] - d64)
+        near = d64 >= d64.max(axis=0, keepdims=True) - 60.0
+        db_abs = max(db_abs, float(err.max()))
+        db_near = max(db_near, float(err[near].max()))
+    return {"mel_power_max_rel_err_per_frame": mel_rel, "db_max_abs_err": db_abs,
+            "db_max_abs_err_within_60db_of_frame_max": db_near, "clips_checked": clips,
+            "oracle": "FP64 restatement (oracle/rppb_oracle.c)",
+            "note": "mel from the plain chain, dB from the fused call (bit-identical chains)"}
 
 
 def read_traffic(kernel):

@@ -61,6 +61,41 @@ SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPt
                                           Rpp32s* srcLengthTensor, Rpp32f* coeffTensor, const RppbFrontendParams* params,
                                           rppHandle_t rppHandle);
 
+/* Down-mix to mono and resample in one launch: equal, bit for bit, to rppt_down_mixing_gpu
+ * (normalizeWeights) followed by a mono rppt_resample_gpu with the window described by
+ * lookup/lookupSize/scale/center/lobes (the RpptResamplingWindow fields, passed as plain values so C
+ * callers can use it; lookup in device or pinned memory, or pageable host memory).  srcDimsTensor =
+ * {length, channels} per sample of interleaved input; dst receives mono samples at outRate.
+ * Extension used by the multi-rate front end (no single counterpart in the reference). */
+SHARED_PUBLIC RppStatus rppb_downmix_resample_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                  RpptDescPtr dstDescPtr, Rpp32f* inRateTensor, Rpp32f* outRateTensor,
+                                                  Rpp32s* srcDimsTensor, bool normalizeWeights, const Rpp32f* lookup,
+                                                  Rpp32s lookupSize, Rpp32f scale, Rpp32f center, Rpp32s lobes,
+                                                  rppHandle_t rppHandle);
+
+/* One clip of a serving batch: buffers anywhere in device memory. */
+typedef struct
+{
+    const Rpp32f* src;   /* mono input at inRate, `length` samples */
+    Rpp32f* work;        /* scratch for the signal resampled to outRate: ceil(length * outRate / inRate) floats */
+    Rpp32f* dst;         /* decibels, NFT [numFilter][dstStride] */
+    Rpp32s length;
+    Rpp32f inRate;
+    Rpp32s dstStride;    /* frames dst holds per filter row (>= the clip's frame count) */
+    Rpp32s pad;
+} RppbClip;
+
+/* The whole multi-rate front end over a table of clips: resample every clip to outRate
+ * (rppt_resample_gpu semantics, mono) into its `work` buffer, then rppb_frontend_gpu on it into
+ * `dst`.  Two launches (+ their work-list scans), no host synchronization, graph-capturable: the
+ * table is read on the device, so a captured graph replays over whatever clips the table holds
+ * (a clip of length 0 is skipped).  clips: device or pinned memory, numClips entries.
+ * Extension for continuous-batching servers (no counterpart in the reference). */
+SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips, Rpp32s numClips, Rpp32f outRate,
+                                                const Rpp32f* lookup, Rpp32s lookupSize, Rpp32f scale, Rpp32f center,
+                                                Rpp32s lobes, Rpp32f preemphCoeff, const RppbFrontendParams* params,
+                                                rppHandle_t rppHandle);
+
 /* Reads (and clears) the handle's device error word: nonzero when a fused launch gave up
  * waiting for a clip's spectrum tiles (a bounded wait; the affected tiles are left unconverted).
  * Synchronizes the handle stream. */

@@ -128,3 +128,13 @@ def device_error(handle):
     if st != 0:
         raise RuntimeError(f"rppb_get_device_error failed with status {st}")
     return v.value
+
+
+def downmix_resample(src, src_desc, dst, dst_desc, in_rate, out_rate, src_dims, normalize_weights, lut, scale, center,
+                     lobes, handle):
+    """rppb_downmix_resample_gpu: down-mix to mono and resample in one launch."""
+    L = _lib.load()
+    return _status(L.rppb_downmix_resample_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                               _addr(in_rate), _addr(out_rate), _addr(src_dims),
+                                               bool(normalize_weights), _addr(lut), int(len(lut)), float(scale),
+                                               float(center), int(lobes), _h(handle)))

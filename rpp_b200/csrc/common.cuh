@@ -97,6 +97,17 @@ __device__ __forceinline__ int reflect_index(int loc, int minLoc, int maxLoc)
     return minLoc + (r < len ? r : period - r);
 }
 
+// Resampled length ceil(length * outRate / inRate) in the reference's float arithmetic
+// (resample.cpp:57); equal rates keep the length.
+__host__ __device__ __forceinline__ int resampled_length(int L, float inRate, float outRate)
+{
+#ifdef __CUDA_ARCH__
+    return inRate == outRate ? L : int(ceilf(__fdiv_rn(__fmul_rn(float(L), outRate), inRate)));
+#else
+    return inRate == outRate ? L : int(ceilf(float(L) * outRate / inRate));
+#endif
+}
+
 // Frames of a sample (spectrogram.cpp:47-52), never negative.
 __host__ __device__ __forceinline__ int num_windows(int length, int windowLength, int windowStep, bool center)
 {

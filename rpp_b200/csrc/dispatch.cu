@@ -333,51 +333,130 @@ extern "C" SHARED_PUBLIC RppStatus rppt_mel_filter_bank_gpu(RppPtr_t srcPtr, Rpp
     });
 }
 
+namespace {
+
+RppStatus resample_common(Handle& h, RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr, RpptDescPtr dstDescPtr,
+                          Rpp32f* inRateTensor, Rpp32f* outRateTensor, Rpp32s* srcDimsTensor, const float* lutHost,
+                          int lutSize, float scale, float center, int lobes, bool downmix, bool normalize)
+{
+    require(srcDescPtr && dstDescPtr, "null descriptor");
+    const Rpp32u tensorDims = Rpp32u(srcDescPtr->numDims - 1);
+    if (tensorDims != 1 && tensorDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+    if (!is_f32(srcDescPtr)) return RPP_ERROR_NOT_IMPLEMENTED;
+    if (downmix && !is_f32(dstDescPtr)) return RPP_ERROR_NOT_IMPLEMENTED;
+    require(srcPtr && dstPtr, "null tensor");
+    const int n = int(srcDescPtr->n);
+    if (n <= 0) return RPP_SUCCESS;
+    require(lutHost != nullptr && lutSize >= 2, "resampling window has no lookup table");
+    require(lobes >= 0, "negative lobes");
+    require(size_t(lutSize) * sizeof(float) <= 200 * 1024, "lookup table above 200 KB");
+    Carver m(nullptr);
+    m.take<float>(n);
+    m.take<float>(n);
+    m.take<int>(2 * n);
+    m.take<float>(lutSize);
+    m.take<char>(prefix_bytes(n));
+    Carver cv(h.workspace(m.used()));
+    float* inStage = cv.take<float>(n);
+    float* outStage = cv.take<float>(n);
+    int* dimsStage = cv.take<int>(2 * n);
+    float* lutStage = cv.take<float>(lutSize);
+    void* scratch = cv.take<char>(prefix_bytes(n));
+    ResampleWindowDev win;
+    win.lut = static_cast<const float*>(h.device_view(lutHost, lutSize * sizeof(float), lutStage));
+    win.lutSize = lutSize;
+    win.scale = scale;
+    win.center = center;
+    win.lobes = lobes;
+    launch_resample(h, scratch, static_cast<const float*>(srcPtr), srcDescPtr->strides.nStride,
+                    static_cast<float*>(dstPtr), dstDescPtr->strides.nStride, n,
+                    static_cast<const float*>(h.device_view(inRateTensor, n * sizeof(float), inStage)),
+                    static_cast<const float*>(h.device_view(outRateTensor, n * sizeof(float), outStage)),
+                    static_cast<const int*>(h.device_view(srcDimsTensor, 2 * n * sizeof(int), dimsStage)), win,
+                    downmix, normalize);
+    return RPP_SUCCESS;
+}
+
+}  // namespace
+
 extern "C" SHARED_PUBLIC RppStatus rppt_resample_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
                                                      RpptDescPtr dstDescPtr, Rpp32f* inRateTensor,
                                                      Rpp32f* outRateTensor, Rpp32s* srcDimsTensor,
                                                      RpptResamplingWindow& window, rppHandle_t rppHandle)
 {
     return guarded(rppHandle, [&](Handle& h) {
-        require(srcDescPtr && dstDescPtr, "null descriptor");
-        const Rpp32u tensorDims = Rpp32u(srcDescPtr->numDims - 1);
-        if (tensorDims != 1 && tensorDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
-        if (!is_f32(srcDescPtr)) return RPP_ERROR_NOT_IMPLEMENTED;
-        require(srcPtr && dstPtr, "null tensor");
-        const int n = int(srcDescPtr->n);
-        if (n <= 0) return RPP_SUCCESS;
         const float* lutHost = window.lookupPinned ? window.lookupPinned : window.lookup.data();
-        const int lutSize = window.lookupSize;
-        require(lutHost != nullptr && lutSize >= 2, "resampling window has no lookup table");
-        require(window.lookupPinned != nullptr || int(window.lookup.size()) >= lutSize, "lookup shorter than lookupSize");
-        require(window.lobes >= 0, "negative lobes");
-        require(size_t(lutSize) * sizeof(float) <= 200 * 1024, "lookup table above 200 KB");
-        Carver m(nullptr);
-        m.take<float>(n);
-        m.take<float>(n);
-        m.take<int>(2 * n);
-        m.take<float>(lutSize);
-        m.take<char>(prefix_bytes(n));
-        Carver cv(h.workspace(m.used()));
-        float* inStage = cv.take<float>(n);
-        float* outStage = cv.take<float>(n);
-        int* dimsStage = cv.take<int>(2 * n);
-        float* lutStage = cv.take<float>(lutSize);
-        void* scratch = cv.take<char>(prefix_bytes(n));
-        ResampleWindowDev win;
-        win.lut = static_cast<const float*>(h.device_view(lutHost, lutSize * sizeof(float), lutStage));
-        win.lutSize = lutSize;
-        win.scale = window.scale;
-        win.center = window.center;
-        win.lobes = window.lobes;
-        launch_resample(h, scratch, static_cast<const float*>(srcPtr), srcDescPtr->strides.nStride,
-                        static_cast<float*>(dstPtr), dstDescPtr->strides.nStride, n,
-                        static_cast<const float*>(h.device_view(inRateTensor, n * sizeof(float), inStage)),
-                        static_cast<const float*>(h.device_view(outRateTensor, n * sizeof(float), outStage)),
-                        static_cast<const int*>(h.device_view(srcDimsTensor, 2 * n * sizeof(int), dimsStage)), win);
-        return RPP_SUCCESS;
+        require(window.lookupPinned != nullptr || int(window.lookup.size()) >= window.lookupSize,
+                "lookup shorter than lookupSize");
+        return resample_common(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, inRateTensor, outRateTensor, srcDimsTensor,
+                               lutHost, window.lookupSize, window.scale, window.center, window.lobes, false, false);
     });
 }
+
+extern "C" SHARED_PUBLIC RppStatus rppb_downmix_resample_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                             RpptDescPtr dstDescPtr, Rpp32f* inRateTensor,
+                                                             Rpp32f* outRateTensor, Rpp32s* srcDimsTensor,
+                                                             bool normalizeWeights, const Rpp32f* lookup,
+                                                             Rpp32s lookupSize, Rpp32f scale, Rpp32f center,
+                                                             Rpp32s lobes, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        return resample_common(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, inRateTensor, outRateTensor, srcDimsTensor,
+                               lookup, lookupSize, scale, center, lobes, true, normalizeWeights);
+    });
+}
+
+namespace {
+
+// Validates the fused-front-end parameters and fills the shared fields of FrontendArgs.
+RppStatus frontend_params(Handle& h, const RppbFrontendParams* params, float* winStage, FrontendArgs& a)
+{
+    require(params != nullptr, "null parameters");
+    const RppbFrontendParams& p = *params;
+    if (!p.multiplier) return RPP_ERROR_ZERO_DIVISION;
+    if (p.maxFreq < 0 || p.maxFreq > p.sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
+    if (p.minFreq < 0 || p.minFreq > p.sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
+    require(p.windowLength > 0 && p.windowStep > 0, "windowLength and windowStep must be positive");
+    const int nfft = p.nfft == 0 ? p.windowLength : p.nfft;
+    require(nfft >= p.windowLength, "nfft must be at least windowLength");
+    require(p.numFilter > 0, "numFilter must be positive");
+    a.border = int(p.borderType);
+    a.center = p.centerWindows;
+    a.reflect = p.reflectPadding;
+    if (p.windowFunction)
+    {
+        h.upload(winStage, p.windowFunction, p.windowLength * sizeof(float));
+        a.window = winStage;
+    }
+    else
+    {
+        a.window = h.table("hann" + std::to_string(p.windowLength), size_t(p.windowLength), build_hann, nullptr);
+    }
+    a.nfft = nfft;
+    a.W = p.windowLength;
+    a.hop = p.windowStep;
+    a.power = p.power;
+    a.mel.minFreq = p.minFreq;
+    a.mel.maxFreq = (p.maxFreq == 0) ? p.sampleRate / 2 : p.maxFreq;
+    a.mel.sampleRate = p.sampleRate;
+    a.mel.htk = p.melFormula == HTK ? 1 : 0;
+    a.mel.numFilter = p.numFilter;
+    a.mel.normalize = p.normalize;
+    // to_decibels.cpp:40-45
+    float minRatio = float(std::pow(10, p.cutOffDB / p.multiplier));
+    if (minRatio == 0.0f) minRatio = std::nextafter(0.0f, 1.0f);
+    const Rpp32f log10Factor = 0.3010299956639812;
+    a.minRatio = minRatio;
+    a.multiplier = p.multiplier * log10Factor;
+    a.refMag = p.referenceMagnitude;
+    a.lookahead = p.lookahead > 0 ? p.lookahead : 8;
+    a.clips = nullptr;
+    a.outRate = 0.f;
+    a.coeffAll = 0.f;
+    return RPP_SUCCESS;
+}
+
+}  // namespace
 
 extern "C" SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
                                                      RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor,
@@ -386,36 +465,31 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPt
 {
     return guarded(rppHandle, [&](Handle& h) {
         require(srcDescPtr && dstDescPtr && params, "null descriptor or parameters");
-        const RppbFrontendParams& p = *params;
         if (srcDescPtr->numDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
         if (dstDescPtr->numDims != 3) return RPP_ERROR_INVALID_DST_DIMS;
         if (dstDescPtr->layout != NFT) return RPP_ERROR_INVALID_DST_LAYOUT;
         if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
-        if (!p.multiplier) return RPP_ERROR_ZERO_DIVISION;
-        if (p.maxFreq < 0 || p.maxFreq > p.sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
-        if (p.minFreq < 0 || p.minFreq > p.sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
         require(srcPtr && dstPtr, "null tensor");
-        require(p.windowLength > 0 && p.windowStep > 0, "windowLength and windowStep must be positive");
-        const int nfft = p.nfft == 0 ? p.windowLength : p.nfft;
-        require(nfft >= p.windowLength, "nfft must be at least windowLength");
-        require(p.numFilter > 0, "numFilter must be positive");
-        if (dstDescPtr->h < Rpp32u(p.numFilter) || dstDescPtr->strides.hStride < dstDescPtr->w)
+        if (dstDescPtr->h < Rpp32u(params->numFilter) || dstDescPtr->strides.hStride < dstDescPtr->w)
             return RPP_ERROR_INVALID_DST_DIMS;
         const int n = int(srcDescPtr->n);
         if (n <= 0) return RPP_SUCCESS;
-        const int lookahead = p.lookahead > 0 ? p.lookahead : 8;
+        const int lookahead = params->lookahead > 0 ? params->lookahead : 8;
         const size_t scratchBytes = frontend_scratch_bytes(n, lookahead);
+        const int W = params->windowLength > 0 ? params->windowLength : 0;
         Carver m(nullptr);
         m.take<int>(n);
         m.take<float>(n);
-        m.take<float>(p.windowFunction ? p.windowLength : 0);
+        m.take<float>(params->windowFunction ? W : 0);
         m.take<char>(scratchBytes);
         Carver cv(h.workspace(m.used()));
         int* lenStage = cv.take<int>(n);
         float* coeffStage = cv.take<float>(n);
-        float* winStage = cv.take<float>(p.windowFunction ? p.windowLength : 0);
+        float* winStage = cv.take<float>(params->windowFunction ? W : 0);
         void* scratch = cv.take<char>(scratchBytes);
         FrontendArgs a;
+        RppStatus st = frontend_params(h, params, winStage, a);
+        if (st != RPP_SUCCESS) return st;
         a.src = static_cast<const float*>(srcPtr);
         a.srcStride = srcDescPtr->strides.nStride;
         a.srcElems = size_t(n) * srcDescPtr->strides.nStride;
@@ -425,37 +499,63 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPt
         a.n = n;
         a.len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
         a.coeff = static_cast<const float*>(h.device_view(coeffTensor, n * sizeof(float), coeffStage));
-        a.border = int(p.borderType);
-        a.center = p.centerWindows;
-        a.reflect = p.reflectPadding;
-        if (p.windowFunction)
-        {
-            h.upload(winStage, p.windowFunction, p.windowLength * sizeof(float));
-            a.window = winStage;
-        }
-        else
-        {
-            a.window = h.table("hann" + std::to_string(p.windowLength), size_t(p.windowLength), build_hann, nullptr);
-        }
-        a.nfft = nfft;
-        a.W = p.windowLength;
-        a.hop = p.windowStep;
         a.maxFrames = int(dstDescPtr->w);
-        a.power = p.power;
-        a.mel.minFreq = p.minFreq;
-        a.mel.maxFreq = (p.maxFreq == 0) ? p.sampleRate / 2 : p.maxFreq;
-        a.mel.sampleRate = p.sampleRate;
-        a.mel.htk = p.melFormula == HTK ? 1 : 0;
-        a.mel.numFilter = p.numFilter;
-        a.mel.normalize = p.normalize;
-        // to_decibels.cpp:40-45
-        float minRatio = float(std::pow(10, p.cutOffDB / p.multiplier));
-        if (minRatio == 0.0f) minRatio = std::nextafter(0.0f, 1.0f);
-        const Rpp32f log10Factor = 0.3010299956639812;
-        a.minRatio = minRatio;
-        a.multiplier = p.multiplier * log10Factor;
-        a.refMag = p.referenceMagnitude;
-        a.lookahead = lookahead;
+        launch_frontend(h, scratch, a);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips, Rpp32s numClips, Rpp32f outRate,
+                                                           const Rpp32f* lookup, Rpp32s lookupSize, Rpp32f scale,
+                                                           Rpp32f center, Rpp32s lobes, Rpp32f preemphCoeff,
+                                                           const RppbFrontendParams* params, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(clips != nullptr && params != nullptr, "null clip table or parameters");
+        require(lookup != nullptr && lookupSize >= 2 && lobes >= 0, "invalid resampling window");
+        require(size_t(lookupSize) * sizeof(float) <= 200 * 1024, "lookup table above 200 KB");
+        require(outRate > 0.f, "outRate must be positive");
+        const int n = numClips;
+        if (n <= 0) return RPP_SUCCESS;
+        const int lookahead = params->lookahead > 0 ? params->lookahead : 8;
+        const size_t scratchBytes = frontend_scratch_bytes(n, lookahead);
+        const int W = params->windowLength > 0 ? params->windowLength : 0;
+        Carver m(nullptr);
+        m.take<RppbClip>(n);
+        m.take<float>(lookupSize);
+        m.take<float>(params->windowFunction ? W : 0);
+        m.take<char>(prefix_bytes(n));
+        m.take<char>(scratchBytes);
+        Carver cv(h.workspace(m.used()));
+        RppbClip* clipStage = cv.take<RppbClip>(n);
+        float* lutStage = cv.take<float>(lookupSize);
+        float* winStage = cv.take<float>(params->windowFunction ? W : 0);
+        void* resampleScratch = cv.take<char>(prefix_bytes(n));
+        void* scratch = cv.take<char>(scratchBytes);
+        FrontendArgs a;
+        RppStatus st = frontend_params(h, params, winStage, a);
+        if (st != RPP_SUCCESS) return st;
+        const RppbClip* dclips = static_cast<const RppbClip*>(h.device_view(clips, n * sizeof(RppbClip), clipStage));
+        ResampleWindowDev win;
+        win.lut = static_cast<const float*>(h.device_view(lookup, lookupSize * sizeof(float), lutStage));
+        win.lutSize = lookupSize;
+        win.scale = scale;
+        win.center = center;
+        win.lobes = lobes;
+        launch_resample_clips(h, resampleScratch, dclips, n, outRate, win);
+        a.src = nullptr;
+        a.srcStride = 0;
+        a.srcElems = 0;
+        a.dst = nullptr;
+        a.dstNStride = 0;
+        a.dstHStride = 0;
+        a.n = n;
+        a.len = nullptr;
+        a.coeff = nullptr;
+        a.maxFrames = 0;
+        a.clips = dclips;
+        a.outRate = outRate;
+        a.coeffAll = preemphCoeff;
         launch_frontend(h, scratch, a);
         return RPP_SUCCESS;
     });

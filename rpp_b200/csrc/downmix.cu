@@ -11,6 +11,7 @@
 // Streaming kernel: persistent CTAs over 1024-output chunks of the ragged batch; consecutive
 // threads take consecutive outputs, so each warp reads one contiguous span of interleaved input.
 #include "common.cuh"
+#include "downmix.cuh"
 #include "ops.hpp"
 
 namespace rppb {
@@ -29,16 +30,6 @@ struct DownmixCount
         return l <= 0 ? 0 : (l + kChunk - 1) / kChunk;
     }
 };
-
-__device__ __forceinline__ float hsum4(const float* p)
-{
-    return __fadd_rn(__fadd_rn(p[0], p[1]), __fadd_rn(p[2], p[3]));
-}
-__device__ __forceinline__ float hsum8(const float* p)
-{
-    return __fadd_rn(__fadd_rn(__fadd_rn(p[0], p[4]), __fadd_rn(p[2], p[6])),
-                     __fadd_rn(__fadd_rn(p[1], p[5]), __fadd_rn(p[3], p[7])));
-}
 
 __global__ void __launch_bounds__(kThreads) down_mixing_kernel(const float* __restrict__ src, uint32_t srcStride,
                                                                float* __restrict__ dst, uint32_t dstStride,
@@ -60,34 +51,10 @@ __global__ void __launch_bounds__(kThreads) down_mixing_kernel(const float* __re
             continue;
         }
         if (C > kMaxChannels) continue;   // rejected by the dispatch layer when it can see the dims
-        const float w0 = 1.f / float(C);
-        float inv = 1.f;
-        if (normalize)
-        {
-            float sum = 0.0f;
-            for (int c = 0; c < C; ++c) sum = __fadd_rn(sum, w0);
-            inv = __double2float_rn(__ddiv_rn(1.0, double(sum)));
-        }
-        const float wc = normalize ? __fmul_rn(w0, inv) : w0;   // every channel has the same weight
-        const int lanes = C > 7 ? 8 : 4;
-        const int aligned = (C / lanes) * lanes;
+        const MonoMix mix{x, C, MonoMix::weight(C, normalize)};
         for (int t = chunk * kChunk + threadIdx.x; t < min(L, (chunk + 1) * kChunk); t += kThreads)
         {
-            const float* xs = x + size_t(t) * C;
-            float acc;
-            if (C == 2)
-            {
-                // fewer than 4 channels: the SIMD part sums nothing, both channels go through the tail
-                acc = __fadd_rn(__fadd_rn(0.f, __fmul_rn(xs[0], wc)), __fmul_rn(xs[1], wc));
-            }
-            else
-            {
-                float p[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                for (int g = 0; g < aligned; g += lanes)
-                    for (int l = 0; l < lanes; ++l) p[l] = __fadd_rn(p[l], __fmul_rn(xs[g + l], wc));
-                acc = lanes == 8 ? hsum8(p) : hsum4(p);
-                for (int c = aligned; c < C; ++c) acc = __fadd_rn(acc, __fmul_rn(xs[c], wc));
-            }
+            const float acc = mix(t);
             y[t] = acc;
         }
     }

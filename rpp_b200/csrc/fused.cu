@@ -33,15 +33,39 @@ constexpr long long kWaitLimit = 1ll << 24;   // x ~128 ns sleeps: a few seconds
 
 namespace {
 
+// Where clip b lives: uniform-stride batch, or one entry of a clip table.
+struct ClipView
+{
+    const float* x;
+    int L;
+    float* y;
+    uint32_t hStride;
+    int maxFrames;
+    float coeff;
+    bool hasSecond;   // x[1] may be read (REFLECT border of a 1-sample clip)
+};
+
+__device__ __forceinline__ ClipView clip_view(const FrontendArgs& a, int b)
+{
+    if (a.clips)
+    {
+        const RppbClip c = a.clips[b];
+        const int L = c.length <= 0 ? 0 : resampled_length(c.length, c.inRate, a.outRate);
+        return {c.work, L, c.dst, uint32_t(c.dstStride), c.dstStride, a.coeffAll, L >= 2};
+    }
+    return {a.src + size_t(b) * a.srcStride, a.len[b], a.dst + size_t(b) * a.dstNStride, a.dstHStride, a.maxFrames,
+            a.coeff[b], size_t(b) * a.srcStride + 1 < a.srcElems};
+}
+
 template <int TF>
 struct SlotCount
 {
-    const int* len;
-    int n, D, W, hop, maxFrames;
-    bool center;
+    FrontendArgs a;
+    int n, D;
     __device__ int tiles(int b) const
     {
-        const int F = min(num_windows(len[b], W, hop, center), maxFrames);
+        const ClipView c = clip_view(a, b);
+        const int F = min(num_windows(c.L, a.W, a.hop, a.center), c.maxFrames);
         return F <= 0 ? 0 : (F + TF - 1) / TF;
     }
     __device__ long long operator()(int s) const
@@ -152,7 +176,7 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
     const int centerOffset = a.center ? a.W / 2 : 0;
     const int nslots = a.n + a.lookahead;
     const long long total = prefix[nslots];
-    const SlotCount<TF> cnt{a.len, a.n, a.lookahead, a.W, a.hop, a.maxFrames, a.center};
+    const SlotCount<TF> cnt{a, a.n, a.lookahead};
     const int f = threadIdx.x % TF;      // frame column this thread owns in mel / decibel tiles
     const int g = threadIdx.x / TF;
     constexpr int kGroups = kFusedThreads / TF;
@@ -169,18 +193,19 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
         const bool spectrumItem = local < c1;
         const int b = spectrumItem ? s : s - a.lookahead;
         const int tile = spectrumItem ? local : local - c1;
-        const int L = a.len[b];
-        const int F = min(num_windows(L, a.W, a.hop, a.center), a.maxFrames);
+        const ClipView cv = clip_view(a, b);
+        const int L = cv.L;
+        const int F = min(num_windows(L, a.W, a.hop, a.center), cv.maxFrames);
         const int f0 = tile * TF;
         const int Tv = min(TF, F - f0);
-        float* y = a.dst + size_t(b) * a.dstNStride + f0;
+        float* y = cv.y + f0;
+        const uint32_t hs = cv.hStride;
 
         if (spectrumItem)
         {
-            const float* x = a.src + size_t(b) * a.srcStride;
-            const size_t base = size_t(b) * a.srcStride;
-            const float bval = a.border == 1 ? x[0] : a.border == 2 ? (base + 1 < a.srcElems ? x[1] : 0.f) : 0.f;
-            const PreemphSource src{x, L, a.reflect, a.coeff[b], bval};
+            const float* x = cv.x;
+            const float bval = a.border == 1 ? x[0] : a.border == 2 ? (cv.hasSecond ? x[1] : 0.f) : 0.f;
+            const PreemphSource src{x, L, a.reflect, cv.coeff, bval};
             stft_tile<NFFT, kFusedThreads>(src, f0, F, a.W, a.hop, centerOffset, a.power, s_win, s_tw, s_fft, s_out);
             __syncthreads();
             float tmax = -FLT_MAX;
@@ -191,7 +216,7 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
                     float acc = 0.0f;
                     for (int e = csrRow[m]; e < csrRow[m + 1]; ++e)
                         acc = __fadd_rn(acc, __fmul_rn(s_out[csrBin[e] * LD + f], csrW[e]));
-                    y[size_t(m) * a.dstHStride + f] = acc;
+                    y[size_t(m) * hs + f] = acc;
                     tmax = fmaxf(tmax, acc);
                 }
             }
@@ -239,7 +264,7 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
                 {
                     for (int m = g; m < nmel; m += kGroups)
                     {
-                        float* p = y + size_t(m) * a.dstHStride + f;
+                        float* p = y + size_t(m) * hs + f;
                         float v = __fmul_rn(__ldcg(p), inv);
                         v = a.minRatio < v ? v : a.minRatio;
                         *p = __fmul_rn(a.multiplier, log2f(v));
@@ -263,8 +288,7 @@ void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
     unsigned* maxKey = cv.take<unsigned>(a.n);
     const size_t clear = reinterpret_cast<char*>(maxKey + a.n) - reinterpret_cast<char*>(counter);
     check_cuda(cudaMemsetAsync(counter, 0, clear, h.stream()), "memset(frontend state)");
-    launch_ragged_prefix(SlotCount<S::TF>{a.len, a.n, a.lookahead, a.W, a.hop, a.maxFrames, a.center}, nslots, prefix,
-                         h.stream());
+    launch_ragged_prefix(SlotCount<S::TF>{a, a.n, a.lookahead}, nslots, prefix, h.stream());
     const FusedLayout<NFFT> lay(a.mel.numFilter);
     if (lay.total > 200 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
     const float2* tw = spectrogram_twiddles(h, NFFT);

@@ -237,22 +237,25 @@ long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 int persistent_grid(const Handle& h, const void* kernel, int threads, size_t smem)
 {
     // Cached per (kernel, device, threads, smem) so that repeated calls, including calls made while
-    // a stream is being captured into a CUDA graph, make no further non-stream CUDA API calls.
+    // a stream is being captured into a CUDA graph, make no further non-stream CUDA API calls.  The
+    // kernel's dynamic shared-memory limit only ever grows (one kernel serves several sizes).
     static std::mutex mu;
     static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
+    static std::map<std::pair<const void*, int>, size_t> smemLimit;
     const auto key = std::make_tuple(kernel, h.device(), threads, smem);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    size_t& limit = smemLimit[std::make_pair(kernel, h.device())];
+    if (smem > 48 * 1024 && smem > limit)
     {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = cache.find(key);
-        if (it != cache.end()) return it->second;
-    }
-    if (smem > 48 * 1024)
         check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem attr");
+        limit = smem;
+    }
     int per_sm = 0;
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem), "occupancy");
     if (per_sm < 1) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "kernel does not fit on an SM");
     const int grid = per_sm * h.num_sms();
-    std::lock_guard<std::mutex> lock(mu);
     cache[key] = grid;
     return grid;
 }

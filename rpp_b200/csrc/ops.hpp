@@ -4,6 +4,7 @@
 // layer out of the handle workspace.
 #pragma once
 
+#include "../../include/rppb_frontend.h"
 #include "handle.hpp"
 
 namespace rppb {
@@ -23,8 +24,14 @@ struct ResampleWindowDev
     float scale, center;
     int lobes;
 };
+// downmix: the input is interleaved {length, channels} and is down-mixed to mono while resampling
+// (equal to rppt_down_mixing_gpu followed by a mono rppt_resample_gpu).
 void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStride, float* dst, uint32_t dstStride, int n,
-                     const float* inRate, const float* outRate, const int* dims, const ResampleWindowDev& win);
+                     const float* inRate, const float* outRate, const int* dims, const ResampleWindowDev& win,
+                     bool downmix = false, bool normalize = false);
+// Mono resample of a clip table: clips[b].src (length at inRate) -> clips[b].work at outRate.
+void launch_resample_clips(Handle& h, void* scratch, const RppbClip* clips, int n, float outRate,
+                           const ResampleWindowDev& win);
 
 struct SpectrogramArgs
 {
@@ -121,6 +128,11 @@ struct FrontendArgs
     MelParams mel;
     float minRatio, multiplier, refMag;
     int lookahead;
+    // clip-table mode (clips != nullptr): clip b reads clips[b].work (clips[b].length resampled from
+    // inRate to outRate), writes clips[b].dst with hStride clips[b].dstStride, pre-emphasis coeffAll
+    const RppbClip* clips;
+    float outRate;
+    float coeffAll;
 };
 size_t frontend_scratch_bytes(int n, int lookahead);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);

@@ -16,6 +16,7 @@
 // others stage the table; then one output per thread.  Inputs are read through L1 (neighbouring
 // outputs share taps).  Compute-bound: 2 * lobes taps of ~10 float operations per output.
 #include "common.cuh"
+#include "downmix.cuh"
 #include "ops.hpp"
 
 namespace rppb {
@@ -34,12 +35,24 @@ struct ResampleCount
     const float* inRate;
     const float* outRate;
     const int* dims;
+    bool mix;
+    const RppbClip* clips;   // table mode when set (mono, outRate = outRateAll)
+    float outRateAll;
     __device__ long long operator()(int b) const
     {
-        const int L = dims[2 * b], C = dims[2 * b + 1];
-        if (L <= 0 || C <= 0) return 0;
-        if (inRate[b] == outRate[b]) return ((long long)L * C + kCopyChunk - 1) / kCopyChunk;
-        const int outEnd = out_length(L, inRate[b], outRate[b]);
+        int L, C, Cs;
+        float ir, orr;
+        if (clips)
+        {
+            L = clips[b].length, C = 1, Cs = 1, ir = clips[b].inRate, orr = outRateAll;
+        }
+        else
+        {
+            L = dims[2 * b], Cs = dims[2 * b + 1], C = mix ? 1 : Cs, ir = inRate[b], orr = outRate[b];
+        }
+        if (L <= 0 || Cs <= 0) return 0;
+        if (ir == orr) return ((long long)L * C + kCopyChunk - 1) / kCopyChunk;
+        const int outEnd = out_length(L, ir, orr);
         return outEnd <= 0 ? 0 : (outEnd + kBlock - 1) / kBlock;
     }
 };
@@ -72,12 +85,16 @@ struct Win
     }
 };
 
+// kMix: the input is interleaved multi-channel and is down-mixed to mono on the fly (MonoMix), so
+// the launch equals rppt_down_mixing_gpu followed by a mono rppt_resample_gpu.
+template <bool kMix, bool kTable>
 __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restrict__ src, uint32_t srcStride,
                                                           float* __restrict__ dst, uint32_t dstStride,
                                                           const float* __restrict__ inRateT,
                                                           const float* __restrict__ outRateT,
                                                           const int* __restrict__ dims, ResampleWindowDev wd,
-                                                          const long long* __restrict__ prefix, int n)
+                                                          bool normalize, const long long* __restrict__ prefix, int n,
+                                                          const RppbClip* __restrict__ clips, float outRateAll)
 {
     extern __shared__ float s_lut[];
     __shared__ float s_phase[kBlock];
@@ -90,13 +107,27 @@ __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restric
     {
         const int b = ragged_find(prefix, n, w);
         const int unit = int(w - prefix[b]);
-        const int L = dims[2 * b], C = dims[2 * b + 1];
-        const float inRate = inRateT[b], outRate = outRateT[b];
-        const float* x = src + size_t(b) * srcStride;
-        float* y = dst + size_t(b) * dstStride;
+        const int L = kTable ? clips[b].length : dims[2 * b];
+        const int Csrc = kTable ? 1 : dims[2 * b + 1];
+        const int C = kMix ? 1 : Csrc;   // channels of the resampled signal
+        const float inRate = kTable ? clips[b].inRate : inRateT[b];
+        const float outRate = kTable ? outRateAll : outRateT[b];
+        const float* x = kTable ? clips[b].src : src + size_t(b) * srcStride;
+        float* y = kTable ? clips[b].work : dst + size_t(b) * dstStride;
+        if (kTable) dstStride = 0x7fffffffu;   // work holds the whole resampled clip
+        const MonoMix mix{x, kMix ? Csrc : 1, kMix ? MonoMix::weight(max(Csrc, 1), normalize) : 1.f};
+        if (kMix && Csrc > 64) continue;
         if (inRate == outRate)
         {
-            const long long count = min((long long)L * C, (long long)min(srcStride, dstStride));
+            if (kMix)
+            {
+                const long long count = min((long long)L, (long long)dstStride);
+                for (long long i = (long long)unit * kCopyChunk + threadIdx.x;
+                     i < min(count, (long long)(unit + 1) * kCopyChunk); i += blockDim.x)
+                    y[i] = mix(i);
+                continue;
+            }
+            const long long count = kTable ? (long long)L : min((long long)L * C, (long long)min(srcStride, dstStride));
             for (long long i = (long long)unit * kCopyChunk + threadIdx.x; i < min(count, (long long)(unit + 1) * kCopyChunk);
                  i += blockDim.x)
                 y[i] = x[i];
@@ -127,8 +158,10 @@ __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restric
             if (loc0 + inBlockRounded < 0) loc0 = -inBlockRounded;
             if (loc1 + inBlockRounded > L) loc1 = L - inBlockRounded;
             const float* in = x + (long long)inBlockRounded * C;
-            if (C == 1)
+            if (kMix || C == 1)
             {
+                // mono input: sample l of the block, down-mixed when kMix
+                auto at = [&](int l) -> float { return kMix ? mix((long long)inBlockRounded + l) : __ldg(in + l); };
                 int l = loc0;
                 const float locBegin = __fsub_rn(float(l), inPos);
                 float lane[4] = {__fadd_rn(locBegin, 0.f), __fadd_rn(locBegin, 1.f), __fadd_rn(locBegin, 2.f),
@@ -139,14 +172,14 @@ __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restric
 #pragma unroll
                     for (int j = 0; j < 4; ++j)
                     {
-                        acc4[j] = __fadd_rn(acc4[j], __fmul_rn(__ldg(in + l + j), win.lane(lane[j])));
+                        acc4[j] = __fadd_rn(acc4[j], __fmul_rn(at(l + j), win.lane(lane[j])));
                         lane[j] = __fadd_rn(lane[j], 4.f);
                     }
                 }
                 float accum = __fadd_rn(__fadd_rn(acc4[0], acc4[2]), __fadd_rn(acc4[1], acc4[3]));
                 float xx = __fsub_rn(float(l), inPos);
                 for (; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
-                    accum = __fadd_rn(accum, __fmul_rn(__ldg(in + l), win.scalar(xx)));
+                    accum = __fadd_rn(accum, __fmul_rn(at(l), win.scalar(xx)));
                 y[outPos] = accum;
             }
             else
@@ -175,17 +208,43 @@ __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restric
 }  // namespace
 
 void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStride, float* dst, uint32_t dstStride,
-                     int n, const float* inRate, const float* outRate, const int* dims, const ResampleWindowDev& win)
+                     int n, const float* inRate, const float* outRate, const int* dims, const ResampleWindowDev& win,
+                     bool downmix, bool normalize)
 {
     if (n <= 0) return;
     long long* prefix = static_cast<long long*>(scratch);
-    launch_ragged_prefix(ResampleCount{inRate, outRate, dims}, n, prefix, h.stream());
+    launch_ragged_prefix(ResampleCount{inRate, outRate, dims, downmix, nullptr, 0.f}, n, prefix, h.stream());
     const size_t smem = size_t(win.lutSize) * sizeof(float);
-    int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel), kBlock, smem);
-    resample_kernel<<<grid, kBlock, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate, outRate, dims, win,
-                                                        prefix, n);
+    if (downmix)
+    {
+        int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel<true, false>), kBlock, smem);
+        resample_kernel<true, false><<<grid, kBlock, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate,
+                                                                         outRate, dims, win, normalize, prefix, n,
+                                                                         nullptr, 0.f);
+    }
+    else
+    {
+        int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel<false, false>), kBlock, smem);
+        resample_kernel<false, false><<<grid, kBlock, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate,
+                                                                          outRate, dims, win, normalize, prefix, n,
+                                                                          nullptr, 0.f);
+    }
     count_launch();
     check_cuda(cudaGetLastError(), "resample_kernel");
+}
+
+void launch_resample_clips(Handle& h, void* scratch, const RppbClip* clips, int n, float outRate,
+                           const ResampleWindowDev& win)
+{
+    if (n <= 0) return;
+    long long* prefix = static_cast<long long*>(scratch);
+    launch_ragged_prefix(ResampleCount{nullptr, nullptr, nullptr, false, clips, outRate}, n, prefix, h.stream());
+    const size_t smem = size_t(win.lutSize) * sizeof(float);
+    int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel<false, true>), kBlock, smem);
+    resample_kernel<false, true><<<grid, kBlock, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr,
+                                                                     win, false, prefix, n, clips, outRate);
+    count_launch();
+    check_cuda(cudaGetLastError(), "resample_kernel(clips)");
 }
 
 }  // namespace rppb

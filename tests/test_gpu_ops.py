@@ -402,3 +402,33 @@ def test_status_codes(gpu):
     assert audio.non_silent_region_detection(x, d3, lens, b, b, -60, 2048, 0.0, 8192,
                                              gpu) == RppStatus.RPP_ERROR_INVALID_SRC_DIMS
     torch.cuda.synchronize()
+
+
+# ---------------------------------------------------------------- fused down-mix + resample
+
+@pytest.mark.parametrize("channels,normalize", [(2, False), (2, True), (1, False), (5, False)])
+def test_downmix_resample_equals_two_calls(gpu, channels, normalize):
+    from rpp_b200.windows import kaiser_sinc
+    r = rng(71 + channels)
+    n, L = 6, 20000
+    lens = r.integers(1, L + 1, n).astype(np.int32)
+    lens[0] = L
+    rates = np.array([16000, 22050, 44100, 48000, 48000, 16000], np.float32)
+    x = r.normal(0, 0.3, (n, L * channels)).astype(np.float32)
+    lut, scale, center, lobes = kaiser_sinc(16)
+    out_len = int(np.ceil(L * 16000 / 16000)) + 8
+    dims = dev(np.stack([lens, np.full(n, channels, np.int32)], 1).astype(np.int32))
+    mono_dims = dev(np.stack([lens, np.ones(n, np.int32)], 1).astype(np.int32))
+    xd = dev(x)
+    mono = canvas((n, L))
+    assert audio.down_mixing(xd, audio_desc(n, L, channels=channels, num_dims=3), mono, audio_desc(n, L), dims,
+                             normalize, gpu) == OK
+    ref = canvas((n, out_len))
+    lut_d = dev(lut)
+    win = audio.resampling_window(lut_d, scale, center, lobes)
+    ir, orr = dev(rates), dev(np.full(n, 16000, np.float32))
+    assert audio.resample(mono, audio_desc(n, L), ref, audio_desc(n, out_len), ir, orr, mono_dims, win, gpu) == OK
+    out = canvas((n, out_len))
+    assert audio.downmix_resample(xd, audio_desc(n, L, channels=channels, num_dims=3), out, audio_desc(n, out_len),
+                                  ir, orr, dims, normalize, lut_d, scale, center, lobes, gpu) == OK
+    np.testing.assert_array_equal(host(out), host(ref))
