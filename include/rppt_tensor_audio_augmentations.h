@@ -48,6 +48,25 @@ SHARED_PUBLIC RppStatus rppt_to_decibels_gpu(RppPtr_t srcPtr, RpptDescPtr srcDes
                                              RpptImagePatchPtr srcDims, Rpp32f cutOffDB, Rpp32f multiplier,
                                              Rpp32f referenceMagnitude, rppHandle_t rppHandle);
 
+/* Allocation-free to_decibels for callers that cannot allocate device memory: code running inside
+ * another runtime's memory pool or under a fixed device-memory budget, real-time audio threads that
+ * must not block on cudaMalloc (it can synchronize the device and take driver locks), and callers
+ * without an rppHandle_t (creating one sets up a workspace).  No counterpart in the reference.
+ *
+ * Same arguments and results as rppt_to_decibels_gpu, except that it takes the CUDA stream directly
+ * instead of a handle, srcDims must be in device or pinned memory, and it allocates nothing: its
+ * scratch (work list and per-sample maxima, ~98 KB) is a fixed array inside the library that every
+ * GPU loading the library holds until the process exits.  Limit: at most 8192 samples per call;
+ * larger batches return RPP_ERROR_OUT_OF_BOUND_SCRATCH_MEMORY_SIZE (split them).  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress, with that device current): make
+ * that first call before any stream capture.  All calls share the one array, so calls that can run
+ * on the GPU at the same time (different streams, overlapping graphs) race: order them on one
+ * stream or with events. */
+SHARED_PUBLIC RppStatus rppt_to_decibels_gpu_static(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                    RpptDescPtr dstDescPtr, RpptImagePatchPtr srcDims, Rpp32f cutOffDB,
+                                                    Rpp32f multiplier, Rpp32f referenceMagnitude,
+                                                    rppAcceleratorQueue_t stream);
+
 /* y[0] = x[0] - coeff * border, y[i] = x[i] - coeff * x[i-1] for 0 < i < length, with border
  * 0 (ZERO), x[0] (CLAMP) or x[1] (REFLECT).  srcDesc numDims = 2.
  * Replaces api/rppt_tensor_audio_augmentations.h:156. */

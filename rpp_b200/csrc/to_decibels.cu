@@ -14,7 +14,10 @@
 // chunks of one row of a 2-D sample.  The log is CUDA's log2f (1 ulp): results agree with the
 // host path within 1e-5 dB, far inside the 1e-3 dB parity bound.
 #include <cfloat>
+#include <cmath>
+#include <mutex>
 
+#include "../../include/rppt_tensor_audio_augmentations.h"
 #include "common.cuh"
 #include "ops.hpp"
 
@@ -157,3 +160,130 @@ void launch_to_decibels(Handle& h, void* scratch, const DecibelArgs& a)
 }
 
 }  // namespace rppb
+
+// ---------------------------------------------------------------- allocation-free variant
+//
+// rppt_to_decibels_gpu_static: the same computation as rppt_to_decibels_gpu for callers that
+// must not allocate device memory (see include/rppt_tensor_audio_augmentations.h).  Its scratch
+// (the work-list prefix and the per-sample maxima) is a file-scope __device__ array that every GPU
+// loading this library holds until the process exits; host code reaches it only through the address
+// cudaGetSymbolAddress returns for the current device, fetched once per device on the first call.
+namespace rppb {
+namespace {
+
+constexpr int kStaticMaxSamples = 8192;
+constexpr size_t kStaticPrefixBytes = (size_t(kStaticMaxSamples) + 1) * sizeof(long long);
+constexpr size_t kStaticScratchBytes = kStaticPrefixBytes + size_t(kStaticMaxSamples) * sizeof(unsigned);
+
+static __device__ __align__(256) unsigned char g_decibel_scratch[kStaticScratchBytes];
+
+constexpr int kStaticMaxDevices = 64;
+struct StaticDevice
+{
+    unsigned char* scratch;   // device address of g_decibel_scratch on this device
+    int gridMax, gridTrue, gridFalse;
+    bool ready;
+};
+StaticDevice g_static[kStaticMaxDevices];
+std::mutex g_static_mutex;
+
+// Once per device, with that device current: the scratch address and the persistent grid sizes.
+cudaError_t static_setup(int device, StaticDevice*& out)
+{
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    StaticDevice& d = g_static[device];
+    if (!d.ready)
+    {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_decibel_scratch);
+        if (e != cudaSuccess) return e;
+        int sms = 0, a = 0, b = 0, c = 0;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, decibel_max_kernel, kThreads, 0)) != cudaSuccess)
+            return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, decibel_kernel<true>, kThreads, 0)) != cudaSuccess)
+            return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, decibel_kernel<false>, kThreads, 0)) != cudaSuccess)
+            return e;
+        d.scratch = static_cast<unsigned char*>(p);
+        d.gridMax = max(a, 1) * sms;
+        d.gridTrue = max(b, 1) * sms;
+        d.gridFalse = max(c, 1) * sms;
+        d.ready = true;
+    }
+    out = &d;
+    return cudaSuccess;
+}
+
+// Device address for a per-sample tensor in device, managed or pinned memory; null otherwise.
+const void* device_address(const void* p)
+{
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) return p;
+    if (attr.type == cudaMemoryTypeHost) return attr.devicePointer;
+    return nullptr;
+}
+
+}  // namespace
+}  // namespace rppb
+
+extern "C" SHARED_PUBLIC RppStatus rppt_to_decibels_gpu_static(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                               RpptDescPtr dstDescPtr, RpptImagePatchPtr srcDims,
+                                                               Rpp32f cutOffDB, Rpp32f multiplier,
+                                                               Rpp32f referenceMagnitude,
+                                                               rppAcceleratorQueue_t stream)
+{
+    using namespace rppb;
+    if (srcDescPtr == nullptr || dstDescPtr == nullptr) return RPP_ERROR_INVALID_ARGUMENTS;
+    const Rpp32u tensorDims = Rpp32u(srcDescPtr->numDims - 1);
+    if (tensorDims != 1 && tensorDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+    if (!multiplier) return RPP_ERROR_ZERO_DIVISION;
+    if (srcDescPtr->dataType != F32) return RPP_ERROR_NOT_IMPLEMENTED;
+    if (srcPtr == nullptr || dstPtr == nullptr || srcDims == nullptr) return RPP_ERROR_INVALID_ARGUMENTS;
+    const int n = int(srcDescPtr->n);
+    if (n <= 0) return RPP_SUCCESS;
+    if (n > kStaticMaxSamples) return RPP_ERROR_OUT_OF_BOUND_SCRATCH_MEMORY_SIZE;   // batch above the fixed scratch
+    const uint32_t* dims = static_cast<const uint32_t*>(device_address(srcDims));
+    if (dims == nullptr) return RPP_ERROR_INVALID_ARGUMENTS;   // srcDims must be device or pinned memory
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kStaticMaxDevices) return RPP_ERROR;
+    StaticDevice* sd = nullptr;
+    if (static_setup(device, sd) != cudaSuccess) return RPP_ERROR;
+
+    // to_decibels.cpp:40-45
+    float minRatio = float(std::pow(10, cutOffDB / multiplier));
+    if (minRatio == 0.0f) minRatio = std::nextafter(0.0f, 1.0f);
+    const Rpp32f log10Factor = 0.3010299956639812;
+    multiplier *= log10Factor;
+
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    long long* prefix = reinterpret_cast<long long*>(sd->scratch);
+    unsigned* maxKey = reinterpret_cast<unsigned*>(sd->scratch + kStaticPrefixBytes);
+    const float* src = static_cast<const float*>(srcPtr);
+    float* dst = static_cast<float*>(dstPtr);
+    const uint32_t sN = srcDescPtr->strides.nStride, sH = srcDescPtr->strides.hStride;
+    const uint32_t dN = dstDescPtr->strides.nStride, dH = dstDescPtr->strides.hStride;
+    launch_ragged_prefix(DecibelCount{dims}, n, prefix, s);
+    if (referenceMagnitude == 0.f)
+    {
+        // the maxima accumulate with atomicMax: start every call from zero keys
+        if (cudaMemsetAsync(maxKey, 0, size_t(n) * sizeof(unsigned), s) != cudaSuccess) return RPP_ERROR;
+        decibel_max_kernel<<<sd->gridMax, kThreads, 0, s>>>(src, sN, sH, dims, maxKey, prefix, n);
+        count_launch();
+        decibel_kernel<true><<<sd->gridTrue, kThreads, 0, s>>>(src, sN, sH, dst, dN, dH, dims, maxKey, 0.f, minRatio,
+                                                               multiplier, prefix, n);
+        count_launch();
+    }
+    else
+    {
+        decibel_kernel<false><<<sd->gridFalse, kThreads, 0, s>>>(src, sN, sH, dst, dN, dH, dims, nullptr,
+                                                                 referenceMagnitude, minRatio, multiplier, prefix, n);
+        count_launch();
+    }
+    return cudaGetLastError() == cudaSuccess ? RPP_SUCCESS : RPP_ERROR;
+}
