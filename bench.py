@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--clips", type=int, default=256)
+    p.add_argument("--serve-requests", type=int, default=600,
+                   help="requests per offered-load point of the serving measurement (0 skips it)")
     return p.parse_args()
 
 
@@ -312,6 +314,126 @@ def error_vs_fp64(chain, x_np, lens_np, clips=8, db_out=None):
             "note": "mel from the plain chain, dB from the fused call (bit-identical chains)"}
 
 
+def serving_measurement(torch, n_requests):
+    """configs[4]: continuous-batching server (rpp_b200/serving.py) over a 40 GB device budget;
+    capacity from a closed burst, then open-loop Poisson arrivals at 10-90 % of it."""
+    from rpp_b200 import serving
+    rng = np.random.Generator(np.random.PCG64(20261203 + 4))
+    pool = serving.ClipPool(torch, rng)
+    server = serving.FrontendServer(torch, budget_bytes=40 << 30, max_clips=256, tables=4)
+    serving.measure(torch, server, pool, rng, 64)                       # warm-up, graph capture
+    cap, _ = serving.measure(torch, server, pool, rng, n_requests)      # closed burst: capacity
+    mean_cs = np.mean([serving.clip_seconds(pool.request(i, rng)) for i in range(2000)])
+    loads = []
+    for frac in (0.1, 0.3, 0.5, 0.7, 0.9):
+        rate = frac * cap / mean_cs
+        thr, lat = serving.measure(torch, server, pool, rng, n_requests, rate_per_s=rate)
+        loads.append({"offered": frac, "requests_per_s": rate, "clip_s_per_s": thr,
+                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
+    return {"capacity_clip_s_per_s": cap, "mean_request_clip_s": float(mean_cs), "requests_per_point": n_requests,
+            "budget_gb": 40, "chain": "resample (Kaiser sinc, 16 zero crossings) -> pre-emphasis -> STFT(512, 400, "
+            "160) -> mel(128) -> dB, one captured graph per step over a device clip table",
+            "latency": "host clock from arrival to output copy complete", "loads": loads}
+
+
+def multirate_measurement(torch, h, steps=10, n=2048):
+    """2048 stereo clips, durations log-normal (median 4 s, sigma 0.25, 0.5-30 s), input
+    rates {16, 22.05, 44.1, 48} kHz -> rppb_downmix_resample_gpu (Kaiser-windowed sinc, 16 zero
+    crossings, beta 8) -> rppb_frontend_gpu (nfft 512, win 400, hop 160, 80 mel) in one CUDA graph.
+    The signal model (3 shared sines + independent noise per channel) is synthesized on the GPU from a
+    seeded generator (the host generator would take minutes for ~8.4k clip-seconds of stereo)."""
+    from rpp_b200 import audio
+    from rpp_b200.types import frontend_params
+    from rpp_b200.windows import kaiser_sinc
+    rng = np.random.Generator(np.random.PCG64(20261203 + 3))
+    dur = np.clip(rng.lognormal(np.log(4.0), 0.25, n), 0.5, 30.0)
+    rates = rng.choice(np.array([16000, 22050, 44100, 48000], np.float32), n)
+    lens = np.maximum(1, (dur * rates).astype(np.int64)).astype(np.int32)
+    L = int(lens.max())
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(20261203 + 3)
+    x = torch.zeros((n, 2 * L), device=dev)
+    chunk = 64
+    for c0 in range(0, n, chunk):
+        c1 = min(n, c0 + chunk)
+        t = torch.arange(L, device=dev, dtype=torch.float32)[None, :] / torch.from_numpy(rates[c0:c1]).to(dev)[:, None]
+        sig = torch.zeros((c1 - c0, L), device=dev)
+        for _ in range(3):
+            f = torch.rand((c1 - c0, 1), device=dev, generator=g) * 5900.0 + 100.0
+            a = torch.rand((c1 - c0, 1), device=dev, generator=g) * 0.45 + 0.05
+            sig += a * torch.sin(2 * np.pi * f * t)
+        for ch in range(2):
+            noise = torch.randn((c1 - c0, L), device=dev, generator=g) * 0.1
+            x[c0:c1, ch::2] = sig + noise
+        mask = torch.arange(L, device=dev)[None, :] >= torch.from_numpy(lens[c0:c1]).to(dev)[:, None]
+        x[c0:c1, 0::2][mask] = 0.0
+        x[c0:c1, 1::2][mask] = 0.0
+        del t, sig
+    lut, scale, center, lobes = kaiser_sinc(16, beta=8.0)
+    lut_d = torch.from_numpy(lut).to(dev)
+    out_len = np.array([int(np.ceil(np.float32(np.float32(l) * np.float32(16000.0)) / np.float32(r))) if r != 16000
+                        else l for l, r in zip(lens, rates)], np.int32)
+    L16 = int(out_len.max()) + 8
+    mono = torch.zeros((n, L16), device=dev)
+    F = out_len // 160 + 1
+    mf = int(F.max())
+    mel = torch.zeros((n, 80, mf), device=dev)
+    dims = torch.from_numpy(np.stack([lens, np.full(n, 2, np.int32)], 1).astype(np.int32)).to(dev)
+    ir = torch.from_numpy(rates).to(dev)
+    orr = torch.full((n,), 16000.0, device=dev)
+    lens16 = torch.from_numpy(out_len).to(dev)
+    coeff = torch.full((n,), 0.97, device=dev)
+    p = frontend_params(num_filter=80)
+    sd, md, d16 = audio_desc(n, L, channels=2, num_dims=3), spectra_desc(n, 80, mf), audio_desc(n, L16)
+
+    def step(evs=None):
+        if evs:
+            evs[0].record()
+        assert audio.downmix_resample(x, sd, mono, d16, ir, orr, dims, False, lut_d, scale, center, lobes, h) == 0
+        if evs:
+            evs[1].record()
+        assert audio.frontend(mono, d16, mel, md, lens16, coeff, p, h) == 0
+        if evs:
+            evs[2].record()
+
+    step()
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    split = np.zeros(2)
+    for _ in range(3):
+        step(evs)
+        torch.cuda.synchronize()
+        split += [evs[0].elapsed_time(evs[1]), evs[1].elapsed_time(evs[2])]
+    split /= 3
+    s = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    h.set_stream(s.cuda_stream)
+    try:
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(graph, stream=s):
+                step()
+        for _ in range(2):
+            graph.replay()
+        torch.cuda.synchronize()
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st.record()
+        for _ in range(steps):
+            graph.replay()
+        en.record()
+        torch.cuda.synchronize()
+        ms = st.elapsed_time(en) / steps
+    finally:
+        h.set_stream(torch.cuda.current_stream().cuda_stream)
+    clip_s = float((lens / rates).sum())
+    in_bytes = float((8 * lens.astype(np.int64)).sum())
+    return {"workload": "configs[3]: 2048 stereo clips, log-normal 4 s median, rates {16k,22.05k,44.1k,48k}; "
+                        "downmix+resample(Kaiser beta 8, 16 zero crossings) -> fused pre-emphasis/STFT(512)/mel(80)/dB",
+            "clip_seconds": clip_s, "ms_per_batch": ms, "clip_s_per_s": clip_s / (ms / 1e3),
+            "split_ms": {"downmix_resample": float(split[0]), "frontend": float(split[1])},
+            "input_bytes": in_bytes, "graph": "both calls captured in one CUDA graph (4 kernels + 1 memset)"}
+
+
 def read_traffic(kernel):
     """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
@@ -437,6 +559,16 @@ def run_b200(args, world, rank, local):
         traffic = read_traffic("frontend_kernel<512>")
         err = error_vs_fp64(chain, x_np, lens_np, db_out=fused.out)
         try:
+            multirate = multirate_measurement(torch, h)
+        except Exception as exc:
+            multirate = {"error": repr(exc)}
+        serve = None
+        if args.serve_requests > 0:
+            try:
+                serve = serving_measurement(torch, args.serve_requests)
+            except Exception as exc:   # report, do not lose the main line
+                serve = {"error": repr(exc)}
+        try:
             cpu = cpu_baseline_sample(x_np, lens_np)
         except Exception as exc:  # the reference host library is optional on a box without it
             cpu = {"value": None, "unit": "clip-s/s", "cores": os.cpu_count(), "kind": "reference",
@@ -463,6 +595,8 @@ def run_b200(args, world, rank, local):
             "err_vs_fp64": err,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "multirate": multirate,
+            "serving": serve,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

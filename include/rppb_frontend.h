@@ -51,7 +51,7 @@ typedef struct
     Rpp32f cutOffDB;
     Rpp32f multiplier;
     Rpp32f referenceMagnitude; /* 0: per-sample maximum */
-    /* schedule: clips by which the decibel tiles trail the spectrum tiles (0 = default 8) */
+    /* schedule: clips by which the decibel tiles trail the spectrum tiles (0 = default 32) */
     Rpp32s lookahead;
 } RppbFrontendParams;
 

@@ -15,16 +15,34 @@ void count_launch(int kernels);
 // computed on the device from the per-sample tensors, so no call reads lengths on the host.
 
 // Largest b in [0, n) with prefix[b] <= w (w < prefix[n]); empty samples are skipped.
-__device__ __forceinline__ int ragged_find(const long long* __restrict__ prefix, int n, long long w)
+// `prefix` may point to global or shared memory (see cache_prefix).
+__device__ __forceinline__ int ragged_find(const long long* prefix, int n, long long w)
 {
     int lo = 0, hi = n - 1;
     while (lo < hi)
     {
         int mid = (lo + hi + 1) >> 1;
-        if (__ldg(prefix + mid) <= w) lo = mid;
+        if (prefix[mid] <= w) lo = mid;
         else hi = mid - 1;
     }
     return lo;
+}
+
+// Shared-memory copy of prefix[0..n] when it fits (batches up to kPrefixCache - 1 samples), so the
+// per-unit binary search costs shared-memory rather than global-memory latency.  All threads of
+// the CTA must call it; it ends with __syncthreads.
+constexpr int kPrefixCache = 512;
+template <int CAP = kPrefixCache>
+__device__ __forceinline__ const long long* cache_prefix(const long long* prefix, int n, long long* s_cache)
+{
+    if (n + 1 > CAP)
+    {
+        __syncthreads();
+        return prefix;
+    }
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) s_cache[i] = prefix[i];
+    __syncthreads();
+    return s_cache;
 }
 
 // One CTA of 1024 threads: prefix[0..n] = exclusive scan of count(b).

@@ -449,7 +449,7 @@ RppStatus frontend_params(Handle& h, const RppbFrontendParams* params, float* wi
     a.minRatio = minRatio;
     a.multiplier = p.multiplier * log10Factor;
     a.refMag = p.referenceMagnitude;
-    a.lookahead = p.lookahead > 0 ? p.lookahead : 8;
+    a.lookahead = p.lookahead > 0 ? p.lookahead : 32;
     a.clips = nullptr;
     a.outRate = 0.f;
     a.coeffAll = 0.f;
@@ -474,7 +474,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPt
             return RPP_ERROR_INVALID_DST_DIMS;
         const int n = int(srcDescPtr->n);
         if (n <= 0) return RPP_SUCCESS;
-        const int lookahead = params->lookahead > 0 ? params->lookahead : 8;
+        const int lookahead = params->lookahead > 0 ? params->lookahead : 32;
         const size_t scratchBytes = frontend_scratch_bytes(n, lookahead);
         const int W = params->windowLength > 0 ? params->windowLength : 0;
         Carver m(nullptr);
@@ -517,7 +517,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips
         require(outRate > 0.f, "outRate must be positive");
         const int n = numClips;
         if (n <= 0) return RPP_SUCCESS;
-        const int lookahead = params->lookahead > 0 ? params->lookahead : 8;
+        const int lookahead = params->lookahead > 0 ? params->lookahead : 32;
         const size_t scratchBytes = frontend_scratch_bytes(n, lookahead);
         const int W = params->windowLength > 0 ? params->windowLength : 0;
         Carver m(nullptr);

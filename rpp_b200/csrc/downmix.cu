@@ -36,6 +36,8 @@ __global__ void __launch_bounds__(kThreads) down_mixing_kernel(const float* __re
                                                                const int* __restrict__ dims, bool normalize,
                                                                const long long* __restrict__ prefix, int n)
 {
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, n, s_prefix);
     const long long total = prefix[n];
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
     {

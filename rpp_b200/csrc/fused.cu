@@ -29,6 +29,8 @@
 namespace rppb {
 
 constexpr int kFusedThreads = 256;
+constexpr int kDbFrames = 64;                 // frames per decibel item
+constexpr int kFusedPrefixCache = 320;        // slots cached in shared memory (n + lookahead + 1)
 constexpr long long kWaitLimit = 1ll << 24;   // x ~128 ns sleeps: a few seconds
 
 namespace {
@@ -62,17 +64,18 @@ struct SlotCount
 {
     FrontendArgs a;
     int n, D;
-    __device__ int tiles(int b) const
+    __device__ int frames(int b) const
     {
         const ClipView c = clip_view(a, b);
-        const int F = min(num_windows(c.L, a.W, a.hop, a.center), c.maxFrames);
-        return F <= 0 ? 0 : (F + TF - 1) / TF;
+        return max(0, min(num_windows(c.L, a.W, a.hop, a.center), c.maxFrames));
     }
+    __device__ int tiles(int b) const { return (frames(b) + TF - 1) / TF; }
+    __device__ int db_tiles(int b) const { return (frames(b) + kDbFrames - 1) / kDbFrames; }
     __device__ long long operator()(int s) const
     {
         long long c = 0;
         if (s < n) c += tiles(s);
-        if (s - D >= 0 && s - D < n) c += tiles(s - D);
+        if (s - D >= 0 && s - D < n) c += db_tiles(s - D);
         return c;
     }
 };
@@ -82,14 +85,15 @@ template <int NFFT>
 struct FusedLayout
 {
     using S = StftShape<NFFT, kFusedThreads>;
-    int nmel;
-    size_t tw, win, work, csrRow, csrBin, csrW, total;
-    __host__ __device__ FusedLayout(int numFilter) : nmel(numFilter)
+    size_t tw, tw1, win, span, work, csrRow, csrBin, csrW, total;
+    __host__ __device__ FusedLayout(int numFilter, int W, int hop)
     {
         const int bins = S::BINS;
         tw = 0;
-        win = tw + size_t(NFFT) * 8;
-        work = win + size_t(NFFT) * 4;
+        tw1 = tw + S::tw_bytes;
+        win = tw1 + S::tw1_bytes;
+        span = win + size_t(NFFT) * 4;
+        work = span + S::span_bytes(W, hop);
         // the FFT slots + power tile, or (before the loop) the mel table build
         size_t fftOut = S::fft_bytes + S::out_bytes;
         size_t tables = 2 * size_t(numFilter + 2) * 4 + size_t(numFilter) * 4 + 2 * size_t(numFilter + 1) * 8 +
@@ -97,13 +101,13 @@ struct FusedLayout
         size_t workBytes = (fftOut > tables ? fftOut : tables);
         csrRow = (work + workBytes + 15) & ~size_t(15);
         csrBin = (csrRow + size_t(numFilter + 1) * 4 + 15) & ~size_t(15);
-        csrW = (csrBin + size_t(2 * bins + 2) * 4 + 15) & ~size_t(15);
+        csrW = (csrBin + size_t(2 * bins + 2) * 2 + 15) & ~size_t(15);
         total = (csrW + size_t(2 * bins + 2) * 4 + 15) & ~size_t(15);
     }
 };
 
 template <int NFFT>
-__global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a, const float2* __restrict__ twiddle,
+__global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend_kernel(FrontendArgs a, const float2* __restrict__ twiddle,
                                                                  const long long* __restrict__ prefix,
                                                                  unsigned long long* __restrict__ workCounter,
                                                                  int* __restrict__ done, unsigned* __restrict__ maxKey,
@@ -112,20 +116,21 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
     using S = StftShape<NFFT, kFusedThreads>;
     constexpr int TF = S::TF, BINS = S::BINS, LD = S::OUT_LD;
     extern __shared__ __align__(16) unsigned char smem[];
-    const FusedLayout<NFFT> lay(a.mel.numFilter);
+    const FusedLayout<NFFT> lay(a.mel.numFilter, a.W, a.hop);
     float2* s_tw = reinterpret_cast<float2*>(smem + lay.tw);
+    float2* s_tw1 = reinterpret_cast<float2*>(smem + lay.tw1);
     float* s_win = reinterpret_cast<float*>(smem + lay.win);
+    float* s_span = reinterpret_cast<float*>(smem + lay.span);
     float2* s_fft = reinterpret_cast<float2*>(smem + lay.work);
     float* s_out = reinterpret_cast<float*>(smem + lay.work + S::fft_bytes);
     int* csrRow = reinterpret_cast<int*>(smem + lay.csrRow);
-    int* csrBin = reinterpret_cast<int*>(smem + lay.csrBin);
+    unsigned short* csrBin = reinterpret_cast<unsigned short*>(smem + lay.csrBin);
     float* csrW = reinterpret_cast<float*>(smem + lay.csrW);
     __shared__ long long s_item;
     __shared__ float s_warpMax[kFusedThreads / 32];
     const int nmel = a.mel.numFilter;
 
-    for (int i = threadIdx.x; i < NFFT; i += kFusedThreads) s_tw[i] = twiddle[i];
-    for (int i = threadIdx.x; i < a.W; i += kFusedThreads) s_win[i] = a.window[i];
+    stft_tables<NFFT, kFusedThreads>(twiddle, a.window, a.W, s_tw, s_tw1, s_win);
 
     // ---- mel weights as CSR rows (filter m: bins of interval m with (1 - wd) * norm, then bins of
     //      interval m + 1 with wd * norm), built in the work region before it holds FFT data
@@ -160,13 +165,13 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
             for (int k = v.first[m]; k < v.last[m]; ++k, ++e)
             {
                 float w = __fsub_rn(1.0f, v.weightsDown[k]);
-                csrBin[e] = k;
+                csrBin[e] = (unsigned short)k;
                 csrW[e] = a.mel.normalize ? __fmul_rn(w, nm) : w;
             }
             for (int k = v.first[m + 1]; k < v.last[m + 1]; ++k, ++e)
             {
                 const float w = v.weightsDown[k];
-                csrBin[e] = k;
+                csrBin[e] = (unsigned short)k;
                 csrW[e] = a.mel.normalize ? __fmul_rn(w, nm) : w;
             }
         }
@@ -175,6 +180,8 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
 
     const int centerOffset = a.center ? a.W / 2 : 0;
     const int nslots = a.n + a.lookahead;
+    __shared__ long long s_prefix[kFusedPrefixCache];
+    prefix = cache_prefix<kFusedPrefixCache>(prefix, nslots, s_prefix);
     const long long total = prefix[nslots];
     const SlotCount<TF> cnt{a, a.n, a.lookahead};
     const int f = threadIdx.x % TF;      // frame column this thread owns in mel / decibel tiles
@@ -196,8 +203,8 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
         const ClipView cv = clip_view(a, b);
         const int L = cv.L;
         const int F = min(num_windows(L, a.W, a.hop, a.center), cv.maxFrames);
-        const int f0 = tile * TF;
-        const int Tv = min(TF, F - f0);
+        const int f0 = tile * (spectrumItem ? TF : kDbFrames);
+        const int Tv = min(spectrumItem ? TF : kDbFrames, F - f0);
         float* y = cv.y + f0;
         const uint32_t hs = cv.hStride;
 
@@ -206,7 +213,8 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
             const float* x = cv.x;
             const float bval = a.border == 1 ? x[0] : a.border == 2 ? (cv.hasSecond ? x[1] : 0.f) : 0.f;
             const PreemphSource src{x, L, a.reflect, cv.coeff, bval};
-            stft_tile<NFFT, kFusedThreads>(src, f0, F, a.W, a.hop, centerOffset, a.power, s_win, s_tw, s_fft, s_out);
+            stft_tile<NFFT, kFusedThreads>(src, f0, F, a.W, a.hop, centerOffset, a.power, s_win, s_tw, s_tw1, s_span,
+                                           s_fft, s_out);
             __syncthreads();
             float tmax = -FLT_MAX;
             if (f < Tv)
@@ -222,6 +230,7 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
             }
             tmax = warp_max(tmax);
             if ((threadIdx.x & 31) == 0) s_warpMax[threadIdx.x >> 5] = tmax;
+            __threadfence();   // each thread's mel stores are visible device-wide before the tile is counted
             __syncthreads();
             if (threadIdx.x == 0)
             {
@@ -260,11 +269,14 @@ __global__ void __launch_bounds__(kFusedThreads) frontend_kernel(FrontendArgs a,
                     ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
                 }
                 const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
-                if (f < Tv)
+                const int fd = threadIdx.x % kDbFrames;
+                const int gd = threadIdx.x / kDbFrames;
+                constexpr int kDbGroups = kFusedThreads / kDbFrames;
+                if (fd < Tv)
                 {
-                    for (int m = g; m < nmel; m += kGroups)
+                    for (int m = gd; m < nmel; m += kDbGroups)
                     {
-                        float* p = y + size_t(m) * hs + f;
+                        float* p = y + size_t(m) * hs + fd;
                         float v = __fmul_rn(__ldcg(p), inv);
                         v = a.minRatio < v ? v : a.minRatio;
                         *p = __fmul_rn(a.multiplier, log2f(v));
@@ -289,8 +301,8 @@ void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
     const size_t clear = reinterpret_cast<char*>(maxKey + a.n) - reinterpret_cast<char*>(counter);
     check_cuda(cudaMemsetAsync(counter, 0, clear, h.stream()), "memset(frontend state)");
     launch_ragged_prefix(SlotCount<S::TF>{a, a.n, a.lookahead}, nslots, prefix, h.stream());
-    const FusedLayout<NFFT> lay(a.mel.numFilter);
-    if (lay.total > 200 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
+    const FusedLayout<NFFT> lay(a.mel.numFilter, a.W, a.hop);
+    if (lay.total > 227 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
     const float2* tw = spectrogram_twiddles(h, NFFT);
     const int grid = persistent_grid(h, reinterpret_cast<const void*>(frontend_kernel<NFFT>), kFusedThreads, lay.total);
     frontend_kernel<NFFT><<<grid, kFusedThreads, lay.total, h.stream()>>>(a, tw, prefix, counter, done, maxKey,

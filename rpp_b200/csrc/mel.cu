@@ -1,23 +1,17 @@
 // mel_filter_bank over NFT spectra.
 //
 // Reference: src/modules/tensor/cpu/kernel/mel_filter_bank.cpp:40-193 and the scales of
-// api/rppdefs.h:795-851.  Per sample, nfft = (bins - 1) * 2 and hzStep = sampleRate / nfft.
-// numFilter + 1 intervals are laid out evenly in mel between hz_to_mel(minFreq) and
-// hz_to_mel(maxFreq) (mel edges accumulate an FP64 step; the scale functions are float
-// functions); bin k belongs to the first interval whose upper edge f1 exceeds k * hzStep and
-// has weightsDown = (f1 - f) / (f1 - f0) (rounded to float); with normalize, filter m is
-// scaled by 2 / (f_{m+2} - f_m).  Filter m sums the bins of interval m with weight
-// (1 - weightsDown) and the bins of interval m+1 with weight weightsDown, in ascending bin
-// order, in float, starting from 0 — exactly the reference's accumulation order, so with the
-// same tables the outputs are bit-identical.  Columns [frames, min(frames + 8, hStride)) of
-// each filter row are zeroed, as the reference does.
+// api/rppdefs.h:795-851 (table construction: mel_tables.cuh).  Filter m sums the bins of interval m
+// with weight (1 - weightsDown) * norm[m] and the bins of interval m+1 with weight
+// weightsDown * norm[m], in ascending bin order, in float, starting from 0 — the reference's
+// accumulation order, so with the same tables the outputs are bit-identical.  Columns
+// [frames, min(frames + 8, hStride)) of each filter row are zeroed, as the reference does.
 //
-// The tables are built on the GPU by the CTA that needs them (rebuilt only when the sample's
-// bin count differs from the last one it built): the float scale functions use logf/expf
-// evaluated as correctly rounded double log/exp, the edges and weights are FP64 like the
-// reference's.  Work list: (sample, 64-frame tile) units; thread (group g, frame t) computes
-// filters g, g+4, ... for frame t, reading the spectrum column through L1 (each bin feeds two
-// filters), and the warp's 32 consecutive frames make every load and store one 128-byte line.
+// Work list: (sample, 32-frame tile) units.  A CTA stages the tile's spectrum rows
+// [binStart, binEnd) x 32 frames in shared memory (one coalesced 128-byte row segment per bin), then
+// thread (group g, frame t) computes filters g, g+8, ... for frame t from shared memory and a warp
+// stores 32 consecutive frames of one filter row.  Tables are built by the CTA (rebuilt only when
+// the sample's bin count changes), sized for this call's numFilter and bins.
 #include <cfloat>
 
 #include "common.cuh"
@@ -28,10 +22,9 @@ namespace rppb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kTile = 64;            // frames per unit
+constexpr int kTile = 32;            // frames per unit
+constexpr int kLd = kTile + 1;       // spectrum tile leading dimension (conflict-free columns)
 constexpr int kGroups = kThreads / kTile;
-constexpr int kMaxBins = 4097;       // nfft up to 8192
-constexpr int kMaxFilters = 1024;
 
 struct MelCount
 {
@@ -45,25 +38,39 @@ struct MelCount
     }
 };
 
-struct MelSmem
+// Shared memory plan for numFilter filters and at most maxBins bins (host and device agree).
+struct MelLayout
 {
-    int range[3];
-    int first[kMaxFilters + 2];
-    int last[kMaxFilters + 2];
-    float norm[kMaxFilters];
-    double f1[kMaxFilters + 1];
-    double f0[kMaxFilters + 1];
-    float weightsDown[kMaxBins];
+    size_t range, first, last, norm, f0, f1, wd, spec, total;
+    __host__ __device__ MelLayout(int numFilter, int maxBins)
+    {
+        range = 0;
+        first = 16;
+        last = first + size_t(numFilter + 2) * 4;
+        norm = last + size_t(numFilter + 2) * 4;
+        f0 = (norm + size_t(numFilter) * 4 + 7) & ~size_t(7);
+        f1 = f0 + size_t(numFilter + 1) * 8;
+        wd = f1 + size_t(numFilter + 1) * 8;
+        spec = (wd + size_t(maxBins) * 4 + 15) & ~size_t(15);
+        total = spec + size_t(maxBins) * kLd * 4;
+    }
 };
 
-__global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq, const long long* __restrict__ prefix)
+__global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq, int maxBins,
+                                                       const long long* __restrict__ prefix)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    MelSmem& T = *reinterpret_cast<MelSmem*>(smem);
-    const MelTableView view{T.first, T.last, T.norm, T.f0, T.f1, T.weightsDown, T.range};
+    const MelLayout lay(a.numFilter, maxBins);
+    int* range = reinterpret_cast<int*>(smem + lay.range);
+    const MelTableView T{reinterpret_cast<int*>(smem + lay.first), reinterpret_cast<int*>(smem + lay.last),
+                         reinterpret_cast<float*>(smem + lay.norm), reinterpret_cast<double*>(smem + lay.f0),
+                         reinterpret_cast<double*>(smem + lay.f1), reinterpret_cast<float*>(smem + lay.wd), range};
+    float* s_spec = reinterpret_cast<float*>(smem + lay.spec);
     const MelParams mp{a.minFreq, maxFreq, a.sampleRate, a.htk, a.numFilter, a.normalize};
-    if (threadIdx.x == 0) T.range[2] = -1;
+    if (threadIdx.x == 0) range[2] = -1;
     __syncthreads();
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, a.n, s_prefix);
     const long long total = prefix[a.n];
     const int t = threadIdx.x % kTile;
     const int g = threadIdx.x / kTile;
@@ -72,18 +79,31 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
         const int b = ragged_find(prefix, a.n, w);
         const int tile = int(w - prefix[b]);
         const int bins = a.dims[2 * b];
-        const int frames = max(a.dims[2 * b + 1], 0);
+        const int frames = min(max(a.dims[2 * b + 1], 0), int(min(a.srcHStride, a.dstHStride)));
         const int nfft = (bins - 1) * 2;
-        const bool ok = nfft >= 2 && nfft / 2 + 1 <= kMaxBins && uint32_t(bins) <= a.srcRows;
-        const int held = T.range[2];
+        const bool ok = nfft >= 2 && bins <= maxBins && uint32_t(bins) <= a.srcRows;
+        const int held = range[2];
         __syncthreads();   // every thread has read the key before a rebuild may change it
-        if (ok && held != nfft) build_mel_tables(view, mp, nfft);
-        const int col = tile * kTile + t;
+        if (ok && held != nfft) build_mel_tables(T, mp, nfft);
+        const int t0 = tile * kTile;
         const int zc = int(min((long long)frames + 8, (long long)a.dstHStride));
+        const int tv = min(kTile, frames - t0);   // valid frames of this tile (may be <= 0)
+        const int k0 = range[0], k1 = range[1];
+        if (ok && tv > 0)
+        {
+            // stage spectrum rows [k0, k1) x frames [t0, t0 + tv)
+            const float* x = a.src + size_t(b) * a.srcNStride + t0;
+            for (int idx = threadIdx.x; idx < (k1 - k0) * kTile; idx += kThreads)
+            {
+                const int r = idx / kTile, c = idx % kTile;
+                if (c < tv) s_spec[r * kLd + c] = __ldg(x + size_t(k0 + r) * a.srcHStride + c);
+            }
+        }
+        __syncthreads();
+        const int col = t0 + t;
         float* y = a.dst + size_t(b) * a.dstNStride;
         if (col < zc)
         {
-            const float* x = a.src + size_t(b) * a.srcNStride + col;
             for (int m = g; m < a.numFilter; m += kGroups)
             {
                 float acc = 0.0f;
@@ -94,20 +114,20 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
                     {
                         float wgt = __fsub_rn(1.0f, T.weightsDown[k]);
                         if (a.normalize) wgt = __fmul_rn(wgt, T.norm[m]);
-                        acc = __fadd_rn(acc, __fmul_rn(__ldg(x + size_t(k) * a.srcHStride), wgt));
+                        acc = __fadd_rn(acc, __fmul_rn(s_spec[(k - k0) * kLd + t], wgt));
                     }
                     // bins of interval m + 1: weight weightsDown * norm[m]
                     for (int k = T.first[m + 1]; k < T.last[m + 1]; ++k)
                     {
                         float wgt = T.weightsDown[k];
                         if (a.normalize) wgt = __fmul_rn(wgt, T.norm[m]);
-                        acc = __fadd_rn(acc, __fmul_rn(__ldg(x + size_t(k) * a.srcHStride), wgt));
+                        acc = __fadd_rn(acc, __fmul_rn(s_spec[(k - k0) * kLd + t], wgt));
                     }
                 }
                 y[size_t(m) * a.dstHStride + col] = acc;
             }
         }
-        __syncthreads();   // the next unit may rebuild the tables
+        __syncthreads();   // the next unit restages the tile and may rebuild the tables
     }
 }
 
@@ -116,13 +136,14 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
 void launch_mel_filter_bank(Handle& h, void* scratch, const MelArgs& a)
 {
     if (a.n <= 0) return;
-    if (a.numFilter > kMaxFilters) fail(RPP_ERROR_INVALID_ARGUMENTS, "numFilter above 1024");
+    const int maxBins = int(a.srcRows);
+    const size_t smem = MelLayout(a.numFilter, maxBins).total;
+    if (smem > 227 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "too many bins or filters for the mel tile");
     long long* prefix = static_cast<long long*>(scratch);
     launch_ragged_prefix(MelCount{a.dims, a.dstHStride}, a.n, prefix, h.stream());
     const float maxFreq = (a.maxFreq == 0) ? a.sampleRate / 2 : a.maxFreq;
-    const size_t smem = sizeof(MelSmem);
     int grid = persistent_grid(h, reinterpret_cast<const void*>(mel_kernel), kThreads, smem);
-    mel_kernel<<<grid, kThreads, smem, h.stream()>>>(a, maxFreq, prefix);
+    mel_kernel<<<grid, kThreads, smem, h.stream()>>>(a, maxFreq, maxBins, prefix);
     count_launch();
     check_cuda(cudaGetLastError(), "mel_kernel");
 }

@@ -50,6 +50,8 @@ __global__ void __launch_bounds__(128) mms_kernel(const float* __restrict__ src,
                                                   float* __restrict__ mms, float* __restrict__ blockMax,
                                                   const long long* __restrict__ prefix, int n)
 {
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, n, s_prefix);
     const long long total = prefix[n];
     const float meanFactor = __fdiv_rn(1.0f, float(windowLength));
     for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;

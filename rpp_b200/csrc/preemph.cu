@@ -36,6 +36,8 @@ __global__ void __launch_bounds__(kThreads) pre_emphasis_kernel(const float* __r
                                                                 size_t srcElems, const long long* __restrict__ prefix,
                                                                 int n)
 {
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, n, s_prefix);
     const long long total = prefix[n];
     const int lane = threadIdx.x & 31;
     for (long long w = blockIdx.x; w < total; w += gridDim.x)

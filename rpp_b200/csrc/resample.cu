@@ -102,6 +102,8 @@ __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restric
     __syncthreads();
     const Win win{s_lut, wd.lutSize, wd.scale, wd.center};
     const int lobes = wd.lobes;
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, n, s_prefix);
     const long long total = prefix[n];
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
     {

@@ -42,35 +42,45 @@ struct SpecCount
     }
 };
 
+// Shared memory plan (bytes) for one nfft, window and hop; identical on host and device.
 template <int NFFT>
 struct SmemLayout
 {
     using S = StftShape<NFFT, kThreads>;
-    static constexpr size_t tw = 0;                          // NFFT float2
-    static constexpr size_t fftBuf = tw + size_t(NFFT) * 8;  // FPP frame slots
-    static constexpr size_t out = fftBuf + S::fft_bytes;     // [BINS][TF+1] floats
-    static constexpr size_t win = out + S::out_bytes;        // NFFT floats (window <= nfft)
-    static constexpr size_t bytes = win + size_t(NFFT) * 4;
+    size_t tw, tw1, win, span, fftBuf, out, bytes;
+    __host__ __device__ SmemLayout(int W, int hop)
+    {
+        tw = 0;
+        tw1 = tw + S::tw_bytes;
+        win = tw1 + S::tw1_bytes;
+        span = win + size_t(NFFT) * 4;
+        fftBuf = span + S::span_bytes(W, hop);
+        out = fftBuf + S::fft_bytes;
+        bytes = out + S::out_bytes;
+    }
 };
 
 template <int NFFT>
-__global__ void __launch_bounds__(kThreads) spectrogram_fft_kernel(SpectrogramArgs a, const float2* __restrict__ twiddle,
-                                                                   const long long* __restrict__ prefix)
+__global__ void __launch_bounds__(kThreads, (NFFT <= 512 ? 3 : 2)) spectrogram_fft_kernel(SpectrogramArgs a,
+                                                                      const float2* __restrict__ twiddle,
+                                                                      const long long* __restrict__ prefix)
 {
-    using L_ = SmemLayout<NFFT>;
     using S = StftShape<NFFT, kThreads>;
     constexpr int TF = S::TF, BINS = S::BINS;
     extern __shared__ __align__(16) unsigned char smem[];
-    float2* s_tw = reinterpret_cast<float2*>(smem + L_::tw);
-    float2* s_fft = reinterpret_cast<float2*>(smem + L_::fftBuf);
-    float* s_out = reinterpret_cast<float*>(smem + L_::out);
-    float* s_win = reinterpret_cast<float*>(smem + L_::win);
+    const SmemLayout<NFFT> lay(a.windowLength, a.windowStep);
+    float2* s_tw = reinterpret_cast<float2*>(smem + lay.tw);
+    float2* s_tw1 = reinterpret_cast<float2*>(smem + lay.tw1);
+    float* s_win = reinterpret_cast<float*>(smem + lay.win);
+    float* s_span = reinterpret_cast<float*>(smem + lay.span);
+    float2* s_fft = reinterpret_cast<float2*>(smem + lay.fftBuf);
+    float* s_out = reinterpret_cast<float*>(smem + lay.out);
 
     const int W = a.windowLength;
-    for (int i = threadIdx.x; i < NFFT; i += kThreads) s_tw[i] = twiddle[i];
-    for (int i = threadIdx.x; i < W; i += kThreads) s_win[i] = a.window[i];
-    __syncthreads();
+    stft_tables<NFFT, kThreads>(twiddle, a.window, W, s_tw, s_tw1, s_win);
     const int centerOffset = a.center ? W / 2 : 0;
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, a.n, s_prefix);
     const long long total = prefix[a.n];
 
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
@@ -80,9 +90,10 @@ __global__ void __launch_bounds__(kThreads) spectrogram_fft_kernel(SpectrogramAr
         const int L = a.len[b];
         const int F = min(num_windows(L, W, a.windowStep, a.center), a.maxFrames);
         const PlainSource src{a.src + size_t(b) * a.srcStride, L, a.reflect};
-        stft_tile<NFFT, kThreads>(src, f0, F, W, a.windowStep, centerOffset, a.power, s_win, s_tw, s_fft, s_out);
+        stft_tile<NFFT, kThreads>(src, f0, F, W, a.windowStep, centerOffset, a.power, s_win, s_tw, s_tw1, s_span,
+                                  s_fft, s_out);
         __syncthreads();
-        // store the tile: a warp writes 32 consecutive frames of one bin (NFT) or bins of one frame (NTF)
+        // store the tile: a warp writes consecutive frames of one bin (NFT) or bins of one frame (NTF)
         const int Tv = min(TF, F - f0);
         float* y = a.dst + size_t(b) * a.dstNStride;
         if (a.nft)
@@ -130,6 +141,8 @@ __global__ void __launch_bounds__(kThreads) spectrogram_dft_kernel(SpectrogramAr
     const int off = (W < N) ? (N - W) / 2 : 0;
     const int centerOffset = a.center ? W / 2 : 0;
     const int bins = N / 2 + 1;
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, a.n, s_prefix);
     const long long total = prefix[a.n];
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
     {
@@ -170,10 +183,10 @@ __global__ void __launch_bounds__(kThreads) spectrogram_dft_kernel(SpectrogramAr
 template <int NFFT>
 void launch_fft(Handle& h, long long* prefix, const SpectrogramArgs& a, const float2* tw)
 {
-    using S = SmemLayout<NFFT>;
     launch_ragged_prefix(SpecCount{a.len, a.windowLength, a.windowStep, a.maxFrames, Plan<NFFT>::TF, a.center}, a.n, prefix,
                          h.stream());
-    const size_t smem = S::bytes;
+    const size_t smem = SmemLayout<NFFT>(a.windowLength, a.windowStep).bytes;
+    if (smem > 227 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "window/hop too large for the frame tile");
     int grid = persistent_grid(h, reinterpret_cast<const void*>(spectrogram_fft_kernel<NFFT>), kThreads, smem);
     spectrogram_fft_kernel<NFFT><<<grid, kThreads, smem, h.stream()>>>(a, tw, prefix);
     count_launch();

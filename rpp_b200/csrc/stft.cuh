@@ -3,14 +3,19 @@
 // Shared by the plain spectrogram kernel and the fused front end so both produce bit-identical
 // spectra.  Framing follows src/modules/tensor/cpu/kernel/spectrogram.cpp:116-212: frame f
 // starts at f * hop - centerOffset, samples outside the signal are reflected or zero, the frame
-// is multiplied by the window and placed at offset (nfft - W)/2 of the nfft buffer.  The signal
-// is read through a Source functor, which lets the fused kernel apply pre-emphasis while it
-// gathers (reflection then applies to the pre-emphasized signal, exactly as when the two ops run
-// one after the other).
+// is multiplied by the window and placed at offset (nfft - W)/2 of the nfft buffer.
 //
-// A frame is transformed by G = R2 threads: pack the nfft real samples as M = nfft/2 complex
-// points, stage-1 R1-point register DFT + twiddle, one shared-memory exchange, stage-2 R2-point
-// register DFT, then unpack the nfft/2+1 bins of the real transform (fft.cuh).
+// Per tile of TF frames:
+//   1. the tile's input span ((TF-1)*hop + W samples) is staged in shared memory with coalesced
+//      loads (float4 when the span lies inside the signal and is 16-byte aligned); the Source
+//      functor applies reflect/zero padding and, in the fused kernel, pre-emphasis, so padding is
+//      resolved once per sample rather than once per frame;
+//   2. each frame is transformed by G = R2 threads as a real FFT: the nfft samples are packed into
+//      M = nfft/2 complex points, stage 1 is an R1-point register DFT with twiddles W_M^(j*k1) from a
+//      [k1][j] table (conflict-free), one shared-memory exchange, stage 2 an R2-point register DFT;
+//   3. the real spectrum is unpacked in bin pairs (k, M-k), which share their two loads:
+//      X[k] = E + W^k O and X[M-k] = conj(E - W^k O) with E = (Z[k] + conj Z[M-k]) / 2,
+//      O = (Z[k] - conj Z[M-k]) / 2i.
 #pragma once
 
 #include "common.cuh"
@@ -25,7 +30,7 @@ struct Plan<128> { static constexpr int R1 = 8, R2 = 8, TF = 32; };
 template <>
 struct Plan<256> { static constexpr int R1 = 16, R2 = 8, TF = 32; };
 template <>
-struct Plan<512> { static constexpr int R1 = 16, R2 = 16, TF = 32; };
+struct Plan<512> { static constexpr int R1 = 16, R2 = 16, TF = 16; };
 template <>
 struct Plan<1024> { static constexpr int R1 = 32, R2 = 16, TF = 16; };
 template <>
@@ -44,8 +49,12 @@ struct StftShape
     static constexpr int OUT_LD = TF + 1;              // leading dimension of the [BINS][TF] tile
     static constexpr size_t fft_bytes = size_t(FPP) * FFT_SLOT * 8;
     static constexpr size_t out_bytes = size_t(BINS) * OUT_LD * 4;
+    static constexpr size_t tw_bytes = (size_t(M / 2 + 1) * 8 + 15) & ~size_t(15);   // W_nfft^k, k <= M/2
+    static constexpr size_t tw1_bytes = size_t(R1) * R2 * 8;      // W_M^(j*k1) as [k1][j]
     static_assert(R1 * R2 == M, "plan");
     static_assert(R1 % G == 0, "stage 2 assigns R1 / G rows per thread");
+    // span staged per tile: (TF - 1) * hop + W floats (runtime), rounded for alignment
+    __host__ __device__ static size_t span_bytes(int W, int hop) { return (size_t((TF - 1) * hop + W) * 4 + 15) & ~size_t(15); }
 };
 
 // The signal as stored.
@@ -60,6 +69,8 @@ struct PlainSource
         if (!reflect || L <= 0) return 0.f;
         return __ldg(x + reflect_index(i, 0, L));
     }
+    // 4 consecutive in-range samples from 16-byte aligned x + i
+    __device__ __forceinline__ float4 quad(int i) const { return __ldg(reinterpret_cast<const float4*>(x + i)); }
 };
 
 // The pre-emphasized signal y[0] = x[0] - c*border, y[i] = x[i] - c*x[i-1]
@@ -81,28 +92,72 @@ struct PreemphSource
         if (!reflect || L <= 0) return 0.f;
         return at(reflect_index(i, 0, L));
     }
+    __device__ __forceinline__ float4 quad(int i) const
+    {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(x + i));
+        const float p = i == 0 ? border : __ldg(x + i - 1);
+        return make_float4(__fsub_rn(v.x, __fmul_rn(c, p)), __fsub_rn(v.y, __fmul_rn(c, v.x)),
+                           __fsub_rn(v.z, __fmul_rn(c, v.y)), __fsub_rn(v.w, __fmul_rn(c, v.z)));
+    }
 };
+
+// Fills the per-CTA constant tables: s_tw[k] = W_nfft^k (k <= M/2, the unpack twiddles), s_tw1[k1][j] =
+// W_M^(j*k1) = W_nfft^(2*j*k1), s_win[t] = window[t].  All threads call; ends with __syncthreads.
+template <int NFFT, int THREADS>
+__device__ __forceinline__ void stft_tables(const float2* __restrict__ twiddle, const float* __restrict__ window, int W,
+                                            float2* s_tw, float2* s_tw1, float* s_win)
+{
+    using S = StftShape<NFFT, THREADS>;
+    for (int i = threadIdx.x; i <= S::M / 2; i += THREADS) s_tw[i] = twiddle[i];
+    for (int i = threadIdx.x; i < S::R1 * S::R2; i += THREADS)
+    {
+        const int k1 = i / S::R2, j = i % S::R2;
+        s_tw1[i] = twiddle[(2 * j * k1) & (NFFT - 1)];
+    }
+    for (int i = threadIdx.x; i < NFFT; i += THREADS) s_win[i] = i < W ? window[i] : 0.f;
+    __syncthreads();
+}
 
 // Computes frames f0 .. f0+TF-1 (those < F) of one sample into s_out[bin * OUT_LD + f] and
 // leaves the other columns undefined.  All THREADS threads of the CTA must call it.
 template <int NFFT, int THREADS, class Src>
 __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, int hop, int centerOffset, int power,
                                           const float* __restrict__ s_win, const float2* __restrict__ s_tw,
+                                          const float2* __restrict__ s_tw1, float* __restrict__ s_span,
                                           float2* __restrict__ s_fft, float* __restrict__ s_out)
 {
     using S = StftShape<NFFT, THREADS>;
     constexpr int M = S::M, R1 = S::R1, R2 = S::R2, TF = S::TF, G = S::G, FPP = S::FPP, BINS = S::BINS;
+
+    // ---- 1. stage the tile's input span
+    const int Tv = min(TF, F - f0);
+    const int spanStart = f0 * hop - centerOffset;
+    const int spanLen = (Tv - 1) * hop + W;
+    if (spanStart >= 0 && spanStart + spanLen <= src.L &&
+        (reinterpret_cast<uintptr_t>(src.x + spanStart) & 15) == 0)
+    {
+        const int quads = spanLen >> 2;
+        for (int q = threadIdx.x; q < quads; q += THREADS)
+            reinterpret_cast<float4*>(s_span)[q] = src.quad(spanStart + 4 * q);
+        for (int i = (quads << 2) + threadIdx.x; i < spanLen; i += THREADS) s_span[i] = src(spanStart + i);
+    }
+    else
+    {
+        for (int i = threadIdx.x; i < spanLen; i += THREADS) s_span[i] = src(spanStart + i);
+    }
+    __syncthreads();
+
     const int j = threadIdx.x % G;
     const int slot = threadIdx.x / G;
     float2* buf = s_fft + slot * S::FFT_SLOT;
     const int off = (W < NFFT) ? (NFFT - W) / 2 : 0;
+    const bool pairs = ((off | hop) & 1) == 0;   // (window index, span index) pairs are 8-byte aligned
 #pragma unroll 1
     for (int pass = 0; pass < S::PASSES; ++pass)
     {
         const int fl = pass * FPP + slot;
-        const int frame = f0 + fl;
-        const int ws = frame * hop - centerOffset;
-        const bool live = fl < TF && frame < F;
+        const bool live = fl < Tv;
+        const float* fs = s_span + fl * hop;     // frame start in the span
         float2 z[R1];
 #pragma unroll
         for (int m = 0; m < R1; ++m)
@@ -111,8 +166,18 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
             float re = 0.f, im = 0.f;
             if (live)
             {
-                if (t0 >= 0 && t0 < W) re = s_win[t0] * src(ws + t0);
-                if (t0 + 1 >= 0 && t0 + 1 < W) im = s_win[t0 + 1] * src(ws + t0 + 1);
+                if (pairs && t0 >= 0 && t0 + 1 < W)
+                {
+                    const float2 d = *reinterpret_cast<const float2*>(fs + t0);
+                    const float2 wv = *reinterpret_cast<const float2*>(s_win + t0);
+                    re = wv.x * d.x;
+                    im = wv.y * d.y;
+                }
+                else
+                {
+                    if (t0 >= 0 && t0 < W) re = s_win[t0] * fs[t0];
+                    if (t0 + 1 >= 0 && t0 + 1 < W) im = s_win[t0 + 1] * fs[t0 + 1];
+                }
             }
             z[m] = make_float2(re, im);
         }
@@ -120,7 +185,7 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
 #pragma unroll
         for (int k1 = 0; k1 < R1; ++k1)
         {
-            const float2 t = s_tw[(2 * j * k1) & (NFFT - 1)];
+            const float2 t = s_tw1[k1 * R2 + j];
             buf[k1 * (R2 + 1) + j] = fft::cmul_conj(z[k1], t.x, t.y);
         }
         __syncwarp();
@@ -145,22 +210,27 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
         __syncwarp();
         if (fl < TF)
         {
-            for (int k = j; k < BINS; k += G)
+            for (int k = j; k <= M / 2; k += G)
             {
-                const float2 A = buf[k & (M - 1)];
+                const float2 A = buf[k];
                 const float2 B = buf[(M - k) & (M - 1)];
-                // E = (A + conj(B)) / 2,  O = (A - conj(B)) / (2i),  X = E + W_nfft^k O
+                // E = (A + conj(B)) / 2,  O = (A - conj(B)) / (2i),  P = W^k O
                 const float er = 0.5f * (A.x + B.x), ei = 0.5f * (A.y - B.y);
                 const float orr = 0.5f * (A.y + B.y), oi = -0.5f * (A.x - B.x);
-                const float2 t = s_tw[k & (NFFT - 1)];
-                const float xr = er + fmaf(orr, t.x, oi * t.y);
-                const float xi = ei + fmaf(oi, t.x, -orr * t.y);
-                const float p = fmaf(xr, xr, xi * xi);
-                s_out[k * S::OUT_LD + fl] = (power == 1) ? sqrtf(p) : p;
+                const float2 t = s_tw[k];
+                const float pr = fmaf(orr, t.x, oi * t.y);
+                const float pi = fmaf(oi, t.x, -orr * t.y);
+                const float xr = er + pr, xi = ei + pi;      // X[k] = E + P
+                const float yr = er - pr, yi = ei - pi;      // X[M-k] = conj(E - P)
+                const float p0 = fmaf(xr, xr, xi * xi);
+                const float p1 = fmaf(yr, yr, yi * yi);
+                s_out[k * S::OUT_LD + fl] = (power == 1) ? sqrtf(p0) : p0;
+                if (k != M - k) s_out[(M - k) * S::OUT_LD + fl] = (power == 1) ? sqrtf(p1) : p1;
             }
         }
         __syncwarp();
     }
+    (void)BINS;
 }
 
 }  // namespace rppb

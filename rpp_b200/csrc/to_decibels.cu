@@ -27,6 +27,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kChunk = 4096;
 
+constexpr int kRowsPerUnit = 8;   // rows of a 2-D sample per work unit
+
 struct DecibelCount
 {
     const uint32_t* dims;
@@ -34,14 +36,14 @@ struct DecibelCount
     {
         long long wdt = dims[2 * b], hgt = dims[2 * b + 1];
         if (wdt == 1) return (hgt + kChunk - 1) / kChunk;
-        return hgt * ((wdt + kChunk - 1) / kChunk);
+        return ((hgt + kRowsPerUnit - 1) / kRowsPerUnit) * ((wdt + kChunk - 1) / kChunk);
     }
 };
 
-// Unit w of sample b -> row, first column, column count.
+// Unit u of a sample -> first row, row count, first column, column count.
 struct UnitSpan
 {
-    uint32_t row, col0, cols;
+    uint32_t row, rows, col0, cols;
 };
 __device__ __forceinline__ UnitSpan unit_span(uint32_t wdt, uint32_t hgt, long long u)
 {
@@ -49,13 +51,15 @@ __device__ __forceinline__ UnitSpan unit_span(uint32_t wdt, uint32_t hgt, long l
     if (wdt == 1)
     {
         s.row = 0;
+        s.rows = 1;
         s.col0 = uint32_t(u) * kChunk;
         s.cols = min(uint32_t(kChunk), hgt - s.col0);
     }
     else
     {
-        uint32_t chunks = (wdt + kChunk - 1) / kChunk;
-        s.row = uint32_t(u / chunks);
+        const uint32_t chunks = (wdt + kChunk - 1) / kChunk;
+        s.row = uint32_t(u / chunks) * kRowsPerUnit;
+        s.rows = min(uint32_t(kRowsPerUnit), hgt - s.row);
         s.col0 = uint32_t(u % chunks) * kChunk;
         s.cols = min(uint32_t(kChunk), wdt - s.col0);
     }
@@ -68,15 +72,20 @@ __global__ void __launch_bounds__(kThreads) decibel_max_kernel(const float* __re
                                                                const long long* __restrict__ prefix, int n)
 {
     __shared__ float warpMax[kThreads / 32];
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, n, s_prefix);
     const long long total = prefix[n];
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
     {
         const int b = ragged_find(prefix, n, w);
         const uint32_t wdt = dims[2 * b], hgt = dims[2 * b + 1];
         const UnitSpan s = unit_span(wdt, hgt, w - prefix[b]);
-        const float* x = src + size_t(b) * nStride + size_t(s.row) * hStride + s.col0;
         float m = -FLT_MAX;
-        for (uint32_t c = threadIdx.x; c < s.cols; c += kThreads) m = fmaxf(m, x[c]);
+        for (uint32_t r = 0; r < s.rows; ++r)
+        {
+            const float* x = src + size_t(b) * nStride + size_t(s.row + r) * hStride + s.col0;
+            for (uint32_t c = threadIdx.x; c < s.cols; c += kThreads) m = fmaxf(m, x[c]);
+        }
         m = warp_max(m);
         if ((threadIdx.x & 31) == 0) warpMax[threadIdx.x >> 5] = m;
         __syncthreads();
@@ -99,6 +108,8 @@ __global__ void __launch_bounds__(kThreads) decibel_kernel(const float* __restri
                                                            float minRatio, float multiplier,
                                                            const long long* __restrict__ prefix, int n)
 {
+    __shared__ long long s_prefix[kPrefixCache];
+    prefix = cache_prefix(prefix, n, s_prefix);
     const long long total = prefix[n];
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
     {
@@ -112,13 +123,16 @@ __global__ void __launch_bounds__(kThreads) decibel_kernel(const float* __restri
             ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
         }
         const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
-        const float* x = src + size_t(b) * srcNStride + size_t(s.row) * srcHStride + s.col0;
-        float* y = dst + size_t(b) * dstNStride + size_t(s.row) * dstHStride + s.col0;
-        for (uint32_t c = threadIdx.x; c < s.cols; c += kThreads)
+        for (uint32_t r = 0; r < s.rows; ++r)
         {
-            float v = __fmul_rn(x[c], inv);
-            v = minRatio < v ? v : minRatio;
-            y[c] = __fmul_rn(multiplier, log2f(v));
+            const float* x = src + size_t(b) * srcNStride + size_t(s.row + r) * srcHStride + s.col0;
+            float* y = dst + size_t(b) * dstNStride + size_t(s.row + r) * dstHStride + s.col0;
+            for (uint32_t c = threadIdx.x; c < s.cols; c += kThreads)
+            {
+                float v = __fmul_rn(x[c], inv);
+                v = minRatio < v ? v : minRatio;
+                y[c] = __fmul_rn(multiplier, log2f(v));
+            }
         }
     }
 }

@@ -117,7 +117,7 @@ def test_frontend_graph_capture(gpu):
     gpu.set_stream(s.cuda_stream)
     try:
         with torch.cuda.stream(s):
-            out.fill_(0.0)
+            out.fill_(-12345.0)   # the canvas value: replay must rewrite exactly the first call's values
             torch.cuda.synchronize()
             with torch.cuda.graph(g, stream=s):
                 assert audio.frontend(xd, sd, out, dd, ld, cd, p, gpu) == OK

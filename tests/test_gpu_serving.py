@@ -1,0 +1,63 @@
+"""The continuous-batching server (rpp_b200/serving.py): each request's result is the same alone and
+in a mix of concurrently admitted requests, and equals the descriptor-based calls
+(rppb_downmix_resample_gpu + rppb_frontend_gpu) on the same clip."""
+import numpy as np
+import pytest
+import torch
+
+from rpp_b200 import audio, serving
+from rpp_b200.types import RppStatus, audio_desc, spectra_desc, frontend_params
+from rpp_b200.windows import kaiser_sinc
+
+pytestmark = pytest.mark.gpu
+
+
+def requests(seed, n):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [serving.make_request(torch, i, rng, max_s=6.0) for i in range(n)]
+
+
+def run(server, reqs, arrivals=None):
+    for r in reqs:
+        serving.attach_outputs(torch, server, r)
+    done = server.run(reqs, arrivals)
+    torch.cuda.synchronize()
+    return {r.rid: [o.clone() for o in r.outputs] for r in done}
+
+
+def test_alone_equals_mixed():
+    server = serving.FrontendServer(torch, budget_bytes=1 << 30, max_clips=64, tables=3)
+    mix = requests(7, 24)
+    probe = mix[5]
+    alone = run(server, [probe])[probe.rid]
+    arrivals = list(np.linspace(0.0, 0.02, len(mix)))
+    mixed = run(server, mix, arrivals)
+    assert len(mixed) == len(mix)
+    for a, b in zip(alone, mixed[probe.rid]):
+        assert torch.equal(a, b)
+    assert server.arena.used == 0
+
+
+def test_server_equals_descriptor_calls(gpu):
+    server = serving.FrontendServer(torch, budget_bytes=1 << 28, max_clips=16, tables=2)
+    reqs = requests(11, 3)
+    out = run(server, reqs)
+    lut, scale, center, lobes = kaiser_sinc(16)
+    lut_d = torch.from_numpy(lut).cuda()
+    p = frontend_params()
+    for r in reqs:
+        for c, rate, got in zip(r.clips, r.rates, out[r.rid]):
+            L = c.numel()
+            x = c.cuda().view(1, L)
+            lr, f = server._frames(L, rate)
+            mono = torch.zeros((1, lr + 8), device="cuda")
+            dims = torch.tensor([[L, 1]], dtype=torch.int32, device="cuda")
+            assert audio.downmix_resample(x, audio_desc(1, L), mono, audio_desc(1, lr + 8),
+                                          torch.tensor([rate], device="cuda"), torch.tensor([16000.0], device="cuda"),
+                                          dims, False, lut_d, scale, center, lobes, gpu) == RppStatus.RPP_SUCCESS
+            dst = torch.full((1, 128, max(f, 1)), -7.0, device="cuda")
+            assert audio.frontend(mono, audio_desc(1, lr + 8), dst, spectra_desc(1, 128, max(f, 1)),
+                                  torch.tensor([lr], dtype=torch.int32, device="cuda"),
+                                  torch.tensor([0.97], device="cuda"), p, gpu) == RppStatus.RPP_SUCCESS
+            torch.cuda.synchronize()
+            assert torch.equal(dst[0].cpu(), got)
