@@ -44,6 +44,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--clips", type=int, default=256)
+    p.add_argument("--precision", type=int, default=1, help="run the configs[2] precision study (0: skip)")
     p.add_argument("--serve-requests", type=int, default=600,
                    help="requests per offered-load point of the serving measurement (0 skips it)")
     return p.parse_args()
@@ -434,6 +435,139 @@ def multirate_measurement(torch, h, steps=10, n=2048):
             "input_bytes": in_bytes, "graph": "both calls captured in one CUDA graph (4 kernels + 1 memset)"}
 
 
+def gpu_config2(torch, n, length, seed=20261203 + 2):
+    """configs[2]-shaped batch synthesized on the GPU for timing: 3 tones per clip plus white noise
+    40 + 20 * (i % 5) dB below the tones' peak (the host generator needs ~20 s for 1024 x 10 s)."""
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    x = torch.empty((n, length), device=dev)
+    t = torch.arange(length, device=dev, dtype=torch.float64) / RATE
+    for c0 in range(0, n, 64):
+        c1 = min(n, c0 + 64)
+        f = torch.rand((c1 - c0, 3, 1), device=dev, generator=g, dtype=torch.float64) * 5900.0 + 100.0
+        a = torch.rand((c1 - c0, 3, 1), device=dev, generator=g, dtype=torch.float64) * 0.45 + 0.05
+        ph = torch.rand((c1 - c0, 3, 1), device=dev, generator=g, dtype=torch.float64) * 2 * np.pi
+        sig = (a * torch.sin(2 * np.pi * f * t[None, None, :] + ph)).sum(1)
+        floors = 40.0 + 20.0 * (torch.arange(c0, c1, device=dev) % 5).to(torch.float64)
+        sigma = sig.abs().amax(1) * 10.0 ** (-floors / 20.0)
+        sig += torch.randn(sig.shape, device=dev, generator=g, dtype=torch.float64) * sigma[:, None]
+        x[c0:c1] = sig.float()
+        del sig
+    return x
+
+
+def precision_measurement(torch, h, check_clips=20, n=1024, length=160000, reps=5):
+    """precision study of the spectrogram (and the mel/dB chain after it) in FP32 (the
+    register-FFT path) and on tensor cores (DFT-as-GEMM with BF16, BF16 hi/lo x3, TF32, FP8 E4M3 with
+    per-frame scaling; FP32 accumulation).  nfft 512 and 1024, window = nfft (Hann), hop = nfft / 4,
+    pre-emphasis 0.97.  Errors: on the first `check_clips` clips of the seeded host batch (two per
+    dynamic range 40..120 dB) against the FP64 oracle chain; power per frame relative (|err| / the
+    frame's largest bin), dB absolute where the FP64 mel power is within 60 dB of its frame's maximum
+    and everywhere above the cutoff.  Time: the full 1024 x 10 s batch (GPU-synthesized, same model),
+    device events around the call (pre-emphasis included in every variant), median of `reps`."""
+    from oracle import Oracle
+    from rpp_b200 import audio
+    orc = Oracle()
+    xs, ls, floors = synth.config2(n=check_clips, length=length)
+    xs_d = torch.from_numpy(xs).cuda()
+    ls_d = torch.from_numpy(ls).cuda()
+    cs_d = torch.full((check_clips,), COEFF, device="cuda")
+    xf = gpu_config2(torch, n, length)
+    lf = torch.full((n,), length, dtype=torch.int32, device="cuda")
+    cf = torch.full((n,), COEFF, device="cuda")
+    tc_modes = {"tc_bf16": audio.TC_BF16, "tc_bf16_hilo3": audio.TC_BF16_HILO3, "tc_tf32": audio.TC_TF32,
+                "tc_fp8_e4m3": audio.TC_FP8_E4M3}
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.isfile(pk):
+        peaks = json.load(open(pk))
+    result = {"workload": "configs[2]: 1024 clips x 10 s @16 kHz, 3 tones + white noise 40/60/80/100/120 dB below "
+                          "the tones' peak; pre-emphasis 0.97 -> spectrogram (Hann, window = nfft, hop = nfft/4, "
+                          "centred, reflect, power 2) -> mel(128, Slaney, normalized) -> dB(x10, -80 dB)",
+              "error_clips": check_clips, "dynamic_ranges_db": [float(f) for f in floors[:5]],
+              "oracle": "FP64 restatement (oracle/rppb_oracle.c)", "nfft": {}}
+    for nfft in (512, 1024):
+        W, hop, bins = nfft, nfft // 4, nfft // 2 + 1
+        F = length // hop + 1
+        spec64 = orc.spectrogram_f64(xs, ls, 1, 1, None, nfft, 2, W, hop, 1, max_frames=F,
+                                     preemph_coeff=np.full(check_clips, COEFF, np.float32))
+        dims = np.stack([np.full(check_clips, bins, np.int32), np.full(check_clips, F, np.int32)], 1).ravel()
+        mel64 = orc.mel_filter_bank_f64(spec64, dims, 8000.0, 0.0, 0, NMEL, float(RATE), 1)
+        db64 = orc.to_decibels_f64(mel64, np.full(check_clips, NMEL, np.int32), np.full(check_clips, F, np.int32),
+                                   CUTOFF_DB, MULT, 0.0)
+
+        def run(name, x, lens, coeff, nn, spec):
+            sd, dd = audio_desc(nn, length), spectra_desc(nn, bins, F)
+            if name == "fp32_fft":
+                pre = torch.empty_like(x)
+                assert audio.pre_emphasis_filter(x, sd, pre, sd, lens, coeff, 0, h) == 0
+                assert audio.spectrogram(pre, sd, spec, dd, lens, True, True, None, nfft, 2, W, hop, h) == 0
+            else:
+                assert audio.spectrogram_tc(x, sd, spec, dd, lens, coeff, 0, True, True, nfft, 2, W, hop,
+                                            tc_modes[name], h) == 0
+
+        per = {}
+        for name in ["fp32_fft"] + list(tc_modes):
+            spec = torch.zeros((check_clips, bins, F), device="cuda")
+            run(name, xs_d, ls_d, cs_d, check_clips, spec)
+            mel = torch.zeros((check_clips, NMEL, F), device="cuda")
+            dimd = torch.from_numpy(dims.reshape(-1, 2).copy()).cuda()
+            assert audio.mel_filter_bank(spec, spectra_desc(check_clips, bins, F), mel,
+                                         spectra_desc(check_clips, NMEL, F), dimd, 8000.0, 0.0, 0, NMEL, float(RATE),
+                                         True, h) == 0
+            db = torch.zeros_like(mel)
+            patches = torch.from_numpy(np.tile(np.array([[F, NMEL]], np.int32), (check_clips, 1))).cuda()
+            md = spectra_desc(check_clips, NMEL, F)
+            assert audio.to_decibels(mel, md, db, md, patches, CUTOFF_DB, MULT, 0.0, h) == 0
+            torch.cuda.synchronize()
+            sp, dbh = spec.cpu().numpy().astype(np.float64), db.cpu().numpy().astype(np.float64)
+            by_dr = {}
+            all_rel, all_db = [], []
+            for i in range(check_clips):
+                rel = np.abs(sp[i] - spec64[i]) / np.maximum(spec64[i].max(axis=0, keepdims=True), 1e-300)
+                e = np.abs(dbh[i] - db64[i])
+                near = db64[i] >= db64[i].max(axis=0, keepdims=True) - 60.0
+                d = by_dr.setdefault(int(floors[i]), {"power_rel_max": 0.0, "db_max_within_60db": 0.0,
+                                                      "db_max": 0.0})
+                d["power_rel_max"] = max(d["power_rel_max"], float(rel.max()))
+                d["db_max_within_60db"] = max(d["db_max_within_60db"], float(e[near].max()))
+                d["db_max"] = max(d["db_max"], float(e.max()))
+                all_rel.append(rel.ravel())
+                all_db.append(e.ravel())
+            rel = np.concatenate(all_rel)
+            e = np.concatenate(all_db)
+            # time on the full batch
+            out = torch.empty((n, bins, F), device="cuda")
+            run(name, xf, lf, cf, n, out)
+            times = []
+            for _ in range(reps):
+                a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a_.record()
+                run(name, xf, lf, cf, n, out)
+                b_.record()
+                torch.cuda.synchronize()
+                times.append(a_.elapsed_time(b_))
+            ms = float(np.median(times))
+            v = {"power_rel_err_max": float(rel.max()), "power_rel_err_rms": float(np.sqrt((rel ** 2).mean())),
+                 "db_err_max": float(e.max()), "db_err_rms": float(np.sqrt((e ** 2).mean())), "by_dynamic_range": by_dr,
+                 "ms": ms, "clip_s_per_s": n * length / RATE / (ms / 1e3)}
+            if name != "fp32_fft":
+                block = 128 // {"tc_bf16": 2, "tc_bf16_hilo3": 2, "tc_tf32": 4, "tc_fp8_e4m3": 1}[name]
+                kpad = -(-W // block) * block
+                mmas = 3 if name == "tc_bf16_hilo3" else 1
+                flops = 2.0 * n * (-(-F // 128) * 128) * nfft * kpad * mmas
+                v["tensor_tflops_issued"] = flops / (ms / 1e3) / 1e12
+                if peaks.get("bf16_tflops"):
+                    v["frac_of_measured_bf16_peak"] = v["tensor_tflops_issued"] / peaks["bf16_tflops"]
+            per[name] = v
+            del out, spec, mel, db
+        result["nfft"][str(nfft)] = per
+    del xf
+    torch.cuda.empty_cache()
+    return result
+
+
 def read_traffic(kernel):
     """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
@@ -562,6 +696,12 @@ def run_b200(args, world, rank, local):
             multirate = multirate_measurement(torch, h)
         except Exception as exc:
             multirate = {"error": repr(exc)}
+        precision = None
+        if args.precision:
+            try:
+                precision = precision_measurement(torch, h)
+            except Exception as exc:
+                precision = {"error": repr(exc)}
         serve = None
         if args.serve_requests > 0:
             try:
@@ -597,6 +737,7 @@ def run_b200(args, world, rank, local):
             "e2e": e2e,
             "multirate": multirate,
             "serving": serve,
+            "precision": precision,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

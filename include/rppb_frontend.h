@@ -96,6 +96,28 @@ SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips, Rpp32s nu
                                                 Rpp32s lobes, Rpp32f preemphCoeff, const RppbFrontendParams* params,
                                                 rppHandle_t rppHandle);
 
+/* Operand precision of the tensor-core spectrogram; every variant accumulates in FP32. */
+typedef enum
+{
+    RPPB_TC_BF16 = 0,        /* BF16 operands, one pass */
+    RPPB_TC_BF16_HILO3 = 1,  /* x = hi + lo, both BF16; hi*hi + hi*lo + lo*hi */
+    RPPB_TC_TF32 = 2,        /* FP32 rounded to TF32 */
+    RPPB_TC_FP8_E4M3 = 3     /* E4M3 with one scale per frame (largest sample -> 448) */
+} RppbTensorCorePrecision;
+
+/* Tensor-core spectrogram (precision study): the short-time DFT as a GEMM on tcgen05 tensor cores
+ * with the window folded into the DFT basis.  Same framing and output layouts as
+ * rppt_spectrogram_gpu with the Hann window (no windowFunction argument); coeffTensor (nullable)
+ * applies pre-emphasis first, as rppt_pre_emphasis_filter_gpu with borderType would.  Requires nfft a
+ * multiple of 256, windowLength <= nfft, and windowStep a multiple of 8 (BF16) or 4 (TF32); otherwise
+ * RPP_ERROR_NOT_IMPLEMENTED.  Extension for the precision study (no counterpart in the reference). */
+SHARED_PUBLIC RppStatus rppb_spectrogram_tc_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor, Rpp32f* coeffTensor,
+                                                RpptAudioBorderType borderType, bool centerWindows,
+                                                bool reflectPadding, Rpp32s nfft, Rpp32s power, Rpp32s windowLength,
+                                                Rpp32s windowStep, RppbTensorCorePrecision precision,
+                                                rppHandle_t rppHandle);
+
 /* Reads (and clears) the handle's device error word: nonzero when a fused launch gave up
  * waiting for a clip's spectrum tiles (a bounded wait; the affected tiles are left unconverted).
  * Synchronizes the handle stream. */

@@ -138,3 +138,17 @@ def downmix_resample(src, src_desc, dst, dst_desc, in_rate, out_rate, src_dims, 
                                                _addr(in_rate), _addr(out_rate), _addr(src_dims),
                                                bool(normalize_weights), _addr(lut), int(len(lut)), float(scale),
                                                float(center), int(lobes), _h(handle)))
+
+
+TC_BF16, TC_BF16_HILO3, TC_TF32, TC_FP8_E4M3 = 0, 1, 2, 3   # RppbTensorCorePrecision
+
+
+def spectrogram_tc(src, src_desc, dst, dst_desc, src_length, coeff, border_type, center_windows, reflect_padding, nfft,
+                   power, window_length, window_step, precision, handle):
+    """rppb_spectrogram_tc_gpu: the tensor-core spectrogram of the precision study (precision: one of
+    TC_BF16, TC_BF16_HILO3, TC_TF32, TC_FP8_E4M3)."""
+    L = _lib.load()
+    return _status(L.rppb_spectrogram_tc_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                             _addr(src_length), _addr(coeff), int(border_type), bool(center_windows),
+                                             bool(reflect_padding), int(nfft), int(power), int(window_length),
+                                             int(window_step), int(precision), _h(handle)))

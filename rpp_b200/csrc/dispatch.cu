@@ -10,10 +10,12 @@
 // are used in place; pageable ones are staged into the workspace), then the launchers of
 // rpp_b200/csrc/*.cu enqueue the kernels on the handle stream.  Nothing here synchronizes the
 // stream except a pageable NSR output, whose device-to-host copy is stream-ordered.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/rppb_frontend.h"
 #include "../../include/rppt_tensor_audio_augmentations.h"
@@ -571,6 +573,91 @@ extern "C" SHARED_PUBLIC RppStatus rppb_get_device_error(rppHandle_t rppHandle, 
         check_cuda(cudaMemsetAsync(flags, 0, sizeof(int), h.stream()), "clear device error");
         check_cuda(cudaStreamSynchronize(h.stream()), "sync");
         *errorCode = v;
+        return RPP_SUCCESS;
+    });
+}
+
+namespace {
+
+struct TcBasisKey
+{
+    int fmt, nfft, W, kPad;
+};
+
+void build_tc_basis(float* out, size_t, const void* ctx)
+{
+    const TcBasisKey k = *static_cast<const TcBasisKey*>(ctx);
+    std::vector<float> win(k.W);
+    build_hann(win.data(), size_t(k.W), nullptr);
+    tc_build_basis(out, k.fmt, k.nfft, k.W, k.kPad, win.data());
+}
+
+}  // namespace
+
+extern "C" SHARED_PUBLIC RppStatus rppb_spectrogram_tc_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                           RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor,
+                                                           Rpp32f* coeffTensor, RpptAudioBorderType borderType,
+                                                           bool centerWindows, bool reflectPadding, Rpp32s nfft,
+                                                           Rpp32s power, Rpp32s windowLength, Rpp32s windowStep,
+                                                           RppbTensorCorePrecision precision, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        if ((dstDescPtr->layout != NFT) && (dstDescPtr->layout != NTF)) return RPP_ERROR_INVALID_DST_LAYOUT;
+        if (srcDescPtr->numDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (dstDescPtr->numDims != 3) return RPP_ERROR_INVALID_DST_DIMS;
+        if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr, "null tensor");
+        require(windowLength > 0 && windowStep > 0 && windowLength <= nfft, "invalid window");
+        const int fmt = int(precision);
+        if (fmt < kTcBf16 || fmt > kTcFp8) return RPP_ERROR_NOT_IMPLEMENTED;
+        // in-place BF16 / TF32 frame rows start every hop elements and must stay 16-byte aligned
+        const int granule = fmt == kTcTf32 ? 4 : fmt == kTcFp8 ? 1 : 8;
+        if (nfft % 256 != 0 || windowStep % granule != 0) return RPP_ERROR_NOT_IMPLEMENTED;
+        const bool nft = dstDescPtr->layout == NFT;
+        const Rpp32u binsCap = nft ? dstDescPtr->h : dstDescPtr->w;
+        if (binsCap < Rpp32u(nfft / 2 + 1)) return RPP_ERROR_INVALID_DST_DIMS;
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        const int maxFrames = int(nft ? dstDescPtr->w : dstDescPtr->h);
+        const TcGeometry geo = tc_geometry(fmt, windowLength, windowStep, maxFrames, nfft);
+        const size_t scratchBytes = tc_spectrogram_scratch_bytes(n, fmt, geo, maxFrames);
+        Carver m(nullptr);
+        m.take<int>(n);
+        m.take<float>(n);
+        m.take<char>(scratchBytes);
+        Carver cv(h.workspace(m.used()));
+        int* lenStage = cv.take<int>(n);
+        float* coeffStage = cv.take<float>(n);
+        void* scratch = cv.take<char>(scratchBytes);
+        TcBasisKey key{fmt, nfft, windowLength, geo.kPad};
+        const float* basis = h.table("tcbasis" + std::to_string(fmt) + "_" + std::to_string(nfft) + "_" +
+                                         std::to_string(windowLength),
+                                     geo.basisFloats, build_tc_basis, &key);
+        TcSpectrogramArgs a;
+        a.src = static_cast<const float*>(srcPtr);
+        a.srcStride = srcDescPtr->strides.nStride;
+        a.srcElems = size_t(n) * srcDescPtr->strides.nStride;
+        a.len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
+        a.coeff = coeffTensor ? static_cast<const float*>(h.device_view(coeffTensor, n * sizeof(float), coeffStage))
+                              : nullptr;
+        a.border = int(borderType);
+        a.center = centerWindows;
+        a.reflect = reflectPadding;
+        a.windowLength = windowLength;
+        a.windowStep = windowStep;
+        a.nfft = nfft;
+        a.fmt = fmt;
+        a.geo = geo;
+        a.maxFrames = maxFrames;
+        a.basis = basis;
+        a.dst = static_cast<float*>(dstPtr);
+        a.dstNStride = dstDescPtr->strides.nStride;
+        a.dstHStride = dstDescPtr->strides.hStride;
+        a.nft = nft;
+        a.power = power;
+        a.n = n;
+        launch_tc_spectrogram(h, scratch, a);
         return RPP_SUCCESS;
     });
 }

@@ -137,4 +137,45 @@ struct FrontendArgs
 size_t frontend_scratch_bytes(int n, int lookahead);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);
 
+// Tensor-core spectrogram (tc_dft.cu).
+enum TcFormat
+{
+    kTcBf16 = 0,       // BF16 operands, one pass
+    kTcBf16x3 = 1,     // BF16 hi + lo split, three passes (hi*hi + hi*lo + lo*hi)
+    kTcTf32 = 2,       // TF32 operands (FP32 rounded to 10 mantissa bits)
+    kTcFp8 = 3,        // FP8 E4M3 operands, frames scaled to the format's range one by one
+};
+struct TcGeometry
+{
+    int kPad;            // window length rounded up to one 128-byte row of operand elements
+    uint32_t rowStep;    // elements between consecutive frames' rows of the A operand
+    uint32_t clipStride; // elements per clip of the A operand
+    size_t basisFloats;  // size of the cached basis table, in floats
+};
+TcGeometry tc_geometry(int fmt, int windowLength, int windowStep, int maxFrames, int nfft);
+// Window-folded DFT basis [nfft][kPad] in the format's element type (hi then lo for kTcBf16x3).
+void tc_build_basis(float* out, int fmt, int nfft, int windowLength, int kPad, const float* window);
+struct TcSpectrogramArgs
+{
+    const float* src;
+    uint32_t srcStride;
+    size_t srcElems;
+    const int* len;
+    const float* coeff;       // pre-emphasis coefficients, nullptr: none
+    int border;
+    bool center, reflect;
+    int windowLength, windowStep, nfft;
+    int fmt;
+    TcGeometry geo;
+    int maxFrames;
+    const void* basis;
+    float* dst;
+    uint32_t dstNStride, dstHStride;
+    bool nft;
+    int power;
+    int n;
+};
+size_t tc_spectrogram_scratch_bytes(int n, int fmt, const TcGeometry& g, int maxFrames);
+void launch_tc_spectrogram(Handle& h, void* scratch, const TcSpectrogramArgs& a);
+
 }  // namespace rppb

@@ -1,0 +1,669 @@
+// Tensor-core spectrogram: the short-time DFT as a GEMM on the 5th-generation tensor cores (tcgen05,
+// accumulators in tensor memory), for the precision study of the front end.
+//
+//   power[f][k] = |sum_t frame_f[t] * w[t] * exp(-2 pi i k (t + off) / nfft)|^2
+//
+// is the GEMM C = A x B^T with A[f][t] = the (pre-emphasized, padded) signal sample of frame f at
+// window position t (M = frames, K = window length padded to one 128-byte row) and B[n][t] = the
+// window-folded DFT basis, n = 2k -> w[t] cos(.), n = 2k + 1 -> -w[t] sin(.) for bins 1..nfft/2-1;
+// column 0 holds bin 0 and column 1 (the identically zero sine of bin 0) holds the Nyquist bin, so
+// N = nfft exactly.  The basis is built in FP64 on the host and rounded once to the operand format.
+//
+// Operand formats (FP32 accumulation in every case):
+//   kTcBf16    BF16, one pass;
+//   kTcBf16x3  x = hi + lo with both parts BF16; hi*hi + hi*lo + lo*hi (three MMAs per K step);
+//   kTcTf32    FP32 rounded to TF32 (round to nearest, ties away) before the MMA;
+//   kTcFp8     E4M3; every frame is materialized and scaled so its largest sample maps to 448, the
+//              basis is scaled by 256, and the epilogue divides both scales out.
+// A is read in place from the padded signal for BF16/TF32 (frame f's row starts at f * hop, so rows
+// overlap and the 16-byte copy granule requires hop * element size to be a multiple of 16); FP8
+// frames are materialized [frame][kPad] because each carries its own scale.
+//
+// Structure (one CTA per SM, 128 threads, persistent over (clip, 128-frame tile, 256-column chunk)
+// work items): shared-memory stages of A (128 rows) and B (256 rows) of one 128-byte K block each,
+// filled with cp.async in the 128-byte-swizzled K-major layout the UMMA descriptors describe; thread
+// 0 issues tcgen05.mma (M = 128, N = 256, 32 bytes of K per instruction) and commits each stage to an
+// mbarrier, so the copies of stage s+1 overlap the MMAs of stage s.  All waits are bounded: a
+// timeout sets the device error word, waits once more (bounded) for the MMAs in flight, frees
+// tensor memory and leaves.  The epilogue reads the accumulator with tcgen05.ld (warp w owns rows
+// 32w..32w+31), forms re^2 + im^2 and stores NFT rows (32 consecutive frames per warp store) or NTF
+// rows.
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "ops.hpp"
+
+namespace rppb {
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kTileM = 128;          // frames per tile
+constexpr int kTileN = 256;          // basis columns per MMA / work item
+constexpr int kRowBytes = 128;       // one swizzled K block per row
+constexpr long long kWaitLimit = 1ll << 21;   // try_wait polls: on the order of a second
+constexpr float kFp8BasisScale = 256.f;
+constexpr float kFp8Max = 448.f;
+
+constexpr size_t kABytes = size_t(kTileM) * kRowBytes;   // 16 KB
+constexpr size_t kBBytes = size_t(kTileN) * kRowBytes;   // 32 KB
+
+template <int FMT>
+struct Fmt
+{
+    static constexpr int kElem = (FMT == kTcTf32) ? 4 : (FMT == kTcFp8) ? 1 : 2;
+    static constexpr int kBlockK = kRowBytes / kElem;       // elements per K block
+    static constexpr bool kSplit = FMT == kTcBf16x3;
+    static constexpr size_t kStageBytes = (kSplit ? 2 : 1) * (kABytes + kBBytes);
+    static constexpr int kStages = kSplit ? 2 : 4;          // 192 KB of stages either way
+    // Instruction descriptor: F32 accumulator (bit 4), A/B formats (bits 7, 10), both K-major,
+    // N >> 3 at bit 17, M >> 4 at bit 24.  Formats: kind::f16 BF16 = 1, kind::tf32 TF32 = 2,
+    // kind::f8f6f4 E4M3 = 0.
+    static constexpr uint32_t kFormat = (FMT == kTcTf32) ? 2u : (FMT == kTcFp8) ? 0u : 1u;
+    static constexpr uint32_t kIdesc = (1u << 4) | (kFormat << 7) | (kFormat << 10) | (uint32_t(kTileN >> 3) << 17) |
+                                       (uint32_t(kTileM >> 4) << 24);
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row atoms 1024 bytes apart.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= uint64_t((saddr >> 4) & 0x3FFF);            // start address
+    d |= uint64_t(1) << 16;                           // leading byte offset (unused for swizzled K-major)
+    d |= uint64_t(1024 >> 4) << 32;                   // stride byte offset: next 8-row atom
+    d |= uint64_t(1) << 46;                           // descriptor version (Blackwell)
+    d |= uint64_t(2) << 61;                           // layout: SWIZZLE_128B
+    return d;
+}
+
+template <int FMT>
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+    if constexpr (FMT == kTcTf32)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(a), "l"(b), "r"(Fmt<FMT>::kIdesc), "r"(accumulate));
+    else if constexpr (FMT == kTcFp8)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(a), "l"(b), "r"(Fmt<FMT>::kIdesc), "r"(accumulate));
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(a), "l"(b), "r"(Fmt<FMT>::kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Bounded wait for the mbarrier phase with parity `parity` to complete; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    const uint32_t a = smem_u32(bar);
+    for (long long i = 0; i < kWaitLimit; ++i)
+    {
+        uint32_t done = 0;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+
+// Byte offset of 16-byte chunk c (0..7) of row r in a 128-byte-swizzled K-major tile.
+__device__ __forceinline__ uint32_t sw128(int r, int c)
+{
+    return uint32_t((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
+}
+
+struct TcArgs
+{
+    const unsigned char* a;     // A operand, [n][clipStride] elements (hi part for the split format)
+    const unsigned char* aLo;   // lo part (split format only)
+    uint32_t clipStride;        // elements
+    uint32_t rowStep;           // elements between frame rows
+    const unsigned char* b;     // basis [nfft][kPad] elements
+    const unsigned char* bLo;
+    int kPad;
+    int nfft;
+    const float* invScale;      // FP8: per frame 1 / (frame scale * basis scale), [n][maxFrames]
+    int maxFrames;
+    float* dst;
+    uint32_t dstNStride, dstHStride;
+    bool nft;
+    int power;
+    const int* frames;          // frames per clip
+    int n;
+    int* errorWord;
+};
+
+struct TcCount
+{
+    const int* frames;
+    int chunks;
+    __device__ long long operator()(int b) const
+    {
+        const int F = max(frames[b], 0);
+        return (long long)((F + kTileM - 1) / kTileM) * chunks;
+    }
+};
+
+template <int FMT>
+__global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const long long* __restrict__ prefix)
+{
+    using T = Fmt<FMT>;
+    constexpr int S = T::kStages;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ uint64_t bars[S];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(kTileN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0)
+    {
+        for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+
+    const int chunks = a.nfft / kTileN;
+    const int kBlocks = a.kPad / T::kBlockK;
+    const long long total = prefix[a.n];
+    uint32_t issued[S], waited[S];   // commits made to / waited on each stage's barrier (every thread)
+#pragma unroll
+    for (int s = 0; s < S; ++s) issued[s] = waited[s] = 0;
+    int stage = 0;
+
+    for (long long w = blockIdx.x; w < total && !s_abort; w += gridDim.x)
+    {
+        const int b = ragged_find(prefix, a.n, w);
+        const int local = int(w - prefix[b]);
+        const int tile = local / chunks, chunk = local % chunks;
+        const int F = a.frames[b];
+        const int f0 = tile * kTileM;
+        const size_t clipOff = size_t(b) * a.clipStride;
+        const int n0 = chunk * kTileN;
+
+        for (int kb = 0; kb < kBlocks; ++kb)
+        {
+            const int s = stage;
+            stage = (stage + 1 == S) ? 0 : stage + 1;
+            // the stage's previous MMAs must have finished reading it
+            if (issued[s] > waited[s])
+            {
+                if (mbar_wait(&bars[s], waited[s] & 1)) waited[s] = issued[s];
+                else
+                {
+                    if (tid == 0) atomicOr(a.errorWord, 2);
+                    s_abort = 1;
+                }
+            }
+            __syncthreads();
+            if (s_abort) break;
+            unsigned char* sA = smem + s * T::kStageBytes;
+            unsigned char* sB = sA + kABytes;
+            unsigned char* sAl = sB + kBBytes;      // split format only
+            unsigned char* sBl = sAl + kABytes;
+            // A: 128 frames x 8 chunks of 16 bytes (frames past F re-read frame F-1; results unused)
+            for (int i = tid; i < kTileM * 8; i += kThreads)
+            {
+                const int r = i >> 3, c = i & 7;
+                const int fr = min(f0 + r, max(F - 1, 0));
+                const size_t off = (clipOff + size_t(fr) * a.rowStep + size_t(kb) * T::kBlockK) * T::kElem + c * 16;
+                cp_async16(sA + sw128(r, c), a.a + off);
+                if constexpr (T::kSplit) cp_async16(sAl + sw128(r, c), a.aLo + off);
+            }
+            // B: 256 basis columns x 8 chunks
+            for (int i = tid; i < kTileN * 8; i += kThreads)
+            {
+                const int r = i >> 3, c = i & 7;
+                const size_t off = (size_t(n0 + r) * a.kPad + size_t(kb) * T::kBlockK) * T::kElem + c * 16;
+                cp_async16(sB + sw128(r, c), a.b + off);
+                if constexpr (T::kSplit) cp_async16(sBl + sw128(r, c), a.bLo + off);
+            }
+            asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic-proxy writes -> tensor core
+            __syncthreads();
+            if (tid == 0)
+            {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint64_t dA = umma_desc(smem_u32(sA)), dB = umma_desc(smem_u32(sB));
+#pragma unroll
+                for (int ks = 0; ks < kRowBytes / 32; ++ks)
+                {
+                    const uint64_t step = uint64_t(ks * 32) >> 4;   // 32 bytes of K along the swizzled row
+                    const uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
+                    mma<FMT>(tmem, dA + step, dB + step, acc0);
+                    if constexpr (T::kSplit)
+                    {
+                        const uint64_t dAl = umma_desc(smem_u32(sAl)), dBl = umma_desc(smem_u32(sBl));
+                        mma<FMT>(tmem, dA + step, dBl + step, 1u);
+                        mma<FMT>(tmem, dAl + step, dB + step, 1u);
+                    }
+                }
+                mma_commit(&bars[s]);
+            }
+            ++issued[s];
+        }
+        if (s_abort) break;
+        // wait for this tile's MMAs (each stage's last commit covers everything issued before it)
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            if (issued[s] > waited[s])
+            {
+                if (mbar_wait(&bars[s], waited[s] & 1)) waited[s] = issued[s];
+                else
+                {
+                    if (tid == 0) atomicOr(a.errorWord, 2);
+                    s_abort = 1;
+                }
+            }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (s_abort) break;
+
+        // ---- epilogue: warp w owns accumulator rows (frames) 32w .. 32w+31
+        const int r = warp * 32 + lane;
+        const int frame = f0 + r;
+        float* y = a.dst + size_t(b) * a.dstNStride;
+        float sc = 1.f;
+        if constexpr (FMT == kTcFp8)
+            if (frame < F) sc = a.invScale[size_t(b) * a.maxFrames + frame];
+#pragma unroll 1
+        for (int c0 = 0; c0 < kTileN; c0 += 32)
+        {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (frame < F)
+            {
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                {
+                    const float re = __uint_as_float(v[2 * q]) * sc, im = __uint_as_float(v[2 * q + 1]) * sc;
+                    const int col = n0 + c0 + 2 * q;   // even column: bin col/2 (cos, -sin)
+                    if (col == 0)
+                    {
+                        // column 0: bin 0 (real); column 1: Nyquist bin (real)
+                        const float p0 = re * re, pn = im * im;
+                        const float o0 = a.power == 1 ? sqrtf(p0) : p0;
+                        const float on = a.power == 1 ? sqrtf(pn) : pn;
+                        const int nyq = a.nfft / 2;
+                        if (a.nft)
+                        {
+                            y[frame] = o0;
+                            y[size_t(nyq) * a.dstHStride + frame] = on;
+                        }
+                        else
+                        {
+                            y[size_t(frame) * a.dstHStride] = o0;
+                            y[size_t(frame) * a.dstHStride + nyq] = on;
+                        }
+                        continue;
+                    }
+                    const int bin = col >> 1;
+                    const float p = fmaf(re, re, im * im);
+                    const float o = a.power == 1 ? sqrtf(p) : p;
+                    if (a.nft) y[size_t(bin) * a.dstHStride + frame] = o;
+                    else y[size_t(frame) * a.dstHStride + bin] = o;
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();   // the next tile's MMAs overwrite the accumulator
+    }
+
+    // leave: make sure no MMA is still writing tensor memory (a second bounded wait after a timeout),
+    // then free it
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        if (issued[s] > waited[s] && mbar_wait(&bars[s], waited[s] & 1)) waited[s] = issued[s];
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTileN));
+}
+
+// The sample the spectrogram frames at padded position i (= signal index i - centerOffset): the
+// (optionally pre-emphasized) signal with reflect or zero padding, as stft.cuh's sources give it.
+struct PaddedSignal
+{
+    const float* x;
+    int L;
+    float c, border;
+    bool preemph, reflect;
+    int centerOffset;
+    __device__ __forceinline__ float operator()(long long i) const
+    {
+        long long t = i - centerOffset;
+        if (!(t >= 0 && t < L))
+        {
+            if (!reflect || L <= 0 || t > 0x3fffffff || t < -0x3fffffff) return 0.f;
+            t = reflect_index(int(t), 0, L);
+        }
+        if (!preemph) return x[t];
+        return __fsub_rn(x[t], __fmul_rn(c, t == 0 ? border : x[t - 1]));
+    }
+};
+
+__device__ __forceinline__ PaddedSignal padded_signal(const float* src, uint32_t srcStride, size_t srcElems,
+                                                      const int* len, const float* coeff, int border, bool reflect,
+                                                      int centerOffset, int b)
+{
+    PaddedSignal p;
+    p.x = src + size_t(b) * srcStride;
+    p.L = min(len[b], int(srcStride));
+    p.preemph = coeff != nullptr;
+    p.c = p.preemph ? coeff[b] : 0.f;
+    const size_t base = size_t(b) * srcStride;
+    p.border = border == 1 ? p.x[0] : border == 2 ? (base + 1 < srcElems ? p.x[1] : 0.f) : 0.f;
+    p.reflect = reflect;
+    p.centerOffset = centerOffset;
+    return p;
+}
+
+struct PrepArgs
+{
+    const float* src;
+    uint32_t srcStride;
+    size_t srcElems;
+    const int* len;
+    const float* coeff;
+    int border;
+    bool reflect;
+    int centerOffset;
+    int n;
+};
+
+// BF16 (hi, and lo for the split format) or TF32 copy of the padded signal, [n][clipStride].
+template <int FMT>
+__global__ void tc_prep_kernel(PrepArgs p, void* __restrict__ outHi, void* __restrict__ outLo, uint32_t clipStride)
+{
+    for (int b = blockIdx.y; b < p.n; b += gridDim.y)
+    {
+        const PaddedSignal sig =
+            padded_signal(p.src, p.srcStride, p.srcElems, p.len, p.coeff, p.border, p.reflect, p.centerOffset, b);
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < clipStride; i += gridDim.x * blockDim.x)
+        {
+            const float v = sig(i);
+            const size_t o = size_t(b) * clipStride + i;
+            if constexpr (FMT == kTcTf32)
+            {
+                uint32_t t;
+                asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
+                static_cast<uint32_t*>(outHi)[o] = t;
+            }
+            else
+            {
+                const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+                static_cast<__nv_bfloat16*>(outHi)[o] = hi;
+                if constexpr (FMT == kTcBf16x3)
+                    static_cast<__nv_bfloat16*>(outLo)[o] = __float2bfloat16_rn(v - __bfloat162float(hi));
+            }
+        }
+    }
+}
+
+// FP8: one warp per frame; frame f of clip b becomes row [f][kPad] scaled by 448 / max|sample|.
+__global__ void tc_prep_fp8_kernel(PrepArgs p, const int* __restrict__ frames, int maxFrames, int W, int hop, int kPad,
+                                   __nv_fp8_e4m3* __restrict__ out, float* __restrict__ invScale)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpsPerBlock = blockDim.x >> 5;
+    for (int b = blockIdx.y; b < p.n; b += gridDim.y)
+    {
+        const PaddedSignal sig =
+            padded_signal(p.src, p.srcStride, p.srcElems, p.len, p.coeff, p.border, p.reflect, p.centerOffset, b);
+        const int F = frames[b];
+        for (int f = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); f < F; f += gridDim.x * warpsPerBlock)
+        {
+            const long long s0 = (long long)f * hop;
+            float m = 0.f;
+            for (int t = lane; t < W; t += 32) m = fmaxf(m, fabsf(sig(s0 + t)));
+            m = warp_max(m);
+            const float scale = m > 0.f ? kFp8Max / m : 1.f;
+            __nv_fp8_e4m3* row = out + (size_t(b) * maxFrames + f) * kPad;
+            for (int t = lane; t < kPad; t += 32) row[t] = __nv_fp8_e4m3(t < W ? sig(s0 + t) * scale : 0.f);
+            if (lane == 0) invScale[size_t(b) * maxFrames + f] = 1.f / (scale * kFp8BasisScale);
+        }
+    }
+}
+
+__global__ void tc_frames_kernel(const int* __restrict__ len, uint32_t srcStride, int n, int W, int hop, bool center,
+                                 int maxFrames, int* __restrict__ frames)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
+        frames[b] = min(num_windows(min(len[b], int(srcStride)), W, hop, center), maxFrames);
+}
+
+template <int FMT>
+void launch_format(Handle& h, const TcArgs& a, const long long* prefix)
+{
+    const size_t smem = Fmt<FMT>::kStages * Fmt<FMT>::kStageBytes + 1024;
+    const int grid = persistent_grid(h, reinterpret_cast<const void*>(tc_dft_kernel<FMT>), kThreads, smem);
+    tc_dft_kernel<FMT><<<grid, kThreads, smem, h.stream()>>>(a, prefix);
+    count_launch(1);
+    check_cuda(cudaGetLastError(), "tc_dft_kernel");
+}
+
+int elem_bytes(int fmt) { return fmt == kTcTf32 ? 4 : fmt == kTcFp8 ? 1 : 2; }
+
+uint16_t bf16_rne(float f)
+{
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return uint16_t((u >> 16) | 0x40);   // NaN stays NaN
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return uint16_t(u >> 16);
+}
+
+float bf16_value(uint16_t h)
+{
+    const uint32_t u = uint32_t(h) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// FP32 -> TF32 (10 explicit mantissa bits), round to nearest with ties away from zero, finite inputs.
+uint32_t tf32_rna(float f)
+{
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return (u + 0x1000u) & 0xffffe000u;
+}
+
+}  // namespace
+
+TcGeometry tc_geometry(int fmt, int windowLength, int windowStep, int maxFrames, int nfft)
+{
+    const int e = elem_bytes(fmt);
+    const int blockK = kRowBytes / e;
+    TcGeometry g;
+    g.kPad = (windowLength + blockK - 1) / blockK * blockK;
+    const int frames = std::max(maxFrames, 1);
+    if (fmt == kTcFp8)
+    {
+        g.rowStep = uint32_t(g.kPad);
+        g.clipStride = uint32_t(size_t(frames) * g.kPad);
+    }
+    else
+    {
+        const size_t span = size_t(frames - 1) * windowStep + g.kPad;
+        const size_t granule = 16 / e;   // elements per 16 bytes: clip rows stay 16-byte aligned
+        g.rowStep = uint32_t(windowStep);
+        g.clipStride = uint32_t((span + granule - 1) / granule * granule);
+    }
+    const size_t bytes = size_t(nfft) * g.kPad * e * (fmt == kTcBf16x3 ? 2 : 1);
+    g.basisFloats = (bytes + 3) / 4;
+    return g;
+}
+
+void tc_build_basis(float* out, int fmt, int nfft, int W, int kPad, const float* win)
+{
+    const int off = (W < nfft) ? (nfft - W) / 2 : 0;
+    const size_t count = size_t(nfft) * kPad;
+    uint16_t* h16 = reinterpret_cast<uint16_t*>(out);
+    uint32_t* h32 = reinterpret_cast<uint32_t*>(out);
+    unsigned char* h8 = reinterpret_cast<unsigned char*>(out);
+    for (int n = 0; n < nfft; ++n)
+        for (int t = 0; t < kPad; ++t)
+        {
+            double v = 0.0;
+            if (t < W)
+            {
+                const long long tt = t + off;
+                double trig;
+                if (n == 0) trig = 1.0;
+                else if (n == 1) trig = (tt & 1) ? -1.0 : 1.0;   // Nyquist bin in the zero sine of bin 0
+                else
+                {
+                    const long long bin = n >> 1;
+                    const double ang = 2.0 * M_PI * double((bin * tt) % nfft) / double(nfft);
+                    trig = (n & 1) ? -std::sin(ang) : std::cos(ang);
+                }
+                v = double(win[t]) * trig;
+            }
+            const size_t i = size_t(n) * kPad + t;
+            if (fmt == kTcTf32) h32[i] = tf32_rna(float(v));
+            else if (fmt == kTcFp8)
+                h8[i] = static_cast<unsigned char>(
+                    __nv_cvt_float_to_fp8(float(v * kFp8BasisScale), __NV_SATFINITE, __NV_E4M3));
+            else
+            {
+                const uint16_t hi = bf16_rne(float(v));
+                h16[i] = hi;
+                if (fmt == kTcBf16x3) h16[count + i] = bf16_rne(float(v - double(bf16_value(hi))));
+            }
+        }
+}
+
+size_t tc_spectrogram_scratch_bytes(int n, int fmt, const TcGeometry& g, int maxFrames)
+{
+    Carver cv(nullptr);
+    cv.take<long long>(n + 1);
+    cv.take<int>(n);
+    const size_t operand = size_t(n) * g.clipStride * elem_bytes(fmt);
+    cv.take<char>(operand);
+    if (fmt == kTcBf16x3) cv.take<char>(operand);
+    if (fmt == kTcFp8) cv.take<float>(size_t(n) * std::max(maxFrames, 1));
+    return cv.used();
+}
+
+void launch_tc_spectrogram(Handle& h, void* scratch, const TcSpectrogramArgs& s)
+{
+    if (s.n <= 0) return;
+    const int e = elem_bytes(s.fmt);
+    Carver cv(scratch);
+    long long* prefix = cv.take<long long>(s.n + 1);
+    int* frames = cv.take<int>(s.n);
+    const size_t operand = size_t(s.n) * s.geo.clipStride * e;
+    unsigned char* aHi = cv.take<unsigned char>(operand);
+    unsigned char* aLo = s.fmt == kTcBf16x3 ? cv.take<unsigned char>(operand) : nullptr;
+    float* invScale = s.fmt == kTcFp8 ? cv.take<float>(size_t(s.n) * std::max(s.maxFrames, 1)) : nullptr;
+
+    tc_frames_kernel<<<(s.n + 255) / 256, 256, 0, h.stream()>>>(s.len, s.srcStride, s.n, s.windowLength,
+                                                                 s.windowStep, s.center, s.maxFrames, frames);
+    count_launch(1);
+    PrepArgs p{s.src, s.srcStride, s.srcElems, s.len, s.coeff, s.border, s.reflect,
+               s.center ? s.windowLength / 2 : 0, s.n};
+    if (s.fmt == kTcFp8)
+    {
+        dim3 pg(std::min((std::max(s.maxFrames, 1) + 7) / 8, 256), std::min(s.n, 65535));
+        tc_prep_fp8_kernel<<<pg, 256, 0, h.stream()>>>(p, frames, std::max(s.maxFrames, 1), s.windowLength,
+                                                       s.windowStep, s.geo.kPad,
+                                                       reinterpret_cast<__nv_fp8_e4m3*>(aHi), invScale);
+    }
+    else
+    {
+        dim3 pg(std::min<uint32_t>((s.geo.clipStride + 255) / 256, 64u), std::min(s.n, 65535));
+        if (s.fmt == kTcTf32) tc_prep_kernel<kTcTf32><<<pg, 256, 0, h.stream()>>>(p, aHi, nullptr, s.geo.clipStride);
+        else if (s.fmt == kTcBf16x3)
+            tc_prep_kernel<kTcBf16x3><<<pg, 256, 0, h.stream()>>>(p, aHi, aLo, s.geo.clipStride);
+        else tc_prep_kernel<kTcBf16><<<pg, 256, 0, h.stream()>>>(p, aHi, nullptr, s.geo.clipStride);
+    }
+    count_launch(1);
+    const int chunks = s.nfft / kTileN;
+    launch_ragged_prefix(TcCount{frames, chunks}, s.n, prefix, h.stream());
+
+    TcArgs a;
+    a.a = aHi;
+    a.aLo = aLo;
+    a.clipStride = s.geo.clipStride;
+    a.rowStep = s.geo.rowStep;
+    a.b = static_cast<const unsigned char*>(s.basis);
+    a.bLo = s.fmt == kTcBf16x3 ? a.b + size_t(s.nfft) * s.geo.kPad * 2 : nullptr;
+    a.kPad = s.geo.kPad;
+    a.nfft = s.nfft;
+    a.invScale = invScale;
+    a.maxFrames = std::max(s.maxFrames, 1);
+    a.dst = s.dst;
+    a.dstNStride = s.dstNStride;
+    a.dstHStride = s.dstHStride;
+    a.nft = s.nft;
+    a.power = s.power;
+    a.frames = frames;
+    a.n = s.n;
+    a.errorWord = h.device_flags();
+    switch (s.fmt)
+    {
+    case kTcBf16: launch_format<kTcBf16>(h, a, prefix); break;
+    case kTcBf16x3: launch_format<kTcBf16x3>(h, a, prefix); break;
+    case kTcTf32: launch_format<kTcTf32>(h, a, prefix); break;
+    default: launch_format<kTcFp8>(h, a, prefix); break;
+    }
+}
+
+}  // namespace rppb

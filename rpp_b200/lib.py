@@ -18,6 +18,7 @@ EXPORTED = (
     "rppt_down_mixing_gpu", "rppt_spectrogram_gpu", "rppt_mel_filter_bank_gpu", "rppt_resample_gpu",
     "rppbGetLastError", "rppbGetLaunchCount", "rppb_frontend_gpu", "rppb_get_device_error",
     "rppb_downmix_resample_gpu", "rppt_to_decibels_gpu_static", "rppb_frontend_clips_gpu",
+    "rppb_spectrogram_tc_gpu",
 )
 
 _lib = None
@@ -66,6 +67,8 @@ def load(path=None):
     L.rppb_downmix_resample_gpu.restype = _I
     L.rppb_frontend_clips_gpu.argtypes = [_V, _I, _F, _V, _I, _F, _F, _I, _F, ctypes.POINTER(RppbFrontendParams), _V]
     L.rppb_frontend_clips_gpu.restype = _I
+    L.rppb_spectrogram_tc_gpu.argtypes = [_V, _D, _V, _D, _V, _V, _I, _B, _B, _I, _I, _I, _I, _I, _V]
+    L.rppb_spectrogram_tc_gpu.restype = _I
     L.rppt_to_decibels_gpu_static.argtypes = [_V, _D, _V, _D, _V, _F, _F, _F, _V]
     L.rppt_to_decibels_gpu_static.restype = _I
     L.rppb_get_device_error.argtypes = [_V, ctypes.POINTER(ctypes.c_int32)]

@@ -4,13 +4,13 @@ configurations (no datasets are available offline).  NumPy PCG64, seed 20261203 
   cfg0  8 mono clips, 16 kHz, lengths U[16000, 60000]
   cfg1  256 mono clips, 16 kHz, lengths U[16000, 256000] (1-16 s), plus 0-3 silent spans of
         0.1-1 s per clip
-  cfg2  1024 mono clips of 160000 samples; an extra white-noise floor sits 40/60/80/100/120 dB
-        below the clip's peak (equal shares), sweeping the dynamic range
+  cfg2  1024 mono clips of 160000 samples; the white noise sits 40/60/80/100/120 dB below the
+        tones' peak (clip i: 40 + 20 * (i % 5) dB) instead of at sigma 0.1, sweeping the dynamic range
   cfg3  2048 stereo clips, durations log-normal (median 4 s, sigma 0.25) clipped to 0.5-30 s, input
         rate uniform over {16000, 22050, 44100, 48000}; both channels share the sines and have
         independent noise
 
-Signal model (every config): Gaussian noise sigma 0.1 plus 3 sinusoids with frequency U[100, 6000]
+Signal model (cfg0, cfg1, cfg3): Gaussian noise sigma 0.1 plus 3 sinusoids with frequency U[100, 6000]
 Hz and amplitude U[0.05, 0.5].
 """
 import numpy as np
@@ -36,8 +36,12 @@ def mono_batch(n, lengths, rng, rate=16000, gaps=False, floor_db=None):
     out = np.zeros((n, L), np.float32)
     for i in range(n):
         li = int(lengths[i])
-        x = _tones(rng, li, rate) + rng.normal(0.0, 0.1, li)
-        if floor_db is not None:
+        x = _tones(rng, li, rate)
+        if floor_db is None:
+            x += rng.normal(0.0, 0.1, li)
+        else:
+            # the white noise sits floor_db below the tones' peak (a fixed sigma of 0.1 would pin the
+            # dynamic range near 20 dB and leave nothing to sweep)
             peak = np.abs(x).max() if li else 1.0
             x += rng.normal(0.0, peak * 10.0 ** (-floor_db[i] / 20.0), li)
         if gaps:
