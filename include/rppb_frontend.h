@@ -96,6 +96,19 @@ SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips, Rpp32s nu
                                                 Rpp32s lobes, Rpp32f preemphCoeff, const RppbFrontendParams* params,
                                                 rppHandle_t rppHandle);
 
+/* The fused front end on HOST tensors: srcHost, dstHost, srcLengthHost and coeffHost are host memory
+ * (pinned for overlap; pageable works but serializes the copies), laid out as for rppb_frontend_gpu.
+ * The batch is split into numChunks contiguous runs of clips with about equal sample counts (<= 0:
+ * 8); chunk c's valid samples are copied in on one stream while chunk c-1 is computed and chunk c-2's
+ * valid output rows (numFilter x frames per clip) are copied out on another, through double-buffered
+ * device staging in the handle workspace.  Output equals rppb_frontend_gpu on the same data and
+ * only the valid region of dstHost is written.  Asynchronous: synchronize the handle stream before
+ * reading dstHost.  Extension (no counterpart in the reference). */
+SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost, RpptDescPtr srcDescPtr, Rpp32f* dstHost,
+                                               RpptDescPtr dstDescPtr, const Rpp32s* srcLengthHost,
+                                               const Rpp32f* coeffHost, const RppbFrontendParams* params,
+                                               Rpp32s numChunks, rppHandle_t rppHandle);
+
 /* Operand precision of the tensor-core spectrogram; every variant accumulates in FP32. */
 typedef enum
 {

@@ -120,6 +120,15 @@ def frontend(src, src_desc, dst, dst_desc, src_length, coeff, params, handle):
                                        _addr(src_length), _addr(coeff), ctypes.byref(params), _h(handle)))
 
 
+def frontend_host(src, src_desc, dst, dst_desc, src_length, coeff, params, num_chunks, handle):
+    """rppb_frontend_host_gpu: the fused chain on host tensors (pinned for overlap), chunked so that
+    copies in, kernels and copies out overlap.  Asynchronous on the handle stream."""
+    L = _lib.load()
+    return _status(L.rppb_frontend_host_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                            _addr(src_length), _addr(coeff), ctypes.byref(params), int(num_chunks),
+                                            _h(handle)))
+
+
 def device_error(handle):
     """Reads and clears the handle's device error word (synchronizes the handle stream)."""
     L = _lib.load()

@@ -452,6 +452,7 @@ RppStatus frontend_params(Handle& h, const RppbFrontendParams* params, float* wi
     a.multiplier = p.multiplier * log10Factor;
     a.refMag = p.referenceMagnitude;
     a.lookahead = p.lookahead > 0 ? p.lookahead : 32;
+    a.reserveSms = 0;
     a.clips = nullptr;
     a.outRate = 0.f;
     a.coeffAll = 0.f;
@@ -503,6 +504,169 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPt
         a.coeff = static_cast<const float*>(h.device_view(coeffTensor, n * sizeof(float), coeffStage));
         a.maxFrames = int(dstDescPtr->w);
         launch_frontend(h, scratch, a);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost, RpptDescPtr srcDescPtr,
+                                                          Rpp32f* dstHost, RpptDescPtr dstDescPtr,
+                                                          const Rpp32s* srcLengthHost, const Rpp32f* coeffHost,
+                                                          const RppbFrontendParams* params, Rpp32s numChunks,
+                                                          rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr && params, "null descriptor or parameters");
+        if (srcDescPtr->numDims != 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (dstDescPtr->numDims != 3) return RPP_ERROR_INVALID_DST_DIMS;
+        if (dstDescPtr->layout != NFT) return RPP_ERROR_INVALID_DST_LAYOUT;
+        if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcHost && dstHost && srcLengthHost && coeffHost, "null tensor");
+        if (dstDescPtr->h < Rpp32u(params->numFilter) || dstDescPtr->strides.hStride < dstDescPtr->w)
+            return RPP_ERROR_INVALID_DST_DIMS;
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        FrontendArgs a;
+        const int W = params->windowLength > 0 ? params->windowLength : 0;
+        const size_t nStride = srcDescPtr->strides.nStride;
+        const int maxFrames = int(dstDescPtr->w);
+        const int nf = params->numFilter;
+
+        // per-clip lengths and frame counts on the host (the call's tensors are host memory)
+        std::vector<int> L(n), F(n);
+        size_t total = 0;
+        for (int b = 0; b < n; ++b)
+        {
+            L[b] = std::max(0, std::min(srcLengthHost[b], int(nStride)));
+            const int len = params->centerWindows ? L[b] : L[b] - W;
+            F[b] = std::min(std::max(params->windowStep > 0 ? len / params->windowStep + 1 : 0, 0), maxFrames);
+            total += size_t(L[b]);
+        }
+        // contiguous chunks of clips with about equal sample counts
+        const int chunks = std::max(1, std::min(n, numChunks > 0 ? numChunks : 8));
+        std::vector<int> bound{0};
+        size_t acc = 0;
+        for (int b = 0; b < n; ++b)
+        {
+            acc += size_t(L[b]);
+            const int c = int(bound.size());
+            if (c < chunks && b + 1 < n && acc * chunks >= total * size_t(c)) bound.push_back(b + 1);
+        }
+        bound.push_back(n);
+        const int nc = int(bound.size()) - 1;
+        std::vector<uint32_t> strideC(nc);
+        std::vector<int> framesC(nc);
+        size_t inElems = 0, outElems = 0;
+        int maxClips = 0;
+        for (int c = 0; c < nc; ++c)
+        {
+            int ml = 2, mf = 1;
+            for (int b = bound[c]; b < bound[c + 1]; ++b)
+            {
+                ml = std::max(ml, L[b]);
+                mf = std::max(mf, F[b]);
+            }
+            strideC[c] = uint32_t((ml + 3) & ~3);
+            framesC[c] = mf;
+            const int clips = bound[c + 1] - bound[c];
+            maxClips = std::max(maxClips, clips);
+            inElems = std::max(inElems, size_t(clips) * strideC[c]);
+            outElems = std::max(outElems, size_t(clips) * nf * size_t(mf));
+        }
+        const int lookahead = params->lookahead > 0 ? params->lookahead : 32;
+        const size_t scratchBytes = frontend_scratch_bytes(maxClips, lookahead);
+        Carver m(nullptr);
+        m.take<int>(2 * n);
+        m.take<float>(n);
+        m.take<float>(params->windowFunction ? W : 0);
+        m.take<char>(scratchBytes);
+        for (int i = 0; i < 2; ++i) m.take<float>(inElems);
+        for (int i = 0; i < 2; ++i) m.take<float>(outElems);
+        Carver cv(h.workspace(m.used()));
+        int* lenDev = cv.take<int>(2 * n);   // lengths, then frame counts
+        int* framesDev = lenDev + n;
+        float* coeffDev = cv.take<float>(n);
+        float* winStage = cv.take<float>(params->windowFunction ? W : 0);
+        void* scratch = cv.take<char>(scratchBytes);
+        float* in[2] = {cv.take<float>(inElems), cv.take<float>(inElems)};
+        float* out[2] = {cv.take<float>(outElems), cv.take<float>(outElems)};
+        RppStatus st = frontend_params(h, params, winStage, a);
+        if (st != RPP_SUCCESS) return st;
+        std::vector<int> LF(2 * n);
+        std::copy(L.begin(), L.end(), LF.begin());
+        std::copy(F.begin(), F.end(), LF.begin() + n);
+        h.upload(lenDev, LF.data(), 2 * n * sizeof(int));
+        h.upload(coeffDev, coeffHost, n * sizeof(float));
+
+        // pinned (mapped) host tensors are moved by kernels; pageable ones by one DMA copy per clip
+        void* srcMapped = nullptr;
+        void* dstMapped = nullptr;
+        const bool gatherK = h.device_writable(srcHost, &srcMapped);
+        const bool scatterK = h.device_writable(dstHost, &dstMapped);
+        constexpr int kMoverCtas = 32;
+        constexpr int kReservedSms = 12;
+        if (gatherK || scatterK) a.reserveSms = kReservedSms;   // room for the movers next to the persistent kernel
+
+        cudaStream_t main = h.stream(), up = h.aux_stream(0), down = h.aux_stream(1);
+        cudaEvent_t start = h.event(0);
+        auto evUp = [&](int c) { return h.event(1 + 3 * c); };
+        auto evComp = [&](int c) { return h.event(2 + 3 * c); };
+        auto evDown = [&](int c) { return h.event(3 + 3 * c); };
+        check_cuda(cudaEventRecord(start, main), "cudaEventRecord");
+        check_cuda(cudaStreamWaitEvent(up, start, 0), "cudaStreamWaitEvent");
+        check_cuda(cudaStreamWaitEvent(down, start, 0), "cudaStreamWaitEvent");
+        for (int c = 0; c < nc; ++c)
+        {
+            const int c0 = bound[c], clips = bound[c + 1] - c0, buf = c & 1;
+            // inputs: the valid samples of each clip (at least 2, which the REFLECT border reads)
+            if (c >= 2) check_cuda(cudaStreamWaitEvent(up, evComp(c - 2), 0), "cudaStreamWaitEvent");
+            if (gatherK)
+                launch_host_gather(up, static_cast<const float*>(srcMapped) + size_t(c0) * nStride, nStride,
+                                   lenDev + c0, clips, in[buf], strideC[c], kMoverCtas);
+            else
+                for (int b = c0; b < c0 + clips; ++b)
+                {
+                    const size_t cnt = std::min(nStride, size_t(std::max(L[b], 2)));
+                    check_cuda(cudaMemcpyAsync(in[buf] + size_t(b - c0) * strideC[c], srcHost + size_t(b) * nStride,
+                                               cnt * sizeof(float), cudaMemcpyHostToDevice, up),
+                               "cudaMemcpyAsync(H2D clip)");
+                }
+            check_cuda(cudaEventRecord(evUp(c), up), "cudaEventRecord");
+            // compute
+            check_cuda(cudaStreamWaitEvent(main, evUp(c), 0), "cudaStreamWaitEvent");
+            if (c >= 2) check_cuda(cudaStreamWaitEvent(main, evDown(c - 2), 0), "cudaStreamWaitEvent");
+            a.src = in[buf];
+            a.srcStride = strideC[c];
+            a.srcElems = size_t(clips) * strideC[c];
+            a.dst = out[buf];
+            a.dstNStride = uint32_t(size_t(nf) * framesC[c]);
+            a.dstHStride = uint32_t(framesC[c]);
+            a.n = clips;
+            a.len = lenDev + c0;
+            a.coeff = coeffDev + c0;
+            a.maxFrames = framesC[c];
+            launch_frontend(h, scratch, a);
+            check_cuda(cudaEventRecord(evComp(c), main), "cudaEventRecord");
+            // outputs: numFilter rows of F frames per clip
+            check_cuda(cudaStreamWaitEvent(down, evComp(c), 0), "cudaStreamWaitEvent");
+            if (scatterK)
+                launch_host_scatter(down, out[buf], a.dstNStride, a.dstHStride, framesDev + c0, clips, nf,
+                                    static_cast<float*>(dstMapped) + size_t(c0) * dstDescPtr->strides.nStride,
+                                    dstDescPtr->strides.nStride, dstDescPtr->strides.hStride, kMoverCtas);
+            else
+                for (int b = c0; b < c0 + clips; ++b)
+                {
+                    if (F[b] <= 0) continue;
+                    check_cuda(cudaMemcpy2DAsync(dstHost + size_t(b) * dstDescPtr->strides.nStride,
+                                                 size_t(dstDescPtr->strides.hStride) * sizeof(float),
+                                                 out[buf] + size_t(b - c0) * a.dstNStride,
+                                                 size_t(framesC[c]) * sizeof(float), size_t(F[b]) * sizeof(float),
+                                                 size_t(nf), cudaMemcpyDeviceToHost, down),
+                               "cudaMemcpy2DAsync(D2H clip)");
+                }
+            check_cuda(cudaEventRecord(evDown(c), down), "cudaEventRecord");
+        }
+        check_cuda(cudaStreamWaitEvent(main, evDown(nc - 1), 0), "cudaStreamWaitEvent");
+        check_cuda(cudaStreamWaitEvent(main, evUp(nc - 1), 0), "cudaStreamWaitEvent");
         return RPP_SUCCESS;
     });
 }

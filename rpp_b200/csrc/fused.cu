@@ -21,6 +21,8 @@
 // 8 L + 4 L + 2*4*bins*frames + ... for the four separate calls.
 #include <cfloat>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "mel_tables.cuh"
 #include "ops.hpp"
@@ -304,7 +306,9 @@ void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
     const FusedLayout<NFFT> lay(a.mel.numFilter, a.W, a.hop);
     if (lay.total > 227 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
     const float2* tw = spectrogram_twiddles(h, NFFT);
-    const int grid = persistent_grid(h, reinterpret_cast<const void*>(frontend_kernel<NFFT>), kFusedThreads, lay.total);
+    int grid = persistent_grid(h, reinterpret_cast<const void*>(frontend_kernel<NFFT>), kFusedThreads, lay.total);
+    if (a.reserveSms > 0 && a.reserveSms < h.num_sms())
+        grid = std::max(1, grid / h.num_sms() * (h.num_sms() - a.reserveSms));
     frontend_kernel<NFFT><<<grid, kFusedThreads, lay.total, h.stream()>>>(a, tw, prefix, counter, done, maxKey,
                                                                           h.device_flags());
     count_launch();

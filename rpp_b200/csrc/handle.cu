@@ -28,6 +28,13 @@ Handle::Handle(size_t batchSize, cudaStream_t stream) : stream_(stream), batch_(
 Handle::~Handle()
 {
     cudaStreamSynchronize(stream_);
+    for (cudaStream_t s : aux_)
+        if (s)
+        {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
     if (ws_) dev_free(ws_);
     for (auto& kv : tables_) cudaFree(kv.second);
     if (flags_) cudaFree(flags_);
@@ -77,6 +84,23 @@ void* Handle::workspace(size_t bytes)
     ws_ = dev_alloc(grown);
     ws_bytes_ = grown;
     return ws_;
+}
+
+cudaStream_t Handle::aux_stream(int i)
+{
+    if (!aux_[i]) check_cuda(cudaStreamCreateWithFlags(&aux_[i], cudaStreamNonBlocking), "cudaStreamCreate(aux)");
+    return aux_[i];
+}
+
+cudaEvent_t Handle::event(int i)
+{
+    while (int(events_.size()) <= i)
+    {
+        cudaEvent_t e;
+        check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate(pool)");
+        events_.push_back(e);
+    }
+    return events_[i];
 }
 
 void* Handle::staging(size_t bytes)

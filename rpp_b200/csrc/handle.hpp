@@ -90,6 +90,13 @@ class Handle
     // A small zeroed device word array that kernels set on bounded-wait timeouts.
     int* device_flags();
 
+    // Extra streams of this handle (created on first use, non-blocking), for copies that overlap
+    // the kernels on stream(); every call that uses them joins them back into stream() before it
+    // returns, so stream order on stream() still covers all of the handle's work.
+    cudaStream_t aux_stream(int i);
+    // Event i of the handle's pool (timing disabled), created on first use.
+    cudaEvent_t event(int i);
+
     // Scratch of size `bytes` in pinned host memory, reused after the previous user's copy ended.
     void* staging(size_t bytes);
     void staging_done();
@@ -110,6 +117,9 @@ class Handle
     size_t pinned_bytes_ = 0;
     cudaEvent_t pinned_free_ = nullptr;
     bool pinned_pending_ = false;
+
+    cudaStream_t aux_[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> events_;
 
     std::map<std::string, void*> tables_;
     int* flags_ = nullptr;

@@ -1,0 +1,116 @@
+// PCIe movers of the host-tensor front end (rppb_frontend_host_gpu): kernels that read pinned host
+// memory (mapped into the device address space) and write it, so that one launch moves a whole chunk
+// of ragged clips.  One DMA copy per clip costs a few microseconds of setup each; a kernel keeps
+// thousands of 16-byte PCIe requests in flight and moves only the valid part of every clip.
+//
+// Both kernels run on their own streams next to the persistent front-end kernel, which leaves them
+// a few SMs (FrontendArgs::reserveSms).
+#include "common.cuh"
+#include "ops.hpp"
+
+namespace rppb {
+namespace {
+
+constexpr int kMoverThreads = 256;
+constexpr int kSegment = 8192;   // floats per (clip, segment) work unit of the gather
+
+// dst[b][0 .. cnt_b) = src[(c0 + b) * nStride ..], cnt_b = min(nStride, max(len_b, 2), dstStride):
+// the valid samples of each clip plus the second sample, which the REFLECT pre-emphasis border reads.
+__global__ void __launch_bounds__(kMoverThreads) host_gather_kernel(const float* __restrict__ src, size_t nStride,
+                                                                    const int* __restrict__ len, int clips,
+                                                                    float* __restrict__ dst, uint32_t dstStride,
+                                                                    int segsPerClip)
+{
+    const long long units = (long long)clips * segsPerClip;
+    for (long long u = blockIdx.x; u < units; u += gridDim.x)
+    {
+        const int b = int(u / segsPerClip), seg = int(u % segsPerClip);
+        const long long cnt = min(min((long long)nStride, (long long)max(len[b], 2)), (long long)dstStride);
+        const long long s0 = (long long)seg * kSegment;
+        if (s0 >= cnt) continue;
+        const int m = int(min((long long)kSegment, cnt - s0));
+        const float* s = src + size_t(b) * nStride + s0;
+        float* d = dst + size_t(b) * dstStride + s0;
+        if (((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(d)) & 15) == 0)
+        {
+            const int q = m >> 2;
+            const float4* s4 = reinterpret_cast<const float4*>(s);
+            float4* d4 = reinterpret_cast<float4*>(d);
+            // 8 loads in flight per thread before the stores
+            constexpr int kUnroll = kSegment / 4 / kMoverThreads;
+            float4 v[kUnroll];
+#pragma unroll
+            for (int k = 0; k < kUnroll; ++k)
+            {
+                const int i = threadIdx.x + k * kMoverThreads;
+                if (i < q) v[k] = s4[i];
+            }
+#pragma unroll
+            for (int k = 0; k < kUnroll; ++k)
+            {
+                const int i = threadIdx.x + k * kMoverThreads;
+                if (i < q) d4[i] = v[k];
+            }
+            for (int i = (q << 2) + threadIdx.x; i < m; i += kMoverThreads) d[i] = s[i];
+        }
+        else
+        {
+            for (int i = threadIdx.x; i < m; i += kMoverThreads) d[i] = s[i];
+        }
+    }
+}
+
+// dst[(c0 + b) * dstNStride + r * dstHStride + f] = src[b * srcNStride + r * srcHStride + f] for
+// rows r < rows and frames f < frames_b: one warp per row, coalesced 128-byte writes.
+__global__ void __launch_bounds__(kMoverThreads) host_scatter_kernel(const float* __restrict__ src, uint32_t srcNStride,
+                                                                     uint32_t srcHStride,
+                                                                     const int* __restrict__ frames, int clips,
+                                                                     int rows, float* __restrict__ dst,
+                                                                     size_t dstNStride, size_t dstHStride)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (kMoverThreads / 32);
+    const long long total = (long long)clips * rows;
+    for (long long w = blockIdx.x * (long long)(kMoverThreads / 32) + (threadIdx.x >> 5); w < total; w += warps)
+    {
+        const int b = int(w / rows), r = int(w % rows);
+        const int F = frames[b];
+        const float* s = src + size_t(b) * srcNStride + size_t(r) * srcHStride;
+        float* d = dst + size_t(b) * dstNStride + size_t(r) * dstHStride;
+        int f = lane;
+        for (; f + 96 < F; f += 128)
+        {
+            const float v0 = s[f], v1 = s[f + 32], v2 = s[f + 64], v3 = s[f + 96];
+            d[f] = v0;
+            d[f + 32] = v1;
+            d[f + 64] = v2;
+            d[f + 96] = v3;
+        }
+        for (; f < F; f += 32) d[f] = s[f];
+    }
+}
+
+}  // namespace
+
+void launch_host_gather(cudaStream_t stream, const float* src, size_t nStride, const int* len, int clips, float* dst,
+                        uint32_t dstStride, int ctas)
+{
+    if (clips <= 0) return;
+    const int segs = int((size_t(dstStride) + kSegment - 1) / kSegment);
+    host_gather_kernel<<<ctas, kMoverThreads, 0, stream>>>(src, nStride, len, clips, dst, dstStride, std::max(segs, 1));
+    count_launch(1);
+    check_cuda(cudaGetLastError(), "host_gather_kernel");
+}
+
+void launch_host_scatter(cudaStream_t stream, const float* src, uint32_t srcNStride, uint32_t srcHStride,
+                         const int* frames, int clips, int rows, float* dst, size_t dstNStride, size_t dstHStride,
+                         int ctas)
+{
+    if (clips <= 0 || rows <= 0) return;
+    host_scatter_kernel<<<ctas, kMoverThreads, 0, stream>>>(src, srcNStride, srcHStride, frames, clips, rows, dst,
+                                                            dstNStride, dstHStride);
+    count_launch(1);
+    check_cuda(cudaGetLastError(), "host_scatter_kernel");
+}
+
+}  // namespace rppb

@@ -133,9 +133,17 @@ struct FrontendArgs
     const RppbClip* clips;
     float outRate;
     float coeffAll;
+    int reserveSms;          // SMs' worth of CTA slots left to kernels on other streams
 };
 size_t frontend_scratch_bytes(int n, int lookahead);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);
+
+// PCIe movers over mapped pinned host memory (host_io.cu).
+void launch_host_gather(cudaStream_t stream, const float* src, size_t nStride, const int* len, int clips, float* dst,
+                        uint32_t dstStride, int ctas);
+void launch_host_scatter(cudaStream_t stream, const float* src, uint32_t srcNStride, uint32_t srcHStride,
+                         const int* frames, int clips, int rows, float* dst, size_t dstNStride, size_t dstHStride,
+                         int ctas);
 
 // Tensor-core spectrogram (tc_dft.cu).
 enum TcFormat

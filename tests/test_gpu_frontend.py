@@ -126,3 +126,31 @@ def test_frontend_graph_capture(gpu):
         np.testing.assert_array_equal(host(out), first)
     finally:
         gpu.set_stream(torch.cuda.current_stream().cuda_stream)
+
+
+@pytest.mark.parametrize("chunks,pinned_io", [(0, True), (1, True), (3, True), (50, True), (4, False)])
+def test_frontend_host_equals_device(gpu, chunks, pinned_io):
+    """rppb_frontend_host_gpu (host tensors, chunked copy/compute overlap) writes exactly what
+    rppb_frontend_gpu writes on the same data, and nothing outside the valid region."""
+    r = np.random.Generator(np.random.PCG64(5))
+    lens = r.integers(0, 40000, 13).astype(np.int32)
+    lens[0], lens[1], lens[2], lens[3] = 40000, 0, 1, 2
+    x, lens = synth.mono_batch(len(lens), lens, r, gaps=True)
+    n, L = x.shape
+    coeff = r.uniform(0.9, 0.99, n).astype(np.float32)
+    p = frontend_params(border=2)
+    mf = 40000 // p.windowStep + 1
+    sd, dd = audio_desc(n, L), spectra_desc(n, p.numFilter, mf)
+    ref = canvas((n, p.numFilter, mf))
+    assert audio.frontend(dev(x), sd, ref, dd, dev(lens), dev(coeff), p, gpu) == OK
+    exp = host(ref)
+    if pinned_io:
+        xs, out = torch.from_numpy(x).pin_memory(), torch.full((n, p.numFilter, mf), -12345.0).pin_memory()
+        ls, cs = torch.from_numpy(lens).pin_memory(), torch.from_numpy(coeff).pin_memory()
+    else:
+        xs, out, ls, cs = x, np.full((n, p.numFilter, mf), -12345.0, np.float32), lens, coeff
+    assert audio.frontend_host(xs, sd, out, dd, ls, cs, p, chunks, gpu) == OK
+    torch.cuda.synchronize()
+    got = out.numpy() if hasattr(out, "numpy") else out
+    np.testing.assert_array_equal(got, exp)
+    assert audio.device_error(gpu) == 0
