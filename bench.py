@@ -332,9 +332,11 @@ def serving_measurement(torch, n_requests):
         thr, lat = serving.measure(torch, server, pool, rng, n_requests, rate_per_s=rate)
         loads.append({"offered": frac, "requests_per_s": rate, "clip_s_per_s": thr,
                       "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
+    server.close()
     return {"capacity_clip_s_per_s": cap, "mean_request_clip_s": float(mean_cs), "requests_per_point": n_requests,
             "budget_gb": 40, "chain": "resample (Kaiser sinc, 16 zero crossings) -> pre-emphasis -> STFT(512, 400, "
-            "160) -> mel(128) -> dB, one captured graph per step over a device clip table",
+            "160) -> mel(128) -> dB, one captured graph per step over a device clip table; native scheduler thread "
+            "(include/rppb_server.h)",
             "latency": "host clock from arrival to output copy complete", "loads": loads}
 
 

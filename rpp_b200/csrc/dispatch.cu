@@ -72,6 +72,10 @@ void build_hann(float* out, size_t count, const void*)
 
 }  // namespace
 
+namespace rppb {
+void record_error(const std::string& what) { g_last_error = what; }
+}  // namespace rppb
+
 extern "C" SHARED_PUBLIC const char* rppbGetLastError() { return g_last_error.c_str(); }
 
 extern "C" SHARED_PUBLIC RppStatus rppt_pre_emphasis_filter_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,

@@ -28,6 +28,8 @@ struct Error
 };
 
 [[noreturn]] void fail(RppStatus status, const std::string& what);
+// Sets the calling thread's message returned by rppbGetLastError.
+void record_error(const std::string& what);
 void check_cuda(cudaError_t err, const char* what);
 
 // Bump allocator over one workspace block: measure with base == nullptr, then carve.

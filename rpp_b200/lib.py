@@ -6,7 +6,8 @@ Loading fails loudly when the library is missing: there is no CPU fallback.  Bui
 import ctypes
 import os
 
-from .types import RpptDesc, RpptImagePatch, RpptResamplingWindow, RppBackend, RppbFrontendParams
+from .types import (RpptDesc, RpptImagePatch, RpptResamplingWindow, RppBackend, RppbFrontendParams, RppbServerConfig,
+                    RppbCompletion)
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "librppb.so")
 
@@ -20,6 +21,8 @@ EXPORTED = (
     "rppb_downmix_resample_gpu", "rppt_to_decibels_gpu_static", "rppb_frontend_clips_gpu",
     "rppb_spectrogram_tc_gpu",
     "rppb_frontend_host_gpu",
+    "rppb_server_create", "rppb_server_destroy", "rppb_server_frames", "rppb_server_submit", "rppb_server_poll",
+    "rppb_server_arena_used",
 )
 
 _lib = None
@@ -74,6 +77,18 @@ def load(path=None):
     L.rppb_spectrogram_tc_gpu.restype = _I
     L.rppt_to_decibels_gpu_static.argtypes = [_V, _D, _V, _D, _V, _F, _F, _F, _V]
     L.rppt_to_decibels_gpu_static.restype = _I
+    L.rppb_server_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(RppbServerConfig)]
+    L.rppb_server_create.restype = _I
+    L.rppb_server_destroy.argtypes = [_V]
+    L.rppb_server_destroy.restype = _I
+    L.rppb_server_frames.argtypes = [_V, ctypes.c_int32, _F]
+    L.rppb_server_frames.restype = ctypes.c_int32
+    L.rppb_server_submit.argtypes = [_V, _V, _V, _V, _V, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]
+    L.rppb_server_submit.restype = _I
+    L.rppb_server_poll.argtypes = [_V, ctypes.POINTER(RppbCompletion), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    L.rppb_server_poll.restype = _I
+    L.rppb_server_arena_used.argtypes = [_V]
+    L.rppb_server_arena_used.restype = ctypes.c_uint64
     L.rppb_get_device_error.argtypes = [_V, ctypes.POINTER(ctypes.c_int32)]
     L.rppb_get_device_error.restype = _I
     L.rppbGetLaunchCount.argtypes = []

@@ -189,3 +189,16 @@ def frontend_params(nfft=512, window_length=400, window_step=160, num_filter=128
     p.cutOffDB, p.multiplier, p.referenceMagnitude = float(cut_off_db), float(multiplier), float(reference_magnitude)
     p.lookahead = int(lookahead)
     return p
+
+
+class RppbServerConfig(ctypes.Structure):
+    """include/rppb_server.h: configuration of the continuous-batching server."""
+    _fields_ = [("budgetBytes", ctypes.c_uint64), ("maxClipsPerStep", ctypes.c_int32), ("tables", ctypes.c_int32),
+                ("outRate", ctypes.c_float), ("lookup", ctypes.c_void_p), ("lookupSize", ctypes.c_int32),
+                ("scale", ctypes.c_float), ("center", ctypes.c_float), ("lobes", ctypes.c_int32),
+                ("preemphCoeff", ctypes.c_float), ("params", RppbFrontendParams)]
+
+
+class RppbCompletion(ctypes.Structure):
+    """include/rppb_server.h: one finished request (steady-clock nanoseconds)."""
+    _fields_ = [("id", ctypes.c_uint64), ("submitNs", ctypes.c_int64), ("finishNs", ctypes.c_int64)]

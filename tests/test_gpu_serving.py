@@ -1,6 +1,7 @@
-"""The continuous-batching server (rpp_b200/serving.py): each request's result is the same alone and
-in a mix of concurrently admitted requests, and equals the descriptor-based calls
-(rppb_downmix_resample_gpu + rppb_frontend_gpu) on the same clip."""
+"""The continuous-batching server (native scheduler of include/rppb_server.h, driven through
+rpp_b200/serving.py): each request's result is the same alone and in a mix of concurrently admitted
+requests, under memory pressure, and equals the descriptor-based calls (rppb_downmix_resample_gpu +
+rppb_frontend_gpu) on the same clip."""
 import numpy as np
 import pytest
 import torch
@@ -35,7 +36,8 @@ def test_alone_equals_mixed():
     assert len(mixed) == len(mix)
     for a, b in zip(alone, mixed[probe.rid]):
         assert torch.equal(a, b)
-    assert server.arena.used == 0
+    assert server.arena_used() == 0
+    server.close()
 
 
 def test_server_equals_descriptor_calls(gpu):
@@ -61,3 +63,26 @@ def test_server_equals_descriptor_calls(gpu):
                                   torch.tensor([0.97], device="cuda"), p, gpu) == RppStatus.RPP_SUCCESS
             torch.cuda.synchronize()
             assert torch.equal(dst[0].cpu(), got)
+    server.close()
+
+
+def test_budget_pressure_and_oversize():
+    """A budget that holds only a few requests at a time: FIFO admission waits for memory, every
+    request completes with the same bits as on a large budget, the arena drains; a request that can
+    never fit is refused at submission."""
+    reqs = requests(23, 40)
+    big = serving.FrontendServer(torch, budget_bytes=1 << 30, max_clips=64, tables=3)
+    ref = run(big, reqs)
+    big.close()
+    small = serving.FrontendServer(torch, budget_bytes=24 << 20, max_clips=64, tables=3)
+    got = run(small, reqs)
+    assert len(got) == len(reqs)
+    for r in reqs:
+        for a, b in zip(ref[r.rid], got[r.rid]):
+            assert torch.equal(a, b)
+    assert small.arena_used() == 0
+    huge = serving.Request(rid=999, clips=[torch.zeros(8 << 20).pin_memory()], rates=[16000.0], arrival=0.0)
+    serving.attach_outputs(torch, small, huge)
+    with pytest.raises(RuntimeError):
+        small.submit(huge)
+    small.close()
