@@ -71,8 +71,25 @@ struct Tw
     static constexpr float s = float(cos_2pi(4 * K - R, 4 * R));   // sin(t) = cos(t - pi/2)
 };
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Paired FP32 arithmetic (sm_100 add/sub/mul.rn.f32x2): one instruction for both components,
+// each rounded exactly as the scalar operation would be.
+#define RPPB_F32X2(NAME, OP)                                                                               \
+    __device__ __forceinline__ float2 NAME(float2 a, float2 b)                                             \
+    {                                                                                                      \
+        float2 r;                                                                                          \
+        asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t" OP \
+            " pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"                                               \
+            : "=f"(r.x), "=f"(r.y)                                                                         \
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                                     \
+        return r;                                                                                          \
+    }
+RPPB_F32X2(add2, "add.rn.f32x2")
+RPPB_F32X2(sub2, "sub.rn.f32x2")
+RPPB_F32X2(mul2, "mul.rn.f32x2")
+#undef RPPB_F32X2
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return add2(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return sub2(a, b); }
 // a * (c - i s)
 __device__ __forceinline__ float2 cmul_conj(float2 a, float c, float s)
 {

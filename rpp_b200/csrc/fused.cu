@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     float2* s_fft = reinterpret_cast<float2*>(smem + lay.work);
     float* s_out = reinterpret_cast<float*>(smem + lay.work + S::fft_bytes);
     int* csrRow = reinterpret_cast<int*>(smem + lay.csrRow);
-    unsigned short* csrBin = reinterpret_cast<unsigned short*>(smem + lay.csrBin);
+    unsigned short* csrBin = reinterpret_cast<unsigned short*>(smem + lay.csrBin);   // bin * LD: tile row offset
     float* csrW = reinterpret_cast<float*>(smem + lay.csrW);
     __shared__ long long s_item;
     __shared__ float s_warpMax[kFusedThreads / 32];
@@ -167,13 +167,13 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
             for (int k = v.first[m]; k < v.last[m]; ++k, ++e)
             {
                 float w = __fsub_rn(1.0f, v.weightsDown[k]);
-                csrBin[e] = (unsigned short)k;
+                csrBin[e] = (unsigned short)(k * LD);
                 csrW[e] = a.mel.normalize ? __fmul_rn(w, nm) : w;
             }
             for (int k = v.first[m + 1]; k < v.last[m + 1]; ++k, ++e)
             {
                 const float w = v.weightsDown[k];
-                csrBin[e] = (unsigned short)k;
+                csrBin[e] = (unsigned short)(k * LD);
                 csrW[e] = a.mel.normalize ? __fmul_rn(w, nm) : w;
             }
         }
@@ -221,12 +221,15 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
             float tmax = -FLT_MAX;
             if (f < Tv)
             {
-                for (int m = g; m < nmel; m += kGroups)
+                const float* so = s_out + f;
+                float* yp = y + size_t(g) * hs + f;
+                const size_t ystep = size_t(kGroups) * hs;
+                for (int m = g; m < nmel; m += kGroups, yp += ystep)
                 {
                     float acc = 0.0f;
-                    for (int e = csrRow[m]; e < csrRow[m + 1]; ++e)
-                        acc = __fadd_rn(acc, __fmul_rn(s_out[csrBin[e] * LD + f], csrW[e]));
-                    y[size_t(m) * hs + f] = acc;
+                    const int e1 = csrRow[m + 1];
+                    for (int e = csrRow[m]; e < e1; ++e) acc = __fadd_rn(acc, __fmul_rn(so[csrBin[e]], csrW[e]));
+                    *yp = acc;
                     tmax = fmaxf(tmax, acc);
                 }
             }

@@ -39,9 +39,11 @@ struct MelCount
 };
 
 // Shared memory plan for numFilter filters and at most maxBins bins (host and device agree).
+// rowStart/entries: filter m's weights as (tile offset of the bin's row, weight) pairs
+// entries[rowStart[m] .. rowStart[m + 1]), in the reference's accumulation order.
 struct MelLayout
 {
-    size_t range, first, last, norm, f0, f1, wd, spec, total;
+    size_t range, first, last, norm, f0, f1, wd, rowStart, entries, spec, total;
     __host__ __device__ MelLayout(int numFilter, int maxBins)
     {
         range = 0;
@@ -51,10 +53,48 @@ struct MelLayout
         f0 = (norm + size_t(numFilter) * 4 + 7) & ~size_t(7);
         f1 = f0 + size_t(numFilter + 1) * 8;
         wd = f1 + size_t(numFilter + 1) * 8;
-        spec = (wd + size_t(maxBins) * 4 + 15) & ~size_t(15);
+        rowStart = (wd + size_t(maxBins) * 4 + 15) & ~size_t(15);
+        entries = (rowStart + size_t(numFilter + 1) * 4 + 15) & ~size_t(15);
+        spec = (entries + size_t(2 * maxBins + 2) * 8 + 15) & ~size_t(15);
         total = spec + size_t(maxBins) * kLd * 4;
     }
 };
+
+// Flattens the tables into (offset, weight) entries: bins of interval m with (1 - weightsDown) *
+// norm[m], then bins of interval m + 1 with weightsDown * norm[m] (norm only when normalizing);
+// offset = (bin - k0) * kLd in the staged tile.  Ends with __syncthreads.
+__device__ void build_entries(const MelTableView& T, int numFilter, bool normalize, int* rowStart, int2* ent)
+{
+    const int k0 = T.range[0];
+    if (threadIdx.x == 0)
+    {
+        int acc = 0;
+        for (int m = 0; m < numFilter; ++m)
+        {
+            rowStart[m] = acc;
+            acc += max(T.last[m] - T.first[m], 0) + max(T.last[m + 1] - T.first[m + 1], 0);
+        }
+        rowStart[numFilter] = acc;
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < numFilter; m += blockDim.x)
+    {
+        int e = rowStart[m];
+        for (int k = T.first[m]; k < T.last[m]; ++k, ++e)
+        {
+            float w = __fsub_rn(1.0f, T.weightsDown[k]);
+            if (normalize) w = __fmul_rn(w, T.norm[m]);
+            ent[e] = make_int2((k - k0) * kLd, __float_as_int(w));
+        }
+        for (int k = T.first[m + 1]; k < T.last[m + 1]; ++k, ++e)
+        {
+            float w = T.weightsDown[k];
+            if (normalize) w = __fmul_rn(w, T.norm[m]);
+            ent[e] = make_int2((k - k0) * kLd, __float_as_int(w));
+        }
+    }
+    __syncthreads();
+}
 
 __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq, int maxBins,
                                                        const long long* __restrict__ prefix)
@@ -66,6 +106,8 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
                          reinterpret_cast<float*>(smem + lay.norm), reinterpret_cast<double*>(smem + lay.f0),
                          reinterpret_cast<double*>(smem + lay.f1), reinterpret_cast<float*>(smem + lay.wd), range};
     float* s_spec = reinterpret_cast<float*>(smem + lay.spec);
+    int* rowStart = reinterpret_cast<int*>(smem + lay.rowStart);
+    int2* ent = reinterpret_cast<int2*>(smem + lay.entries);
     const MelParams mp{a.minFreq, maxFreq, a.sampleRate, a.htk, a.numFilter, a.normalize};
     if (threadIdx.x == 0) range[2] = -1;
     __syncthreads();
@@ -84,7 +126,11 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
         const bool ok = nfft >= 2 && bins <= maxBins && uint32_t(bins) <= a.srcRows;
         const int held = range[2];
         __syncthreads();   // every thread has read the key before a rebuild may change it
-        if (ok && held != nfft) build_mel_tables(T, mp, nfft);
+        if (ok && held != nfft)
+        {
+            build_mel_tables(T, mp, nfft);
+            build_entries(T, a.numFilter, a.normalize, rowStart, ent);
+        }
         const int t0 = tile * kTile;
         const int zc = int(min((long long)frames + 8, (long long)a.dstHStride));
         const int tv = min(kTile, frames - t0);   // valid frames of this tile (may be <= 0)
@@ -101,30 +147,25 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
         }
         __syncthreads();
         const int col = t0 + t;
-        float* y = a.dst + size_t(b) * a.dstNStride;
         if (col < zc)
         {
-            for (int m = g; m < a.numFilter; m += kGroups)
+            const bool live = ok && col < frames;
+            const float* sp = s_spec + t;
+            float* yp = a.dst + size_t(b) * a.dstNStride + size_t(g) * a.dstHStride + col;
+            const size_t ystep = size_t(kGroups) * a.dstHStride;
+            for (int m = g; m < a.numFilter; m += kGroups, yp += ystep)
             {
                 float acc = 0.0f;
-                if (ok && col < frames)
+                if (live)
                 {
-                    // bins of interval m: weight (1 - weightsDown) * norm[m]
-                    for (int k = T.first[m]; k < T.last[m]; ++k)
+                    const int e1 = rowStart[m + 1];
+                    for (int e = rowStart[m]; e < e1; ++e)
                     {
-                        float wgt = __fsub_rn(1.0f, T.weightsDown[k]);
-                        if (a.normalize) wgt = __fmul_rn(wgt, T.norm[m]);
-                        acc = __fadd_rn(acc, __fmul_rn(s_spec[(k - k0) * kLd + t], wgt));
-                    }
-                    // bins of interval m + 1: weight weightsDown * norm[m]
-                    for (int k = T.first[m + 1]; k < T.last[m + 1]; ++k)
-                    {
-                        float wgt = T.weightsDown[k];
-                        if (a.normalize) wgt = __fmul_rn(wgt, T.norm[m]);
-                        acc = __fadd_rn(acc, __fmul_rn(s_spec[(k - k0) * kLd + t], wgt));
+                        const int2 en = ent[e];
+                        acc = __fadd_rn(acc, __fmul_rn(sp[en.x], __int_as_float(en.y)));
                     }
                 }
-                y[size_t(m) * a.dstHStride + col] = acc;
+                *yp = acc;
             }
         }
         __syncthreads();   // the next unit restages the tile and may rebuild the tables

@@ -98,10 +98,16 @@ __global__ void __launch_bounds__(kThreads, (NFFT <= 512 ? 3 : 2)) spectrogram_f
         float* y = a.dst + size_t(b) * a.dstNStride;
         if (a.nft)
         {
-            for (int idx = threadIdx.x; idx < BINS * TF; idx += kThreads)
+            // thread -> (frame f, bins k, k + kThreads / TF, ...): pointers advance by a fixed step
+            constexpr int KS = kThreads / TF;
+            const int f = threadIdx.x % TF;
+            int k = threadIdx.x / TF;
+            if (f < Tv)
             {
-                const int k = idx / TF, f = idx % TF;
-                if (f < Tv) y[size_t(k) * a.dstHStride + f0 + f] = s_out[k * S::OUT_LD + f];
+                const float* sp = s_out + k * S::OUT_LD + f;
+                float* yp = y + size_t(k) * a.dstHStride + f0 + f;
+                const size_t ystep = size_t(KS) * a.dstHStride;
+                for (; k < BINS; k += KS, sp += KS * S::OUT_LD, yp += ystep) *yp = *sp;
             }
         }
         else

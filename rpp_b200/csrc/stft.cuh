@@ -170,8 +170,9 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
                 {
                     const float2 d = *reinterpret_cast<const float2*>(fs + t0);
                     const float2 wv = *reinterpret_cast<const float2*>(s_win + t0);
-                    re = wv.x * d.x;
-                    im = wv.y * d.y;
+                    const float2 p = fft::mul2(wv, d);
+                    re = p.x;
+                    im = p.y;
                 }
                 else
                 {
@@ -215,15 +216,17 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
                 const float2 A = buf[k];
                 const float2 B = buf[(M - k) & (M - 1)];
                 // E = (A + conj(B)) / 2,  O = (A - conj(B)) / (2i),  P = W^k O
-                const float er = 0.5f * (A.x + B.x), ei = 0.5f * (A.y - B.y);
-                const float orr = 0.5f * (A.y + B.y), oi = -0.5f * (A.x - B.x);
+                const float2 sum = fft::mul2(make_float2(0.5f, 0.5f), fft::add2(A, B));   // (er, orr)
+                const float2 dif = fft::mul2(make_float2(-0.5f, 0.5f), fft::sub2(A, B));  // (oi, ei)
+                const float er = sum.x, orr = sum.y, oi = dif.x, ei = dif.y;
                 const float2 t = s_tw[k];
                 const float pr = fmaf(orr, t.x, oi * t.y);
                 const float pi = fmaf(oi, t.x, -orr * t.y);
-                const float xr = er + pr, xi = ei + pi;      // X[k] = E + P
-                const float yr = er - pr, yi = ei - pi;      // X[M-k] = conj(E - P)
-                const float p0 = fmaf(xr, xr, xi * xi);
-                const float p1 = fmaf(yr, yr, yi * yi);
+                const float2 X = fft::add2(make_float2(er, ei), make_float2(pr, pi));   // X[k] = E + P
+                const float2 Y = fft::sub2(make_float2(er, ei), make_float2(pr, pi));   // X[M-k] = conj(E - P)
+                const float2 sq = fft::mul2(make_float2(X.y, Y.y), make_float2(X.y, Y.y));
+                const float p0 = fmaf(X.x, X.x, sq.x);
+                const float p1 = fmaf(Y.x, Y.x, sq.y);
                 s_out[k * S::OUT_LD + fl] = (power == 1) ? sqrtf(p0) : p0;
                 if (k != M - k) s_out[(M - k) * S::OUT_LD + fl] = (power == 1) ? sqrtf(p1) : p1;
             }
