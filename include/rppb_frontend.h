@@ -53,6 +53,12 @@ typedef struct
     Rpp32f referenceMagnitude; /* 0: per-sample maximum */
     /* schedule: clips by which the decibel tiles trail the spectrum tiles (0 = default 32) */
     Rpp32s lookahead;
+    /* schedule (never the results; rppb_frontend_tune_gpu picks them): frames per spectrum tile
+     * (0 = default, else the default or twice it), frames per decibel item (0 = 64, else a power
+     * of two from 16 to 256), CTAs per SM (0 = as many as fit) */
+    Rpp32s tileFrames;
+    Rpp32s dbFrames;
+    Rpp32s ctasPerSm;
 } RppbFrontendParams;
 
 /* srcDesc numDims = 2 (F32 1-D signals); dstDesc numDims = 3, layout NFT, F32.
@@ -95,6 +101,19 @@ SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips, Rpp32s nu
                                                 const Rpp32f* lookup, Rpp32s lookupSize, Rpp32f scale, Rpp32f center,
                                                 Rpp32s lobes, Rpp32f preemphCoeff, const RppbFrontendParams* params,
                                                 rppHandle_t rppHandle);
+
+/* Autotuner of the schedule of rppb_frontend_gpu (extension; no counterpart in the reference): runs
+ * the call on the given batch once per candidate (frames per spectrum tile, frames per decibel item,
+ * lookahead, CTAs per SM; outputs are identical for all of them), times `reps` runs of each with
+ * CUDA events on the handle stream, and writes the fastest into params->tileFrames, dbFrames,
+ * lookahead and ctasPerSm (bestMs, if not null, receives its time).  dstPtr is overwritten with
+ * the call's result.  Winners are remembered per device and call shape for the process, and in the
+ * file named by the RPPB_TUNE_CACHE environment variable if set.  Synchronizes the handle stream;
+ * not capturable. */
+SHARED_PUBLIC RppStatus rppb_frontend_tune_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                               RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor, Rpp32f* coeffTensor,
+                                               RppbFrontendParams* params, Rpp32s reps, Rpp32f* bestMs,
+                                               rppHandle_t rppHandle);
 
 /* The fused front end on HOST tensors: srcHost, dstHost, srcLengthHost and coeffHost are host memory
  * (pinned for overlap; pageable works but serializes the copies), laid out as for rppb_frontend_gpu.

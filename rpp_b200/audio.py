@@ -129,6 +129,17 @@ def frontend_host(src, src_desc, dst, dst_desc, src_length, coeff, params, num_c
                                             _h(handle)))
 
 
+def frontend_tune(src, src_desc, dst, dst_desc, src_length, coeff, params, handle, reps=3):
+    """rppb_frontend_tune_gpu: times the schedule candidates of rppb_frontend_gpu on this batch and
+    writes the fastest into `params` (in place).  Returns (status, best ms)."""
+    L = _lib.load()
+    ms = ctypes.c_float(0.0)
+    st = L.rppb_frontend_tune_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                  _addr(src_length), _addr(coeff), ctypes.byref(params), int(reps), ctypes.byref(ms),
+                                  _h(handle))
+    return _status(st), ms.value
+
+
 def device_error(handle):
     """Reads and clears the handle's device error word (synchronizes the handle stream)."""
     L = _lib.load()

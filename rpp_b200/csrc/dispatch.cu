@@ -24,6 +24,8 @@
 
 using namespace rppb;
 
+static_assert(sizeof(RppbFrontendParams) == 88, "RppbFrontendParams layout (rpp_b200/types.py mirrors it)");
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -457,6 +459,9 @@ RppStatus frontend_params(Handle& h, const RppbFrontendParams* params, float* wi
     a.refMag = p.referenceMagnitude;
     a.lookahead = p.lookahead > 0 ? p.lookahead : 32;
     a.reserveSms = 0;
+    a.tileFrames = p.tileFrames;
+    a.dbFrames = p.dbFrames;
+    a.ctasPerSm = p.ctasPerSm;
     a.clips = nullptr;
     a.outRate = 0.f;
     a.coeffAll = 0.f;

@@ -22,6 +22,7 @@
 #include <cfloat>
 
 #include <algorithm>
+#include <string>
 
 #include "common.cuh"
 #include "mel_tables.cuh"
@@ -31,7 +32,7 @@
 namespace rppb {
 
 constexpr int kFusedThreads = 256;
-constexpr int kDbFrames = 64;                 // frames per decibel item
+constexpr int kDbFramesDefault = 64;          // frames per decibel item unless tuned
 constexpr int kFusedPrefixCache = 320;        // slots cached in shared memory (n + lookahead + 1)
 constexpr long long kWaitLimit = 1ll << 24;   // x ~128 ns sleeps: a few seconds
 
@@ -72,7 +73,7 @@ struct SlotCount
         return max(0, min(num_windows(c.L, a.W, a.hop, a.center), c.maxFrames));
     }
     __device__ int tiles(int b) const { return (frames(b) + TF - 1) / TF; }
-    __device__ int db_tiles(int b) const { return (frames(b) + kDbFrames - 1) / kDbFrames; }
+    __device__ int db_tiles(int b) const { return (frames(b) + a.dbFrames - 1) / a.dbFrames; }
     __device__ long long operator()(int s) const
     {
         long long c = 0;
@@ -83,10 +84,10 @@ struct SlotCount
 };
 
 // Shared memory plan (bytes), computed identically on host and device.
-template <int NFFT>
+template <int NFFT, int TF>
 struct FusedLayout
 {
-    using S = StftShape<NFFT, kFusedThreads>;
+    using S = StftShape<NFFT, kFusedThreads, TF>;
     size_t tw, tw1, win, span, work, csrRow, csrBin, csrW, total;
     __host__ __device__ FusedLayout(int numFilter, int W, int hop)
     {
@@ -108,17 +109,17 @@ struct FusedLayout
     }
 };
 
-template <int NFFT>
+template <int NFFT, int TFX>
 __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend_kernel(FrontendArgs a, const float2* __restrict__ twiddle,
                                                                  const long long* __restrict__ prefix,
                                                                  unsigned long long* __restrict__ workCounter,
                                                                  int* __restrict__ done, unsigned* __restrict__ maxKey,
                                                                  int* __restrict__ errorWord)
 {
-    using S = StftShape<NFFT, kFusedThreads>;
+    using S = StftShape<NFFT, kFusedThreads, TFX>;
     constexpr int TF = S::TF, BINS = S::BINS, LD = S::OUT_LD;
     extern __shared__ __align__(16) unsigned char smem[];
-    const FusedLayout<NFFT> lay(a.mel.numFilter, a.W, a.hop);
+    const FusedLayout<NFFT, TFX> lay(a.mel.numFilter, a.W, a.hop);
     float2* s_tw = reinterpret_cast<float2*>(smem + lay.tw);
     float2* s_tw1 = reinterpret_cast<float2*>(smem + lay.tw1);
     float* s_win = reinterpret_cast<float*>(smem + lay.win);
@@ -205,8 +206,8 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         const ClipView cv = clip_view(a, b);
         const int L = cv.L;
         const int F = min(num_windows(L, a.W, a.hop, a.center), cv.maxFrames);
-        const int f0 = tile * (spectrumItem ? TF : kDbFrames);
-        const int Tv = min(spectrumItem ? TF : kDbFrames, F - f0);
+        const int f0 = tile * (spectrumItem ? TF : a.dbFrames);
+        const int Tv = min(spectrumItem ? TF : a.dbFrames, F - f0);
         float* y = cv.y + f0;
         const uint32_t hs = cv.hStride;
 
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
             const float* x = cv.x;
             const float bval = a.border == 1 ? x[0] : a.border == 2 ? (cv.hasSecond ? x[1] : 0.f) : 0.f;
             const PreemphSource src{x, L, a.reflect, cv.coeff, bval};
-            stft_tile<NFFT, kFusedThreads>(src, f0, F, a.W, a.hop, centerOffset, a.power, s_win, s_tw, s_tw1, s_span,
+            stft_tile<NFFT, kFusedThreads, TFX>(src, f0, F, a.W, a.hop, centerOffset, a.power, s_win, s_tw, s_tw1, s_span,
                                            s_fft, s_out);
             __syncthreads();
             float tmax = -FLT_MAX;
@@ -274,9 +275,9 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                     ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
                 }
                 const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
-                const int fd = threadIdx.x % kDbFrames;
-                const int gd = threadIdx.x / kDbFrames;
-                constexpr int kDbGroups = kFusedThreads / kDbFrames;
+                const int fd = threadIdx.x & (a.dbFrames - 1);   // dbFrames: power of two <= threads
+                const int gd = threadIdx.x / a.dbFrames;
+                const int kDbGroups = kFusedThreads / a.dbFrames;
                 if (fd < Tv)
                 {
                     for (int m = gd; m < nmel; m += kDbGroups)
@@ -293,10 +294,10 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     }
 }
 
-template <int NFFT>
+template <int NFFT, int TFX>
 void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
 {
-    using S = StftShape<NFFT, kFusedThreads>;
+    using S = StftShape<NFFT, kFusedThreads, TFX>;
     const int nslots = a.n + a.lookahead;
     Carver cv(scratch);
     long long* prefix = cv.take<long long>(nslots + 1);
@@ -306,13 +307,14 @@ void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
     const size_t clear = reinterpret_cast<char*>(maxKey + a.n) - reinterpret_cast<char*>(counter);
     check_cuda(cudaMemsetAsync(counter, 0, clear, h.stream()), "memset(frontend state)");
     launch_ragged_prefix(SlotCount<S::TF>{a, a.n, a.lookahead}, nslots, prefix, h.stream());
-    const FusedLayout<NFFT> lay(a.mel.numFilter, a.W, a.hop);
+    const FusedLayout<NFFT, TFX> lay(a.mel.numFilter, a.W, a.hop);
     if (lay.total > 227 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
     const float2* tw = spectrogram_twiddles(h, NFFT);
-    int grid = persistent_grid(h, reinterpret_cast<const void*>(frontend_kernel<NFFT>), kFusedThreads, lay.total);
+    int grid = persistent_grid(h, reinterpret_cast<const void*>(frontend_kernel<NFFT, TFX>), kFusedThreads, lay.total);
+    if (a.ctasPerSm > 0) grid = std::min(grid, a.ctasPerSm * h.num_sms());
     if (a.reserveSms > 0 && a.reserveSms < h.num_sms())
         grid = std::max(1, grid / h.num_sms() * (h.num_sms() - a.reserveSms));
-    frontend_kernel<NFFT><<<grid, kFusedThreads, lay.total, h.stream()>>>(a, tw, prefix, counter, done, maxKey,
+    frontend_kernel<NFFT, TFX><<<grid, kFusedThreads, lay.total, h.stream()>>>(a, tw, prefix, counter, done, maxKey,
                                                                           h.device_flags());
     count_launch();
     check_cuda(cudaGetLastError(), "frontend_kernel");
@@ -330,16 +332,35 @@ size_t frontend_scratch_bytes(int n, int lookahead)
     return cv.used();
 }
 
-void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a)
+namespace {
+
+// Tile frames: the plan's default or twice it (both bit-identical; the autotuner picks).
+template <int NFFT>
+void launch_nfft(Handle& h, const FrontendArgs& a, void* scratch)
 {
-    if (a.n <= 0) return;
+    constexpr int T0 = Plan<NFFT>::TF;
+    if (a.tileFrames == 0 || a.tileFrames == T0) launch_fused<NFFT, T0>(h, a, scratch);
+    else if (a.tileFrames == 2 * T0) launch_fused<NFFT, 2 * T0>(h, a, scratch);
+    else fail(RPP_ERROR_NOT_IMPLEMENTED, "tileFrames must be 0, " + std::to_string(T0) + " or " + std::to_string(2 * T0));
+}
+
+}  // namespace
+
+void launch_frontend(Handle& h, void* scratch, const FrontendArgs& args)
+{
+    if (args.n <= 0) return;
+    FrontendArgs a = args;
+    if (a.dbFrames == 0) a.dbFrames = kDbFramesDefault;
+    if (a.dbFrames < 16 || a.dbFrames > kFusedThreads || (a.dbFrames & (a.dbFrames - 1)))
+        fail(RPP_ERROR_NOT_IMPLEMENTED, "dbFrames must be 0 or a power of two from 16 to 256");
+    if (a.ctasPerSm < 0) fail(RPP_ERROR_INVALID_ARGUMENTS, "ctasPerSm must not be negative");
     switch (a.nfft)
     {
-        case 128: launch_fused<128>(h, a, scratch); return;
-        case 256: launch_fused<256>(h, a, scratch); return;
-        case 512: launch_fused<512>(h, a, scratch); return;
-        case 1024: launch_fused<1024>(h, a, scratch); return;
-        case 2048: launch_fused<2048>(h, a, scratch); return;
+        case 128: launch_nfft<128>(h, a, scratch); return;
+        case 256: launch_nfft<256>(h, a, scratch); return;
+        case 512: launch_nfft<512>(h, a, scratch); return;
+        case 1024: launch_nfft<1024>(h, a, scratch); return;
+        case 2048: launch_nfft<2048>(h, a, scratch); return;
         default: fail(RPP_ERROR_NOT_IMPLEMENTED, "fused front end needs a power-of-two nfft from 128 to 2048");
     }
 }

@@ -134,6 +134,9 @@ struct FrontendArgs
     float outRate;
     float coeffAll;
     int reserveSms;          // SMs' worth of CTA slots left to kernels on other streams
+    // schedule (never the arithmetic): frames per spectrum tile (0: plan default), frames per
+    // decibel item (0: 64), CTAs per SM (0: as many as fit)
+    int tileFrames, dbFrames, ctasPerSm;
 };
 size_t frontend_scratch_bytes(int n, int lookahead);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);

@@ -36,11 +36,13 @@ struct Plan<1024> { static constexpr int R1 = 32, R2 = 16, TF = 16; };
 template <>
 struct Plan<2048> { static constexpr int R1 = 32, R2 = 32, TF = 16; };
 
-template <int NFFT, int THREADS>
+// TFX: frames per tile (Plan<NFFT>::TF by default; the fused kernel also instantiates other sizes,
+// which change the schedule and never the arithmetic of a frame).
+template <int NFFT, int THREADS, int TFX = Plan<NFFT>::TF>
 struct StftShape
 {
     static constexpr int M = NFFT / 2;
-    static constexpr int R1 = Plan<NFFT>::R1, R2 = Plan<NFFT>::R2, TF = Plan<NFFT>::TF;
+    static constexpr int R1 = Plan<NFFT>::R1, R2 = Plan<NFFT>::R2, TF = TFX;
     static constexpr int G = R2;                       // threads per frame
     static constexpr int FPP = THREADS / G;            // frames per pass
     static constexpr int PASSES = (TF + FPP - 1) / FPP;
@@ -120,13 +122,13 @@ __device__ __forceinline__ void stft_tables(const float2* __restrict__ twiddle, 
 
 // Computes frames f0 .. f0+TF-1 (those < F) of one sample into s_out[bin * OUT_LD + f] and
 // leaves the other columns undefined.  All THREADS threads of the CTA must call it.
-template <int NFFT, int THREADS, class Src>
+template <int NFFT, int THREADS, int TFX = Plan<NFFT>::TF, class Src>
 __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, int hop, int centerOffset, int power,
                                           const float* __restrict__ s_win, const float2* __restrict__ s_tw,
                                           const float2* __restrict__ s_tw1, float* __restrict__ s_span,
                                           float2* __restrict__ s_fft, float* __restrict__ s_out)
 {
-    using S = StftShape<NFFT, THREADS>;
+    using S = StftShape<NFFT, THREADS, TFX>;
     constexpr int M = S::M, R1 = S::R1, R2 = S::R2, TF = S::TF, G = S::G, FPP = S::FPP, BINS = S::BINS;
 
     // ---- 1. stage the tile's input span

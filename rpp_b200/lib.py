@@ -20,7 +20,7 @@ EXPORTED = (
     "rppbGetLastError", "rppbGetLaunchCount", "rppb_frontend_gpu", "rppb_get_device_error",
     "rppb_downmix_resample_gpu", "rppt_to_decibels_gpu_static", "rppb_frontend_clips_gpu",
     "rppb_spectrogram_tc_gpu",
-    "rppb_frontend_host_gpu",
+    "rppb_frontend_host_gpu", "rppb_frontend_tune_gpu",
     "rppb_server_create", "rppb_server_destroy", "rppb_server_frames", "rppb_server_submit", "rppb_server_poll",
     "rppb_server_arena_used",
 )
@@ -73,6 +73,9 @@ def load(path=None):
     L.rppb_frontend_clips_gpu.restype = _I
     L.rppb_frontend_host_gpu.argtypes = [_V, _D, _V, _D, _V, _V, ctypes.POINTER(RppbFrontendParams), _I, _V]
     L.rppb_frontend_host_gpu.restype = _I
+    L.rppb_frontend_tune_gpu.argtypes = [_V, _D, _V, _D, _V, _V, ctypes.POINTER(RppbFrontendParams), _I,
+                                         ctypes.POINTER(ctypes.c_float), _V]
+    L.rppb_frontend_tune_gpu.restype = _I
     L.rppb_spectrogram_tc_gpu.argtypes = [_V, _D, _V, _D, _V, _V, _I, _B, _B, _I, _I, _I, _I, _I, _V]
     L.rppb_spectrogram_tc_gpu.restype = _I
     L.rppt_to_decibels_gpu_static.argtypes = [_V, _D, _V, _D, _V, _F, _F, _F, _V]

@@ -154,3 +154,51 @@ def test_frontend_host_equals_device(gpu, chunks, pinned_io):
     got = out.numpy() if hasattr(out, "numpy") else out
     np.testing.assert_array_equal(got, exp)
     assert audio.device_error(gpu) == 0
+
+
+SCHEDULES = [dict(tile_frames=32), dict(db_frames=32, lookahead=8), dict(db_frames=128, ctas_per_sm=1),
+             dict(tile_frames=32, db_frames=256, lookahead=96, ctas_per_sm=2)]
+
+
+@pytest.mark.parametrize("sched", SCHEDULES)
+def test_frontend_schedule_knobs_are_bit_identical(gpu, sched):
+    """Tile frames, decibel item frames, lookahead and CTAs per SM move work between CTAs and in
+    time only: every schedule writes exactly the default schedule's bits."""
+    x, lens = synth.config1(n=20, max_len=64000)
+    n, L = x.shape
+    mf = 64000 // 160 + 1
+    xd, ld, cd = dev(x), dev(lens), dev(np.full(n, 0.97, np.float32))
+    sd, dd = audio_desc(n, L), spectra_desc(n, 128, mf)
+    ref = canvas((n, 128, mf))
+    assert audio.frontend(xd, sd, ref, dd, ld, cd, frontend_params(), gpu) == OK
+    out = canvas((n, 128, mf))
+    assert audio.frontend(xd, sd, out, dd, ld, cd, frontend_params(**sched), gpu) == OK
+    np.testing.assert_array_equal(host(out), host(ref))
+    assert audio.device_error(gpu) == 0
+
+
+def test_frontend_tune(gpu):
+    """The autotuner picks a valid schedule, leaves the result unchanged, and answers a repeated
+    shape from its cache."""
+    x, lens = synth.config1(n=32, max_len=96000)
+    n, L = x.shape
+    mf = 96000 // 160 + 1
+    xd, ld, cd = dev(x), dev(lens), dev(np.full(n, 0.97, np.float32))
+    sd, dd = audio_desc(n, L), spectra_desc(n, 128, mf)
+    ref = canvas((n, 128, mf))
+    assert audio.frontend(xd, sd, ref, dd, ld, cd, frontend_params(), gpu) == OK
+    p = frontend_params()
+    out = canvas((n, 128, mf))
+    st, ms = audio.frontend_tune(xd, sd, out, dd, ld, cd, p, gpu, reps=2)
+    assert st == OK and ms > 0
+    assert p.tileFrames in (16, 32) and p.dbFrames in (32, 64, 128) and p.lookahead in (8, 32, 96)
+    assert p.ctasPerSm in (0, 2)
+    np.testing.assert_array_equal(host(out), host(ref))
+    q = frontend_params()
+    st2, ms2 = audio.frontend_tune(xd, sd, out, dd, ld, cd, q, gpu)
+    assert st2 == OK and ms2 == ms
+    assert (q.tileFrames, q.dbFrames, q.lookahead, q.ctasPerSm) == (p.tileFrames, p.dbFrames, p.lookahead,
+                                                                     p.ctasPerSm)
+    out2 = canvas((n, 128, mf))
+    assert audio.frontend(xd, sd, out2, dd, ld, cd, q, gpu) == OK
+    np.testing.assert_array_equal(host(out2), host(ref))
