@@ -8,11 +8,12 @@
 // windowLength - 1 (clamped at 0); no such MMS gives (0, 0).
 //
 // The running sum is a dependent float chain, so its value depends on operation order.  Each
-// reset block is independent, and one GPU thread replays one block's chain in exactly the
+// reset block is independent, and one GPU lane replays one block's chain in exactly the
 // reference's order (add the new square, store sum * (1/windowLength), subtract the square
 // leaving the window; explicit round-to-nearest intrinsics, no FMA): the MMS values, and hence
 // the begin/length integers, are bit-identical to the host path.
-//   1. mms_kernel:    one thread per (sample, reset block): MMS into scratch, block maximum;
+//   1. mms_kernel:    one warp per (sample, reset block): coalesced loads and squares by the warp,
+//                     the chain by one lane, MMS into scratch, block maximum;
 //   2. region_kernel: one warp per sample: cutoff from the block maxima, then the first and
 //                     last qualifying block are scanned (ballot over 32 MMS at a time).
 // Latency-bound by the per-block chain (resetInterval + windowLength dependent steps); the
@@ -45,17 +46,34 @@ struct NsrCount
 
 __device__ __forceinline__ float sq(float v) { return __fmul_rn(v, v); }
 
-__global__ void __launch_bounds__(128) mms_kernel(const float* __restrict__ src, uint32_t stride,
-                                                  const int* __restrict__ len, int windowLength, int reset,
-                                                  float* __restrict__ mms, float* __restrict__ blockMax,
-                                                  const long long* __restrict__ prefix, int n)
+constexpr int kMmsThreads = 256;
+constexpr int kMmsWarps = kMmsThreads / 32;
+constexpr int kChunk = 256;   // samples per warp step
+
+// One warp per (sample, reset block).  Per chunk of 256 samples the warp loads the samples entering
+// and leaving the window (coalesced), squares them in parallel into shared memory, then lane 0
+// runs the block's float chain over the chunk (two dependent adds per sample -- the only serial
+// part; squares and the scaled stores are off the chain) and the warp stores the MMS values.  A
+// square of zero stands for "nothing leaves the window yet": sum - 0 == sum exactly for the
+// non-negative sums of squares, so the chain is bit-identical to the reference's conditional
+// subtraction.
+__global__ void __launch_bounds__(kMmsThreads) mms_kernel(const float* __restrict__ src, uint32_t stride,
+                                                         const int* __restrict__ len, int windowLength, int reset,
+                                                         float* __restrict__ mms, float* __restrict__ blockMax,
+                                                         const long long* __restrict__ prefix, int n)
 {
     __shared__ long long s_prefix[kPrefixCache];
+    __shared__ __align__(16) float s_in[kMmsWarps][kChunk];
+    __shared__ __align__(16) float s_out[kMmsWarps][kChunk];
+    __shared__ __align__(16) float s_val[kMmsWarps][kChunk];
     prefix = cache_prefix(prefix, n, s_prefix);
     const long long total = prefix[n];
     const float meanFactor = __fdiv_rn(1.0f, float(windowLength));
-    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
-         w += (long long)gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    float* qi = s_in[wi];
+    float* qo = s_out[wi];
+    float* vv = s_val[wi];
+    for (long long w = blockIdx.x * (long long)kMmsWarps + wi; w < total; w += (long long)gridDim.x * kMmsWarps)
     {
         const int b = ragged_find(prefix, n, w);
         const int L = min(len[b], int(stride));
@@ -64,21 +82,68 @@ __global__ void __launch_bounds__(128) mms_kernel(const float* __restrict__ src,
         const int end = int(min((long long)L, start + R));
         const float* x = src + size_t(b) * stride;
         float* m = mms + size_t(b) * stride;
+        float sum = 0.0f;   // meaningful in lane 0
         // fresh sum over the window that precedes the block (reference :131-133)
-        float sum = 0.0f;
-        for (int i = max(start - windowLength + 1, 0); i < start; ++i) sum = __fadd_rn(sum, sq(__ldg(x + i)));
-        float bmax = -FLT_MAX;
-        int wb = start - windowLength + 1;
-#pragma unroll 4
-        for (int p = start; p < end; ++p, ++wb)
+        for (int c = max(start - windowLength + 1, 0); c < start; c += kChunk)
         {
-            sum = __fadd_rn(sum, sq(__ldg(x + p)));
-            const float v = __fmul_rn(sum, meanFactor);
-            m[p] = v;
-            bmax = fmaxf(bmax, v);
-            if (wb >= 0) sum = __fsub_rn(sum, sq(__ldg(x + wb)));
+            const int cnt = min(kChunk, start - c);
+            for (int k = lane; k < cnt; k += 32) qi[k] = sq(__ldg(x + c + k));
+            __syncwarp();
+            if (lane == 0)
+                for (int k = 0; k < cnt; ++k) sum = __fadd_rn(sum, qi[k]);
+            __syncwarp();
         }
-        blockMax[w] = bmax;
+        float bmax = -FLT_MAX;
+        for (int c = start; c < end; c += kChunk)
+        {
+            const int cnt = min(kChunk, end - c);
+            for (int k = lane; k < cnt; k += 32)
+            {
+                qi[k] = sq(__ldg(x + c + k));
+                const int wb = c + k - windowLength + 1;
+                qo[k] = wb >= 0 ? sq(__ldg(x + wb)) : 0.0f;
+            }
+            __syncwarp();
+            if (lane == 0)
+            {
+                int k = 0;
+                for (; k + 4 <= cnt; k += 4)
+                {
+                    const float4 a4 = *reinterpret_cast<const float4*>(qi + k);
+                    const float4 o4 = *reinterpret_cast<const float4*>(qo + k);
+                    float4 v4;
+                    sum = __fadd_rn(sum, a4.x);
+                    v4.x = __fmul_rn(sum, meanFactor);
+                    sum = __fsub_rn(sum, o4.x);
+                    sum = __fadd_rn(sum, a4.y);
+                    v4.y = __fmul_rn(sum, meanFactor);
+                    sum = __fsub_rn(sum, o4.y);
+                    sum = __fadd_rn(sum, a4.z);
+                    v4.z = __fmul_rn(sum, meanFactor);
+                    sum = __fsub_rn(sum, o4.z);
+                    sum = __fadd_rn(sum, a4.w);
+                    v4.w = __fmul_rn(sum, meanFactor);
+                    sum = __fsub_rn(sum, o4.w);
+                    *reinterpret_cast<float4*>(vv + k) = v4;
+                }
+                for (; k < cnt; ++k)
+                {
+                    sum = __fadd_rn(sum, qi[k]);
+                    vv[k] = __fmul_rn(sum, meanFactor);
+                    sum = __fsub_rn(sum, qo[k]);
+                }
+            }
+            __syncwarp();
+            for (int k = lane; k < cnt; k += 32)
+            {
+                const float v = vv[k];
+                m[c + k] = v;
+                bmax = fmaxf(bmax, v);
+            }
+            __syncwarp();
+        }
+        bmax = warp_max(bmax);
+        if (lane == 0) blockMax[w] = bmax;
     }
 }
 
@@ -184,8 +249,8 @@ void launch_nsr(Handle& h, void* scratch, const NsrArgs& a)
     float* mms = cv.take<float>(size_t(a.n) * a.srcStride);
     float* blockMax = cv.take<float>(blocks + 1);
     launch_ragged_prefix(NsrCount{a.len, a.srcStride, a.resetInterval}, a.n, prefix, h.stream());
-    int grid = persistent_grid(h, reinterpret_cast<const void*>(mms_kernel), 128, 0);
-    mms_kernel<<<grid, 128, 0, h.stream()>>>(a.src, a.srcStride, a.len, a.windowLength, a.resetInterval, mms,
+    int grid = persistent_grid(h, reinterpret_cast<const void*>(mms_kernel), kMmsThreads, 0);
+    mms_kernel<<<grid, kMmsThreads, 0, h.stream()>>>(a.src, a.srcStride, a.len, a.windowLength, a.resetInterval, mms,
                                              blockMax, prefix, a.n);
     count_launch();
     check_cuda(cudaGetLastError(), "mms_kernel");
