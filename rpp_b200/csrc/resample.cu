@@ -12,9 +12,10 @@
 // summed per channel in order.  Every product and sum is explicitly rounded, so outputs are
 // bit-identical to the host path.
 //
-// One CTA per 256-output block: thread 0 replays the phase sum into shared memory while the
-// others stage the table; then one output per thread.  Inputs are read through L1 (neighbouring
-// outputs share taps).  Compute-bound: 2 * lobes taps of ~10 float operations per output.
+// One CTA per 256-output block: thread 0 replays the phase sum into shared memory; when down-mixing,
+// the CTA then stages the block's input span (down-mixed once per input sample) in shared memory;
+// every thread computes one output.  Compute-bound: 2 * lobes taps of ~10 float
+// operations per output.
 #include "common.cuh"
 #include "downmix.cuh"
 #include "ops.hpp"
@@ -24,6 +25,9 @@ namespace {
 
 constexpr int kBlock = 256;        // outputs per block (the reference's block size)
 constexpr int kCopyChunk = 4096;   // floats per unit of an equal-rate copy
+constexpr int kSpan = 4096;        // input samples of one block staged in shared memory (mono paths)
+
+__host__ __device__ __forceinline__ size_t resample_smem_floats(int lutSize) { return ((lutSize + 3) & ~3) + kSpan; }
 
 __device__ __forceinline__ int out_length(int L, float inRate, float outRate)
 {
@@ -96,7 +100,8 @@ __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restric
                                                           bool normalize, const long long* __restrict__ prefix, int n,
                                                           const RppbClip* __restrict__ clips, float outRateAll)
 {
-    extern __shared__ float s_lut[];
+    extern __shared__ float s_lut[];   // the table, then the staged input span
+    float* s_in = s_lut + ((wd.lutSize + 3) & ~3);
     __shared__ float s_phase[kBlock];
     for (int i = threadIdx.x; i < wd.lutSize; i += blockDim.x) s_lut[i] = wd.lut[i];
     __syncthreads();
@@ -151,6 +156,26 @@ __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restric
             }
         }
         __syncthreads();
+        const float* in = x + (long long)inBlockRounded * C;
+        // down-mixing path: the block's input span [lo, hi), down-mixed once per sample, goes to
+        // shared memory (every tap of the block lies inside it because the phases increase); plain
+        // mono input is read through L1 directly, which measured faster than staging it
+        int lo = 0;
+        bool staged = false;
+        if (kMix)
+        {
+            const int cnt = min(kBlock, outEnd - outBlock);
+            if (cnt > 0)
+            {
+                lo = max(int(ceilf(s_phase[0])) - lobes, -inBlockRounded);
+                const int hi = min(int(ceilf(s_phase[cnt - 1])) + lobes, L - inBlockRounded);
+                staged = hi - lo <= kSpan;
+                if (staged)
+                    for (int i = threadIdx.x; i < hi - lo; i += kBlock)
+                        s_in[i] = kMix ? mix((long long)inBlockRounded + lo + i) : __ldg(in + lo + i);
+            }
+            __syncthreads();
+        }
         const int outPos = outBlock + threadIdx.x;
         if (outPos < outEnd)
         {
@@ -159,11 +184,13 @@ __global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restric
             int loc0 = xc - lobes, loc1 = xc + lobes;
             if (loc0 + inBlockRounded < 0) loc0 = -inBlockRounded;
             if (loc1 + inBlockRounded > L) loc1 = L - inBlockRounded;
-            const float* in = x + (long long)inBlockRounded * C;
             if (kMix || C == 1)
             {
                 // mono input: sample l of the block, down-mixed when kMix
-                auto at = [&](int l) -> float { return kMix ? mix((long long)inBlockRounded + l) : __ldg(in + l); };
+                auto at = [&](int l) -> float {
+                    if (staged) return s_in[l - lo];
+                    return kMix ? mix((long long)inBlockRounded + l) : __ldg(in + l);
+                };
                 int l = loc0;
                 const float locBegin = __fsub_rn(float(l), inPos);
                 float lane[4] = {__fadd_rn(locBegin, 0.f), __fadd_rn(locBegin, 1.f), __fadd_rn(locBegin, 2.f),
@@ -216,7 +243,7 @@ void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStr
     if (n <= 0) return;
     long long* prefix = static_cast<long long*>(scratch);
     launch_ragged_prefix(ResampleCount{inRate, outRate, dims, downmix, nullptr, 0.f}, n, prefix, h.stream());
-    const size_t smem = size_t(win.lutSize) * sizeof(float);
+    const size_t smem = resample_smem_floats(win.lutSize) * sizeof(float);
     if (downmix)
     {
         int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel<true, false>), kBlock, smem);
@@ -241,7 +268,7 @@ void launch_resample_clips(Handle& h, void* scratch, const RppbClip* clips, int 
     if (n <= 0) return;
     long long* prefix = static_cast<long long*>(scratch);
     launch_ragged_prefix(ResampleCount{nullptr, nullptr, nullptr, false, clips, outRate}, n, prefix, h.stream());
-    const size_t smem = size_t(win.lutSize) * sizeof(float);
+    const size_t smem = resample_smem_floats(win.lutSize) * sizeof(float);
     int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel<false, true>), kBlock, smem);
     resample_kernel<false, true><<<grid, kBlock, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr,
                                                                      win, false, prefix, n, clips, outRate);
