@@ -14,6 +14,7 @@
  *   RpptStrides          api/rppdefs.h:570-576
  *   RpptDesc             api/rppdefs.h:581-589
  *   RpptImagePatch       api/rppdefs.h:645-649
+ *   RpptGenericDesc      api/rppdefs.h:591-602 (rppt_slice_gpu)
  *   RpptResamplingWindow api/rppdefs.h:751-790 (C++ only: it holds a std::vector and __m128)
  * Only the subset the audio entry points use is restated.
  */
@@ -161,6 +162,20 @@ typedef struct
     Rpp32u width;
     Rpp32u height;
 } RpptImagePatch, *RpptImagePatchPtr;
+
+typedef size_t RppSize_t;
+#define RPPT_MAX_DIMS (5)
+
+/* N-dimensional tensor descriptor: dims[0] is the batch, strides in elements. */
+typedef struct
+{
+    RppSize_t numDims;
+    Rpp32u offsetInBytes;
+    RpptDataType dataType;
+    Rpp32u dims[RPPT_MAX_DIMS];
+    Rpp32u strides[RPPT_MAX_DIMS];
+    RpptLayout layout;
+} RpptGenericDesc, *RpptGenericDescPtr;
 
 #ifdef __cplusplus
 /* Resampling window: a lookup table of the windowed-sinc kernel, sampled so that

@@ -33,7 +33,7 @@ H
 INC=(-I"$GEN" -I"$RPP_REF/api" -I"$RPP_REF/src/include/common" -I"$RPP_REF/src/include/common/cpu"
      -I"$RPP_REF/src/include/tensor" -I"$RPP_REF/third_party/ffts/include")
 COMMON=(-O3 -DNDEBUG -DAUDIO_SUPPORT -fopenmp -mavx2 -mf16c -std=gnu++17 -fPIC -w)
-KERNELS=(non_silent_region_detection to_decibels pre_emphasis_filter down_mixing spectrogram mel_filter_bank resample)
+KERNELS=(non_silent_region_detection to_decibels pre_emphasis_filter down_mixing spectrogram mel_filter_bank resample slice)
 OBJS=()
 CXX="${CXX:-g++}"
 # some gcc installs on PATH lack libgomp.spec; point -B at a gcc lib dir that has it

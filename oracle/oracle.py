@@ -109,6 +109,8 @@ class Oracle:
                                              ctypes.c_double, ctypes.c_double]
         L.oracle_nsr.argtypes = [_F32P, _L, _I, _I32P, _I32P, _I32P, _F, _I, _F, _I, _F32P, _F32P]
         L.oracle_windowed_sinc.argtypes = [_I, _I, _F32P, _F32P]
+        L.oracle_slice.argtypes = [ctypes.c_void_p, _L, _L, ctypes.c_void_p, _L, _L, _I, _I, _I32P, _I32P, _U32P,
+                                   ctypes.c_void_p, _I, _I]
 
     def windowed_sinc(self, coeffs, lobes):
         """The test suite's Hann-windowed sinc table: (lut, scale, center, lobes)."""
@@ -220,6 +222,22 @@ class Oracle:
                                         float(multiplier), float(ref_mag))
         return dst
 
+    def slice(self, src, dst, anchor, shape, roi, fill, enable_padding, num_dims):
+        """src/dst: [n][stride0] (1-D) or [n][rows][stride1] (2-D) float32 or uint8 arrays; dst is
+        updated in place (fill + box copy) and returned."""
+        n = src.shape[0]
+        es = src.dtype.itemsize
+        s0 = int(np.prod(src.shape[1:]))
+        d0 = int(np.prod(dst.shape[1:]))
+        s1 = src.shape[-1] if num_dims == 2 else 0
+        d1 = dst.shape[-1] if num_dims == 2 else 0
+        f = np.array([fill], dtype=src.dtype)
+        self.lib.oracle_slice(src.ctypes.data, s0, s1, dst.ctypes.data, d0, d1, n, int(num_dims),
+                              _p(np.ascontiguousarray(anchor, np.int32), _I32P),
+                              _p(np.ascontiguousarray(shape, np.int32), _I32P),
+                              _p(np.ascontiguousarray(roi, np.uint32), _U32P), f.ctypes.data, int(enable_padding), es)
+        return dst
+
     def nsr(self, src, lengths, cutoff_db, window_length, ref_power, reset_interval, want_mms=False):
         n, ss = src.shape
         begin = np.zeros(n, np.int32)
@@ -244,6 +262,9 @@ class Reference:
         L.ref_create.argtypes = [ctypes.c_size_t, ctypes.c_uint]
         L.ref_create.restype = ctypes.c_void_p
         L.ref_destroy.argtypes = [ctypes.c_void_p]
+        L.ref_slice_f32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _I32P, _I32P,
+                                    ctypes.c_void_p, ctypes.c_bool, _U32P, ctypes.c_void_p]
+        L.ref_slice_u8.argtypes = L.ref_slice_f32.argtypes
         D = ctypes.POINTER(RpptDesc)
         V = ctypes.c_void_p
         L.rppt_pre_emphasis_filter_host.argtypes = [V, D, V, D, _I32P, _F32P, _I, V]
@@ -327,3 +348,21 @@ class Reference:
         return self.lib.ref_resample(self._v(src), ctypes.byref(sd), self._v(dst), ctypes.byref(dd),
                                      _p(in_rate, _F32P), _p(out_rate, _F32P), _p(dims, _I32P), _p(lut, _F32P),
                                      len(lut), float(scale), float(center), int(lobes), int(coeffs), self.h)
+
+
+def _reference_slice(self, src, dst, anchor, shape, roi, fill, enable_padding, num_dims):
+    """The reference's host slice on the same arrays as Oracle.slice (dst updated in place)."""
+    from rpp_b200.types import generic_desc, RpptDataType
+    dt = RpptDataType.U8 if src.dtype == np.uint8 else RpptDataType.F32
+    sd = generic_desc(src.shape, dt)
+    dd = generic_desc(dst.shape, dt)
+    f = np.array([fill], dtype=src.dtype)
+    fn = self.lib.ref_slice_u8 if src.dtype == np.uint8 else self.lib.ref_slice_f32
+    st = fn(src.ctypes.data, ctypes.addressof(sd), dst.ctypes.data, ctypes.addressof(dd),
+            _p(np.ascontiguousarray(anchor, np.int32), _I32P), _p(np.ascontiguousarray(shape, np.int32), _I32P),
+            f.ctypes.data, bool(enable_padding), _p(np.ascontiguousarray(roi, np.uint32), _U32P), self.h)
+    assert st == 0, st
+    return dst
+
+
+Reference.slice = _reference_slice

@@ -8,6 +8,8 @@
 #include "rpp.h"
 #include "rppdefs.h"
 #include "rppt_tensor_audio_augmentations.h"
+#include "handle.hpp"
+#include "host_tensor_executors.hpp"
 
 extern "C" {
 
@@ -43,5 +45,26 @@ __attribute__((visibility("default"))) int ref_resample(float* src, RpptDesc* sr
     w.pCenter = _mm_set1_ps(center);
     w.pScale = _mm_set1_ps(scale);
     return rppt_resample_host(src, srcDesc, dst, dstDesc, inRate, outRate, srcDims, w, static_cast<rppHandle_t>(h));
+}
+
+// The reference's host slice (src/modules/tensor/cpu/kernel/slice.cpp:27-238), called at the
+// kernel level: rppt_slice_host lives in the geometric-augmentations dispatch file, which pulls in
+// every image kernel.  The 1-D and 2-D cases read no layout parameters.
+__attribute__((visibility("default"))) int ref_slice_f32(float* src, RpptGenericDesc* srcDesc, float* dst,
+                                                         RpptGenericDesc* dstDesc, int* anchor, int* shape, float* fill,
+                                                         bool enablePadding, unsigned* roi, void* h)
+{
+    RppLayoutParams lp{};
+    rpp::Handle& handle = *static_cast<rpp::Handle*>(static_cast<rppHandle_t>(h));
+    return slice_host_tensor<Rpp32f>(src, srcDesc, dst, dstDesc, anchor, shape, fill, enablePadding, roi, lp, handle);
+}
+
+__attribute__((visibility("default"))) int ref_slice_u8(unsigned char* src, RpptGenericDesc* srcDesc, unsigned char* dst,
+                                                        RpptGenericDesc* dstDesc, int* anchor, int* shape,
+                                                        unsigned char* fill, bool enablePadding, unsigned* roi, void* h)
+{
+    RppLayoutParams lp{};
+    rpp::Handle& handle = *static_cast<rpp::Handle*>(static_cast<rppHandle_t>(h));
+    return slice_host_tensor<Rpp8u>(src, srcDesc, dst, dstDesc, anchor, shape, fill, enablePadding, roi, lp, handle);
 }
 }

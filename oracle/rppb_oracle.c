@@ -675,3 +675,41 @@ EXPORT void oracle_windowed_sinc(int coeffs, int lobes, float *lut, float *out)
     out[1] = center + 1;
     out[2] = (float)lobes;
 }
+
+/* ---------------------------------------------------------------- slice (1-D and 2-D)
+ * src/modules/tensor/cpu/kernel/slice.cpp:40-60 (per-sample anchor, shape, roi lengths) and
+ * :197-228: maxLen_d = min(shape_d, length_d - anchor_d) with length_d = roi[numDims + d] (the roi
+ * begin values are not read); when any anchor_d + shape_d > length_d and padding is enabled, the
+ * first dstStride0 - 1 elements of the sample are filled with the fill value; then the box
+ * [anchor, anchor + maxLen) is copied.  Negative box extents (anchor beyond the length) copy
+ * nothing here; the reference converts them to huge unsigned sizes.  elemSize 4 (float) or 1 (u8). */
+EXPORT void oracle_slice(const void *src, long srcStride0, long srcStride1, void *dst, long dstStride0,
+                         long dstStride1, int n, int numDims, const int *anchor, const int *shape,
+                         const unsigned *roi, const void *fill, int enablePadding, int elemSize)
+{
+    for (int b = 0; b < n; b++)
+    {
+        const int *a = anchor + b * numDims, *s = shape + b * numDims;
+        const int *len = (const int *)(roi + b * numDims * 2 + numDims);
+        const char *sp = (const char *)src + (size_t)b * srcStride0 * elemSize;
+        char *dp = (char *)dst + (size_t)b * dstStride0 * elemSize;
+        int need = 0;
+        for (int d = 0; d < numDims; d++)
+            if (a[d] + s[d] > len[d]) need = 1;
+        if (need && enablePadding)
+            for (long i = 0; i < dstStride0 - 1; i++) memcpy(dp + i * elemSize, fill, elemSize);
+        if (numDims == 1)
+        {
+            int m = s[0] < len[0] - a[0] ? s[0] : len[0] - a[0];
+            if (m > 0) memcpy(dp, sp + (size_t)a[0] * elemSize, (size_t)m * elemSize);
+        }
+        else
+        {
+            int mh = s[0] < len[0] - a[0] ? s[0] : len[0] - a[0];
+            int mw = s[1] < len[1] - a[1] ? s[1] : len[1] - a[1];
+            for (int r = 0; r < mh && mw > 0; r++)
+                memcpy(dp + (size_t)r * dstStride1 * elemSize,
+                       sp + ((size_t)(a[0] + r) * srcStride1 + a[1]) * elemSize, (size_t)mw * elemSize);
+        }
+    }
+}

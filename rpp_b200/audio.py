@@ -140,6 +140,15 @@ def frontend_tune(src, src_desc, dst, dst_desc, src_length, coeff, params, handl
     return _status(st), ms.value
 
 
+def slice(src, src_desc, dst, dst_desc, anchor, shape, fill_value, enable_padding, roi, handle):
+    """rppt_slice_gpu (api/rppt_tensor_geometric_augmentations.h:486); fill_value: a one-element
+    array or tensor of the data type (host, pinned or device)."""
+    L = _lib.load()
+    return _status(L.rppt_slice_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                    _addr(anchor), _addr(shape), _addr(fill_value), bool(enable_padding), _addr(roi),
+                                    _h(handle)))
+
+
 def device_error(handle):
     """Reads and clears the handle's device error word (synchronizes the handle stream)."""
     L = _lib.load()

@@ -19,6 +19,7 @@
 
 #include "../../include/rppb_frontend.h"
 #include "../../include/rppt_tensor_audio_augmentations.h"
+#include "../../include/rppt_tensor_geometric_augmentations.h"
 #include "handle.hpp"
 #include "ops.hpp"
 
@@ -831,6 +832,61 @@ extern "C" SHARED_PUBLIC RppStatus rppb_spectrogram_tc_gpu(RppPtr_t srcPtr, Rppt
         a.power = power;
         a.n = n;
         launch_tc_spectrogram(h, scratch, a);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppt_slice_gpu(RppPtr_t srcPtr, RpptGenericDescPtr srcGenericDescPtr,
+                                                  RppPtr_t dstPtr, RpptGenericDescPtr dstGenericDescPtr,
+                                                  Rpp32s* anchorTensor, Rpp32s* shapeTensor, RppPtr_t fillValue,
+                                                  bool enablePadding, Rpp32u* roiTensor, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcGenericDescPtr && dstGenericDescPtr, "null descriptor");
+        const RpptGenericDesc& sd = *srcGenericDescPtr;
+        const RpptGenericDesc& dd = *dstGenericDescPtr;
+        // rppt_tensor_geometric_augmentations.cpp:2520-2522
+        if (sd.dataType != F32 && sd.dataType != U8) return RPP_ERROR_INVALID_SRC_DATATYPE;
+        if (dd.dataType != F32 && dd.dataType != U8) return RPP_ERROR_INVALID_DST_DATATYPE;
+        if (sd.layout != dd.layout) return RPP_ERROR_LAYOUT_MISMATCH;
+        if (sd.dataType != dd.dataType) return RPP_ERROR_NOT_IMPLEMENTED;
+        // the audio path's 1-D signals and 2-D spectra; 3-D / 4-D image and voxel boxes are not built
+        if (sd.numDims < 2 || sd.numDims > 3 || dd.numDims != sd.numDims) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr && anchorTensor && shapeTensor && roiTensor, "null tensor");
+        require(!enablePadding || fillValue, "null fill value");
+        const int n = int(dd.dims[0]);
+        if (n <= 0) return RPP_SUCCESS;
+        require(sd.dims[0] >= dd.dims[0], "source batch smaller than destination batch");
+        const int nd = int(sd.numDims) - 1;
+        const int eb = sd.dataType == U8 ? 1 : 4;
+        Carver m(nullptr);
+        m.take<int>(size_t(n) * nd);
+        m.take<int>(size_t(n) * nd);
+        m.take<uint32_t>(size_t(n) * nd * 2);
+        m.take<float>(1);
+        Carver cv(h.workspace(m.used()));
+        int* aStage = cv.take<int>(size_t(n) * nd);
+        int* sStage = cv.take<int>(size_t(n) * nd);
+        uint32_t* rStage = cv.take<uint32_t>(size_t(n) * nd * 2);
+        float* fStage = cv.take<float>(1);
+        SliceArgs a;
+        a.n = n;
+        a.numDims = nd;
+        a.elemBytes = eb;
+        a.srcStride0 = sd.strides[0];
+        a.srcStride1 = nd == 2 ? sd.strides[1] : 0;
+        a.dstStride0 = dd.strides[0];
+        a.dstStride1 = nd == 2 ? dd.strides[1] : 0;
+        a.srcDim0 = sd.dims[1];
+        a.srcDim1 = nd == 2 ? sd.dims[2] : 1;
+        if (nd == 2 && (a.dstStride1 == 0 || a.srcStride1 < a.srcDim1)) return RPP_ERROR_INVALID_ARGUMENTS;
+        a.anchor = static_cast<const int*>(h.device_view(anchorTensor, size_t(n) * nd * sizeof(int), aStage));
+        a.shape = static_cast<const int*>(h.device_view(shapeTensor, size_t(n) * nd * sizeof(int), sStage));
+        a.roi = static_cast<const uint32_t*>(h.device_view(roiTensor, size_t(n) * nd * 2 * sizeof(uint32_t), rStage));
+        a.enablePadding = enablePadding;
+        const void* fill = enablePadding ? h.device_view(fillValue, size_t(eb), fStage) : nullptr;
+        const size_t off = sd.offsetInBytes, doff = dd.offsetInBytes;
+        launch_slice(h, a, static_cast<const char*>(srcPtr) + off, static_cast<char*>(dstPtr) + doff, fill);
         return RPP_SUCCESS;
     });
 }

@@ -141,6 +141,20 @@ struct FrontendArgs
 size_t frontend_scratch_bytes(int n, int lookahead);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);
 
+// slice (slice.cu): 1-D or 2-D boxes per sample, strides in elements.
+struct SliceArgs
+{
+    int n, numDims, elemBytes;
+    uint32_t srcStride0, srcStride1, dstStride0, dstStride1;
+    uint32_t srcDim0, srcDim1;   // extents of a sample (lengths are clamped to them)
+    const int* anchor;           // device views, n * numDims
+    const int* shape;
+    const uint32_t* roi;         // n * numDims * 2: begins (unused), then lengths
+    bool enablePadding;
+    int unitsPerSample;          // set by launch_slice
+};
+void launch_slice(Handle& h, const SliceArgs& a, const void* src, void* dst, const void* fill);
+
 // PCIe movers over mapped pinned host memory (host_io.cu).
 void launch_host_gather(cudaStream_t stream, const float* src, size_t nStride, const int* len, int clips, float* dst,
                         uint32_t dstStride, int ctas);

@@ -6,7 +6,7 @@ Loading fails loudly when the library is missing: there is no CPU fallback.  Bui
 import ctypes
 import os
 
-from .types import (RpptDesc, RpptImagePatch, RpptResamplingWindow, RppBackend, RppbFrontendParams, RppbServerConfig,
+from .types import (RpptGenericDesc, RpptDesc, RpptImagePatch, RpptResamplingWindow, RppBackend, RppbFrontendParams, RppbServerConfig,
                     RppbCompletion)
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "librppb.so")
@@ -23,6 +23,7 @@ EXPORTED = (
     "rppb_frontend_host_gpu", "rppb_frontend_tune_gpu",
     "rppb_server_create", "rppb_server_destroy", "rppb_server_frames", "rppb_server_submit", "rppb_server_poll",
     "rppb_server_arena_used",
+    "rppt_slice_gpu",
 )
 
 _lib = None
@@ -80,6 +81,9 @@ def load(path=None):
     L.rppb_spectrogram_tc_gpu.restype = _I
     L.rppt_to_decibels_gpu_static.argtypes = [_V, _D, _V, _D, _V, _F, _F, _F, _V]
     L.rppt_to_decibels_gpu_static.restype = _I
+    L.rppt_slice_gpu.argtypes = [_V, ctypes.POINTER(RpptGenericDesc), _V, ctypes.POINTER(RpptGenericDesc), _V, _V, _V,
+                                 _B, _V, _V]
+    L.rppt_slice_gpu.restype = _I
     L.rppb_server_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(RppbServerConfig)]
     L.rppb_server_create.restype = _I
     L.rppb_server_destroy.argtypes = [_V]

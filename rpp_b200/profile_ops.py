@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import audio, lib, synth
-from .types import audio_desc, spectra_desc, frontend_params
+from .types import audio_desc, spectra_desc, frontend_params, generic_desc
 from .windows import kaiser_sinc
 
 
@@ -68,6 +68,11 @@ def main():
     dims_small = patches[:min(n, 8)].contiguous()
     sd_small = spectra_desc(min(n, 8), 128, mf)
     stream = torch.cuda.current_stream().cuda_stream
+    gd = generic_desc((n, L))
+    sl_anchor = torch.full((n,), 10, dtype=torch.int32, device=dev)
+    sl_shape = torch.from_numpy((lens_np // 2).astype(np.int32)).to(dev)
+    sl_roi = torch.from_numpy(np.stack([np.full(n, 10), lens_np], 1).astype(np.uint32).ravel().view(np.int32)).to(dev)
+    sl_fill = torch.zeros(1, device=dev)
 
     ops = [
         ("pre_emphasis_filter", lambda: audio.pre_emphasis_filter(x, sd, pre, sd, lens, coeff, 0, h)),
@@ -90,6 +95,8 @@ def main():
                                                                          512, 2, 400, 160, audio.TC_BF16_HILO3, h)),
         ("frontend_host (pinned host tensors)", lambda: audio.frontend_host(x_host, sd, out_host, md, lens_host,
                                                                             coeff_host, p, 0, h)),
+        ("slice (1-D, anchor 10, length/2)", lambda: audio.slice(x, gd, pre, gd, sl_anchor, sl_shape, sl_fill, True,
+                                                                 sl_roi, h)),
         ("to_decibels_gpu_static (8 clips)", lambda: L_.rppt_to_decibels_gpu_static(
             mel.data_ptr(), ctypes.byref(sd_small), db_small.data_ptr(), ctypes.byref(sd_small),
             dims_small.data_ptr(), ctypes.c_float(-80.0), ctypes.c_float(10.0), ctypes.c_float(0.0),

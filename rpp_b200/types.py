@@ -204,3 +204,25 @@ class RppbServerConfig(ctypes.Structure):
 class RppbCompletion(ctypes.Structure):
     """include/rppb_server.h: one finished request (steady-clock nanoseconds)."""
     _fields_ = [("id", ctypes.c_uint64), ("submitNs", ctypes.c_int64), ("finishNs", ctypes.c_int64)]
+
+
+class RpptGenericDesc(ctypes.Structure):
+    """include/rppdefs.h RpptGenericDesc (api/rppdefs.h:591-602): dims[0] is the batch."""
+    _fields_ = [("numDims", ctypes.c_size_t), ("offsetInBytes", ctypes.c_uint32), ("dataType", ctypes.c_int),
+                ("dims", ctypes.c_uint32 * 5), ("strides", ctypes.c_uint32 * 5), ("layout", ctypes.c_int)]
+
+
+def generic_desc(shape, dtype=None, layout=None):
+    """Dense generic descriptor of a [n, d1, ...] tensor (numDims = len(shape))."""
+    d = RpptGenericDesc()
+    d.numDims = len(shape)
+    d.offsetInBytes = 0
+    d.dataType = int(RpptDataType.F32 if dtype is None else dtype)
+    for i, v in enumerate(shape):
+        d.dims[i] = int(v)
+    st = 1
+    for i in range(len(shape) - 1, -1, -1):
+        d.strides[i] = st
+        st *= int(shape[i])
+    d.layout = int(RpptLayout.NCHW if layout is None else layout)
+    return d

@@ -31,6 +31,20 @@ def reference():
 
 
 @pytest.fixture(scope="session")
+def reference_or_none():
+    """The reference's host library when it is built (or buildable), else None."""
+    from oracle import Reference, build_reference, reference_lib_path
+    if not os.path.isfile(reference_lib_path()):
+        try:
+            build_reference()
+        except Exception:
+            return None
+    if not os.path.isfile(reference_lib_path()):
+        return None
+    return Reference(threads=min(8, os.cpu_count() or 1))
+
+
+@pytest.fixture(scope="session")
 def golden():
     import numpy as np
     return np.load(os.path.join(ROOT, "tests", "golden", "reference_audio_qa.npz"))

@@ -32,7 +32,7 @@ def main():
     for i, p in enumerate(pcm):
         out[f"pcm{i}"] = p
     gold = os.path.join(SUITE, "REFERENCE_OUTPUTS_AUDIO")
-    for op in ("pre_emphasis_filter", "to_decibels", "spectrogram", "mel_filter_bank", "resample"):
+    for op in ("pre_emphasis_filter", "to_decibels", "spectrogram", "mel_filter_bank", "resample", "slice"):
         out[op] = np.fromfile(os.path.join(gold, op, op + ".bin"), dtype="<f4")
     out["nsr_begin"] = np.array([0, 0, 0], dtype=np.int32)
     out["nsr_length"] = np.array([35840, 33680, 34160], dtype=np.int32)

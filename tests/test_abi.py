@@ -63,6 +63,8 @@ int main() {
   std::printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(RpptDesc), offsetof(RpptDesc, strides), offsetof(RpptDesc, layout),
               sizeof(RpptImagePatch), sizeof(RpptResamplingWindow), offsetof(RpptResamplingWindow, lookup),
               offsetof(RpptResamplingWindow, pCenter));
+  std::printf("%zu %zu %zu %zu\n", sizeof(RpptGenericDesc), offsetof(RpptGenericDesc, dims),
+              offsetof(RpptGenericDesc, strides), offsetof(RpptGenericDesc, layout));
   std::printf("%d %d %d %d %d %d %d %d\n", (int)RPP_ERROR_INVALID_AXIS, (int)RPP_ERROR_OUT_OF_BOUND_SCRATCH_MEMORY_SIZE,
               (int)NFT, (int)NTF, (int)REFLECT, (int)HTK, (int)F32, (int)RPP_HIP_BACKEND);
   return 0;
@@ -90,6 +92,9 @@ def test_header_layout_matches_ctypes():
     assert sizes[4] == ctypes.sizeof(T.RpptResamplingWindow)
     assert sizes[5] == T.RpptResamplingWindow.lookup.offset
     assert sizes[6] == T.RpptResamplingWindow.pCenter.offset
+    g = [int(v) for v in out[1].split()]
+    assert g == [ctypes.sizeof(T.RpptGenericDesc), T.RpptGenericDesc.dims.offset, T.RpptGenericDesc.strides.offset,
+                 T.RpptGenericDesc.layout.offset]
 
 
 def test_header_layout_matches_reference():

@@ -432,3 +432,77 @@ def test_downmix_resample_equals_two_calls(gpu, channels, normalize):
     assert audio.downmix_resample(xd, audio_desc(n, L, channels=channels, num_dims=3), out, audio_desc(n, out_len),
                                   ir, orr, dims, normalize, lut_d, scale, center, lobes, gpu) == OK
     np.testing.assert_array_equal(host(out), host(ref))
+
+
+# ---------------------------------------------------------------- slice (api/rppt_tensor_geometric_augmentations.h:486)
+
+def test_slice_golden_case(gpu, oracle, golden):
+    """The audio QA slice (1-D, anchor 10, shape length/2, roi {10, length}, padding with fill 0)
+    through the C ABI equals the oracle on every element the call writes."""
+    from rpp_b200.types import generic_desc
+    lens = golden["lengths"].astype(np.int32)
+    n = len(lens)
+    w = (int(lens.max()) // 8) * 8 + 8
+    x = np.zeros((n, w), np.float32)
+    for i in range(n):
+        x[i, :lens[i]] = golden[f"pcm{i}"].astype(np.float32) / 32768.0
+    anchor = np.full(n, 10, np.int32)
+    shape = (lens // 2).astype(np.int32)
+    roi = np.stack([np.full(n, 10), lens], 1).astype(np.uint32).ravel()
+    d = generic_desc((n, w))
+    out = torch.full((n, w), -7.0, device="cuda")
+    fill = np.zeros(1, np.float32)
+    assert audio.slice(dev(x), d, out, d, anchor, shape, fill, True, roi, gpu) == RppStatus.RPP_SUCCESS
+    exp = np.full((n, w), -7.0, np.float32)
+    oracle.slice(x, exp, anchor, shape, roi, 0.0, True, 1)
+    np.testing.assert_array_equal(host(out), exp)
+
+
+@pytest.mark.parametrize("num_dims", [1, 2])
+@pytest.mark.parametrize("dtype", [np.float32, np.uint8])
+@pytest.mark.parametrize("pad", [False, True])
+def test_slice_vs_oracle(gpu, oracle, num_dims, dtype, pad):
+    """Random boxes, some past the roi lengths (padding), some with anchors beyond the length
+    (nothing copied), per-sample tensors in pageable, pinned and device memory."""
+    from rpp_b200.types import generic_desc, RpptDataType
+    r = np.random.Generator(np.random.PCG64(77 + num_dims))
+    n = 9
+    shp = (n, 20000) if num_dims == 1 else (n, 33, 70)
+    src = (r.integers(0, 255, shp).astype(np.uint8) if dtype == np.uint8
+           else r.standard_normal(shp).astype(np.float32))
+    ext = np.array(shp[1:])
+    length = np.stack([r.integers(1, e + 1, n) for e in ext], 1).astype(np.int32)
+    anchor = np.stack([r.integers(0, e, n) for e in ext], 1).astype(np.int32)
+    shape = np.stack([r.integers(1, e + 1, n) for e in ext], 1).astype(np.int32)
+    roi = np.concatenate([np.zeros_like(length), length], 1).astype(np.uint32).ravel()
+    fill = np.array([5 if dtype == np.uint8 else -2.5], dtype)
+    dt = RpptDataType.U8 if dtype == np.uint8 else RpptDataType.F32
+    d = generic_desc(shp, dt)
+    canvas_v = 9 if dtype == np.uint8 else 9.75
+    out = torch.from_numpy(np.full(shp, canvas_v, dtype)).cuda()
+    a_t, s_t = anchor.ravel(), shape.ravel()
+    args = [(a_t, s_t, roi), (pinned(a_t), pinned(s_t), pinned(roi)), (dev(a_t), dev(s_t), dev(roi))]
+    for k, (aa, ss, rr) in enumerate(args):
+        out.fill_(canvas_v)
+        st = audio.slice(dev(src), d, out, d, aa, ss, fill, pad, rr, gpu)
+        assert st == RppStatus.RPP_SUCCESS
+        exp = np.full(shp, canvas_v, dtype)
+        oracle.slice(src, exp, a_t, s_t, roi, fill[0], pad, num_dims)
+        np.testing.assert_array_equal(host(out), exp)
+
+
+def test_slice_status_codes(gpu):
+    from rpp_b200.types import generic_desc, RpptDataType, RpptLayout
+    x = torch.zeros((2, 100), device="cuda")
+    a = np.zeros(2, np.int32)
+    s = np.full(2, 10, np.int32)
+    roi = np.array([0, 100, 0, 100], np.uint32)
+    f = np.zeros(1, np.float32)
+    d = generic_desc((2, 100))
+    bad = generic_desc((2, 100), RpptDataType.F16)
+    assert audio.slice(x, bad, x, d, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_INVALID_SRC_DATATYPE
+    assert audio.slice(x, d, x, bad, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_INVALID_DST_DATATYPE
+    other = generic_desc((2, 100), layout=RpptLayout.NHWC)
+    assert audio.slice(x, d, x, other, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_LAYOUT_MISMATCH
+    d4 = generic_desc((2, 1, 10, 10))
+    assert audio.slice(x, d4, x, d4, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_NOT_IMPLEMENTED

@@ -124,3 +124,33 @@ def test_reference_library_golden(reference, golden):
     gold = golden["to_decibels"].reshape(N, d.w)
     for i in range(N):
         np.testing.assert_array_equal(db[i, :lens[i]], gold[i, :lens[i]])
+
+
+def slice_qa_args(lens):
+    """The audio QA slice (utilities/test_suite/HOST/Tensor_audio_host.cpp:290-313): 1-D, anchor 10,
+    shape length/2, roi {10, length}, padding on with fill 0."""
+    anchor = np.full(N, 10, np.int32)
+    shape = (lens // 2).astype(np.int32)
+    roi = np.stack([np.full(N, 10), lens], 1).astype(np.uint32).ravel()
+    return anchor, shape, roi
+
+
+def test_slice_golden(oracle, reference_or_none, golden):
+    """slice.bin holds each sample's copied run, then zeros up to length/2 (the width the QA compares).  Its runs are 17920, 16832 and
+    17064 samples long where length/2 of the QA WAVs gives 17920, 16840 and 17080: the golden was
+    evidently made from inputs 16 and 32 samples shorter for samples 2 and 3 (the reference's own
+    host library, built here, differs from it in exactly those tails).  The oracle is pinned on the
+    golden's runs and, where the library is built, against the library on the whole output."""
+    src, lens, d = qa_inputs(golden)
+    anchor, shape, roi = slice_qa_args(lens)
+    dst = np.zeros_like(src)
+    oracle.slice(src, dst, anchor, shape, roi, 0.0, True, 1)
+    gold = golden["slice"].reshape(N, d.w)
+    runs = [17920, 16832, 17064]
+    for i in range(N):
+        np.testing.assert_array_equal(dst[i, :runs[i]], gold[i, :runs[i]])
+        assert not gold[i, runs[i]:shape[i]].any()   # within the compared width
+    if reference_or_none is not None:
+        ref = np.zeros_like(src)
+        reference_or_none.slice(src, ref, anchor, shape, roi, 0.0, True, 1)
+        np.testing.assert_array_equal(dst, ref)

@@ -149,3 +149,32 @@ def test_spectrogram_f64_vs_reference(oracle, reference, nfft, W, hop, center, r
         e = o[i, :, :F[i]] if nft else o[i, :F[i], :].T
         scale = np.maximum(g.max(axis=0, keepdims=True), 1e-30)
         assert (np.abs(e - g) / scale).max() < 2e-6
+
+
+@pytest.mark.parametrize("num_dims", [1, 2])
+@pytest.mark.parametrize("dtype", [np.float32, np.uint8])
+@pytest.mark.parametrize("pad", [False, True])
+def test_slice(oracle, reference, num_dims, dtype, pad):
+    """Boxes inside and overlapping the roi lengths (padding needed), both element types."""
+    r = rng(50 + num_dims)
+    n = 7
+    shape_t = (n, 3000) if num_dims == 1 else (n, 40, 64)
+    if dtype == np.uint8:
+        src = r.integers(0, 255, shape_t).astype(np.uint8)
+    else:
+        src = r.standard_normal(shape_t).astype(np.float32)
+    ext = np.array(shape_t[1:])
+    length = np.stack([r.integers(e // 2, e + 1, n) for e in ext], 1).astype(np.int32)
+    # anchors stay below the roi lengths: beyond them the reference copies a negative length
+    # converted to unsigned (slice.cpp:203-204), i.e. crashes
+    anchor = np.stack([r.integers(0, e // 2, n) for e in ext], 1).astype(np.int32)
+    shape = np.stack([r.integers(1, e, n) for e in ext], 1).astype(np.int32)
+    anchor[0] = 0
+    shape[1] = ext - anchor[1]        # reaches past a short roi: padding
+    roi = np.concatenate([np.zeros_like(length), length], 1).astype(np.uint32)
+    fill = 7 if dtype == np.uint8 else -3.5
+    a = np.full_like(src, 9 if dtype == np.uint8 else 9.25)
+    b = a.copy()
+    oracle.slice(src, a, anchor.ravel(), shape.ravel(), roi.ravel(), fill, pad, num_dims)
+    reference.slice(src, b, anchor.ravel(), shape.ravel(), roi.ravel(), fill, pad, num_dims)
+    np.testing.assert_array_equal(a, b)
