@@ -28,12 +28,12 @@ printf '#pragma once\n#define RPP_LEGACY_SUPPORT 0\n' > "$GEN/rpp_legacy_support
 cat > "$GEN/half/half.hpp" <<'H'
 #pragma once
 #include <cstdint>
-namespace half_float { struct half { std::uint16_t bits; half() : bits(0) {} explicit half(float) : bits(0) {} operator float() const { return 0.f; } }; }
+namespace half_float { struct half { std::uint16_t bits; half() : bits(0) {} explicit half(float) : bits(0) {} half& operator=(float) { bits = 0; return *this; } operator float() const { return 0.f; } }; }
 H
 INC=(-I"$GEN" -I"$RPP_REF/api" -I"$RPP_REF/src/include/common" -I"$RPP_REF/src/include/common/cpu"
      -I"$RPP_REF/src/include/tensor" -I"$RPP_REF/third_party/ffts/include")
 COMMON=(-O3 -DNDEBUG -DAUDIO_SUPPORT -fopenmp -mavx2 -mf16c -std=gnu++17 -fPIC -w)
-KERNELS=(non_silent_region_detection to_decibels pre_emphasis_filter down_mixing spectrogram mel_filter_bank resample slice)
+KERNELS=(non_silent_region_detection to_decibels pre_emphasis_filter down_mixing spectrogram mel_filter_bank resample slice normalize)
 OBJS=()
 CXX="${CXX:-g++}"
 # some gcc installs on PATH lack libgomp.spec; point -B at a gcc lib dir that has it

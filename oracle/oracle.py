@@ -109,6 +109,9 @@ class Oracle:
                                              ctypes.c_double, ctypes.c_double]
         L.oracle_nsr.argtypes = [_F32P, _L, _I, _I32P, _I32P, _I32P, _F, _I, _F, _I, _F32P, _F32P]
         L.oracle_windowed_sinc.argtypes = [_I, _I, _F32P, _F32P]
+        L.oracle_normalize_2d.argtypes = [_F32P, _L, _L, _F32P, _L, _L, _I, ctypes.c_uint, _F32P, _F32P, _I, _F, _F,
+                                          _U32P]
+        L.oracle_normalize_2d.restype = _I
         L.oracle_slice.argtypes = [ctypes.c_void_p, _L, _L, ctypes.c_void_p, _L, _L, _I, _I, _I32P, _I32P, _U32P,
                                    ctypes.c_void_p, _I, _I]
 
@@ -220,6 +223,17 @@ class Oracle:
                                         _p(np.ascontiguousarray(rows, np.int32), _I32P),
                                         _p(np.ascontiguousarray(cols, np.int32), _I32P), float(cutoff_db),
                                         float(multiplier), float(ref_mag))
+        return dst
+
+    def normalize_2d(self, src, dst, axis_mask, mean, std, compute, scale, shift, roi):
+        """src/dst float32 [n][rows][cols]; mean/std float32 arrays updated in place as the
+        reference does; roi uint32 n*4 (begin0, begin1, length0, length1).  Returns dst."""
+        n, R, C = src.shape
+        st = self.lib.oracle_normalize_2d(_p(src, _F32P), R * C, C, _p(dst, _F32P), dst.shape[1] * dst.shape[2],
+                                          dst.shape[2], n, int(axis_mask), _p(mean, _F32P), _p(std, _F32P),
+                                          int(compute), float(scale), float(shift),
+                                          _p(np.ascontiguousarray(roi, np.uint32), _U32P))
+        assert st == 0
         return dst
 
     def slice(self, src, dst, anchor, shape, roi, fill, enable_padding, num_dims):
@@ -366,3 +380,20 @@ def _reference_slice(self, src, dst, anchor, shape, roi, fill, enable_padding, n
 
 
 Reference.slice = _reference_slice
+
+
+def _reference_normalize_2d(self, src, dst, axis_mask, mean, std, compute, scale, shift, roi):
+    """The reference's host normalize (F32, 2-D) on the same arrays as Oracle.normalize_2d."""
+    from rpp_b200.types import generic_desc
+    sd, dd = generic_desc(src.shape), generic_desc(dst.shape)
+    L = self.lib
+    L.ref_normalize_f32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint,
+                                    _F32P, _F32P, ctypes.c_ubyte, _F, _F, _U32P, ctypes.c_void_p]
+    st = L.ref_normalize_f32(src.ctypes.data, ctypes.addressof(sd), dst.ctypes.data, ctypes.addressof(dd),
+                             int(axis_mask), _p(mean, _F32P), _p(std, _F32P), int(compute), float(scale), float(shift),
+                             _p(np.ascontiguousarray(roi, np.uint32), _U32P), self.h)
+    assert st == 0, st
+    return dst
+
+
+Reference.normalize_2d = _reference_normalize_2d

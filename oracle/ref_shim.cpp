@@ -67,4 +67,18 @@ __attribute__((visibility("default"))) int ref_slice_u8(unsigned char* src, Rppt
     rpp::Handle& handle = *static_cast<rpp::Handle*>(static_cast<rppHandle_t>(h));
     return slice_host_tensor<Rpp8u>(src, srcDesc, dst, dstDesc, anchor, shape, fill, enablePadding, roi, lp, handle);
 }
+
+// The reference's host normalize for F32 (src/modules/tensor/cpu/kernel/normalize.cpp:507-767),
+// called at the kernel level for the same reason as slice; the 2-D branch reads no layout
+// parameters.
+__attribute__((visibility("default"))) int ref_normalize_f32(float* src, RpptGenericDesc* srcDesc, float* dst,
+                                                             RpptGenericDesc* dstDesc, unsigned axisMask, float* mean,
+                                                             float* stdDev, unsigned char computeMeanStddev, float scale,
+                                                             float shift, unsigned* roi, void* h)
+{
+    RppLayoutParams lp{};
+    rpp::Handle& handle = *static_cast<rpp::Handle*>(static_cast<rppHandle_t>(h));
+    return normalize_f32_f32_host_tensor(src, srcDesc, dst, dstDesc, axisMask, mean, stdDev, computeMeanStddev, scale,
+                                         shift, roi, lp, handle);
+}
 }

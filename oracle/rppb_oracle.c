@@ -713,3 +713,169 @@ EXPORT void oracle_slice(const void *src, long srcStride0, long srcStride1, void
         }
     }
 }
+
+/* ---------------------------------------------------------------- normalize (2-D, F32)
+ * src/modules/tensor/cpu/kernel/normalize.cpp:29-120 (recursive sums, inverse std dev), :417-470
+ * (normalize_2D_tensor) and :507-600 (the 2-D branch of normalize_f32_f32_host_tensor);
+ * rpp_rsqrt_sse / rpp_rsqrt_ps of src/include/common/cpu/rpp_cpu_simd_math.hpp:870-930, restated
+ * with the same SSE reciprocal-square-root instruction so that the restatement matches the
+ * reference on the same CPU.  mean / stdDev are in-out arrays as in the reference: computed
+ * values are written into them; with computeMeanStddev == 0 the caller's stdDev values are
+ * replaced by scale / stdDev (1 where 0) for the first maxSize entries. */
+#include <immintrin.h>
+
+static void n_sum(float *out, const float *in, int stride, int n)
+{
+    if (n > 32)
+    {
+        int h = n >> 1;
+        float t1 = 0, t2 = 0;
+        n_sum(&t1, in, stride, h);
+        n_sum(&t2, in + h * stride, stride, n - h);
+        t1 += t2;
+        *out += t1;
+    }
+    else
+    {
+        float t = 0;
+        for (int i = 0; i < n; i++) t += in[i * stride];
+        *out += t;
+    }
+}
+
+static void n_dsq(float *out, const float *in, int stride, int n, float mean)
+{
+    if (n > 32)
+    {
+        int h = n >> 1;
+        float t1 = 0, t2 = 0;
+        n_dsq(&t1, in, stride, h, mean);
+        n_dsq(&t2, in + h * stride, stride, n - h, mean);
+        t1 += t2;
+        *out += t1;
+    }
+    else
+    {
+        float t = 0;
+        for (int i = 0; i < n; i++)
+        {
+            float c = in[i * stride] - mean;
+            float c2 = c * c;
+            t += c2;
+        }
+        *out += t;
+    }
+}
+
+static float n_rsqrt_ps(float x)
+{
+    float y = _mm_cvtss_f32(_mm_rsqrt_ss(_mm_set_ss(x)));
+    return y * (1.5f - x * 0.5f * y * y);
+}
+
+static void n_rsqrt_sse(float *v, long n, float rdiv, float mul)
+{
+    long i = 0;
+    __m128 r4 = _mm_set1_ps(rdiv), m4 = _mm_set1_ps(mul * 0.5f), three = _mm_set1_ps(3.0f), zero = _mm_set1_ps(0.0f);
+    for (; i + 4 <= n; i += 4)
+    {
+        __m128 x = _mm_mul_ps(_mm_loadu_ps(v + i), r4);
+        __m128 mask = _mm_cmpneq_ps(x, zero);
+        __m128 y = _mm_and_ps(_mm_rsqrt_ps(x), mask);
+        __m128 y2 = _mm_mul_ps(y, y);
+        __m128 xy2 = _mm_mul_ps(x, y2);
+        y = _mm_mul_ps(y, _mm_sub_ps(three, xy2));
+        y = _mm_mul_ps(y, m4);
+        _mm_storeu_ps(v + i, y);
+    }
+    for (; i < n; i++)
+    {
+        float x = v[i] * rdiv;
+        v[i] = x ? n_rsqrt_ps(x) * mul : 0;
+    }
+}
+
+/* src/dst: [n][srcStride0] samples with row stride stride1 (elements); roi: n * 4 (begin0, begin1,
+ * length0, length1; the begins are not read).  Returns 0, or -1 for an axisMask other than 1..3. */
+EXPORT int oracle_normalize_2d(const float *src, long srcStride0, long srcStride1, float *dst, long dstStride0,
+                               long dstStride1, int n, unsigned axisMask, float *mean, float *stdDev, int computeMeanStddev,
+                               float scale, float shift, const unsigned *roi)
+{
+    if (axisMask < 1 || axisMask > 3) return -1;
+    unsigned maxSize = 1;
+    for (int b = 0; b < n; b++)
+    {
+        unsigned size = 1;
+        for (int i = 0; i < 2; i++) size *= (axisMask & (1u << i)) ? 1 : roi[4 * b + 2 + i];
+        if (size > maxSize) maxSize = size;
+    }
+    if (!computeMeanStddev)
+    {
+        for (unsigned i = 0; i < maxSize; i++) stdDev[i] = (!stdDev[i]) ? 1.0f : scale / stdDev[i];
+        maxSize = 0;
+    }
+    for (int b = 0; b < n; b++)
+    {
+        const unsigned *length = roi + 4 * b + 2;
+        const float *s = src + (long)b * srcStride0;
+        float *d = dst + (long)b * dstStride0;
+        float *mn = mean + (long)b * maxSize, *sd = stdDev + (long)b * maxSize;
+        for (long i = 0; i < dstStride0; i++) d[i] = 0.0f;
+        int stride[2], red[2], ps[2];
+        if (axisMask == 3) { stride[0] = stride[1] = 1; red[0] = 1; red[1] = length[0] * length[1]; ps[0] = ps[1] = 0; }
+        else if (axisMask == 1) { stride[0] = (int)srcStride1; stride[1] = 1; red[0] = length[1]; red[1] = length[0]; ps[0] = 1; ps[1] = 0; }
+        else { stride[0] = 1; stride[1] = (int)srcStride1; red[0] = length[0]; red[1] = length[1]; ps[0] = 0; ps[1] = 1; }
+        if (computeMeanStddev & 1)
+        {
+            float nf = (float)(1.0 / red[1]);
+            const float *p = s;
+            for (int i = 0; i < red[0]; i++)
+            {
+                mn[i] = 0;
+                n_sum(&mn[i], p, stride[0], red[1]);
+                p += stride[1];
+                mn[i] *= nf;
+            }
+        }
+        if (computeMeanStddev & 2)
+        {
+            float nf = (float)(1.0 / red[1]);
+            const float *p = s;
+            for (int i = 0; i < red[0]; i++)
+            {
+                sd[i] = 0;
+                n_dsq(&sd[i], p, stride[0], red[1], mn[i]);
+                p += stride[1];
+            }
+            n_rsqrt_sse(sd, red[0], nf, scale);
+        }
+        if (ps[1])
+        {
+            for (unsigned i = 0; i < length[0]; i++)
+            {
+                const float *sr = s + i * srcStride1;
+                float *dr = d + i * dstStride1;
+                float m = mn[i], iv = sd[i];
+                for (unsigned j = 0; j < length[1]; j++) dr[j] = (sr[j] - m) * iv + shift;
+            }
+        }
+        else
+        {
+            int pi = 0;
+            const float *sr = s;
+            float *dr = d;
+            for (unsigned i = 0; i < length[0]; i++)
+            {
+                for (unsigned j = 0; j < length[1]; j++)
+                {
+                    dr[j] = (sr[j] - mn[pi]) * sd[pi] + shift;
+                    pi += ps[0];
+                }
+                pi = (!ps[1]) ? 0 : pi + ps[1];
+                sr += srcStride1;
+                dr += dstStride1;
+            }
+        }
+    }
+    return 0;
+}

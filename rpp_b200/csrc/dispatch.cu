@@ -20,6 +20,7 @@
 #include "../../include/rppb_frontend.h"
 #include "../../include/rppt_tensor_audio_augmentations.h"
 #include "../../include/rppt_tensor_geometric_augmentations.h"
+#include "../../include/rppt_tensor_statistical_operations.h"
 #include "handle.hpp"
 #include "ops.hpp"
 
@@ -887,6 +888,147 @@ extern "C" SHARED_PUBLIC RppStatus rppt_slice_gpu(RppPtr_t srcPtr, RpptGenericDe
         const void* fill = enablePadding ? h.device_view(fillValue, size_t(eb), fStage) : nullptr;
         const size_t off = sd.offsetInBytes, doff = dd.offsetInBytes;
         launch_slice(h, a, static_cast<const char*>(srcPtr) + off, static_cast<char*>(dstPtr) + doff, fill);
+        return RPP_SUCCESS;
+    });
+}
+
+extern "C" SHARED_PUBLIC RppStatus rppt_normalize_gpu(RppPtr_t srcPtr, RpptGenericDescPtr srcGenericDescPtr,
+                                                      RppPtr_t dstPtr, RpptGenericDescPtr dstGenericDescPtr,
+                                                      Rpp32u axisMask, Rpp32f* meanTensor, Rpp32f* stdDevTensor,
+                                                      Rpp8u computeMeanStddev, Rpp32f scale, Rpp32f shift,
+                                                      Rpp32u* roiTensor, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcGenericDescPtr && dstGenericDescPtr, "null descriptor");
+        const RpptGenericDesc& sd = *srcGenericDescPtr;
+        const RpptGenericDesc& dd = *dstGenericDescPtr;
+        // built: the audio path's 2-D F32 tensors (normalize.cpp's tensorDims == 2 branch)
+        if (sd.dataType != F32 || dd.dataType != F32) return RPP_ERROR_NOT_IMPLEMENTED;
+        if (sd.numDims != 3 || dd.numDims != 3) return RPP_ERROR_NOT_IMPLEMENTED;
+        if (axisMask < 1 || axisMask > 3) return RPP_ERROR_INVALID_ARGUMENTS;
+        require(srcPtr && dstPtr && roiTensor && meanTensor && stdDevTensor, "null tensor");
+        const int n = int(dd.dims[0]);
+        if (n <= 0) return RPP_SUCCESS;
+        const int compute = computeMeanStddev & 3;
+        // roi lengths are needed on the host (parameter counts, work list)
+        std::vector<uint32_t> roi(size_t(n) * 4);
+        cudaPointerAttributes attr{};
+        if (cudaPointerGetAttributes(&attr, roiTensor) == cudaSuccess && attr.type == cudaMemoryTypeDevice)
+        {
+            check_cuda(cudaMemcpyAsync(roi.data(), roiTensor, roi.size() * 4, cudaMemcpyDeviceToHost, h.stream()),
+                       "cudaMemcpyAsync(roi)");
+            check_cuda(cudaStreamSynchronize(h.stream()), "cudaStreamSynchronize(roi)");
+        }
+        else
+        {
+            cudaGetLastError();
+            std::memcpy(roi.data(), roiTensor, roi.size() * 4);
+        }
+        int maxSize = 1;
+        std::vector<NormalizeSample> samples(n);
+        std::vector<int4> tasks;
+        for (int b = 0; b < n; ++b)
+        {
+            const uint32_t l0 = roi[4 * b + 2], l1 = roi[4 * b + 3];
+            int size = 1;
+            if (!(axisMask & 1)) size *= int(l0);
+            if (!(axisMask & 2)) size *= int(l1);
+            maxSize = std::max(maxSize, size);
+            NormalizeSample& s = samples[b];
+            s.len0 = int(std::min(l0, sd.dims[1]));
+            s.len1 = int(std::min(l1, sd.dims[2]));
+            int params;
+            if (axisMask == 3)
+            {
+                s.count = s.len0 * s.len1;
+                s.elemStride = int(sd.strides[2]);
+                s.paramStride = 0;
+                params = 1;
+            }
+            else if (axisMask == 1)
+            {
+                s.count = s.len0;
+                s.elemStride = int(sd.strides[1]);
+                s.paramStride = int(sd.strides[2]);
+                params = s.len1;
+            }
+            else
+            {
+                s.count = s.len1;
+                s.elemStride = int(sd.strides[2]);
+                s.paramStride = int(sd.strides[1]);
+                params = s.len0;
+            }
+            s.normFactor = float(1.0 / double(s.count));
+            if (compute)
+            {
+                if (s.count >= 2048)
+                    for (int p = 0; p < params; ++p) tasks.push_back(make_int4(b, p, 1, 1));
+                else
+                    for (int p = 0; p < params; p += 32) tasks.push_back(make_int4(b, p, std::min(32, params - p), 0));
+            }
+        }
+        const size_t perAll = size_t(n) * maxSize;
+        const size_t meanInCount = compute == 0 ? size_t(maxSize) : perAll;
+        Carver m(nullptr);
+        m.take<NormalizeSample>(n);
+        m.take<int4>(tasks.size());
+        m.take<float>(perAll);
+        m.take<float>(perAll);
+        m.take<float>(maxSize);
+        m.take<float>(meanInCount);
+        m.take<float>(meanInCount);
+        Carver cv(h.workspace(m.used()));
+        NormalizeSample* dSamples = cv.take<NormalizeSample>(n);
+        int4* dTasks = cv.take<int4>(tasks.size());
+        float* meanOut = cv.take<float>(perAll);
+        float* invOut = cv.take<float>(perAll);
+        float* inverted = cv.take<float>(maxSize);
+        float* meanStage = cv.take<float>(meanInCount);
+        float* stdStage = cv.take<float>(meanInCount);
+        h.upload(dSamples, samples.data(), samples.size() * sizeof(NormalizeSample));
+        if (!tasks.empty()) h.upload(dTasks, tasks.data(), tasks.size() * sizeof(int4));
+        NormalizeArgs a;
+        a.src = reinterpret_cast<const float*>(static_cast<const char*>(srcPtr) + sd.offsetInBytes);
+        a.dst = reinterpret_cast<float*>(static_cast<char*>(dstPtr) + dd.offsetInBytes);
+        a.n = n;
+        a.srcStride0 = sd.strides[0];
+        a.srcStride1 = sd.strides[1];
+        a.srcStride2 = sd.strides[2];
+        a.dstStride0 = dd.strides[0];
+        a.dstStride1 = dd.strides[1];
+        if (a.dstStride1 == 0) return RPP_ERROR_INVALID_ARGUMENTS;
+        a.axisMask = axisMask;
+        a.compute = compute;
+        a.scale = scale;
+        a.shift = shift;
+        a.maxSize = maxSize;
+        a.samples = dSamples;
+        a.meanIn = (compute & 1) ? nullptr
+                                 : static_cast<const float*>(h.device_view(meanTensor, meanInCount * 4, meanStage));
+        a.meanOut = meanOut;
+        a.invOut = invOut;
+        const float* stdIn = (compute & 2) ? nullptr
+                                           : static_cast<const float*>(h.device_view(stdDevTensor, meanInCount * 4,
+                                                                                     stdStage));
+        const float* meanEff = (compute & 1) ? meanOut : a.meanIn;
+        const float* invEff = (compute & 2) ? invOut : compute == 0 ? inverted : stdIn;
+        // entries past a sample's parameter count keep the caller's values, as in the reference
+        if (compute & 1)
+            check_cuda(cudaMemcpyAsync(meanOut, meanTensor, perAll * 4, cudaMemcpyDefault, h.stream()),
+                       "cudaMemcpyAsync(mean in)");
+        if (compute & 2)
+            check_cuda(cudaMemcpyAsync(invOut, stdDevTensor, perAll * 4, cudaMemcpyDefault, h.stream()),
+                       "cudaMemcpyAsync(stdDev in)");
+        launch_normalize(h, a, dTasks, int(tasks.size()), meanEff, invEff, compute == 0 ? 0 : maxSize, stdIn,
+                         inverted, compute == 0 ? maxSize : 0);
+        // computed statistics go back to the caller's arrays, as the reference writes them
+        if (compute & 1)
+            check_cuda(cudaMemcpyAsync(meanTensor, meanOut, perAll * 4, cudaMemcpyDefault, h.stream()),
+                       "cudaMemcpyAsync(mean)");
+        if (compute & 2)
+            check_cuda(cudaMemcpyAsync(stdDevTensor, invOut, perAll * 4, cudaMemcpyDefault, h.stream()),
+                       "cudaMemcpyAsync(stdDev)");
         return RPP_SUCCESS;
     });
 }

@@ -155,6 +155,34 @@ struct SliceArgs
 };
 void launch_slice(Handle& h, const SliceArgs& a, const void* src, void* dst, const void* fill);
 
+// normalize (normalize.cu): 2-D F32, per-sample roi lengths.
+struct NormalizeSample
+{
+    int len0, len1;          // roi lengths (rows, columns)
+    int count;               // elements per parameter
+    int elemStride;          // stride between a parameter's elements
+    int paramStride;         // stride between consecutive parameters
+    float normFactor;        // float(1.0 / count)
+};
+struct NormalizeArgs
+{
+    const float* src;
+    float* dst;
+    int n;
+    uint32_t srcStride0, srcStride1, srcStride2, dstStride0, dstStride1;
+    unsigned axisMask;
+    int compute;             // computeMeanStddev
+    float scale, shift;
+    int maxSize;             // parameters per sample in the mean / std arrays
+    const NormalizeSample* samples;   // device, n
+    const float* meanIn;     // caller's means (device view) when not computed
+    float* meanOut;          // computed means, n * maxSize
+    float* invOut;           // computed inverse std devs, n * maxSize
+};
+void launch_normalize(Handle& h, const NormalizeArgs& a, const int4* tasks, int numTasks, const float* meanEff,
+                      const float* invEff, int paramOffsetPerSample, const float* stdToInvert, float* invertOut,
+                      int invertCount);
+
 // PCIe movers over mapped pinned host memory (host_io.cu).
 void launch_host_gather(cudaStream_t stream, const float* src, size_t nStride, const int* len, int clips, float* dst,
                         uint32_t dstStride, int ctas);

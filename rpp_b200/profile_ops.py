@@ -73,6 +73,11 @@ def main():
     sl_shape = torch.from_numpy((lens_np // 2).astype(np.int32)).to(dev)
     sl_roi = torch.from_numpy(np.stack([np.full(n, 10), lens_np], 1).astype(np.uint32).ravel().view(np.int32)).to(dev)
     sl_fill = torch.zeros(1, device=dev)
+    nd = generic_desc((n, 128, mf))
+    n_roi = torch.from_numpy(np.stack([np.zeros(n), np.zeros(n), np.full(n, 128), F], 1).astype(np.uint32).ravel()
+                             .view(np.int32))
+    n_mean, n_std = torch.zeros(n * 128, device=dev), torch.zeros(n * 128, device=dev)
+    n_out = torch.empty_like(db)
 
     ops = [
         ("pre_emphasis_filter", lambda: audio.pre_emphasis_filter(x, sd, pre, sd, lens, coeff, 0, h)),
@@ -97,6 +102,8 @@ def main():
                                                                             coeff_host, p, 0, h)),
         ("slice (1-D, anchor 10, length/2)", lambda: audio.slice(x, gd, pre, gd, sl_anchor, sl_shape, sl_fill, True,
                                                                  sl_roi, h)),
+        ("normalize (per filter over time)", lambda: audio.normalize(db, nd, n_out, nd, 2, n_mean, n_std, 3, 1.0, 0.0,
+                                                                     n_roi, h)),
         ("to_decibels_gpu_static (8 clips)", lambda: L_.rppt_to_decibels_gpu_static(
             mel.data_ptr(), ctypes.byref(sd_small), db_small.data_ptr(), ctypes.byref(sd_small),
             dims_small.data_ptr(), ctypes.c_float(-80.0), ctypes.c_float(10.0), ctypes.c_float(0.0),

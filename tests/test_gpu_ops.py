@@ -506,3 +506,66 @@ def test_slice_status_codes(gpu):
     assert audio.slice(x, d, x, other, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_LAYOUT_MISMATCH
     d4 = generic_desc((2, 1, 10, 10))
     assert audio.slice(x, d4, x, d4, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_NOT_IMPLEMENTED
+
+
+# ---------------------------------------------------------------- normalize (api/rppt_tensor_statistical_operations.h:193)
+
+@pytest.mark.parametrize("cols", [700, 3000])
+@pytest.mark.parametrize("axis_mask", [1, 2, 3])
+@pytest.mark.parametrize("compute", [0, 1, 2, 3])
+def test_normalize_vs_oracle(gpu, oracle, cols, axis_mask, compute):
+    """2-D F32 normalize against the oracle (itself bit-exact to the reference host library): the
+    computed means bit for bit (the same halving-tree sums), the inverse std devs and the outputs
+    within 1e-5 (the reference refines an SSE rsqrt estimate, CUDA rounds rsqrt correctly); the
+    destination outside the roi is zeroed."""
+    from rpp_b200.types import generic_desc
+    r = np.random.Generator(np.random.PCG64(300 + cols + 10 * axis_mask + compute))
+    n, R = 5, 40
+    src = (r.standard_normal((n, R, cols)) * 3 + 1).astype(np.float32)
+    src[2, 3, :] = 0.5
+    roi = np.zeros((n, 4), np.uint32)
+    roi[:, 2] = r.integers(20, R + 1, n)
+    roi[:, 3] = r.integers(cols // 2, cols + 1, n)
+    roi[0, 2:] = (R, cols)
+    size = max(int(np.prod([1 if axis_mask & (1 << i) else roi[b, 2 + i] for i in range(2)])) for b in range(n))
+    per = n * size
+    mean = (r.standard_normal(per) * 0.1).astype(np.float32)
+    std = r.uniform(0.5, 2.0, per).astype(np.float32)
+    std[1] = 0.0
+    m_ref, s_ref = mean.copy(), std.copy()
+    exp = np.full((n, R, cols), 7.0, np.float32)
+    oracle.normalize_2d(src, exp, axis_mask, m_ref, s_ref, compute, 1.5, 0.25, roi.ravel())
+    d = generic_desc((n, R, cols))
+    out = torch.full((n, R, cols), 7.0, device="cuda")
+    m_gpu, s_gpu = dev(mean.copy()), dev(std.copy())
+    st = audio.normalize(dev(src), d, out, d, axis_mask, m_gpu, s_gpu, compute, 1.5, 0.25, roi.ravel(), gpu)
+    assert st == RppStatus.RPP_SUCCESS
+    got = host(out)
+    np.testing.assert_allclose(got, exp, rtol=1e-5, atol=1e-5)
+    if compute & 1:
+        np.testing.assert_array_equal(host(m_gpu)[:per], m_ref[:per])
+    if compute & 2:
+        np.testing.assert_allclose(host(s_gpu)[:per], s_ref[:per], rtol=1e-6, atol=0)
+
+
+def test_normalize_frontend_output(gpu, oracle):
+    """The RNN-T-style step: per-filter normalisation over time of the fused front end's decibels."""
+    from rpp_b200.types import generic_desc, frontend_params
+    x, lens = synth.config1(n=6, max_len=48000)
+    n, L = x.shape
+    mf = 48000 // 160 + 1
+    db = torch.zeros((n, 128, mf), device="cuda")
+    assert audio.frontend(dev(x), audio_desc(n, L), db, spectra_desc(n, 128, mf), dev(lens),
+                          dev(np.full(n, 0.97, np.float32)), frontend_params(), gpu) == RppStatus.RPP_SUCCESS
+    F = lens // 160 + 1
+    roi = np.stack([np.zeros(n), np.zeros(n), np.full(n, 128), F], 1).astype(np.uint32).ravel()
+    d = generic_desc((n, 128, mf))
+    out = torch.zeros_like(db)
+    mean, std = torch.zeros(n * 128, device="cuda"), torch.zeros(n * 128, device="cuda")
+    assert audio.normalize(db, d, out, d, 2, mean, std, 3, 1.0, 0.0, roi, gpu) == RppStatus.RPP_SUCCESS
+    src = host(db)
+    exp = np.zeros_like(src)
+    m, s = np.zeros(n * 128, np.float32), np.zeros(n * 128, np.float32)
+    oracle.normalize_2d(src, exp, 2, m, s, 3, 1.0, 0.0, roi)
+    np.testing.assert_allclose(host(out), exp, rtol=1e-5, atol=1e-5)
+    np.testing.assert_array_equal(host(mean), m)

@@ -178,3 +178,33 @@ def test_slice(oracle, reference, num_dims, dtype, pad):
     oracle.slice(src, a, anchor.ravel(), shape.ravel(), roi.ravel(), fill, pad, num_dims)
     reference.slice(src, b, anchor.ravel(), shape.ravel(), roi.ravel(), fill, pad, num_dims)
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("axis_mask", [1, 2, 3])
+@pytest.mark.parametrize("compute", [0, 1, 2, 3])
+def test_normalize_2d(oracle, reference, axis_mask, compute):
+    """2-D F32 normalize (the audio branch of normalize.cpp): rois smaller than the tensor, long
+    reductions (the recursive halving sums), internal and external mean / std dev, bit for bit
+    including the in-out mean and std-dev arrays (same CPU, same rsqrt instruction)."""
+    r = rng(60 + axis_mask * 4 + compute)
+    n, R, C = 5, 40, 700
+    src = (r.standard_normal((n, R, C)) * 3 + 1).astype(np.float32)
+    src[2, 3, :] = 0.5      # a constant row: zero variance
+    roi = np.zeros((n, 4), np.uint32)
+    roi[:, 2] = r.integers(20, R + 1, n)
+    roi[:, 3] = r.integers(300, C + 1, n)
+    roi[0, 2:] = (R, C)
+    size = max(int(np.prod([1 if axis_mask & (1 << i) else roi[b, 2 + i] for i in range(2)])) for b in range(n))
+    per = n * size
+    mean = (r.standard_normal(per) * 0.1).astype(np.float32)
+    std = r.uniform(0.5, 2.0, per).astype(np.float32)
+    std[1] = 0.0
+    outs = []
+    for impl in (oracle, reference):
+        m, s_ = mean.copy(), std.copy()
+        dst = np.full((n, R, C), 7.0, np.float32)
+        impl.normalize_2d(src, dst, axis_mask, m, s_, compute, 1.5, 0.25, roi.ravel())
+        outs.append((dst, m, s_))
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    np.testing.assert_array_equal(outs[0][2], outs[1][2])
