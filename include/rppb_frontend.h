@@ -128,6 +128,14 @@ SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost, RpptDescPt
                                                const Rpp32f* coeffHost, const RppbFrontendParams* params,
                                                Rpp32s numChunks, rppHandle_t rppHandle);
 
+/* 16-bit PCM ingest (extension; the reference converts WAV data on the host in its test suite,
+ * utilities/test_suite/rpp_test_suite_audio.h:143-178): srcDesc dataType I16, dstDesc F32, both
+ * [n][nStride] with c interleaved channels; converts srcLengthTensor[b] frames x c samples of each
+ * clip to float / 32768 (exact), leaving the destination tail as it was.  Lengths may be device,
+ * pinned or pageable memory; srcPtr/dstPtr device memory. */
+SHARED_PUBLIC RppStatus rppb_pcm16_to_f32_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                              RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor, rppHandle_t rppHandle);
+
 /* Operand precision of the tensor-core spectrogram; every variant accumulates in FP32. */
 typedef enum
 {

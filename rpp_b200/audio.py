@@ -157,6 +157,13 @@ def normalize(src, src_desc, dst, dst_desc, axis_mask, mean, std_dev, compute_me
                                         float(scale), float(shift), _addr(roi), _h(handle)))
 
 
+def pcm16_to_f32(src, src_desc, dst, dst_desc, src_length, handle):
+    """rppb_pcm16_to_f32_gpu: int16 PCM (interleaved channels) to float / 32768 on the device."""
+    L = _lib.load()
+    return _status(L.rppb_pcm16_to_f32_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
+                                           _addr(src_length), _h(handle)))
+
+
 def device_error(handle):
     """Reads and clears the handle's device error word (synchronizes the handle stream)."""
     L = _lib.load()

@@ -1032,3 +1032,28 @@ extern "C" SHARED_PUBLIC RppStatus rppt_normalize_gpu(RppPtr_t srcPtr, RpptGener
         return RPP_SUCCESS;
     });
 }
+
+extern "C" SHARED_PUBLIC RppStatus rppb_pcm16_to_f32_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                         RpptDescPtr dstDescPtr, Rpp32s* srcLengthTensor,
+                                                         rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        if (srcDescPtr->dataType != I16) return RPP_ERROR_INVALID_SRC_DATATYPE;
+        if (dstDescPtr->dataType != F32) return RPP_ERROR_INVALID_DST_DATATYPE;
+        if (srcDescPtr->c != dstDescPtr->c || srcDescPtr->c == 0) return RPP_ERROR_INVALID_ARGUMENTS;
+        require(srcPtr && dstPtr, "null tensor");
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        Carver m(nullptr);
+        m.take<int>(n);
+        Carver cv(h.workspace(m.used()));
+        int* lenStage = cv.take<int>(n);
+        const int* len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
+        launch_pcm16(h, reinterpret_cast<const short*>(static_cast<const char*>(srcPtr) + srcDescPtr->offsetInBytes),
+                     srcDescPtr->strides.nStride,
+                     reinterpret_cast<float*>(static_cast<char*>(dstPtr) + dstDescPtr->offsetInBytes),
+                     dstDescPtr->strides.nStride, len, int(srcDescPtr->c), n);
+        return RPP_SUCCESS;
+    });
+}

@@ -183,6 +183,10 @@ void launch_normalize(Handle& h, const NormalizeArgs& a, const int4* tasks, int 
                       const float* invEff, int paramOffsetPerSample, const float* stdToInvert, float* invertOut,
                       int invertCount);
 
+// 16-bit PCM ingest (pcm.cu).
+void launch_pcm16(Handle& h, const short* src, uint32_t srcStride, float* dst, uint32_t dstStride, const int* len,
+                  int channels, int n);
+
 // PCIe movers over mapped pinned host memory (host_io.cu).
 void launch_host_gather(cudaStream_t stream, const float* src, size_t nStride, const int* len, int clips, float* dst,
                         uint32_t dstStride, int ctas);

@@ -23,7 +23,7 @@ EXPORTED = (
     "rppb_frontend_host_gpu", "rppb_frontend_tune_gpu",
     "rppb_server_create", "rppb_server_destroy", "rppb_server_frames", "rppb_server_submit", "rppb_server_poll",
     "rppb_server_arena_used",
-    "rppt_slice_gpu", "rppt_normalize_gpu",
+    "rppt_slice_gpu", "rppt_normalize_gpu", "rppb_pcm16_to_f32_gpu",
 )
 
 _lib = None
@@ -87,6 +87,8 @@ def load(path=None):
     L.rppt_normalize_gpu.argtypes = [_V, ctypes.POINTER(RpptGenericDesc), _V, ctypes.POINTER(RpptGenericDesc),
                                      ctypes.c_uint32, _V, _V, ctypes.c_uint8, _F, _F, _V, _V]
     L.rppt_normalize_gpu.restype = _I
+    L.rppb_pcm16_to_f32_gpu.argtypes = [_V, _D, _V, _D, _V, _V]
+    L.rppb_pcm16_to_f32_gpu.restype = _I
     L.rppb_server_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(RppbServerConfig)]
     L.rppb_server_create.restype = _I
     L.rppb_server_destroy.argtypes = [_V]

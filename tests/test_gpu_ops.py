@@ -569,3 +569,40 @@ def test_normalize_frontend_output(gpu, oracle):
     oracle.normalize_2d(src, exp, 2, m, s, 3, 1.0, 0.0, roi)
     np.testing.assert_allclose(host(out), exp, rtol=1e-5, atol=1e-5)
     np.testing.assert_array_equal(host(mean), m)
+
+
+# ---------------------------------------------------------------- 16-bit PCM ingest (extension)
+
+@pytest.mark.parametrize("channels", [1, 2, 6])
+def test_pcm16_to_f32(gpu, golden, channels):
+    """int16 -> float / 32768 on the device equals the test suite's host conversion (exact), only
+    over each clip's frames x channels; the QA WAVs convert to the goldens' inputs."""
+    r = np.random.Generator(np.random.PCG64(90 + channels))
+    n = 7
+    frames = r.integers(0, 5000, n).astype(np.int32)
+    frames[0] = 5000
+    L = 5000 * channels + 3
+    pcm = r.integers(-32768, 32768, (n, L)).astype(np.int16)
+    sd = audio_desc(n, L // channels if channels > 1 else L, channels=channels)
+    sd.strides.nStride = L
+    sd.dataType = RpptDataType.I16
+    dd = audio_desc(n, L // channels if channels > 1 else L, channels=channels)
+    dd.strides.nStride = L
+    out = torch.full((n, L), -9.0, device="cuda")
+    assert audio.pcm16_to_f32(dev(pcm), sd, out, dd, frames, gpu) == RppStatus.RPP_SUCCESS
+    got = host(out)
+    for b in range(n):
+        k = int(frames[b]) * channels
+        np.testing.assert_array_equal(got[b, :k], pcm[b, :k].astype(np.float32) / np.float32(32768.0))
+        assert (got[b, k:] == -9.0).all()
+    # the QA WAVs
+    lens = golden["lengths"].astype(np.int32)
+    w = int(lens.max())
+    q = np.zeros((3, w), np.int16)
+    for i in range(3):
+        q[i, :lens[i]] = golden[f"pcm{i}"]
+    qs = audio_desc(3, w)
+    qs.dataType = RpptDataType.I16
+    qo = torch.zeros((3, w), device="cuda")
+    assert audio.pcm16_to_f32(dev(q), qs, qo, audio_desc(3, w), lens, gpu) == RppStatus.RPP_SUCCESS
+    np.testing.assert_array_equal(host(qo), q.astype(np.float32) / 32768.0)
