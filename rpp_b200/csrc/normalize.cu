@@ -26,7 +26,9 @@ namespace rppb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kWarpMinElems = 2048;   // warp-parallel tree from this reduction length on
+// warp-parallel tree from this reduction length on: every node of the top five levels then holds
+// at least floor(n / 16) >= 34 > 32 elements, so it splits as the lanes assume
+constexpr int kWarpMinElems = 544;
 
 // The reference's compute_sum / compute_diff_square_sum value (the "+= into 0" steps are exact:
 // the partial sums are never -0).
@@ -55,8 +57,7 @@ __device__ float tree_sum(const float* in, int stride, int n, float mean)
     return t;
 }
 
-// Same value, the 32 subtrees five levels down summed by the 32 lanes (n >= kWarpMinElems, so every
-// node above them splits).
+// Same value, the 32 subtrees five levels down summed by the 32 lanes (n >= kWarpMinElems).
 template <bool kSq>
 __device__ float warp_tree_sum(const float* in, int stride, int n, float mean)
 {

@@ -510,7 +510,7 @@ def test_slice_status_codes(gpu):
 
 # ---------------------------------------------------------------- normalize (api/rppt_tensor_statistical_operations.h:193)
 
-@pytest.mark.parametrize("cols", [700, 3000])
+@pytest.mark.parametrize("cols", [300, 700, 3000])
 @pytest.mark.parametrize("axis_mask", [1, 2, 3])
 @pytest.mark.parametrize("compute", [0, 1, 2, 3])
 def test_normalize_vs_oracle(gpu, oracle, cols, axis_mask, compute):
