@@ -556,6 +556,50 @@ def precision_measurement(torch, h, check_clips=20, n=1024, length=160000, reps=
             v = {"power_rel_err_max": float(rel.max()), "power_rel_err_rms": float(np.sqrt((rel ** 2).mean())),
                  "db_err_max": float(e.max()), "db_err_rms": float(np.sqrt((e ** 2).mean())), "by_dynamic_range": by_dr,
                  "ms": ms, "clip_s_per_s": n * length / RATE / (ms / 1e3)}
+            # mel power error of the FP32 mel on this spectrum, and (tensor-core variants) of the whole
+            # chain on tensor cores: the same precision for the mel projection
+            mel_np = mel.cpu().numpy().astype(np.float64)
+            def mel_err(mv):
+                worst = 0.0
+                for i in range(check_clips):
+                    scale = np.maximum(mel64[i].max(axis=0, keepdims=True), 1e-300)
+                    worst = max(worst, float((np.abs(mv[i] - mel64[i]) / scale).max()))
+                return worst
+            v["mel_power_rel_err_max_fp32_mel"] = mel_err(mel_np)
+            if name != "fp32_fft":
+                melt = torch.zeros_like(mel)
+                assert audio.mel_filter_bank_tc(spec, spectra_desc(check_clips, bins, F), melt,
+                                                spectra_desc(check_clips, NMEL, F), dimd, 8000.0, 0.0, 0, NMEL,
+                                                float(RATE), True, tc_modes[name], h) == 0
+                torch.cuda.synchronize()
+                v["mel_power_rel_err_max_tc_chain"] = mel_err(melt.cpu().numpy().astype(np.float64))
+                del melt
+            # time of the chain spectrogram + mel on the full batch (tensor-core mel for the tensor-core
+            # variants, the FP32 mel kernel for the FP32 path)
+            outm = torch.empty((n, NMEL, F), device="cuda")
+            dimf = torch.from_numpy(np.stack([np.full(n, bins, np.int32), np.full(n, F, np.int32)], 1)
+                                    .astype(np.int32)).cuda()
+            spf = torch.empty((n, bins, F), device="cuda")
+
+            def chain():
+                run(name, xf, lf, cf, n, spf)
+                if name == "fp32_fft":
+                    assert audio.mel_filter_bank(spf, spectra_desc(n, bins, F), outm, spectra_desc(n, NMEL, F), dimf,
+                                                 8000.0, 0.0, 0, NMEL, float(RATE), True, h) == 0
+                else:
+                    assert audio.mel_filter_bank_tc(spf, spectra_desc(n, bins, F), outm, spectra_desc(n, NMEL, F), dimf,
+                                                    8000.0, 0.0, 0, NMEL, float(RATE), True, tc_modes[name], h) == 0
+            chain()
+            tt = []
+            for _ in range(reps):
+                a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a_.record()
+                chain()
+                b_.record()
+                torch.cuda.synchronize()
+                tt.append(a_.elapsed_time(b_))
+            v["spectrogram_mel_chain_ms"] = float(np.median(tt))
+            del outm, spf
             if name != "fp32_fft":
                 block = 128 // {"tc_bf16": 2, "tc_bf16_hilo3": 2, "tc_tf32": 4, "tc_fp8_e4m3": 1}[name]
                 kpad = -(-W // block) * block

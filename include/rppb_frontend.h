@@ -158,6 +158,19 @@ SHARED_PUBLIC RppStatus rppb_spectrogram_tc_gpu(RppPtr_t srcPtr, RpptDescPtr src
                                                 Rpp32s windowStep, RppbTensorCorePrecision precision,
                                                 rppHandle_t rppHandle);
 
+/* Tensor-core mel projection (precision study; extension, no counterpart in the reference): the
+ * mel filter bank of rppt_mel_filter_bank_gpu (same arguments and tables) as a GEMM on tcgen05
+ * tensor cores, spectrum frames x dense filter matrix, with the operand precision of `precision`
+ * (FP8: per-frame spectrum scale and one power-of-two weight scale) and FP32 accumulation.
+ * NFT in and out, numFilter <= 256; the spectrum's bin count is srcDesc->h.  Only the valid frames
+ * (srcDimsTensor) are written; the sums are in the tensor core's order, so the results carry the
+ * operand precision's error instead of matching the reference bit for bit. */
+SHARED_PUBLIC RppStatus rppb_mel_filter_bank_tc_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                    RpptDescPtr dstDescPtr, Rpp32s* srcDimsTensor, Rpp32f maxFreq,
+                                                    Rpp32f minFreq, RpptMelScaleFormula melFormula, Rpp32s numFilter,
+                                                    Rpp32f sampleRate, bool normalize,
+                                                    RppbTensorCorePrecision precision, rppHandle_t rppHandle);
+
 /* Reads (and clears) the handle's device error word: nonzero when a fused launch gave up
  * waiting for a clip's spectrum tiles (a bounded wait; the affected tiles are left unconverted).
  * Synchronizes the handle stream. */

@@ -164,6 +164,16 @@ def pcm16_to_f32(src, src_desc, dst, dst_desc, src_length, handle):
                                            _addr(src_length), _h(handle)))
 
 
+def mel_filter_bank_tc(src, src_desc, dst, dst_desc, src_dims, max_freq, min_freq, mel_formula, num_filter,
+                       sample_rate, normalize, precision, handle):
+    """rppb_mel_filter_bank_tc_gpu: the mel filter bank as a tensor-core GEMM (precision study)."""
+    L = _lib.load()
+    return _status(L.rppb_mel_filter_bank_tc_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst),
+                                                 ctypes.byref(dst_desc), _addr(src_dims), float(max_freq),
+                                                 float(min_freq), int(mel_formula), int(num_filter), float(sample_rate),
+                                                 bool(normalize), int(precision), _h(handle)))
+
+
 def device_error(handle):
     """Reads and clears the handle's device error word (synchronizes the handle stream)."""
     L = _lib.load()

@@ -1057,3 +1057,58 @@ extern "C" SHARED_PUBLIC RppStatus rppb_pcm16_to_f32_gpu(RppPtr_t srcPtr, RpptDe
         return RPP_SUCCESS;
     });
 }
+
+extern "C" SHARED_PUBLIC RppStatus rppb_mel_filter_bank_tc_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
+                                                               RpptDescPtr dstDescPtr, Rpp32s* srcDimsTensor,
+                                                               Rpp32f maxFreq, Rpp32f minFreq,
+                                                               RpptMelScaleFormula melFormula, Rpp32s numFilter,
+                                                               Rpp32f sampleRate, bool normalize,
+                                                               RppbTensorCorePrecision precision, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        require(srcDescPtr && dstDescPtr, "null descriptor");
+        if (srcDescPtr->numDims != 3) return RPP_ERROR_INVALID_SRC_DIMS;
+        if (srcDescPtr->layout != NFT) return RPP_ERROR_INVALID_SRC_LAYOUT;
+        if (dstDescPtr->layout != NFT) return RPP_ERROR_INVALID_DST_LAYOUT;
+        if (maxFreq < 0 || maxFreq > sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
+        if (minFreq < 0 || minFreq > sampleRate / 2) return RPP_ERROR_INVALID_ARGUMENTS;
+        if (!(is_f32(srcDescPtr) && is_f32(dstDescPtr))) return RPP_ERROR_NOT_IMPLEMENTED;
+        require(srcPtr && dstPtr && srcDimsTensor, "null tensor");
+        require(numFilter > 0, "numFilter must be positive");
+        const int fmt = int(precision);
+        if (fmt < kTcBf16 || fmt > kTcFp8 || numFilter > 256) return RPP_ERROR_NOT_IMPLEMENTED;
+        if (dstDescPtr->h < Rpp32u(numFilter)) return RPP_ERROR_INVALID_DST_DIMS;
+        const int bins = int(srcDescPtr->h);
+        if (bins < 2) return RPP_ERROR_INVALID_SRC_DIMS;
+        const int n = int(srcDescPtr->n);
+        if (n <= 0) return RPP_SUCCESS;
+        const int maxFrames = int(std::min(dstDescPtr->w, srcDescPtr->strides.hStride));
+        const size_t scratchBytes = tc_mel_scratch_bytes(n, fmt, bins, maxFrames);
+        Carver m(nullptr);
+        m.take<int>(2 * n);
+        m.take<char>(scratchBytes);
+        Carver cv(h.workspace(m.used()));
+        int* dimsStage = cv.take<int>(2 * n);
+        void* scratch = cv.take<char>(scratchBytes);
+        TcMelArgs a;
+        a.src = static_cast<const float*>(srcPtr);
+        a.srcNStride = srcDescPtr->strides.nStride;
+        a.srcHStride = srcDescPtr->strides.hStride;
+        a.bins = bins;
+        a.dims = static_cast<const int*>(h.device_view(srcDimsTensor, 2 * n * sizeof(int), dimsStage));
+        a.n = n;
+        a.maxFrames = maxFrames;
+        a.fmt = fmt;
+        a.mel.minFreq = minFreq;
+        a.mel.maxFreq = (maxFreq == 0) ? sampleRate / 2 : maxFreq;
+        a.mel.sampleRate = sampleRate;
+        a.mel.htk = melFormula == HTK ? 1 : 0;
+        a.mel.numFilter = numFilter;
+        a.mel.normalize = normalize;
+        a.dst = static_cast<float*>(dstPtr);
+        a.dstNStride = dstDescPtr->strides.nStride;
+        a.dstHStride = dstDescPtr->strides.hStride;
+        launch_tc_mel(h, scratch, a);
+        return RPP_SUCCESS;
+    });
+}

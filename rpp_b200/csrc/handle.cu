@@ -271,7 +271,10 @@ int persistent_grid(const Handle& h, const void* kernel, int threads, size_t sme
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
     size_t& limit = smemLimit[std::make_pair(kernel, h.device())];
-    if (smem > 48 * 1024 && smem > limit)
+    // without the opt-in attribute, static + dynamic shared memory must stay within 48 KB
+    cudaFuncAttributes fa{};
+    check_cuda(cudaFuncGetAttributes(&fa, kernel), "cudaFuncGetAttributes");
+    if (smem + fa.sharedSizeBytes > 48 * 1024 && smem > limit)
     {
         check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem attr");
         limit = smem;

@@ -233,6 +233,20 @@ struct TcSpectrogramArgs
     int n;
 };
 size_t tc_spectrogram_scratch_bytes(int n, int fmt, const TcGeometry& g, int maxFrames);
+// Mel projection on tensor cores (tc_dft.cu): NFT spectra -> NFT mel, numFilter <= 256.
+struct TcMelArgs
+{
+    const float* src;
+    uint32_t srcNStride, srcHStride;
+    int bins;                 // spectrum rows (nfft / 2 + 1)
+    const int* dims;          // device: per sample {bins, frames}
+    int n, maxFrames, fmt;
+    MelParams mel;
+    float* dst;
+    uint32_t dstNStride, dstHStride;
+};
+size_t tc_mel_scratch_bytes(int n, int fmt, int bins, int maxFrames);
+void launch_tc_mel(Handle& h, void* scratch, const TcMelArgs& a);
 void launch_tc_spectrogram(Handle& h, void* scratch, const TcSpectrogramArgs& a);
 
 }  // namespace rppb

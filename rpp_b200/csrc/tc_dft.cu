@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "mel_tables.cuh"
 #include "ops.hpp"
 
 namespace rppb {
@@ -167,7 +168,11 @@ struct TcArgs
     const int* frames;          // frames per clip
     int n;
     int* errorWord;
+    int validN;                 // linear epilogue: output columns (mel filters)
 };
+
+constexpr int kEpiPower = 0;
+constexpr int kEpiLinear = 1;
 
 struct TcCount
 {
@@ -180,7 +185,9 @@ struct TcCount
     }
 };
 
-template <int FMT>
+// EPI: kEpiPower -- column pairs (cos, -sin) of one bin -> power / magnitude (the spectrogram);
+//      kEpiLinear -- column n < validN -> the accumulator itself (the mel projection).
+template <int FMT, int EPI>
 __global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const long long* __restrict__ prefix)
 {
     using T = Fmt<FMT>;
@@ -327,7 +334,19 @@ __global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const lon
                   "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (frame < F)
+            if (EPI == kEpiLinear && frame < F)
+            {
+#pragma unroll
+                for (int q = 0; q < 32; ++q)
+                {
+                    const int col = n0 + c0 + q;
+                    if (col >= a.validN) break;
+                    const float o = __uint_as_float(v[q]) * sc;
+                    if (a.nft) y[size_t(col) * a.dstHStride + frame] = o;
+                    else y[size_t(frame) * a.dstHStride + col] = o;
+                }
+            }
+            if (EPI == kEpiPower && frame < F)
             {
 #pragma unroll
                 for (int q = 0; q < 16; ++q)
@@ -488,12 +507,12 @@ __global__ void tc_frames_kernel(const int* __restrict__ len, uint32_t srcStride
         frames[b] = min(num_windows(min(len[b], int(srcStride)), W, hop, center), maxFrames);
 }
 
-template <int FMT>
+template <int FMT, int EPI = kEpiPower>
 void launch_format(Handle& h, const TcArgs& a, const long long* prefix)
 {
     const size_t smem = Fmt<FMT>::kStages * Fmt<FMT>::kStageBytes + 1024;
-    const int grid = persistent_grid(h, reinterpret_cast<const void*>(tc_dft_kernel<FMT>), kThreads, smem);
-    tc_dft_kernel<FMT><<<grid, kThreads, smem, h.stream()>>>(a, prefix);
+    const int grid = persistent_grid(h, reinterpret_cast<const void*>(tc_dft_kernel<FMT, EPI>), kThreads, smem);
+    tc_dft_kernel<FMT, EPI><<<grid, kThreads, smem, h.stream()>>>(a, prefix);
     count_launch(1);
     check_cuda(cudaGetLastError(), "tc_dft_kernel");
 }
@@ -523,6 +542,168 @@ uint32_t tf32_rna(float f)
     uint32_t u;
     std::memcpy(&u, &f, 4);
     return (u + 0x1000u) & 0xffffe000u;
+}
+
+// ---------------------------------------------------------------- mel projection on tensor cores
+// mel[f][m] = sum_k power[f][k] * W[m][k] as the GEMM C = A x B^T, A = the spectrum transposed to
+// [frame][bin] (K-major, bins padded to one 128-byte row of operand elements), B = the dense filter
+// bank [256][kPad] (rows >= numFilter zero).  W holds the mel_filter_bank kernel's weights (same
+// tables, same float expressions); the GEMM sums them in the tensor core's order, not the
+// reference's, so the result carries the operand precision's error, not bit-exactness.
+
+constexpr int kMelN = 256;
+
+struct MelWeightArgs
+{
+    MelParams mel;
+    int nfft;            // (bins - 1) * 2
+    int bins, kPad, fmt;
+    unsigned char* b;    // operand [256][kPad] (hi, then lo for the split format)
+    float* bScale;       // FP8: scale applied to W (device scalar)
+};
+
+// One CTA: the reference's mel tables in shared memory, the dense weights, their largest magnitude
+// (FP8 scale: a power of two keeping it <= 448), then the operand copy.
+__global__ void __launch_bounds__(256) mel_weights_kernel(MelWeightArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nf = a.mel.numFilter;
+    MelTableView T;
+    T.range = reinterpret_cast<int*>(smem);
+    T.first = T.range + 4;
+    T.last = T.first + (nf + 2);
+    T.norm = reinterpret_cast<float*>(T.last + (nf + 2));
+    size_t off = (size_t(reinterpret_cast<unsigned char*>(T.norm + nf) - smem) + 7) & ~size_t(7);
+    T.f0 = reinterpret_cast<double*>(smem + off);
+    T.f1 = T.f0 + (nf + 1);
+    T.weightsDown = reinterpret_cast<float*>(T.f1 + (nf + 1));
+    __shared__ float s_max[8];
+    build_mel_tables(T, a.mel, a.nfft);   // ends with __syncthreads
+    auto weight = [&](int m, int k) -> float {
+        if (m >= nf || k >= a.bins) return 0.f;
+        float w = 0.f;
+        if (k >= T.first[m] && k < T.last[m]) w = __fsub_rn(1.0f, T.weightsDown[k]);
+        else if (k >= T.first[m + 1] && k < T.last[m + 1]) w = T.weightsDown[k];
+        else return 0.f;
+        return a.mel.normalize ? __fmul_rn(w, T.norm[m]) : w;
+    };
+    float mx = 0.f;
+    for (int i = threadIdx.x; i < kMelN * a.kPad; i += blockDim.x) mx = fmaxf(mx, fabsf(weight(i / a.kPad, i % a.kPad)));
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    float scale = 1.f;
+    if (a.fmt == kTcFp8)
+    {
+        float m = 0.f;
+        for (int i = 0; i < 8; ++i) m = fmaxf(m, s_max[i]);
+        if (m > 0.f) scale = exp2f(floorf(log2f(kFp8Max / m)));
+        if (threadIdx.x == 0) *a.bScale = scale;
+    }
+    const size_t count = size_t(kMelN) * a.kPad;
+    for (int i = threadIdx.x; i < kMelN * a.kPad; i += blockDim.x)
+    {
+        const float w = weight(i / a.kPad, i % a.kPad);
+        if (a.fmt == kTcTf32)
+        {
+            uint32_t t;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(w));
+            reinterpret_cast<uint32_t*>(a.b)[i] = t;
+        }
+        else if (a.fmt == kTcFp8)
+            reinterpret_cast<__nv_fp8_e4m3*>(a.b)[i] = __nv_fp8_e4m3(w * scale);
+        else
+        {
+            const __nv_bfloat16 hi = __float2bfloat16_rn(w);
+            reinterpret_cast<__nv_bfloat16*>(a.b)[i] = hi;
+            if (a.fmt == kTcBf16x3)
+                reinterpret_cast<__nv_bfloat16*>(a.b)[count + i] = __float2bfloat16_rn(w - __bfloat162float(hi));
+        }
+    }
+}
+
+struct MelPrepArgs
+{
+    const float* src;            // NFT spectra [n][srcRows][srcHStride]
+    uint32_t srcNStride, srcHStride;
+    int bins, kPad, maxFrames, fmt, n;
+    const int* frames;
+    unsigned char* aHi;          // [n][maxFrames][kPad]
+    unsigned char* aLo;
+    float* invScale;             // FP8: 1 / (frame scale * weight scale), [n][maxFrames]
+    const float* bScale;
+};
+
+// FP8 only: per frame, 448 / the frame's largest power.
+__global__ void mel_frame_scale_kernel(MelPrepArgs a)
+{
+    for (int b = blockIdx.y; b < a.n; b += gridDim.y)
+    {
+        const float* x = a.src + size_t(b) * a.srcNStride;
+        const int F = a.frames[b];
+        for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < F; f += gridDim.x * blockDim.x)
+        {
+            float m = 0.f;
+            for (int k = 0; k < a.bins; ++k) m = fmaxf(m, fabsf(x[size_t(k) * a.srcHStride + f]));
+            const float sc = m > 0.f ? kFp8Max / m : 1.f;
+            a.invScale[size_t(b) * a.maxFrames + f] = 1.f / (sc * *a.bScale);
+        }
+    }
+}
+
+// [bin][frame] -> [frame][bin] in the operand format, 32 x 32 tiles through shared memory; bins
+// past the spectrum and up to kPad are zero.
+__global__ void __launch_bounds__(256) mel_prep_kernel(MelPrepArgs a)
+{
+    __shared__ float tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+    for (int b = blockIdx.z; b < a.n; b += gridDim.z)
+    {
+        const int F = a.frames[b];
+        const int f0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+        if (f0 >= F || k0 >= a.kPad) continue;
+        const float* x = a.src + size_t(b) * a.srcNStride;
+        for (int r = ty; r < 32; r += 8)
+        {
+            const int k = k0 + r, f = f0 + tx;
+            tile[r][tx] = (k < a.bins && f < F) ? x[size_t(k) * a.srcHStride + f] : 0.f;
+        }
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8)
+        {
+            const int f = f0 + r, k = k0 + tx;
+            if (f < F && k < a.kPad)
+            {
+                const float v = tile[tx][r];
+                const size_t o = (size_t(b) * a.maxFrames + f) * a.kPad + k;
+                if (a.fmt == kTcTf32)
+                {
+                    uint32_t t;
+                    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
+                    reinterpret_cast<uint32_t*>(a.aHi)[o] = t;
+                }
+                else if (a.fmt == kTcFp8)
+                {
+                    const float sc = 1.f / (a.invScale[size_t(b) * a.maxFrames + f] * *a.bScale);
+                    reinterpret_cast<__nv_fp8_e4m3*>(a.aHi)[o] = __nv_fp8_e4m3(v * sc);
+                }
+                else
+                {
+                    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+                    reinterpret_cast<__nv_bfloat16*>(a.aHi)[o] = hi;
+                    if (a.fmt == kTcBf16x3)
+                        reinterpret_cast<__nv_bfloat16*>(a.aLo)[o] = __float2bfloat16_rn(v - __bfloat162float(hi));
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void mel_frames_kernel(const int* __restrict__ dims, int n, int maxFrames, int* __restrict__ frames)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
+        frames[b] = min(max(dims[2 * b + 1], 0), maxFrames);
 }
 
 }  // namespace
@@ -657,12 +838,113 @@ void launch_tc_spectrogram(Handle& h, void* scratch, const TcSpectrogramArgs& s)
     a.frames = frames;
     a.n = s.n;
     a.errorWord = h.device_flags();
+    a.validN = 0;
     switch (s.fmt)
     {
     case kTcBf16: launch_format<kTcBf16>(h, a, prefix); break;
     case kTcBf16x3: launch_format<kTcBf16x3>(h, a, prefix); break;
     case kTcTf32: launch_format<kTcTf32>(h, a, prefix); break;
     default: launch_format<kTcFp8>(h, a, prefix); break;
+    }
+}
+
+}  // namespace rppb
+
+namespace rppb {
+
+namespace {
+int mel_kpad(int fmt, int bins)
+{
+    const int blockK = kRowBytes / elem_bytes(fmt);
+    return (bins + blockK - 1) / blockK * blockK;
+}
+}  // namespace
+
+size_t tc_mel_scratch_bytes(int n, int fmt, int bins, int maxFrames)
+{
+    const int kPad = mel_kpad(fmt, bins);
+    const size_t e = elem_bytes(fmt);
+    const size_t rows = size_t(n) * std::max(maxFrames, 1);
+    Carver cv(nullptr);
+    cv.take<long long>(n + 1);
+    cv.take<int>(n);
+    cv.take<float>(1);
+    cv.take<char>(size_t(kMelN) * kPad * e * (fmt == kTcBf16x3 ? 2 : 1));
+    cv.take<char>(rows * kPad * e);
+    if (fmt == kTcBf16x3) cv.take<char>(rows * kPad * e);
+    cv.take<float>(rows);
+    return cv.used();
+}
+
+void launch_tc_mel(Handle& h, void* scratch, const TcMelArgs& s)
+{
+    if (s.n <= 0) return;
+    const int kPad = mel_kpad(s.fmt, s.bins);
+    const size_t e = elem_bytes(s.fmt);
+    const int maxFrames = std::max(s.maxFrames, 1);
+    const size_t rows = size_t(s.n) * maxFrames;
+    Carver cv(scratch);
+    long long* prefix = cv.take<long long>(s.n + 1);
+    int* frames = cv.take<int>(s.n);
+    float* bScale = cv.take<float>(1);
+    const size_t bBytes = size_t(kMelN) * kPad * e;
+    unsigned char* bOp = cv.take<unsigned char>(bBytes * (s.fmt == kTcBf16x3 ? 2 : 1));
+    unsigned char* aHi = cv.take<unsigned char>(rows * kPad * e);
+    unsigned char* aLo = s.fmt == kTcBf16x3 ? cv.take<unsigned char>(rows * kPad * e) : nullptr;
+    float* invScale = cv.take<float>(rows);
+
+    // dense weights (one CTA) in the operand format
+    MelWeightArgs w{s.mel, (s.bins - 1) * 2, s.bins, kPad, s.fmt, bOp, bScale};
+    const int nf = s.mel.numFilter;
+    size_t tbl = 16 + size_t(2 * (nf + 2)) * 4 + size_t(nf) * 4;
+    tbl = ((tbl + 7) & ~size_t(7)) + size_t(2 * (nf + 1)) * 8 + size_t(s.bins) * 4;
+    if (tbl > 200 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "mel tables too large");
+    check_cuda(cudaFuncSetAttribute(mel_weights_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tbl)),
+               "cudaFuncSetAttribute(mel_weights_kernel)");
+    if (s.fmt != kTcFp8) check_cuda(cudaMemsetAsync(bScale, 0, sizeof(float), h.stream()), "memset(bScale)");
+    mel_weights_kernel<<<1, 256, tbl, h.stream()>>>(w);
+    count_launch(1);
+    mel_frames_kernel<<<(s.n + 255) / 256, 256, 0, h.stream()>>>(s.dims, s.n, maxFrames, frames);
+    count_launch(1);
+    MelPrepArgs p{s.src, s.srcNStride, s.srcHStride, s.bins, kPad, maxFrames, s.fmt, s.n, frames, aHi, aLo, invScale,
+                  bScale};
+    if (s.fmt == kTcFp8)
+    {
+        dim3 g(std::min((maxFrames + 255) / 256, 64), std::min(s.n, 65535));
+        mel_frame_scale_kernel<<<g, 256, 0, h.stream()>>>(p);
+        count_launch(1);
+    }
+    dim3 pg((maxFrames + 31) / 32, (kPad + 31) / 32, std::min(s.n, 65535));
+    mel_prep_kernel<<<pg, 256, 0, h.stream()>>>(p);
+    count_launch(1);
+    launch_ragged_prefix(TcCount{frames, 1}, s.n, prefix, h.stream());
+
+    TcArgs a;
+    a.a = aHi;
+    a.aLo = aLo;
+    a.clipStride = uint32_t(size_t(maxFrames) * kPad);
+    a.rowStep = uint32_t(kPad);
+    a.b = bOp;
+    a.bLo = s.fmt == kTcBf16x3 ? bOp + bBytes : nullptr;
+    a.kPad = kPad;
+    a.nfft = kMelN;          // one 256-column chunk
+    a.invScale = invScale;
+    a.maxFrames = maxFrames;
+    a.dst = s.dst;
+    a.dstNStride = s.dstNStride;
+    a.dstHStride = s.dstHStride;
+    a.nft = true;
+    a.power = 2;
+    a.frames = frames;
+    a.n = s.n;
+    a.errorWord = h.device_flags();
+    a.validN = nf;
+    switch (s.fmt)
+    {
+    case kTcBf16: launch_format<kTcBf16, kEpiLinear>(h, a, prefix); break;
+    case kTcBf16x3: launch_format<kTcBf16x3, kEpiLinear>(h, a, prefix); break;
+    case kTcTf32: launch_format<kTcTf32, kEpiLinear>(h, a, prefix); break;
+    default: launch_format<kTcFp8, kEpiLinear>(h, a, prefix); break;
     }
 }
 

@@ -23,7 +23,7 @@ EXPORTED = (
     "rppb_frontend_host_gpu", "rppb_frontend_tune_gpu",
     "rppb_server_create", "rppb_server_destroy", "rppb_server_frames", "rppb_server_submit", "rppb_server_poll",
     "rppb_server_arena_used",
-    "rppt_slice_gpu", "rppt_normalize_gpu", "rppb_pcm16_to_f32_gpu",
+    "rppt_slice_gpu", "rppt_normalize_gpu", "rppb_pcm16_to_f32_gpu", "rppb_mel_filter_bank_tc_gpu",
 )
 
 _lib = None
@@ -89,6 +89,8 @@ def load(path=None):
     L.rppt_normalize_gpu.restype = _I
     L.rppb_pcm16_to_f32_gpu.argtypes = [_V, _D, _V, _D, _V, _V]
     L.rppb_pcm16_to_f32_gpu.restype = _I
+    L.rppb_mel_filter_bank_tc_gpu.argtypes = [_V, _D, _V, _D, _V, _F, _F, _I, _I, _F, _B, _I, _V]
+    L.rppb_mel_filter_bank_tc_gpu.restype = _I
     L.rppb_server_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(RppbServerConfig)]
     L.rppb_server_create.restype = _I
     L.rppb_server_destroy.argtypes = [_V]

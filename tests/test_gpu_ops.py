@@ -606,3 +606,21 @@ def test_pcm16_to_f32(gpu, golden, channels):
     qo = torch.zeros((3, w), device="cuda")
     assert audio.pcm16_to_f32(dev(q), qs, qo, audio_desc(3, w), lens, gpu) == RppStatus.RPP_SUCCESS
     np.testing.assert_array_equal(host(qo), q.astype(np.float32) / 32768.0)
+
+
+def test_mel_filter_bank_256_filters(gpu, oracle):
+    """256 filters: the mel tile's dynamic shared memory plus its static part passes 48 KB, which
+    needs the kernel's opt-in attribute."""
+    r = np.random.Generator(np.random.PCG64(123))
+    n, mf = 3, 200
+    spec = r.uniform(0, 4, (n, 257, mf)).astype(np.float32)
+    F = np.array([200, 150, 1], np.int32)
+    dims = np.stack([np.full(n, 257, np.int32), F], 1).astype(np.int32)
+    out = torch.zeros((n, 256, mf), device="cuda")
+    assert audio.mel_filter_bank(dev(spec), spectra_desc(n, 257, mf), out, spectra_desc(n, 256, mf), dev(dims), 8000.0,
+                                 0.0, 0, 256, 16000.0, True, gpu) == RppStatus.RPP_SUCCESS
+    exp = np.zeros((n, 256, mf), np.float32)
+    oracle.mel_filter_bank(spec, exp, dims.ravel(), 8000.0, 0.0, 0, 256, 16000.0, 1)
+    got = host(out)
+    for i in range(n):
+        np.testing.assert_array_equal(got[i, :, :F[i]], exp[i, :, :F[i]])

@@ -3,6 +3,7 @@ Bounds are per-frame relative (error / the frame's largest bin) and follow the o
 BF16 keeps 8 significant bits, the hi/lo split (hi*hi + hi*lo + lo*hi) about 16, TF32 11, E4M3 4."""
 import numpy as np
 import pytest
+import torch
 
 from rpp_b200 import audio, synth
 from rpp_b200.types import RppStatus, RpptLayout, audio_desc, spectra_desc
@@ -91,3 +92,34 @@ def test_tc_spectrogram_rejects(gpu):
     assert audio.spectrogram_tc(*args(512, 160, 4)) == NI                     # unknown precision
     assert audio.spectrogram_tc(*args(1024, 160, audio.TC_TF32)) == RppStatus.RPP_ERROR_INVALID_DST_DIMS  # 513 bins
     assert audio.spectrogram_tc(*args(512, 150, audio.TC_FP8_E4M3)) == OK     # FP8 frames are materialized
+
+
+MEL_BOUND = {audio.TC_BF16: 1e-2, audio.TC_BF16_HILO3: 5e-5, audio.TC_TF32: 3e-3, audio.TC_FP8_E4M3: 0.25}
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("nmel,htk,normalize", [(128, 0, True), (80, 1, False), (256, 0, True)])
+def test_tc_mel_vs_fp32(gpu, precision, nmel, htk, normalize):
+    """rppb_mel_filter_bank_tc_gpu against the FP32 mel_filter_bank (bit-exact to the reference) on
+    the same spectrum: per-frame relative error within the operand precision's bound; only the
+    valid frames are written."""
+    x, lens = synth.config1(n=10, max_len=80000)
+    n, L = x.shape
+    F = (lens // 160 + 1).astype(np.int32)
+    mf = int(F.max())
+    xd, ld = dev(x), dev(lens)
+    spec = torch.zeros((n, 257, mf), device="cuda")
+    sd, spd = audio_desc(n, L), spectra_desc(n, 257, mf)
+    assert audio.spectrogram(xd, sd, spec, spd, ld, True, True, None, 512, 2, 400, 160, gpu) == OK
+    dims = dev(np.stack([np.full(n, 257, np.int32), F], 1).astype(np.int32))
+    md = spectra_desc(n, nmel, mf)
+    ref = torch.zeros((n, nmel, mf), device="cuda")
+    assert audio.mel_filter_bank(spec, spd, ref, md, dims, 8000.0, 0.0, htk, nmel, 16000.0, normalize, gpu) == OK
+    out = canvas((n, nmel, mf))
+    assert audio.mel_filter_bank_tc(spec, spd, out, md, dims, 8000.0, 0.0, htk, nmel, 16000.0, normalize, precision,
+                                    gpu) == OK
+    r, o = host(ref), host(out)
+    for i in range(n):
+        assert (o[i, :, F[i]:] == -12345.0).all()
+        assert frame_rel_err(o[i, :, :F[i]], r[i, :, :F[i]]) < MEL_BOUND[precision]
+    assert audio.device_error(gpu) == 0
