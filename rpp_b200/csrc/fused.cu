@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 {
                     float acc = 0.0f;
                     const int e1 = csrRow[m + 1];
+#pragma unroll 4
                     for (int e = csrRow[m]; e < e1; ++e) acc = __fadd_rn(acc, __fmul_rn(so[csrBin[e]], csrW[e]));
                     *yp = acc;
                     tmax = fmaxf(tmax, acc);
@@ -280,12 +281,29 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 const int kDbGroups = kFusedThreads / a.dbFrames;
                 if (fd < Tv)
                 {
-                    for (int m = gd; m < nmel; m += kDbGroups)
+                    // 8 rows per step: the loads (mostly L2 hits) are in flight together
+                    constexpr int kRows = 8;
+                    const size_t step = size_t(kDbGroups) * hs;
+                    float* p = y + size_t(gd) * hs + fd;
+                    int m = gd;
+                    for (; m + (kRows - 1) * kDbGroups < nmel; m += kRows * kDbGroups, p += kRows * step)
                     {
-                        float* p = y + size_t(m) * hs + fd;
-                        float v = __fmul_rn(__ldcg(p), inv);
-                        v = a.minRatio < v ? v : a.minRatio;
-                        *p = __fmul_rn(a.multiplier, log2f(v));
+                        float v[kRows];
+#pragma unroll
+                        for (int r = 0; r < kRows; ++r) v[r] = __ldcg(p + r * step);
+#pragma unroll
+                        for (int r = 0; r < kRows; ++r)
+                        {
+                            float t = __fmul_rn(v[r], inv);
+                            t = a.minRatio < t ? t : a.minRatio;
+                            p[r * step] = __fmul_rn(a.multiplier, log2f(t));
+                        }
+                    }
+                    for (; m < nmel; m += kDbGroups, p += step)
+                    {
+                        float t = __fmul_rn(__ldcg(p), inv);
+                        t = a.minRatio < t ? t : a.minRatio;
+                        *p = __fmul_rn(a.multiplier, log2f(t));
                     }
                 }
             }

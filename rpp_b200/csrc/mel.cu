@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
                 if (live)
                 {
                     const int e1 = rowStart[m + 1];
+#pragma unroll 4
                     for (int e = rowStart[m]; e < e1; ++e)
                     {
                         const int2 en = ent[e];

@@ -139,8 +139,17 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
         (reinterpret_cast<uintptr_t>(src.x + spanStart) & 15) == 0)
     {
         const int quads = spanLen >> 2;
-        for (int q = threadIdx.x; q < quads; q += THREADS)
-            reinterpret_cast<float4*>(s_span)[q] = src.quad(spanStart + 4 * q);
+        // 4 quads per thread in flight before their stores
+        for (int q0 = threadIdx.x; q0 < quads; q0 += 4 * THREADS)
+        {
+            float4 v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (q0 + j * THREADS < quads) v[j] = src.quad(spanStart + 4 * (q0 + j * THREADS));
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (q0 + j * THREADS < quads) reinterpret_cast<float4*>(s_span)[q0 + j * THREADS] = v[j];
+        }
         for (int i = (quads << 2) + threadIdx.x; i < spanLen; i += THREADS) s_span[i] = src(spanStart + i);
     }
     else

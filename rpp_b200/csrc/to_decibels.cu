@@ -81,10 +81,25 @@ __global__ void __launch_bounds__(kThreads) decibel_max_kernel(const float* __re
         const uint32_t wdt = dims[2 * b], hgt = dims[2 * b + 1];
         const UnitSpan s = unit_span(wdt, hgt, w - prefix[b]);
         float m = -FLT_MAX;
-        for (uint32_t r = 0; r < s.rows; ++r)
+        // the unit's rows x cols elements, 4 loads per thread in flight
+        const uint32_t count = s.rows * s.cols;
+        const float* base = src + size_t(b) * nStride + size_t(s.row) * hStride + s.col0;
+        for (uint32_t i0 = threadIdx.x; i0 < count; i0 += 4 * kThreads)
         {
-            const float* x = src + size_t(b) * nStride + size_t(s.row + r) * hStride + s.col0;
-            for (uint32_t c = threadIdx.x; c < s.cols; c += kThreads) m = fmaxf(m, x[c]);
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const uint32_t i = i0 + j * kThreads;
+                v[j] = -FLT_MAX;
+                if (i < count)
+                {
+                    const uint32_t r = i / s.cols, c = i - r * s.cols;
+                    v[j] = base[size_t(r) * hStride + c];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) m = fmaxf(m, v[j]);
         }
         m = warp_max(m);
         if ((threadIdx.x & 31) == 0) warpMax[threadIdx.x >> 5] = m;
@@ -123,15 +138,30 @@ __global__ void __launch_bounds__(kThreads) decibel_kernel(const float* __restri
             ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
         }
         const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
-        for (uint32_t r = 0; r < s.rows; ++r)
+        // the unit's rows x cols elements, 4 per thread loaded before they are converted and stored
+        // (in-place calls alias src and dst: every element is loaded before its own store)
+        const uint32_t count = s.rows * s.cols;
+        const float* xb = src + size_t(b) * srcNStride + size_t(s.row) * srcHStride + s.col0;
+        float* yb = dst + size_t(b) * dstNStride + size_t(s.row) * dstHStride + s.col0;
+        for (uint32_t i0 = threadIdx.x; i0 < count; i0 += 4 * kThreads)
         {
-            const float* x = src + size_t(b) * srcNStride + size_t(s.row + r) * srcHStride + s.col0;
-            float* y = dst + size_t(b) * dstNStride + size_t(s.row + r) * dstHStride + s.col0;
-            for (uint32_t c = threadIdx.x; c < s.cols; c += kThreads)
+            float v[4];
+            uint32_t rr[4], cc[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
             {
-                float v = __fmul_rn(x[c], inv);
-                v = minRatio < v ? v : minRatio;
-                y[c] = __fmul_rn(multiplier, log2f(v));
+                const uint32_t i = i0 + j * kThreads;
+                rr[j] = i / s.cols;
+                cc[j] = i - rr[j] * s.cols;
+                if (i < count) v[j] = xb[size_t(rr[j]) * srcHStride + cc[j]];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                if (i0 + j * kThreads >= count) break;
+                float t = __fmul_rn(v[j], inv);
+                t = minRatio < t ? t : minRatio;
+                yb[size_t(rr[j]) * dstHStride + cc[j]] = __fmul_rn(multiplier, log2f(t));
             }
         }
     }
