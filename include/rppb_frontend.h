@@ -53,9 +53,10 @@ typedef struct
     Rpp32f referenceMagnitude; /* 0: per-sample maximum */
     /* schedule: clips by which the decibel tiles trail the spectrum tiles (0 = default 32) */
     Rpp32s lookahead;
-    /* schedule (never the results; rppb_frontend_tune_gpu picks them): frames per spectrum tile
-     * (0 = default, else the default or twice it), frames per decibel item (0 = 64, else a power
-     * of two from 16 to 256), CTAs per SM (0 = as many as fit) */
+    /* schedule (never the results; rppb_frontend_tune_gpu picks them): frames per spectrum item
+     * (0 = default, else 1, 2 or 4 times the FFT plan's tile of 16 frames for nfft >= 512, 32
+     * below), frames per decibel item (0 = 64, else a power of two from 16 to 256), CTAs per SM
+     * (0 = as many as fit) */
     Rpp32s tileFrames;
     Rpp32s dbFrames;
     Rpp32s ctasPerSm;

@@ -1,6 +1,6 @@
 // Autotuner of the fused front end's schedule (rppb_frontend_tune_gpu, include/rppb_frontend.h).
 //
-// The schedule knobs of RppbFrontendParams -- frames per spectrum tile, frames per decibel item,
+// The schedule knobs of RppbFrontendParams -- frames per spectrum item, frames per decibel item,
 // the decibel lookahead in clips and CTAs per SM -- change which CTA does what and when, never the
 // arithmetic of a frame, so every candidate writes the same bits.  The tuner times each candidate
 // on the caller's own batch (one untimed call, then the fastest of `reps` timed calls, CUDA events
@@ -112,7 +112,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_tune_gpu(RppPtr_t srcPtr, RpptD
         }
         const int t0 = plan_tile_frames(params->nfft);
         std::vector<Choice> cands;
-        for (int tf : {t0, 2 * t0})
+        for (int tf : {t0, 2 * t0, 4 * t0})
             for (int db : {32, 64, 128})
                 for (int la : {8, 32, 96})
                     for (int cps : {0, 2}) cands.push_back(Choice{tf, db, la, cps, 0.f});

@@ -4,10 +4,10 @@
 // Work items of two kinds walk one queue, claimed in order with an atomic counter:
 //   spectrum tile (clip b, frames f0..f0+TF): gather the pre-emphasized, reflected, windowed
 //     frames straight from the raw signal (stft.cuh, PreemphSource), FFT them into a shared
-//     power tile, project onto the mel filters from a shared CSR weight table (same weights and
-//     the same ascending-bin float accumulation as the mel_filter_bank kernel), write the mel
-//     power into dst, fold the tile maximum into the clip's float-ordered atomicMax, then count
-//     the tile done;
+//     power tile, project onto the mel filters with one sweep over the bins per thread group
+//     (same weights and the same ascending-bin float accumulation per filter as the
+//     mel_filter_bank kernel), write the mel power into dst, fold the tile maximum into the
+//     clip's float-ordered atomicMax, then count the tile done;
 //   decibel tile (clip b, same frames): wait until every spectrum tile of clip b is counted (a
 //     bounded wait: a timeout sets the handle's device error word and skips the tile), then
 //     convert the tile in place with the clip's maximum.
@@ -33,6 +33,7 @@ namespace rppb {
 
 constexpr int kFusedThreads = 256;
 constexpr int kDbFramesDefault = 64;          // frames per decibel item unless tuned
+constexpr int kSubTilesDefault = 2;           // spectrum tiles per spectrum item unless tuned
 constexpr int kFusedPrefixCache = 320;        // slots cached in shared memory (n + lookahead + 1)
 constexpr long long kWaitLimit = 1ll << 24;   // x ~128 ns sleeps: a few seconds
 
@@ -72,7 +73,8 @@ struct SlotCount
         const ClipView c = clip_view(a, b);
         return max(0, min(num_windows(c.L, a.W, a.hop, a.center), c.maxFrames));
     }
-    __device__ int tiles(int b) const { return (frames(b) + TF - 1) / TF; }
+    // spectrum items of clip b: subTiles tiles of TF frames each
+    __device__ int tiles(int b) const { return (frames(b) + TF * a.subTiles - 1) / (TF * a.subTiles); }
     __device__ int db_tiles(int b) const { return (frames(b) + a.dbFrames - 1) / a.dbFrames; }
     __device__ long long operator()(int s) const
     {
@@ -83,12 +85,56 @@ struct SlotCount
     }
 };
 
+// One claimed work item, decoded by thread 0 and handed to the CTA through shared memory.
+struct Item
+{
+    const float* x;
+    float* y;          // clip output at the item's first frame
+    uint32_t hs;
+    int L, F, f0, Tv, b;
+    int kind;          // 0 spectrum tile, 1 decibel tile, -1 queue exhausted
+    float coeff, bval;
+};
+
+template <int TF>
+__device__ Item decode_item(const FrontendArgs& a, const SlotCount<TF>& cnt, const long long* prefix, int nslots,
+                            long long total, long long w)
+{
+    Item it{};
+    if (w >= total)
+    {
+        it.kind = -1;
+        return it;
+    }
+    const int s = ragged_find(prefix, nslots, w);
+    const int local = int(w - prefix[s]);
+    const int c1 = s < a.n ? cnt.tiles(s) : 0;
+    const bool spectrumItem = local < c1;
+    it.kind = spectrumItem ? 0 : 1;
+    it.b = spectrumItem ? s : s - a.lookahead;
+    const int tile = spectrumItem ? local : local - c1;
+    const ClipView cv = clip_view(a, it.b);
+    it.x = cv.x;
+    it.L = cv.L;
+    it.F = min(num_windows(cv.L, a.W, a.hop, a.center), cv.maxFrames);
+    const int itemFrames = spectrumItem ? TF * a.subTiles : a.dbFrames;
+    it.f0 = tile * itemFrames;
+    it.Tv = min(itemFrames, it.F - it.f0);
+    it.y = cv.y + it.f0;
+    it.hs = cv.hStride;
+    it.coeff = cv.coeff;
+    it.bval = 0.f;
+    if (spectrumItem && a.border == 1) it.bval = cv.x[0];
+    else if (spectrumItem && a.border == 2 && cv.hasSecond) it.bval = cv.x[1];
+    return it;
+}
+
 // Shared memory plan (bytes), computed identically on host and device.
 template <int NFFT, int TF>
 struct FusedLayout
 {
     using S = StftShape<NFFT, kFusedThreads, TF>;
-    size_t tw, tw1, win, span, work, csrRow, csrBin, csrW, total;
+    size_t tw, tw1, win, span, work, melW, melIv, melGrp, total;
     __host__ __device__ FusedLayout(int numFilter, int W, int hop)
     {
         const int bins = S::BINS;
@@ -102,10 +148,10 @@ struct FusedLayout
         size_t tables = 2 * size_t(numFilter + 2) * 4 + size_t(numFilter) * 4 + 2 * size_t(numFilter + 1) * 8 +
                         size_t(bins) * 4 + 64;
         size_t workBytes = (fftOut > tables ? fftOut : tables);
-        csrRow = (work + workBytes + 15) & ~size_t(15);
-        csrBin = (csrRow + size_t(numFilter + 1) * 4 + 15) & ~size_t(15);
-        csrW = (csrBin + size_t(2 * bins + 2) * 2 + 15) & ~size_t(15);
-        total = (csrW + size_t(2 * bins + 2) * 4 + 15) & ~size_t(15);
+        melW = (work + workBytes + 15) & ~size_t(15);
+        melIv = (melW + size_t(bins) * 8 + 15) & ~size_t(15);
+        melGrp = (melIv + size_t(numFilter + 1) * 8 + 15) & ~size_t(15);
+        total = (melGrp + size_t(kFusedThreads / TF + 1) * 4 + 15) & ~size_t(15);
     }
 };
 
@@ -126,17 +172,20 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     float* s_span = reinterpret_cast<float*>(smem + lay.span);
     float2* s_fft = reinterpret_cast<float2*>(smem + lay.work);
     float* s_out = reinterpret_cast<float*>(smem + lay.work + S::fft_bytes);
-    int* csrRow = reinterpret_cast<int*>(smem + lay.csrRow);
-    unsigned short* csrBin = reinterpret_cast<unsigned short*>(smem + lay.csrBin);   // bin * LD: tile row offset
-    float* csrW = reinterpret_cast<float*>(smem + lay.csrW);
-    __shared__ long long s_item;
+    float2* melW = reinterpret_cast<float2*>(smem + lay.melW);   // bin k: (weight into filter i, into filter i - 1)
+    int2* melIv = reinterpret_cast<int2*>(smem + lay.melIv);     // interval i: bins [x, y)
+    int* melGrp = reinterpret_cast<int*>(smem + lay.melGrp);     // thread group g: filters [g], [g + 1])
     __shared__ float s_warpMax[kFusedThreads / 32];
     const int nmel = a.mel.numFilter;
 
     stft_tables<NFFT, kFusedThreads>(twiddle, a.window, a.W, s_tw, s_tw1, s_win);
 
-    // ---- mel weights as CSR rows (filter m: bins of interval m with (1 - wd) * norm, then bins of
-    //      interval m + 1 with wd * norm), built in the work region before it holds FFT data
+    // ---- mel weights by bin.  Bin k of interval i (between mel points i and i + 1) weighs
+    //      (1 - wd_k) * norm_i into filter i and wd_k * norm_(i-1) into filter i - 1, so filter m
+    //      sums interval m's bins, then interval m + 1's, in ascending bin order -- the order and
+    //      the weights of the mel_filter_bank kernel.  The tables are built in the work region
+    //      before it holds FFT data.
+    constexpr int kGroups = kFusedThreads / TF;
     {
         unsigned char* t = smem + lay.work;
         MelTableView v;
@@ -149,34 +198,38 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         v.weightsDown = reinterpret_cast<float*>(v.f1 + (nmel + 1));
         v.range = reinterpret_cast<int*>(v.weightsDown + BINS);
         build_mel_tables(v, a.mel, NFFT);   // ends with __syncthreads
+        for (int i = threadIdx.x; i <= nmel; i += kFusedThreads)
+        {
+            const int k0 = v.first[i], k1 = v.last[i];
+            melIv[i] = k1 > k0 ? make_int2(k0, k1) : make_int2(0, 0);
+            for (int k = k0; k < k1; ++k)
+            {
+                const float wd = v.weightsDown[k];
+                float rise = 0.f, fall = 0.f;
+                if (i < nmel)
+                {
+                    rise = __fsub_rn(1.0f, wd);
+                    if (a.mel.normalize) rise = __fmul_rn(rise, v.norm[i]);
+                }
+                if (i > 0) fall = a.mel.normalize ? __fmul_rn(wd, v.norm[i - 1]) : wd;
+                melW[k] = make_float2(rise, fall);
+            }
+        }
         if (threadIdx.x == 0)
         {
-            int acc = 0;
-            for (int m = 0; m < nmel; ++m)
+            // group g emits filters [melGrp[g], melGrp[g + 1]) and sweeps their intervals; the
+            // groups' shares of (bins + 2) per interval are balanced
+            auto cost = [&](int i) { return (v.last[i] > v.first[i] ? v.last[i] - v.first[i] : 0) + 2; };
+            int totalCost = 0;
+            for (int i = 0; i <= nmel; ++i) totalCost += cost(i);
+            int acc = cost(0), grp = 1;
+            melGrp[0] = 0;
+            for (int m = 0; m < nmel && grp < kGroups; ++m)
             {
-                csrRow[m] = acc;
-                if (v.last[m] > v.first[m]) acc += v.last[m] - v.first[m];
-                if (v.last[m + 1] > v.first[m + 1]) acc += v.last[m + 1] - v.first[m + 1];
+                acc += cost(m + 1);
+                while (grp < kGroups && acc * kGroups >= grp * totalCost) melGrp[grp++] = m + 1;
             }
-            csrRow[nmel] = acc;
-        }
-        __syncthreads();
-        for (int m = threadIdx.x; m < nmel; m += kFusedThreads)
-        {
-            int e = csrRow[m];
-            const float nm = v.norm[m];
-            for (int k = v.first[m]; k < v.last[m]; ++k, ++e)
-            {
-                float w = __fsub_rn(1.0f, v.weightsDown[k]);
-                csrBin[e] = (unsigned short)(k * LD);
-                csrW[e] = a.mel.normalize ? __fmul_rn(w, nm) : w;
-            }
-            for (int k = v.first[m + 1]; k < v.last[m + 1]; ++k, ++e)
-            {
-                const float w = v.weightsDown[k];
-                csrBin[e] = (unsigned short)(k * LD);
-                csrW[e] = a.mel.normalize ? __fmul_rn(w, nm) : w;
-            }
+            while (grp <= kGroups) melGrp[grp++] = nmel;
         }
         __syncthreads();
     }
@@ -189,64 +242,74 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     const SlotCount<TF> cnt{a, a.n, a.lookahead};
     const int f = threadIdx.x % TF;      // frame column this thread owns in mel / decibel tiles
     const int g = threadIdx.x / TF;
-    constexpr int kGroups = kFusedThreads / TF;
 
+    // Thread 0 claims one item ahead (the claim's latency overlaps the current item) and decodes
+    // the next item for the CTA while finishing the current one.  A CTA's current item always has
+    // a lower index than the one it holds claimed, so the lowest unfinished item is always some
+    // CTA's current one, whose decibel wait (on lower spectrum items only) ends: claiming ahead
+    // keeps the waits deadlock-free.
+    __shared__ Item s_it;
+    __shared__ int s_ok;
+    long long wNext = 0;
+    if (threadIdx.x == 0)
+    {
+        const long long w0 = (long long)atomicAdd(workCounter, 1ull);
+        wNext = (long long)atomicAdd(workCounter, 1ull);
+        s_it = decode_item<TF>(a, cnt, prefix, nslots, total, w0);
+    }
+    __syncthreads();
     for (;;)
     {
-        if (threadIdx.x == 0) s_item = (long long)atomicAdd(workCounter, 1ull);
-        __syncthreads();
-        const long long w = s_item;
-        if (w >= total) break;
-        const int s = ragged_find(prefix, nslots, w);
-        const int local = int(w - prefix[s]);
-        const int c1 = s < a.n ? cnt.tiles(s) : 0;
-        const bool spectrumItem = local < c1;
-        const int b = spectrumItem ? s : s - a.lookahead;
-        const int tile = spectrumItem ? local : local - c1;
-        const ClipView cv = clip_view(a, b);
-        const int L = cv.L;
-        const int F = min(num_windows(L, a.W, a.hop, a.center), cv.maxFrames);
-        const int f0 = tile * (spectrumItem ? TF : a.dbFrames);
-        const int Tv = min(spectrumItem ? TF : a.dbFrames, F - f0);
-        float* y = cv.y + f0;
-        const uint32_t hs = cv.hStride;
+        // s_it is rewritten only after the barrier that ends this item's work
+        const Item it = s_it;
+        if (it.kind < 0) break;
+        const int b = it.b;
+        const uint32_t hs = it.hs;
 
-        if (spectrumItem)
+        if (it.kind == 0)
         {
-            const float* x = cv.x;
-            const float bval = a.border == 1 ? x[0] : a.border == 2 ? (cv.hasSecond ? x[1] : 0.f) : 0.f;
-            const PreemphSource src{x, L, a.reflect, cv.coeff, bval};
-            stft_tile<NFFT, kFusedThreads, TFX>(src, f0, F, a.W, a.hop, centerOffset, a.power, s_win, s_tw, s_tw1, s_span,
-                                           s_fft, s_out);
-            __syncthreads();
+            // subTiles tiles of TF frames; each tile's staging barrier also orders the previous
+            // tile's mel reads of s_out before this tile's FFT overwrites it
+            const PreemphSource src{it.x, it.L, a.reflect, it.coeff, it.bval};
             float tmax = -FLT_MAX;
-            if (f < Tv)
+            for (int t = 0; t < a.subTiles; ++t)
             {
-                const float* so = s_out + f;
-                float* yp = y + size_t(g) * hs + f;
-                const size_t ystep = size_t(kGroups) * hs;
-                for (int m = g; m < nmel; m += kGroups, yp += ystep)
+                const int f0 = it.f0 + t * TF;
+                if (f0 >= it.F) break;   // uniform over the CTA
+                stft_tile<NFFT, kFusedThreads, TFX>(src, f0, it.F, a.W, a.hop, centerOffset, a.power, s_win, s_tw,
+                                                    s_tw1, s_span, s_fft, s_out);
+                __syncthreads();
+                if (f < it.F - f0)
                 {
-                    float acc = 0.0f;
-                    const int e1 = csrRow[m + 1];
-#pragma unroll 4
-                    for (int e = csrRow[m]; e < e1; ++e) acc = __fadd_rn(acc, __fmul_rn(so[csrBin[e]], csrW[e]));
-                    *yp = acc;
-                    tmax = fmaxf(tmax, acc);
+                    // one sweep over the group's intervals; each power value is read once
+                    const int m0 = melGrp[g], m1 = melGrp[g + 1];
+                    float* yp = it.y + size_t(f0 - it.f0) + size_t(m0) * hs + f;
+                    float fall = 0.f;   // filter i - 1: its rising sum, then its falling terms
+                    for (int i = m0; i <= m1; ++i)
+                    {
+                        const int2 iv = melIv[i];
+                        const float* sp = s_out + iv.x * LD + f;
+                        float rise = 0.f;   // filter i
+#pragma unroll 2
+                        for (int k = iv.x; k < iv.y; ++k, sp += LD)
+                        {
+                            const float pw = *sp;
+                            const float2 w = melW[k];
+                            fall = __fadd_rn(fall, __fmul_rn(pw, w.y));
+                            rise = __fadd_rn(rise, __fmul_rn(pw, w.x));
+                        }
+                        if (i > m0)
+                        {
+                            *yp = fall;
+                            yp += hs;
+                            tmax = fmaxf(tmax, fall);
+                        }
+                        fall = rise;
+                    }
                 }
             }
             tmax = warp_max(tmax);
             if ((threadIdx.x & 31) == 0) s_warpMax[threadIdx.x >> 5] = tmax;
-            __threadfence();   // each thread's mel stores are visible device-wide before the tile is counted
-            __syncthreads();
-            if (threadIdx.x == 0)
-            {
-                float v = s_warpMax[0];
-                for (int i = 1; i < kFusedThreads / 32; ++i) v = fmaxf(v, s_warpMax[i]);
-                atomicMax(maxKey + b, float_key(v));
-                __threadfence();
-                atomicAdd(done + b, 1);
-            }
         }
         else
         {
@@ -264,10 +327,10 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                     __nanosleep(128);
                 }
                 __threadfence();
-                s_item = spins > kWaitLimit ? -1 : w;
+                s_ok = spins <= kWaitLimit;
             }
             __syncthreads();
-            if (s_item >= 0)
+            if (s_ok)
             {
                 float ref = a.refMag;
                 if (a.refMag == 0.f)
@@ -279,12 +342,12 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 const int fd = threadIdx.x & (a.dbFrames - 1);   // dbFrames: power of two <= threads
                 const int gd = threadIdx.x / a.dbFrames;
                 const int kDbGroups = kFusedThreads / a.dbFrames;
-                if (fd < Tv)
+                if (fd < it.Tv)
                 {
                     // 8 rows per step: the loads (mostly L2 hits) are in flight together
                     constexpr int kRows = 8;
                     const size_t step = size_t(kDbGroups) * hs;
-                    float* p = y + size_t(gd) * hs + fd;
+                    float* p = it.y + size_t(gd) * hs + fd;
                     int m = gd;
                     for (; m + (kRows - 1) * kDbGroups < nmel; m += kRows * kDbGroups, p += kRows * step)
                     {
@@ -296,17 +359,35 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                         {
                             float t = __fmul_rn(v[r], inv);
                             t = a.minRatio < t ? t : a.minRatio;
-                            p[r * step] = __fmul_rn(a.multiplier, log2f(t));
+                            p[r * step] = __fmul_rn(a.multiplier, __log2f(t));
                         }
                     }
                     for (; m < nmel; m += kDbGroups, p += step)
                     {
                         float t = __fmul_rn(__ldcg(p), inv);
                         t = a.minRatio < t ? t : a.minRatio;
-                        *p = __fmul_rn(a.multiplier, log2f(t));
+                        *p = __fmul_rn(a.multiplier, __log2f(t));
                     }
                 }
             }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            const long long w = wNext;
+            if (w < total) wNext = (long long)atomicAdd(workCounter, 1ull);
+            const Item nx = decode_item<TF>(a, cnt, prefix, nslots, total, w);
+            if (it.kind == 0)
+            {
+                // the barrier orders every thread's mel stores before this thread's device-scope
+                // fence, which orders them before the count (the grid-barrier release pattern)
+                float v = s_warpMax[0];
+                for (int i = 1; i < kFusedThreads / 32; ++i) v = fmaxf(v, s_warpMax[i]);
+                atomicMax(maxKey + b, float_key(v));
+                __threadfence();
+                atomicAdd(done + b, 1);
+            }
+            s_it = nx;
         }
         __syncthreads();
     }
@@ -352,14 +433,17 @@ size_t frontend_scratch_bytes(int n, int lookahead)
 
 namespace {
 
-// Tile frames: the plan's default or twice it (both bit-identical; the autotuner picks).
+// Frames per spectrum item: the plan's tile (default) or 2 or 4 of them, computed one tile after
+// another (all bit-identical; the autotuner picks).
 template <int NFFT>
-void launch_nfft(Handle& h, const FrontendArgs& a, void* scratch)
+void launch_nfft(Handle& h, const FrontendArgs& args, void* scratch)
 {
     constexpr int T0 = Plan<NFFT>::TF;
-    if (a.tileFrames == 0 || a.tileFrames == T0) launch_fused<NFFT, T0>(h, a, scratch);
-    else if (a.tileFrames == 2 * T0) launch_fused<NFFT, 2 * T0>(h, a, scratch);
-    else fail(RPP_ERROR_NOT_IMPLEMENTED, "tileFrames must be 0, " + std::to_string(T0) + " or " + std::to_string(2 * T0));
+    FrontendArgs a = args;
+    a.subTiles = a.tileFrames == 0 ? kSubTilesDefault : a.tileFrames / T0;
+    if (a.tileFrames != 0 && (a.tileFrames % T0 != 0 || (a.subTiles != 1 && a.subTiles != 2 && a.subTiles != 4)))
+        fail(RPP_ERROR_NOT_IMPLEMENTED, "tileFrames must be 0 or 1, 2 or 4 times " + std::to_string(T0));
+    launch_fused<NFFT, T0>(h, a, scratch);
 }
 
 }  // namespace

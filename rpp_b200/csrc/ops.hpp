@@ -134,9 +134,10 @@ struct FrontendArgs
     float outRate;
     float coeffAll;
     int reserveSms;          // SMs' worth of CTA slots left to kernels on other streams
-    // schedule (never the arithmetic): frames per spectrum tile (0: plan default), frames per
-    // decibel item (0: 64), CTAs per SM (0: as many as fit)
+    // schedule (never the arithmetic): frames per spectrum item (0: the plan's tile; else 1, 2 or
+    // 4 tiles), frames per decibel item (0: 64), CTAs per SM (0: as many as fit)
     int tileFrames, dbFrames, ctasPerSm;
+    int subTiles;            // set by launch_frontend: tiles per spectrum item
 };
 size_t frontend_scratch_bytes(int n, int lookahead);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);

@@ -156,7 +156,8 @@ def test_frontend_host_equals_device(gpu, chunks, pinned_io):
     assert audio.device_error(gpu) == 0
 
 
-SCHEDULES = [dict(tile_frames=32), dict(db_frames=32, lookahead=8), dict(db_frames=128, ctas_per_sm=1),
+SCHEDULES = [dict(tile_frames=32), dict(tile_frames=64, db_frames=16), dict(db_frames=32, lookahead=8),
+             dict(db_frames=128, ctas_per_sm=1),
              dict(tile_frames=32, db_frames=256, lookahead=96, ctas_per_sm=2)]
 
 
@@ -191,7 +192,7 @@ def test_frontend_tune(gpu):
     out = canvas((n, 128, mf))
     st, ms = audio.frontend_tune(xd, sd, out, dd, ld, cd, p, gpu, reps=2)
     assert st == OK and ms > 0
-    assert p.tileFrames in (16, 32) and p.dbFrames in (32, 64, 128) and p.lookahead in (8, 32, 96)
+    assert p.tileFrames in (16, 32, 64) and p.dbFrames in (32, 64, 128) and p.lookahead in (8, 32, 96)
     assert p.ctasPerSm in (0, 2)
     np.testing.assert_array_equal(host(out), host(ref))
     q = frontend_params()
