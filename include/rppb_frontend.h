@@ -54,8 +54,8 @@ typedef struct
     /* schedule: clips by which the decibel tiles trail the spectrum tiles (0 = default 32) */
     Rpp32s lookahead;
     /* schedule (never the results; rppb_frontend_tune_gpu picks them): frames per spectrum item
-     * (0 = default, else 1, 2 or 4 times the FFT plan's tile of 16 frames for nfft >= 512, 32
-     * below), frames per decibel item (0 = 64, else a power of two from 16 to 256), CTAs per SM
+     * (0 = 2 tiles, else 1, 2 or 4 times the FFT plan's tile of 16 frames for nfft >= 512, 32
+     * below), frames per decibel item (0 = 128, else a power of two from 16 to 256), CTAs per SM
      * (0 = as many as fit) */
     Rpp32s tileFrames;
     Rpp32s dbFrames;

@@ -32,7 +32,7 @@
 namespace rppb {
 
 constexpr int kFusedThreads = 256;
-constexpr int kDbFramesDefault = 64;          // frames per decibel item unless tuned
+constexpr int kDbFramesDefault = 128;         // frames per decibel item unless tuned
 constexpr int kSubTilesDefault = 2;           // spectrum tiles per spectrum item unless tuned
 constexpr int kFusedPrefixCache = 320;        // slots cached in shared memory (n + lookahead + 1)
 constexpr long long kWaitLimit = 1ll << 24;   // x ~128 ns sleeps: a few seconds
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     __shared__ float s_warpMax[kFusedThreads / 32];
     const int nmel = a.mel.numFilter;
 
-    stft_tables<NFFT, kFusedThreads>(twiddle, a.window, a.W, s_tw, s_tw1, s_win);
+    stft_tables<NFFT, kFusedThreads>(twiddle, a.window, a.W, s_tw, s_tw1, s_win, s_span);
 
     // ---- mel weights by bin.  Bin k of interval i (between mel points i and i + 1) weighs
     //      (1 - wd_k) * norm_i into filter i and wd_k * norm_(i-1) into filter i - 1, so filter m

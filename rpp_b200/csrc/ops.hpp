@@ -135,7 +135,7 @@ struct FrontendArgs
     float coeffAll;
     int reserveSms;          // SMs' worth of CTA slots left to kernels on other streams
     // schedule (never the arithmetic): frames per spectrum item (0: the plan's tile; else 1, 2 or
-    // 4 tiles), frames per decibel item (0: 64), CTAs per SM (0: as many as fit)
+    // 4 tiles), frames per decibel item (0: 128), CTAs per SM (0: as many as fit)
     int tileFrames, dbFrames, ctasPerSm;
     int subTiles;            // set by launch_frontend: tiles per spectrum item
 };

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kThreads, (NFFT <= 512 ? 3 : 2)) spectrogram_f
     float* s_out = reinterpret_cast<float*>(smem + lay.out);
 
     const int W = a.windowLength;
-    stft_tables<NFFT, kThreads>(twiddle, a.window, W, s_tw, s_tw1, s_win);
+    stft_tables<NFFT, kThreads>(twiddle, a.window, W, s_tw, s_tw1, s_win, s_span);
     const int centerOffset = a.center ? W / 2 : 0;
     __shared__ long long s_prefix[kPrefixCache];
     prefix = cache_prefix(prefix, a.n, s_prefix);

@@ -18,6 +18,8 @@
 //      O = (Z[k] - conj Z[M-k]) / 2i.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -55,8 +57,21 @@ struct StftShape
     static constexpr size_t tw1_bytes = size_t(R1) * R2 * 8;      // W_M^(j*k1) as [k1][j]
     static_assert(R1 * R2 == M, "plan");
     static_assert(R1 % G == 0, "stage 2 assigns R1 / G rows per thread");
-    // span staged per tile: (TF - 1) * hop + W floats (runtime), rounded for alignment
-    __host__ __device__ static size_t span_bytes(int W, int hop) { return (size_t((TF - 1) * hop + W) * 4 + 15) & ~size_t(15); }
+    // The window starts at offset (nfft - W) / 2 of the nfft buffer (0 when W >= nfft).
+    __host__ __device__ static int window_offset(int W) { return W < NFFT ? (NFFT - W) / 2 : 0; }
+    // Span buffer: span_pad zero floats (>= the window offset, a multiple of 4), the tile's
+    // (TF - 1) * hop + W staged samples, then up to nfft - offset - W more zeros, so every frame
+    // reads a full nfft-sample buffer without bounds checks (the window is 0 outside [0, W)).
+    __host__ __device__ static int span_pad(int W) { return (window_offset(W) + 3) & ~3; }
+    __host__ __device__ static int span_tail(int W)
+    {
+        const int t = NFFT - window_offset(W) - W;
+        return t > 0 ? t : 0;
+    }
+    __host__ __device__ static size_t span_bytes(int W, int hop)
+    {
+        return (size_t(span_pad(W) + (TF - 1) * hop + W + span_tail(W)) * 4 + 15) & ~size_t(15);
+    }
 };
 
 // The signal as stored.
@@ -104,10 +119,12 @@ struct PreemphSource
 };
 
 // Fills the per-CTA constant tables: s_tw[k] = W_nfft^k (k <= M/2, the unpack twiddles), s_tw1[k1][j] =
-// W_M^(j*k1) = W_nfft^(2*j*k1), s_win[t] = window[t].  All threads call; ends with __syncthreads.
+// W_M^(j*k1) = W_nfft^(2*j*k1), s_win[n] = the window in buffer coordinates (window[n - offset] for
+// n - offset in [0, W), else 0), and zeroes the span buffer's leading pad (never staged over).
+// All threads call; ends with __syncthreads.
 template <int NFFT, int THREADS>
 __device__ __forceinline__ void stft_tables(const float2* __restrict__ twiddle, const float* __restrict__ window, int W,
-                                            float2* s_tw, float2* s_tw1, float* s_win)
+                                            float2* s_tw, float2* s_tw1, float* s_win, float* s_span)
 {
     using S = StftShape<NFFT, THREADS>;
     for (int i = threadIdx.x; i <= S::M / 2; i += THREADS) s_tw[i] = twiddle[i];
@@ -116,7 +133,9 @@ __device__ __forceinline__ void stft_tables(const float2* __restrict__ twiddle, 
         const int k1 = i / S::R2, j = i % S::R2;
         s_tw1[i] = twiddle[(2 * j * k1) & (NFFT - 1)];
     }
-    for (int i = threadIdx.x; i < NFFT; i += THREADS) s_win[i] = i < W ? window[i] : 0.f;
+    const int off = S::window_offset(W);
+    for (int i = threadIdx.x; i < NFFT; i += THREADS) s_win[i] = (i >= off && i - off < W) ? window[i - off] : 0.f;
+    for (int i = threadIdx.x; i < S::span_pad(W); i += THREADS) s_span[i] = 0.f;
     __syncthreads();
 }
 
@@ -131,10 +150,11 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
     using S = StftShape<NFFT, THREADS, TFX>;
     constexpr int M = S::M, R1 = S::R1, R2 = S::R2, TF = S::TF, G = S::G, FPP = S::FPP, BINS = S::BINS;
 
-    // ---- 1. stage the tile's input span
+    // ---- 1. stage the tile's input span (after the zero pad), then zero its tail
     const int Tv = min(TF, F - f0);
     const int spanStart = f0 * hop - centerOffset;
     const int spanLen = (Tv - 1) * hop + W;
+    float* const s_data = s_span + S::span_pad(W);
     if (spanStart >= 0 && spanStart + spanLen <= src.L &&
         (reinterpret_cast<uintptr_t>(src.x + spanStart) & 15) == 0)
     {
@@ -148,50 +168,77 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
                 if (q0 + j * THREADS < quads) v[j] = src.quad(spanStart + 4 * (q0 + j * THREADS));
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (q0 + j * THREADS < quads) reinterpret_cast<float4*>(s_span)[q0 + j * THREADS] = v[j];
+                if (q0 + j * THREADS < quads) reinterpret_cast<float4*>(s_data)[q0 + j * THREADS] = v[j];
         }
-        for (int i = (quads << 2) + threadIdx.x; i < spanLen; i += THREADS) s_span[i] = src(spanStart + i);
+        for (int i = (quads << 2) + threadIdx.x; i < spanLen; i += THREADS) s_data[i] = src(spanStart + i);
     }
     else
     {
-        for (int i = threadIdx.x; i < spanLen; i += THREADS) s_span[i] = src(spanStart + i);
+        for (int i = threadIdx.x; i < spanLen; i += THREADS) s_data[i] = src(spanStart + i);
     }
+    for (int i = threadIdx.x; i < S::span_tail(W); i += THREADS) s_data[spanLen + i] = 0.f;
     __syncthreads();
 
     const int j = threadIdx.x % G;
     const int slot = threadIdx.x / G;
     float2* buf = s_fft + slot * S::FFT_SLOT;
-    const int off = (W < NFFT) ? (NFFT - W) / 2 : 0;
-    const bool pairs = ((off | hop) & 1) == 0;   // (window index, span index) pairs are 8-byte aligned
+    const int off = S::window_offset(W);
+    const bool pairs = ((off | hop) & 1) == 0;   // (window, sample) pairs are 8-byte aligned
+
+    // power (2) or magnitude (1) of bins k and M - k, as the two halves of the unpack share loads
+    auto unpack = [&](auto magTag, int fl) {
+        constexpr bool kMag = decltype(magTag)::value;
+        for (int k = j; k <= M / 2; k += G)
+        {
+            const float2 A = buf[k];
+            const float2 B = buf[(M - k) & (M - 1)];
+            // E = (A + conj(B)) / 2,  O = (A - conj(B)) / (2i),  P = W^k O
+            const float2 sum = fft::mul2(make_float2(0.5f, 0.5f), fft::add2(A, B));   // (er, orr)
+            const float2 dif = fft::mul2(make_float2(-0.5f, 0.5f), fft::sub2(A, B));  // (oi, ei)
+            const float er = sum.x, orr = sum.y, oi = dif.x, ei = dif.y;
+            const float2 t = s_tw[k];
+            const float pr = fmaf(orr, t.x, oi * t.y);
+            const float pi = fmaf(oi, t.x, -orr * t.y);
+            const float2 X = fft::add2(make_float2(er, ei), make_float2(pr, pi));   // X[k] = E + P
+            const float2 Y = fft::sub2(make_float2(er, ei), make_float2(pr, pi));   // X[M-k] = conj(E - P)
+            const float2 sq = fft::mul2(make_float2(X.y, Y.y), make_float2(X.y, Y.y));
+            const float p0 = fmaf(X.x, X.x, sq.x);
+            const float p1 = fmaf(Y.x, Y.x, sq.y);
+            s_out[k * S::OUT_LD + fl] = kMag ? sqrtf(p0) : p0;
+            if (k != M - k) s_out[(M - k) * S::OUT_LD + fl] = kMag ? sqrtf(p1) : p1;
+        }
+    };
+
 #pragma unroll 1
     for (int pass = 0; pass < S::PASSES; ++pass)
     {
         const int fl = pass * FPP + slot;
         const bool live = fl < Tv;
-        const float* fs = s_span + fl * hop;     // frame start in the span
+        // buffer sample n of frame fl is fs[n]; the pads make every n in [0, nfft) readable
+        const float* fs = s_data + fl * hop - off;
         float2 z[R1];
-#pragma unroll
-        for (int m = 0; m < R1; ++m)
+        if (live && pairs)
         {
-            const int t0 = 2 * (j + R2 * m) - off;   // window index of the real part
-            float re = 0.f, im = 0.f;
-            if (live)
+#pragma unroll
+            for (int m = 0; m < R1; ++m)
             {
-                if (pairs && t0 >= 0 && t0 + 1 < W)
-                {
-                    const float2 d = *reinterpret_cast<const float2*>(fs + t0);
-                    const float2 wv = *reinterpret_cast<const float2*>(s_win + t0);
-                    const float2 p = fft::mul2(wv, d);
-                    re = p.x;
-                    im = p.y;
-                }
-                else
-                {
-                    if (t0 >= 0 && t0 < W) re = s_win[t0] * fs[t0];
-                    if (t0 + 1 >= 0 && t0 + 1 < W) im = s_win[t0 + 1] * fs[t0 + 1];
-                }
+                const int n = 2 * (j + R2 * m);
+                z[m] = fft::mul2(*reinterpret_cast<const float2*>(s_win + n), *reinterpret_cast<const float2*>(fs + n));
             }
-            z[m] = make_float2(re, im);
+        }
+        else if (live)
+        {
+#pragma unroll
+            for (int m = 0; m < R1; ++m)
+            {
+                const int n = 2 * (j + R2 * m);
+                z[m] = make_float2(s_win[n] * fs[n], s_win[n + 1] * fs[n + 1]);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int m = 0; m < R1; ++m) z[m] = make_float2(0.f, 0.f);
         }
         fft::Dft<R1>::run(z);
 #pragma unroll
@@ -222,25 +269,8 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
         __syncwarp();
         if (fl < TF)
         {
-            for (int k = j; k <= M / 2; k += G)
-            {
-                const float2 A = buf[k];
-                const float2 B = buf[(M - k) & (M - 1)];
-                // E = (A + conj(B)) / 2,  O = (A - conj(B)) / (2i),  P = W^k O
-                const float2 sum = fft::mul2(make_float2(0.5f, 0.5f), fft::add2(A, B));   // (er, orr)
-                const float2 dif = fft::mul2(make_float2(-0.5f, 0.5f), fft::sub2(A, B));  // (oi, ei)
-                const float er = sum.x, orr = sum.y, oi = dif.x, ei = dif.y;
-                const float2 t = s_tw[k];
-                const float pr = fmaf(orr, t.x, oi * t.y);
-                const float pi = fmaf(oi, t.x, -orr * t.y);
-                const float2 X = fft::add2(make_float2(er, ei), make_float2(pr, pi));   // X[k] = E + P
-                const float2 Y = fft::sub2(make_float2(er, ei), make_float2(pr, pi));   // X[M-k] = conj(E - P)
-                const float2 sq = fft::mul2(make_float2(X.y, Y.y), make_float2(X.y, Y.y));
-                const float p0 = fmaf(X.x, X.x, sq.x);
-                const float p1 = fmaf(Y.x, Y.x, sq.y);
-                s_out[k * S::OUT_LD + fl] = (power == 1) ? sqrtf(p0) : p0;
-                if (k != M - k) s_out[(M - k) * S::OUT_LD + fl] = (power == 1) ? sqrtf(p1) : p1;
-            }
+            if (power == 1) unpack(std::true_type{}, fl);
+            else unpack(std::false_type{}, fl);
         }
         __syncwarp();
     }
