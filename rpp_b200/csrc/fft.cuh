@@ -72,7 +72,10 @@ struct Tw
 };
 
 // Paired FP32 arithmetic (sm_100 add/sub/mul.rn.f32x2): one instruction for both components,
-// each rounded exactly as the scalar operation would be.
+// each rounded as the scalar operation would be.  The assembler may still contract a paired
+// multiply whose only use is a paired add into a fused multiply-add, so code that must round the
+// product and the sum separately (the mel sums, which replay the reference) uses __fmul_rn and
+// __fadd_rn instead.
 #define RPPB_F32X2(NAME, OP)                                                                               \
     __device__ __forceinline__ float2 NAME(float2 a, float2 b)                                             \
     {                                                                                                      \

@@ -151,7 +151,7 @@ struct FusedLayout
         melW = (work + workBytes + 15) & ~size_t(15);
         melIv = (melW + size_t(bins) * 8 + 15) & ~size_t(15);
         melGrp = (melIv + size_t(numFilter + 1) * 8 + 15) & ~size_t(15);
-        total = (melGrp + size_t(kFusedThreads / TF + 1) * 4 + 15) & ~size_t(15);
+        total = (melGrp + size_t(2 * kFusedThreads / TF + 1) * 4 + 15) & ~size_t(15);
     }
 };
 
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     //      sums interval m's bins, then interval m + 1's, in ascending bin order -- the order and
     //      the weights of the mel_filter_bank kernel.  The tables are built in the work region
     //      before it holds FFT data.
-    constexpr int kGroups = kFusedThreads / TF;
+    constexpr int kGroups = 2 * kFusedThreads / TF;   // mel thread groups: TF / 2 frame pairs each
     {
         unsigned char* t = smem + lay.work;
         MelTableView v;
@@ -240,8 +240,8 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     prefix = cache_prefix<kFusedPrefixCache>(prefix, nslots, s_prefix);
     const long long total = prefix[nslots];
     const SlotCount<TF> cnt{a, a.n, a.lookahead};
-    const int f = threadIdx.x % TF;      // frame column this thread owns in mel / decibel tiles
-    const int g = threadIdx.x / TF;
+    const int f = 2 * (threadIdx.x % (TF / 2));   // first of the two frame columns this thread owns in mel tiles
+    const int g = threadIdx.x / (TF / 2);
 
     // Thread 0 claims one item ahead (the claim's latency overlaps the current item) and decodes
     // the next item for the CTA while finishing the current one.  A CTA's current item always has
@@ -281,28 +281,38 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 __syncthreads();
                 if (f < it.F - f0)
                 {
-                    // one sweep over the group's intervals; each power value is read once
+                    // one sweep over the group's intervals for frames f and f + 1; each power
+                    // pair is read once.  Scalar __fmul_rn / __fadd_rn: a paired multiply feeding
+                    // a paired add may be contracted into one rounding by the assembler.
+                    const bool second = f + 1 < it.F - f0;
                     const int m0 = melGrp[g], m1 = melGrp[g + 1];
                     float* yp = it.y + size_t(f0 - it.f0) + size_t(m0) * hs + f;
-                    float fall = 0.f;   // filter i - 1: its rising sum, then its falling terms
+                    float2 fall = make_float2(0.f, 0.f);   // filter i - 1: rising sum, then falling terms
                     for (int i = m0; i <= m1; ++i)
                     {
                         const int2 iv = melIv[i];
                         const float* sp = s_out + iv.x * LD + f;
-                        float rise = 0.f;   // filter i
+                        float2 rise = make_float2(0.f, 0.f);   // filter i
 #pragma unroll 2
                         for (int k = iv.x; k < iv.y; ++k, sp += LD)
                         {
-                            const float pw = *sp;
+                            const float2 pw = *reinterpret_cast<const float2*>(sp);
                             const float2 w = melW[k];
-                            fall = __fadd_rn(fall, __fmul_rn(pw, w.y));
-                            rise = __fadd_rn(rise, __fmul_rn(pw, w.x));
+                            fall.x = __fadd_rn(fall.x, __fmul_rn(pw.x, w.y));
+                            fall.y = __fadd_rn(fall.y, __fmul_rn(pw.y, w.y));
+                            rise.x = __fadd_rn(rise.x, __fmul_rn(pw.x, w.x));
+                            rise.y = __fadd_rn(rise.y, __fmul_rn(pw.y, w.x));
                         }
                         if (i > m0)
                         {
-                            *yp = fall;
+                            yp[0] = fall.x;
+                            tmax = fmaxf(tmax, fall.x);
+                            if (second)
+                            {
+                                yp[1] = fall.y;
+                                tmax = fmaxf(tmax, fall.y);
+                            }
                             yp += hs;
-                            tmax = fmaxf(tmax, fall);
                         }
                         fall = rise;
                     }

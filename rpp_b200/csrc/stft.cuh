@@ -50,7 +50,8 @@ struct StftShape
     static constexpr int PASSES = (TF + FPP - 1) / FPP;
     static constexpr int BINS = M + 1;
     static constexpr int FFT_SLOT = R1 * (R2 + 1);     // float2 per frame slot (padded rows)
-    static constexpr int OUT_LD = TF + 1;              // leading dimension of the [BINS][TF] tile
+    static constexpr int OUT_LD = TF + 2;              // leading dimension of the [BINS][TF] tile: even, so
+                                                       // frame pairs load as float2; conflict-free unpack stores
     static constexpr size_t fft_bytes = size_t(FPP) * FFT_SLOT * 8;
     static constexpr size_t out_bytes = size_t(BINS) * OUT_LD * 4;
     static constexpr size_t tw_bytes = (size_t(M / 2 + 1) * 8 + 15) & ~size_t(15);   // W_nfft^k, k <= M/2
