@@ -82,6 +82,18 @@ inline void launch_ragged_prefix(Count count, int n, long long* prefix, cudaStre
 
 // ---------------------------------------------------------------- float helpers
 // Monotone map of float to uint32 so that atomicMax on the key is a float max (NaN excluded).
+// Asks L2 to fetch the bytes of [begin, end) (rounded inward to 16-byte boundaries; nothing when
+// that leaves no whole 16-byte block).  A hint: no completion to wait for.
+__device__ __forceinline__ void l2_prefetch(const float* begin, const float* end)
+{
+    const uintptr_t b = (reinterpret_cast<uintptr_t>(begin) + 15) & ~uintptr_t(15);
+    const uintptr_t e = reinterpret_cast<uintptr_t>(end) & ~uintptr_t(15);
+    if (e <= b) return;
+    const uintptr_t n = e - b;
+    const uint32_t bytes = n < (uintptr_t(1) << 20) ? uint32_t(n) : (1u << 20);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ unsigned float_key(float f)
 {
     unsigned u = __float_as_uint(f);

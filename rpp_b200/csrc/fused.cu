@@ -243,25 +243,38 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     const int f = 2 * (threadIdx.x % (TF / 2));   // first of the two frame columns this thread owns in mel tiles
     const int g = threadIdx.x / (TF / 2);
 
-    // Thread 0 claims one item ahead (the claim's latency overlaps the current item) and decodes
-    // the next item for the CTA while finishing the current one.  A CTA's current item always has
-    // a lower index than the one it holds claimed, so the lowest unfinished item is always some
-    // CTA's current one, whose decibel wait (on lower spectrum items only) ends: claiming ahead
-    // keeps the waits deadlock-free.
-    __shared__ Item s_it;
+    // Thread 0 keeps two items decoded ahead in a two-entry ring (the claim's and the decode's
+    // latencies overlap the current item) and asks L2 for each decoded spectrum item's input span
+    // one item before it is staged.  A CTA's current item always has a lower index than the ones
+    // it holds claimed, so the lowest unfinished item is always some CTA's current one, whose
+    // decibel wait (on lower spectrum items only) ends: claiming ahead keeps the waits
+    // deadlock-free.
+    __shared__ Item s_it[2];
     __shared__ int s_ok;
-    long long wNext = 0;
+    const int itemFrames = TF * a.subTiles;
+    auto prefetch_span = [&](const Item& n) {
+        if (n.kind != 0) return;
+        const int last = min(n.f0 + itemFrames, n.F) - 1;
+        const long long s0 = max(0ll, (long long)n.f0 * a.hop - centerOffset);
+        const long long s1 = min((long long)n.L, (long long)last * a.hop - centerOffset + a.W);
+        l2_prefetch(n.x + s0, n.x + s1);
+    };
+    long long wAfter = 0;   // thread 0: the claimed item two after the current one
+    int cur = 0;
     if (threadIdx.x == 0)
     {
         const long long w0 = (long long)atomicAdd(workCounter, 1ull);
-        wNext = (long long)atomicAdd(workCounter, 1ull);
-        s_it = decode_item<TF>(a, cnt, prefix, nslots, total, w0);
+        const long long w1 = (long long)atomicAdd(workCounter, 1ull);
+        wAfter = (long long)atomicAdd(workCounter, 1ull);
+        s_it[0] = decode_item<TF>(a, cnt, prefix, nslots, total, w0);
+        s_it[1] = decode_item<TF>(a, cnt, prefix, nslots, total, w1);
+        prefetch_span(s_it[1]);
     }
     __syncthreads();
     for (;;)
     {
-        // s_it is rewritten only after the barrier that ends this item's work
-        const Item it = s_it;
+        // s_it[cur] is rewritten only after the barrier that ends this item's work
+        const Item it = s_it[cur];
         if (it.kind < 0) break;
         const int b = it.b;
         const uint32_t hs = it.hs;
@@ -384,9 +397,10 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         __syncthreads();
         if (threadIdx.x == 0)
         {
-            const long long w = wNext;
-            if (w < total) wNext = (long long)atomicAdd(workCounter, 1ull);
+            const long long w = wAfter;
+            if (w < total) wAfter = (long long)atomicAdd(workCounter, 1ull);
             const Item nx = decode_item<TF>(a, cnt, prefix, nslots, total, w);
+            prefetch_span(nx);
             if (it.kind == 0)
             {
                 // the barrier orders every thread's mel stores before this thread's device-scope
@@ -397,8 +411,9 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 __threadfence();
                 atomicAdd(done + b, 1);
             }
-            s_it = nx;
+            s_it[cur] = nx;
         }
+        cur ^= 1;
         __syncthreads();
     }
 }
