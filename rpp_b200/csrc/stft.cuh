@@ -186,27 +186,49 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
     const int off = S::window_offset(W);
     const bool pairs = ((off | hop) & 1) == 0;   // (window, sample) pairs are 8-byte aligned
 
-    // power (2) or magnitude (1) of bins k and M - k, as the two halves of the unpack share loads
-    auto unpack = [&](auto magTag, int fl) {
+    // power (2) or magnitude (1) of bins k and M - k, as the two halves of the unpack share loads;
+    // thread j takes k = j + G*i for i < M / (2G) (every k below M/2 once), thread 0 also k = M/2.
+    // Fully unrolled with constant offsets: Z[M] (a copy of Z[0], stored with the natural-order
+    // spectrum) stands in for Z[(M - k) mod M] at k = 0.
+    constexpr int LD = S::OUT_LD;
+    auto bin_pair = [&](auto magTag, float2 A, float2 B, float2 t, float& p0, float& p1) {
         constexpr bool kMag = decltype(magTag)::value;
-        for (int k = j; k <= M / 2; k += G)
+        // E = (A + conj(B)) / 2,  O = (A - conj(B)) / (2i),  P = W^k O
+        const float2 sum = fft::mul2(make_float2(0.5f, 0.5f), fft::add2(A, B));   // (er, orr)
+        const float2 dif = fft::mul2(make_float2(-0.5f, 0.5f), fft::sub2(A, B));  // (oi, ei)
+        const float er = sum.x, orr = sum.y, oi = dif.x, ei = dif.y;
+        const float pr = fmaf(orr, t.x, oi * t.y);
+        const float pi = fmaf(oi, t.x, -orr * t.y);
+        const float2 X = fft::add2(make_float2(er, ei), make_float2(pr, pi));   // X[k] = E + P
+        const float2 Y = fft::sub2(make_float2(er, ei), make_float2(pr, pi));   // X[M-k] = conj(E - P)
+        const float2 sq = fft::mul2(make_float2(X.y, Y.y), make_float2(X.y, Y.y));
+        p0 = fmaf(X.x, X.x, sq.x);
+        p1 = fmaf(Y.x, Y.x, sq.y);
+        if (kMag)
         {
-            const float2 A = buf[k];
-            const float2 B = buf[(M - k) & (M - 1)];
-            // E = (A + conj(B)) / 2,  O = (A - conj(B)) / (2i),  P = W^k O
-            const float2 sum = fft::mul2(make_float2(0.5f, 0.5f), fft::add2(A, B));   // (er, orr)
-            const float2 dif = fft::mul2(make_float2(-0.5f, 0.5f), fft::sub2(A, B));  // (oi, ei)
-            const float er = sum.x, orr = sum.y, oi = dif.x, ei = dif.y;
-            const float2 t = s_tw[k];
-            const float pr = fmaf(orr, t.x, oi * t.y);
-            const float pi = fmaf(oi, t.x, -orr * t.y);
-            const float2 X = fft::add2(make_float2(er, ei), make_float2(pr, pi));   // X[k] = E + P
-            const float2 Y = fft::sub2(make_float2(er, ei), make_float2(pr, pi));   // X[M-k] = conj(E - P)
-            const float2 sq = fft::mul2(make_float2(X.y, Y.y), make_float2(X.y, Y.y));
-            const float p0 = fmaf(X.x, X.x, sq.x);
-            const float p1 = fmaf(Y.x, Y.x, sq.y);
-            s_out[k * S::OUT_LD + fl] = kMag ? sqrtf(p0) : p0;
-            if (k != M - k) s_out[(M - k) * S::OUT_LD + fl] = kMag ? sqrtf(p1) : p1;
+            p0 = sqrtf(p0);
+            p1 = sqrtf(p1);
+        }
+    };
+    auto unpack = [&](auto magTag, int fl) {
+        const float2* pa = buf + j;
+        const float2* pb = buf + (M - j);
+        const float2* pt = s_tw + j;
+        float* o1 = s_out + j * LD + fl;
+        float* o2 = s_out + (M - j) * LD + fl;
+#pragma unroll
+        for (int i = 0; i < M / (2 * G); ++i)
+        {
+            float p0, p1;
+            bin_pair(magTag, pa[G * i], pb[-G * i], pt[G * i], p0, p1);
+            o1[G * i * LD] = p0;
+            o2[-G * i * LD] = p1;
+        }
+        if (j == 0)
+        {
+            float p0, p1;
+            bin_pair(magTag, buf[M / 2], buf[M / 2], s_tw[M / 2], p0, p1);
+            s_out[(M / 2) * LD + fl] = p0;
         }
     };
 
@@ -242,8 +264,9 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
             for (int m = 0; m < R1; ++m) z[m] = make_float2(0.f, 0.f);
         }
         fft::Dft<R1>::run(z);
+        buf[j] = z[0];   // W_M^(j*0) = 1
 #pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1)
+        for (int k1 = 1; k1 < R1; ++k1)
         {
             const float2 t = s_tw1[k1 * R2 + j];
             buf[k1 * (R2 + 1) + j] = fft::cmul_conj(z[k1], t.x, t.y);
@@ -266,6 +289,7 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
             fft::Dft<R2>::run(y[r]);
 #pragma unroll
             for (int k2 = 0; k2 < R2; ++k2) buf[k1 + R1 * k2] = y[r][k2];   // Z in natural order
+            if (k1 == 0) buf[M] = y[r][0];                                    // Z[M] = Z[0]
         }
         __syncwarp();
         if (fl < TF)
