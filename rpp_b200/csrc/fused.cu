@@ -395,23 +395,25 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
             }
         }
         __syncthreads();
+        // between the two barriers, in parallel: warp 0 claims and decodes the item after next;
+        // warp 1 publishes a finished spectrum item
         if (threadIdx.x == 0)
         {
             const long long w = wAfter;
             if (w < total) wAfter = (long long)atomicAdd(workCounter, 1ull);
             const Item nx = decode_item<TF>(a, cnt, prefix, nslots, total, w);
             prefetch_span(nx);
-            if (it.kind == 0)
-            {
-                // the barrier orders every thread's mel stores before this thread's device-scope
-                // fence, which orders them before the count (the grid-barrier release pattern)
-                float v = s_warpMax[0];
-                for (int i = 1; i < kFusedThreads / 32; ++i) v = fmaxf(v, s_warpMax[i]);
-                atomicMax(maxKey + b, float_key(v));
-                __threadfence();
-                atomicAdd(done + b, 1);
-            }
             s_it[cur] = nx;
+        }
+        else if (threadIdx.x == 32 && it.kind == 0)
+        {
+            // the barrier orders every thread's mel stores before this thread's device-scope
+            // fence, which orders them before the count (the grid-barrier release pattern)
+            float v = s_warpMax[0];
+            for (int i = 1; i < kFusedThreads / 32; ++i) v = fmaxf(v, s_warpMax[i]);
+            atomicMax(maxKey + b, float_key(v));
+            __threadfence();
+            atomicAdd(done + b, 1);
         }
         cur ^= 1;
         __syncthreads();
