@@ -215,21 +215,48 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 melW[k] = make_float2(rise, fall);
             }
         }
-        if (threadIdx.x == 0)
+        // group g emits filters [melGrp[g], melGrp[g + 1]) and sweeps their intervals; the groups'
+        // shares of (bins + 2) per interval are balanced.  cum[i] = cost of intervals 0..i (an
+        // inclusive scan by warp 0, in the power tile's space, which is free until the first FFT);
+        // boundary g is 1 + the first filter m whose intervals 0..m+1 reach g / kGroups of the total.
+        int* cum = reinterpret_cast<int*>(s_out);
+        for (int i = threadIdx.x; i <= nmel; i += kFusedThreads)
+            cum[i] = (v.last[i] > v.first[i] ? v.last[i] - v.first[i] : 0) + 2;
+        __syncthreads();
+        if (threadIdx.x < 32)
         {
-            // group g emits filters [melGrp[g], melGrp[g + 1]) and sweeps their intervals; the
-            // groups' shares of (bins + 2) per interval are balanced
-            auto cost = [&](int i) { return (v.last[i] > v.first[i] ? v.last[i] - v.first[i] : 0) + 2; };
-            int totalCost = 0;
-            for (int i = 0; i <= nmel; ++i) totalCost += cost(i);
-            int acc = cost(0), grp = 1;
-            melGrp[0] = 0;
-            for (int m = 0; m < nmel && grp < kGroups; ++m)
+            const int lane = threadIdx.x, chunk = (nmel + 1 + 31) / 32;
+            const int i0 = min(lane * chunk, nmel + 1), i1 = min(i0 + chunk, nmel + 1);
+            int sum = 0;
+            for (int i = i0; i < i1; ++i) sum += cum[i];
+            int incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
             {
-                acc += cost(m + 1);
-                while (grp < kGroups && acc * kGroups >= grp * totalCost) melGrp[grp++] = m + 1;
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
             }
-            while (grp <= kGroups) melGrp[grp++] = nmel;
+            int run = incl - sum;
+            for (int i = i0; i < i1; ++i)
+            {
+                run += cum[i];
+                cum[i] = run;
+            }
+        }
+        __syncthreads();
+        const int totalCost = cum[nmel];
+        for (int grp = threadIdx.x; grp <= kGroups; grp += kFusedThreads)
+        {
+            int lo = 0, hi = nmel;   // first m in [0, nmel) with cum[m + 1] * kGroups >= grp * total, else nmel
+            if (grp == 0) hi = -1;
+            else
+                while (lo < hi)
+                {
+                    const int mid = (lo + hi) >> 1;
+                    if (cum[mid + 1] * kGroups >= grp * totalCost) hi = mid;
+                    else lo = mid + 1;
+                }
+            melGrp[grp] = grp == 0 ? 0 : grp == kGroups ? nmel : min(lo + 1, nmel);
         }
         __syncthreads();
     }
