@@ -4,10 +4,12 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <utility>
 
 namespace rppb {
 
 void count_launch(int kernels);
+void check_cuda(cudaError_t err, const char* what);
 
 // ---------------------------------------------------------------- ragged batches
 // A batch of uneven samples is addressed as one flat list of work units (chunks, frame tiles,
@@ -45,10 +47,16 @@ __device__ __forceinline__ const long long* cache_prefix(const long long* prefix
     return s_cache;
 }
 
-// One CTA of 1024 threads: prefix[0..n] = exclusive scan of count(b).
+// One CTA of 1024 threads: prefix[0..n] = exclusive scan of count(b), and zero[0..zeroWords) = 0
+// (the work counters of the kernel that follows).  It lets a kernel launched after it with
+// programmatic stream serialization (launch_dependent) start at once; that kernel runs its
+// independent setup, then grid_dependency_wait() before it reads what this kernel writes.
 template <class Count>
-__global__ void __launch_bounds__(1024) ragged_prefix_kernel(Count count, int n, long long* __restrict__ prefix)
+__global__ void __launch_bounds__(1024) ragged_prefix_kernel(Count count, int n, long long* __restrict__ prefix,
+                                                             unsigned* __restrict__ zero, int zeroWords)
 {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    for (int i = threadIdx.x; i < zeroWords; i += 1024) zero[i] = 0u;
     __shared__ long long part[1024];
     const int t = threadIdx.x;
     const int per = (n + 1023) / 1024;
@@ -74,10 +82,36 @@ __global__ void __launch_bounds__(1024) ragged_prefix_kernel(Count count, int n,
 }
 
 template <class Count>
-inline void launch_ragged_prefix(Count count, int n, long long* prefix, cudaStream_t s)
+inline void launch_ragged_prefix(Count count, int n, long long* prefix, cudaStream_t s, unsigned* zero = nullptr,
+                                 int zeroWords = 0)
 {
-    ragged_prefix_kernel<Count><<<1, 1024, 0, s>>>(count, n, prefix);
+    ragged_prefix_kernel<Count><<<1, 1024, 0, s>>>(count, n, prefix, zero, zeroWords);
     count_launch(1);
+}
+
+// In a kernel launched by launch_dependent: waits until the kernel before it in the stream has
+// completed and its writes are visible (a no-op for a kernel launched the ordinary way).
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Launches `kernel` with programmatic stream serialization: it may start while the kernel before
+// it (which must allow it, as ragged_prefix_kernel does) is still running, so its setup overlaps
+// that kernel and the launch gap; it must call grid_dependency_wait() before touching that
+// kernel's results.  Kernels earlier in the stream have completed by then.
+template <class... KArgs, class... Args>
+inline void launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                             const char* what, Args&&... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    check_cuda(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...), what);
 }
 
 // ---------------------------------------------------------------- float helpers

@@ -264,6 +264,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     const int centerOffset = a.center ? a.W / 2 : 0;
     const int nslots = a.n + a.lookahead;
     __shared__ long long s_prefix[kFusedPrefixCache];
+    grid_dependency_wait();   // the prefix and the zeroed counters of the prefix kernel
     prefix = cache_prefix<kFusedPrefixCache>(prefix, nslots, s_prefix);
     const long long total = prefix[nslots];
     const SlotCount<TF> cnt{a, a.n, a.lookahead};
@@ -457,9 +458,10 @@ void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
     unsigned long long* counter = cv.take<unsigned long long>(1);
     int* done = cv.take<int>(a.n);
     unsigned* maxKey = cv.take<unsigned>(a.n);
+    // the prefix kernel also zeroes the queue counter, the tile counts and the maxima
     const size_t clear = reinterpret_cast<char*>(maxKey + a.n) - reinterpret_cast<char*>(counter);
-    check_cuda(cudaMemsetAsync(counter, 0, clear, h.stream()), "memset(frontend state)");
-    launch_ragged_prefix(SlotCount<S::TF>{a, a.n, a.lookahead}, nslots, prefix, h.stream());
+    launch_ragged_prefix(SlotCount<S::TF>{a, a.n, a.lookahead}, nslots, prefix, h.stream(),
+                         reinterpret_cast<unsigned*>(counter), int(clear / 4));
     const FusedLayout<NFFT, TFX> lay(a.mel.numFilter, a.W, a.hop);
     if (lay.total > 227 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
     const float2* tw = spectrogram_twiddles(h, NFFT);
@@ -467,10 +469,11 @@ void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
     if (a.ctasPerSm > 0) grid = std::min(grid, a.ctasPerSm * h.num_sms());
     if (a.reserveSms > 0 && a.reserveSms < h.num_sms())
         grid = std::max(1, grid / h.num_sms() * (h.num_sms() - a.reserveSms));
-    frontend_kernel<NFFT, TFX><<<grid, kFusedThreads, lay.total, h.stream()>>>(a, tw, prefix, counter, done, maxKey,
-                                                                          h.device_flags());
+    // starts while the prefix kernel runs: the tables are built before grid_dependency_wait()
+    launch_dependent(frontend_kernel<NFFT, TFX>, dim3(grid), dim3(kFusedThreads), lay.total, h.stream(),
+                     "frontend_kernel", a, tw, static_cast<const long long*>(prefix), counter, done, maxKey,
+                     h.device_flags());
     count_launch();
-    check_cuda(cudaGetLastError(), "frontend_kernel");
 }
 
 }  // namespace
