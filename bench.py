@@ -666,7 +666,7 @@ def run_b200(args, world, rank, local):
             p_ = fused.params
             tune = {"tuned": True, "tile_frames": p_.tileFrames, "db_frames": p_.dbFrames,
                     "lookahead": p_.lookahead, "ctas_per_sm": p_.ctasPerSm, "tuner_best_ms": tune_ms,
-                    "by": "rppb_frontend_tune_gpu (36 schedule candidates timed on this batch)"}
+                    "by": "rppb_frontend_tune_gpu (54 schedule candidates timed on this batch)"}
 
     def timed(fn, steps, per_op=False):
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(steps)] if per_op else None
