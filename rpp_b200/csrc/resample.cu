@@ -12,9 +12,11 @@
 // summed per channel in order.  Every product and sum is explicitly rounded, so outputs are
 // bit-identical to the host path.
 //
-// One CTA per 256-output block: thread 0 replays the phase sum into shared memory; when down-mixing,
-// the CTA then stages the block's input span (down-mixed once per input sample) in shared memory;
-// every thread computes one output.  Compute-bound: 2 * lobes taps of ~10 float
+// One CTA of 8 + 1 warps walks the 256-output blocks: the ninth warp replays the next block's phase
+// sum into shared memory (double-buffered) while the eight compute this block, one output per
+// thread; when down-mixing, the block's input span is staged (down-mixed once per input sample) in
+// shared memory first.  The lookup table sits in shared memory as (value, next - value) pairs when
+// they fit, so a tap reads one 8-byte entry.  Compute-bound: 2 * lobes taps of ~10 float
 // operations per output.
 #include "common.cuh"
 #include "downmix.cuh"
@@ -27,7 +29,15 @@ constexpr int kBlock = 256;        // outputs per block (the reference's block s
 constexpr int kCopyChunk = 4096;   // floats per unit of an equal-rate copy
 constexpr int kSpan = 4096;        // input samples of one block staged in shared memory (mono paths)
 
-__host__ __device__ __forceinline__ size_t resample_smem_floats(int lutSize) { return ((lutSize + 3) & ~3) + kSpan; }
+constexpr int kThreads = kBlock + 32;   // 8 warps compute outputs, the ninth replays the next unit's phases
+
+// Shared memory (floats): the table -- as (value, next - value) pairs when kPairs, else plain --
+// then the staged input span.
+__host__ __device__ __forceinline__ size_t resample_smem_floats(int lutSize, bool pairs)
+{
+    return (pairs ? 2 * size_t(lutSize) : ((size_t(lutSize) + 3) & ~size_t(3))) + kSpan;
+}
+constexpr size_t kPairTableLimit = 200 * 1024;   // bytes of shared memory for the pair layout
 
 __device__ __forceinline__ int out_length(int L, float inRate, float outRate)
 {
@@ -61,176 +71,235 @@ struct ResampleCount
     }
 };
 
+template <bool kPairs>
 struct Win
 {
-    const float* lut;   // shared memory
+    const float* lut;   // shared memory: floats, or (value, next - value) pairs when kPairs
     int lutSize;
     float scale, center;
 
+    __device__ __forceinline__ float interp(int idx, float weight) const
+    {
+        idx = min(max(idx, 0), lutSize - 2);
+        if constexpr (kPairs)
+        {
+            const float2 e = reinterpret_cast<const float2*>(lut)[idx];
+            return __fadd_rn(e.x, __fmul_rn(weight, e.y));
+        }
+        else
+        {
+            const float cur = lut[idx], nxt = lut[idx + 1];
+            return __fadd_rn(cur, __fmul_rn(weight, __fsub_rn(nxt, cur)));
+        }
+    }
     // rppdefs.h:771-782: truncating index (the SSE lanes)
     __device__ __forceinline__ float lane(float x) const
     {
         const float locRaw = __fadd_rn(__fmul_rn(x, scale), center);
-        int idx = int(locRaw);
-        const float weight = __fsub_rn(locRaw, float(idx));
-        idx = min(max(idx, 0), lutSize - 2);
-        const float cur = lut[idx], nxt = lut[idx + 1];
-        return __fadd_rn(cur, __fmul_rn(weight, __fsub_rn(nxt, cur)));
+        const int idx = int(locRaw);
+        return interp(idx, __fsub_rn(locRaw, float(idx)));
     }
     // rppdefs.h:760-769: floor, clamped index (the scalar tail and the multi-channel path)
     __device__ __forceinline__ float scalar(float x) const
     {
         const float locRaw = __fadd_rn(__fmul_rn(x, scale), center);
-        int idx = int(floorf(locRaw));
-        const float weight = __fsub_rn(locRaw, float(idx));
-        idx = min(max(idx, 0), lutSize - 2);
-        const float cur = lut[idx], nxt = lut[idx + 1];
-        return __fadd_rn(cur, __fmul_rn(weight, __fsub_rn(nxt, cur)));
+        const int idx = int(floorf(locRaw));
+        return interp(idx, __fsub_rn(locRaw, float(idx)));
     }
+};
+
+// Where unit w of the flat work list lives and, for a resampling unit, its phases.
+struct UnitInfo
+{
+    int b, unit, L, Csrc, C;
+    float inRate, outRate;
+    const float* x;
+    float* y;
+    uint32_t dstStride;
 };
 
 // kMix: the input is interleaved multi-channel and is down-mixed to mono on the fly (MonoMix), so
 // the launch equals rppt_down_mixing_gpu followed by a mono rppt_resample_gpu.
-template <bool kMix, bool kTable>
-__global__ void __launch_bounds__(kBlock) resample_kernel(const float* __restrict__ src, uint32_t srcStride,
-                                                          float* __restrict__ dst, uint32_t dstStride,
-                                                          const float* __restrict__ inRateT,
-                                                          const float* __restrict__ outRateT,
-                                                          const int* __restrict__ dims, ResampleWindowDev wd,
-                                                          bool normalize, const long long* __restrict__ prefix, int n,
-                                                          const RppbClip* __restrict__ clips, float outRateAll)
+template <bool kMix, bool kTable, bool kPairs>
+__global__ void __launch_bounds__(kThreads) resample_kernel(const float* __restrict__ src, uint32_t srcStride,
+                                                            float* __restrict__ dst, uint32_t dstStride,
+                                                            const float* __restrict__ inRateT,
+                                                            const float* __restrict__ outRateT,
+                                                            const int* __restrict__ dims, ResampleWindowDev wd,
+                                                            bool normalize, const long long* __restrict__ prefix,
+                                                            int n, const RppbClip* __restrict__ clips,
+                                                            float outRateAll)
 {
     extern __shared__ float s_lut[];   // the table, then the staged input span
-    float* s_in = s_lut + ((wd.lutSize + 3) & ~3);
-    __shared__ float s_phase[kBlock];
-    for (int i = threadIdx.x; i < wd.lutSize; i += blockDim.x) s_lut[i] = wd.lut[i];
-    __syncthreads();
-    const Win win{s_lut, wd.lutSize, wd.scale, wd.center};
+    float* s_in = s_lut + (kPairs ? 2 * wd.lutSize : ((wd.lutSize + 3) & ~3));
+    __shared__ float s_phase[2][kBlock];
+    if (kPairs)
+        for (int i = threadIdx.x; i < wd.lutSize - 1; i += kThreads)
+            reinterpret_cast<float2*>(s_lut)[i] = make_float2(wd.lut[i], __fsub_rn(wd.lut[i + 1], wd.lut[i]));
+    else
+        for (int i = threadIdx.x; i < wd.lutSize; i += kThreads) s_lut[i] = wd.lut[i];
+    const Win<kPairs> win{s_lut, wd.lutSize, wd.scale, wd.center};
     const int lobes = wd.lobes;
     __shared__ long long s_prefix[kPrefixCache];
-    prefix = cache_prefix(prefix, n, s_prefix);
+    prefix = cache_prefix(prefix, n, s_prefix);   // ends with __syncthreads
     const long long total = prefix[n];
-    for (long long w = blockIdx.x; w < total; w += gridDim.x)
-    {
-        const int b = ragged_find(prefix, n, w);
-        const int unit = int(w - prefix[b]);
-        const int L = kTable ? clips[b].length : dims[2 * b];
-        const int Csrc = kTable ? 1 : dims[2 * b + 1];
-        const int C = kMix ? 1 : Csrc;   // channels of the resampled signal
-        const float inRate = kTable ? clips[b].inRate : inRateT[b];
-        const float outRate = kTable ? outRateAll : outRateT[b];
-        const float* x = kTable ? clips[b].src : src + size_t(b) * srcStride;
-        float* y = kTable ? clips[b].work : dst + size_t(b) * dstStride;
-        if (kTable) dstStride = 0x7fffffffu;   // work holds the whole resampled clip
-        const MonoMix mix{x, kMix ? Csrc : 1, kMix ? MonoMix::weight(max(Csrc, 1), normalize) : 1.f};
-        if (kMix && Csrc > 64) continue;
-        if (inRate == outRate)
-        {
-            if (kMix)
-            {
-                const long long count = min((long long)L, (long long)dstStride);
-                for (long long i = (long long)unit * kCopyChunk + threadIdx.x;
-                     i < min(count, (long long)(unit + 1) * kCopyChunk); i += blockDim.x)
-                    y[i] = mix(i);
-                continue;
-            }
-            const long long count = kTable ? (long long)L : min((long long)L * C, (long long)min(srcStride, dstStride));
-            for (long long i = (long long)unit * kCopyChunk + threadIdx.x; i < min(count, (long long)(unit + 1) * kCopyChunk);
-                 i += blockDim.x)
-                y[i] = x[i];
-            continue;
-        }
-        const int outEnd = min(out_length(L, inRate, outRate), int(dstStride / uint32_t(C)));   // stay inside dst
-        const double scale = __ddiv_rn(double(inRate), double(outRate));
+
+    auto info = [&](long long w) {
+        UnitInfo u;
+        u.b = ragged_find(prefix, n, w);
+        u.unit = int(w - prefix[u.b]);
+        u.L = kTable ? clips[u.b].length : dims[2 * u.b];
+        u.Csrc = kTable ? 1 : dims[2 * u.b + 1];
+        u.C = kMix ? 1 : u.Csrc;   // channels of the resampled signal
+        u.inRate = kTable ? clips[u.b].inRate : inRateT[u.b];
+        u.outRate = kTable ? outRateAll : outRateT[u.b];
+        u.x = kTable ? clips[u.b].src : src + size_t(u.b) * srcStride;
+        u.y = kTable ? clips[u.b].work : dst + size_t(u.b) * dstStride;
+        u.dstStride = kTable ? 0x7fffffffu : dstStride;   // a clip's work buffer holds the whole resampled clip
+        return u;
+    };
+    // the reference's phase sum of a resampling unit (one thread; replayed in its float order)
+    auto phases = [&](long long w, float* out) {
+        if (w >= total) return;
+        const UnitInfo u = info(w);
+        if (u.inRate == u.outRate || (kMix && u.Csrc > 64)) return;
+        const double scale = __ddiv_rn(double(u.inRate), double(u.outRate));
         const float fscale = __double2float_rn(scale);
-        const int outBlock = unit * kBlock;
-        const double inBlockRaw = __dmul_rn(double(outBlock), scale);
-        const int inBlockRounded = int(inBlockRaw);
-        if (threadIdx.x == 0)
+        const double inBlockRaw = __dmul_rn(double(u.unit * kBlock), scale);
+        float p = __double2float_rn(__dsub_rn(inBlockRaw, double(int(inBlockRaw))));
+        for (int k = 0; k < kBlock; ++k)
         {
-            float p = __double2float_rn(__dsub_rn(inBlockRaw, double(inBlockRounded)));
-            for (int k = 0; k < kBlock; ++k)
-            {
-                s_phase[k] = p;
-                p = __fadd_rn(p, fscale);
-            }
+            out[k] = p;
+            p = __fadd_rn(p, fscale);
         }
-        __syncthreads();
-        const float* in = x + (long long)inBlockRounded * C;
-        // down-mixing path: the block's input span [lo, hi), down-mixed once per sample, goes to
-        // shared memory (every tap of the block lies inside it because the phases increase); plain
-        // mono input is read through L1 directly, which measured faster than staging it
-        int lo = 0;
-        bool staged = false;
-        if (kMix)
+    };
+
+    if (threadIdx.x == kBlock) phases(blockIdx.x, s_phase[0]);
+    __syncthreads();
+    int cur = 0;
+    for (long long w = blockIdx.x; w < total; w += gridDim.x, cur ^= 1)
+    {
+        if (threadIdx.x >= kBlock)
         {
-            const int cnt = min(kBlock, outEnd - outBlock);
-            if (cnt > 0)
-            {
-                lo = max(int(ceilf(s_phase[0])) - lobes, -inBlockRounded);
-                const int hi = min(int(ceilf(s_phase[cnt - 1])) + lobes, L - inBlockRounded);
-                staged = hi - lo <= kSpan;
-                if (staged)
-                    for (int i = threadIdx.x; i < hi - lo; i += kBlock)
-                        s_in[i] = kMix ? mix((long long)inBlockRounded + lo + i) : __ldg(in + lo + i);
-            }
-            __syncthreads();
+            // the ninth warp: the next unit's phases while the others compute this one
+            if (threadIdx.x == kBlock) phases(w + gridDim.x, s_phase[cur ^ 1]);
         }
-        const int outPos = outBlock + threadIdx.x;
-        if (outPos < outEnd)
+        else
         {
-            const float inPos = s_phase[threadIdx.x];
-            const int xc = int(ceilf(inPos));
-            int loc0 = xc - lobes, loc1 = xc + lobes;
-            if (loc0 + inBlockRounded < 0) loc0 = -inBlockRounded;
-            if (loc1 + inBlockRounded > L) loc1 = L - inBlockRounded;
-            if (kMix || C == 1)
+            const UnitInfo u = info(w);
+            const float* x = u.x;
+            float* y = u.y;
+            const int L = u.L, Csrc = u.Csrc, C = u.C;
+            const MonoMix mix{x, kMix ? Csrc : 1, kMix ? MonoMix::weight(max(Csrc, 1), normalize) : 1.f};
+            if (kMix && Csrc > 64)
             {
-                // mono input: sample l of the block, down-mixed when kMix
-                auto at = [&](int l) -> float {
-                    if (staged) return s_in[l - lo];
-                    return kMix ? mix((long long)inBlockRounded + l) : __ldg(in + l);
-                };
-                int l = loc0;
-                const float locBegin = __fsub_rn(float(l), inPos);
-                float lane[4] = {__fadd_rn(locBegin, 0.f), __fadd_rn(locBegin, 1.f), __fadd_rn(locBegin, 2.f),
-                                 __fadd_rn(locBegin, 3.f)};
-                float acc4[4] = {0.f, 0.f, 0.f, 0.f};
-                for (; l + 3 < loc1; l += 4)
+                // not handled here (rejected by the caller)
+            }
+            else if (u.inRate == u.outRate)
+            {
+                if (kMix)
                 {
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                    {
-                        acc4[j] = __fadd_rn(acc4[j], __fmul_rn(at(l + j), win.lane(lane[j])));
-                        lane[j] = __fadd_rn(lane[j], 4.f);
-                    }
+                    const long long count = min((long long)L, (long long)u.dstStride);
+                    for (long long i = (long long)u.unit * kCopyChunk + threadIdx.x;
+                         i < min(count, (long long)(u.unit + 1) * kCopyChunk); i += kBlock)
+                        y[i] = mix(i);
                 }
-                float accum = __fadd_rn(__fadd_rn(acc4[0], acc4[2]), __fadd_rn(acc4[1], acc4[3]));
-                float xx = __fsub_rn(float(l), inPos);
-                for (; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
-                    accum = __fadd_rn(accum, __fmul_rn(at(l), win.scalar(xx)));
-                y[outPos] = accum;
+                else
+                {
+                    const long long count =
+                        kTable ? (long long)L : min((long long)L * C, (long long)min(srcStride, u.dstStride));
+                    for (long long i = (long long)u.unit * kCopyChunk + threadIdx.x;
+                         i < min(count, (long long)(u.unit + 1) * kCopyChunk); i += kBlock)
+                        y[i] = x[i];
+                }
             }
             else
             {
-                constexpr int kMaxC = 16;
-                float acc[kMaxC];
-#pragma unroll
-                for (int c = 0; c < kMaxC; ++c) acc[c] = 0.f;
-                float xx = __fsub_rn(float(loc0), inPos);
-                for (int l = loc0; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
+                const float* ph = s_phase[cur];
+                const int outEnd = min(out_length(L, u.inRate, u.outRate), int(u.dstStride / uint32_t(C)));
+                const double scale = __ddiv_rn(double(u.inRate), double(u.outRate));
+                const int outBlock = u.unit * kBlock;
+                const int inBlockRounded = int(__dmul_rn(double(outBlock), scale));
+                const float* in = x + (long long)inBlockRounded * C;
+                // down-mixing path: the unit's input span [lo, hi), down-mixed once per sample, goes to
+                // shared memory (every tap of the unit lies inside it because the phases increase);
+                // plain mono input is read through L1 directly, which measured faster than staging it
+                int lo = 0;
+                bool staged = false;
+                if (kMix)
                 {
-                    const float wv = win.scalar(xx);
-#pragma unroll
-                    for (int c = 0; c < kMaxC; ++c)
-                        if (c < C) acc[c] = __fadd_rn(acc[c], __fmul_rn(__ldg(in + (long long)l * C + c), wv));
+                    const int cnt = min(kBlock, outEnd - outBlock);
+                    if (cnt > 0)
+                    {
+                        lo = max(int(ceilf(ph[0])) - lobes, -inBlockRounded);
+                        const int hi = min(int(ceilf(ph[cnt - 1])) + lobes, L - inBlockRounded);
+                        staged = hi - lo <= kSpan;
+                        if (staged)
+                            for (int i = threadIdx.x; i < hi - lo; i += kBlock)
+                                s_in[i] = mix((long long)inBlockRounded + lo + i);
+                    }
+                    asm volatile("bar.sync 1, %0;" ::"n"(kBlock) : "memory");   // the compute warps only
                 }
+                const int outPos = outBlock + threadIdx.x;
+                if (outPos < outEnd)
+                {
+                    const float inPos = ph[threadIdx.x];
+                    const int xc = int(ceilf(inPos));
+                    int loc0 = xc - lobes, loc1 = xc + lobes;
+                    if (loc0 + inBlockRounded < 0) loc0 = -inBlockRounded;
+                    if (loc1 + inBlockRounded > L) loc1 = L - inBlockRounded;
+                    if (kMix || C == 1)
+                    {
+                        // mono input: 4 lanes, folded as (l0 + l2) + (l1 + l3), then a scalar tail
+                        auto taps = [&](auto at) {
+                            int l = loc0;
+                            const float locBegin = __fsub_rn(float(l), inPos);
+                            float lane[4] = {__fadd_rn(locBegin, 0.f), __fadd_rn(locBegin, 1.f),
+                                             __fadd_rn(locBegin, 2.f), __fadd_rn(locBegin, 3.f)};
+                            float acc4[4] = {0.f, 0.f, 0.f, 0.f};
+                            for (; l + 3 < loc1; l += 4)
+                            {
 #pragma unroll
-                for (int c = 0; c < kMaxC; ++c)
-                    if (c < C) y[(long long)outPos * C + c] = acc[c];
+                                for (int j = 0; j < 4; ++j)
+                                {
+                                    acc4[j] = __fadd_rn(acc4[j], __fmul_rn(at(l + j), win.lane(lane[j])));
+                                    lane[j] = __fadd_rn(lane[j], 4.f);
+                                }
+                            }
+                            float accum = __fadd_rn(__fadd_rn(acc4[0], acc4[2]), __fadd_rn(acc4[1], acc4[3]));
+                            float xx = __fsub_rn(float(l), inPos);
+                            for (; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
+                                accum = __fadd_rn(accum, __fmul_rn(at(l), win.scalar(xx)));
+                            return accum;
+                        };
+                        float r;
+                        if (kMix && staged) r = taps([&](int l) { return s_in[l - lo]; });
+                        else if (kMix) r = taps([&](int l) { return mix((long long)inBlockRounded + l); });
+                        else r = taps([&](int l) { return __ldg(in + l); });
+                        y[outPos] = r;
+                    }
+                    else
+                    {
+                        constexpr int kMaxC = 16;
+                        float acc[kMaxC];
+#pragma unroll
+                        for (int c = 0; c < kMaxC; ++c) acc[c] = 0.f;
+                        float xx = __fsub_rn(float(loc0), inPos);
+                        for (int l = loc0; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
+                        {
+                            const float wv = win.scalar(xx);
+#pragma unroll
+                            for (int c = 0; c < kMaxC; ++c)
+                                if (c < C) acc[c] = __fadd_rn(acc[c], __fmul_rn(__ldg(in + (long long)l * C + c), wv));
+                        }
+#pragma unroll
+                        for (int c = 0; c < kMaxC; ++c)
+                            if (c < C) y[(long long)outPos * C + c] = acc[c];
+                    }
+                }
             }
         }
-        __syncthreads();   // s_phase is rewritten by the next unit
+        __syncthreads();   // s_phase[cur] is rewritten two units on; s_phase[cur ^ 1] is ready
     }
 }
 
@@ -243,21 +312,17 @@ void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStr
     if (n <= 0) return;
     long long* prefix = static_cast<long long*>(scratch);
     launch_ragged_prefix(ResampleCount{inRate, outRate, dims, downmix, nullptr, 0.f}, n, prefix, h.stream());
-    const size_t smem = resample_smem_floats(win.lutSize) * sizeof(float);
-    if (downmix)
-    {
-        int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel<true, false>), kBlock, smem);
-        resample_kernel<true, false><<<grid, kBlock, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate,
-                                                                         outRate, dims, win, normalize, prefix, n,
-                                                                         nullptr, 0.f);
-    }
-    else
-    {
-        int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel<false, false>), kBlock, smem);
-        resample_kernel<false, false><<<grid, kBlock, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate,
-                                                                          outRate, dims, win, normalize, prefix, n,
-                                                                          nullptr, 0.f);
-    }
+    const bool pairs = resample_smem_floats(win.lutSize, true) * sizeof(float) <= kPairTableLimit;
+    const size_t smem = resample_smem_floats(win.lutSize, pairs) * sizeof(float);
+    auto go = [&](auto kernel) {
+        const int grid = persistent_grid(h, reinterpret_cast<const void*>(kernel), kThreads, smem);
+        kernel<<<grid, kThreads, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate, outRate, dims, win,
+                                                     normalize, prefix, n, nullptr, 0.f);
+    };
+    if (downmix && pairs) go(resample_kernel<true, false, true>);
+    else if (downmix) go(resample_kernel<true, false, false>);
+    else if (pairs) go(resample_kernel<false, false, true>);
+    else go(resample_kernel<false, false, false>);
     count_launch();
     check_cuda(cudaGetLastError(), "resample_kernel");
 }
@@ -268,10 +333,15 @@ void launch_resample_clips(Handle& h, void* scratch, const RppbClip* clips, int 
     if (n <= 0) return;
     long long* prefix = static_cast<long long*>(scratch);
     launch_ragged_prefix(ResampleCount{nullptr, nullptr, nullptr, false, clips, outRate}, n, prefix, h.stream());
-    const size_t smem = resample_smem_floats(win.lutSize) * sizeof(float);
-    int grid = persistent_grid(h, reinterpret_cast<const void*>(resample_kernel<false, true>), kBlock, smem);
-    resample_kernel<false, true><<<grid, kBlock, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr,
-                                                                     win, false, prefix, n, clips, outRate);
+    const bool pairs = resample_smem_floats(win.lutSize, true) * sizeof(float) <= kPairTableLimit;
+    const size_t smem = resample_smem_floats(win.lutSize, pairs) * sizeof(float);
+    auto go = [&](auto kernel) {
+        const int grid = persistent_grid(h, reinterpret_cast<const void*>(kernel), kThreads, smem);
+        kernel<<<grid, kThreads, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, win, false,
+                                                     prefix, n, clips, outRate);
+    };
+    if (pairs) go(resample_kernel<false, true, true>);
+    else go(resample_kernel<false, true, false>);
     count_launch();
     check_cuda(cudaGetLastError(), "resample_kernel(clips)");
 }
