@@ -16,9 +16,10 @@
 // (about 1e-7 relative apart).
 //
 // Kernels: stats_kernel (only when something is computed) -- one thread per parameter for short
-// reductions, one warp per parameter for long ones (the 32 lanes take the 32 subtrees five levels
-// down the same halving tree and combine them pairwise in tree order); normalize_kernel -- one
-// thread per destination element.  HBM-bound.
+// reductions, one warp per parameter for long ones (the parameter's elements staged once in shared
+// memory when contiguous; the 32 lanes take the 32 subtrees five levels down the same halving tree
+// and combine them pairwise in tree order); normalize_kernel -- one destination row per CTA step,
+// four columns per thread.  HBM-bound.
 #include "common.cuh"
 #include "ops.hpp"
 
@@ -29,6 +30,7 @@ constexpr int kThreads = 256;
 // warp-parallel tree from this reduction length on: every node of the top five levels then holds
 // at least floor(n / 16) >= 34 > 32 elements, so it splits as the lanes assume
 constexpr int kWarpMinElems = 544;
+constexpr int kStageElems = 1024;   // per warp: 4 KB of shared memory
 
 // The reference's compute_sum / compute_diff_square_sum value (the "+= into 0" steps are exact:
 // the partial sums are never -0).
@@ -88,6 +90,10 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormalizeArgs a, const 
 {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * kThreads) >> 5;
+    // warp mode: a parameter's contiguous elements are read once, coalesced, into this warp's
+    // buffer, and both tree sums run from there
+    __shared__ float s_stage[kThreads / 32][kStageElems];
+    float* stage = s_stage[threadIdx.x >> 5];
     for (int t = (blockIdx.x * kThreads + threadIdx.x) >> 5; t < numTasks; t += warps)
     {
         const int4 task = tasks[t];   // sample, first parameter, parameters, warp mode
@@ -96,11 +102,19 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormalizeArgs a, const 
         const float* base = a.src + size_t(b) * a.srcStride0;
         auto one = [&](int p, bool warp) {
             const float* in = base + (long long)p * s.paramStride;
+            int es = s.elemStride;
+            if (warp && es == 1 && s.count <= kStageElems)
+            {
+                __syncwarp();   // the previous task's reads of the buffer are done
+                for (int k = lane; k < s.count; k += 32) stage[k] = __ldg(in + k);
+                __syncwarp();
+                in = stage;
+            }
             float mean;
             if (a.compute & 1)
             {
-                const float sum = warp ? warp_tree_sum<false>(in, s.elemStride, s.count, 0.f)
-                                       : tree_sum<false>(in, s.elemStride, s.count, 0.f);
+                const float sum = warp ? warp_tree_sum<false>(in, es, s.count, 0.f)
+                                       : tree_sum<false>(in, es, s.count, 0.f);
                 mean = __fmul_rn(sum, s.normFactor);
             }
             else
@@ -108,8 +122,8 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormalizeArgs a, const 
             float inv = 0.f;
             if (a.compute & 2)
             {
-                const float sq = warp ? warp_tree_sum<true>(in, s.elemStride, s.count, mean)
-                                      : tree_sum<true>(in, s.elemStride, s.count, mean);
+                const float sq = warp ? warp_tree_sum<true>(in, es, s.count, mean)
+                                      : tree_sum<true>(in, es, s.count, mean);
                 const float x = __fmul_rn(sq, s.normFactor);
                 inv = x != 0.f ? __fmul_rn(__frsqrt_rn(x), a.scale) : 0.f;
             }
@@ -134,25 +148,64 @@ __global__ void __launch_bounds__(kThreads) invert_kernel(const float* __restric
     }
 }
 
+// One destination row (dstStride1 elements of a sample) per CTA step, 4 consecutive columns per
+// thread: roi elements get (x - mean) * inv + shift, the rest of the sample's stride zeros.
+// 16-byte loads and stores where the strides and addresses allow.
 __global__ void __launch_bounds__(kThreads) normalize_kernel(NormalizeArgs a, const float* __restrict__ mean,
-                                                             const float* __restrict__ inv, int paramOffsetPerSample)
+                                                             const float* __restrict__ inv, int paramOffsetPerSample,
+                                                             int rowsPerSample, bool vecSrc, bool vecDst)
 {
-    const long long total = (long long)a.n * a.dstStride0;
-    for (long long e = blockIdx.x * (long long)kThreads + threadIdx.x; e < total; e += (long long)gridDim.x * kThreads)
+    const long long units = (long long)a.n * rowsPerSample;
+    for (long long u = blockIdx.x; u < units; u += gridDim.x)
     {
-        const int b = int(e / a.dstStride0);
-        const uint32_t i = uint32_t(e - (long long)b * a.dstStride0);
+        const int b = int(u / rowsPerSample);
+        const uint32_t r = uint32_t(u - (long long)b * rowsPerSample);
         const NormalizeSample s = a.samples[b];
-        const uint32_t r = i / a.dstStride1, c = i - r * a.dstStride1;
-        float v = 0.f;
-        if (r < uint32_t(s.len0) && c < uint32_t(s.len1))
+        const uint32_t rowBegin = r * a.dstStride1;
+        const uint32_t rowLen = min(a.dstStride1, a.dstStride0 - rowBegin);
+        float* d = a.dst + size_t(b) * a.dstStride0 + rowBegin;
+        const bool rowIn = r < uint32_t(s.len0);
+        const float* x = a.src + size_t(b) * a.srcStride0 + size_t(r) * a.srcStride1;
+        const size_t q0 = size_t(b) * paramOffsetPerSample;
+        float rowMean = 0.f, rowInv = 0.f;
+        if (rowIn && a.axisMask != 1)
         {
-            const int p = a.axisMask == 2 ? int(r) : a.axisMask == 1 ? int(c) : 0;
-            const size_t q = size_t(b) * paramOffsetPerSample + p;
-            const float x = a.src[size_t(b) * a.srcStride0 + size_t(r) * a.srcStride1 + size_t(c) * a.srcStride2];
-            v = __fadd_rn(__fmul_rn(__fsub_rn(x, mean[q]), inv[q]), a.shift);
+            const size_t q = q0 + (a.axisMask == 2 ? r : 0);
+            rowMean = mean[q];
+            rowInv = inv[q];
         }
-        a.dst[size_t(b) * a.dstStride0 + i] = v;
+        const uint32_t len1 = rowIn ? uint32_t(s.len1) : 0u;
+        for (uint32_t c = 4 * threadIdx.x; c < rowLen; c += 4 * kThreads)
+        {
+            float xv[4] = {0.f, 0.f, 0.f, 0.f};
+            if (c + 4 <= len1 && vecSrc)
+            {
+                const float4 v = __ldg(reinterpret_cast<const float4*>(x + c));
+                xv[0] = v.x; xv[1] = v.y; xv[2] = v.z; xv[3] = v.w;
+            }
+            else
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (c + t < len1) xv[t] = __ldg(x + size_t(c + t) * a.srcStride2);
+            float ov[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+            {
+                float m = rowMean, iv = rowInv;
+                if (a.axisMask == 1 && c + t < len1)
+                {
+                    m = mean[q0 + c + t];
+                    iv = inv[q0 + c + t];
+                }
+                ov[t] = c + t < len1 ? __fadd_rn(__fmul_rn(__fsub_rn(xv[t], m), iv), a.shift) : 0.f;
+            }
+            if (c + 4 <= rowLen && vecDst)
+                *reinterpret_cast<float4*>(d + c) = make_float4(ov[0], ov[1], ov[2], ov[3]);
+            else
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (c + t < rowLen) d[c + t] = ov[t];
+        }
     }
 }
 
@@ -176,13 +229,18 @@ void launch_normalize(Handle& h, const NormalizeArgs& a, const int4* tasks, int 
         stats_kernel<<<std::max(grid, 1), kThreads, 0, h.stream()>>>(a, tasks, numTasks);
         count_launch(1);
     }
-    const long long total = (long long)a.n * a.dstStride0;
-    if (total > 0)
+    if (a.dstStride0 > 0)
     {
-        const int grid = int(std::min<long long>((total + kThreads - 1) / kThreads,
-                                                 persistent_grid(h, reinterpret_cast<const void*>(normalize_kernel),
-                                                                 kThreads, 0)));
-        normalize_kernel<<<grid, kThreads, 0, h.stream()>>>(a, meanEff, invEff, paramOffsetPerSample);
+        const int rowsPerSample = int((a.dstStride0 + a.dstStride1 - 1) / a.dstStride1);
+        const long long units = (long long)a.n * rowsPerSample;
+        const bool vecSrc = a.srcStride2 == 1 && (a.srcStride0 & 3) == 0 && (a.srcStride1 & 3) == 0 &&
+                            (reinterpret_cast<uintptr_t>(a.src) & 15) == 0;
+        const bool vecDst = (a.dstStride0 & 3) == 0 && (a.dstStride1 & 3) == 0 &&
+                            (reinterpret_cast<uintptr_t>(a.dst) & 15) == 0;
+        const int grid = int(std::min<long long>(
+            units, persistent_grid(h, reinterpret_cast<const void*>(normalize_kernel), kThreads, 0)));
+        normalize_kernel<<<grid, kThreads, 0, h.stream()>>>(a, meanEff, invEff, paramOffsetPerSample, rowsPerSample,
+                                                            vecSrc, vecDst);
         count_launch(1);
     }
     check_cuda(cudaGetLastError(), "normalize");
