@@ -42,6 +42,9 @@ CASES = [
     dict(nfft=1024, window_length=1024, window_step=256, num_filter=64, reference_magnitude=1.0, lookahead=64),
     dict(nfft=512, window_length=400, window_step=160, num_filter=128, center=False, reflect=False,
          cut_off_db=-60.0),
+    dict(nfft=2048, window_length=1600, window_step=400, num_filter=128),
+    dict(nfft=128, window_length=100, window_step=51, num_filter=20),    # odd hop: unpaired window gather
+    dict(nfft=512, window_length=400, window_step=160, num_filter=128, power=1),
 ]
 
 
