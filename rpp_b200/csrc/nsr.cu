@@ -12,8 +12,8 @@
 // reference's order (add the new square, store sum * (1/windowLength), subtract the square
 // leaving the window; explicit round-to-nearest intrinsics, no FMA): the MMS values, and hence
 // the begin/length integers, are bit-identical to the host path.
-//   1. mms_kernel:    one warp per (sample, reset block): coalesced loads and squares by the warp,
-//                     the chain by one lane, MMS into scratch, block maximum;
+//   1. mms_kernel:    one warp per 4 (sample, reset block) units: coalesced loads and squares by
+//                     the warp, the 4 chains by 4 lanes together, MMS into scratch, block maxima;
 //   2. region_kernel: one warp per sample: cutoff from the block maxima, then the first and
 //                     last qualifying block are scanned (ballot over 32 MMS at a time).
 // Latency-bound by the per-block chain (resetInterval + windowLength dependent steps); the
@@ -48,69 +48,146 @@ __device__ __forceinline__ float sq(float v) { return __fmul_rn(v, v); }
 
 constexpr int kMmsThreads = 256;
 constexpr int kMmsWarps = kMmsThreads / 32;
-constexpr int kChunk = 256;   // samples per warp step
+constexpr int kBlocksPerWarp = 4;            // chains per warp (lanes 0, 8, 16, 24): 2 and 8 measured slower
+constexpr int kChunk = 128;                  // samples of each block per warp step
+constexpr int kRowPitch = kChunk + 4;        // rows 16-byte aligned, the 4 chain lanes' quads in distinct banks
+constexpr int kWarpFloats = 3 * kBlocksPerWarp * kRowPitch;   // entering, leaving, MMS rows
 
-// One warp per (sample, reset block).  Per chunk of 256 samples the warp loads the samples entering
-// and leaving the window (coalesced), squares them in parallel into shared memory, then lane 0
-// runs the block's float chain over the chunk (two dependent adds per sample -- the only serial
+// One warp per 4 consecutive (sample, reset block) units; lane 8j replays block j's float chain.
+// Per step of 128 samples per block the warp loads the samples entering and leaving each block's
+// window (coalesced), squares them in parallel into shared memory, then the 4 chain lanes run
+// their blocks' chains together over the step (two dependent adds per sample -- the only serial
 // part; squares and the scaled stores are off the chain) and the warp stores the MMS values.  A
-// square of zero stands for "nothing leaves the window yet": sum - 0 == sum exactly for the
+// square of zero stands for "nothing enters / leaves": sum + 0 and sum - 0 == sum exactly for the
 // non-negative sums of squares, so the chain is bit-identical to the reference's conditional
-// subtraction.
+// subtraction, and the padding past a shorter block's end neither changes its stored values nor
+// raises its maximum.
 __global__ void __launch_bounds__(kMmsThreads) mms_kernel(const float* __restrict__ src, uint32_t stride,
                                                          const int* __restrict__ len, int windowLength, int reset,
                                                          float* __restrict__ mms, float* __restrict__ blockMax,
                                                          const long long* __restrict__ prefix, int n)
 {
+    extern __shared__ __align__(16) float s_mms[];
     __shared__ long long s_prefix[kPrefixCache];
-    __shared__ __align__(16) float s_in[kMmsWarps][kChunk];
-    __shared__ __align__(16) float s_out[kMmsWarps][kChunk];
-    __shared__ __align__(16) float s_val[kMmsWarps][kChunk];
     prefix = cache_prefix(prefix, n, s_prefix);
     const long long total = prefix[n];
     const float meanFactor = __fdiv_rn(1.0f, float(windowLength));
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-    float* qi = s_in[wi];
-    float* qo = s_out[wi];
-    float* vv = s_val[wi];
-    for (long long w = blockIdx.x * (long long)kMmsWarps + wi; w < total; w += (long long)gridDim.x * kMmsWarps)
+    float* qi = s_mms + wi * kWarpFloats;                 // [4][kRowPitch]
+    float* qo = qi + kBlocksPerWarp * kRowPitch;
+    float* vv = qo + kBlocksPerWarp * kRowPitch;
+    constexpr int kLaneGap = 32 / kBlocksPerWarp;
+    const int chainBlock = lane / kLaneGap;               // the block this lane replays (lanes kLaneGap * j)
+    const bool chainLane = lane % kLaneGap == 0;
+    // group g = 4 consecutive units; groups go to CTAs first, so every SM gets work
+    for (long long g = blockIdx.x + (long long)wi * gridDim.x; g * kBlocksPerWarp < total;
+         g += (long long)gridDim.x * kMmsWarps)
     {
-        const int b = ragged_find(prefix, n, w);
-        const int L = min(len[b], int(stride));
-        const long long R = block_len(L, reset);
-        const int start = int((w - prefix[b]) * R);
-        const int end = int(min((long long)L, start + R));
-        const float* x = src + size_t(b) * stride;
-        float* m = mms + size_t(b) * stride;
-        float sum = 0.0f;   // meaningful in lane 0
-        // fresh sum over the window that precedes the block (reference :131-133)
-        for (int c = max(start - windowLength + 1, 0); c < start; c += kChunk)
+        int bb[kBlocksPerWarp], st[kBlocksPerWarp], en[kBlocksPerWarp], pre[kBlocksPerWarp];
+        int preMax = 0, blkMax = 0;
+#pragma unroll
+        for (int j = 0; j < kBlocksPerWarp; ++j)
         {
-            const int cnt = min(kChunk, start - c);
-            for (int k = lane; k < cnt; k += 32) qi[k] = sq(__ldg(x + c + k));
-            __syncwarp();
-            if (lane == 0)
-                for (int k = 0; k < cnt; ++k) sum = __fadd_rn(sum, qi[k]);
-            __syncwarp();
-        }
-        float bmax = -FLT_MAX;
-        for (int c = start; c < end; c += kChunk)
-        {
-            const int cnt = min(kChunk, end - c);
-            for (int k = lane; k < cnt; k += 32)
+            const long long w = g * kBlocksPerWarp + j;
+            bb[j] = 0, st[j] = 0, en[j] = 0, pre[j] = 0;
+            if (w < total)
             {
-                qi[k] = sq(__ldg(x + c + k));
-                const int wb = c + k - windowLength + 1;
-                qo[k] = wb >= 0 ? sq(__ldg(x + wb)) : 0.0f;
+                bb[j] = ragged_find(prefix, n, w);
+                const int L = min(len[bb[j]], int(stride));
+                const long long R = block_len(L, reset);
+                st[j] = int((w - prefix[bb[j]]) * R);
+                en[j] = int(min((long long)L, st[j] + R));
+                pre[j] = max(st[j] - windowLength + 1, 0);   // fresh-sum range [pre, st) (reference :131-133)
+            }
+            preMax = max(preMax, st[j] - pre[j]);
+            blkMax = max(blkMax, en[j] - st[j]);
+        }
+        float sum = 0.0f, bmax = -FLT_MAX;   // meaningful in the chain lanes
+        for (int c = 0; c < preMax; c += kChunk)
+        {
+            // all of the step's loads are in flight before the first is used
+            float r[kBlocksPerWarp][kChunk / 32];
+#pragma unroll
+            for (int j = 0; j < kBlocksPerWarp; ++j)
+            {
+                const float* x = src + size_t(bb[j]) * stride;
+#pragma unroll
+                for (int t = 0; t < kChunk / 32; ++t)
+                {
+                    const int i = pre[j] + c + lane + 32 * t;
+                    r[j][t] = i < st[j] ? __ldg(x + i) : 0.0f;
+                }
+            }
+            if (lane < kBlocksPerWarp)   // the next steps' samples, from L2
+            {
+                const int i0 = pre[lane] + c + 2 * kChunk;
+                l2_prefetch(src + size_t(bb[lane]) * stride + i0,
+                            src + size_t(bb[lane]) * stride + max(i0, min(st[lane], i0 + 2 * kChunk)));
+            }
+#pragma unroll
+            for (int j = 0; j < kBlocksPerWarp; ++j)
+#pragma unroll
+                for (int t = 0; t < kChunk / 32; ++t) qi[j * kRowPitch + lane + 32 * t] = sq(r[j][t]);
+            __syncwarp();
+            if (chainLane)
+            {
+                const float* row = qi + chainBlock * kRowPitch;
+                for (int k = 0; k < kChunk; k += 4)
+                {
+                    const float4 a4 = *reinterpret_cast<const float4*>(row + k);
+                    sum = __fadd_rn(sum, a4.x);
+                    sum = __fadd_rn(sum, a4.y);
+                    sum = __fadd_rn(sum, a4.z);
+                    sum = __fadd_rn(sum, a4.w);
+                }
             }
             __syncwarp();
-            if (lane == 0)
+        }
+        // software-pipelined: the next step's loads are issued before this step's chains run
+        float ri[kBlocksPerWarp][kChunk / 32], ro[kBlocksPerWarp][kChunk / 32];
+        auto load_step = [&](int c) {
+#pragma unroll
+            for (int j = 0; j < kBlocksPerWarp; ++j)
             {
-                int k = 0;
-                for (; k + 4 <= cnt; k += 4)
+                const float* x = src + size_t(bb[j]) * stride;
+#pragma unroll
+                for (int t = 0; t < kChunk / 32; ++t)
                 {
-                    const float4 a4 = *reinterpret_cast<const float4*>(qi + k);
-                    const float4 o4 = *reinterpret_cast<const float4*>(qo + k);
+                    const int i = st[j] + c + lane + 32 * t, o = i - windowLength + 1;
+                    const bool live = i < en[j];
+                    ri[j][t] = live ? __ldg(x + i) : 0.0f;
+                    ro[j][t] = live && o >= 0 ? __ldg(x + o) : 0.0f;
+                }
+            }
+            if (lane < kBlocksPerWarp)   // later steps' entering samples, from L2
+            {
+                const int i0 = st[lane] + c + 2 * kChunk;
+                l2_prefetch(src + size_t(bb[lane]) * stride + i0,
+                            src + size_t(bb[lane]) * stride + max(i0, min(en[lane], i0 + 2 * kChunk)));
+            }
+        };
+        if (blkMax > 0) load_step(0);
+        for (int c = 0; c < blkMax; c += kChunk)
+        {
+#pragma unroll
+            for (int j = 0; j < kBlocksPerWarp; ++j)
+#pragma unroll
+                for (int t = 0; t < kChunk / 32; ++t)
+                {
+                    qi[j * kRowPitch + lane + 32 * t] = sq(ri[j][t]);
+                    qo[j * kRowPitch + lane + 32 * t] = sq(ro[j][t]);
+                }
+            if (c + kChunk < blkMax) load_step(c + kChunk);
+            __syncwarp();
+            if (chainLane)
+            {
+                const float* ri = qi + chainBlock * kRowPitch;
+                const float* ro = qo + chainBlock * kRowPitch;
+                float* rv = vv + chainBlock * kRowPitch;
+                for (int k = 0; k < kChunk; k += 4)
+                {
+                    const float4 a4 = *reinterpret_cast<const float4*>(ri + k);
+                    const float4 o4 = *reinterpret_cast<const float4*>(ro + k);
                     float4 v4;
                     sum = __fadd_rn(sum, a4.x);
                     v4.x = __fmul_rn(sum, meanFactor);
@@ -124,26 +201,29 @@ __global__ void __launch_bounds__(kMmsThreads) mms_kernel(const float* __restric
                     sum = __fadd_rn(sum, a4.w);
                     v4.w = __fmul_rn(sum, meanFactor);
                     sum = __fsub_rn(sum, o4.w);
-                    *reinterpret_cast<float4*>(vv + k) = v4;
-                }
-                for (; k < cnt; ++k)
-                {
-                    sum = __fadd_rn(sum, qi[k]);
-                    vv[k] = __fmul_rn(sum, meanFactor);
-                    sum = __fsub_rn(sum, qo[k]);
+                    bmax = fmaxf(fmaxf(bmax, fmaxf(v4.x, v4.y)), fmaxf(v4.z, v4.w));
+                    *reinterpret_cast<float4*>(rv + k) = v4;
                 }
             }
             __syncwarp();
-            for (int k = lane; k < cnt; k += 32)
+#pragma unroll
+            for (int j = 0; j < kBlocksPerWarp; ++j)
             {
-                const float v = vv[k];
-                m[c + k] = v;
-                bmax = fmaxf(bmax, v);
+                float* m = mms + size_t(bb[j]) * stride;
+#pragma unroll
+                for (int k = lane; k < kChunk; k += 32)
+                    if (st[j] + c + k < en[j]) m[st[j] + c + k] = vv[j * kRowPitch + k];
             }
             __syncwarp();
         }
-        bmax = warp_max(bmax);
-        if (lane == 0) blockMax[w] = bmax;
+        // chain lane 8j holds block j's maximum (values past a shorter block's end are below its last)
+#pragma unroll
+        for (int j = 0; j < kBlocksPerWarp; ++j)
+        {
+            const float bm = __shfl_sync(0xffffffffu, bmax, kLaneGap * j);
+            const long long w = g * kBlocksPerWarp + j;
+            if (lane == 0 && w < total) blockMax[w] = bm;
+        }
     }
 }
 
@@ -249,8 +329,9 @@ void launch_nsr(Handle& h, void* scratch, const NsrArgs& a)
     float* mms = cv.take<float>(size_t(a.n) * a.srcStride);
     float* blockMax = cv.take<float>(blocks + 1);
     launch_ragged_prefix(NsrCount{a.len, a.srcStride, a.resetInterval}, a.n, prefix, h.stream());
-    int grid = persistent_grid(h, reinterpret_cast<const void*>(mms_kernel), kMmsThreads, 0);
-    mms_kernel<<<grid, kMmsThreads, 0, h.stream()>>>(a.src, a.srcStride, a.len, a.windowLength, a.resetInterval, mms,
+    const size_t smem = size_t(kMmsWarps) * kWarpFloats * sizeof(float);
+    int grid = persistent_grid(h, reinterpret_cast<const void*>(mms_kernel), kMmsThreads, smem);
+    mms_kernel<<<grid, kMmsThreads, smem, h.stream()>>>(a.src, a.srcStride, a.len, a.windowLength, a.resetInterval, mms,
                                              blockMax, prefix, a.n);
     count_launch();
     check_cuda(cudaGetLastError(), "mms_kernel");
