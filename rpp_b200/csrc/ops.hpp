@@ -23,6 +23,7 @@ struct ResampleWindowDev
     int lutSize;
     float scale, center;
     int lobes;
+    int padLeft = 0, padRight = 0;   // set by the resample launchers (shared-memory pair table padding)
 };
 // downmix: the input is interleaved {length, channels} and is down-mixed to mono while resampling
 // (equal to rppt_down_mixing_gpu followed by a mono rppt_resample_gpu).

@@ -18,6 +18,8 @@
 // shared memory first.  The lookup table sits in shared memory as (value, next - value) pairs when
 // they fit, so a tap reads one 8-byte entry.  Compute-bound: 2 * lobes taps of ~10 float
 // operations per output.
+#include <cmath>
+
 #include "common.cuh"
 #include "downmix.cuh"
 #include "ops.hpp"
@@ -31,13 +33,31 @@ constexpr int kSpan = 4096;        // input samples of one block staged in share
 
 constexpr int kThreads = kBlock + 32;   // 8 warps compute outputs, the ninth replays the next unit's phases
 
-// Shared memory (floats): the table -- as (value, next - value) pairs when kPairs, else plain --
-// then the staged input span.
-__host__ __device__ __forceinline__ size_t resample_smem_floats(int lutSize, bool pairs)
+// Shared memory (floats): the table -- as padded (value, next - value) pairs when kPairs, else
+// plain -- then the staged input span.
+__host__ __device__ __forceinline__ size_t resample_pair_entries(int lutSize, int padLeft, int padRight)
 {
-    return (pairs ? 2 * size_t(lutSize) : ((size_t(lutSize) + 3) & ~size_t(3))) + kSpan;
+    return size_t(padLeft) + size_t(lutSize - 1) + size_t(padRight);
+}
+__host__ __device__ __forceinline__ size_t resample_smem_floats(const ResampleWindowDev& w, bool pairs)
+{
+    return (pairs ? 2 * resample_pair_entries(w.lutSize, w.padLeft, w.padRight)
+                  : ((size_t(w.lutSize) + 3) & ~size_t(3))) +
+           kSpan;
 }
 constexpr size_t kPairTableLimit = 200 * 1024;   // bytes of shared memory for the pair layout
+
+// Pair-table padding: a tap's x lies in (-(lobes + 1), lobes + 1), so its index, trunc or floor of
+// x * scale + center, lies within [center - (lobes + 1)|scale| - 2, center + (lobes + 1)|scale| + 2].
+inline void resample_pads(ResampleWindowDev& w)
+{
+    const double reach = (double(w.lobes) + 1.0) * std::fabs(double(w.scale));
+    const double lo = std::floor(double(w.center) - reach) - 2.0, hi = std::ceil(double(w.center) + reach) + 2.0;
+    const double padL = lo < 0.0 ? -lo : 0.0, padR = hi > double(w.lutSize - 2) ? hi - double(w.lutSize - 2) : 0.0;
+    const bool ok = padL < 65536.0 && padR < 65536.0;
+    w.padLeft = ok ? int(padL) : -1;
+    w.padRight = ok ? int(padR) : -1;
+}
 
 __device__ __forceinline__ int out_length(int L, float inRate, float outRate)
 {
@@ -74,20 +94,23 @@ struct ResampleCount
 template <bool kPairs>
 struct Win
 {
-    const float* lut;   // shared memory: floats, or (value, next - value) pairs when kPairs
+    const float* lut;     // shared memory: the table (plain layout)
+    const float2* pairs;  // shared memory: (value, next - value) at index 0 of the padded pair layout
     int lutSize;
     float scale, center;
 
     __device__ __forceinline__ float interp(int idx, float weight) const
     {
-        idx = min(max(idx, 0), lutSize - 2);
         if constexpr (kPairs)
         {
-            const float2 e = reinterpret_cast<const float2*>(lut)[idx];
+            // pairs[i] for i in [-padLeft, lutSize - 2 + padRight] holds the entry the clamped index
+            // [0, lutSize - 2] selects: no clamp for the indices a tap can produce
+            const float2 e = pairs[idx];
             return __fadd_rn(e.x, __fmul_rn(weight, e.y));
         }
         else
         {
+            idx = min(max(idx, 0), lutSize - 2);
             const float cur = lut[idx], nxt = lut[idx + 1];
             return __fadd_rn(cur, __fmul_rn(weight, __fsub_rn(nxt, cur)));
         }
@@ -131,14 +154,19 @@ __global__ void __launch_bounds__(kThreads) resample_kernel(const float* __restr
                                                             float outRateAll)
 {
     extern __shared__ float s_lut[];   // the table, then the staged input span
-    float* s_in = s_lut + (kPairs ? 2 * wd.lutSize : ((wd.lutSize + 3) & ~3));
+    const int pairCount = kPairs ? int(resample_pair_entries(wd.lutSize, wd.padLeft, wd.padRight)) : 0;
+    float* s_in = s_lut + (kPairs ? 2 * pairCount : ((wd.lutSize + 3) & ~3));
     __shared__ float s_phase[2][kBlock];
     if (kPairs)
-        for (int i = threadIdx.x; i < wd.lutSize - 1; i += kThreads)
-            reinterpret_cast<float2*>(s_lut)[i] = make_float2(wd.lut[i], __fsub_rn(wd.lut[i + 1], wd.lut[i]));
+        for (int i = threadIdx.x; i < pairCount; i += kThreads)
+        {
+            const int e = min(max(i - wd.padLeft, 0), wd.lutSize - 2);   // the clamped entry
+            reinterpret_cast<float2*>(s_lut)[i] = make_float2(wd.lut[e], __fsub_rn(wd.lut[e + 1], wd.lut[e]));
+        }
     else
         for (int i = threadIdx.x; i < wd.lutSize; i += kThreads) s_lut[i] = wd.lut[i];
-    const Win<kPairs> win{s_lut, wd.lutSize, wd.scale, wd.center};
+    const Win<kPairs> win{s_lut, reinterpret_cast<const float2*>(s_lut) + (kPairs ? wd.padLeft : 0), wd.lutSize,
+                          wd.scale, wd.center};
     const int lobes = wd.lobes;
     __shared__ long long s_prefix[kPrefixCache];
     prefix = cache_prefix(prefix, n, s_prefix);   // ends with __syncthreads
@@ -312,11 +340,13 @@ void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStr
     if (n <= 0) return;
     long long* prefix = static_cast<long long*>(scratch);
     launch_ragged_prefix(ResampleCount{inRate, outRate, dims, downmix, nullptr, 0.f}, n, prefix, h.stream());
-    const bool pairs = resample_smem_floats(win.lutSize, true) * sizeof(float) <= kPairTableLimit;
-    const size_t smem = resample_smem_floats(win.lutSize, pairs) * sizeof(float);
+    ResampleWindowDev w = win;
+    resample_pads(w);
+    const bool pairs = w.padLeft >= 0 && resample_smem_floats(w, true) * sizeof(float) <= kPairTableLimit;
+    const size_t smem = resample_smem_floats(w, pairs) * sizeof(float);
     auto go = [&](auto kernel) {
         const int grid = persistent_grid(h, reinterpret_cast<const void*>(kernel), kThreads, smem);
-        kernel<<<grid, kThreads, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate, outRate, dims, win,
+        kernel<<<grid, kThreads, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate, outRate, dims, w,
                                                      normalize, prefix, n, nullptr, 0.f);
     };
     if (downmix && pairs) go(resample_kernel<true, false, true>);
@@ -333,11 +363,13 @@ void launch_resample_clips(Handle& h, void* scratch, const RppbClip* clips, int 
     if (n <= 0) return;
     long long* prefix = static_cast<long long*>(scratch);
     launch_ragged_prefix(ResampleCount{nullptr, nullptr, nullptr, false, clips, outRate}, n, prefix, h.stream());
-    const bool pairs = resample_smem_floats(win.lutSize, true) * sizeof(float) <= kPairTableLimit;
-    const size_t smem = resample_smem_floats(win.lutSize, pairs) * sizeof(float);
+    ResampleWindowDev w = win;
+    resample_pads(w);
+    const bool pairs = w.padLeft >= 0 && resample_smem_floats(w, true) * sizeof(float) <= kPairTableLimit;
+    const size_t smem = resample_smem_floats(w, pairs) * sizeof(float);
     auto go = [&](auto kernel) {
         const int grid = persistent_grid(h, reinterpret_cast<const void*>(kernel), kThreads, smem);
-        kernel<<<grid, kThreads, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, win, false,
+        kernel<<<grid, kThreads, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, w, false,
                                                      prefix, n, clips, outRate);
     };
     if (pairs) go(resample_kernel<false, true, true>);
