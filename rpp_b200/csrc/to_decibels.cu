@@ -68,10 +68,14 @@ __device__ __forceinline__ UnitSpan unit_span(uint32_t wdt, uint32_t hgt, long l
     return s;
 }
 
+// Both kernels walk a unit's elements in (row, column) runs: warp wi takes rows s.row + wi,
+// s.row + wi + 8, ...; its lanes walk the row 4 columns at a time (16-byte accesses when the strides
+// and addresses allow), so no element index is divided.  A 1-D unit (one row of up to 4096 values)
+// is walked by all threads.
 __global__ void __launch_bounds__(kThreads) decibel_max_kernel(const float* __restrict__ src, uint32_t nStride,
                                                                uint32_t hStride, const uint32_t* __restrict__ dims,
                                                                unsigned* __restrict__ maxKey,
-                                                               const long long* __restrict__ prefix, int n)
+                                                               const long long* __restrict__ prefix, int n, bool vec)
 {
     __shared__ float warpMax[kThreads / 32];
     __shared__ long long s_prefix[kPrefixCache];
@@ -82,26 +86,38 @@ __global__ void __launch_bounds__(kThreads) decibel_max_kernel(const float* __re
         const int b = ragged_find(prefix, n, w);
         const uint32_t wdt = dims[2 * b], hgt = dims[2 * b + 1];
         const UnitSpan s = unit_span(wdt, hgt, w - prefix[b]);
-        float m = -FLT_MAX;
-        // the unit's rows x cols elements, 4 loads per thread in flight
-        const uint32_t count = s.rows * s.cols;
         const float* base = src + size_t(b) * nStride + size_t(s.row) * hStride + s.col0;
-        for (uint32_t i0 = threadIdx.x; i0 < count; i0 += 4 * kThreads)
+        // a lane loads 4 column steps (16 values) before folding them, so the loads overlap
+        float m = -FLT_MAX;
+        const bool oneD = wdt == 1;
+        const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+        const uint32_t step = oneD ? 4u * kThreads : 128u;
+        const uint32_t first = oneD ? 4u * threadIdx.x : 4u * lane;
+        const uint32_t r0 = oneD ? 0u : uint32_t(wi), rstep = oneD ? 1u : uint32_t(kThreads / 32);
+        constexpr int kBatch = 4;
+        for (uint32_t r = r0; r < s.rows; r += rstep)
         {
-            float v[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
+            const float* p = base + size_t(r) * hStride;
+            for (uint32_t c0 = first; c0 < s.cols; c0 += kBatch * step)
             {
-                const uint32_t i = i0 + j * kThreads;
-                v[j] = -FLT_MAX;
-                if (i < count)
-                {
-                    const uint32_t r = i / s.cols, c = i - r * s.cols;
-                    v[j] = base[size_t(r) * hStride + c];
-                }
-            }
+                float4 x[kBatch];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) m = fmaxf(m, v[j]);
+                for (int k = 0; k < kBatch; ++k)
+                {
+                    const uint32_t c = c0 + k * step;
+                    x[k] = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX);
+                    if (vec && c + 4 <= s.cols) x[k] = __ldg(reinterpret_cast<const float4*>(p + c));
+                    else
+                    {
+                        if (c < s.cols) x[k].x = __ldg(p + c);
+                        if (c + 1 < s.cols) x[k].y = __ldg(p + c + 1);
+                        if (c + 2 < s.cols) x[k].z = __ldg(p + c + 2);
+                        if (c + 3 < s.cols) x[k].w = __ldg(p + c + 3);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) m = fmaxf(m, fmaxf(fmaxf(x[k].x, x[k].y), fmaxf(x[k].z, x[k].w)));
+            }
         }
         m = warp_max(m);
         if ((threadIdx.x & 31) == 0) warpMax[threadIdx.x >> 5] = m;
@@ -123,7 +139,7 @@ __global__ void __launch_bounds__(kThreads) decibel_kernel(const float* __restri
                                                            const uint32_t* __restrict__ dims,
                                                            const unsigned* __restrict__ maxKey, float refMag,
                                                            float minRatio, float multiplier,
-                                                           const long long* __restrict__ prefix, int n)
+                                                           const long long* __restrict__ prefix, int n, bool vec)
 {
     __shared__ long long s_prefix[kPrefixCache];
     prefix = cache_prefix(prefix, n, s_prefix);
@@ -140,30 +156,56 @@ __global__ void __launch_bounds__(kThreads) decibel_kernel(const float* __restri
             ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
         }
         const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
-        // the unit's rows x cols elements, 4 per thread loaded before they are converted and stored
-        // (in-place calls alias src and dst: every element is loaded before its own store)
-        const uint32_t count = s.rows * s.cols;
+        auto db = [&](float x) {
+            float t = __fmul_rn(x, inv);
+            t = minRatio < t ? t : minRatio;
+            return __fmul_rn(multiplier, __log2f(t));
+        };
+        // in-place calls alias src and dst: every element is loaded before its own store.  A lane
+        // loads 4 column steps (16 values) before converting and storing them, so the loads overlap.
         const float* xb = src + size_t(b) * srcNStride + size_t(s.row) * srcHStride + s.col0;
         float* yb = dst + size_t(b) * dstNStride + size_t(s.row) * dstHStride + s.col0;
-        for (uint32_t i0 = threadIdx.x; i0 < count; i0 += 4 * kThreads)
+        const bool oneD = wdt == 1;
+        const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+        const uint32_t step = oneD ? 4u * kThreads : 128u;
+        const uint32_t first = oneD ? 4u * threadIdx.x : 4u * lane;
+        const uint32_t r0 = oneD ? 0u : uint32_t(wi), rstep = oneD ? 1u : uint32_t(kThreads / 32);
+        constexpr int kBatch = 4;
+        for (uint32_t r = r0; r < s.rows; r += rstep)
         {
-            float v[4];
-            uint32_t rr[4], cc[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
+            const float* p = xb + size_t(r) * srcHStride;
+            float* q = yb + size_t(r) * dstHStride;
+            for (uint32_t c0 = first; c0 < s.cols; c0 += kBatch * step)
             {
-                const uint32_t i = i0 + j * kThreads;
-                rr[j] = i / s.cols;
-                cc[j] = i - rr[j] * s.cols;
-                if (i < count) v[j] = xb[size_t(rr[j]) * srcHStride + cc[j]];
-            }
+                float4 x[kBatch];
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-            {
-                if (i0 + j * kThreads >= count) break;
-                float t = __fmul_rn(v[j], inv);
-                t = minRatio < t ? t : minRatio;
-                yb[size_t(rr[j]) * dstHStride + cc[j]] = __fmul_rn(multiplier, __log2f(t));
+                for (int k = 0; k < kBatch; ++k)
+                {
+                    const uint32_t c = c0 + k * step;
+                    x[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (vec && c + 4 <= s.cols) x[k] = *reinterpret_cast<const float4*>(p + c);
+                    else
+                    {
+                        if (c < s.cols) x[k].x = p[c];
+                        if (c + 1 < s.cols) x[k].y = p[c + 1];
+                        if (c + 2 < s.cols) x[k].z = p[c + 2];
+                        if (c + 3 < s.cols) x[k].w = p[c + 3];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k)
+                {
+                    const uint32_t c = c0 + k * step;
+                    const float4 y = make_float4(db(x[k].x), db(x[k].y), db(x[k].z), db(x[k].w));
+                    if (vec && c + 4 <= s.cols) *reinterpret_cast<float4*>(q + c) = y;
+                    else
+                    {
+                        if (c < s.cols) q[c] = y.x;
+                        if (c + 1 < s.cols) q[c + 1] = y.y;
+                        if (c + 2 < s.cols) q[c + 2] = y.z;
+                        if (c + 3 < s.cols) q[c + 3] = y.w;
+                    }
+                }
             }
         }
     }
@@ -179,18 +221,21 @@ void launch_to_decibels(Handle& h, void* scratch, const DecibelArgs& a)
     unsigned* maxKey = cv.take<unsigned>(a.n);
     launch_ragged_prefix(DecibelCount{a.dims}, a.n, prefix, h.stream());
     const bool useMax = (a.referenceMagnitude == 0.f);
+    auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    const bool vecSrc = aligned(a.src) && (a.srcNStride & 3) == 0 && (a.srcHStride & 3) == 0;
+    const bool vec = vecSrc && aligned(a.dst) && (a.dstNStride & 3) == 0 && (a.dstHStride & 3) == 0;
     if (useMax)
     {
         check_cuda(cudaMemsetAsync(maxKey, 0, size_t(a.n) * sizeof(unsigned), h.stream()), "memset(max)");
         int grid = persistent_grid(h, reinterpret_cast<const void*>(decibel_max_kernel), kThreads, 0);
         decibel_max_kernel<<<grid, kThreads, 0, h.stream()>>>(a.src, a.srcNStride, a.srcHStride, a.dims, maxKey,
-                                                              prefix, a.n);
+                                                              prefix, a.n, vecSrc);
         count_launch();
         check_cuda(cudaGetLastError(), "decibel_max_kernel");
         grid = persistent_grid(h, reinterpret_cast<const void*>(decibel_kernel<true>), kThreads, 0);
         decibel_kernel<true><<<grid, kThreads, 0, h.stream()>>>(a.src, a.srcNStride, a.srcHStride, a.dst, a.dstNStride,
                                                                 a.dstHStride, a.dims, maxKey, 0.f, a.minRatio,
-                                                                a.multiplier, prefix, a.n);
+                                                                a.multiplier, prefix, a.n, vec);
         count_launch();
     }
     else
@@ -199,7 +244,7 @@ void launch_to_decibels(Handle& h, void* scratch, const DecibelArgs& a)
         decibel_kernel<false><<<grid, kThreads, 0, h.stream()>>>(a.src, a.srcNStride, a.srcHStride, a.dst,
                                                                  a.dstNStride, a.dstHStride, a.dims, nullptr,
                                                                  a.referenceMagnitude, a.minRatio, a.multiplier,
-                                                                 prefix, a.n);
+                                                                 prefix, a.n, vec);
         count_launch();
     }
     check_cuda(cudaGetLastError(), "decibel_kernel");
@@ -315,20 +360,24 @@ extern "C" SHARED_PUBLIC RppStatus rppt_to_decibels_gpu_static(RppPtr_t srcPtr, 
     const uint32_t sN = srcDescPtr->strides.nStride, sH = srcDescPtr->strides.hStride;
     const uint32_t dN = dstDescPtr->strides.nStride, dH = dstDescPtr->strides.hStride;
     launch_ragged_prefix(DecibelCount{dims}, n, prefix, s);
+    auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    const bool vecSrc = aligned(src) && (sN & 3) == 0 && (sH & 3) == 0;
+    const bool vec = vecSrc && aligned(dst) && (dN & 3) == 0 && (dH & 3) == 0;
     if (referenceMagnitude == 0.f)
     {
         // the maxima accumulate with atomicMax: start every call from zero keys
         if (cudaMemsetAsync(maxKey, 0, size_t(n) * sizeof(unsigned), s) != cudaSuccess) return RPP_ERROR;
-        decibel_max_kernel<<<sd->gridMax, kThreads, 0, s>>>(src, sN, sH, dims, maxKey, prefix, n);
+        decibel_max_kernel<<<sd->gridMax, kThreads, 0, s>>>(src, sN, sH, dims, maxKey, prefix, n, vecSrc);
         count_launch();
         decibel_kernel<true><<<sd->gridTrue, kThreads, 0, s>>>(src, sN, sH, dst, dN, dH, dims, maxKey, 0.f, minRatio,
-                                                               multiplier, prefix, n);
+                                                               multiplier, prefix, n, vec);
         count_launch();
     }
     else
     {
         decibel_kernel<false><<<sd->gridFalse, kThreads, 0, s>>>(src, sN, sH, dst, dN, dH, dims, nullptr,
-                                                                 referenceMagnitude, minRatio, multiplier, prefix, n);
+                                                                 referenceMagnitude, minRatio, multiplier, prefix, n,
+                                                                 vec);
         count_launch();
     }
     return cudaGetLastError() == cudaSuccess ? RPP_SUCCESS : RPP_ERROR;
