@@ -9,8 +9,9 @@
 //
 // Work list: (sample, 32-frame tile) units.  A CTA stages the tile's spectrum rows
 // [binStart, binEnd) x 32 frames in shared memory (one coalesced 128-byte row segment per bin), then
-// thread (group g, frame t) computes filters g, g+8, ... for frame t from shared memory and a warp
-// stores 32 consecutive frames of one filter row.  Tables are built by the CTA (rebuilt only when
+// thread (group g, frame pair t) sweeps the bins of group g's contiguous filter range once for two
+// frames (each power pair read once, feeding its two filters) and a warp stores 32 consecutive
+// frames of two filter rows.  Tables are built by the CTA (rebuilt only when
 // the sample's bin count changes), sized for this call's numFilter and bins.
 #include <cfloat>
 
@@ -23,8 +24,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kTile = 32;            // frames per unit
-constexpr int kLd = kTile + 1;       // spectrum tile leading dimension (conflict-free columns)
-constexpr int kGroups = kThreads / kTile;
+constexpr int kLd = kTile + 2;       // spectrum tile leading dimension: even, so frame pairs load as float2
+constexpr int kPairs = kTile / 2;    // frame pairs per tile
+constexpr int kGroups = kThreads / kPairs;   // filter groups
 
 struct MelCount
 {
@@ -39,11 +41,12 @@ struct MelCount
 };
 
 // Shared memory plan for numFilter filters and at most maxBins bins (host and device agree).
-// rowStart/entries: filter m's weights as (tile offset of the bin's row, weight) pairs
-// entries[rowStart[m] .. rowStart[m + 1]), in the reference's accumulation order.
+// weights: bin k -> (weight into filter i, weight into filter i - 1) for k in interval i;
+// intervals: interval i -> its bins [x, y); groups: thread group g emits filters
+// [groups[g], groups[g + 1]).
 struct MelLayout
 {
-    size_t range, first, last, norm, f0, f1, wd, rowStart, entries, spec, total;
+    size_t range, first, last, norm, f0, f1, wd, weights, intervals, groups, cum, spec, total;
     __host__ __device__ MelLayout(int numFilter, int maxBins)
     {
         range = 0;
@@ -53,45 +56,77 @@ struct MelLayout
         f0 = (norm + size_t(numFilter) * 4 + 7) & ~size_t(7);
         f1 = f0 + size_t(numFilter + 1) * 8;
         wd = f1 + size_t(numFilter + 1) * 8;
-        rowStart = (wd + size_t(maxBins) * 4 + 15) & ~size_t(15);
-        entries = (rowStart + size_t(numFilter + 1) * 4 + 15) & ~size_t(15);
-        spec = (entries + size_t(2 * maxBins + 2) * 8 + 15) & ~size_t(15);
+        weights = (wd + size_t(maxBins) * 4 + 15) & ~size_t(15);
+        intervals = (weights + size_t(maxBins) * 8 + 15) & ~size_t(15);
+        groups = (intervals + size_t(numFilter + 1) * 8 + 15) & ~size_t(15);
+        cum = (groups + size_t(kGroups + 1) * 4 + 15) & ~size_t(15);
+        spec = (cum + size_t(numFilter + 1) * 4 + 15) & ~size_t(15);
         total = spec + size_t(maxBins) * kLd * 4;
     }
 };
 
-// Flattens the tables into (offset, weight) entries: bins of interval m with (1 - weightsDown) *
-// norm[m], then bins of interval m + 1 with weightsDown * norm[m] (norm only when normalizing);
-// offset = (bin - k0) * kLd in the staged tile.  Ends with __syncthreads.
-__device__ void build_entries(const MelTableView& T, int numFilter, bool normalize, int* rowStart, int2* ent)
+// Bin-major form of the tables: bin k of interval i (between mel points i and i + 1) weighs
+// (1 - weightsDown) * norm[i] into filter i and weightsDown * norm[i - 1] into filter i - 1 (norm
+// only when normalizing), so filter m sums interval m's bins, then interval m + 1's, in ascending
+// bin order -- the reference's accumulation.  The filter ranges of the kGroups thread groups are
+// balanced by (bins + 2) per interval: cum[i] = cost of intervals 0..i by a warp scan, boundary g
+// at 1 + the first filter m whose intervals 0..m+1
+// reach g / kGroups of the total (cum: numFilter + 1 ints of scratch).  Ends with __syncthreads.
+__device__ void build_sweep(const MelTableView& T, int numFilter, bool normalize, float2* weights, int2* intervals,
+                            int* groups, int* cum)
 {
-    const int k0 = T.range[0];
-    if (threadIdx.x == 0)
+    for (int i = threadIdx.x; i <= numFilter; i += blockDim.x)
     {
-        int acc = 0;
-        for (int m = 0; m < numFilter; ++m)
+        const int k0 = T.first[i], k1 = T.last[i];
+        intervals[i] = k1 > k0 ? make_int2(k0, k1) : make_int2(0, 0);
+        for (int k = k0; k < k1; ++k)
         {
-            rowStart[m] = acc;
-            acc += max(T.last[m] - T.first[m], 0) + max(T.last[m + 1] - T.first[m + 1], 0);
+            const float wd = T.weightsDown[k];
+            float rise = 0.f, fall = 0.f;
+            if (i < numFilter)
+            {
+                rise = __fsub_rn(1.0f, wd);
+                if (normalize) rise = __fmul_rn(rise, T.norm[i]);
+            }
+            if (i > 0) fall = normalize ? __fmul_rn(wd, T.norm[i - 1]) : wd;
+            weights[k] = make_float2(rise, fall);
         }
-        rowStart[numFilter] = acc;
+        cum[i] = (k1 > k0 ? k1 - k0 : 0) + 2;
     }
     __syncthreads();
-    for (int m = threadIdx.x; m < numFilter; m += blockDim.x)
+    if (threadIdx.x < 32)
     {
-        int e = rowStart[m];
-        for (int k = T.first[m]; k < T.last[m]; ++k, ++e)
+        const int lane = threadIdx.x, chunk = (numFilter + 1 + 31) / 32;
+        const int i0 = min(lane * chunk, numFilter + 1), i1 = min(i0 + chunk, numFilter + 1);
+        int sum = 0;
+        for (int i = i0; i < i1; ++i) sum += cum[i];
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
         {
-            float w = __fsub_rn(1.0f, T.weightsDown[k]);
-            if (normalize) w = __fmul_rn(w, T.norm[m]);
-            ent[e] = make_int2((k - k0) * kLd, __float_as_int(w));
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
-        for (int k = T.first[m + 1]; k < T.last[m + 1]; ++k, ++e)
+        int run = incl - sum;
+        for (int i = i0; i < i1; ++i)
         {
-            float w = T.weightsDown[k];
-            if (normalize) w = __fmul_rn(w, T.norm[m]);
-            ent[e] = make_int2((k - k0) * kLd, __float_as_int(w));
+            run += cum[i];
+            cum[i] = run;
         }
+    }
+    __syncthreads();
+    const int total = cum[numFilter];
+    for (int g = threadIdx.x; g <= kGroups; g += blockDim.x)
+    {
+        int lo = 0, hi = numFilter;
+        if (g > 0)
+            while (lo < hi)
+            {
+                const int mid = (lo + hi) >> 1;
+                if (cum[mid + 1] * kGroups >= g * total) hi = mid;
+                else lo = mid + 1;
+            }
+        groups[g] = g == 0 ? 0 : g == kGroups ? numFilter : min(lo + 1, numFilter);
     }
     __syncthreads();
 }
@@ -106,16 +141,17 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
                          reinterpret_cast<float*>(smem + lay.norm), reinterpret_cast<double*>(smem + lay.f0),
                          reinterpret_cast<double*>(smem + lay.f1), reinterpret_cast<float*>(smem + lay.wd), range};
     float* s_spec = reinterpret_cast<float*>(smem + lay.spec);
-    int* rowStart = reinterpret_cast<int*>(smem + lay.rowStart);
-    int2* ent = reinterpret_cast<int2*>(smem + lay.entries);
+    float2* weights = reinterpret_cast<float2*>(smem + lay.weights);
+    int2* intervals = reinterpret_cast<int2*>(smem + lay.intervals);
+    int* groups = reinterpret_cast<int*>(smem + lay.groups);
     const MelParams mp{a.minFreq, maxFreq, a.sampleRate, a.htk, a.numFilter, a.normalize};
     if (threadIdx.x == 0) range[2] = -1;
     __syncthreads();
     __shared__ long long s_prefix[kPrefixCache];
     prefix = cache_prefix(prefix, a.n, s_prefix);
     const long long total = prefix[a.n];
-    const int t = threadIdx.x % kTile;
-    const int g = threadIdx.x / kTile;
+    const int t = 2 * (threadIdx.x % kPairs);   // first of this thread's two frames
+    const int g = threadIdx.x / kPairs;
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
     {
         const int b = ragged_find(prefix, a.n, w);
@@ -129,7 +165,7 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
         if (ok && held != nfft)
         {
             build_mel_tables(T, mp, nfft);
-            build_entries(T, a.numFilter, a.normalize, rowStart, ent);
+            build_sweep(T, a.numFilter, a.normalize, weights, intervals, groups, reinterpret_cast<int*>(smem + lay.cum));
         }
         const int t0 = tile * kTile;
         const int zc = int(min((long long)frames + 8, (long long)a.dstHStride));
@@ -137,37 +173,67 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
         const int k0 = range[0], k1 = range[1];
         if (ok && tv > 0)
         {
-            // stage spectrum rows [k0, k1) x frames [t0, t0 + tv)
+            // stage spectrum rows [k0, k1) x frames [t0, t0 + tv): 8 loads per thread in flight
             const float* x = a.src + size_t(b) * a.srcNStride + t0;
-            for (int idx = threadIdx.x; idx < (k1 - k0) * kTile; idx += kThreads)
+            const int count = (k1 - k0) * kTile;
+            constexpr int kBatch = 8;
+            for (int i0 = threadIdx.x; i0 < count; i0 += kBatch * kThreads)
             {
-                const int r = idx / kTile, c = idx % kTile;
-                if (c < tv) s_spec[r * kLd + c] = __ldg(x + size_t(k0 + r) * a.srcHStride + c);
+                float v[kBatch];
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j)
+                {
+                    const int idx = i0 + j * kThreads, r = idx / kTile, c = idx % kTile;
+                    v[j] = (idx < count && c < tv) ? __ldg(x + size_t(k0 + r) * a.srcHStride + c) : 0.0f;
+                }
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j)
+                {
+                    const int idx = i0 + j * kThreads, r = idx / kTile, c = idx % kTile;
+                    if (idx < count) s_spec[r * kLd + c] = v[j];
+                }
             }
         }
         __syncthreads();
+        // one sweep over the group's intervals for frames t0 + t and t0 + t + 1; each power pair is
+        // read once.  Columns at or past `frames` (below zc) get zeros.
         const int col = t0 + t;
         if (col < zc)
         {
-            const bool live = ok && col < frames;
-            const float* sp = s_spec + t;
-            float* yp = a.dst + size_t(b) * a.dstNStride + size_t(g) * a.dstHStride + col;
-            const size_t ystep = size_t(kGroups) * a.dstHStride;
-            for (int m = g; m < a.numFilter; m += kGroups, yp += ystep)
+            const bool live0 = ok && col < frames, live1 = ok && col + 1 < frames, has1 = col + 1 < zc;
+            const int m0 = ok ? groups[g] : 0, m1 = ok ? groups[g + 1] : 0;
+            float* yp = a.dst + size_t(b) * a.dstNStride + size_t(m0) * a.dstHStride + col;
+            float2 fall = make_float2(0.f, 0.f);   // filter i - 1: rising sum, then falling terms
+            for (int i = m0; i <= m1 && ok; ++i)
             {
-                float acc = 0.0f;
-                if (live)
+                const int2 iv = intervals[i];
+                const float* sp = s_spec + (iv.x - k0) * kLd + t;
+                float2 rise = make_float2(0.f, 0.f);   // filter i
+#pragma unroll 2
+                for (int k = iv.x; k < iv.y; ++k, sp += kLd)
                 {
-                    const int e1 = rowStart[m + 1];
-#pragma unroll 4
-                    for (int e = rowStart[m]; e < e1; ++e)
-                    {
-                        const int2 en = ent[e];
-                        acc = __fadd_rn(acc, __fmul_rn(sp[en.x], __int_as_float(en.y)));
-                    }
+                    const float2 pw = *reinterpret_cast<const float2*>(sp);
+                    const float2 w = weights[k];
+                    fall.x = __fadd_rn(fall.x, __fmul_rn(pw.x, w.y));
+                    fall.y = __fadd_rn(fall.y, __fmul_rn(pw.y, w.y));
+                    rise.x = __fadd_rn(rise.x, __fmul_rn(pw.x, w.x));
+                    rise.y = __fadd_rn(rise.y, __fmul_rn(pw.y, w.x));
                 }
-                *yp = acc;
+                if (i > m0)
+                {
+                    yp[0] = live0 ? fall.x : 0.0f;
+                    if (has1) yp[1] = live1 ? fall.y : 0.0f;
+                    yp += a.dstHStride;
+                }
+                fall = rise;
             }
+            if (!ok)   // no tables for this sample: zeros, as the reference leaves its output
+                for (int m = g; m < a.numFilter; m += kGroups)
+                {
+                    float* z = a.dst + size_t(b) * a.dstNStride + size_t(m) * a.dstHStride + col;
+                    z[0] = 0.0f;
+                    if (has1) z[1] = 0.0f;
+                }
         }
         __syncthreads();   // the next unit restages the tile and may rebuild the tables
     }
