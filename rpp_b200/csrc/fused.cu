@@ -435,13 +435,12 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         }
         else if (threadIdx.x == 32 && it.kind == 0)
         {
-            // the barrier orders every thread's mel stores before this thread's device-scope
-            // fence, which orders them before the count (the grid-barrier release pattern)
+            // the barrier orders every thread's mel stores before this thread's release, which
+            // orders them (and the maximum) before the count
             float v = s_warpMax[0];
             for (int i = 1; i < kFusedThreads / 32; ++i) v = fmaxf(v, s_warpMax[i]);
             atomicMax(maxKey + b, float_key(v));
-            __threadfence();
-            atomicAdd(done + b, 1);
+            asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(done + b) : "memory");
         }
         cur ^= 1;
         __syncthreads();
