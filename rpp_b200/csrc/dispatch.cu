@@ -962,7 +962,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_normalize_gpu(RppPtr_t srcPtr, RpptGener
             s.normFactor = float(1.0 / double(s.count));
             if (compute)
             {
-                if (s.count >= 544)   // normalize.cu kWarpMinElems
+                if (s.count >= kNormalizeWarpMinElems)
                     for (int p = 0; p < params; ++p) tasks.push_back(make_int4(b, p, 1, 1));
                 else
                     for (int p = 0; p < params; p += 32) tasks.push_back(make_int4(b, p, std::min(32, params - p), 0));

@@ -27,9 +27,9 @@ namespace rppb {
 namespace {
 
 constexpr int kThreads = 256;
-// warp-parallel tree from this reduction length on: every node of the top five levels then holds
-// at least floor(n / 16) >= 34 > 32 elements, so it splits as the lanes assume
-constexpr int kWarpMinElems = 544;
+// warp-parallel tree from kNormalizeWarpMinElems (544) elements on: every node of the top five
+// levels then holds at least floor(n / 16) >= 34 > 32 elements, so it splits as the lanes assume
+static_assert(kNormalizeWarpMinElems / 16 > 32, "the warp tree's top five levels must all split");
 constexpr int kStageElems = 1024;   // per warp: 4 KB of shared memory
 
 // The reference's compute_sum / compute_diff_square_sum value (the "+= into 0" steps are exact:
@@ -59,7 +59,7 @@ __device__ float tree_sum(const float* in, int stride, int n, float mean)
     return t;
 }
 
-// Same value, the 32 subtrees five levels down summed by the 32 lanes (n >= kWarpMinElems).
+// Same value, the 32 subtrees five levels down summed by the 32 lanes (n >= kNormalizeWarpMinElems).
 template <bool kSq>
 __device__ float warp_tree_sum(const float* in, int stride, int n, float mean)
 {

@@ -158,6 +158,9 @@ struct SliceArgs
 void launch_slice(Handle& h, const SliceArgs& a, const void* src, void* dst, const void* fill);
 
 // normalize (normalize.cu): 2-D F32, per-sample roi lengths.
+// Reductions of at least this many elements run one warp per parameter (normalize.cu).
+constexpr int kNormalizeWarpMinElems = 544;
+
 struct NormalizeSample
 {
     int len0, len1;          // roi lengths (rows, columns)

@@ -437,7 +437,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_server_create(rppbServer_t* server, cons
         s->arena = new Arena(c.budgetBytes);
         check_cuda(cudaMalloc(&s->lut, size_t(c.lookupSize) * 4), "cudaMalloc(lut)");
         check_cuda(cudaMemcpy(s->lut, c.lookup, size_t(c.lookupSize) * 4, cudaMemcpyHostToDevice), "cudaMemcpy(lut)");
-        if (rppCreate(&s->handle, size_t(c.maxClipsPerStep), 0, s->compute, RPP_HIP_BACKEND) != RPP_SUCCESS)
+        if (rppCreate(&s->handle, size_t(c.maxClipsPerStep), 0, s->compute, RPP_HIP_BACKEND) != rppStatusSuccess)
             fail(RPP_ERROR, "rppCreate failed");
         const size_t tableBytes = sizeof(RppbClip) * c.maxClipsPerStep;
         for (int t = 0; t < c.tables; ++t)
