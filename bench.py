@@ -25,7 +25,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from rpp_b200 import synth  # noqa: E402
+from rpp_b200 import replicas, synth  # noqa: E402
 from rpp_b200.types import RpptLayout, audio_desc, spectra_desc  # noqa: E402
 
 METRIC = "clip-sec/s for preemph→STFT→mel→dB at stated err vs FP64; p50/p99 serve latency"
@@ -121,10 +121,7 @@ class ClockSampler:
 # ---------------------------------------------------------------- distributed plumbing
 
 def dist_init():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return replicas.env()
 
 
 # ---------------------------------------------------------------- the reference arm
@@ -634,10 +631,7 @@ def read_traffic(kernel):
 def run_b200(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    replicas.init("nccl")
     from rpp_b200 import lib
     L_ = lib.load()
     L_.rppbGetLaunchCount.restype = ctypes.c_longlong
@@ -651,8 +645,7 @@ def run_b200(args, world, rank, local):
 
     def barrier():
         torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
 
     fused = Fused(torch, h, chain)
@@ -680,9 +673,7 @@ def run_b200(args, world, rank, local):
                 fn(x)
         end.record()
         barrier()
-        t = torch.tensor([start.elapsed_time(end)], device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t = replicas.max_over_ranks(start.elapsed_time(end), "cuda")
         ops = None
         if per_op:
             ops = np.zeros(4)
@@ -690,7 +681,7 @@ def run_b200(args, world, rank, local):
                 for o in range(4):
                     ops[o] += evs[k][o].elapsed_time(evs[k][o + 1])
             ops /= steps
-        return float(t.item()) / steps, ops
+        return t / steps, ops
 
     # ---- device-resident throughput: plain four-call chain, then the fused call (the headline)
     for _ in range(max(args.warmup, 3)):
@@ -704,8 +695,8 @@ def run_b200(args, world, rank, local):
     ms_step, _ = timed(fused.run, args.steps)
     launches = L_.rppbGetLaunchCount() - launches0
     clocks = sampler.stop() if sampler else None
-    value = world * clip_s / (ms_step / 1e3)
-    plain_value = world * clip_s / (plain_ms / 1e3)
+    value = replicas.job_throughput(clip_s, ms_step, world)
+    plain_value = replicas.job_throughput(clip_s, plain_ms, world)
 
     # ---- end to end through the C ABI with host buffers.  Headline: rppb_frontend_host_gpu on pinned
     # host tensors (valid samples in, valid decibel rows out, chunked so copies overlap the kernels).
@@ -730,10 +721,7 @@ def run_b200(args, world, rank, local):
             fn()
         en.record()
         barrier()
-        tt = torch.tensor([st.elapsed_time(en)], device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        return float(tt.item()) / steps
+        return replicas.max_over_ranks(st.elapsed_time(en), "cuda") / steps
 
     e_steps = max(3, args.steps // 2)
     e2e_ms = timed_host(e2e_step, e_steps)
@@ -747,11 +735,11 @@ def run_b200(args, world, rank, local):
         out_host.copy_(fused.run(x_dev), non_blocking=True)
 
     full_ms = timed_host(e2e_full_step, e_steps)
-    e2e = {"value": world * clip_s / (e2e_ms / 1e3), "unit": "clip-s/s", "h2d_bytes_per_step": h2d,
+    e2e = {"value": replicas.job_throughput(clip_s, e2e_ms, world), "unit": "clip-s/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
            "path": "pinned host tensors -> rppb_frontend_host_gpu (C ABI): valid samples copied in, valid decibel "
                    "rows copied out, %s chunks overlapping copy-in / kernels / copy-out" % (args.chunks or 8),
-           "whole_tensor_copies": {"value": world * clip_s / (full_ms / 1e3), "ms_per_step": full_ms,
+           "whole_tensor_copies": {"value": replicas.job_throughput(clip_s, full_ms, world), "ms_per_step": full_ms,
                                    "h2d_bytes_per_step": int(x_host.numel() * 4),
                                    "d2h_bytes_per_step": int(out_host.numel() * 4),
                                    "path": "padded host tensors copied whole around rppb_frontend_gpu, one stream"}}
@@ -826,8 +814,7 @@ def run_b200(args, world, rank, local):
         }
         print(json.dumps(line), flush=True)
     h.close()
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finish()
 
 
 def main():
