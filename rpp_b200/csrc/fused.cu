@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                         const int2 iv = melIv[i];
                         const float* sp = s_out + iv.x * LD + f;
                         float2 rise = make_float2(0.f, 0.f);   // filter i
-#pragma unroll 2
+#pragma unroll 1
                         for (int k = iv.x; k < iv.y; ++k, sp += LD)
                         {
                             const float2 pw = *reinterpret_cast<const float2*>(sp);

@@ -173,26 +173,26 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
         const int k0 = range[0], k1 = range[1];
         if (ok && tv > 0)
         {
-            // stage spectrum rows [k0, k1) x frames [t0, t0 + tv): 8 loads per thread in flight
-            const float* x = a.src + size_t(b) * a.srcNStride + t0;
-            const int count = (k1 - k0) * kTile;
-            constexpr int kBatch = 8;
-            for (int i0 = threadIdx.x; i0 < count; i0 += kBatch * kThreads)
+            // stage spectrum rows [k0, k1) x frames [t0, t0 + tv) (zeros past tv): lane = frame
+            // column, warp w takes rows w, w + kWarps, ...; both pointers advance by a fixed row step
+            // and kBatch loads per thread are in flight before their stores
+            static_assert(kTile == 32, "one warp per staged row");
+            constexpr int kWarps = kThreads / 32, kBatch = 8;
+            const int lane = threadIdx.x & 31, rows = k1 - k0;
+            const bool colOk = lane < tv;
+            const size_t rowStep = size_t(kWarps) * a.srcHStride;
+            int r = threadIdx.x >> 5;
+            const float* xs = a.src + size_t(b) * a.srcNStride + t0 + size_t(k0 + r) * a.srcHStride + lane;
+            float* ss = s_spec + r * kLd + lane;
+            for (; r + (kBatch - 1) * kWarps < rows; r += kBatch * kWarps)
             {
                 float v[kBatch];
 #pragma unroll
-                for (int j = 0; j < kBatch; ++j)
-                {
-                    const int idx = i0 + j * kThreads, r = idx / kTile, c = idx % kTile;
-                    v[j] = (idx < count && c < tv) ? __ldg(x + size_t(k0 + r) * a.srcHStride + c) : 0.0f;
-                }
+                for (int j = 0; j < kBatch; ++j, xs += rowStep) v[j] = colOk ? __ldg(xs) : 0.0f;
 #pragma unroll
-                for (int j = 0; j < kBatch; ++j)
-                {
-                    const int idx = i0 + j * kThreads, r = idx / kTile, c = idx % kTile;
-                    if (idx < count) s_spec[r * kLd + c] = v[j];
-                }
+                for (int j = 0; j < kBatch; ++j, ss += kWarps * kLd) *ss = v[j];
             }
+            for (; r < rows; r += kWarps, xs += rowStep, ss += kWarps * kLd) *ss = colOk ? __ldg(xs) : 0.0f;
         }
         __syncthreads();
         // one sweep over the group's intervals for frames t0 + t and t0 + t + 1; each power pair is
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
                 const int2 iv = intervals[i];
                 const float* sp = s_spec + (iv.x - k0) * kLd + t;
                 float2 rise = make_float2(0.f, 0.f);   // filter i
-#pragma unroll 2
+#pragma unroll 1
                 for (int k = iv.x; k < iv.y; ++k, sp += kLd)
                 {
                     const float2 pw = *reinterpret_cast<const float2*>(sp);
