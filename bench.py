@@ -32,7 +32,7 @@ METRIC = "clip-sec/s for preemph→STFT→mel→dB at stated err vs FP64; p50/p9
 RATE = 16000
 NFFT, WIN, HOP, NMEL = 512, 400, 160, 128
 COEFF, CUTOFF_DB, MULT = 0.97, -80.0, 10.0
-WORKLOAD = ("configs[1]: 256 mono f32 clips @16 kHz, lengths U[1 s, 16 s] with silent gaps; "
+WORKLOAD = ("256 mono f32 clips @16 kHz, lengths U[1 s, 16 s] with silent gaps; "
             "pre_emphasis(0.97, ZERO) -> spectrogram(nfft 512, win 400, hop 160, Hann, centred, reflect, power 2, NFT) "
             "-> mel_filter_bank(128, 0-8 kHz, Slaney, normalized) -> to_decibels(x10, -80 dB, ref = per-clip max)")
 
@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--clips", type=int, default=256)
     p.add_argument("--tune", type=int, default=1, help="autotune the fused call's schedule first (0: defaults)")
     p.add_argument("--chunks", type=int, default=0, help="chunks of the host-tensor call (0: library default)")
-    p.add_argument("--precision", type=int, default=1, help="run the configs[2] precision study (0: skip)")
+    p.add_argument("--precision", type=int, default=1, help="run the precision study on 1024 x 10 s clips (0: skip)")
     p.add_argument("--serve-requests", type=int, default=600,
                    help="requests per offered-load point of the serving measurement (0 skips it)")
     return p.parse_args()
@@ -133,7 +133,7 @@ def run_reference(args, world, rank):
     from rpp_b200.types import RpptImagePatch
     threads = os.cpu_count() or 1
     ref = Reference(threads=threads)
-    x, lens = synth.config1(n=args.clips)
+    x, lens = synth.gapped_clips(n=args.clips)
     n, L = x.shape
     F = frames_of(lens)
     mf = int(F.max())
@@ -167,7 +167,7 @@ def run_reference(args, world, rank):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "clip-s/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": med * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, configs[1] signal model)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; 3 tones + Gaussian noise, silent gaps)",
         "config": {"workload": WORKLOAD, "clips": n, "clip_seconds": clip_s},
         "cpu_baseline": {"value": value, "unit": "clip-s/s", "cores": threads, "kind": "reference",
                          "sample": f"the full {n}-clip batch per step, median of {args.steps} steps"},
@@ -315,7 +315,7 @@ def error_vs_fp64(chain, x_np, lens_np, clips=8, db_out=None):
 
 
 def serving_measurement(torch, n_requests):
-    """configs[4]: continuous-batching server (rpp_b200/serving.py) over a 40 GB device budget;
+    """Serving: continuous-batching server (rpp_b200/serving.py) over a 40 GB device budget;
     capacity from a closed burst, then open-loop Poisson arrivals at 10-90 % of it."""
     from rpp_b200 import serving
     rng = np.random.Generator(np.random.PCG64(20261203 + 4))
@@ -339,7 +339,7 @@ def serving_measurement(torch, n_requests):
 
 
 def multirate_measurement(torch, h, steps=10, n=2048):
-    """2048 stereo clips, durations log-normal (median 4 s, sigma 0.25, 0.5-30 s), input
+    """Multi-rate chain: 2048 stereo clips, durations log-normal (median 4 s, sigma 0.25, 0.5-30 s), input
     rates {16, 22.05, 44.1, 48} kHz -> rppb_downmix_resample_gpu (Kaiser-windowed sinc, 16 zero
     crossings, beta 8) -> rppb_frontend_gpu (nfft 512, win 400, hop 160, 80 mel) in one CUDA graph.
     The signal model (3 shared sines + independent noise per channel) is synthesized on the GPU from a
@@ -429,15 +429,15 @@ def multirate_measurement(torch, h, steps=10, n=2048):
         h.set_stream(torch.cuda.current_stream().cuda_stream)
     clip_s = float((lens / rates).sum())
     in_bytes = float((8 * lens.astype(np.int64)).sum())
-    return {"workload": "configs[3]: 2048 stereo clips, log-normal 4 s median, rates {16k,22.05k,44.1k,48k}; "
+    return {"workload": "2048 stereo clips, log-normal 4 s median, rates {16k,22.05k,44.1k,48k}; "
                         "downmix+resample(Kaiser beta 8, 16 zero crossings) -> fused pre-emphasis/STFT(512)/mel(80)/dB",
             "clip_seconds": clip_s, "ms_per_batch": ms, "clip_s_per_s": clip_s / (ms / 1e3),
             "split_ms": {"downmix_resample": float(split[0]), "frontend": float(split[1])},
             "input_bytes": in_bytes, "graph": "both calls captured in one CUDA graph (4 kernels + 1 memset)"}
 
 
-def gpu_config2(torch, n, length, seed=20261203 + 2):
-    """configs[2]-shaped batch synthesized on the GPU for timing: 3 tones per clip plus white noise
+def gpu_dynamic_range_clips(torch, n, length, seed=20261203 + 2):
+    """The precision study's batch (1024 x 10 s) synthesized on the GPU for timing: 3 tones per clip plus white noise
     40 + 20 * (i % 5) dB below the tones' peak (the host generator needs ~20 s for 1024 x 10 s)."""
     dev = torch.device("cuda")
     g = torch.Generator(device=dev)
@@ -459,7 +459,7 @@ def gpu_config2(torch, n, length, seed=20261203 + 2):
 
 
 def precision_measurement(torch, h, check_clips=20, n=1024, length=160000, reps=5):
-    """precision study of the spectrogram (and the mel/dB chain after it) in FP32 (the
+    """Precision study of the spectrogram (and the mel/dB chain after it) in FP32 (the
     register-FFT path) and on tensor cores (DFT-as-GEMM with BF16, BF16 hi/lo x3, TF32, FP8 E4M3 with
     per-frame scaling; FP32 accumulation).  nfft 512 and 1024, window = nfft (Hann), hop = nfft / 4,
     pre-emphasis 0.97.  Errors: on the first `check_clips` clips of the seeded host batch (two per
@@ -470,11 +470,11 @@ def precision_measurement(torch, h, check_clips=20, n=1024, length=160000, reps=
     from oracle import Oracle
     from rpp_b200 import audio
     orc = Oracle()
-    xs, ls, floors = synth.config2(n=check_clips, length=length)
+    xs, ls, floors = synth.dynamic_range_clips(n=check_clips, length=length)
     xs_d = torch.from_numpy(xs).cuda()
     ls_d = torch.from_numpy(ls).cuda()
     cs_d = torch.full((check_clips,), COEFF, device="cuda")
-    xf = gpu_config2(torch, n, length)
+    xf = gpu_dynamic_range_clips(torch, n, length)
     lf = torch.full((n,), length, dtype=torch.int32, device="cuda")
     cf = torch.full((n,), COEFF, device="cuda")
     tc_modes = {"tc_bf16": audio.TC_BF16, "tc_bf16_hilo3": audio.TC_BF16_HILO3, "tc_tf32": audio.TC_TF32,
@@ -483,7 +483,7 @@ def precision_measurement(torch, h, check_clips=20, n=1024, length=160000, reps=
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.isfile(pk):
         peaks = json.load(open(pk))
-    result = {"workload": "configs[2]: 1024 clips x 10 s @16 kHz, 3 tones + white noise 40/60/80/100/120 dB below "
+    result = {"workload": "1024 clips x 10 s @16 kHz, 3 tones + white noise 40/60/80/100/120 dB below "
                           "the tones' peak; pre-emphasis 0.97 -> spectrogram (Hann, window = nfft, hop = nfft/4, "
                           "centred, reflect, power 2) -> mel(128, Slaney, normalized) -> dB(x10, -80 dB)",
               "error_clips": check_clips, "dynamic_ranges_db": [float(f) for f in floors[:5]],
@@ -635,7 +635,7 @@ def run_b200(args, world, rank, local):
     from rpp_b200 import lib
     L_ = lib.load()
     L_.rppbGetLaunchCount.restype = ctypes.c_longlong
-    x_np, lens_np = synth.config1(n=args.clips)
+    x_np, lens_np = synth.gapped_clips(n=args.clips)
     n, L = x_np.shape
     clip_s = float(lens_np.sum()) / RATE
     stream = torch.cuda.current_stream()
@@ -788,7 +788,7 @@ def run_b200(args, world, rank, local):
         line = {
             "metric": METRIC, "value": value, "unit": "clip-s/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, configs[1] signal model)",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; 3 tones + Gaussian noise, silent gaps)",
             "config": {"workload": WORKLOAD,
                        "path": "fused: one rppb_frontend_gpu call per step (pre-emphasis, STFT, mel, dB in one "
                                "persistent launch); bit-identical to the four rppt_*_gpu calls",

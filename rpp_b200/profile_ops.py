@@ -1,5 +1,5 @@
-"""Runs every entry point of the audio path once on the configs[1] batch (256 ragged 16 kHz clips,
-1-16 s) and the first 256 clips of configs[3] (stereo, mixed rates), for kernel profiling:
+"""Runs every entry point of the audio path once on the 256-clip batch (ragged 16 kHz clips,
+1-16 s) and the first 256 clips of the stereo multi-rate batch (mixed rates), for kernel profiling:
 
     python -m rpp_b200.profile_ops [--clips N] [--repeat R]
 
@@ -26,7 +26,7 @@ def main():
     L_ = lib.load()
     dev = torch.device("cuda")
     h = lib.Handle(batch_size=args.clips, stream=torch.cuda.current_stream().cuda_stream)
-    x_np, lens_np = synth.config1(n=args.clips)
+    x_np, lens_np = synth.gapped_clips(n=args.clips)
     n, L = x_np.shape
     x = torch.from_numpy(x_np).to(dev)
     lens = torch.from_numpy(lens_np).to(dev)
@@ -45,8 +45,8 @@ def main():
     length = torch.empty(n, dtype=torch.int32, device=dev)
     p = frontend_params()
 
-    # configs[3] subset: stereo at mixed rates
-    xs_np, ls_np, rates_np = synth.config3(n=args.clips)
+    # stereo multi-rate subset
+    xs_np, ls_np, rates_np = synth.stereo_multirate_clips(n=args.clips)
     Ls = int(ls_np.max())
     xs = torch.from_numpy(xs_np).to(dev)
     sdims = torch.from_numpy(np.stack([ls_np, np.full(args.clips, 2, np.int32)], 1).astype(np.int32)).to(dev)

@@ -151,7 +151,7 @@ class FrontendServer:
 
 def make_request(torch, rid, rng, max_clips=8, rates=(16000.0, 44100.0, 48000.0), median_s=2.0, sigma=0.6,
                  max_s=30.0, num_filter=128):
-    """configs[4] request: 1..max_clips mono clips, durations log-normal (median 2 s, sigma 0.6,
+    """One serving request: 1..max_clips mono clips, durations log-normal (median 2 s, sigma 0.6,
     clipped to 0.1..max_s s), rates uniform over `rates`, same signal model as the other configs."""
     from . import synth
     k = int(rng.integers(1, max_clips + 1))

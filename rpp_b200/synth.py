@@ -1,17 +1,18 @@
 """Seeded synthetic audio batches with the shapes and value distributions of the benchmark
-configurations (no datasets are available offline).  NumPy PCG64, seed 20261203 + config index.
+workloads (no datasets are available offline).  NumPy PCG64; each batch kind has its own seed.
 
-  cfg0  8 mono clips, 16 kHz, lengths U[16000, 60000]
-  cfg1  256 mono clips, 16 kHz, lengths U[16000, 256000] (1-16 s), plus 0-3 silent spans of
-        0.1-1 s per clip
-  cfg2  1024 mono clips of 160000 samples; the white noise sits 40/60/80/100/120 dB below the
-        tones' peak (clip i: 40 + 20 * (i % 5) dB) instead of at sigma 0.1, sweeping the dynamic range
-  cfg3  2048 stereo clips, durations log-normal (median 4 s, sigma 0.25) clipped to 0.5-30 s, input
-        rate uniform over {16000, 22050, 44100, 48000}; both channels share the sines and have
-        independent noise
+  short_clips            8 mono clips, 16 kHz, lengths U[16000, 60000] (seed 20261203)
+  gapped_clips           256 mono clips, 16 kHz, lengths U[16000, 256000] (1-16 s), plus 0-3 silent
+                         spans of 0.1-1 s per clip (seed 20261204)
+  dynamic_range_clips    1024 mono clips of 160000 samples; the white noise sits 40/60/80/100/120 dB
+                         below the tones' peak (clip i: 40 + 20 * (i % 5) dB) instead of at sigma 0.1,
+                         sweeping the dynamic range (seed 20261205)
+  stereo_multirate_clips 2048 stereo clips, durations log-normal (median 4 s, sigma 0.25) clipped to
+                         0.5-30 s, input rate uniform over {16000, 22050, 44100, 48000}; both channels
+                         share the sines and have independent noise (seed 20261206)
 
-Signal model (cfg0, cfg1, cfg3): Gaussian noise sigma 0.1 plus 3 sinusoids with frequency U[100, 6000]
-Hz and amplitude U[0.05, 0.5].
+Signal model (all but dynamic_range_clips): Gaussian noise sigma 0.1 plus 3 sinusoids with
+frequency U[100, 6000] Hz and amplitude U[0.05, 0.5].
 """
 import numpy as np
 
@@ -53,25 +54,25 @@ def mono_batch(n, lengths, rng, rate=16000, gaps=False, floor_db=None):
     return out, lengths
 
 
-def config0(n=8):
+def short_clips(n=8):
     rng = np.random.Generator(np.random.PCG64(SEED + 0))
     lengths = rng.integers(16000, 60001, n)
     return mono_batch(n, lengths, rng)
 
 
-def config1(n=256, max_len=256000):
+def gapped_clips(n=256, max_len=256000):
     rng = np.random.Generator(np.random.PCG64(SEED + 1))
     lengths = rng.integers(16000, max_len + 1, n)
     return mono_batch(n, lengths, rng, gaps=True)
 
 
-def config2(n=1024, length=160000):
+def dynamic_range_clips(n=1024, length=160000):
     rng = np.random.Generator(np.random.PCG64(SEED + 2))
     floors = np.array([40, 60, 80, 100, 120], np.float64)[np.arange(n) % 5]
     return mono_batch(n, np.full(n, length), rng, floor_db=floors) + (floors,)
 
 
-def config3(n=2048):
+def stereo_multirate_clips(n=2048):
     """Returns (float32 [n][maxLen*2] interleaved stereo, int32 lengths, float32 in rates)."""
     rng = np.random.Generator(np.random.PCG64(SEED + 3))
     dur = np.clip(rng.lognormal(np.log(4.0), 0.25, n), 0.5, 30.0)

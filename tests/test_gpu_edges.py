@@ -1,4 +1,4 @@
-"""Edge cases across the entry points: empty batches, and the full configs[1] batch checked through
+"""Edge cases across the entry points: empty batches, and the full 256-clip batch checked through
 properties that hold at any size (fused == plain chain bit for bit; decibels within [cutoff, 0]
 with ~0 dB reached at each clip's maximum)."""
 import numpy as np
@@ -44,12 +44,12 @@ def test_empty_batch_every_entry_point(gpu):
 
 @pytest.fixture(scope="module")
 def full_batch():
-    x, lens = synth.config1(n=256)
+    x, lens = synth.gapped_clips(n=256)
     return x, lens
 
 
 def test_full_size_fused_equals_plain(gpu, full_batch):
-    """configs[1] at full size (256 clips, 1-16 s): the fused call and the four plain calls give the same
+    """The 256-clip batch at full size (1-16 s): the fused call and the four plain calls give the same
     bits over every valid decibel, compared on the device."""
     x, lens = full_batch
     n, L = x.shape

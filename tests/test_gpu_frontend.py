@@ -81,7 +81,7 @@ def test_frontend_vs_fp64_oracle(gpu, oracle):
     host path included (up to 1.9e-3 dB on this input), loses accuracy in bins far below the frame's
     largest, so the bound is 1e-3 dB where the mel power is within 60 dB of its frame's maximum and
     1e-2 dB everywhere else above the cutoff."""
-    x, lens = synth.config1(n=12, max_len=64000)
+    x, lens = synth.gapped_clips(n=12, max_len=64000)
     n, L = x.shape
     coeff = np.full(n, 0.97, np.float32)
     p = frontend_params()
@@ -106,7 +106,7 @@ def test_frontend_vs_fp64_oracle(gpu, oracle):
 def test_frontend_graph_capture(gpu):
     """After one uncaptured call sized the workspace, the fused call captures into a CUDA graph
     and replays to the same result."""
-    x, lens = synth.config1(n=16, max_len=48000)
+    x, lens = synth.gapped_clips(n=16, max_len=48000)
     n, L = x.shape
     p = frontend_params()
     mf = 48000 // 160 + 1
@@ -168,7 +168,7 @@ SCHEDULES = [dict(tile_frames=32), dict(tile_frames=64, db_frames=16), dict(db_f
 def test_frontend_schedule_knobs_are_bit_identical(gpu, sched):
     """Tile frames, decibel item frames, lookahead and CTAs per SM move work between CTAs and in
     time only: every schedule writes exactly the default schedule's bits."""
-    x, lens = synth.config1(n=20, max_len=64000)
+    x, lens = synth.gapped_clips(n=20, max_len=64000)
     n, L = x.shape
     mf = 64000 // 160 + 1
     xd, ld, cd = dev(x), dev(lens), dev(np.full(n, 0.97, np.float32))
@@ -184,7 +184,7 @@ def test_frontend_schedule_knobs_are_bit_identical(gpu, sched):
 def test_frontend_tune(gpu):
     """The autotuner picks a valid schedule, leaves the result unchanged, and answers a repeated
     shape from its cache."""
-    x, lens = synth.config1(n=32, max_len=96000)
+    x, lens = synth.gapped_clips(n=32, max_len=96000)
     n, L = x.shape
     mf = 96000 // 160 + 1
     xd, ld, cd = dev(x), dev(lens), dev(np.full(n, 0.97, np.float32))

@@ -551,7 +551,7 @@ def test_normalize_vs_oracle(gpu, oracle, cols, axis_mask, compute):
 def test_normalize_frontend_output(gpu, oracle):
     """The RNN-T-style step: per-filter normalisation over time of the fused front end's decibels."""
     from rpp_b200.types import generic_desc, frontend_params
-    x, lens = synth.config1(n=6, max_len=48000)
+    x, lens = synth.gapped_clips(n=6, max_len=48000)
     n, L = x.shape
     mf = 48000 // 160 + 1
     db = torch.zeros((n, 128, mf), device="cuda")

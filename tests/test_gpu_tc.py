@@ -67,7 +67,7 @@ def test_tc_spectrogram_vs_fp64(gpu, oracle, ci, precision):
 
 def test_tc_spectrogram_many_tiles(gpu, oracle):
     """Clips long enough for several 128-frame tiles per clip and more work items than SMs."""
-    x, lens = synth.config1(n=24, max_len=160000)
+    x, lens = synth.gapped_clips(n=24, max_len=160000)
     n, L = x.shape
     coeff = np.full(n, 0.97, np.float32)
     c = dict(CASES[0])
@@ -103,7 +103,7 @@ def test_tc_mel_vs_fp32(gpu, precision, nmel, htk, normalize):
     """rppb_mel_filter_bank_tc_gpu against the FP32 mel_filter_bank (bit-exact to the reference) on
     the same spectrum: per-frame relative error within the operand precision's bound; only the
     valid frames are written."""
-    x, lens = synth.config1(n=10, max_len=80000)
+    x, lens = synth.gapped_clips(n=10, max_len=80000)
     n, L = x.shape
     F = (lens // 160 + 1).astype(np.int32)
     mf = int(F.max())
