@@ -423,8 +423,12 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
             }
         }
         __syncthreads();
-        // between the two barriers, in parallel: warp 0 claims and decodes the item after next;
-        // warp 1 publishes a finished spectrum item
+        // after the item's last barrier, in parallel with the other warps starting the next item:
+        // warp 0 claims and decodes the item after next into the slot just read (no thread reads
+        // that slot again before the next item's end barrier); warp 1 publishes a finished
+        // spectrum item.  No second barrier: the next item was decoded one item earlier, and the
+        // shared values written here (s_it[cur]) or read here (s_warpMax) are next touched by the
+        // other threads only after a later barrier that warps 0 and 1 also reach.
         if (threadIdx.x == 0)
         {
             const long long w = wAfter;
@@ -443,7 +447,6 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
             asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(done + b) : "memory");
         }
         cur ^= 1;
-        __syncthreads();
     }
 }
 
