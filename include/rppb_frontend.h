@@ -177,6 +177,14 @@ SHARED_PUBLIC RppStatus rppb_mel_filter_bank_tc_gpu(RppPtr_t srcPtr, RpptDescPtr
  * Synchronizes the handle stream. */
 SHARED_PUBLIC RppStatus rppb_get_device_error(rppHandle_t rppHandle, Rpp32s* errorCode);
 
+/* Failure-detection test hook; no counterpart in the reference.  While enabled, every decibel item
+ * of the fused front end (rppb_frontend_gpu, rppb_frontend_host_gpu, rppb_frontend_clips_gpu) waits
+ * for one spectrum tile more than its clip has, a count that nothing reaches, and gives up after
+ * ~1024 polls (about 0.1 ms) instead of a few seconds: the kernel sets the device error word, leaves
+ * that item's mel power unconverted and finishes, so the context stays usable.  Lets a test check the
+ * timeout path without a fault or a hang.  Off by default; affects only this handle. */
+SHARED_PUBLIC RppStatus rppb_set_wait_fault_injection(rppHandle_t rppHandle, bool enable);
+
 #ifdef __cplusplus
 }
 #endif

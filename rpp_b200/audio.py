@@ -184,6 +184,13 @@ def device_error(handle):
     return v.value
 
 
+def set_wait_fault_injection(handle, enable):
+    """rppb_set_wait_fault_injection (test hook): the fused front end's decibel items wait for a tile
+    that is never counted and give up after ~0.1 ms, setting the device error word."""
+    L = _lib.load()
+    return _status(L.rppb_set_wait_fault_injection(_h(handle), bool(enable)))
+
+
 def downmix_resample(src, src_desc, dst, dst_desc, in_rate, out_rate, src_dims, normalize_weights, lut, scale, center,
                      lobes, handle):
     """rppb_downmix_resample_gpu: down-mix to mono and resample in one launch."""

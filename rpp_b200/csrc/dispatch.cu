@@ -738,6 +738,14 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips
     });
 }
 
+extern "C" SHARED_PUBLIC RppStatus rppb_set_wait_fault_injection(rppHandle_t rppHandle, bool enable)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        h.set_wait_injection(enable);
+        return RPP_SUCCESS;
+    });
+}
+
 extern "C" SHARED_PUBLIC RppStatus rppb_get_device_error(rppHandle_t rppHandle, Rpp32s* errorCode)
 {
     return guarded(rppHandle, [&](Handle& h) {

@@ -36,6 +36,7 @@ constexpr int kDbFramesDefault = 128;         // frames per decibel item unless 
 constexpr int kSubTilesDefault = 2;           // spectrum tiles per spectrum item unless tuned
 constexpr int kFusedPrefixCache = 320;        // slots cached in shared memory (n + lookahead + 1)
 constexpr long long kWaitLimit = 1ll << 24;   // x ~128 ns sleeps: a few seconds
+constexpr long long kInjectedWaitLimit = 1024; // wait fault injection: ~0.1 ms per decibel item
 
 namespace {
 
@@ -366,11 +367,12 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         {
             if (threadIdx.x == 0)
             {
-                const int need = cnt.tiles(b);
+                const int need = cnt.tiles(b) + a.waitExtra;
+                const long long limit = a.waitLimit > 0 ? a.waitLimit : kWaitLimit;
                 long long spins = 0;
                 while (atomicAdd(done + b, 0) < need)
                 {
-                    if (++spins > kWaitLimit)
+                    if (++spins > limit)
                     {
                         atomicOr(errorWord, 1);
                         break;
@@ -378,7 +380,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                     __nanosleep(128);
                 }
                 __threadfence();
-                s_ok = spins <= kWaitLimit;
+                s_ok = spins <= limit;
             }
             __syncthreads();
             if (s_ok)
@@ -515,6 +517,9 @@ void launch_frontend(Handle& h, void* scratch, const FrontendArgs& args)
     if (a.dbFrames < 16 || a.dbFrames > kFusedThreads || (a.dbFrames & (a.dbFrames - 1)))
         fail(RPP_ERROR_NOT_IMPLEMENTED, "dbFrames must be 0 or a power of two from 16 to 256");
     if (a.ctasPerSm < 0) fail(RPP_ERROR_INVALID_ARGUMENTS, "ctasPerSm must not be negative");
+    // wait fault injection (test only): every decibel item waits for a tile that is never counted
+    a.waitExtra = h.wait_injection() ? 1 : 0;
+    a.waitLimit = h.wait_injection() ? kInjectedWaitLimit : 0;
     switch (a.nfft)
     {
         case 128: launch_nfft<128>(h, a, scratch); return;

@@ -91,6 +91,10 @@ class Handle
 
     // A small zeroed device word array that kernels set on bounded-wait timeouts.
     int* device_flags();
+    // Test setting (rppb_set_wait_fault_injection): the fused front end's decibel items wait for one
+    // spectrum tile more than their clip has, with a short poll limit, so the wait runs out.
+    void set_wait_injection(bool on) { wait_injection_ = on; }
+    bool wait_injection() const { return wait_injection_; }
 
     // Extra streams of this handle (created on first use, non-blocking), for copies that overlap
     // the kernels on stream(); every call that uses them joins them back into stream() before it
@@ -125,6 +129,7 @@ class Handle
 
     std::map<std::string, void*> tables_;
     int* flags_ = nullptr;
+    bool wait_injection_ = false;
 
     rppAllocatorFunction alloc_fn_ = nullptr;
     rppDeallocatorFunction free_fn_ = nullptr;

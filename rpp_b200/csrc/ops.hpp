@@ -139,6 +139,10 @@ struct FrontendArgs
     // 4 tiles), frames per decibel item (0: 128), CTAs per SM (0: as many as fit)
     int tileFrames, dbFrames, ctasPerSm;
     int subTiles;            // set by launch_frontend: tiles per spectrum item
+    // set by launch_frontend from the handle's wait fault injection (test only): tiles a decibel
+    // item waits for beyond its clip's, and the poll limit of that wait (0: the default)
+    int waitExtra;
+    long long waitLimit;
 };
 size_t frontend_scratch_bytes(int n, int lookahead);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);

@@ -17,7 +17,7 @@ EXPORTED = (
     "rppSetAllocator", "rppGetKernelTime", "rppEnableProfiling",
     "rppt_non_silent_region_detection_gpu", "rppt_to_decibels_gpu", "rppt_pre_emphasis_filter_gpu",
     "rppt_down_mixing_gpu", "rppt_spectrogram_gpu", "rppt_mel_filter_bank_gpu", "rppt_resample_gpu",
-    "rppbGetLastError", "rppbGetLaunchCount", "rppb_frontend_gpu", "rppb_get_device_error",
+    "rppbGetLastError", "rppbGetLaunchCount", "rppb_frontend_gpu", "rppb_get_device_error", "rppb_set_wait_fault_injection",
     "rppb_downmix_resample_gpu", "rppt_to_decibels_gpu_static", "rppb_frontend_clips_gpu",
     "rppb_spectrogram_tc_gpu",
     "rppb_frontend_host_gpu", "rppb_frontend_tune_gpu",
@@ -105,6 +105,8 @@ def load(path=None):
     L.rppb_server_arena_used.restype = ctypes.c_uint64
     L.rppb_get_device_error.argtypes = [_V, ctypes.POINTER(ctypes.c_int32)]
     L.rppb_get_device_error.restype = _I
+    L.rppb_set_wait_fault_injection.argtypes = [_V, _B]
+    L.rppb_set_wait_fault_injection.restype = _I
     L.rppbGetLaunchCount.argtypes = []
     L.rppbGetLaunchCount.restype = ctypes.c_longlong
     L.rppbGetLastError.argtypes = []

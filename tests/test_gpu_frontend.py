@@ -206,3 +206,48 @@ def test_frontend_tune(gpu):
     out2 = canvas((n, 128, mf))
     assert audio.frontend(xd, sd, out2, dd, ld, cd, q, gpu) == OK
     np.testing.assert_array_equal(host(out2), host(ref))
+
+
+def test_frontend_wait_timeout_reports_device_error():
+    """Failure detection without a fault or a hang.  With the wait fault injection on, every decibel
+    item of the fused kernel waits for a spectrum tile that is never counted; its bounded wait gives
+    up (~1024 polls), sets the device error word, leaves the item's mel power unconverted, and the
+    launch ends.  The host reads the error, and the same handle, injection off, then computes the
+    batch exactly as before."""
+    from rpp_b200 import lib
+    h = lib.Handle(batch_size=1, stream=torch.cuda.current_stream().cuda_stream)
+    try:
+        x, lens = synth.gapped_clips(n=6, max_len=32000)
+        n, L = x.shape
+        coeff = np.full(n, 0.97, np.float32)
+        p = frontend_params()
+        F = (lens // 160 + 1).astype(np.int32)
+        mf = int(F.max())
+        args = (dev(x), audio_desc(n, L))
+        rest = (spectra_desc(n, 128, mf), dev(lens), dev(coeff), p, h)
+        ref = canvas((n, 128, mf))
+        assert audio.frontend(*args, ref, *rest) == OK
+        assert audio.device_error(h) == 0
+        r = host(ref)
+
+        assert audio.set_wait_fault_injection(h, True) == OK
+        try:
+            out = canvas((n, 128, mf))
+            assert audio.frontend(*args, out, *rest) == OK
+            assert audio.device_error(h) == 1
+        finally:
+            assert audio.set_wait_fault_injection(h, False) == OK
+        o = host(out)
+        for i in range(n):
+            # decibels are <= 0 (reference = the clip's maximum); the skipped items hold mel power >= 0
+            assert (r[i, :, :F[i]] <= 0).all()
+            assert (o[i, :, :F[i]] >= 0).all()
+            assert (o[i, :, F[i]:] == -12345.0).all()
+
+        again = canvas((n, 128, mf))
+        assert audio.frontend(*args, again, *rest) == OK
+        assert audio.device_error(h) == 0
+        np.testing.assert_array_equal(host(again), r)
+    finally:
+        torch.cuda.synchronize()
+        h.close()
