@@ -274,10 +274,11 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
 
     // Thread 0 keeps two items decoded ahead in a two-entry ring (the claim's and the decode's
     // latencies overlap the current item) and asks L2 for each decoded spectrum item's input span
-    // one item before it is staged.  A CTA's current item always has a lower index than the ones
-    // it holds claimed, so the lowest unfinished item is always some CTA's current one, whose
-    // decibel wait (on lower spectrum items only) ends: claiming ahead keeps the waits
-    // deadlock-free.
+    // one item before it is staged; in the last 2 x grid items of the queue it reserves nothing
+    // beyond the next item and claims each one when it decodes it.  A CTA's current item always has
+    // a lower index than the ones it holds claimed, so the lowest unfinished item is always some
+    // CTA's current one, whose decibel wait (on lower spectrum items only) ends: claiming ahead
+    // keeps the waits deadlock-free.
     __shared__ Item s_it[2];
     __shared__ int s_ok;
     const int itemFrames = TF * a.subTiles;
@@ -288,13 +289,13 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         const long long s1 = min((long long)n.L, (long long)last * a.hop - centerOffset + a.W);
         l2_prefetch(n.x + s0, n.x + s1);
     };
-    long long wAfter = 0;   // thread 0: the claimed item two after the current one
+    long long wAfter = 0;   // thread 0: the claimed item two after the current one (-1: none reserved)
     int cur = 0;
     if (threadIdx.x == 0)
     {
         const long long w0 = (long long)atomicAdd(workCounter, 1ull);
         const long long w1 = (long long)atomicAdd(workCounter, 1ull);
-        wAfter = (long long)atomicAdd(workCounter, 1ull);
+        wAfter = w1 < total - 2ll * gridDim.x ? (long long)atomicAdd(workCounter, 1ull) : -1ll;
         s_it[0] = decode_item<TF>(a, cnt, prefix, nslots, total, w0);
         s_it[1] = decode_item<TF>(a, cnt, prefix, nslots, total, w1);
         prefetch_span(s_it[1]);
@@ -433,8 +434,10 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         // other threads only after a later barrier that warps 0 and 1 also reach.
         if (threadIdx.x == 0)
         {
-            const long long w = wAfter;
-            if (w < total) wAfter = (long long)atomicAdd(workCounter, 1ull);
+            // the last 2 x grid items are claimed when needed, not reserved ahead, so that no CTA
+            // holds work that an idle one could start (small batches: 0.039 -> 0.033 ms for one 1 s clip)
+            const long long w = wAfter >= 0 ? wAfter : (long long)atomicAdd(workCounter, 1ull);
+            wAfter = w < total - 2ll * gridDim.x ? (long long)atomicAdd(workCounter, 1ull) : -1ll;
             const Item nx = decode_item<TF>(a, cnt, prefix, nslots, total, w);
             prefetch_span(nx);
             s_it[cur] = nx;
