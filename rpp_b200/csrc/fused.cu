@@ -405,8 +405,8 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 const int kDbGroups = kFusedThreads / a.dbFrames;
                 if (fd < it.Tv)
                 {
-                    // 8 rows per step: the loads (mostly L2 hits) are in flight together
-                    constexpr int kRows = 8;
+                    // 16 rows per step: the loads (mostly L2 hits) are in flight together (8: 1 % slower)
+                    constexpr int kRows = 16;
                     const size_t step = size_t(kDbGroups) * hs;
                     float* p = it.y + size_t(gd) * hs + fd;
                     int m = gd;
