@@ -22,6 +22,7 @@
 #include <cfloat>
 
 #include <algorithm>
+#include <cstring>
 #include <string>
 
 #include "common.cuh"
@@ -156,15 +157,122 @@ struct FusedLayout
     }
 };
 
+// The fused kernel's mel tables in its shared-memory layout, built by the whole CTA in the work region
+// (free until the first FFT); ends with __syncthreads.
+    // ---- mel weights by bin.  Bin k of interval i (between mel points i and i + 1) weighs
+    //      (1 - wd_k) * norm_i into filter i and wd_k * norm_(i-1) into filter i - 1, so filter m
+    //      sums interval m's bins, then interval m + 1's, in ascending bin order -- the order and
+    //      the weights of the mel_filter_bank kernel.  The tables are built in the work region
+    //      before it holds FFT data.
+template <int NFFT, int TFX>
+__device__ __forceinline__ void build_fused_mel(const FrontendArgs& a, unsigned char* smem,
+                                                const FusedLayout<NFFT, TFX>& lay)
+{
+    using S = StftShape<NFFT, kFusedThreads, TFX>;
+    constexpr int TF = S::TF, BINS = S::BINS;
+    constexpr int kGroups = 2 * kFusedThreads / TF;   // mel thread groups: TF / 2 frame pairs each
+    const int nmel = a.mel.numFilter;
+    float* s_out = reinterpret_cast<float*>(smem + lay.work + S::fft_bytes);
+    float2* melW = reinterpret_cast<float2*>(smem + lay.melW);   // bin k: (weight into filter i, into filter i - 1)
+    int2* melIv = reinterpret_cast<int2*>(smem + lay.melIv);     // interval i: bins [x, y)
+    int* melGrp = reinterpret_cast<int*>(smem + lay.melGrp);     // thread group g: filters [g], [g + 1])
+    unsigned char* t = smem + lay.work;
+    MelTableView v;
+    v.first = reinterpret_cast<int*>(t);
+    v.last = v.first + (nmel + 2);
+    v.norm = reinterpret_cast<float*>(v.last + (nmel + 2));
+    size_t o = (size_t(reinterpret_cast<unsigned char*>(v.norm + nmel) - t) + 7) & ~size_t(7);
+    v.f0 = reinterpret_cast<double*>(t + o);
+    v.f1 = v.f0 + (nmel + 1);
+    v.weightsDown = reinterpret_cast<float*>(v.f1 + (nmel + 1));
+    v.range = reinterpret_cast<int*>(v.weightsDown + BINS);
+    build_mel_tables(v, a.mel, NFFT);   // ends with __syncthreads
+    for (int i = threadIdx.x; i <= nmel; i += kFusedThreads)
+    {
+        const int k0 = v.first[i], k1 = v.last[i];
+        melIv[i] = k1 > k0 ? make_int2(k0, k1) : make_int2(0, 0);
+        for (int k = k0; k < k1; ++k)
+        {
+            const float wd = v.weightsDown[k];
+            float rise = 0.f, fall = 0.f;
+            if (i < nmel)
+            {
+                rise = __fsub_rn(1.0f, wd);
+                if (a.mel.normalize) rise = __fmul_rn(rise, v.norm[i]);
+            }
+            if (i > 0) fall = a.mel.normalize ? __fmul_rn(wd, v.norm[i - 1]) : wd;
+            melW[k] = make_float2(rise, fall);
+        }
+    }
+    // group g emits filters [melGrp[g], melGrp[g + 1]) and sweeps their intervals; the groups'
+    // shares of (bins + 2) per interval are balanced.  cum[i] = cost of intervals 0..i (an
+    // inclusive scan by warp 0, in the power tile's space, which is free until the first FFT);
+    // boundary g is 1 + the first filter m whose intervals 0..m+1 reach g / kGroups of the total.
+    int* cum = reinterpret_cast<int*>(s_out);
+    for (int i = threadIdx.x; i <= nmel; i += kFusedThreads)
+        cum[i] = (v.last[i] > v.first[i] ? v.last[i] - v.first[i] : 0) + 2;
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        const int lane = threadIdx.x, chunk = (nmel + 1 + 31) / 32;
+        const int i0 = min(lane * chunk, nmel + 1), i1 = min(i0 + chunk, nmel + 1);
+        int sum = 0;
+        for (int i = i0; i < i1; ++i) sum += cum[i];
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        int run = incl - sum;
+        for (int i = i0; i < i1; ++i)
+        {
+            run += cum[i];
+            cum[i] = run;
+        }
+    }
+    __syncthreads();
+    const int totalCost = cum[nmel];
+    for (int grp = threadIdx.x; grp <= kGroups; grp += kFusedThreads)
+    {
+        int lo = 0, hi = nmel;   // first m in [0, nmel) with cum[m + 1] * kGroups >= grp * total, else nmel
+        if (grp == 0) hi = -1;
+        else
+            while (lo < hi)
+            {
+                const int mid = (lo + hi) >> 1;
+                if (cum[mid + 1] * kGroups >= grp * totalCost) hi = mid;
+                else lo = mid + 1;
+            }
+        melGrp[grp] = grp == 0 ? 0 : grp == kGroups ? nmel : min(lo + 1, nmel);
+    }
+    __syncthreads();
+}
+
+// Builds the fused kernel's mel tables once, with one CTA, into `out`: the bytes [melW, total) of its
+// shared-memory layout (melW, melIv, melGrp), which every launch with the same mel parameters and tile
+// copies instead of building them in each CTA.
+template <int NFFT, int TFX>
+__global__ void __launch_bounds__(kFusedThreads) fused_mel_tables_kernel(FrontendArgs a, uint4* __restrict__ out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const FusedLayout<NFFT, TFX> lay(a.mel.numFilter, a.W, a.hop);
+    build_fused_mel<NFFT, TFX>(a, smem, lay);
+    const uint4* src = reinterpret_cast<const uint4*>(smem + lay.melW);
+    for (int i = threadIdx.x; i < int((lay.total - lay.melW) / 16); i += kFusedThreads) out[i] = src[i];
+}
+
 template <int NFFT, int TFX>
 __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend_kernel(FrontendArgs a, const float2* __restrict__ twiddle,
                                                                  const long long* __restrict__ prefix,
                                                                  unsigned long long* __restrict__ workCounter,
                                                                  int* __restrict__ done, unsigned* __restrict__ maxKey,
-                                                                 int* __restrict__ errorWord)
+                                                                 int* __restrict__ errorWord,
+                                                                 const uint4* __restrict__ melTables)
 {
     using S = StftShape<NFFT, kFusedThreads, TFX>;
-    constexpr int TF = S::TF, BINS = S::BINS, LD = S::OUT_LD;
+    constexpr int TF = S::TF, LD = S::OUT_LD;
     extern __shared__ __align__(16) unsigned char smem[];
     const FusedLayout<NFFT, TFX> lay(a.mel.numFilter, a.W, a.hop);
     float2* s_tw = reinterpret_cast<float2*>(smem + lay.tw);
@@ -187,86 +295,15 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     {
         stft_tables<NFFT, kFusedThreads>(twiddle, a.window, a.W, s_tw, s_tw1, s_win, s_span);
 
-        // ---- mel weights by bin.  Bin k of interval i (between mel points i and i + 1) weighs
-        //      (1 - wd_k) * norm_i into filter i and wd_k * norm_(i-1) into filter i - 1, so filter m
-        //      sums interval m's bins, then interval m + 1's, in ascending bin order -- the order and
-        //      the weights of the mel_filter_bank kernel.  The tables are built in the work region
-        //      before it holds FFT data.
-        constexpr int kGroups = 2 * kFusedThreads / TF;   // mel thread groups: TF / 2 frame pairs each
+        // the mel tables: copied from the handle's cache when the launch has them, else built here
+        if (melTables)
         {
-            unsigned char* t = smem + lay.work;
-            MelTableView v;
-            v.first = reinterpret_cast<int*>(t);
-            v.last = v.first + (nmel + 2);
-            v.norm = reinterpret_cast<float*>(v.last + (nmel + 2));
-            size_t o = (size_t(reinterpret_cast<unsigned char*>(v.norm + nmel) - t) + 7) & ~size_t(7);
-            v.f0 = reinterpret_cast<double*>(t + o);
-            v.f1 = v.f0 + (nmel + 1);
-            v.weightsDown = reinterpret_cast<float*>(v.f1 + (nmel + 1));
-            v.range = reinterpret_cast<int*>(v.weightsDown + BINS);
-            build_mel_tables(v, a.mel, NFFT);   // ends with __syncthreads
-            for (int i = threadIdx.x; i <= nmel; i += kFusedThreads)
-            {
-                const int k0 = v.first[i], k1 = v.last[i];
-                melIv[i] = k1 > k0 ? make_int2(k0, k1) : make_int2(0, 0);
-                for (int k = k0; k < k1; ++k)
-                {
-                    const float wd = v.weightsDown[k];
-                    float rise = 0.f, fall = 0.f;
-                    if (i < nmel)
-                    {
-                        rise = __fsub_rn(1.0f, wd);
-                        if (a.mel.normalize) rise = __fmul_rn(rise, v.norm[i]);
-                    }
-                    if (i > 0) fall = a.mel.normalize ? __fmul_rn(wd, v.norm[i - 1]) : wd;
-                    melW[k] = make_float2(rise, fall);
-                }
-            }
-            // group g emits filters [melGrp[g], melGrp[g + 1]) and sweeps their intervals; the groups'
-            // shares of (bins + 2) per interval are balanced.  cum[i] = cost of intervals 0..i (an
-            // inclusive scan by warp 0, in the power tile's space, which is free until the first FFT);
-            // boundary g is 1 + the first filter m whose intervals 0..m+1 reach g / kGroups of the total.
-            int* cum = reinterpret_cast<int*>(s_out);
-            for (int i = threadIdx.x; i <= nmel; i += kFusedThreads)
-                cum[i] = (v.last[i] > v.first[i] ? v.last[i] - v.first[i] : 0) + 2;
-            __syncthreads();
-            if (threadIdx.x < 32)
-            {
-                const int lane = threadIdx.x, chunk = (nmel + 1 + 31) / 32;
-                const int i0 = min(lane * chunk, nmel + 1), i1 = min(i0 + chunk, nmel + 1);
-                int sum = 0;
-                for (int i = i0; i < i1; ++i) sum += cum[i];
-                int incl = sum;
-    #pragma unroll
-                for (int o = 1; o < 32; o <<= 1)
-                {
-                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += t;
-                }
-                int run = incl - sum;
-                for (int i = i0; i < i1; ++i)
-                {
-                    run += cum[i];
-                    cum[i] = run;
-                }
-            }
-            __syncthreads();
-            const int totalCost = cum[nmel];
-            for (int grp = threadIdx.x; grp <= kGroups; grp += kFusedThreads)
-            {
-                int lo = 0, hi = nmel;   // first m in [0, nmel) with cum[m + 1] * kGroups >= grp * total, else nmel
-                if (grp == 0) hi = -1;
-                else
-                    while (lo < hi)
-                    {
-                        const int mid = (lo + hi) >> 1;
-                        if (cum[mid + 1] * kGroups >= grp * totalCost) hi = mid;
-                        else lo = mid + 1;
-                    }
-                melGrp[grp] = grp == 0 ? 0 : grp == kGroups ? nmel : min(lo + 1, nmel);
-            }
+            uint4* t = reinterpret_cast<uint4*>(smem + lay.melW);
+            for (int i = threadIdx.x; i < int((lay.total - lay.melW) / 16); i += kFusedThreads) t[i] = __ldg(melTables + i);
             __syncthreads();
         }
+        else
+            build_fused_mel<NFFT, TFX>(a, smem, lay);
     }
 
     const int centerOffset = a.center ? a.W / 2 : 0;
@@ -472,13 +509,38 @@ void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
     unsigned long long* counter = cv.take<unsigned long long>(1);
     int* done = cv.take<int>(a.n);
     unsigned* maxKey = cv.take<unsigned>(a.n);
+    const FusedLayout<NFFT, TFX> lay(a.mel.numFilter, a.W, a.hop);
+    if (lay.total > 227 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
+    const float2* tw = spectrogram_twiddles(h, NFFT);
+    // the mel tables, built once per handle, mel parameters and tile (not while the stream is being
+    // captured: then each CTA builds them).  Launched before the prefix kernel: the fused kernel reads
+    // them before its grid-dependency wait, which orders it only after the kernel just before it.
+    uint4* melTables = nullptr;
+    {
+        auto bits = [](float v) {
+            uint32_t u;
+            std::memcpy(&u, &v, sizeof u);
+            return std::to_string(u);
+        };
+        const std::string key = "fusedmel:" + std::to_string(NFFT) + ":" + std::to_string(TFX) + ":" +
+                                std::to_string(a.mel.numFilter) + ":" + bits(a.mel.minFreq) + ":" +
+                                bits(a.mel.maxFreq) + ":" + bits(a.mel.sampleRate) + ":" + std::to_string(a.mel.htk) +
+                                ":" + std::to_string(int(a.mel.normalize));
+        bool fresh = false;
+        melTables = static_cast<uint4*>(h.device_table(key, lay.total - lay.melW, &fresh));
+        if (fresh)
+        {
+            const void* tk = reinterpret_cast<const void*>(fused_mel_tables_kernel<NFFT, TFX>);
+            persistent_grid(h, tk, kFusedThreads, lay.total);   // sets the kernel's shared-memory opt-in
+            fused_mel_tables_kernel<NFFT, TFX><<<1, kFusedThreads, lay.total, h.stream()>>>(a, melTables);
+            count_launch();
+            check_cuda(cudaGetLastError(), "fused_mel_tables_kernel");
+        }
+    }
     // the prefix kernel also zeroes the queue counter, the tile counts and the maxima
     const size_t clear = reinterpret_cast<char*>(maxKey + a.n) - reinterpret_cast<char*>(counter);
     launch_ragged_prefix(SlotCount<S::TF>{a, a.n, a.lookahead}, nslots, prefix, h.stream(),
                          reinterpret_cast<unsigned*>(counter), int(clear / 4));
-    const FusedLayout<NFFT, TFX> lay(a.mel.numFilter, a.W, a.hop);
-    if (lay.total > 227 * 1024) fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "numFilter too large for the fused tile");
-    const float2* tw = spectrogram_twiddles(h, NFFT);
     int grid = persistent_grid(h, reinterpret_cast<const void*>(frontend_kernel<NFFT, TFX>), kFusedThreads, lay.total);
     if (a.ctasPerSm > 0) grid = std::min(grid, a.ctasPerSm * h.num_sms());
     if (a.reserveSms > 0 && a.reserveSms < h.num_sms())
@@ -486,7 +548,7 @@ void launch_fused(Handle& h, const FrontendArgs& a, void* scratch)
     // starts while the prefix kernel runs: the tables are built before grid_dependency_wait()
     launch_dependent(frontend_kernel<NFFT, TFX>, dim3(grid), dim3(kFusedThreads), lay.total, h.stream(),
                      "frontend_kernel", a, tw, static_cast<const long long*>(prefix), counter, done, maxKey,
-                     h.device_flags());
+                     h.device_flags(), static_cast<const uint4*>(melTables));
     count_launch();
 }
 

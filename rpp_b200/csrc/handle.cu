@@ -192,6 +192,21 @@ const float* Handle::table(const std::string& key, size_t count, void (*build)(f
     return static_cast<const float*>(d);
 }
 
+void* Handle::device_table(const std::string& key, size_t bytes, bool* fresh)
+{
+    *fresh = false;
+    auto it = tables_.find(key);
+    if (it != tables_.end()) return it->second;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    check_cuda(cudaStreamIsCapturing(stream_, &cap), "cudaStreamIsCapturing");
+    if (cap != cudaStreamCaptureStatusNone) return nullptr;
+    void* d = nullptr;
+    check_cuda(cudaMalloc(&d, bytes), "cudaMalloc(device table)");
+    tables_[key] = d;
+    *fresh = true;
+    return d;
+}
+
 int* Handle::device_flags()
 {
     if (!flags_)

@@ -78,6 +78,11 @@ class Handle
     // fills `host` once; the table is uploaded and kept until the handle is destroyed.
     const float* table(const std::string& key, size_t count, void (*build)(float*, size_t, const void*),
                        const void* ctx);
+    // Cached device buffer of `bytes` for tables that a kernel builds: returns the buffer for `key`
+    // and sets *fresh when it was just allocated (the caller then fills it on stream() before any
+    // use).  While stream() is being captured a missing key returns nullptr (nothing is allocated
+    // during capture) and the caller builds the tables some other way.
+    void* device_table(const std::string& key, size_t bytes, bool* fresh);
     // Uploads `bytes` of host data to a device region that stays valid for this call.
     void upload(void* dDst, const void* hSrc, size_t bytes);
 

@@ -131,6 +131,47 @@ def test_frontend_graph_capture(gpu):
         gpu.set_stream(torch.cuda.current_stream().cuda_stream)
 
 
+def test_frontend_capture_builds_uncached_tables():
+    """The fused kernel's mel tables are cached per handle and mel parameters by the first uncaptured
+    call.  A call captured with parameters not cached yet (here 80 filters, after a 128-filter call
+    sized the workspace of a fresh handle) builds them in every CTA instead; both ways give the same
+    bits."""
+    from rpp_b200 import lib
+    h = lib.Handle(batch_size=1, stream=torch.cuda.current_stream().cuda_stream)
+    g = None
+    try:
+        x, lens = synth.gapped_clips(n=12, max_len=48000)
+        n, L = x.shape
+        mf = 48000 // 160 + 1
+        xd, ld, cd = dev(x), dev(lens), dev(np.full(n, 0.97, np.float32))
+        sd = audio_desc(n, L)
+        out128 = canvas((n, 128, mf))
+        assert audio.frontend(xd, sd, out128, spectra_desc(n, 128, mf), ld, cd, frontend_params(), h) == OK
+        p80 = frontend_params(num_filter=80)
+        d80 = spectra_desc(n, 80, mf)
+        out80 = canvas((n, 80, mf))
+        s = torch.cuda.Stream()
+        g = torch.cuda.CUDAGraph()
+        h.set_stream(s.cuda_stream)
+        with torch.cuda.stream(s):
+            torch.cuda.synchronize()
+            with torch.cuda.graph(g, stream=s):
+                assert audio.frontend(xd, sd, out80, d80, ld, cd, p80, h) == OK
+        g.replay()
+        torch.cuda.synchronize()
+        h.set_stream(torch.cuda.current_stream().cuda_stream)
+        captured = host(out80).copy()
+        # the same call uncaptured now builds and caches the 80-filter tables
+        out80.fill_(-12345.0)
+        assert audio.frontend(xd, sd, out80, d80, ld, cd, p80, h) == OK
+        np.testing.assert_array_equal(captured, host(out80))
+        assert audio.device_error(h) == 0
+    finally:
+        torch.cuda.synchronize()
+        del g
+        h.close()
+
+
 @pytest.mark.parametrize("chunks,pinned_io", [(0, True), (1, True), (3, True), (50, True), (4, False)])
 def test_frontend_host_equals_device(gpu, chunks, pinned_io):
     """rppb_frontend_host_gpu (host tensors, chunked copy/compute overlap) writes exactly what
