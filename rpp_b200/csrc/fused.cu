@@ -158,12 +158,10 @@ struct FusedLayout
 };
 
 // The fused kernel's mel tables in its shared-memory layout, built by the whole CTA in the work region
-// (free until the first FFT); ends with __syncthreads.
-    // ---- mel weights by bin.  Bin k of interval i (between mel points i and i + 1) weighs
-    //      (1 - wd_k) * norm_i into filter i and wd_k * norm_(i-1) into filter i - 1, so filter m
-    //      sums interval m's bins, then interval m + 1's, in ascending bin order -- the order and
-    //      the weights of the mel_filter_bank kernel.  The tables are built in the work region
-    //      before it holds FFT data.
+// (free until the first FFT); ends with __syncthreads.  Mel weights by bin: bin k of interval i (between
+// mel points i and i + 1) weighs (1 - wd_k) * norm_i into filter i and wd_k * norm_(i-1) into filter
+// i - 1, so filter m sums interval m's bins, then interval m + 1's, in ascending bin order -- the order
+// and the weights of the mel_filter_bank kernel.
 template <int NFFT, int TFX>
 __device__ __forceinline__ void build_fused_mel(const FrontendArgs& a, unsigned char* smem,
                                                 const FusedLayout<NFFT, TFX>& lay)
