@@ -107,3 +107,20 @@ def test_header_layout_matches_reference():
     ours = _probe([INCLUDE])
     theirs = _probe([gen, os.path.join(REF, "api")], extra=["-mavx2", "-mf16c"])
     assert ours == theirs
+
+
+def test_headers_compile_as_c():
+    """Every public header compiles in a C translation unit (gnu11, as gcc builds C by default), so
+    C callers and FFI bindings generated from the headers can include them; the C++-only
+    RpptResamplingWindow is hidden from C by the headers themselves."""
+    import shutil
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc absent")
+    headers = sorted(f for f in os.listdir(INCLUDE) if f.endswith(".h"))
+    src = "".join(f'#include "{h}"\n' for h in headers) + "int main(void) { return sizeof(RpptDesc) == 0; }\n"
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "c_headers.c")
+        open(path, "w").write(src)
+        r = subprocess.run(["gcc", "-std=gnu11", "-Wall", "-Wextra", "-Werror", f"-I{INCLUDE}", "-fsyntax-only", path],
+                           capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
