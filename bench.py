@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--tune", type=int, default=1, help="autotune the fused call's schedule first (0: defaults)")
     p.add_argument("--chunks", type=int, default=0, help="chunks of the host-tensor call (0: library default)")
     p.add_argument("--precision", type=int, default=1, help="run the precision study on 1024 x 10 s clips (0: skip)")
+    p.add_argument("--profile", action="store_true", help="run each entry point once for ncu captures, then exit")
+    p.add_argument("--profile-repeat", type=int, default=1)
+    p.add_argument("--profile-only", default="", help="with --profile: only entry points whose name contains this")
     p.add_argument("--serve-requests", type=int, default=600,
                    help="requests per offered-load point of the serving measurement (0 skips it)")
     return p.parse_args()
@@ -210,8 +213,10 @@ def cpu_baseline_sample(x, lens, sample_clips=256, repeats=5):
             times.append(time.perf_counter() - t0)
     ref.close()
     clip_s = float(lens.sum()) / RATE
-    return {"value": clip_s / statistics.median(times), "unit": "clip-s/s", "cores": threads, "kind": "reference",
+    info = {"value": clip_s / statistics.median(times), "unit": "clip-s/s", "cores": threads, "kind": "reference",
             "sample": f"{n} clips ({clip_s:.0f} clip-s) of the same batch, median of {repeats} runs"}
+    # the reference's outputs of the last run: the parity leg compares the GPU results with them
+    return info, {"pre": pre, "spec": spec, "mel": mel, "db": db, "frames": F}
 
 
 # ---------------------------------------------------------------- the B200 arm
@@ -613,9 +618,10 @@ def precision_measurement(torch, h, check_clips=20, n=1024, length=160000, reps=
     return result
 
 
-def read_traffic(kernel):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+def read_traffic(kernel, name="dram_traffic.txt"):
+    """Per-launch figure of `kernel` from a committed ncu summary table (profiles/dram_traffic.txt:
+    DRAM read + write bytes; profiles/issue_counts.txt: warp instructions), if present."""
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.isfile(path):
         return None
     for line in open(path):
@@ -626,6 +632,61 @@ def read_traffic(kernel):
             except ValueError:
                 return None
     return None
+
+
+def nsr_measurement(torch, h, x, lens_np, steps=10):
+    """rppt_non_silent_region_detection_gpu on the raw benchmark clips (-60 dB, window 2048, reset 8192):
+    device time (CUDA events, median of `steps`) and the detected (begin, length) per clip."""
+    from rpp_b200 import audio
+    n, L = x.shape
+    lens = torch.from_numpy(lens_np).cuda()
+    begin = torch.empty(n, dtype=torch.int32, device="cuda")
+    length = torch.empty(n, dtype=torch.int32, device="cuda")
+    sd = audio_desc(n, L)
+
+    def call():
+        assert audio.non_silent_region_detection(x, sd, lens, begin, length, -60.0, 2048, 0.0, 8192, h) == 0
+
+    for _ in range(3):
+        call()
+    times = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        call()
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = float(np.median(times))
+    clip_s = float(lens_np.sum()) / RATE
+    return {"ms": ms, "clip_s_per_s": clip_s / (ms / 1e3), "cut_off_db": -60.0, "window": 2048,
+            "reset_interval": 8192, "input_bytes": int(4 * lens_np.astype(np.int64).sum())}, \
+        begin.cpu().numpy(), length.cpu().numpy()
+
+
+def parity_vs_reference(chain, fused, refo, lens_np, x_np, nsr_out):
+    """The GPU results on the full batch against the reference host library's own outputs (the last
+    run of the CPU-baseline leg): the plain chain op by op, the fused call's decibels, and NSR begin/length
+    against rppt_non_silent_region_detection_host on the raw clips."""
+    from oracle import Reference, parity
+    res = {"reference": "oracle/_ref/librpp_audio_ref.so (the reference's rppt_*_host, built from its sources)",
+           "bars": {"pre_emphasis": "bit-exact", "spectrogram_mel": "|err| / frame max <= 1e-5",
+                    "db": "<= 1e-3 dB (stated: overall, and within 60 dB of the frame maximum)",
+                    "nsr": "bit-exact"}}
+    res["plain_chain"] = parity.chain_parity(refo, pre=chain.pre.cpu().numpy(), spec=chain.spec.cpu().numpy(),
+                                             mel=chain.mel.cpu().numpy(), db=chain.db.cpu().numpy(), lens=lens_np)
+    res["fused"] = parity.chain_parity(refo, db=fused.out.cpu().numpy())
+    if nsr_out is not None:
+        ref = Reference(threads=os.cpu_count() or 1)
+        try:
+            rb, rl = parity.reference_nsr(ref, x_np, lens_np, -60.0, 2048, 0.0, 8192)
+        finally:
+            ref.close()
+        gb, gl = nsr_out
+        mism = int(((gb != rb) | (gl != rl)).sum())
+        res["nsr"] = {"clips": int(len(rb)), "mismatches": mism, "bit_exact": mism == 0,
+                      "max_resets_crossed": int(lens_np.max()) // 8192}
+    return res
 
 
 def run_b200(args, world, rank, local):
@@ -759,10 +820,25 @@ def run_b200(args, world, rank, local):
                   for i, o in enumerate(ops)}
         L64 = lens_np.astype(np.int64)
         F64 = L64 // HOP + 1
-        fused_bytes = int((4 * L64 + 3 * 4 * NMEL * F64).sum())
+        # compulsory bytes of the fused call: each input sample read once, each decibel value written once
+        fused_bytes = int((4 * L64 + 4 * NMEL * F64).sum())
         fused_gbs = fused_bytes / (ms_step / 1e3) / 1e9
         traffic = read_traffic("frontend_kernel<512>")
+        # issue roofline: warp instructions of one launch (ncu) against 4 issue slots per SM per clock
+        inst = read_traffic("frontend_kernel<512>", "issue_counts.txt")
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        clk = (clocks or {}).get("sm_mhz") or peaks.get("sm_max_mhz") or 1965.0
+        issue = None
+        if inst:
+            floor_ms = inst / (sms * 4 * clk * 1e6) * 1e3
+            issue = {"warp_instructions_per_launch": inst, "sms": sms, "sm_mhz": clk,
+                     "issue_floor_ms": floor_ms, "issue_frac": floor_ms / ms_step,
+                     "source": "profiles/issue_counts.txt (ncu smsp__inst_executed.sum of one launch)"}
         err = error_vs_fp64(chain, x_np, lens_np, db_out=fused.out)
+        try:
+            nsr, nsr_b, nsr_l = nsr_measurement(torch, h, x, lens_np)
+        except Exception as exc:
+            nsr, nsr_b, nsr_l = {"error": repr(exc)}, None, None
         try:
             multirate = multirate_measurement(torch, h)
         except Exception as exc:
@@ -780,10 +856,21 @@ def run_b200(args, world, rank, local):
             except Exception as exc:   # report, do not lose the main line
                 serve = {"error": repr(exc)}
         try:
-            cpu = cpu_baseline_sample(x_np, lens_np)
+            cpu, refo = cpu_baseline_sample(x_np, lens_np)
         except Exception as exc:  # the reference host library is optional on a box without it
-            cpu = {"value": None, "unit": "clip-s/s", "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"unavailable: {exc}"}
+            cpu, refo = {"value": None, "unit": "clip-s/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"unavailable: {exc}"}, None
+        parity_ref = None
+        if refo is not None:
+            try:
+                chain.run(x)
+                fused.run(x)
+                torch.cuda.synchronize()
+                parity_ref = parity_vs_reference(chain, fused, refo, lens_np, x_np,
+                                                 (nsr_b, nsr_l) if nsr_b is not None else None)
+            except Exception as exc:
+                parity_ref = {"error": repr(exc)}
+            del refo
         total_bytes = sum(ab.values())
         line = {
             "metric": METRIC, "value": value, "unit": "clip-s/s", "n_gpus": world, "steps": args.steps,
@@ -797,13 +884,18 @@ def run_b200(args, world, rank, local):
             "roofline": {"bound": "hbm", "kernel": "frontend_kernel<512> (rppb_frontend_gpu)", "achieved": fused_gbs,
                          "peak": hbm, "unit": "GB/s", "frac": fused_gbs / hbm, "peak_source": peak_src + " hbm_gbs",
                          "traffic": traffic, "algorithmic_bytes_per_launch": fused_bytes, "launch_ms": ms_step,
-                         "algorithmic_bytes": "4 B x samples read + (mel write, mel re-read, dB write) 12 B x 128 x frames"},
+                         "algorithmic_bytes": "4 B x samples read + 4 B x 128 x frames of decibels written",
+                         "issue": issue,
+                         "note": "the kernel is issue-bound, not HBM-bound: issue_frac is the launch's warp "
+                                 "instructions over 4 issue slots per SM per clock at the sampled SM clock"},
             "plain_chain": {"value": plain_value, "unit": "clip-s/s", "ms_per_step": plain_ms,
                             "path": "four rppt_*_gpu C-ABI calls per step",
                             "algorithmic_bytes_per_step": sum(ab.values()),
                             "frac_of_hbm": sum(ab.values()) / (plain_ms / 1e3) / 1e9 / hbm, "per_op": per_op},
             "fused_over_plain": plain_ms / ms_step,
             "err_vs_fp64": err,
+            "parity_vs_reference": parity_ref,
+            "nsr": nsr,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "multirate": multirate,
@@ -817,8 +909,127 @@ def run_b200(args, world, rank, local):
     replicas.finish()
 
 
+def profile_ops(args):
+    """Every entry point of the audio path once (--profile-repeat times) on the 256-clip batch and the first
+    256 clips of the stereo multi-rate batch, for ncu captures (profiles/):
+
+        python bench.py --profile [--clips N] [--profile-repeat R] [--profile-only SUBSTRING]
+
+    With one repeat each kernel launches once per entry point (plus the small ragged-prefix kernels), so
+    `ncu -k regex:... -c <count>` captures each kernel once; --profile-only runs just the entry points whose
+    name contains SUBSTRING (fewer launches before the captured one).  Inputs are larger than L2.  Prints
+    one line per entry point with its CUDA-event time of the last repeat."""
+    import torch
+    from rpp_b200 import audio, lib
+    from rpp_b200.types import frontend_params, generic_desc
+    from rpp_b200.windows import kaiser_sinc
+    L_ = lib.load()
+    dev = torch.device("cuda")
+    h = lib.Handle(batch_size=args.clips, stream=torch.cuda.current_stream().cuda_stream)
+    x_np, lens_np = synth.gapped_clips(n=args.clips)
+    n, L = x_np.shape
+    x = torch.from_numpy(x_np).to(dev)
+    lens = torch.from_numpy(lens_np).to(dev)
+    coeff = torch.full((n,), 0.97, device=dev)
+    F = (lens_np // 160 + 1).astype(np.int32)
+    mf = int(F.max())
+    sd = audio_desc(n, L)
+    spd, md = spectra_desc(n, 257, mf), spectra_desc(n, 128, mf)
+    pre = torch.empty_like(x)
+    spec = torch.empty((n, 257, mf), device=dev)
+    mel = torch.empty((n, 128, mf), device=dev)
+    db = torch.empty_like(mel)
+    dims = torch.from_numpy(np.stack([np.full(n, 257, np.int32), F], 1).astype(np.int32)).to(dev)
+    patches = torch.from_numpy(np.stack([F, np.full(n, 128, np.int32)], 1).astype(np.int32)).to(dev)
+    begin = torch.empty(n, dtype=torch.int32, device=dev)
+    length = torch.empty(n, dtype=torch.int32, device=dev)
+    p = frontend_params()
+
+    # stereo multi-rate subset
+    xs_np, ls_np, rates_np = synth.stereo_multirate_clips(n=args.clips)
+    Ls = int(ls_np.max())
+    xs = torch.from_numpy(xs_np).to(dev)
+    sdims = torch.from_numpy(np.stack([ls_np, np.full(args.clips, 2, np.int32)], 1).astype(np.int32)).to(dev)
+    mono = torch.empty((args.clips, Ls), device=dev)
+    lut, scale, center, lobes = kaiser_sinc(16, beta=8.0)
+    lut_d = torch.from_numpy(lut).to(dev)
+    win = audio.resampling_window(lut_d, scale, center, lobes)
+    ir = torch.from_numpy(rates_np).to(dev)
+    orr = torch.full((args.clips,), 16000.0, device=dev)
+    L16 = int(np.ceil(Ls * 16000.0 / float(rates_np.min()))) + 8
+    mono16 = torch.empty((args.clips, L16), device=dev)
+    mdims = torch.from_numpy(np.stack([ls_np, np.ones(args.clips, np.int32)], 1).astype(np.int32)).to(dev)
+
+    x_host = torch.from_numpy(x_np).pin_memory()
+    out_host = torch.empty((n, 128, mf)).pin_memory()
+    lens_host = torch.from_numpy(lens_np).pin_memory()
+    coeff_host = torch.full((n,), 0.97).pin_memory()
+    db_small = torch.empty((min(n, 8), 128, mf), device=dev)
+    dims_small = patches[:min(n, 8)].contiguous()
+    sd_small = spectra_desc(min(n, 8), 128, mf)
+    stream = torch.cuda.current_stream().cuda_stream
+    gd = generic_desc((n, L))
+    sl_anchor = torch.full((n,), 10, dtype=torch.int32, device=dev)
+    sl_shape = torch.from_numpy((lens_np // 2).astype(np.int32)).to(dev)
+    sl_roi = torch.from_numpy(np.stack([np.full(n, 10), lens_np], 1).astype(np.uint32).ravel().view(np.int32)).to(dev)
+    sl_fill = torch.zeros(1, device=dev)
+    nd = generic_desc((n, 128, mf))
+    n_roi = torch.from_numpy(np.stack([np.zeros(n), np.zeros(n), np.full(n, 128), F], 1).astype(np.uint32).ravel()
+                             .view(np.int32))
+    n_mean, n_std = torch.zeros(n * 128, device=dev), torch.zeros(n * 128, device=dev)
+    n_out = torch.empty_like(db)
+
+    ops = [
+        ("pre_emphasis_filter", lambda: audio.pre_emphasis_filter(x, sd, pre, sd, lens, coeff, 0, h)),
+        ("spectrogram", lambda: audio.spectrogram(pre, sd, spec, spd, lens, True, True, None, 512, 2, 400, 160, h)),
+        ("mel_filter_bank", lambda: audio.mel_filter_bank(spec, spd, mel, md, dims, 8000.0, 0.0, 0, 128, 16000.0,
+                                                          True, h)),
+        ("to_decibels", lambda: audio.to_decibels(mel, md, db, md, patches, -80.0, 10.0, 0.0, h)),
+        ("frontend (fused)", lambda: audio.frontend(x, sd, db, md, lens, coeff, p, h)),
+        ("non_silent_region_detection", lambda: audio.non_silent_region_detection(x, sd, lens, begin, length, -60.0,
+                                                                                  2048, 0.0, 8192, h)),
+        ("down_mixing", lambda: audio.down_mixing(xs, audio_desc(args.clips, Ls, channels=2, num_dims=3), mono,
+                                                  audio_desc(args.clips, Ls), sdims, False, h)),
+        ("resample", lambda: audio.resample(mono, audio_desc(args.clips, Ls), mono16, audio_desc(args.clips, L16), ir,
+                                            orr, mdims, win, h)),
+        ("downmix_resample (fused)", lambda: audio.downmix_resample(xs, audio_desc(args.clips, Ls, channels=2,
+                                                                                   num_dims=3),
+                                                                    mono16, audio_desc(args.clips, L16), ir, orr,
+                                                                    sdims, False, lut_d, scale, center, lobes, h)),
+        ("spectrogram_tc (BF16 hi/lo x3)", lambda: audio.spectrogram_tc(x, sd, spec, spd, lens, coeff, 0, True, True,
+                                                                         512, 2, 400, 160, audio.TC_BF16_HILO3, h)),
+        ("frontend_host (pinned host tensors)", lambda: audio.frontend_host(x_host, sd, out_host, md, lens_host,
+                                                                            coeff_host, p, 0, h)),
+        ("slice (1-D, anchor 10, length/2)", lambda: audio.slice(x, gd, pre, gd, sl_anchor, sl_shape, sl_fill, True,
+                                                                 sl_roi, h)),
+        ("normalize (per filter over time)", lambda: audio.normalize(db, nd, n_out, nd, 2, n_mean, n_std, 3, 1.0, 0.0,
+                                                                     n_roi, h)),
+        ("to_decibels_gpu_static (8 clips)", lambda: L_.rppt_to_decibels_gpu_static(
+            mel.data_ptr(), ctypes.byref(sd_small), db_small.data_ptr(), ctypes.byref(sd_small),
+            dims_small.data_ptr(), ctypes.c_float(-80.0), ctypes.c_float(10.0), ctypes.c_float(0.0),
+            ctypes.c_void_p(stream))),
+    ]
+    for name, fn in ops:
+        if args.profile_only and args.profile_only not in name:
+            continue
+        for _ in range(args.profile_repeat):
+            st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            st.record()
+            rc = fn()
+            en.record()
+            torch.cuda.synchronize()
+            if rc != 0:
+                raise RuntimeError(f"{name}: status {rc} {lib.last_error()}")
+        print(f"{name:40s} {st.elapsed_time(en):9.3f} ms")
+    assert audio.device_error(h) == 0
+    h.close()
+
+
 def main():
     args = parse()
+    if args.profile:
+        profile_ops(args)
+        return
     world, rank, local = dist_init()
     if args.impl == "reference":
         run_reference(args, world, rank)

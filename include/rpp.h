@@ -61,8 +61,12 @@ SHARED_PUBLIC rppStatus_t rppGetBatchSize(rppHandle_t handle, size_t* batchSize)
 SHARED_PUBLIC rppStatus_t rppSetStream(rppHandle_t handle, rppAcceleratorQueue_t streamID);
 SHARED_PUBLIC rppStatus_t rppGetStream(rppHandle_t handle, rppAcceleratorQueue_t* streamID);
 
-/* Routes the handle's device-workspace allocations through the caller's allocator; passing
- * null restores cudaMallocAsync/cudaFreeAsync on the handle stream.  Replaces api/rpp.h:244. */
+/* Routes every device allocation the handle makes (its workspace, its cached tables and its device
+ * error word) through the caller's allocator; passing null restores cudaMalloc/cudaFree.  The
+ * current workspace is released (after the handle's stream drains) and the next call allocates a
+ * new one from the allocator now in force; every other block goes back, when the handle is
+ * destroyed, to the deallocator that was in force when it was allocated (none when that was null).
+ * Replaces api/rpp.h:244. */
 SHARED_PUBLIC rppStatus_t rppSetAllocator(rppHandle_t handle, rppAllocatorFunction allocator,
                                           rppDeallocatorFunction deallocator, void* allocatorContext);
 

@@ -61,7 +61,9 @@ SHARED_PUBLIC RppStatus rppt_to_decibels_gpu(RppPtr_t srcPtr, RpptDescPtr srcDes
  * device looks up the array's device address (cudaGetSymbolAddress, with that device current): make
  * that first call before any stream capture.  All calls share the one array, so calls that can run
  * on the GPU at the same time (different streams, overlapping graphs) race: order them on one
- * stream or with events. */
+ * stream or with events.  Launch failures are read right after each launch; a CUDA error that earlier
+ * work left pending on the calling thread makes the call return RPP_ERROR without launching (the
+ * error is left in place for its owner). */
 SHARED_PUBLIC RppStatus rppt_to_decibels_gpu_static(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr,
                                                     RpptDescPtr dstDescPtr, RpptImagePatchPtr srcDims, Rpp32f cutOffDB,
                                                     Rpp32f multiplier, Rpp32f referenceMagnitude,

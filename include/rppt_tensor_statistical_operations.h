@@ -19,7 +19,11 @@
  * sums follow the reference host path's recursive halving tree bit for bit
  * (src/modules/tensor/cpu/kernel/normalize.cpp:29-120, :417-600); the inverse square root is
  * correctly rounded where the reference refines the SSE estimate (~1e-7 relative apart).
- * Asynchronous on the handle stream except that a device roiTensor is read back first.
+ * Synchronization: the roi lengths size the work list on the host, so unless roiTensor is pageable
+ * host memory the call first synchronizes the handle stream (a device roiTensor is copied back; a
+ * pinned or managed one is read once earlier work on the stream, which may have written it, is
+ * done).  This is the one call of the library that synchronizes; everything after the roi read is
+ * asynchronous on the handle stream.
  */
 #ifndef RPPB_RPPT_TENSOR_STATISTICAL_OPERATIONS_H
 #define RPPB_RPPT_TENSOR_STATISTICAL_OPERATIONS_H

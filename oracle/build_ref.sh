@@ -11,7 +11,8 @@
 # shipped goldens under utilities/test_suite/REFERENCE_OUTPUTS_AUDIO/.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-RPP_REF="${RPP_REF:-/root/reference}"
+# default: the reference checkout beside this repository (../reference)
+RPP_REF="${RPP_REF:-$(cd "$(dirname "$0")/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 GEN="$OUT/gen"
 if [ ! -d "$RPP_REF/src/modules/tensor/cpu/kernel" ]; then

@@ -58,7 +58,8 @@ def build_reference(ref_root=None):
 
     Returns the library path, or None when the reference sources are absent (the GPU box uses
     the prebuilt oracle/_ref/librpp_audio_ref.so)."""
-    root = ref_root or os.environ.get("RPP_REF", "/root/reference")
+    # default: the reference checkout beside this repository (../reference), or $RPP_REF
+    root = ref_root or os.environ.get("RPP_REF", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
     if not os.path.isdir(os.path.join(root, "src", "modules", "tensor", "cpu", "kernel")):
         return _REF_SO if os.path.isfile(_REF_SO) else None
     env = dict(os.environ, RPP_REF=root)

@@ -918,10 +918,15 @@ extern "C" SHARED_PUBLIC RppStatus rppt_normalize_gpu(RppPtr_t srcPtr, RpptGener
         const int n = int(dd.dims[0]);
         if (n <= 0) return RPP_SUCCESS;
         const int compute = computeMeanStddev & 3;
-        // roi lengths are needed on the host (parameter counts, work list)
+        // roi lengths are needed on the host (parameter counts, work list).  Memory the device can write
+        // (device, managed, pinned) may still be written by earlier work on the handle stream, so the
+        // stream is synchronized before the host reads it; pageable memory is read as it is.
         std::vector<uint32_t> roi(size_t(n) * 4);
         cudaPointerAttributes attr{};
-        if (cudaPointerGetAttributes(&attr, roiTensor) == cudaSuccess && attr.type == cudaMemoryTypeDevice)
+        const bool known = cudaPointerGetAttributes(&attr, roiTensor) == cudaSuccess;
+        if (!known) cudaGetLastError();
+        const cudaMemoryType mt = known ? attr.type : cudaMemoryTypeUnregistered;
+        if (mt == cudaMemoryTypeDevice)
         {
             check_cuda(cudaMemcpyAsync(roi.data(), roiTensor, roi.size() * 4, cudaMemcpyDeviceToHost, h.stream()),
                        "cudaMemcpyAsync(roi)");
@@ -929,7 +934,8 @@ extern "C" SHARED_PUBLIC RppStatus rppt_normalize_gpu(RppPtr_t srcPtr, RpptGener
         }
         else
         {
-            cudaGetLastError();
+            if (mt == cudaMemoryTypeHost || mt == cudaMemoryTypeManaged)
+                check_cuda(cudaStreamSynchronize(h.stream()), "cudaStreamSynchronize(roi)");
             std::memcpy(roi.data(), roiTensor, roi.size() * 4);
         }
         int maxSize = 1;

@@ -36,8 +36,8 @@ Handle::~Handle()
         }
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
     if (ws_) dev_free(ws_);
-    for (auto& kv : tables_) cudaFree(kv.second);
-    if (flags_) cudaFree(flags_);
+    for (auto& kv : tables_) block_free(kv.second);
+    block_free(flags_);
     if (pinned_) cudaFreeHost(pinned_);
     if (pinned_free_) cudaEventDestroy(pinned_free_);
     if (ev_begin_) cudaEventDestroy(ev_begin_);
@@ -65,6 +65,27 @@ void Handle::dev_free(void* p)
         return;
     }
     cudaFree(p);
+}
+
+Handle::Block Handle::block_alloc(size_t bytes)
+{
+    Block b;
+    b.p = dev_alloc(bytes);
+    b.custom = alloc_fn_ != nullptr;
+    b.free_fn = free_fn_;
+    b.ctx = alloc_ctx_;
+    return b;
+}
+
+void Handle::block_free(const Block& b)
+{
+    if (!b.p) return;
+    if (b.custom)
+    {
+        if (b.free_fn) b.free_fn(b.ctx, b.p);
+        return;
+    }
+    cudaFree(b.p);
 }
 
 void* Handle::workspace(size_t bytes)
@@ -181,40 +202,43 @@ const float* Handle::table(const std::string& key, size_t count, void (*build)(f
                            const void* ctx)
 {
     auto it = tables_.find(key);
-    if (it != tables_.end()) return static_cast<const float*>(it->second);
+    if (it != tables_.end()) return static_cast<const float*>(it->second.p);
     std::vector<float> host(count);
     build(host.data(), count, ctx);
-    void* d = nullptr;
-    check_cuda(cudaMalloc(&d, count * sizeof(float)), "cudaMalloc(table)");
+    const Block b = block_alloc(count * sizeof(float));
     // Synchronous copy from pageable memory: tables are built once per key, before any capture.
-    check_cuda(cudaMemcpy(d, host.data(), count * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(table)");
-    tables_[key] = d;
-    return static_cast<const float*>(d);
+    const cudaError_t e = cudaMemcpy(b.p, host.data(), count * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) block_free(b);
+    check_cuda(e, "cudaMemcpy(table)");
+    tables_[key] = b;
+    return static_cast<const float*>(b.p);
 }
 
 void* Handle::device_table(const std::string& key, size_t bytes, bool* fresh)
 {
     *fresh = false;
     auto it = tables_.find(key);
-    if (it != tables_.end()) return it->second;
+    if (it != tables_.end()) return it->second.p;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     check_cuda(cudaStreamIsCapturing(stream_, &cap), "cudaStreamIsCapturing");
     if (cap != cudaStreamCaptureStatusNone) return nullptr;
-    void* d = nullptr;
-    check_cuda(cudaMalloc(&d, bytes), "cudaMalloc(device table)");
-    tables_[key] = d;
+    const Block b = block_alloc(bytes);
+    tables_[key] = b;
     *fresh = true;
-    return d;
+    return b.p;
 }
 
 int* Handle::device_flags()
 {
-    if (!flags_)
+    if (!flags_.p)
     {
-        check_cuda(cudaMalloc(&flags_, 64 * sizeof(int)), "cudaMalloc(flags)");
-        check_cuda(cudaMemset(flags_, 0, 64 * sizeof(int)), "cudaMemset(flags)");
+        const Block b = block_alloc(64 * sizeof(int));
+        const cudaError_t e = cudaMemset(b.p, 0, 64 * sizeof(int));
+        if (e != cudaSuccess) block_free(b);
+        check_cuda(e, "cudaMemset(flags)");
+        flags_ = b;
     }
-    return flags_;
+    return static_cast<int*>(flags_.p);
 }
 
 void Handle::set_allocator(rppAllocatorFunction a, rppDeallocatorFunction d, void* ctx)

@@ -113,8 +113,19 @@ class Handle
     void staging_done();
 
   private:
+    // A device block and the deallocator it must go back to (the allocator in force when it was
+    // allocated: rppSetAllocator may change it while blocks are alive).
+    struct Block
+    {
+        void* p = nullptr;
+        rppDeallocatorFunction free_fn = nullptr;
+        void* ctx = nullptr;
+        bool custom = false;
+    };
     void* dev_alloc(size_t bytes);
     void dev_free(void* p);
+    Block block_alloc(size_t bytes);
+    static void block_free(const Block& b);
 
     int device_ = 0;
     int num_sms_ = 148;
@@ -132,8 +143,8 @@ class Handle
     cudaStream_t aux_[2] = {nullptr, nullptr};
     std::vector<cudaEvent_t> events_;
 
-    std::map<std::string, void*> tables_;
-    int* flags_ = nullptr;
+    std::map<std::string, Block> tables_;
+    Block flags_;
     bool wait_injection_ = false;
 
     rppAllocatorFunction alloc_fn_ = nullptr;

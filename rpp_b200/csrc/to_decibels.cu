@@ -343,6 +343,9 @@ extern "C" SHARED_PUBLIC RppStatus rppt_to_decibels_gpu_static(RppPtr_t srcPtr, 
     if (dims == nullptr) return RPP_ERROR_INVALID_ARGUMENTS;   // srcDims must be device or pinned memory
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kStaticMaxDevices) return RPP_ERROR;
+    // a CUDA error left pending on this thread by earlier work belongs to its owner: refuse the call
+    // without launching (and without clearing it) rather than report it as this call's failure
+    if (cudaPeekAtLastError() != cudaSuccess) return RPP_ERROR;
     StaticDevice* sd = nullptr;
     if (static_setup(device, sd) != cudaSuccess) return RPP_ERROR;
 
@@ -359,7 +362,9 @@ extern "C" SHARED_PUBLIC RppStatus rppt_to_decibels_gpu_static(RppPtr_t srcPtr, 
     float* dst = static_cast<float*>(dstPtr);
     const uint32_t sN = srcDescPtr->strides.nStride, sH = srcDescPtr->strides.hStride;
     const uint32_t dN = dstDescPtr->strides.nStride, dH = dstDescPtr->strides.hStride;
+    // every launch is checked at once: the first failure ends the call before later kernels queue
     launch_ragged_prefix(DecibelCount{dims}, n, prefix, s);
+    if (cudaGetLastError() != cudaSuccess) return RPP_ERROR;
     auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
     const bool vecSrc = aligned(src) && (sN & 3) == 0 && (sH & 3) == 0;
     const bool vec = vecSrc && aligned(dst) && (dN & 3) == 0 && (dH & 3) == 0;
@@ -369,6 +374,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_to_decibels_gpu_static(RppPtr_t srcPtr, 
         if (cudaMemsetAsync(maxKey, 0, size_t(n) * sizeof(unsigned), s) != cudaSuccess) return RPP_ERROR;
         decibel_max_kernel<<<sd->gridMax, kThreads, 0, s>>>(src, sN, sH, dims, maxKey, prefix, n, vecSrc);
         count_launch();
+        if (cudaGetLastError() != cudaSuccess) return RPP_ERROR;
         decibel_kernel<true><<<sd->gridTrue, kThreads, 0, s>>>(src, sN, sH, dst, dN, dH, dims, maxKey, 0.f, minRatio,
                                                                multiplier, prefix, n, vec);
         count_launch();

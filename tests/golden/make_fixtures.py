@@ -1,6 +1,7 @@
 """Captures the reference's audio QA fixtures as compact .npz files under tests/golden/.
 
-Run once in a checkout that has the reference sources (default /root/reference, or $RPP_REF);
+Run once in a checkout that has the reference sources (default ../reference beside this repository,
+or $RPP_REF);
 the GPU tests read only the .npz files this writes.  Sources of each array:
   inputs  utilities/test_suite/TEST_AUDIO_FILES/three_samples_single_channel_src1/sample{1,2,3}.wav
           (16 kHz mono int16; the test suite reads them with libsndfile's sf_read_float, i.e.
@@ -15,7 +16,7 @@ import wave
 
 import numpy as np
 
-REF = os.environ.get("RPP_REF", "/root/reference")
+REF = os.environ.get("RPP_REF", os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))), "reference"))
 HERE = os.path.dirname(os.path.abspath(__file__))
 SUITE = os.path.join(REF, "utilities", "test_suite")
 

@@ -13,7 +13,7 @@ from rpp_b200 import types as T
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INCLUDE = os.path.join(ROOT, "include")
-REF = os.environ.get("RPP_REF", "/root/reference")
+REF = os.environ.get("RPP_REF", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def declared_symbols():

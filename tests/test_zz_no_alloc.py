@@ -2,10 +2,11 @@
 
 Some callers cannot allocate device memory (a fixed device-memory budget owned by another runtime, a
 real-time thread that must not block in cudaMalloc, code with no rppHandle_t).  This entry point
-serves them with scratch held in a fixed array inside the library.  The test checks, on two calls in
-a row with different batches (the shared array keeps the previous call's contents), that its output
-equals the handle-based rppt_to_decibels_gpu output within the decibel tolerance of the other GPU
-tests, and that a batch above the array's limit is refused.  It needs no other test to run first.
+serves them with scratch held in a fixed array inside the library.  The test checks, on calls in a
+row with different batches (the shared array keeps the previous call's contents), that its output is
+bit for bit the handle-based rppt_to_decibels_gpu output (both run the same kernels with the same
+arguments; a maximum left over from the previous call would show as a difference), and that a batch
+above the array's limit is refused.  It needs no other test to run first.
 """
 import ctypes
 
@@ -17,8 +18,6 @@ from rpp_b200 import audio, lib
 from rpp_b200.types import RppStatus, audio_desc, spectra_desc
 
 pytestmark = pytest.mark.gpu
-
-DB_TOL = 1e-4   # same bound as tests/test_gpu_ops.py (DB_ABS / 10)
 
 
 def call_static(src, sdesc, dst, ddesc, dims, cutoff, mult, ref, stream):
@@ -47,7 +46,7 @@ def one_case(h, stream, n, H, W, seed, ref_mag, two_d):
     torch.cuda.synchronize()
     e, g = expect.cpu().numpy(), got.cpu().numpy()
     assert np.array_equal(e == -7.0, g == -7.0)       # same elements written
-    assert np.abs(g - e).max() <= DB_TOL
+    assert np.array_equal(g, e)                       # same bits
 
 
 def test_static_to_decibels_matches_handle_path():
