@@ -47,7 +47,7 @@ std::string tune_key(int device, const RpptDesc* sd, const RpptDesc* dd, const R
     // the shape of the work: clips, longest clip (power-of-two bucket) and the front-end geometry
     k << name << "/n" << sd->n << "/L" << (sd->strides.nStride ? 1u << (31 - __builtin_clz(sd->strides.nStride)) : 0)
       << "/nfft" << p.nfft << "/W" << p.windowLength << "/hop" << p.windowStep << "/mel" << p.numFilter << "/F"
-      << dd->w;
+      << dd->w << "/engine" << p.spectrumEngine;
     (void)lenHost;
     return k.str();
 }
@@ -115,7 +115,8 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_tune_gpu(RppPtr_t srcPtr, RpptD
         for (int tf : {t0, 2 * t0, 4 * t0})
             for (int db : {32, 64, 128})
                 for (int la : {8, 32, 96})
-                    for (int cps : {0, 2}) cands.push_back(Choice{tf, db, la, cps, 0.f});
+                    // CTAs per SM: all that fit (3 for the FP32 engine, 2 for the tensor-core one) or fewer
+                    for (int cps : {0, params->spectrumEngine == 1 ? 1 : 2}) cands.push_back(Choice{tf, db, la, cps, 0.f});
         cudaEvent_t e0, e1;
         check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
         check_cuda(cudaEventCreate(&e1), "cudaEventCreate");

@@ -464,6 +464,7 @@ RppStatus frontend_params(Handle& h, const RppbFrontendParams* params, float* wi
     a.tileFrames = p.tileFrames;
     a.dbFrames = p.dbFrames;
     a.ctasPerSm = p.ctasPerSm;
+    a.engine = int(p.spectrumEngine);
     a.clips = nullptr;
     a.outRate = 0.f;
     a.coeffAll = 0.f;
@@ -489,7 +490,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPt
         const int n = int(srcDescPtr->n);
         if (n <= 0) return RPP_SUCCESS;
         const int lookahead = params->lookahead > 0 ? params->lookahead : 32;
-        const size_t scratchBytes = frontend_scratch_bytes(n, lookahead);
+        const size_t scratchBytes = frontend_scratch_bytes(n, lookahead, params->numFilter);
         const int W = params->windowLength > 0 ? params->windowLength : 0;
         Carver m(nullptr);
         m.take<int>(n);
@@ -584,7 +585,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost,
             outElems = std::max(outElems, size_t(clips) * nf * size_t(mf));
         }
         const int lookahead = params->lookahead > 0 ? params->lookahead : 32;
-        const size_t scratchBytes = frontend_scratch_bytes(maxClips, lookahead);
+        const size_t scratchBytes = frontend_scratch_bytes(maxClips, lookahead, params->numFilter);
         Carver m(nullptr);
         m.take<int>(2 * n);
         m.take<float>(n);
@@ -695,7 +696,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips
         const int n = numClips;
         if (n <= 0) return RPP_SUCCESS;
         const int lookahead = params->lookahead > 0 ? params->lookahead : 32;
-        const size_t scratchBytes = frontend_scratch_bytes(n, lookahead);
+        const size_t scratchBytes = frontend_scratch_bytes(n, lookahead, params->numFilter);
         const int W = params->windowLength > 0 ? params->windowLength : 0;
         Carver m(nullptr);
         m.take<RppbClip>(n);

@@ -143,9 +143,16 @@ struct FrontendArgs
     // item waits for beyond its clip's, and the poll limit of that wait (0: the default)
     int waitExtra;
     long long waitLimit;
+    // spectrum engine: 0 the FP32 register FFT (bit-identical to the plain calls), 1 the factored DFT
+    // on tensor cores in BF16 hi/lo x3 (fused_tc.cu; nfft 512 only)
+    int engine;
 };
-size_t frontend_scratch_bytes(int n, int lookahead);
+size_t frontend_scratch_bytes(int n, int lookahead, int numFilter);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);
+// The tensor-core engine (fused_tc.cu): launched by launch_frontend for engine 1; `melScratch` holds the
+// mel tables when the handle's cache cannot provide them (stream capture with new parameters).
+bool frontend_tc_supported(const FrontendArgs& a);
+void launch_frontend_tc(Handle& h, const FrontendArgs& a, void* scratch, uint4* melScratch);
 
 // slice (slice.cu): 1-D or 2-D boxes per sample, strides in elements.
 struct SliceArgs

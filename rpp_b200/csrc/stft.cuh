@@ -140,18 +140,15 @@ __device__ __forceinline__ void stft_tables(const float2* __restrict__ twiddle, 
     __syncthreads();
 }
 
-// Computes frames f0 .. f0+TF-1 (those < F) of one sample into s_out[bin * OUT_LD + f] and
-// leaves the other columns undefined.  All THREADS threads of the CTA must call it.
+// Stages the input span of frames f0 .. f0+TF-1 (those < F) in s_span after its zero pad and zeroes
+// the tail, so that buffer sample n of tile frame fl is s_span[span_pad(W) + fl * hop - offset + n]
+// for every n in [0, nfft).  All THREADS threads call it; ends with __syncthreads.
 template <int NFFT, int THREADS, int TFX = Plan<NFFT>::TF, class Src>
-__device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, int hop, int centerOffset, int power,
-                                          const float* __restrict__ s_win, const float2* __restrict__ s_tw,
-                                          const float2* __restrict__ s_tw1, float* __restrict__ s_span,
-                                          float2* __restrict__ s_fft, float* __restrict__ s_out)
+__device__ __forceinline__ void stft_stage_span(const Src& src, int f0, int F, int W, int hop, int centerOffset,
+                                                float* __restrict__ s_span)
 {
     using S = StftShape<NFFT, THREADS, TFX>;
-    constexpr int M = S::M, R1 = S::R1, R2 = S::R2, TF = S::TF, G = S::G, FPP = S::FPP, BINS = S::BINS;
-
-    // ---- 1. stage the tile's input span (after the zero pad), then zero its tail
+    constexpr int TF = S::TF;
     const int Tv = min(TF, F - f0);
     const int spanStart = f0 * hop - centerOffset;
     const int spanLen = (Tv - 1) * hop + W;
@@ -179,6 +176,23 @@ __device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, 
     }
     for (int i = threadIdx.x; i < S::span_tail(W); i += THREADS) s_data[spanLen + i] = 0.f;
     __syncthreads();
+}
+
+// Computes frames f0 .. f0+TF-1 (those < F) of one sample into s_out[bin * OUT_LD + f] and
+// leaves the other columns undefined.  All THREADS threads of the CTA must call it.
+template <int NFFT, int THREADS, int TFX = Plan<NFFT>::TF, class Src>
+__device__ __forceinline__ void stft_tile(const Src& src, int f0, int F, int W, int hop, int centerOffset, int power,
+                                          const float* __restrict__ s_win, const float2* __restrict__ s_tw,
+                                          const float2* __restrict__ s_tw1, float* __restrict__ s_span,
+                                          float2* __restrict__ s_fft, float* __restrict__ s_out)
+{
+    using S = StftShape<NFFT, THREADS, TFX>;
+    constexpr int M = S::M, R1 = S::R1, R2 = S::R2, TF = S::TF, G = S::G, FPP = S::FPP, BINS = S::BINS;
+
+    // ---- 1. stage the tile's input span (after the zero pad), then zero its tail
+    stft_stage_span<NFFT, THREADS, TFX>(src, f0, F, W, hop, centerOffset, s_span);
+    const int Tv = min(TF, F - f0);
+    float* const s_data = s_span + S::span_pad(W);
 
     const int j = threadIdx.x % G;
     const int slot = threadIdx.x / G;

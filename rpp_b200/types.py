@@ -168,16 +168,20 @@ class RppbFrontendParams(ctypes.Structure):
                 ("sampleRate", ctypes.c_float), ("normalize", ctypes.c_bool), ("cutOffDB", ctypes.c_float),
                 ("multiplier", ctypes.c_float), ("referenceMagnitude", ctypes.c_float),
                 ("lookahead", ctypes.c_int32), ("tileFrames", ctypes.c_int32), ("dbFrames", ctypes.c_int32),
-                ("ctasPerSm", ctypes.c_int32)]
+                ("ctasPerSm", ctypes.c_int32), ("spectrumEngine", ctypes.c_int32)]
 
 
-assert ctypes.sizeof(RppbFrontendParams) == 88
+assert ctypes.sizeof(RppbFrontendParams) == 88   # sizeof in C (the engine field fills the tail padding)
+
+# RppbSpectrumEngine
+ENGINE_FP32_FFT = 0
+ENGINE_TENSOR_CORE_BF16X3 = 1
 
 
 def frontend_params(nfft=512, window_length=400, window_step=160, num_filter=128, sample_rate=16000.0,
                     min_freq=0.0, max_freq=8000.0, mel_formula=0, normalize=True, cut_off_db=-80.0,
                     multiplier=10.0, reference_magnitude=0.0, border=0, center=True, reflect=True, power=2,
-                    window=None, lookahead=0, tile_frames=0, db_frames=0, ctas_per_sm=0):
+                    window=None, lookahead=0, tile_frames=0, db_frames=0, ctas_per_sm=0, engine=0):
     p = RppbFrontendParams()
     p.borderType = int(border)
     p.centerWindows = bool(center)
@@ -190,6 +194,7 @@ def frontend_params(nfft=512, window_length=400, window_step=160, num_filter=128
     p.cutOffDB, p.multiplier, p.referenceMagnitude = float(cut_off_db), float(multiplier), float(reference_magnitude)
     p.lookahead = int(lookahead)
     p.tileFrames, p.dbFrames, p.ctasPerSm = int(tile_frames), int(db_frames), int(ctas_per_sm)
+    p.spectrumEngine = int(engine)
     return p
 
 
