@@ -944,6 +944,7 @@ def profile_ops(args):
     begin = torch.empty(n, dtype=torch.int32, device=dev)
     length = torch.empty(n, dtype=torch.int32, device=dev)
     p = frontend_params()
+    p_tc = frontend_params(engine=1)
 
     # stereo multi-rate subset
     xs_np, ls_np, rates_np = synth.stereo_multirate_clips(n=args.clips)
@@ -986,6 +987,7 @@ def profile_ops(args):
                                                           True, h)),
         ("to_decibels", lambda: audio.to_decibels(mel, md, db, md, patches, -80.0, 10.0, 0.0, h)),
         ("frontend (fused)", lambda: audio.frontend(x, sd, db, md, lens, coeff, p, h)),
+        ("frontend tensor-core engine (fused)", lambda: audio.frontend(x, sd, db, md, lens, coeff, p_tc, h)),
         ("non_silent_region_detection", lambda: audio.non_silent_region_detection(x, sd, lens, begin, length, -60.0,
                                                                                   2048, 0.0, 8192, h)),
         ("down_mixing", lambda: audio.down_mixing(xs, audio_desc(args.clips, Ls, channels=2, num_dims=3), mono,

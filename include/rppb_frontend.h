@@ -13,7 +13,7 @@
  *
  * and, with the default FP32 spectrum engine, its outputs are bit-identical to that sequence run
  * through this library (the tensor-core engine, RppbSpectrumEngine, computes the spectrum as a factored
- * DFT on tcgen05 tensor cores instead, within ~1e-5 of each frame's largest bin).  The
+ * DFT on tcgen05 tensor cores instead, within ~1e-6 of each frame's largest bin).  The
  * intermediate pre-emphasized signal, spectrum and mel tensors never reach memory except the mel
  * power, which is written into dst and converted to decibels in place once the clip's maximum is
  * known.  dst is NFT [numFilter][frames] per sample (hStride >= frames); only the valid frames
@@ -73,12 +73,13 @@ typedef enum
     /* FP32 register FFT: the outputs are bit for bit those of the four plain calls */
     RPPB_ENGINE_FP32_FFT = 0,
     /* The 512-point real DFT factored as 16 x 32 and computed as two GEMM stages on tcgen05 tensor cores
-     * (32-point real DFTs, an FP32 twiddle, 16-point complex DFTs), every operand split into BF16
-     * hi + lo and hi*hi + hi*lo + lo*hi accumulated in FP32: the spectrum keeps ~1e-5 of each frame's
-     * largest bin against FP64 (the mel and decibel steps are the FP32 engine's), so the outputs are
-     * not bit-identical to the plain calls.  nfft must be 512 (windowLength <= 512, tileFrames 0, 16,
-     * 32 or 64); otherwise RPP_ERROR_NOT_IMPLEMENTED. */
-    RPPB_ENGINE_TENSOR_CORE_BF16X3 = 1
+     * (32-point real DFTs, an FP32 twiddle, 16-point complex DFTs).  Each frame is scaled by a power of
+     * two, every operand is split into F16 hi + lo, and hi*hi + hi*lo + lo*hi is accumulated in FP32:
+     * the spectrum stays within ~1e-6 of each frame's largest bin against FP64 (the mel and decibel
+     * steps are the FP32 engine's), so the outputs are close to, not bit-identical with, the plain
+     * calls.  nfft must be 512 (windowLength <= 512, tileFrames 0, 16, 32 or 64); otherwise
+     * RPP_ERROR_NOT_IMPLEMENTED. */
+    RPPB_ENGINE_TENSOR_CORE_F16X3 = 1
 } RppbSpectrumEngine;
 
 /* srcDesc numDims = 2 (F32 1-D signals); dstDesc numDims = 3, layout NFT, F32.

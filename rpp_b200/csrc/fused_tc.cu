@@ -1,6 +1,6 @@
 // Fused front end on tensor cores: pre-emphasis -> STFT power -> mel filter bank -> decibels in one
 // persistent launch, with the spectrum of each tile of 16 frames computed as a factored DFT on the
-// 5th-generation tensor cores (tcgen05) in BF16 hi/lo x3 with FP32 accumulation.  Same work queue,
+// 5th-generation tensor cores (tcgen05) in F16 hi/lo x3 with FP32 accumulation.  Same work queue,
 // mel sums and decibel items as the FP32 fused kernel (fused_queue.cuh, fused.cu); only the
 // spectrum engine differs, so the outputs carry the factored DFT's rounding instead of matching the
 // plain calls bit for bit.
@@ -17,17 +17,24 @@
 //           B1 = the real 32-point DFT basis, columns (Re k2=0, Re k2=16, Re k2, Im k2 for k2 = 1..15);
 //   stage 2, for i = 0, 1, 2: A2_i row (f, q') = the twiddled Y'[.][k2 = 8 i + q'] over K = (q, j, re/im)
 //           (i = 2 holds k2 = 16 in rows q' = 0); B2 = the complex 16-point DFT basis as a real 32 x 32.
-// Each operand is split x = hi + lo into two BF16 values and the products hi*hi + hi*lo + lo*hi are
-// accumulated in FP32 in tensor memory (6 MMAs of K = 16 per 32 of K), so the spectrum keeps ~1e-5 of
-// each frame's largest bin against FP64.  The operand tiles (128 rows x 128 bytes: 32 BF16 of hi then
-// 32 of lo per row) use the 128-byte-swizzled K-major layout; A2 reuses A1's shared memory.
+// Each frame is scaled by a power of two so that its largest windowed sample lies in [0.5, 1) (then
+// |Y| <= 32, inside the F16 range at both stages; the power is scaled back at the end).  Each operand
+// is split x = hi + lo into two F16 values (hi + lo holds x to ~2^-22 of the frame's scale) and the
+// products hi*hi + hi*lo + lo*hi are accumulated in FP32 in tensor memory (6 MMAs of K = 16 per 32 of
+// K), so the spectrum stays within ~1e-6 of each frame's largest bin against FP64.  The operand tiles
+// (128 rows x 128 bytes: 32 F16 of hi then 32 of lo per row) use the 128-byte-swizzled K-major layout;
+// A2 reuses A1's shared memory.
 //
 // Per tile: stage the span (CUDA cores) -> build A1 -> one thread issues 12 MMAs and commits to an
 // mbarrier -> epilogue 1 reads the stage-1 accumulators (tcgen05.ld), twiddles and splits them into A2
 // -> 18 MMAs -> epilogue 2 reads the bins and writes the power tile -> the mel sums of the FP32 kernel.
 // Every mbarrier wait is bounded: on a timeout the kernel sets bit 4 of the handle's device error word,
 // waits once more (bounded) for its MMAs in flight, frees its tensor memory and leaves.
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <map>
+#include <mutex>
+#include <set>
 
 #include "fused_queue.cuh"
 #include "tcgen05.cuh"
@@ -42,8 +49,11 @@ constexpr uint32_t kTcABytes = 3 * kTcTile;       // A1 (tiles 0-1) and A2 (tile
 constexpr uint32_t kTcBBytes = 32 * 128;          // one 32-row basis tile
 constexpr int kTcTmemCols = 256;
 constexpr uint32_t kTcD1 = 0, kTcD2 = 64;         // tensor-memory columns of the accumulators
-constexpr uint32_t kTcIdesc = tc::idesc_bf16(128, 32);
+constexpr uint32_t kTcIdesc = tc::idesc_f16(128, 32);
 constexpr long long kTcWaitLimit = 1ll << 21;     // mbarrier polls before a tensor-core wait gives up
+
+// Stage-1 K order: index kk < 16 holds n2 = 2 kk, kk >= 16 holds n2 = 2 (kk - 16) + 1.
+__host__ __device__ constexpr int s1_n2(int kk) { return kk < 16 ? 2 * kk : 2 * (kk - 16) + 1; }
 
 // Row of the stage-2 operand for frame f (of 16) within the 16-row block of its k2: a permutation
 // that puts frames f and f + 1 four rows apart inside their 8-row swizzle atom, so the epilogue's
@@ -54,7 +64,7 @@ __host__ __device__ constexpr int s2_frame(int r) { return 8 * (r >> 3) + 2 * (r
 // Shared memory plan (bytes from a 1024-byte aligned base).
 struct TcLayout
 {
-    size_t a, b1, b2, w512, win, span, out, mel, melIv, melGrp, total, melBytes;
+    size_t a, b1, b2, w512, scale, win, span, out, mel, melIv, melGrp, total, melBytes;
     __host__ __device__ TcLayout(int numFilter, int W, int hop)
     {
         using S = StftShape<kTcNfft, kFusedThreads, kTcTF>;
@@ -63,7 +73,8 @@ struct TcLayout
         b1 = a + kTcABytes;
         b2 = b1 + kTcBBytes;
         w512 = b2 + kTcBBytes;
-        win = w512 + 256 * 8;
+        scale = w512 + 16 * 17 * 8;
+        win = scale + kTcTF * 4;
         span = win + size_t(kTcNfft) * 4;
         out = (span + S::span_bytes(W, hop) + 15) & ~size_t(15);
         mel = (out + S::out_bytes + 15) & ~size_t(15);
@@ -75,21 +86,23 @@ struct TcLayout
     }
 };
 
-// Per-CTA constant tables: the two BF16 hi/lo bases in the swizzled layout and W512^e for e < 256.
+// Per-CTA constant tables: the two F16 hi/lo bases in the swizzled layout and the twiddles
+// W512^(n1 k2) as [n1][k2] (n1 < 16, k2 <= 16).
 // twiddle[e] = (cos, sin)(2 pi e / 512), so W512^e = x - i y.
 __device__ __forceinline__ void tc_tables(const float2* __restrict__ twiddle, unsigned char* b1, unsigned char* b2,
                                           float2* w512)
 {
     auto put = [](unsigned char* t, int row, int k, float v) {
-        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-        *reinterpret_cast<__nv_bfloat16*>(t + tc::sw128(row, 2 * k)) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(t + tc::sw128(row, 64 + 2 * k)) = lo;
+        const __half hi = __float2half_rn(v);
+        const __half lo = __float2half_rn(v - __half2float(hi));
+        *reinterpret_cast<__half*>(t + tc::sw128(row, 2 * k)) = hi;
+        *reinterpret_cast<__half*>(t + tc::sw128(row, 64 + 2 * k)) = lo;
     };
     for (int i = threadIdx.x; i < 32 * 32; i += kFusedThreads)
     {
-        // B1 row c, K = n2: Re k2 = 0, Re k2 = 16, then (Re, Im) of W32^(n2 k2) for k2 = 1..15
-        const int c = i >> 5, n2 = i & 31;
+        // B1 row c, K index kk (n2 = s1_n2(kk)): Re k2 = 0, Re k2 = 16, then (Re, Im) of W32^(n2 k2) for
+        // k2 = 1..15
+        const int c = i >> 5, kk = i & 31, n2 = s1_n2(kk);
         float v;
         if (c == 0) v = 1.f;
         else if (c == 1) v = (n2 & 1) ? -1.f : 1.f;
@@ -98,7 +111,7 @@ __device__ __forceinline__ void tc_tables(const float2* __restrict__ twiddle, un
             const float2 w = twiddle[(16 * (c >> 1) * n2) & (kTcNfft - 1)];
             v = (c & 1) ? -w.y : w.x;
         }
-        put(b1, c, n2, v);
+        put(b1, c, kk, v);
         // B2 row c = 2 k1 + (0: Re X, 1: Im X), K = 4 q + 2 j + (0: Re Y', 1: Im Y') with n1 = 8 j + q:
         // X = sum Y' W16^(n1 k1), W = wc + i ws, wc = cos, ws = -sin
         const int r2 = i >> 5, K = i & 31;
@@ -110,16 +123,18 @@ __device__ __forceinline__ void tc_tables(const float2* __restrict__ twiddle, un
         else u = reY ? ws : wc;
         put(b2, r2, K, u);
     }
-    for (int e = threadIdx.x; e < 256; e += kFusedThreads) w512[e] = twiddle[e];
+    // the twiddles of epilogue 1 by (n1, k2): W512^(n1 k2), 17 per n1
+    for (int e = threadIdx.x; e < 16 * 17; e += kFusedThreads) w512[e] = twiddle[(e / 17) * (e % 17)];
 }
 
-// Stage-1 operand: A1_j row (f, q) = q + 8 f, K = n2 (hi 0..31 | lo 0..31), value = window * sample of
-// buffer position n = 8 j + q + 16 n2 of tile frame f (zero for frames past the tile's valid ones).
-// Lane l of warp w takes n1 = l % 16 and the n2 of parity l / 16 of frame 8 p + w (p = pass), so the
-// 32 lanes read 32 consecutive buffer samples; partners l and l ^ 16 then trade halves so each holds
-// 16 consecutive n2 and writes them as 16-byte chunks.
+// Stage-1 operand: A1_j row (f, q) = q + 8 f, K index kk (hi 0..31 | lo 0..31) holding n2 = s1_n2(kk), value
+// = window * sample of buffer position n = 8 j + q + 16 n2 of tile frame f (zero for frames past the
+// tile's valid ones).  Lane l of warp w takes n1 = l % 16 and the 16 n2 of parity h = l / 16 of frame
+// 8 p + w (p = pass), so the 32 lanes read 32 consecutive buffer samples, and writes them as K indices
+// 16 h .. 16 h + 15: the even n2 first, then the odd ones (B1 uses the same order).
 __device__ __forceinline__ void tc_build_a1(unsigned char* A, const float* __restrict__ s_data,
-                                            const float* __restrict__ s_win, int hop, int off, int Tv)
+                                            const float* __restrict__ s_win, int hop, int off, int Tv,
+                                            float* __restrict__ s_scale)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n1 = lane & 15, h = lane >> 4;
@@ -144,16 +159,19 @@ __device__ __forceinline__ void tc_build_a1(unsigned char* A, const float* __res
 #pragma unroll
             for (int m = 0; m < 16; ++m) v[m] = 0.f;
         }
+        // the warp holds the whole frame: scale it by a power of two so its largest |value| lies in
+        // [0.5, 1) (F16 range for both stages: |Y| <= 32); the power is scaled back in epilogue 2
+        float m = 0.f;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) m = fmaxf(m, fabsf(v[i]));
+        m = warp_max(m);
+        int ex = int((__float_as_uint(m) >> 23) & 0xFFu) - 126;   // m = [0.5, 1) * 2^ex for normal m
+        ex = m > 0.f ? min(max(ex, -120), 120) : -120;
+        const float sc = __uint_as_float(uint32_t(127 - ex) << 23);
+        if (lane == 0) s_scale[f] = __uint_as_float(uint32_t(127 + ex) << 23);
         uint32_t hi[8], lo[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
-        {
-            const float send = h ? v[i] : v[8 + i];
-            const float recv = __shfl_xor_sync(0xffffffffu, send, 16);
-            const float e = h ? recv : v[i];        // n2 = 16 h + 2 i
-            const float o = h ? v[8 + i] : recv;    // n2 = 16 h + 2 i + 1
-            tc::split_bf16x2(e, o, hi[i], lo[i]);
-        }
+        for (int i = 0; i < 8; ++i) tc::split_f16x2(v[2 * i] * sc, v[2 * i + 1] * sc, hi[i], lo[i]);
         unsigned char* t = A + j * kTcTile;
         const int r = q + 8 * f;
         *reinterpret_cast<uint4*>(t + tc::sw128(r, 32 * h)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
@@ -202,14 +220,14 @@ __device__ __forceinline__ void tc_epilogue1(unsigned char* A, uint32_t tmem, co
             else
             {
                 // Y * W512^(n1 k2), W = c - i s
-                const float2 t = w512[(8 * jj + q) * k2];
+                const float2 t = w512[(8 * jj + q) * 17 + k2];
                 y[jj][0] = fmaf(yr, t.x, yi * t.y);
                 y[jj][1] = fmaf(yi, t.x, -yr * t.y);
             }
         }
         uint32_t h0, l0, h1, l1;
-        tc::split_bf16x2(y[0][0], y[0][1], h0, l0);
-        tc::split_bf16x2(y[1][0], y[1][1], h1, l1);
+        tc::split_f16x2(y[0][0], y[0][1], h0, l0);
+        tc::split_f16x2(y[1][0], y[1][1], h1, l1);
         *reinterpret_cast<uint2*>(A + 2048 * k2 + offHi) = make_uint2(h0, h1);
         *reinterpret_cast<uint2*>(A + 2048 * k2 + offLo) = make_uint2(l0, l1);
     }
@@ -217,7 +235,9 @@ __device__ __forceinline__ void tc_epilogue1(unsigned char* A, uint32_t tmem, co
 
 // Epilogue 2: stage-2 accumulator i of this thread's row (f, q') holds X[32 k1 + k2], k2 = 8 i + q',
 // k1 = 0..15; the needed bins (<= 256) go to the power tile.
-__device__ __forceinline__ void tc_epilogue2(uint32_t tmem, int i, float* __restrict__ s_out, int power)
+template <bool MAGNITUDE>
+__device__ __forceinline__ void tc_epilogue2(uint32_t tmem, int i, float* __restrict__ s_out,
+                                             const float* __restrict__ s_scale)
 {
     constexpr int LD = StftShape<kTcNfft, kFusedThreads, kTcTF>::OUT_LD;
     const int lane = threadIdx.x & 31, quarter = (threadIdx.x >> 5) & 3;
@@ -228,6 +248,7 @@ __device__ __forceinline__ void tc_epilogue2(uint32_t tmem, int i, float* __rest
     tc::tmem_ld32(tmem + (uint32_t(32 * quarter) << 16) + kTcD2 + 32 * i, v);
     tc::tmem_ld_wait();
     if (i == 2 && qp != 0) return;   // tile 2 holds k2 = 16 in rows q' = 0 only
+    const float u = s_scale[f];      // the frame's scale: X = u * (the accumulator)
     float* lo = s_out + k2 * LD + f;                 // bins 32 k1 + k2
     float* hi = s_out + (kTcNfft - k2) * LD + f;     // bins 512 - 32 k1 - k2
 #pragma unroll
@@ -235,7 +256,7 @@ __device__ __forceinline__ void tc_epilogue2(uint32_t tmem, int i, float* __rest
     {
         const float re = __uint_as_float(v[2 * k1]), im = __uint_as_float(v[2 * k1 + 1]);
         float p = fmaf(re, re, im * im);
-        if (power == 1) p = sqrtf(p);
+        p = MAGNITUDE ? sqrtf(p) * u : p * (u * u);
         if (k1 < 8) lo[32 * k1 * LD] = p;
         else if (k2 == 0 && k1 == 8) lo[32 * 8 * LD] = p;   // bin 256
         else if (k2 != 0 && k2 != 16) hi[-32 * k1 * LD] = p;
@@ -259,6 +280,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     unsigned char* sB1 = smem + lay.b1;
     unsigned char* sB2 = smem + lay.b2;
     float2* s_w512 = reinterpret_cast<float2*>(smem + lay.w512);
+    float* s_scale = reinterpret_cast<float*>(smem + lay.scale);
     float* s_win = reinterpret_cast<float*>(smem + lay.win);
     float* s_span = reinterpret_cast<float*>(smem + lay.span);
     float* s_out = reinterpret_cast<float*>(smem + lay.out);
@@ -306,15 +328,18 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     const int fcol = 2 * (threadIdx.x % (TF / 2));   // first of the two frame columns this thread owns in mel tiles
     const int g = threadIdx.x / (TF / 2);
 
-    // one bounded wait for the MMAs committed last; every thread learns whether any thread timed out
+    // one bounded wait for the MMAs committed last: thread 0 polls the mbarrier (the others wait at the
+    // barrier, issuing nothing), and the barrier hands its observation of the MMAs' completion to every
+    // thread, each of which then orders its tensor-memory reads after it (fence::after_thread_sync)
     auto wait_mma = [&]() -> bool {
-        const bool ok = tc::mbar_wait(&s_bar, phase, kTcWaitLimit);
-        if (ok)
+        bool ok = true;
+        if (threadIdx.x == 0) ok = tc::mbar_wait(&s_bar, phase, kTcWaitLimit);
+        const bool bad = __syncthreads_or(!ok);
+        if (!bad)
         {
             phase ^= 1u;
             pending = 0;
         }
-        const bool bad = __syncthreads_or(!ok);
         tc::fence_after();
         if (bad && threadIdx.x == 0) atomicOr(errorWord, 4);
         return !bad;
@@ -360,7 +385,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                 const int Tv = min(TF, it.F - f0);
                 // span -> stage-1 operand (the span barrier also ends the previous tile's mel reads)
                 stft_stage_span<kTcNfft, kFusedThreads, TFX>(src, f0, it.F, a.W, a.hop, centerOffset, s_span);
-                tc_build_a1(sA, s_span + S::span_pad(a.W), s_win, a.hop, off, Tv);
+                tc_build_a1(sA, s_span + S::span_pad(a.W), s_win, a.hop, off, Tv, s_scale);
                 tc::fence_async_smem();
                 __syncthreads();
                 if (threadIdx.x == 0)
@@ -373,12 +398,12 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                         const uint64_t dA = tc::desc_sw128(tc::smem_addr(sA + j * kTcTile));
                         const uint32_t d = tmem + kTcD1 + 32 * j;
                         // K steps of 32 bytes: hi at +0, +32; lo at +64, +96 (descriptor units of 16 bytes)
-                        tc::mma_bf16(d, dA + 0, dB + 0, kTcIdesc, 0u);
-                        tc::mma_bf16(d, dA + 2, dB + 2, kTcIdesc, 1u);
-                        tc::mma_bf16(d, dA + 0, dB + 4, kTcIdesc, 1u);
-                        tc::mma_bf16(d, dA + 2, dB + 6, kTcIdesc, 1u);
-                        tc::mma_bf16(d, dA + 4, dB + 0, kTcIdesc, 1u);
-                        tc::mma_bf16(d, dA + 6, dB + 2, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 0, dB + 0, kTcIdesc, 0u);
+                        tc::mma_f16(d, dA + 2, dB + 2, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 0, dB + 4, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 2, dB + 6, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 4, dB + 0, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 6, dB + 2, kTcIdesc, 1u);
                     }
                     tc::commit(&s_bar);
                 }
@@ -403,12 +428,12 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                     {
                         const uint64_t dA = tc::desc_sw128(tc::smem_addr(sA + i * kTcTile));
                         const uint32_t d = tmem + kTcD2 + 32 * i;
-                        tc::mma_bf16(d, dA + 0, dB + 0, kTcIdesc, 0u);
-                        tc::mma_bf16(d, dA + 2, dB + 2, kTcIdesc, 1u);
-                        tc::mma_bf16(d, dA + 0, dB + 4, kTcIdesc, 1u);
-                        tc::mma_bf16(d, dA + 2, dB + 6, kTcIdesc, 1u);
-                        tc::mma_bf16(d, dA + 4, dB + 0, kTcIdesc, 1u);
-                        tc::mma_bf16(d, dA + 6, dB + 2, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 0, dB + 0, kTcIdesc, 0u);
+                        tc::mma_f16(d, dA + 2, dB + 2, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 0, dB + 4, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 2, dB + 6, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 4, dB + 0, kTcIdesc, 1u);
+                        tc::mma_f16(d, dA + 6, dB + 2, kTcIdesc, 1u);
                     }
                     tc::commit(&s_bar);
                 }
@@ -420,8 +445,16 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                 }
                 // epilogue 2: warps 0-3 take k2 = q' (tile 0), warps 4-7 k2 = 8 + q' (tile 1); warp 0
                 // also k2 = 16 (tile 2)
-                tc_epilogue2(tmem, threadIdx.x < 128 ? 0 : 1, s_out, a.power);
-                if (threadIdx.x < 32) tc_epilogue2(tmem, 2, s_out, a.power);
+                if (a.power == 1)
+                {
+                    tc_epilogue2<true>(tmem, threadIdx.x < 128 ? 0 : 1, s_out, s_scale);
+                    if (threadIdx.x < 32) tc_epilogue2<true>(tmem, 2, s_out, s_scale);
+                }
+                else
+                {
+                    tc_epilogue2<false>(tmem, threadIdx.x < 128 ? 0 : 1, s_out, s_scale);
+                    if (threadIdx.x < 32) tc_epilogue2<false>(tmem, 2, s_out, s_scale);
+                }
                 tc::fence_before();
                 __syncthreads();
                 if (fcol < Tv)
@@ -545,7 +578,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     }
 
     // leave: after a timeout, wait once more (bounded) for the MMAs in flight, then free tensor memory
-    if (pending) tc::mbar_wait(&s_bar, phase, kTcWaitLimit);
+    if (pending && threadIdx.x == 0) tc::mbar_wait(&s_bar, phase, kTcWaitLimit);
     tc::fence_before();
     __syncthreads();
     if (threadIdx.x < 32) tc::tmem_dealloc<kTcTmemCols>(tmem);
@@ -586,8 +619,40 @@ void launch_frontend_tc(Handle& h, const FrontendArgs& a, void* scratch, uint4* 
     launch_ragged_prefix(SlotCount<kTcTF>{a, a.n, a.lookahead}, nslots, prefix, h.stream(),
                          reinterpret_cast<unsigned*>(counter), int(clear / 4));
     const void* k = reinterpret_cast<const void*>(frontend_tc_kernel<kTcTF>);
-    int grid = persistent_grid(h, k, kFusedThreads, smem);
-    grid = std::min(grid, 2 * h.num_sms());   // two CTAs per SM at most: 2 x 256 tensor-memory columns
+    // two CTAs need 2 x ~100 KB of shared memory: ask for the largest carveout, or the driver may pick
+    // one that holds a single CTA (a function attribute of this kernel only)
+    {
+        static std::mutex mu;
+        static std::set<int> done;
+        std::lock_guard<std::mutex> lock(mu);
+        if (done.insert(h.device()).second)
+            check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            int(cudaSharedmemCarveoutMaxShared)),
+                       "shared memory carveout");
+    }
+    persistent_grid(h, k, kFusedThreads, smem);   // sets the kernel's shared-memory opt-in
+    // CTAs per SM: two (registers: 256 threads x 128; tensor memory: 2 x 256 columns) when their shared
+    // memory fits the SM, counted directly (the occupancy query reports one for this kernel, while two
+    // run side by side)
+    int perSm = 2;
+    {
+        static std::mutex mu;
+        static std::map<int, std::pair<int, size_t>> smInfo;   // device -> (shared memory per SM, static)
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = smInfo.find(h.device());
+        if (it == smInfo.end())
+        {
+            int perSmBytes = 0;
+            check_cuda(cudaDeviceGetAttribute(&perSmBytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h.device()),
+                       "shared memory per SM");
+            cudaFuncAttributes fa{};
+            check_cuda(cudaFuncGetAttributes(&fa, k), "cudaFuncGetAttributes");
+            it = smInfo.emplace(h.device(), std::make_pair(perSmBytes, size_t(fa.sharedSizeBytes))).first;
+        }
+        const size_t perCta = smem + it->second.second + 1024;   // + the driver's reserved 1 KB per CTA
+        perSm = std::max(1, std::min(2, int(size_t(it->second.first) / perCta)));
+    }
+    int grid = perSm * h.num_sms();
     if (a.ctasPerSm > 0) grid = std::min(grid, a.ctasPerSm * h.num_sms());
     if (a.reserveSms > 0 && a.reserveSms < h.num_sms())
         grid = std::max(1, grid / h.num_sms() * (h.num_sms() - a.reserveSms));

@@ -50,8 +50,15 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
     return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
 }
 
-// D[tmem] (+)= A[a] x B[b]^T, issued by one thread.
-__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+// The same with F16 A and B (format 0).
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N)
+{
+    return (1u << 4) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[a] x B[b]^T, issued by one thread (kind::f16: BF16 or F16 operands, as the
+// instruction descriptor says; both operands of one MMA have the same type).
+__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -160,6 +167,29 @@ __device__ __forceinline__ void split_bf16x2(float a, float b, uint32_t& hi, uin
 {
     hi = pack_bf16x2(a, b);
     lo = pack_bf16x2(a - bf16_lo(hi), b - bf16_hi(hi));
+}
+
+// (lo, hi) -> one 32-bit word of two F16 values, each rounded to nearest even; lo in bits 0-15.
+__device__ __forceinline__ uint32_t pack_f16x2(float lo, float hi)
+{
+    uint32_t d;
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+__device__ __forceinline__ void unpack_f16x2(uint32_t w, float& lo, float& hi)
+{
+    asm("{\n\t.reg .f16 a, b;\n\tmov.b32 {a, b}, %2;\n\tcvt.f32.f16 %0, a;\n\tcvt.f32.f16 %1, b;\n\t}"
+        : "=f"(lo), "=f"(hi)
+        : "r"(w));
+}
+// x = hi + lo split of two floats into F16 words: hi = f16(x), lo = f16(x - hi).  For |x| <= 2^15 the
+// pair keeps x to about 2^-22 |x| (and 2^-25 absolute, where lo falls into the F16 subnormals).
+__device__ __forceinline__ void split_f16x2(float a, float b, uint32_t& hi, uint32_t& lo)
+{
+    hi = pack_f16x2(a, b);
+    float ha, hb;
+    unpack_f16x2(hi, ha, hb);
+    lo = pack_f16x2(a - ha, b - hb);
 }
 
 }  // namespace tc

@@ -175,7 +175,7 @@ assert ctypes.sizeof(RppbFrontendParams) == 88   # sizeof in C (the engine field
 
 # RppbSpectrumEngine
 ENGINE_FP32_FFT = 0
-ENGINE_TENSOR_CORE_BF16X3 = 1
+ENGINE_TENSOR_CORE_F16X3 = 1
 
 
 def frontend_params(nfft=512, window_length=400, window_step=160, num_filter=128, sample_rate=16000.0,
