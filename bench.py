@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--profile", action="store_true", help="run each entry point once for ncu captures, then exit")
     p.add_argument("--profile-repeat", type=int, default=1)
     p.add_argument("--profile-only", default="", help="with --profile: only entry points whose name contains this")
-    p.add_argument("--serve-requests", type=int, default=600,
+    p.add_argument("--serve-requests", type=int, default=5000,
                    help="requests per offered-load point of the serving measurement (0 skips it)")
     return p.parse_args()
 
@@ -288,6 +288,81 @@ class Fused:
         return self.out
 
 
+def tensor_core_engine(torch, h, chain, x, x_np, lens_np, plain_ms, fp32_ms, fp32_db, steps):
+    """The fused call with the tensor-core spectrum engine (rppb_frontend_gpu, spectrumEngine 1: the
+    512-point DFT factored 16 x 32 into two F16 hi/lo x3 GEMM stages on tcgen05) on the same batch:
+    device time per call (CUDA events, autotuned schedule), against the plain four calls and the FP32
+    engine; mel power error against the FP64 oracle chain on 8 clips (decibels read back as power with
+    reference 1 and a -200 dB cutoff); decibel difference from the FP32 engine on the full batch where the
+    mel power is within 60 dB of its frame maximum; tensor-pipe work issued."""
+    from oracle import Oracle
+    from rpp_b200 import audio
+    from rpp_b200.types import ENGINE_TENSOR_CORE_F16X3, frontend_params
+    c = chain
+    n = len(lens_np)
+    p = frontend_params(engine=ENGINE_TENSOR_CORE_F16X3)
+    out = torch.empty_like(c.db)
+    tuned = None
+    st, tms = audio.frontend_tune(x, c.sd, out, c.md, c.lens, c.coeff, p, h)
+    if st == 0:
+        tuned = {"tile_frames": p.tileFrames, "db_frames": p.dbFrames, "lookahead": p.lookahead,
+                 "ctas_per_sm": p.ctasPerSm, "tuner_best_ms": tms}
+    for _ in range(3):
+        assert audio.frontend(x, c.sd, out, c.md, c.lens, c.coeff, p, h) == 0
+    torch.cuda.synchronize()
+    a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a_.record()
+    for _ in range(steps):
+        assert audio.frontend(x, c.sd, out, c.md, c.lens, c.coeff, p, h) == 0
+    b_.record()
+    torch.cuda.synchronize()
+    ms = a_.elapsed_time(b_) / steps
+    assert audio.device_error(h) == 0
+    clip_s = float(lens_np.sum()) / RATE
+    # decibels against the FP32 engine, full batch
+    tc_db = out.cpu().numpy()
+    F = frames_of(lens_np)
+    worst_near, worst = 0.0, 0.0
+    for i in range(n):
+        a, b = fp32_db[i, :, :F[i]], tc_db[i, :, :F[i]]
+        d = np.abs(a.astype(np.float64) - b)
+        near = a >= a.max(axis=0, keepdims=True) - 60.0
+        worst_near = max(worst_near, float(d[near].max()))
+        worst = max(worst, float(d.max()))
+    # mel power against FP64 on 8 clips (the four longest and four others)
+    idx = np.sort(np.concatenate([np.argsort(lens_np)[-4:], np.arange(4)]))
+    xs = np.ascontiguousarray(x_np[idx, :int(lens_np[idx].max())])
+    ls = np.ascontiguousarray(lens_np[idx])
+    Fs = frames_of(ls)
+    mf = int(Fs.max())
+    pm = frontend_params(engine=ENGINE_TENSOR_CORE_F16X3, cut_off_db=-200.0, reference_magnitude=1.0)
+    from rpp_b200.types import audio_desc as _ad, spectra_desc as _sd
+    o = torch.empty((len(idx), NMEL, mf), device="cuda")
+    assert audio.frontend(torch.from_numpy(xs).cuda(), _ad(len(idx), xs.shape[1]), o, _sd(len(idx), NMEL, mf),
+                          torch.from_numpy(ls).cuda(), torch.full((len(idx),), COEFF, device="cuda"), pm, h) == 0
+    got = 10.0 ** (o.cpu().numpy().astype(np.float64) / 10.0)
+    orc = Oracle()
+    spec64 = orc.spectrogram_f64(xs, ls, 1, 1, None, NFFT, 2, WIN, HOP, 1, max_frames=mf,
+                                 preemph_coeff=np.full(len(idx), COEFF, np.float32), border=0)
+    dims = np.stack([np.full(len(idx), NFFT // 2 + 1, np.int32), Fs], 1).astype(np.int32).ravel()
+    mel64 = orc.mel_filter_bank_f64(spec64, dims, 8000.0, 0.0, 0, NMEL, float(RATE), 1)
+    mel_err = 0.0
+    for i in range(len(idx)):
+        g = got[i, :, :Fs[i]]
+        g[g <= 1.0001e-20] = 0.0
+        e = mel64[i, :, :Fs[i]]
+        scale = np.maximum(e.max(axis=0, keepdims=True), max(1e-12 * e.max(), 1e-30))
+        mel_err = max(mel_err, float((np.abs(g - e) / scale).max()))
+    tiles = int(np.sum(-(-F.astype(np.int64) // 16)))
+    flops = tiles * 30 * (2.0 * 128 * 32 * 16)   # 30 MMAs of M 128, N 32, K 16 per 16-frame tile
+    return {"engine": "tcgen05 factored DFT (16 x 32), F16 hi/lo x3, FP32 accumulate; mel + dB on CUDA cores",
+            "ms_per_step": ms, "value": clip_s / (ms / 1e3), "unit": "clip-s/s",
+            "over_plain": plain_ms / ms, "over_fp32_engine": fp32_ms / ms, "schedule": tuned,
+            "mel_power_rel_err_per_frame_vs_fp64": mel_err, "err_clips": int(len(idx)),
+            "db_diff_vs_fp32_engine_within_60db": worst_near, "db_diff_vs_fp32_engine_max": worst,
+            "tensor_tflops_issued": flops / (ms / 1e3) / 1e12}
+
+
 def error_vs_fp64(chain, x_np, lens_np, clips=8, db_out=None):
     """Max errors of the GPU chain against the FP64 oracle chain on the first `clips` clips."""
     from oracle import Oracle
@@ -320,27 +395,34 @@ def error_vs_fp64(chain, x_np, lens_np, clips=8, db_out=None):
 
 
 def serving_measurement(torch, n_requests):
-    """Serving: continuous-batching server (rpp_b200/serving.py) over a 40 GB device budget;
-    capacity from a closed burst, then open-loop Poisson arrivals at 10-90 % of it."""
+    """Serving: continuous-batching server (rpp_b200/serving.py) over a 40 GB device budget, with each step
+    run by the fused front end and, for comparison on the same GPU, by the plain FP32 path (resample + the
+    four rppt_*_gpu calls on a batch buffer); per mode the capacity from a closed burst, then open-loop
+    Poisson arrivals at 10-90 % of it, n_requests per load point."""
     from rpp_b200 import serving
     rng = np.random.Generator(np.random.PCG64(20261203 + 4))
     pool = serving.ClipPool(torch, rng)
-    server = serving.FrontendServer(torch, budget_bytes=40 << 30, max_clips=256, tables=4)
-    serving.measure(torch, server, pool, rng, 64)                       # warm-up, graph capture
-    cap, _ = serving.measure(torch, server, pool, rng, n_requests)      # closed burst: capacity
     mean_cs = np.mean([serving.clip_seconds(pool.request(i, rng)) for i in range(2000)])
-    loads = []
-    for frac in (0.1, 0.3, 0.5, 0.7, 0.9):
-        rate = frac * cap / mean_cs
-        thr, lat = serving.measure(torch, server, pool, rng, n_requests, rate_per_s=rate)
-        loads.append({"offered": frac, "requests_per_s": rate, "clip_s_per_s": thr,
-                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
-    server.close()
-    return {"capacity_clip_s_per_s": cap, "mean_request_clip_s": float(mean_cs), "requests_per_point": n_requests,
-            "budget_gb": 40, "chain": "resample (Kaiser sinc, 16 zero crossings) -> pre-emphasis -> STFT(512, 400, "
-            "160) -> mel(128) -> dB, one captured graph per step over a device clip table; native scheduler thread "
-            "(include/rppb_server.h)",
-            "latency": "host clock from arrival to output copy complete", "loads": loads}
+    modes = {}
+    for mode, plain in (("fused", False), ("plain_fp32", True)):
+        server = serving.FrontendServer(torch, budget_bytes=40 << 30, max_clips=256, tables=4, plain=plain)
+        serving.measure(torch, server, pool, rng, 64)                       # warm-up
+        cap, _ = serving.measure(torch, server, pool, rng, n_requests)      # closed burst: capacity
+        loads = []
+        for frac in (0.1, 0.3, 0.5, 0.7, 0.9):
+            rate = frac * cap / mean_cs
+            thr, lat = serving.measure(torch, server, pool, rng, n_requests, rate_per_s=rate)
+            loads.append({"offered": frac, "requests_per_s": rate, "clip_s_per_s": thr,
+                          "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
+        server.close()
+        modes[mode] = {"capacity_clip_s_per_s": cap, "loads": loads}
+    f = modes["fused"]
+    return {"capacity_clip_s_per_s": f["capacity_clip_s_per_s"], "loads": f["loads"], "modes": modes,
+            "mean_request_clip_s": float(mean_cs), "requests_per_point": n_requests, "budget_gb": 40,
+            "chain": "resample (Kaiser sinc, 16 zero crossings) -> pre-emphasis -> STFT(512, 400, 160) -> mel(128) -> "
+                     "dB, one captured graph per step over a device clip table; native scheduler thread "
+                     "(include/rppb_server.h); pinned clips and outputs moved by copy kernels",
+            "latency": "host clock from arrival to output copy complete"}
 
 
 def multirate_measurement(torch, h, steps=10, n=2048):
@@ -634,6 +716,33 @@ def read_traffic(kernel, name="dram_traffic.txt"):
     return None
 
 
+def summary_block(plain_ms, fused_ms, tce, par, nsr, serve, e2e):
+    """The headline results in a few keys (repeated from the detailed blocks above them)."""
+    out = {"plain_ms": plain_ms, "fused_fp32_ms": fused_ms, "fused_fp32_over_plain": plain_ms / fused_ms,
+           "e2e_ms": e2e.get("ms_per_step")}
+    if isinstance(tce, dict) and "ms_per_step" in tce:
+        out.update({"fused_tensor_core_ms": tce["ms_per_step"], "fused_tensor_core_over_plain": tce["over_plain"],
+                    "tensor_core_mel_err_vs_fp64": tce["mel_power_rel_err_per_frame_vs_fp64"]})
+    if isinstance(par, dict) and "plain_chain" in par:
+        pc = par["plain_chain"]
+        out["parity_vs_reference"] = {
+            "pre_emphasis_bit_exact": pc.get("pre_emphasis_bit_exact"),
+            "spectrogram_err": pc.get("spectrogram_power_rel_err_per_frame_max"),
+            "mel_err": pc.get("mel_power_rel_err_per_frame_max"),
+            "db_max": pc.get("db_max_abs_err"), "db_max_within_60db": pc.get("db_max_abs_err_within_60db_of_frame_max"),
+            "db_share_above_1e-3": pc.get("db_share_above_1e-3"),
+            "fused_db_max_within_60db": par.get("fused", {}).get("db_max_abs_err_within_60db_of_frame_max"),
+            "nsr_bit_exact": par.get("nsr", {}).get("bit_exact")}
+    if isinstance(nsr, dict) and "ms" in nsr:
+        out["nsr_ms"] = nsr["ms"]
+    if isinstance(serve, dict) and "modes" in serve:
+        out["serving"] = {m: {"capacity_clip_s_per_s": v["capacity_clip_s_per_s"],
+                              "p50_p99_ms": {str(l["offered"]): [round(l["p50_ms"], 3), round(l["p99_ms"], 3)]
+                                             for l in v["loads"]}}
+                          for m, v in serve["modes"].items()}
+    return out
+
+
 def nsr_measurement(torch, h, x, lens_np, steps=10):
     """rppt_non_silent_region_detection_gpu on the raw benchmark clips (-60 dB, window 2048, reset 8192):
     device time (CUDA events, median of `steps`) and the detected (begin, length) per clip."""
@@ -835,6 +944,13 @@ def run_b200(args, world, rank, local):
                      "issue_floor_ms": floor_ms, "issue_frac": floor_ms / ms_step,
                      "source": "profiles/issue_counts.txt (ncu smsp__inst_executed.sum of one launch)"}
         err = error_vs_fp64(chain, x_np, lens_np, db_out=fused.out)
+        fused.run(x)
+        torch.cuda.synchronize()
+        try:
+            tce = tensor_core_engine(torch, h, chain, x, x_np, lens_np, plain_ms, ms_step, fused.out.cpu().numpy(),
+                                     args.steps)
+        except Exception as exc:
+            tce = {"error": repr(exc)}
         try:
             nsr, nsr_b, nsr_l = nsr_measurement(torch, h, x, lens_np)
         except Exception as exc:
@@ -892,15 +1008,18 @@ def run_b200(args, world, rank, local):
                             "path": "four rppt_*_gpu C-ABI calls per step",
                             "algorithmic_bytes_per_step": sum(ab.values()),
                             "frac_of_hbm": sum(ab.values()) / (plain_ms / 1e3) / 1e9 / hbm, "per_op": per_op},
-            "fused_over_plain": plain_ms / ms_step,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            # detailed blocks first; the compact results last (the end of the line is what a truncated log keeps)
+            "precision": precision,
+            "multirate": multirate,
+            "serving": serve,
             "err_vs_fp64": err,
             "parity_vs_reference": parity_ref,
             "nsr": nsr,
-            "cpu_baseline": cpu,
-            "e2e": e2e,
-            "multirate": multirate,
-            "serving": serve,
-            "precision": precision,
+            "tensor_core_engine": tce,
+            "summary": summary_block(plain_ms, ms_step, tce, parity_ref, nsr, serve, e2e),
+            "fused_over_plain": plain_ms / ms_step,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

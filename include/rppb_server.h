@@ -6,13 +6,19 @@
  * scheduler thread owned by the server
  *   - admits requests first come, first served when all their device buffers (input at its rate,
  *     the outRate signal, the decibel output) fit in a fixed device arena (the memory budget);
- *   - copies each admitted request's clips in on an upload stream;
+ *   - copies each admitted request's clips in on an upload stream: clips in pinned (device-mapped)
+ *     memory are read by one copy kernel per admission round, pageable ones by one DMA copy each;
  *   - runs steps on a compute stream: every uploaded, not yet processed clip (up to maxClipsPerStep)
  *     gets an entry in a pinned clip table, and one CUDA graph (table copy + rppb_frontend_clips_gpu:
  *     resample -> pre-emphasis -> STFT -> mel -> decibels) is replayed; up to `tables` steps are in
  *     flight and requests that arrive meanwhile join the next step;
  *   - copies each finished clip's decibels [numFilter][frames] to the request's output on a
- *     download stream, and reports the request complete when all of its copies have ended.
+ *     download stream (one copy kernel per retired step for pinned outputs, a DMA copy each for
+ *     pageable ones), and reports the request complete when all of its copies have ended.
+ * Two step paths: the fused front end (rppb_frontend_clips_gpu), or, with plainChain set, the plain
+ * FP32 path -- resample, then the four calls rppt_pre_emphasis_filter_gpu, rppt_spectrogram_gpu,
+ * rppt_mel_filter_bank_gpu and rppt_to_decibels_gpu on a batch buffer of maxClipsPerStep rows of
+ * maxSamples samples (the clips are copied in and the decibels out by kernels).
  * Every clip's result depends only on that clip, so a request gives the same bits alone and in any
  * mix of requests.  Host clip and output buffers must stay valid until the request completes;
  * pinned memory lets the copies run asynchronously.
@@ -41,6 +47,8 @@ typedef struct
     Rpp32s lobes;
     Rpp32f preemphCoeff;
     RppbFrontendParams params; /* windowFunction must be null (Hann) */
+    Rpp32s plainChain;         /* 0: fused front end; 1: the plain FP32 four-call path per step */
+    Rpp32s maxSamples;         /* plain path: longest clip at outRate (0: 30 s); longer requests are refused */
 } RppbServerConfig;
 
 typedef struct

@@ -683,12 +683,13 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost,
     });
 }
 
-extern "C" SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips, Rpp32s numClips, Rpp32f outRate,
-                                                           const Rpp32f* lookup, Rpp32s lookupSize, Rpp32f scale,
-                                                           Rpp32f center, Rpp32s lobes, Rpp32f preemphCoeff,
-                                                           const RppbFrontendParams* params, rppHandle_t rppHandle)
+namespace rppb {
+
+RppStatus frontend_clips(Handle& h, const RppbClip* clips, int numClips, float outRate, const float* lookup,
+                         int lookupSize, float scale, float center, int lobes, float preemphCoeff,
+                         const RppbFrontendParams* params, int reserveSms)
 {
-    return guarded(rppHandle, [&](Handle& h) {
+    {
         require(clips != nullptr && params != nullptr, "null clip table or parameters");
         require(lookup != nullptr && lookupSize >= 2 && lobes >= 0, "invalid resampling window");
         require(size_t(lookupSize) * sizeof(float) <= 200 * 1024, "lookup table above 200 KB");
@@ -734,8 +735,22 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips
         a.clips = dclips;
         a.outRate = outRate;
         a.coeffAll = preemphCoeff;
+        a.reserveSms = reserveSms;
         launch_frontend(h, scratch, a);
         return RPP_SUCCESS;
+    }
+}
+
+}  // namespace rppb
+
+extern "C" SHARED_PUBLIC RppStatus rppb_frontend_clips_gpu(const RppbClip* clips, Rpp32s numClips, Rpp32f outRate,
+                                                           const Rpp32f* lookup, Rpp32s lookupSize, Rpp32f scale,
+                                                           Rpp32f center, Rpp32s lobes, Rpp32f preemphCoeff,
+                                                           const RppbFrontendParams* params, rppHandle_t rppHandle)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        return frontend_clips(h, clips, numClips, outRate, lookup, lookupSize, scale, center, lobes, preemphCoeff,
+                              params, 0);
     });
 }
 

@@ -90,7 +90,68 @@ __global__ void __launch_bounds__(kMoverThreads) host_scatter_kernel(const float
     }
 }
 
+// A list of contiguous copies (host pinned <-> device, or device <-> device) done by one launch:
+// job j moves jobs[j].count floats from jobs[j].src to jobs[j].dst, split into segments of kSegment
+// floats numbered from jobs[j].unit0 (an exclusive scan of the segment counts, so the grid walks a
+// flat list of segments); 16-byte loads and stores where both ends are 16-byte aligned.  The job list
+// itself may sit in pinned host memory.
+__global__ void __launch_bounds__(kMoverThreads) copy_jobs_kernel(const CopyJob* __restrict__ jobs, int njobs,
+                                                                  long long units)
+{
+    for (long long u = blockIdx.x; u < units; u += gridDim.x)
+    {
+        int lo = 0, hi = njobs - 1;   // last job with unit0 <= u
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].unit0 <= u) lo = mid;
+            else hi = mid - 1;
+        }
+        const CopyJob jb = jobs[lo];
+        const long long s0 = (u - jb.unit0) * kSegment;
+        if (s0 >= jb.count) continue;
+        const int m = int(min((long long)kSegment, jb.count - s0));
+        const float* s = jb.src + s0;
+        float* d = jb.dst + s0;
+        if (((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(d)) & 15) == 0)
+        {
+            const int q = m >> 2;
+            const float4* s4 = reinterpret_cast<const float4*>(s);
+            float4* d4 = reinterpret_cast<float4*>(d);
+            constexpr int kUnroll = kSegment / 4 / kMoverThreads;
+            float4 v[kUnroll];
+#pragma unroll
+            for (int k = 0; k < kUnroll; ++k)
+            {
+                const int i = threadIdx.x + k * kMoverThreads;
+                if (i < q) v[k] = s4[i];
+            }
+#pragma unroll
+            for (int k = 0; k < kUnroll; ++k)
+            {
+                const int i = threadIdx.x + k * kMoverThreads;
+                if (i < q) d4[i] = v[k];
+            }
+            for (int i = (q << 2) + threadIdx.x; i < m; i += kMoverThreads) d[i] = s[i];
+        }
+        else
+        {
+            for (int i = threadIdx.x; i < m; i += kMoverThreads) d[i] = s[i];
+        }
+    }
+}
+
 }  // namespace
+
+long long copy_job_segments(long long count) { return (count + kSegment - 1) / kSegment; }
+
+void launch_copy_jobs(cudaStream_t stream, const CopyJob* jobs, int njobs, long long units, int ctas)
+{
+    if (njobs <= 0 || units <= 0) return;
+    copy_jobs_kernel<<<ctas, kMoverThreads, 0, stream>>>(jobs, njobs, units);
+    count_launch(1);
+    check_cuda(cudaGetLastError(), "copy_jobs_kernel");
+}
 
 void launch_host_gather(cudaStream_t stream, const float* src, size_t nStride, const int* len, int clips, float* dst,
                         uint32_t dstStride, int ctas)

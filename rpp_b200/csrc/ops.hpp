@@ -151,6 +151,11 @@ size_t frontend_scratch_bytes(int n, int lookahead, int numFilter);
 void launch_frontend(Handle& h, void* scratch, const FrontendArgs& a);
 // The tensor-core engine (fused_tc.cu): launched by launch_frontend for engine 1; `melScratch` holds the
 // mel tables when the handle's cache cannot provide them (stream capture with new parameters).
+// rppb_frontend_clips_gpu on a handle, leaving `reserveSms` SMs' worth of CTA slots of the fused kernel
+// to kernels on other streams (the server's copy movers).
+RppStatus frontend_clips(Handle& h, const RppbClip* clips, int numClips, float outRate, const float* lookup,
+                         int lookupSize, float scale, float center, int lobes, float preemphCoeff,
+                         const RppbFrontendParams* params, int reserveSms);
 bool frontend_tc_supported(const FrontendArgs& a);
 void launch_frontend_tc(Handle& h, const FrontendArgs& a, void* scratch, uint4* melScratch);
 
@@ -204,6 +209,18 @@ void launch_pcm16(Handle& h, const short* src, uint32_t srcStride, float* dst, u
                   int channels, int n);
 
 // PCIe movers over mapped pinned host memory (host_io.cu).
+// A contiguous copy of `count` floats for launch_copy_jobs (host_io.cu); unit0 = the segments of the
+// jobs before it (copy_job_segments per job, scanned).
+struct CopyJob
+{
+    const float* src;
+    float* dst;
+    long long count;
+    long long unit0;
+};
+long long copy_job_segments(long long count);
+// One launch that performs every job of `jobs` (device-visible memory: device, or pinned host).
+void launch_copy_jobs(cudaStream_t stream, const CopyJob* jobs, int njobs, long long units, int ctas);
 void launch_host_gather(cudaStream_t stream, const float* src, size_t nStride, const int* len, int clips, float* dst,
                         uint32_t dstStride, int ctas);
 void launch_host_scatter(cudaStream_t stream, const float* src, uint32_t srcNStride, uint32_t srcHStride,

@@ -3,10 +3,15 @@
 //
 // Scheduler round (repeated until stopped):
 //   finish  - requests whose output copies ended: stamp, free their arena blocks, report;
-//   retire  - steps whose graph ended: queue each clip's output copy on the download stream;
-//   admit   - FIFO: allocate every clip's block (input, outRate signal, decibels) or wait;
-//             queue the clip copies on the upload stream;
+//   retire  - steps whose graph ended: queue the clips' output copies on the download stream (one copy
+//             kernel over every pinned output of the round's steps, a DMA copy per pageable one);
+//   admit   - FIFO: allocate every clip's block (input, outRate signal, decibels) or wait; queue the
+//             clips' copies on the upload stream (one copy kernel over the round's pinned clips, a DMA
+//             copy per pageable one);
 //   step    - while a table is free and uploaded clips wait: fill the pinned table, replay its graph.
+// The copy kernels read their job lists from pinned rings (a slot is reused once its kernel ended) and
+// leave the fused kernel's CTA slots on kServerReserveSms SMs to run beside it.  Steps run either the
+// fused front end or, with plainChain, the plain four-call path on a batch buffer (plain_step below).
 // All CUDA state lives on the scheduler thread except creation and destruction.
 #include <algorithm>
 #include <atomic>
@@ -18,16 +23,86 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/rppb_server.h"
+#include "../../include/rppt_tensor_audio_augmentations.h"
 #include "common.cuh"
 #include "handle.hpp"
+#include "ops.hpp"
 
 namespace rppb {
 namespace {
 
 constexpr size_t kAlign = 256;
+constexpr int kJobCap = 4096;        // copy jobs per mover launch
+constexpr int kJobRing = 8;          // mover job lists in flight per direction
+constexpr int kMoverCtas = 32;
+constexpr int kServerReserveSms = 8; // SMs left to the movers beside the fused kernel
+constexpr int kSeg = 8192;           // floats per work unit of the plain path's copy kernels
+
+// Plain path, step input: clip b of the table (resampled into clips[b].work) -> row b of the batch
+// buffer, with the per-sample tensors of the four plain calls (length, coefficient, {bins, frames},
+// {frames, numFilter}).  Empty slots get length 0 and no frames.
+__global__ void clips_to_batch_kernel(const RppbClip* __restrict__ clips, int n, float outRate, int S, int Fmax,
+                                      float* __restrict__ xb, int* __restrict__ len, float* __restrict__ coeff,
+                                      float c, int* __restrict__ dims, uint32_t* __restrict__ patches, int bins,
+                                      int nf, int W, int hop, bool center)
+{
+    const int segs = (S + kSeg - 1) / kSeg;
+    for (long long u = blockIdx.x; u < (long long)n * segs; u += gridDim.x)
+    {
+        const int b = int(u / segs), sg = int(u % segs);
+        const RppbClip cl = clips[b];
+        const int L = cl.length <= 0 ? 0 : min(resampled_length(cl.length, cl.inRate, outRate), S);
+        if (sg == 0 && threadIdx.x == 0)
+        {
+            const int F = L <= 0 ? 0 : max(0, min(num_windows(L, W, hop, center), min(Fmax, cl.dstStride)));
+            len[b] = L;
+            coeff[b] = c;
+            dims[2 * b] = bins;
+            dims[2 * b + 1] = F;
+            patches[2 * b] = uint32_t(F);
+            patches[2 * b + 1] = uint32_t(nf);
+        }
+        const int i0 = sg * kSeg, i1 = min(L, i0 + kSeg);
+        for (int i = i0 + int(threadIdx.x); i < i1; i += blockDim.x) xb[size_t(b) * S + i] = cl.work[i];
+    }
+}
+
+// Plain path, step output: rows [numFilter][frames] of each clip's decibels -> the clip's dst (row
+// stride dstStride), a warp per (clip, row).
+__global__ void batch_to_clips_kernel(const float* __restrict__ db, int n, int nf, int Fmax,
+                                      const RppbClip* __restrict__ clips, const int* __restrict__ dims)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+    for (long long w = blockIdx.x * (long long)(blockDim.x / 32) + (threadIdx.x >> 5); w < (long long)n * nf;
+         w += warps)
+    {
+        const int b = int(w / nf), r = int(w % nf);
+        const RppbClip cl = clips[b];
+        const int F = dims[2 * b + 1];
+        if (cl.dst == nullptr || F <= 0) continue;
+        const float* s = db + (size_t(b) * nf + r) * Fmax;
+        float* d = cl.dst + size_t(r) * cl.dstStride;
+        for (int f = lane; f < F; f += 32) d[f] = s[f];
+    }
+}
+
+// Device address of a pinned (mapped) host buffer, or null for pageable memory.
+const void* mapped_address(const void* p)
+{
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (attr.type == cudaMemoryTypeHost) return attr.devicePointer;
+    return nullptr;
+}
 
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
@@ -95,6 +170,8 @@ struct Request
     std::vector<int> len;
     std::vector<float> rate;
     std::vector<float*> out;
+    std::vector<const float*> srcMapped;          // device address of a pinned clip (null: DMA copy)
+    std::vector<float*> outMapped;                // device address of a pinned output (null: DMA copy)
     std::vector<int> lr, frames;                  // outRate length and frames per clip
     std::vector<size_t> off, bytes;               // arena block per clip
     cudaEvent_t uploaded = nullptr, downloaded = nullptr;
@@ -130,6 +207,23 @@ struct RppbServer
     std::vector<cudaEvent_t> tableBusy;
     std::vector<bool> tableUsed;
     std::vector<cudaEvent_t> eventPool;
+    // copy-kernel job lists (pinned rings) per direction
+    struct JobRing
+    {
+        std::vector<CopyJob*> lists;
+        std::vector<cudaEvent_t> free;
+        std::vector<bool> used;
+        int next = 0;
+        CopyJob* cur = nullptr;
+        int slot = -1, count = 0;
+        long long units = 0;
+    } upRing, downRing;
+    // plain path buffers (plainChain)
+    int plainS = 0, plainF = 0, plainBins = 0;
+    float *xb = nullptr, *pb = nullptr, *spec = nullptr, *mel = nullptr, *db = nullptr, *pcoeff = nullptr;
+    int *plen = nullptr, *pdims = nullptr;
+    uint32_t* ppatches = nullptr;
+    void* rsScratch = nullptr;
 
     std::mutex mu;
     std::deque<Request*> submitted;
@@ -146,6 +240,7 @@ struct RppbServer
     std::deque<std::pair<Request*, int>> ready;
     std::deque<Step> inflight;
     std::vector<Request*> finishing;
+    std::vector<Request*> admitted;
     int nextTable = 0;
 
     int frames_of(int length, float rate, int* lr) const
@@ -168,6 +263,35 @@ struct RppbServer
         return e;
     }
     void give_event(cudaEvent_t e) { eventPool.push_back(e); }
+
+    // Adds a copy of `count` floats to the ring's current job list (launching the list first when full).
+    void add_job(JobRing& ring, cudaStream_t st, const float* src, float* dst, long long count)
+    {
+        if (count <= 0) return;
+        if (ring.cur && ring.count == kJobCap) flush_jobs(ring, st);
+        if (!ring.cur)
+        {
+            const int t = ring.next;
+            if (ring.used[t]) check_cuda(cudaEventSynchronize(ring.free[t]), "cudaEventSynchronize(job list)");
+            ring.cur = ring.lists[t];
+            ring.slot = t;
+            ring.count = 0;
+            ring.units = 0;
+        }
+        ring.cur[ring.count++] = CopyJob{src, dst, count, ring.units};
+        ring.units += copy_job_segments(count);
+    }
+    // Launches the ring's current job list on `st` (one kernel for all of its copies).
+    void flush_jobs(JobRing& ring, cudaStream_t st)
+    {
+        if (!ring.cur) return;
+        launch_copy_jobs(st, ring.cur, ring.count, ring.units, kMoverCtas);
+        check_cuda(cudaEventRecord(ring.free[ring.slot], st), "cudaEventRecord(job list)");
+        ring.used[ring.slot] = true;
+        ring.next = (ring.slot + 1) % int(ring.lists.size());
+        ring.cur = nullptr;
+        ring.count = 0;
+    }
 
     bool finish_round()
     {
@@ -203,6 +327,7 @@ struct RppbServer
     {
         bool work = false;
         const int nf = cfg.params.numFilter;
+        std::vector<Request*> completing;
         while (!inflight.empty())
         {
             Step& s = inflight.front();
@@ -213,18 +338,23 @@ struct RppbServer
             for (auto& [r, i] : s.clips)
             {
                 const size_t outOff = r->off[i] + align_up(size_t(r->len[i]) * 4) + align_up(size_t(r->lr[i] + 4) * 4);
-                check_cuda(cudaMemcpyAsync(r->out[i], arenaBase + outOff, size_t(nf) * std::max(r->frames[i], 1) * 4,
-                                           cudaMemcpyDeviceToHost, down),
-                           "cudaMemcpyAsync(output)");
-                if (++r->retired == int(r->src.size()))
-                {
-                    check_cuda(cudaEventRecord(r->downloaded, down), "cudaEventRecord(download)");
-                    finishing.push_back(r);
-                }
+                const long long count = (long long)nf * std::max(r->frames[i], 1);
+                const float* src = reinterpret_cast<const float*>(arenaBase + outOff);
+                if (r->outMapped[i]) add_job(downRing, down, src, r->outMapped[i], count);
+                else
+                    check_cuda(cudaMemcpyAsync(r->out[i], src, size_t(count) * 4, cudaMemcpyDeviceToHost, down),
+                               "cudaMemcpyAsync(output)");
+                if (++r->retired == int(r->src.size())) completing.push_back(r);
             }
             give_event(s.done);
             inflight.pop_front();
             work = true;
+        }
+        flush_jobs(downRing, down);
+        for (Request* r : completing)
+        {
+            check_cuda(cudaEventRecord(r->downloaded, down), "cudaEventRecord(download)");
+            finishing.push_back(r);
         }
         return work;
     }
@@ -255,16 +385,27 @@ struct RppbServer
             arenaUsed = arena->used();
             pending.pop_front();
             for (size_t c = 0; c < k; ++c)
-                if (r->len[c] > 0)
-                    check_cuda(cudaMemcpyAsync(arenaBase + r->off[c], r->src[c], size_t(r->len[c]) * 4,
-                                               cudaMemcpyHostToDevice, up),
+            {
+                if (r->len[c] <= 0) continue;
+                float* dst = reinterpret_cast<float*>(arenaBase + r->off[c]);
+                if (r->srcMapped[c]) add_job(upRing, up, r->srcMapped[c], dst, r->len[c]);
+                else
+                    check_cuda(cudaMemcpyAsync(dst, r->src[c], size_t(r->len[c]) * 4, cudaMemcpyHostToDevice, up),
                                "cudaMemcpyAsync(clip)");
+            }
+            admitted.push_back(r);
+            work = true;
+        }
+        // one copy kernel for the round's pinned clips, then each request's upload event after it
+        flush_jobs(upRing, up);
+        for (Request* r : admitted)
+        {
             r->uploaded = take_event();
             r->downloaded = take_event();
             check_cuda(cudaEventRecord(r->uploaded, up), "cudaEventRecord(upload)");
-            for (size_t c = 0; c < k; ++c) ready.emplace_back(r, int(c));
-            work = true;
+            for (size_t c = 0; c < r->src.size(); ++c) ready.emplace_back(r, int(c));
         }
+        admitted.clear();
         return work;
     }
 
@@ -322,6 +463,64 @@ struct RppbServer
             work = true;
         }
         return work;
+    }
+
+    static RpptDesc desc(int n, int h, int w, int numDims)
+    {
+        RpptDesc d{};
+        d.numDims = numDims;
+        d.offsetInBytes = 0;
+        d.dataType = F32;
+        d.n = Rpp32u(n);
+        d.c = 1;
+        d.h = Rpp32u(h);
+        d.w = Rpp32u(w);
+        d.strides.nStride = Rpp32u(h) * Rpp32u(w);
+        d.strides.hStride = Rpp32u(w);
+        d.strides.wStride = 1;
+        d.strides.cStride = 1;
+        d.layout = NFT;
+        return d;
+    }
+
+    // The plain FP32 path of one step on the compute stream: resample the table's clips, copy them into
+    // the batch buffer, the four plain calls (pre-emphasis, spectrogram, mel filter bank, decibels) on it,
+    // then copy each clip's decibels to its output block.  Captured once per table.
+    void plain_step(const RppbClip* table)
+    {
+        Handle& h = deref(handle);
+        const RppbFrontendParams& p = cfg.params;
+        const int n = cfg.maxClipsPerStep, nf = p.numFilter;
+        ResampleWindowDev win;
+        win.lut = lut;
+        win.lutSize = cfg.lookupSize;
+        win.scale = cfg.scale;
+        win.center = cfg.center;
+        win.lobes = cfg.lobes;
+        launch_resample_clips(h, rsScratch, table, n, cfg.outRate, win);
+        const int grid = 2 * h.num_sms();
+        clips_to_batch_kernel<<<grid, 256, 0, compute>>>(table, n, cfg.outRate, plainS, plainF, xb, plen, pcoeff,
+                                                         cfg.preemphCoeff, pdims, ppatches, plainBins, nf,
+                                                         p.windowLength, p.windowStep, p.centerWindows);
+        count_launch(1);
+        check_cuda(cudaGetLastError(), "clips_to_batch_kernel");
+        RpptDesc sd = desc(n, 1, plainS, 2), spd = desc(n, plainBins, plainF, 3), md = desc(n, nf, plainF, 3);
+        auto ok = [](RppStatus st, const char* what) {
+            if (st != RPP_SUCCESS) fail(st, std::string(what) + ": " + rppbGetLastError());
+        };
+        ok(rppt_pre_emphasis_filter_gpu(xb, &sd, pb, &sd, plen, pcoeff, p.borderType, handle), "pre_emphasis");
+        ok(rppt_spectrogram_gpu(pb, &sd, spec, &spd, plen, p.centerWindows, p.reflectPadding, nullptr,
+                                p.nfft ? p.nfft : p.windowLength, p.power, p.windowLength, p.windowStep, handle),
+           "spectrogram");
+        ok(rppt_mel_filter_bank_gpu(spec, &spd, mel, &md, pdims, p.maxFreq, p.minFreq, p.melFormula, nf, p.sampleRate,
+                                    p.normalize, handle),
+           "mel_filter_bank");
+        ok(rppt_to_decibels_gpu(mel, &md, db, &md, reinterpret_cast<RpptImagePatch*>(ppatches), p.cutOffDB,
+                                p.multiplier, p.referenceMagnitude, handle),
+           "to_decibels");
+        batch_to_clips_kernel<<<grid, 256, 0, compute>>>(db, n, nf, plainF, table, pdims);
+        count_launch(1);
+        check_cuda(cudaGetLastError(), "batch_to_clips_kernel");
     }
 
     void run()
@@ -402,6 +601,18 @@ void release(RppbServer* s)
     for (auto e : s->eventPool) cudaEventDestroy(e);
     for (auto p : s->hostTables)
         if (p) cudaFreeHost(p);
+    for (auto* ring : {&s->upRing, &s->downRing})
+    {
+        for (auto p : ring->lists)
+            if (p) cudaFreeHost(p);
+        for (auto e : ring->free)
+            if (e) cudaEventDestroy(e);
+    }
+    for (void* p : {static_cast<void*>(s->xb), static_cast<void*>(s->pb), static_cast<void*>(s->spec),
+                    static_cast<void*>(s->mel), static_cast<void*>(s->db), static_cast<void*>(s->pcoeff),
+                    static_cast<void*>(s->plen), static_cast<void*>(s->pdims), static_cast<void*>(s->ppatches),
+                    s->rsScratch})
+        if (p) cudaFree(p);
     for (auto p : s->devTables)
         if (p) cudaFree(p);
     if (s->handle) rppDestroy(s->handle, RPP_HIP_BACKEND);
@@ -439,6 +650,42 @@ extern "C" SHARED_PUBLIC RppStatus rppb_server_create(rppbServer_t* server, cons
         check_cuda(cudaMemcpy(s->lut, c.lookup, size_t(c.lookupSize) * 4, cudaMemcpyHostToDevice), "cudaMemcpy(lut)");
         if (rppCreate(&s->handle, size_t(c.maxClipsPerStep), 0, s->compute, RPP_HIP_BACKEND) != rppStatusSuccess)
             fail(RPP_ERROR, "rppCreate failed");
+        for (auto* ring : {&s->upRing, &s->downRing})
+            for (int t = 0; t < kJobRing; ++t)
+            {
+                void* hp = nullptr;
+                check_cuda(cudaMallocHost(&hp, sizeof(CopyJob) * kJobCap), "cudaMallocHost(job list)");
+                ring->lists.push_back(static_cast<CopyJob*>(hp));
+                cudaEvent_t e;
+                check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+                ring->free.push_back(e);
+                ring->used.push_back(false);
+            }
+        if (c.plainChain)
+        {
+            const RppbFrontendParams& p = c.params;
+            const int n = c.maxClipsPerStep, nf = p.numFilter;
+            const int nfft = p.nfft ? p.nfft : p.windowLength;
+            s->plainS = ((c.maxSamples > 0 ? c.maxSamples : int(30.0f * c.outRate) + 8) + 3) & ~3;
+            s->plainF = std::max(1, num_windows(s->plainS, p.windowLength, p.windowStep, p.centerWindows));
+            s->plainBins = nfft / 2 + 1;
+            auto dalloc = [](auto*& ptr, size_t bytes) {
+                void* q = nullptr;
+                check_cuda(cudaMalloc(&q, bytes), "cudaMalloc(plain path)");
+                ptr = static_cast<std::remove_reference_t<decltype(ptr)>>(q);
+            };
+            const size_t sig = size_t(n) * s->plainS * 4;
+            dalloc(s->xb, sig);
+            dalloc(s->pb, sig);
+            dalloc(s->spec, size_t(n) * s->plainBins * s->plainF * 4);
+            dalloc(s->mel, size_t(n) * nf * s->plainF * 4);
+            dalloc(s->db, size_t(n) * nf * s->plainF * 4);
+            dalloc(s->pcoeff, size_t(n) * 4);
+            dalloc(s->plen, size_t(n) * 4);
+            dalloc(s->pdims, size_t(n) * 8);
+            dalloc(s->ppatches, size_t(n) * 8);
+            dalloc(s->rsScratch, size_t(n + 1) * 8 + 4096);
+        }
         const size_t tableBytes = sizeof(RppbClip) * c.maxClipsPerStep;
         for (int t = 0; t < c.tables; ++t)
         {
@@ -456,10 +703,13 @@ extern "C" SHARED_PUBLIC RppStatus rppb_server_create(rppbServer_t* server, cons
             s->tableUsed.push_back(false);
         }
         auto call = [&](int t) {
-            const RppStatus r = rppb_frontend_clips_gpu(s->devTables[t], c.maxClipsPerStep, c.outRate, s->lut,
-                                                        c.lookupSize, c.scale, c.center, c.lobes, c.preemphCoeff,
-                                                        &s->cfg.params, s->handle);
-            if (r != RPP_SUCCESS) fail(r, std::string("rppb_frontend_clips_gpu: ") + rppbGetLastError());
+            if (c.plainChain)
+            {
+                s->plain_step(s->devTables[t]);
+                return;
+            }
+            frontend_clips(deref(s->handle), s->devTables[t], c.maxClipsPerStep, c.outRate, s->lut, c.lookupSize,
+                           c.scale, c.center, c.lobes, c.preemphCoeff, &s->cfg.params, kServerReserveSms);
         };
         // one uncaptured call (empty table) sizes the handle workspace and builds the cached tables
         call(0);
@@ -525,6 +775,13 @@ extern "C" SHARED_PUBLIC RppStatus rppb_server_submit(rppbServer_t server, const
             }
             int lr = 0;
             const int f = server->frames_of(lengths[i], rates[i], &lr);
+            if (server->cfg.plainChain && lr > server->plainS)
+            {
+                delete r;
+                fail(RPP_ERROR_NOT_ENOUGH_MEMORY, "clip longer than the plain path's maxSamples");
+            }
+            r->srcMapped.push_back(lengths[i] > 0 ? static_cast<const float*>(mapped_address(clips[i])) : nullptr);
+            r->outMapped.push_back(const_cast<float*>(static_cast<const float*>(mapped_address(outputs[i]))));
             r->src.push_back(clips[i]);
             r->len.push_back(lengths[i]);
             r->rate.push_back(rates[i]);

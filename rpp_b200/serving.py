@@ -4,10 +4,12 @@ mel -> decibels per clip): the Python face of the native server in include/rppb_
 
 Requests (1..k mono clips at any input rate, pinned host tensors) arrive at arbitrary times.  The
 native scheduler thread admits them first come, first served into a fixed device arena (the memory
-budget), copies their clips in on an upload stream, runs steps that replay one captured graph of
-rppb_frontend_clips_gpu over a clip table (every uploaded clip not yet processed joins the next
-step; several steps in flight), copies each finished clip's decibels out on a download stream and
-reports the request complete.
+budget), copies their clips in on an upload stream (one copy kernel per admission round over the
+pinned clips), runs steps that replay one captured graph of the front end over a clip table (every
+uploaded clip not yet processed joins the next step; several steps in flight), copies each finished
+clip's decibels out on a download stream (one copy kernel per round) and reports the request
+complete.  A step runs the fused front end (rppb_frontend_clips_gpu) or, for comparison, the plain
+FP32 path (resample, then the four rppt_*_gpu calls on a batch buffer).
 
 Every clip's result depends only on that clip (the kernels index clips through the table), so a
 request gives the same bits alone and in any mix -- tests/test_gpu_serving.py checks it.  Latency is
@@ -38,7 +40,10 @@ class FrontendServer:
     """Owns one native server (rppb_server_create) on the current device."""
 
     def __init__(self, torch, budget_bytes=40 << 30, max_clips=256, tables=4, out_rate=16000.0, lut=None,
-                 params=None, preemph=0.97):
+                 params=None, preemph=0.97, plain=False, max_samples=0):
+        """plain=True runs each step through the plain FP32 path (resample, then the four rppt_*_gpu
+        calls on a batch buffer of max_clips rows of max_samples samples at out_rate; 0 = 30 s) instead
+        of the fused front end."""
         from .windows import kaiser_sinc
         self.torch = torch
         self.L = lib.load()
@@ -56,6 +61,9 @@ class FrontendServer:
         cfg.scale, cfg.center, cfg.lobes = float(scale), float(center), int(lobes)
         cfg.preemphCoeff = float(preemph)
         cfg.params = self.params
+        cfg.plainChain = 1 if plain else 0
+        cfg.maxSamples = int(max_samples)
+        self.plain = bool(plain)
         self._cfg = cfg
         self._h = ctypes.c_void_p()
         st = self.L.rppb_server_create(ctypes.byref(self._h), ctypes.byref(cfg))
@@ -196,13 +204,33 @@ class ClipPool:
 
     def request(self, rid, rng, max_clips=8):
         k = int(rng.integers(1, max_clips + 1))
-        clips, rates = [], []
+        clips, rates, keys = [], [], []
         for _ in range(k):
             rate = self.rates[int(rng.integers(0, len(self.rates)))]
             lst = self.clips[rate]
-            clips.append(lst[int(rng.integers(0, len(lst)))])
+            i = int(rng.integers(0, len(lst)))
+            clips.append(lst[i])
             rates.append(rate)
-        return Request(rid=rid, clips=clips, rates=rates, arrival=0.0)
+            keys.append((rate, i))
+        r = Request(rid=rid, clips=clips, rates=rates, arrival=0.0)
+        r.keys = keys
+        return r
+
+    def attach_shared_outputs(self, torch, server, req):
+        """Outputs of `req` from one pinned buffer per pool clip, allocated on first use: requests that
+        share a clip write the same values to the same buffer, so long request streams need no new
+        host memory per request."""
+        cache = self.__dict__.setdefault("_outs", {})
+        nf = server.params.numFilter
+        outs = []
+        for key, c, rate in zip(req.keys, req.clips, req.rates):
+            if key not in cache:
+                cache[key] = torch.empty((nf, max(server.frames(c.numel(), rate), 1)),
+                                         dtype=torch.float32).pin_memory()
+            outs.append(cache[key])
+        req.outputs = outs
+        req._args = None
+        return req
 
 
 def clip_seconds(req):
@@ -212,7 +240,7 @@ def clip_seconds(req):
 def measure(torch, server, pool, rng, n_requests, rate_per_s=None):
     """Serves n_requests (all at t=0 when rate_per_s is None, else Poisson arrivals at rate_per_s)
     and returns (clip-s/s over the run, latencies in ms)."""
-    reqs = [attach_outputs(torch, server, pool.request(i, rng)) for i in range(n_requests)]
+    reqs = [pool.attach_shared_outputs(torch, server, pool.request(i, rng)) for i in range(n_requests)]
     if rate_per_s is None:
         arrivals = None
     else:

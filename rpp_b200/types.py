@@ -203,7 +203,8 @@ class RppbServerConfig(ctypes.Structure):
     _fields_ = [("budgetBytes", ctypes.c_uint64), ("maxClipsPerStep", ctypes.c_int32), ("tables", ctypes.c_int32),
                 ("outRate", ctypes.c_float), ("lookup", ctypes.c_void_p), ("lookupSize", ctypes.c_int32),
                 ("scale", ctypes.c_float), ("center", ctypes.c_float), ("lobes", ctypes.c_int32),
-                ("preemphCoeff", ctypes.c_float), ("params", RppbFrontendParams)]
+                ("preemphCoeff", ctypes.c_float), ("params", RppbFrontendParams), ("plainChain", ctypes.c_int32),
+                ("maxSamples", ctypes.c_int32)]
 
 
 class RppbCompletion(ctypes.Structure):

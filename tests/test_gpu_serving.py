@@ -1,7 +1,8 @@
 """The continuous-batching server (native scheduler of include/rppb_server.h, driven through
 rpp_b200/serving.py): each request's result is the same alone and in a mix of concurrently admitted
-requests, under memory pressure, and equals the descriptor-based calls (rppb_downmix_resample_gpu +
-rppb_frontend_gpu) on the same clip."""
+requests, under memory pressure, with pinned or pageable host buffers (copy kernels or DMA copies),
+through the fused or the plain four-call step, and equals the descriptor-based calls
+(rppb_downmix_resample_gpu + rppb_frontend_gpu) on the same clip."""
 import numpy as np
 import pytest
 import torch
@@ -86,3 +87,50 @@ def test_budget_pressure_and_oversize():
     with pytest.raises(RuntimeError):
         small.submit(huge)
     small.close()
+
+
+def test_plain_step_equals_fused_step():
+    """The plain FP32 path (resample, then the four rppt_*_gpu calls on a batch buffer) gives the fused
+    server's bits: the fused front end equals the four calls, and both read the same resampled clips."""
+    reqs = requests(31, 16)
+    fused = serving.FrontendServer(torch, budget_bytes=1 << 30, max_clips=32, tables=2)
+    ref = run(fused, reqs)
+    fused.close()
+    plain = serving.FrontendServer(torch, budget_bytes=1 << 30, max_clips=32, tables=2, plain=True,
+                                   max_samples=6 * 16000 + 16)
+    got = run(plain, reqs, list(np.linspace(0.0, 0.01, len(reqs))))
+    assert len(got) == len(reqs)
+    for r in reqs:
+        for a, b in zip(ref[r.rid], got[r.rid]):
+            assert torch.equal(a, b)
+    assert plain.arena_used() == 0
+    # a clip longer than the plain path's batch rows is refused at submission
+    long = serving.Request(rid=998, clips=[torch.zeros(7 * 16000).pin_memory()], rates=[16000.0], arrival=0.0)
+    serving.attach_outputs(torch, plain, long)
+    with pytest.raises(RuntimeError):
+        plain.submit(long)
+    plain.close()
+
+
+def test_pageable_buffers_equal_pinned():
+    """Clips and outputs in pageable host memory go through DMA copies instead of the copy kernels; the
+    bits are the same."""
+    reqs = requests(37, 10)
+    server = serving.FrontendServer(torch, budget_bytes=1 << 30, max_clips=32, tables=2)
+    ref = run(server, reqs)
+    pageable = []
+    for r in reqs:
+        q = serving.Request(rid=r.rid + 1000, clips=[c.clone() for c in r.clips], rates=list(r.rates), arrival=0.0)
+        assert not q.clips[0].is_pinned()
+        pageable.append(q)
+    for q in pageable:
+        serving.attach_outputs(torch, server, q)
+        q.outputs = [o.clone() for o in q.outputs]   # pageable outputs too
+        q._args = None
+    done = server.run(pageable)
+    torch.cuda.synchronize()
+    got = {q.rid - 1000: q.outputs for q in done}
+    for r in reqs:
+        for a, b in zip(ref[r.rid], got[r.rid]):
+            assert torch.equal(a, b)
+    server.close()
