@@ -18,6 +18,7 @@
 // shared memory first.  The lookup table sits in shared memory as (value, next - value) pairs when
 // they fit, so a tap reads one 8-byte entry.  Compute-bound: 2 * lobes taps of ~10 float
 // operations per output.
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -49,6 +50,18 @@ constexpr size_t kPairTableLimit = 200 * 1024;   // bytes of shared memory for t
 
 // Pair-table padding: a tap's x lies in (-(lobes + 1), lobes + 1), so its index, trunc or floor of
 // x * scale + center, lies within [center - (lobes + 1)|scale| - 2, center + (lobes + 1)|scale| + 2].
+// Whether every table position a tap can produce lies in [0, 2^22): the bound the magic-number index of
+// Win<kPairs, true> needs (with the pair table, whose padding covers the indices; the clamp of the plain
+// table is not applied on that path).  A tap's offset x = l - phase lies in [-lobes, lobes + 1): the
+// first tap is ceil(phase) - lobes (or later, at the signal's start), and float rounding keeps x >= -lobes
+// because -lobes is representable; x * scale + center is then bounded by its values at the two ends.
+inline bool resample_magic_ok(const ResampleWindowDev& w, bool pairs)
+{
+    const double a = -double(w.lobes) * double(w.scale), b = (double(w.lobes) + 1.0) * double(w.scale);
+    const double lo = double(w.center) + std::min(a, b), hi = double(w.center) + std::max(a, b);
+    return pairs && lo >= 0.0 && hi < 4194304.0;
+}
+
 inline void resample_pads(ResampleWindowDev& w)
 {
     const double reach = (double(w.lobes) + 1.0) * std::fabs(double(w.scale));
@@ -91,7 +104,11 @@ struct ResampleCount
     }
 };
 
-template <bool kPairs>
+// kMagic: the table index comes from adding 1.5 * 2^23 with rounding toward minus infinity, which leaves
+// floor(locRaw) in the low mantissa bits and float(floor(locRaw)) one subtraction away, instead of two
+// float <-> int conversions per tap (low-throughput instructions).  Used when the host has shown that
+// every locRaw a tap can produce lies in [0, 2^22): then trunc == floor, and both are exact this way.
+template <bool kPairs, bool kMagic = false>
 struct Win
 {
     const float* lut;     // shared memory: the table (plain layout)
@@ -115,10 +132,17 @@ struct Win
             return __fadd_rn(cur, __fmul_rn(weight, __fsub_rn(nxt, cur)));
         }
     }
+    __device__ __forceinline__ float magic_floor(float locRaw) const
+    {
+        constexpr float kM = 12582912.0f;   // 1.5 * 2^23
+        const float m = __fadd_rd(locRaw, kM);
+        return interp(__float_as_int(m) - __float_as_int(kM), __fsub_rn(locRaw, __fsub_rn(m, kM)));
+    }
     // rppdefs.h:771-782: truncating index (the SSE lanes)
     __device__ __forceinline__ float lane(float x) const
     {
         const float locRaw = __fadd_rn(__fmul_rn(x, scale), center);
+        if constexpr (kMagic) return magic_floor(locRaw);
         const int idx = int(locRaw);
         return interp(idx, __fsub_rn(locRaw, float(idx)));
     }
@@ -126,6 +150,7 @@ struct Win
     __device__ __forceinline__ float scalar(float x) const
     {
         const float locRaw = __fadd_rn(__fmul_rn(x, scale), center);
+        if constexpr (kMagic) return magic_floor(locRaw);
         const int idx = int(floorf(locRaw));
         return interp(idx, __fsub_rn(locRaw, float(idx)));
     }
@@ -143,7 +168,7 @@ struct UnitInfo
 
 // kMix: the input is interleaved multi-channel and is down-mixed to mono on the fly (MonoMix), so
 // the launch equals rppt_down_mixing_gpu followed by a mono rppt_resample_gpu.
-template <bool kMix, bool kTable, bool kPairs>
+template <bool kMix, bool kTable, bool kPairs, bool kMagic = false>
 __global__ void __launch_bounds__(kThreads) resample_kernel(const float* __restrict__ src, uint32_t srcStride,
                                                             float* __restrict__ dst, uint32_t dstStride,
                                                             const float* __restrict__ inRateT,
@@ -165,8 +190,8 @@ __global__ void __launch_bounds__(kThreads) resample_kernel(const float* __restr
         }
     else
         for (int i = threadIdx.x; i < wd.lutSize; i += kThreads) s_lut[i] = wd.lut[i];
-    const Win<kPairs> win{s_lut, reinterpret_cast<const float2*>(s_lut) + (kPairs ? wd.padLeft : 0), wd.lutSize,
-                          wd.scale, wd.center};
+    const Win<kPairs, kMagic> win{s_lut, reinterpret_cast<const float2*>(s_lut) + (kPairs ? wd.padLeft : 0),
+                                  wd.lutSize, wd.scale, wd.center};
     const int lobes = wd.lobes;
     __shared__ long long s_prefix[kPrefixCache];
     prefix = cache_prefix(prefix, n, s_prefix);   // ends with __syncthreads
@@ -349,8 +374,11 @@ void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStr
         kernel<<<grid, kThreads, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate, outRate, dims, w,
                                                      normalize, prefix, n, nullptr, 0.f);
     };
-    if (downmix && pairs) go(resample_kernel<true, false, true>);
+    const bool magic = resample_magic_ok(w, pairs);
+    if (downmix && magic) go(resample_kernel<true, false, true, true>);
+    else if (downmix && pairs) go(resample_kernel<true, false, true>);
     else if (downmix) go(resample_kernel<true, false, false>);
+    else if (magic) go(resample_kernel<false, false, true, true>);
     else if (pairs) go(resample_kernel<false, false, true>);
     else go(resample_kernel<false, false, false>);
     count_launch();
@@ -372,7 +400,8 @@ void launch_resample_clips(Handle& h, void* scratch, const RppbClip* clips, int 
         kernel<<<grid, kThreads, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, w, false,
                                                      prefix, n, clips, outRate);
     };
-    if (pairs) go(resample_kernel<false, true, true>);
+    if (resample_magic_ok(w, pairs)) go(resample_kernel<false, true, true, true>);
+    else if (pairs) go(resample_kernel<false, true, true>);
     else go(resample_kernel<false, true, false>);
     count_launch();
     check_cuda(cudaGetLastError(), "resample_kernel(clips)");
