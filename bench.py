@@ -918,7 +918,7 @@ def run_b200(args, world, rank, local):
     e2e = {"value": replicas.job_throughput(clip_s, e2e_ms, world), "unit": "clip-s/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
            "path": "pinned host tensors -> rppb_frontend_host_gpu (C ABI): valid samples copied in, valid decibel "
-                   "rows copied out, %s chunks overlapping copy-in / kernels / copy-out" % (args.chunks or 8),
+                   "rows copied out, %s chunks overlapping copy-in / kernels / copy-out" % (args.chunks or 16),
            "whole_tensor_copies": {"value": replicas.job_throughput(clip_s, full_ms, world), "ms_per_step": full_ms,
                                    "h2d_bytes_per_step": int(x_host.numel() * 4),
                                    "d2h_bytes_per_step": int(out_host.numel() * 4),

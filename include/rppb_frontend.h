@@ -138,8 +138,11 @@ SHARED_PUBLIC RppStatus rppb_frontend_tune_gpu(RppPtr_t srcPtr, RpptDescPtr srcD
 
 /* The fused front end on HOST tensors: srcHost, dstHost, srcLengthHost and coeffHost are host memory
  * (pinned for overlap; pageable works but serializes the copies), laid out as for rppb_frontend_gpu.
- * The batch is split into numChunks contiguous runs of clips with about equal sample counts (<= 0:
- * 8); chunk c's valid samples are copied in on one stream while chunk c-1 is computed and chunk c-2's
+ * The batch is split into numChunks contiguous runs of clips (<= 0: 16) with about equal sample
+ * counts, except that from 6 chunks on the first and last carry a quarter and the second and
+ * second-to-last half of a middle chunk's samples (the copy-in before the first kernel and the
+ * copy-out after the last one run with the other direction idle, so they are kept short); chunk
+ * c's valid samples are copied in on one stream while chunk c-1 is computed and chunk c-2's
  * valid output rows (numFilter x frames per clip) are copied out on another, through double-buffered
  * device staging in the handle workspace.  Output equals rppb_frontend_gpu on the same data and
  * only the valid region of dstHost is written.  Asynchronous: synchronize the handle stream before

@@ -418,6 +418,13 @@ extern "C" SHARED_PUBLIC RppStatus rppb_downmix_resample_gpu(RppPtr_t srcPtr, Rp
 
 namespace {
 
+// Host-tensor call: default chunk count, the first/last two chunks' share of a middle chunk's samples,
+// the copy kernels' CTAs per chunk and the SMs the persistent kernel leaves to them.
+constexpr int kHostChunks = 16;
+constexpr double kEdgeWeight[2] = {0.25, 0.5};
+constexpr int kMoverCtas = 96;
+constexpr int kReservedSms = 40;
+
 // Validates the fused-front-end parameters and fills the shared fields of FrontendArgs.
 RppStatus frontend_params(Handle& h, const RppbFrontendParams* params, float* winStage, FrontendArgs& a)
 {
@@ -553,15 +560,24 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost,
             F[b] = std::min(std::max(params->windowStep > 0 ? len / params->windowStep + 1 : 0, 0), maxFrames);
             total += size_t(L[b]);
         }
-        // contiguous chunks of clips with about equal sample counts
-        const int chunks = std::max(1, std::min(n, numChunks > 0 ? numChunks : 8));
+        // contiguous chunks of clips; the middle ones carry about equal sample counts, the first and the
+        // last two less (kEdgeWeight of a middle chunk), so that the copy-in before the first kernel and
+        // the copy-out after the last one, each running with the other direction idle, are short
+        const int chunks = std::max(1, std::min(n, numChunks > 0 ? numChunks : kHostChunks));
+        std::vector<double> weight(chunks, 1.0);
+        if (chunks >= 6)
+            for (int e = 0; e < 2; ++e) weight[e] = weight[chunks - 1 - e] = kEdgeWeight[e];
+        std::vector<double> cut(chunks);   // samples up to the end of chunk c
+        double wsum = 0.0, run = 0.0;
+        for (double w : weight) wsum += w;
+        for (int c = 0; c < chunks; ++c) cut[c] = (run += weight[c]) / wsum * double(total);
         std::vector<int> bound{0};
         size_t acc = 0;
         for (int b = 0; b < n; ++b)
         {
             acc += size_t(L[b]);
-            const int c = int(bound.size());
-            if (c < chunks && b + 1 < n && acc * chunks >= total * size_t(c)) bound.push_back(b + 1);
+            const int c = int(bound.size()) - 1;
+            if (c + 1 < chunks && b + 1 < n && double(acc) >= cut[c]) bound.push_back(b + 1);
         }
         bound.push_back(n);
         const int nc = int(bound.size()) - 1;
@@ -614,8 +630,6 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost,
         void* dstMapped = nullptr;
         const bool gatherK = h.device_writable(srcHost, &srcMapped);
         const bool scatterK = h.device_writable(dstHost, &dstMapped);
-        constexpr int kMoverCtas = 32;
-        constexpr int kReservedSms = 12;
         if (gatherK || scatterK) a.reserveSms = kReservedSms;   // room for the movers next to the persistent kernel
 
         cudaStream_t main = h.stream(), up = h.aux_stream(0), down = h.aux_stream(1);
