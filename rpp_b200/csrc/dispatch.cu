@@ -833,7 +833,8 @@ extern "C" SHARED_PUBLIC RppStatus rppb_spectrogram_tc_gpu(RppPtr_t srcPtr, Rppt
         const int n = int(srcDescPtr->n);
         if (n <= 0) return RPP_SUCCESS;
         const int maxFrames = int(nft ? dstDescPtr->w : dstDescPtr->h);
-        const TcGeometry geo = tc_geometry(fmt, windowLength, windowStep, maxFrames, nfft);
+        const TcGeometry geo =
+            tc_geometry(fmt, windowLength, windowStep, maxFrames, nfft, tc_overlap_supported(h.device_flags()));
         const size_t scratchBytes = tc_spectrogram_scratch_bytes(n, fmt, geo, maxFrames);
         Carver m(nullptr);
         m.take<int>(n);

@@ -241,8 +241,12 @@ struct TcGeometry
     uint32_t rowStep;    // elements between consecutive frames' rows of the A operand
     uint32_t clipStride; // elements per clip of the A operand
     size_t basisFloats;  // size of the cached basis table, in floats
+    bool materialized;   // frame rows written out [frame][kPad] (FP8, or no overlapping-row tensor map)
 };
-TcGeometry tc_geometry(int fmt, int windowLength, int windowStep, int maxFrames, int nfft);
+// Whether the driver encodes a tensor map whose rows overlap (frame rows hop elements apart);
+// anyDevicePtr: any 16-byte aligned device allocation (only encoded, never accessed).
+bool tc_overlap_supported(const void* anyDevicePtr);
+TcGeometry tc_geometry(int fmt, int windowLength, int windowStep, int maxFrames, int nfft, bool overlapRows);
 // Window-folded DFT basis [nfft][kPad] in the format's element type (hi then lo for kTcBf16x3).
 void tc_build_basis(float* out, int fmt, int nfft, int windowLength, int kPad, const float* window);
 struct TcSpectrogramArgs

@@ -28,6 +28,8 @@
 // tensor memory and leaves.  The epilogue reads the accumulator with tcgen05.ld (warp w owns rows
 // 32w..32w+31), forms re^2 + im^2 and stores NFT rows (32 consecutive frames per warp store) or NTF
 // rows.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 
@@ -44,31 +46,36 @@
 namespace rppb {
 namespace {
 
-constexpr int kThreads = 128;
+constexpr int kThreads = 192;        // warp 0: TMA producer; warp 1: MMA issuer and tensor-memory owner;
+                                     // warps 2-5: epilogue (one 32-lane quarter of tensor memory each)
 constexpr int kTileM = 128;          // frames per tile
 constexpr int kTileN = 256;          // basis columns per MMA / work item
-constexpr int kRowBytes = 128;       // one swizzled K block per row
-constexpr long long kWaitLimit = 1ll << 21;   // try_wait polls: on the order of a second
+constexpr int kKBytes = 64;          // bytes of K per operand row and stage (64-byte swizzle)
+constexpr int kRowBytes = 128;       // K padding granule of the operands (kPad is a multiple of 128 bytes)
+constexpr int kTmemCols = 2 * kTileN;           // two accumulators: MMAs fill one while the epilogue drains the other
+constexpr size_t kRingBytes = 192 * 1024;       // shared memory of the stage ring
+constexpr long long kWaitLimit = 1ll << 21;     // try_wait polls: on the order of a second
 constexpr float kFp8BasisScale = 256.f;
 constexpr float kFp8Max = 448.f;
 
-constexpr size_t kABytes = size_t(kTileM) * kRowBytes;   // 16 KB
-constexpr size_t kBBytes = size_t(kTileN) * kRowBytes;   // 32 KB
+constexpr size_t kABytes = size_t(kTileM) * kKBytes;   // 8 KB
+constexpr size_t kBBytes = size_t(kTileN) * kKBytes;   // 16 KB
 
 template <int FMT>
 struct Fmt
 {
     static constexpr int kElem = (FMT == kTcTf32) ? 4 : (FMT == kTcFp8) ? 1 : 2;
-    static constexpr int kBlockK = kRowBytes / kElem;       // elements per K block
+    static constexpr int kBlockK = kKBytes / kElem;         // elements per stage row
     static constexpr bool kSplit = FMT == kTcBf16x3;
-    static constexpr size_t kStageBytes = (kSplit ? 2 : 1) * (kABytes + kBBytes);
-    static constexpr int kStages = kSplit ? 2 : 4;          // 192 KB of stages either way
+    static constexpr uint32_t kStageBytes = uint32_t((kSplit ? 2 : 1) * (kABytes + kBBytes));
+    static constexpr int kStages = int(kRingBytes / kStageBytes);   // 8, or 4 for the split format
     // Instruction descriptor: F32 accumulator (bit 4), A/B formats (bits 7, 10), both K-major,
     // N >> 3 at bit 17, M >> 4 at bit 24.  Formats: kind::f16 BF16 = 1, kind::tf32 TF32 = 2,
     // kind::f8f6f4 E4M3 = 0.
     static constexpr uint32_t kFormat = (FMT == kTcTf32) ? 2u : (FMT == kTcFp8) ? 0u : 1u;
     static constexpr uint32_t kIdesc = (1u << 4) | (kFormat << 7) | (kFormat << 10) | (uint32_t(kTileN >> 3) << 17) |
                                        (uint32_t(kTileM >> 4) << 24);
+    static_assert(kStages >= 3, "stage ring");
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -76,15 +83,17 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row atoms 1024 bytes apart.
+// UMMA shared-memory descriptor: K-major, 64-byte swizzle (the layout TMA writes with
+// CU_TENSOR_MAP_SWIZZLE_64B), 8-row atoms 512 bytes apart.  Each MMA reads 32 bytes of K; the next
+// 32 bytes of a row start 32 bytes later (the swizzle is a function of the address).
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
 {
     uint64_t d = 0;
     d |= uint64_t((saddr >> 4) & 0x3FFF);            // start address
     d |= uint64_t(1) << 16;                           // leading byte offset (unused for swizzled K-major)
-    d |= uint64_t(1024 >> 4) << 32;                   // stride byte offset: next 8-row atom
+    d |= uint64_t(512 >> 4) << 32;                    // stride byte offset: next 8-row atom
     d |= uint64_t(1) << 46;                           // descriptor version (Blackwell)
-    d |= uint64_t(2) << 61;                           // layout: SWIZZLE_128B
+    d |= uint64_t(4) << 61;                           // layout: SWIZZLE_64B
     return d;
 }
 
@@ -108,6 +117,7 @@ __device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint3
             "l"(a), "l"(b), "r"(Fmt<FMT>::kIdesc), "r"(accumulate));
 }
 
+// Arrives on the mbarrier once every tcgen05 operation this thread issued so far has completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -119,8 +129,20 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, int count)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-// Bounded wait for the mbarrier phase with parity `parity` to complete; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Bounded wait for the mbarrier phase with parity `parity` to complete (a fresh barrier counts its
+// phase before the first as complete, so a wait on parity 1 returns at once).  False on timeout, or
+// when another role of the CTA has set *abortFlag.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abortFlag)
 {
     const uint32_t a = smem_u32(bar);
     for (long long i = 0; i < kWaitLimit; ++i)
@@ -134,31 +156,34 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
+        if ((i & 63) == 63 && *abortFlag) return false;
     }
     return false;
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+// TMA tile loads into shared memory, completing bytes on the mbarrier (this GPU's memory only).
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar)
 {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
 }
 
-// Byte offset of 16-byte chunk c (0..7) of row r in a 128-byte-swizzled K-major tile.
-__device__ __forceinline__ uint32_t sw128(int r, int c)
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
 {
-    return uint32_t((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
 }
 
 struct TcArgs
 {
-    const unsigned char* a;     // A operand, [n][clipStride] elements (hi part for the split format)
-    const unsigned char* aLo;   // lo part (split format only)
-    uint32_t clipStride;        // elements
-    uint32_t rowStep;           // elements between frame rows
-    const unsigned char* b;     // basis [nfft][kPad] elements
-    const unsigned char* bLo;
     int kPad;
-    int nfft;
+    int nfft;                   // basis rows (N)
     const float* invScale;      // FP8: per frame 1 / (frame scale * basis scale), [n][maxFrames]
     int maxFrames;
     float* dst;
@@ -169,6 +194,13 @@ struct TcArgs
     int n;
     int* errorWord;
     int validN;                 // linear epilogue: output columns (mel filters)
+};
+
+// Tensor maps of the operands: A [clip][frame row][K] (rows may overlap: row stride = hop), B [N][K],
+// and the lo parts of the split format.
+struct TcMaps
+{
+    CUtensorMap a, aLo, b, bLo;
 };
 
 constexpr int kEpiPower = 0;
@@ -185,214 +217,310 @@ struct TcCount
     }
 };
 
+// Work item w: clip b, frames f0 .. f0 + 127, basis columns n0 .. n0 + 255.
+struct TcItem
+{
+    int b, f0, n0;
+};
+
+__device__ __forceinline__ TcItem tc_item(const long long* prefix, int n, int chunks, long long w)
+{
+    TcItem it;
+    it.b = ragged_find(prefix, n, w);
+    const int local = int(w - prefix[it.b]);
+    it.f0 = (local / chunks) * kTileM;
+    it.n0 = (local % chunks) * kTileN;
+    return it;
+}
+
 // EPI: kEpiPower -- column pairs (cos, -sin) of one bin -> power / magnitude (the spectrogram);
 //      kEpiLinear -- column n < validN -> the accumulator itself (the mel projection).
+//
+// Persistent over work items (every role walks the same sequence w = blockIdx.x + k * gridDim.x):
+//   producer (warp 0, one lane): per K block of 64 bytes, wait until the ring stage is free, then TMA
+//     loads of A (128 frame rows) and B (256 basis rows), plus their lo parts, onto the stage's
+//     "full" barrier with the expected byte count;
+//   MMA (warp 1, one lane): per work item, wait until the epilogue has drained the accumulator it
+//     fills next; per stage, wait for "full", issue the MMAs (M 128, N 256, 32 bytes of K each; the
+//     split format adds hi*lo and lo*hi), commit to the stage's "empty" barrier (frees it for the
+//     producer when the MMAs finish); after the last K block, commit to the accumulator's "full";
+//   epilogue (warps 2-5): wait for the accumulator, read it with tcgen05.ld (the warp's 32 lanes = 32
+//     frames), form power / the linear output, store, and arrive on the accumulator's "empty".
+// Every wait is bounded; the first role to time out sets the device error word (bit 2) and the CTA's
+// abort flag, and the others leave their loops at their next wait.  Before the tensor memory is
+// freed the producer waits (bounded) for its last loads and the MMA thread for its last MMAs.
 template <int FMT, int EPI>
-__global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const long long* __restrict__ prefix)
+__global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const long long* __restrict__ prefix,
+                                                              const __grid_constant__ TcMaps maps)
 {
     using T = Fmt<FMT>;
     constexpr int S = T::kStages;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    __shared__ uint64_t bars[S];
+    __shared__ uint64_t fullBar[S], emptyBar[S], accFull[2], accEmpty[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    if (warp == 0)
+    if (warp == 1)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(kTileN));
+                     "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0)
     {
-        for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s < S; ++s)
+        {
+            mbar_init(&fullBar[s], 1);
+            mbar_init(&emptyBar[s], 1);
+        }
+        for (int i = 0; i < 2; ++i)
+        {
+            mbar_init(&accFull[i], 1);
+            mbar_init(&accEmpty[i], 4);   // one arrival per epilogue warp
+        }
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (tid == 32)
+    {
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.a)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.b)) : "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
+    volatile int* abortFlag = &s_abort;
+    auto fail = [&]() {
+        if (!*abortFlag)
+        {
+            *abortFlag = 1;
+            atomicOr(a.errorWord, 2);
+        }
+    };
 
     const int chunks = a.nfft / kTileN;
     const int kBlocks = a.kPad / T::kBlockK;
     const long long total = prefix[a.n];
-    uint32_t issued[S], waited[S];   // commits made to / waited on each stage's barrier (every thread)
-#pragma unroll
-    for (int s = 0; s < S; ++s) issued[s] = waited[s] = 0;
-    int stage = 0;
 
-    for (long long w = blockIdx.x; w < total && !s_abort; w += gridDim.x)
+    if (warp == 0)
     {
-        const int b = ragged_find(prefix, a.n, w);
-        const int local = int(w - prefix[b]);
-        const int tile = local / chunks, chunk = local % chunks;
-        const int F = a.frames[b];
-        const int f0 = tile * kTileM;
-        const size_t clipOff = size_t(b) * a.clipStride;
-        const int n0 = chunk * kTileN;
-
-        for (int kb = 0; kb < kBlocks; ++kb)
+        if (lane == 0)
         {
-            const int s = stage;
-            stage = (stage + 1 == S) ? 0 : stage + 1;
-            // the stage's previous MMAs must have finished reading it
-            if (issued[s] > waited[s])
+            long long loads = 0;   // stage loads issued
+            int s = 0;
+            uint32_t ph = 0;
+            for (long long w = blockIdx.x; w < total && !*abortFlag; w += gridDim.x)
             {
-                if (mbar_wait(&bars[s], waited[s] & 1)) waited[s] = issued[s];
-                else
+                const TcItem it = tc_item(prefix, a.n, chunks, w);
+                for (int kb = 0; kb < kBlocks; ++kb)
                 {
-                    if (tid == 0) atomicOr(a.errorWord, 2);
-                    s_abort = 1;
-                }
-            }
-            __syncthreads();
-            if (s_abort) break;
-            unsigned char* sA = smem + s * T::kStageBytes;
-            unsigned char* sB = sA + kABytes;
-            unsigned char* sAl = sB + kBBytes;      // split format only
-            unsigned char* sBl = sAl + kABytes;
-            // A: 128 frames x 8 chunks of 16 bytes (frames past F re-read frame F-1; results unused)
-            for (int i = tid; i < kTileM * 8; i += kThreads)
-            {
-                const int r = i >> 3, c = i & 7;
-                const int fr = min(f0 + r, max(F - 1, 0));
-                const size_t off = (clipOff + size_t(fr) * a.rowStep + size_t(kb) * T::kBlockK) * T::kElem + c * 16;
-                cp_async16(sA + sw128(r, c), a.a + off);
-                if constexpr (T::kSplit) cp_async16(sAl + sw128(r, c), a.aLo + off);
-            }
-            // B: 256 basis columns x 8 chunks
-            for (int i = tid; i < kTileN * 8; i += kThreads)
-            {
-                const int r = i >> 3, c = i & 7;
-                const size_t off = (size_t(n0 + r) * a.kPad + size_t(kb) * T::kBlockK) * T::kElem + c * 16;
-                cp_async16(sB + sw128(r, c), a.b + off);
-                if constexpr (T::kSplit) cp_async16(sBl + sw128(r, c), a.bLo + off);
-            }
-            asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic-proxy writes -> tensor core
-            __syncthreads();
-            if (tid == 0)
-            {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint64_t dA = umma_desc(smem_u32(sA)), dB = umma_desc(smem_u32(sB));
-#pragma unroll
-                for (int ks = 0; ks < kRowBytes / 32; ++ks)
-                {
-                    const uint64_t step = uint64_t(ks * 32) >> 4;   // 32 bytes of K along the swizzled row
-                    const uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
-                    mma<FMT>(tmem, dA + step, dB + step, acc0);
+                    if (!mbar_wait(&emptyBar[s], ph ^ 1u, abortFlag))
+                    {
+                        fail();
+                        break;
+                    }
+                    unsigned char* sA = smem + size_t(s) * T::kStageBytes;
+                    unsigned char* sB = sA + kABytes;
+                    mbar_expect_tx(&fullBar[s], T::kStageBytes);
+                    const int x = kb * T::kBlockK;
+                    tma_load_3d(sA, &maps.a, x, it.f0, it.b, &fullBar[s]);
+                    tma_load_2d(sB, &maps.b, x, it.n0, &fullBar[s]);
                     if constexpr (T::kSplit)
                     {
-                        const uint64_t dAl = umma_desc(smem_u32(sAl)), dBl = umma_desc(smem_u32(sBl));
-                        mma<FMT>(tmem, dA + step, dBl + step, 1u);
-                        mma<FMT>(tmem, dAl + step, dB + step, 1u);
+                        tma_load_3d(sB + kBBytes, &maps.aLo, x, it.f0, it.b, &fullBar[s]);
+                        tma_load_2d(sB + kBBytes + kABytes, &maps.bLo, x, it.n0, &fullBar[s]);
                     }
-                }
-                mma_commit(&bars[s]);
-            }
-            ++issued[s];
-        }
-        if (s_abort) break;
-        // wait for this tile's MMAs (each stage's last commit covers everything issued before it)
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            if (issued[s] > waited[s])
-            {
-                if (mbar_wait(&bars[s], waited[s] & 1)) waited[s] = issued[s];
-                else
-                {
-                    if (tid == 0) atomicOr(a.errorWord, 2);
-                    s_abort = 1;
-                }
-            }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (s_abort) break;
-
-        // ---- epilogue: warp w owns accumulator rows (frames) 32w .. 32w+31
-        const int r = warp * 32 + lane;
-        const int frame = f0 + r;
-        float* y = a.dst + size_t(b) * a.dstNStride;
-        float sc = 1.f;
-        if constexpr (FMT == kTcFp8)
-            if (frame < F) sc = a.invScale[size_t(b) * a.maxFrames + frame];
-#pragma unroll 1
-        for (int c0 = 0; c0 < kTileN; c0 += 32)
-        {
-            uint32_t v[32];
-            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (EPI == kEpiLinear && frame < F)
-            {
-#pragma unroll
-                for (int q = 0; q < 32; ++q)
-                {
-                    const int col = n0 + c0 + q;
-                    if (col >= a.validN) break;
-                    const float o = __uint_as_float(v[q]) * sc;
-                    if (a.nft) y[size_t(col) * a.dstHStride + frame] = o;
-                    else y[size_t(frame) * a.dstHStride + col] = o;
-                }
-            }
-            if (EPI == kEpiPower && frame < F)
-            {
-#pragma unroll
-                for (int q = 0; q < 16; ++q)
-                {
-                    const float re = __uint_as_float(v[2 * q]) * sc, im = __uint_as_float(v[2 * q + 1]) * sc;
-                    const int col = n0 + c0 + 2 * q;   // even column: bin col/2 (cos, -sin)
-                    if (col == 0)
+                    ++loads;
+                    if (++s == S)
                     {
-                        // column 0: bin 0 (real); column 1: Nyquist bin (real)
-                        const float p0 = re * re, pn = im * im;
-                        const float o0 = a.power == 1 ? sqrtf(p0) : p0;
-                        const float on = a.power == 1 ? sqrtf(pn) : pn;
-                        const int nyq = a.nfft / 2;
-                        if (a.nft)
-                        {
-                            y[frame] = o0;
-                            y[size_t(nyq) * a.dstHStride + frame] = on;
-                        }
-                        else
-                        {
-                            y[size_t(frame) * a.dstHStride] = o0;
-                            y[size_t(frame) * a.dstHStride + nyq] = on;
-                        }
-                        continue;
+                        s = 0;
+                        ph ^= 1u;
                     }
-                    const int bin = col >> 1;
-                    const float p = fmaf(re, re, im * im);
-                    const float o = a.power == 1 ? sqrtf(p) : p;
-                    if (a.nft) y[size_t(bin) * a.dstHStride + frame] = o;
-                    else y[size_t(frame) * a.dstHStride + bin] = o;
                 }
             }
+            // before the CTA leaves: every issued load has landed (stage s' last load completes the
+            // phase with parity (its loads - 1) & 1)
+            for (int st = 0; st < S; ++st)
+            {
+                const long long cnt = loads > st ? (loads - st + S - 1) / S : 0;
+                if (cnt > 0) mbar_wait(&fullBar[st], uint32_t((cnt - 1) & 1), abortFlag);
+            }
         }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();   // the next tile's MMAs overwrite the accumulator
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            int s = 0, acc = 0;
+            uint32_t ph = 0, aph = 0;
+            uint64_t* lastBar = nullptr;
+            uint32_t lastParity = 0;
+            for (long long w = blockIdx.x; w < total && !*abortFlag; w += gridDim.x)
+            {
+                if (!mbar_wait(&accEmpty[acc], aph ^ 1u, abortFlag))
+                {
+                    fail();
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + uint32_t(acc * kTileN);
+                bool ok = true;
+                for (int kb = 0; kb < kBlocks; ++kb)
+                {
+                    if (!mbar_wait(&fullBar[s], ph, abortFlag))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sA = smem_u32(smem + size_t(s) * T::kStageBytes);
+                    const uint32_t sB = sA + uint32_t(kABytes);
+                    const uint64_t dA = umma_desc(sA), dB = umma_desc(sB);
+#pragma unroll
+                    for (int ks = 0; ks < kKBytes / 32; ++ks)
+                    {
+                        const uint64_t step = uint64_t(ks * 32) >> 4;   // 32 bytes of K along the swizzled row
+                        mma<FMT>(d, dA + step, dB + step, (kb > 0 || ks > 0) ? 1u : 0u);
+                        if constexpr (T::kSplit)
+                        {
+                            const uint64_t dAl = umma_desc(sB + uint32_t(kBBytes));
+                            const uint64_t dBl = umma_desc(sB + uint32_t(kBBytes + kABytes));
+                            mma<FMT>(d, dA + step, dBl + step, 1u);
+                            mma<FMT>(d, dAl + step, dB + step, 1u);
+                        }
+                    }
+                    mma_commit(&emptyBar[s]);
+                    lastBar = &emptyBar[s];
+                    lastParity = ph;
+                    if (++s == S)
+                    {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok)
+                {
+                    fail();
+                    break;
+                }
+                mma_commit(&accFull[acc]);
+                if (++acc == 2)
+                {
+                    acc = 0;
+                    aph ^= 1u;
+                }
+            }
+            // the MMAs in flight end before the tensor memory is freed (the last commit covers all)
+            if (lastBar) mbar_wait(lastBar, lastParity, abortFlag);
+        }
+    }
+    else
+    {
+        // ---- epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 = tile rows (frames)
+        const int q = warp & 3;
+        const int r = q * 32 + lane;
+        int acc = 0;
+        uint32_t aph = 0;
+        for (long long w = blockIdx.x; w < total && !*abortFlag; w += gridDim.x)
+        {
+            const TcItem it = tc_item(prefix, a.n, chunks, w);
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&accFull[acc], aph, abortFlag));
+            if (!ok)
+            {
+                if (lane == 0) fail();
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int F = a.frames[it.b];
+            const int frame = it.f0 + r;
+            float* y = a.dst + size_t(it.b) * a.dstNStride;
+            float sc = 1.f;
+            if constexpr (FMT == kTcFp8)
+                if (frame < F) sc = a.invScale[size_t(it.b) * a.maxFrames + frame];
+#pragma unroll 1
+            for (int c0 = 0; c0 < kTileN; c0 += 32)
+            {
+                uint32_t v[32];
+                const uint32_t taddr = tmem + (uint32_t(q * 32) << 16) + uint32_t(acc * kTileN + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                const int n0 = it.n0 + c0;
+                if (EPI == kEpiLinear && frame < F)
+                {
+#pragma unroll
+                    for (int k = 0; k < 32; ++k)
+                    {
+                        const int col = n0 + k;
+                        if (col >= a.validN) break;
+                        const float o = __uint_as_float(v[k]) * sc;
+                        if (a.nft) y[size_t(col) * a.dstHStride + frame] = o;
+                        else y[size_t(frame) * a.dstHStride + col] = o;
+                    }
+                }
+                if (EPI == kEpiPower && frame < F)
+                {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k)
+                    {
+                        const float re = __uint_as_float(v[2 * k]) * sc, im = __uint_as_float(v[2 * k + 1]) * sc;
+                        const int col = n0 + 2 * k;   // even column: bin col/2 (cos, -sin)
+                        if (col == 0)
+                        {
+                            // column 0: bin 0 (real); column 1: Nyquist bin (real)
+                            const float p0 = re * re, pn = im * im;
+                            const float o0 = a.power == 1 ? sqrtf(p0) : p0;
+                            const float on = a.power == 1 ? sqrtf(pn) : pn;
+                            const int nyq = a.nfft / 2;
+                            if (a.nft)
+                            {
+                                y[frame] = o0;
+                                y[size_t(nyq) * a.dstHStride + frame] = on;
+                            }
+                            else
+                            {
+                                y[size_t(frame) * a.dstHStride] = o0;
+                                y[size_t(frame) * a.dstHStride + nyq] = on;
+                            }
+                            continue;
+                        }
+                        const int bin = col >> 1;
+                        const float p = fmaf(re, re, im * im);
+                        const float o = a.power == 1 ? sqrtf(p) : p;
+                        if (a.nft) y[size_t(bin) * a.dstHStride + frame] = o;
+                        else y[size_t(frame) * a.dstHStride + bin] = o;
+                    }
+                }
+            }
+            // this warp's reads of the accumulator are done: the MMA thread may overwrite it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&accEmpty[acc]);
+            if (++acc == 2)
+            {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
     }
 
-    // leave: make sure no MMA is still writing tensor memory (a second bounded wait after a timeout),
-    // then free it
-#pragma unroll
-    for (int s = 0; s < S; ++s)
-        if (issued[s] > waited[s] && mbar_wait(&bars[s], waited[s] & 1)) waited[s] = issued[s];
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTileN));
+    if (warp == 1)
+    {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    }
 }
 
 // The sample the spectrogram frames at padded position i (= signal index i - centerOffset): the
@@ -500,6 +628,44 @@ __global__ void tc_prep_fp8_kernel(PrepArgs p, const int* __restrict__ frames, i
     }
 }
 
+// BF16 (hi, lo) or TF32 frame rows [n][maxFrames][kPad] (window positions >= W are zero): the A
+// operand when the driver does not accept a tensor map whose frame rows overlap.
+template <int FMT>
+__global__ void tc_prep_rows_kernel(PrepArgs p, const int* __restrict__ frames, int maxFrames, int W, int hop,
+                                    int kPad, void* __restrict__ outHi, void* __restrict__ outLo)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpsPerBlock = blockDim.x >> 5;
+    for (int b = blockIdx.y; b < p.n; b += gridDim.y)
+    {
+        const PaddedSignal sig =
+            padded_signal(p.src, p.srcStride, p.srcElems, p.len, p.coeff, p.border, p.reflect, p.centerOffset, b);
+        const int F = frames[b];
+        for (int f = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); f < F; f += gridDim.x * warpsPerBlock)
+        {
+            const long long s0 = (long long)f * hop;
+            const size_t row = (size_t(b) * maxFrames + f) * kPad;
+            for (int t = lane; t < kPad; t += 32)
+            {
+                const float v = t < W ? sig(s0 + t) : 0.f;
+                if constexpr (FMT == kTcTf32)
+                {
+                    uint32_t u;
+                    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(v));
+                    static_cast<uint32_t*>(outHi)[row + t] = u;
+                }
+                else
+                {
+                    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+                    static_cast<__nv_bfloat16*>(outHi)[row + t] = hi;
+                    if constexpr (FMT == kTcBf16x3)
+                        static_cast<__nv_bfloat16*>(outLo)[row + t] = __float2bfloat16_rn(v - __bfloat162float(hi));
+                }
+            }
+        }
+    }
+}
+
 __global__ void tc_frames_kernel(const int* __restrict__ len, uint32_t srcStride, int n, int W, int hop, bool center,
                                  int maxFrames, int* __restrict__ frames)
 {
@@ -507,12 +673,81 @@ __global__ void tc_frames_kernel(const int* __restrict__ len, uint32_t srcStride
         frames[b] = min(num_windows(min(len[b], int(srcStride)), W, hop, center), maxFrames);
 }
 
-template <int FMT, int EPI = kEpiPower>
-void launch_format(Handle& h, const TcArgs& a, const long long* prefix)
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver
+// library); null if the driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
-    const size_t smem = Fmt<FMT>::kStages * Fmt<FMT>::kStageBytes + 1024;
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+CUtensorMapDataType map_type(int fmt)
+{
+    // TF32 operands are FP32 words already rounded to TF32: copied bit for bit
+    return fmt == kTcTf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                          : fmt == kTcFp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+}
+
+// A tiled map with 64-byte swizzle, zero fill outside the tensor; false if the driver refuses it.
+bool encode_map(CUtensorMap* m, int fmt, int rank, const void* base, const cuuint64_t* dims,
+                const cuuint64_t* strides, const cuuint32_t* box)
+{
+    const auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint32_t one[3] = {1, 1, 1};
+    return enc(m, map_type(fmt), cuuint32_t(rank), const_cast<void*>(base), dims, strides, box, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The operands as the kernel's tensor maps see them.
+struct TcOperands
+{
+    const void* a;          // [n][clipStride] elements; frame row f of clip b starts at b * clipStride + f * rowStep
+    const void* aLo;        // split format only
+    uint32_t rowStep, clipStride;
+    int rowsPerClip;        // frame rows a clip may address
+    const void* b;          // [bRows][kPad]
+    const void* bLo;
+    int bRows;
+};
+
+template <int FMT>
+TcMaps encode_maps(const TcOperands& op, int kPad, int n)
+{
+    using T = Fmt<FMT>;
+    TcMaps maps;
+    std::memset(&maps, 0, sizeof maps);
+    const cuuint64_t e = T::kElem;
+    const cuuint64_t aDims[3] = {cuuint64_t(kPad), cuuint64_t(std::max(op.rowsPerClip, 1)), cuuint64_t(n)};
+    const cuuint64_t aStrides[2] = {op.rowStep * e, op.clipStride * e};
+    const cuuint32_t aBox[3] = {cuuint32_t(T::kBlockK), cuuint32_t(kTileM), 1};
+    const cuuint64_t bDims[2] = {cuuint64_t(kPad), cuuint64_t(op.bRows)};
+    const cuuint64_t bStrides[1] = {cuuint64_t(kPad) * e};
+    const cuuint32_t bBox[2] = {cuuint32_t(T::kBlockK), cuuint32_t(kTileN)};
+    bool ok = encode_map(&maps.a, FMT, 3, op.a, aDims, aStrides, aBox) &&
+              encode_map(&maps.b, FMT, 2, op.b, bDims, bStrides, bBox);
+    if (T::kSplit)
+        ok = ok && encode_map(&maps.aLo, FMT, 3, op.aLo, aDims, aStrides, aBox) &&
+             encode_map(&maps.bLo, FMT, 2, op.bLo, bDims, bStrides, bBox);
+    if (!ok) fail(RPP_ERROR, "cuTensorMapEncodeTiled refused an operand map of the tensor-core kernel");
+    return maps;
+}
+
+template <int FMT, int EPI = kEpiPower>
+void launch_format(Handle& h, const TcArgs& a, const TcOperands& op, const long long* prefix)
+{
+    const TcMaps maps = encode_maps<FMT>(op, a.kPad, a.n);
+    const size_t smem = size_t(Fmt<FMT>::kStages) * Fmt<FMT>::kStageBytes + 1024;
     const int grid = persistent_grid(h, reinterpret_cast<const void*>(tc_dft_kernel<FMT, EPI>), kThreads, smem);
-    tc_dft_kernel<FMT, EPI><<<grid, kThreads, smem, h.stream()>>>(a, prefix);
+    tc_dft_kernel<FMT, EPI><<<grid, kThreads, smem, h.stream()>>>(a, prefix, maps);
     count_launch(1);
     check_cuda(cudaGetLastError(), "tc_dft_kernel");
 }
@@ -708,14 +943,28 @@ __global__ void mel_frames_kernel(const int* __restrict__ dims, int n, int maxFr
 
 }  // namespace
 
-TcGeometry tc_geometry(int fmt, int windowLength, int windowStep, int maxFrames, int nfft)
+bool tc_overlap_supported(const void* anyDevicePtr)
+{
+    // one encode per process of a map whose 128 rows of 512 BF16 elements start 256 bytes apart
+    static const bool ok = [anyDevicePtr] {
+        CUtensorMap m;
+        const cuuint64_t dims[3] = {512, 128, 1};
+        const cuuint64_t strides[2] = {256, 65536};
+        const cuuint32_t box[3] = {32, 128, 1};
+        return encode_map(&m, kTcBf16, 3, anyDevicePtr, dims, strides, box);
+    }();
+    return ok;
+}
+
+TcGeometry tc_geometry(int fmt, int windowLength, int windowStep, int maxFrames, int nfft, bool overlapRows)
 {
     const int e = elem_bytes(fmt);
     const int blockK = kRowBytes / e;
     TcGeometry g;
     g.kPad = (windowLength + blockK - 1) / blockK * blockK;
     const int frames = std::max(maxFrames, 1);
-    if (fmt == kTcFp8)
+    g.materialized = fmt == kTcFp8 || !overlapRows;
+    if (g.materialized)
     {
         g.rowStep = uint32_t(g.kPad);
         g.clipStride = uint32_t(size_t(frames) * g.kPad);
@@ -807,6 +1056,20 @@ void launch_tc_spectrogram(Handle& h, void* scratch, const TcSpectrogramArgs& s)
                                                        s.windowStep, s.geo.kPad,
                                                        reinterpret_cast<__nv_fp8_e4m3*>(aHi), invScale);
     }
+    else if (s.geo.materialized)
+    {
+        dim3 pg(std::min((std::max(s.maxFrames, 1) + 7) / 8, 256), std::min(s.n, 65535));
+        const int mf = std::max(s.maxFrames, 1);
+        if (s.fmt == kTcTf32)
+            tc_prep_rows_kernel<kTcTf32><<<pg, 256, 0, h.stream()>>>(p, frames, mf, s.windowLength, s.windowStep,
+                                                                     s.geo.kPad, aHi, nullptr);
+        else if (s.fmt == kTcBf16x3)
+            tc_prep_rows_kernel<kTcBf16x3><<<pg, 256, 0, h.stream()>>>(p, frames, mf, s.windowLength, s.windowStep,
+                                                                       s.geo.kPad, aHi, aLo);
+        else
+            tc_prep_rows_kernel<kTcBf16><<<pg, 256, 0, h.stream()>>>(p, frames, mf, s.windowLength, s.windowStep,
+                                                                     s.geo.kPad, aHi, nullptr);
+    }
     else
     {
         dim3 pg(std::min<uint32_t>((s.geo.clipStride + 255) / 256, 64u), std::min(s.n, 65535));
@@ -819,13 +1082,16 @@ void launch_tc_spectrogram(Handle& h, void* scratch, const TcSpectrogramArgs& s)
     const int chunks = s.nfft / kTileN;
     launch_ragged_prefix(TcCount{frames, chunks}, s.n, prefix, h.stream());
 
+    TcOperands op;
+    op.a = aHi;
+    op.aLo = aLo;
+    op.rowStep = s.geo.rowStep;
+    op.clipStride = s.geo.clipStride;
+    op.rowsPerClip = std::max(s.maxFrames, 1);
+    op.b = s.basis;
+    op.bLo = s.fmt == kTcBf16x3 ? static_cast<const unsigned char*>(s.basis) + size_t(s.nfft) * s.geo.kPad * 2 : nullptr;
+    op.bRows = s.nfft;
     TcArgs a;
-    a.a = aHi;
-    a.aLo = aLo;
-    a.clipStride = s.geo.clipStride;
-    a.rowStep = s.geo.rowStep;
-    a.b = static_cast<const unsigned char*>(s.basis);
-    a.bLo = s.fmt == kTcBf16x3 ? a.b + size_t(s.nfft) * s.geo.kPad * 2 : nullptr;
     a.kPad = s.geo.kPad;
     a.nfft = s.nfft;
     a.invScale = invScale;
@@ -841,10 +1107,10 @@ void launch_tc_spectrogram(Handle& h, void* scratch, const TcSpectrogramArgs& s)
     a.validN = 0;
     switch (s.fmt)
     {
-    case kTcBf16: launch_format<kTcBf16>(h, a, prefix); break;
-    case kTcBf16x3: launch_format<kTcBf16x3>(h, a, prefix); break;
-    case kTcTf32: launch_format<kTcTf32>(h, a, prefix); break;
-    default: launch_format<kTcFp8>(h, a, prefix); break;
+    case kTcBf16: launch_format<kTcBf16>(h, a, op, prefix); break;
+    case kTcBf16x3: launch_format<kTcBf16x3>(h, a, op, prefix); break;
+    case kTcTf32: launch_format<kTcTf32>(h, a, op, prefix); break;
+    default: launch_format<kTcFp8>(h, a, op, prefix); break;
     }
 }
 
@@ -919,13 +1185,16 @@ void launch_tc_mel(Handle& h, void* scratch, const TcMelArgs& s)
     count_launch(1);
     launch_ragged_prefix(TcCount{frames, 1}, s.n, prefix, h.stream());
 
+    TcOperands op;
+    op.a = aHi;
+    op.aLo = aLo;
+    op.rowStep = uint32_t(kPad);
+    op.clipStride = uint32_t(size_t(maxFrames) * kPad);
+    op.rowsPerClip = maxFrames;
+    op.b = bOp;
+    op.bLo = s.fmt == kTcBf16x3 ? bOp + bBytes : nullptr;
+    op.bRows = kMelN;
     TcArgs a;
-    a.a = aHi;
-    a.aLo = aLo;
-    a.clipStride = uint32_t(size_t(maxFrames) * kPad);
-    a.rowStep = uint32_t(kPad);
-    a.b = bOp;
-    a.bLo = s.fmt == kTcBf16x3 ? bOp + bBytes : nullptr;
     a.kPad = kPad;
     a.nfft = kMelN;          // one 256-column chunk
     a.invScale = invScale;
@@ -941,10 +1210,10 @@ void launch_tc_mel(Handle& h, void* scratch, const TcMelArgs& s)
     a.validN = nf;
     switch (s.fmt)
     {
-    case kTcBf16: launch_format<kTcBf16, kEpiLinear>(h, a, prefix); break;
-    case kTcBf16x3: launch_format<kTcBf16x3, kEpiLinear>(h, a, prefix); break;
-    case kTcTf32: launch_format<kTcTf32, kEpiLinear>(h, a, prefix); break;
-    default: launch_format<kTcFp8, kEpiLinear>(h, a, prefix); break;
+    case kTcBf16: launch_format<kTcBf16, kEpiLinear>(h, a, op, prefix); break;
+    case kTcBf16x3: launch_format<kTcBf16x3, kEpiLinear>(h, a, op, prefix); break;
+    case kTcTf32: launch_format<kTcTf32, kEpiLinear>(h, a, op, prefix); break;
+    default: launch_format<kTcFp8, kEpiLinear>(h, a, op, prefix); break;
     }
 }
 
