@@ -15,19 +15,27 @@
 //   kTcTf32    FP32 rounded to TF32 (round to nearest, ties away) before the MMA;
 //   kTcFp8     E4M3; every frame is materialized and scaled so its largest sample maps to 448, the
 //              basis is scaled by 256, and the epilogue divides both scales out.
-// A is read in place from the padded signal for BF16/TF32 (frame f's row starts at f * hop, so rows
-// overlap and the 16-byte copy granule requires hop * element size to be a multiple of 16); FP8
-// frames are materialized [frame][kPad] because each carries its own scale.
+// A is read in place from the padded signal for BF16/TF32: a 3-D tensor map (window position,
+// frame, clip) whose frame rows start hop elements apart and overlap, so TMA needs hop * element
+// size to be a multiple of 16 bytes; if the driver refuses such a map, or for FP8 (each frame
+// carries its own scale), the frames are materialized [frame][kPad] first.
 //
-// Structure (one CTA per SM, 128 threads, persistent over (clip, 128-frame tile, 256-column chunk)
-// work items): shared-memory stages of A (128 rows) and B (256 rows) of one 128-byte K block each,
-// filled with cp.async in the 128-byte-swizzled K-major layout the UMMA descriptors describe; thread
-// 0 issues tcgen05.mma (M = 128, N = 256, 32 bytes of K per instruction) and commits each stage to an
-// mbarrier, so the copies of stage s+1 overlap the MMAs of stage s.  All waits are bounded: a
-// timeout sets the device error word, waits once more (bounded) for the MMAs in flight, frees
-// tensor memory and leaves.  The epilogue reads the accumulator with tcgen05.ld (warp w owns rows
-// 32w..32w+31), forms re^2 + im^2 and stores NFT rows (32 consecutive frames per warp store) or NTF
-// rows.
+// Structure: one persistent CTA per SM (192 threads; work items = (clip, 128-frame tile, 256-column
+// chunk)), warp-specialized around a ring of shared-memory stages, each one 64-byte K block of A
+// (128 rows) and B (256 rows) in the 64-byte-swizzled K-major layout (8 stages; 4 for the split
+// format, which stages hi and lo parts):
+//   warp 0, one lane: TMA producer (tiled bulk tensor loads of this GPU's memory, into this CTA only),
+//     completing bytes on the stage's "full" mbarrier;
+//   warp 1, one lane: issues tcgen05.mma (M 128, N 256, 32 bytes of K per instruction) into one of
+//     two tensor-memory accumulators and commits each stage to its "empty" mbarrier, and each
+//     finished tile to the accumulator's "full" mbarrier;
+//   warps 2-5: epilogue, tcgen05.ld of the finished accumulator (each warp its 32-lane quarter =
+//     32 frames), re^2 + im^2 (or the linear output), NFT rows (32 consecutive frames per warp store)
+//     or NTF rows, then an arrival on the accumulator's "empty" mbarrier, while the MMAs fill the
+//     other accumulator.
+// All waits are bounded: a timeout sets the device error word and a CTA abort flag that ends the
+// other roles' waits; before the tensor memory is freed the producer waits (bounded) for its last
+// loads and the MMA thread for its last MMAs.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
