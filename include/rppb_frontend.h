@@ -208,6 +208,13 @@ SHARED_PUBLIC RppStatus rppb_get_device_error(rppHandle_t rppHandle, Rpp32s* err
  * timeout path without a fault or a hang.  Off by default; affects only this handle. */
 SHARED_PUBLIC RppStatus rppb_set_wait_fault_injection(rppHandle_t rppHandle, bool enable);
 
+/* Tensor-core spectrogram setting; no counterpart in the reference.  rppb_spectrogram_tc_gpu reads the
+ * BF16/TF32 frames in place, through a tensor map whose rows (frames) start windowStep samples apart
+ * and overlap; when the driver refuses such a map it writes every frame out as a [frame][kPad] row
+ * first.  With materialize = true this handle always takes the second form (more memory traffic,
+ * the same bits), e.g. to test it.  Off by default; affects only this handle. */
+SHARED_PUBLIC RppStatus rppb_set_tc_materialized_frames(rppHandle_t rppHandle, bool materialize);
+
 #ifdef __cplusplus
 }
 #endif

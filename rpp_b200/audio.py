@@ -191,6 +191,13 @@ def set_wait_fault_injection(handle, enable):
     return _status(L.rppb_set_wait_fault_injection(_h(handle), bool(enable)))
 
 
+def set_tc_materialized_frames(handle, materialize):
+    """rppb_set_tc_materialized_frames: the tensor-core spectrogram writes frame rows out instead of
+    reading overlapping rows through its tensor map (same bits)."""
+    L = _lib.load()
+    return _status(L.rppb_set_tc_materialized_frames(_h(handle), bool(materialize)))
+
+
 def downmix_resample(src, src_desc, dst, dst_desc, in_rate, out_rate, src_dims, normalize_weights, lut, scale, center,
                      lobes, handle):
     """rppb_downmix_resample_gpu: down-mix to mono and resample in one launch."""

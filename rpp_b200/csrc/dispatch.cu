@@ -776,6 +776,14 @@ extern "C" SHARED_PUBLIC RppStatus rppb_set_wait_fault_injection(rppHandle_t rpp
     });
 }
 
+extern "C" SHARED_PUBLIC RppStatus rppb_set_tc_materialized_frames(rppHandle_t rppHandle, bool materialize)
+{
+    return guarded(rppHandle, [&](Handle& h) {
+        h.set_tc_materialize(materialize);
+        return RPP_SUCCESS;
+    });
+}
+
 extern "C" SHARED_PUBLIC RppStatus rppb_get_device_error(rppHandle_t rppHandle, Rpp32s* errorCode)
 {
     return guarded(rppHandle, [&](Handle& h) {
@@ -834,7 +842,8 @@ extern "C" SHARED_PUBLIC RppStatus rppb_spectrogram_tc_gpu(RppPtr_t srcPtr, Rppt
         if (n <= 0) return RPP_SUCCESS;
         const int maxFrames = int(nft ? dstDescPtr->w : dstDescPtr->h);
         const TcGeometry geo =
-            tc_geometry(fmt, windowLength, windowStep, maxFrames, nfft, tc_overlap_supported(h.device_flags()));
+            tc_geometry(fmt, windowLength, windowStep, maxFrames, nfft,
+                        !h.tc_materialize() && tc_overlap_supported(h.device_flags()));
         const size_t scratchBytes = tc_spectrogram_scratch_bytes(n, fmt, geo, maxFrames);
         Carver m(nullptr);
         m.take<int>(n);

@@ -100,6 +100,10 @@ class Handle
     // spectrum tile more than their clip has, with a short poll limit, so the wait runs out.
     void set_wait_injection(bool on) { wait_injection_ = on; }
     bool wait_injection() const { return wait_injection_; }
+    // rppb_set_tc_materialized_frames: the tensor-core spectrogram writes frame rows out instead of
+    // reading overlapping rows through its tensor map.
+    void set_tc_materialize(bool on) { tc_materialize_ = on; }
+    bool tc_materialize() const { return tc_materialize_; }
 
     // Extra streams of this handle (created on first use, non-blocking), for copies that overlap
     // the kernels on stream(); every call that uses them joins them back into stream() before it
@@ -146,6 +150,7 @@ class Handle
     std::map<std::string, Block> tables_;
     Block flags_;
     bool wait_injection_ = false;
+    bool tc_materialize_ = false;
 
     rppAllocatorFunction alloc_fn_ = nullptr;
     rppDeallocatorFunction free_fn_ = nullptr;

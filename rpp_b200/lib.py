@@ -19,7 +19,7 @@ EXPORTED = (
     "rppt_down_mixing_gpu", "rppt_spectrogram_gpu", "rppt_mel_filter_bank_gpu", "rppt_resample_gpu",
     "rppbGetLastError", "rppbGetLaunchCount", "rppb_frontend_gpu", "rppb_get_device_error", "rppb_set_wait_fault_injection",
     "rppb_downmix_resample_gpu", "rppt_to_decibels_gpu_static", "rppb_frontend_clips_gpu",
-    "rppb_spectrogram_tc_gpu",
+    "rppb_spectrogram_tc_gpu", "rppb_set_tc_materialized_frames",
     "rppb_frontend_host_gpu", "rppb_frontend_tune_gpu",
     "rppb_server_create", "rppb_server_destroy", "rppb_server_frames", "rppb_server_submit", "rppb_server_poll",
     "rppb_server_arena_used",
@@ -107,6 +107,8 @@ def load(path=None):
     L.rppb_get_device_error.restype = _I
     L.rppb_set_wait_fault_injection.argtypes = [_V, _B]
     L.rppb_set_wait_fault_injection.restype = _I
+    L.rppb_set_tc_materialized_frames.argtypes = [_V, _B]
+    L.rppb_set_tc_materialized_frames.restype = _I
     L.rppbGetLaunchCount.argtypes = []
     L.rppbGetLaunchCount.restype = ctypes.c_longlong
     L.rppbGetLastError.argtypes = []

@@ -79,6 +79,29 @@ def test_tc_spectrogram_many_tiles(gpu, oracle):
         assert frame_rel_err(got[i, :, :F[i]], exp[i, :, :F[i]]) < BOUND[audio.TC_BF16_HILO3]
 
 
+@pytest.mark.parametrize("precision", [audio.TC_BF16, audio.TC_BF16_HILO3, audio.TC_TF32])
+@pytest.mark.parametrize("ci", [0, 3])
+def test_tc_spectrogram_materialized_frames_same_bits(gpu, ci, precision):
+    """Frames written out as [frame][kPad] rows (the form taken when the driver refuses an
+    overlapping-row tensor map) give the same bits as frames read in place: the padding columns
+    meet zero basis entries either way, and the MMAs run in the same order."""
+    c = CASES[ci]
+    r = np.random.Generator(np.random.PCG64(101 + ci))
+    lens = r.integers(1, 60000, 7).astype(np.int32)
+    lens[0], lens[1] = 60000, c["W"] + 1
+    x, lens = synth.mono_batch(len(lens), lens, r, gaps=True)
+    coeff = r.uniform(0.9, 0.99, len(lens)).astype(np.float32)
+    maxf = int(60000 // c["hop"]) + 1
+    inplace = run_tc(gpu, x, lens, coeff, c, precision, maxf)
+    assert audio.set_tc_materialized_frames(gpu, True) == OK
+    try:
+        rows = run_tc(gpu, x, lens, coeff, c, precision, maxf)
+    finally:
+        assert audio.set_tc_materialized_frames(gpu, False) == OK
+    np.testing.assert_array_equal(rows, inplace)
+    assert audio.device_error(gpu) == 0
+
+
 def test_tc_spectrogram_rejects(gpu):
     x = np.zeros((2, 4000), np.float32)
     lens = np.array([4000, 4000], np.int32)
