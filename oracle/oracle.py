@@ -115,6 +115,9 @@ class Oracle:
         L.oracle_normalize_2d.restype = _I
         L.oracle_slice.argtypes = [ctypes.c_void_p, _L, _L, ctypes.c_void_p, _L, _L, _I, _I, _I32P, _I32P, _U32P,
                                    ctypes.c_void_p, _I, _I]
+        _LP = ctypes.POINTER(_L)
+        L.oracle_slice_nd.argtypes = [ctypes.c_void_p, _LP, ctypes.c_void_p, _LP, _I32P, _I, _I, _I, _I32P, _I32P,
+                                      _U32P, ctypes.c_void_p, _I, _I]
 
     def windowed_sinc(self, coeffs, lobes):
         """The test suite's Hann-windowed sinc table: (lut, scale, center, lobes)."""
@@ -253,6 +256,22 @@ class Oracle:
                               _p(np.ascontiguousarray(roi, np.uint32), _U32P), f.ctypes.data, int(enable_padding), es)
         return dst
 
+    def slice_nd(self, src, dst, anchor, shape, roi, fill, enable_padding, layout):
+        """3-D or 4-D slice of dense [n][...] float32 or uint8 arrays (numDims = src.ndim - 1) in the
+        given layout (0 NCHW, 1 NHWC, 2 NCDHW, 3 NDHWC); dst is updated in place and returned."""
+        nd = src.ndim - 1
+        def strides(a):
+            return (_L * (nd + 1))(*[st // a.itemsize for st in a.strides])
+        dims = np.ascontiguousarray(src.shape[1:], np.int32)
+        f = np.array([fill], dtype=src.dtype)
+        self.lib.oracle_slice_nd(src.ctypes.data, strides(src), dst.ctypes.data, strides(dst), _p(dims, _I32P),
+                                 src.shape[0], nd, int(layout),
+                                 _p(np.ascontiguousarray(anchor, np.int32), _I32P),
+                                 _p(np.ascontiguousarray(shape, np.int32), _I32P),
+                                 _p(np.ascontiguousarray(roi, np.uint32), _U32P), f.ctypes.data, int(enable_padding),
+                                 src.dtype.itemsize)
+        return dst
+
     def nsr(self, src, lengths, cutoff_db, window_length, ref_power, reset_interval, want_mms=False):
         n, ss = src.shape
         begin = np.zeros(n, np.int32)
@@ -381,6 +400,25 @@ def _reference_slice(self, src, dst, anchor, shape, roi, fill, enable_padding, n
 
 
 Reference.slice = _reference_slice
+
+
+def _reference_slice_nd(self, src, dst, anchor, shape, roi, fill, enable_padding, layout):
+    """The reference's host slice on 3-D / 4-D arrays in the given layout (dst updated in place)."""
+    from rpp_b200.types import generic_desc, RpptDataType
+    dt = RpptDataType.U8 if src.dtype == np.uint8 else RpptDataType.F32
+    sd = generic_desc(src.shape, dt, layout)
+    dd = generic_desc(dst.shape, dt, layout)
+    f = np.array([fill], dtype=src.dtype)
+    fn = self.lib.ref_slice_nd_u8 if src.dtype == np.uint8 else self.lib.ref_slice_nd_f32
+    fn.argtypes = self.lib.ref_slice_f32.argtypes
+    st = fn(src.ctypes.data, ctypes.addressof(sd), dst.ctypes.data, ctypes.addressof(dd),
+            _p(np.ascontiguousarray(anchor, np.int32), _I32P), _p(np.ascontiguousarray(shape, np.int32), _I32P),
+            f.ctypes.data, bool(enable_padding), _p(np.ascontiguousarray(roi, np.uint32), _U32P), self.h)
+    assert st == 0, st
+    return dst
+
+
+Reference.slice_nd = _reference_slice_nd
 
 
 def _reference_normalize_2d(self, src, dst, axis_mask, mean, std, compute, scale, shift, roi):

@@ -10,6 +10,7 @@
 #include "rppt_tensor_audio_augmentations.h"
 #include "handle.hpp"
 #include "host_tensor_executors.hpp"
+#include "rppi_validate.hpp"
 
 extern "C" {
 
@@ -66,6 +67,37 @@ __attribute__((visibility("default"))) int ref_slice_u8(unsigned char* src, Rppt
     RppLayoutParams lp{};
     rpp::Handle& handle = *static_cast<rpp::Handle*>(static_cast<rppHandle_t>(h));
     return slice_host_tensor<Rpp8u>(src, srcDesc, dst, dstDesc, anchor, shape, fill, enablePadding, roi, lp, handle);
+}
+
+// The same with the layout parameters rppt_slice_host derives from the source descriptor
+// (src/modules/tensor/rppt_tensor_geometric_augmentations.cpp:1074-1082), for 3-D and 4-D tensors.
+static RppLayoutParams slice_layout(const RpptGenericDesc* d)
+{
+    RppLayoutParams lp{};
+    if (d->layout == RpptLayout::NCDHW) lp = get_layout_params(d->layout, d->dims[1]);
+    else if (d->layout == RpptLayout::NDHWC) lp = get_layout_params(d->layout, d->dims[4]);
+    else if (d->layout == RpptLayout::NCHW) lp = get_layout_params(d->layout, d->dims[1]);
+    else if (d->layout == RpptLayout::NHWC) lp = get_layout_params(d->layout, d->dims[3]);
+    return lp;
+}
+
+__attribute__((visibility("default"))) int ref_slice_nd_f32(float* src, RpptGenericDesc* srcDesc, float* dst,
+                                                            RpptGenericDesc* dstDesc, int* anchor, int* shape,
+                                                            float* fill, bool enablePadding, unsigned* roi, void* h)
+{
+    rpp::Handle& handle = *static_cast<rpp::Handle*>(static_cast<rppHandle_t>(h));
+    return slice_host_tensor<Rpp32f>(src, srcDesc, dst, dstDesc, anchor, shape, fill, enablePadding, roi,
+                                     slice_layout(srcDesc), handle);
+}
+
+__attribute__((visibility("default"))) int ref_slice_nd_u8(unsigned char* src, RpptGenericDesc* srcDesc,
+                                                           unsigned char* dst, RpptGenericDesc* dstDesc, int* anchor,
+                                                           int* shape, unsigned char* fill, bool enablePadding,
+                                                           unsigned* roi, void* h)
+{
+    rpp::Handle& handle = *static_cast<rpp::Handle*>(static_cast<rppHandle_t>(h));
+    return slice_host_tensor<Rpp8u>(src, srcDesc, dst, dstDesc, anchor, shape, fill, enablePadding, roi,
+                                    slice_layout(srcDesc), handle);
 }
 
 // The reference's host normalize for F32 (src/modules/tensor/cpu/kernel/normalize.cpp:507-767),

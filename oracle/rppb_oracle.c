@@ -714,6 +714,95 @@ EXPORT void oracle_slice(const void *src, long srcStride0, long srcStride1, void
     }
 }
 
+/* ---------------------------------------------------------------- slice (3-D and 4-D)
+ * src/modules/tensor/cpu/kernel/slice.cpp:61-199, with the layout parameters of
+ * rppt_tensor_geometric_augmentations.cpp:1074-1082 (src/include/common/rppi_validate.hpp:41-64).
+ * strides: the descriptor's strides[0 .. numDims] (batch first); dims: its dims[1 .. numDims].
+ * layout: 0 NCHW, 1 NHWC (3-D), 2 NCDHW, 3 NDHWC (4-D); any other layout copies nothing.
+ * Channel-first: the spatial dims are 1.., every channel's box is copied (the channel anchor and
+ * shape are not read), and the destination advances by the SOURCE's channel stride between
+ * channels, as the reference does; channelParam is the channel count (the reference defines it
+ * for 1 and 3 channels only).  Channel-last: the spatial dims are 0.., a row copies width x
+ * channels elements.  Padding: when any spatial anchor + shape > length, the first dstStride0 - 1
+ * elements are filled first.  Negative extents copy nothing (the reference turns them into huge
+ * unsigned sizes). */
+EXPORT void oracle_slice_nd(const void *src, const long *srcStrides, void *dst, const long *dstStrides,
+                            const int *srcDims, int n, int numDims, int layout, const int *anchor, const int *shape,
+                            const unsigned *roi, const void *fill, int enablePadding, int elemSize)
+{
+    const int chFirst = (numDims == 3 && layout == 0) || (numDims == 4 && layout == 2);
+    const int chLast = (numDims == 3 && layout == 1) || (numDims == 4 && layout == 3);
+    const int sp = numDims - 1;           /* spatial dims */
+    const int o0 = chFirst ? 1 : 0;       /* first spatial dim */
+    for (int b = 0; b < n; b++)
+    {
+        const int *a = anchor + b * numDims, *s = shape + b * numDims;
+        const int *len = (const int *)(roi + b * numDims * 2 + numDims);
+        const char *sb = (const char *)src + (size_t)b * srcStrides[0] * elemSize;
+        char *db = (char *)dst + (size_t)b * dstStrides[0] * elemSize;
+        int m[3] = {1, 1, 1}, need = 0, neg = 0;
+        for (int k = 0; k < sp; k++)
+        {
+            const int d = o0 + k;
+            if (a[d] + s[d] > len[d]) need = 1;
+            m[k] = s[d] < len[d] - a[d] ? s[d] : len[d] - a[d];
+            if (m[k] <= 0) neg = 1;
+        }
+        if (need && enablePadding)
+            for (long i = 0; i < dstStrides[0] - 1; i++) memcpy(db + i * elemSize, fill, elemSize);
+        if (neg || !(chFirst || chLast)) continue;
+        if (chFirst)
+        {
+            const int C = srcDims[0];
+            long sOff = 0;
+            for (int k = 0; k < sp; k++) sOff += (long)a[o0 + k] * (k + 1 < sp ? srcStrides[o0 + k + 1] : 1);
+            long dCh = 0;
+            for (int c = 0; c < C; c++)
+            {
+                for (int i = 0; i < (sp == 3 ? m[0] : 1); i++)
+                    for (int j = 0; j < m[sp - 2]; j++)
+                    {
+                        long so = sOff + (long)c * srcStrides[1], dof = dCh;
+                        if (sp == 3)
+                        {
+                            so += (long)i * srcStrides[2] + (long)j * srcStrides[3];
+                            dof += (long)i * dstStrides[2] + (long)j * dstStrides[3];
+                        }
+                        else
+                        {
+                            so += (long)j * srcStrides[2];
+                            dof += (long)j * dstStrides[2];
+                        }
+                        memcpy(db + dof * elemSize, sb + so * elemSize, (size_t)m[sp - 1] * elemSize);
+                    }
+                dCh += srcStrides[1];   /* the source's channel stride (slice.cpp:111, :181) */
+            }
+        }
+        else
+        {
+            const int C = srcDims[numDims - 1];
+            long sOff = (long)a[0] * srcStrides[1] + (sp == 3 ? (long)a[1] * srcStrides[2] + (long)a[2] * C
+                                                              : (long)a[1] * C);
+            for (int i = 0; i < (sp == 3 ? m[0] : 1); i++)
+                for (int j = 0; j < m[sp - 2]; j++)
+                {
+                    long so = sOff, dof = 0;
+                    if (sp == 3)
+                    {
+                        so += (long)i * srcStrides[1] + (long)j * srcStrides[2];
+                        dof += (long)i * dstStrides[1] + (long)j * dstStrides[2];
+                    }
+                    else
+                    {
+                        so += (long)j * srcStrides[1];
+                        dof += (long)j * dstStrides[1];
+                    }
+                    memcpy(db + dof * elemSize, sb + so * elemSize, (size_t)m[sp - 1] * C * elemSize);
+                }
+        }
+    }
+}
+
 /* ---------------------------------------------------------------- normalize (2-D, F32)
  * src/modules/tensor/cpu/kernel/normalize.cpp:29-120 (recursive sums, inverse std dev), :417-470
  * (normalize_2D_tensor) and :507-600 (the 2-D branch of normalize_f32_f32_host_tensor);

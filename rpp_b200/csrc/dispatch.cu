@@ -899,8 +899,13 @@ extern "C" SHARED_PUBLIC RppStatus rppt_slice_gpu(RppPtr_t srcPtr, RpptGenericDe
         if (dd.dataType != F32 && dd.dataType != U8) return RPP_ERROR_INVALID_DST_DATATYPE;
         if (sd.layout != dd.layout) return RPP_ERROR_LAYOUT_MISMATCH;
         if (sd.dataType != dd.dataType) return RPP_ERROR_NOT_IMPLEMENTED;
-        // the audio path's 1-D signals and 2-D spectra; 3-D / 4-D image and voxel boxes are not built
-        if (sd.numDims < 2 || sd.numDims > 3 || dd.numDims != sd.numDims) return RPP_ERROR_NOT_IMPLEMENTED;
+        // 1-D signals and 2-D spectra in any layout; 3-D images (NCHW, NHWC) and 4-D volumes (NCDHW,
+        // NDHWC), the layouts the reference slices (cpu/kernel/slice.cpp:61-199)
+        if (sd.numDims < 2 || sd.numDims > 5 || dd.numDims != sd.numDims) return RPP_ERROR_NOT_IMPLEMENTED;
+        int layoutKind = 0;
+        if (sd.numDims == 4) layoutKind = sd.layout == NCHW ? 1 : sd.layout == NHWC ? 2 : 0;
+        if (sd.numDims == 5) layoutKind = sd.layout == NCDHW ? 1 : sd.layout == NDHWC ? 2 : 0;
+        if (sd.numDims >= 4 && layoutKind == 0) return RPP_ERROR_NOT_IMPLEMENTED;
         require(srcPtr && dstPtr && anchorTensor && shapeTensor && roiTensor, "null tensor");
         require(!enablePadding || fillValue, "null fill value");
         const int n = int(dd.dims[0]);
@@ -929,6 +934,43 @@ extern "C" SHARED_PUBLIC RppStatus rppt_slice_gpu(RppPtr_t srcPtr, RpptGenericDe
         a.srcDim0 = sd.dims[1];
         a.srcDim1 = nd == 2 ? sd.dims[2] : 1;
         if (nd == 2 && (a.dstStride1 == 0 || a.srcStride1 < a.srcDim1)) return RPP_ERROR_INVALID_ARGUMENTS;
+        a.layoutKind = layoutKind;
+        for (int k = 0; k <= nd; ++k)
+        {
+            a.srcStrides[k] = sd.strides[k];
+            a.dstStrides[k] = dd.strides[k];
+            if (k < nd)
+            {
+                a.srcDims[k] = sd.dims[k + 1];
+                a.dstDims[k] = dd.dims[k + 1];
+            }
+        }
+        if (nd >= 3)
+        {
+            // rows are contiguous, both tensors hold the same channels, and the destination's strides
+            // nest (each level at least the next level's extent), so that every destination element
+            // belongs to one box position
+            if (sd.strides[nd] != 1 || dd.strides[nd] != 1) return RPP_ERROR_INVALID_ARGUMENTS;
+            const int ch = layoutKind == 1 ? 0 : nd - 1;
+            if (sd.dims[ch + 1] != dd.dims[ch + 1]) return RPP_ERROR_INVALID_ARGUMENTS;
+            // channel-last rows are width x channels contiguous elements
+            if (layoutKind == 2 && (sd.strides[nd - 1] != sd.dims[nd] || dd.strides[nd - 1] != dd.dims[nd]))
+                return RPP_ERROR_INVALID_ARGUMENTS;
+            // destination levels, outermost first: (stride, extent of one step of the next level)
+            std::vector<std::pair<size_t, size_t>> lv;
+            if (layoutKind == 1)
+            {
+                lv.push_back({sd.strides[1], size_t(dd.dims[2]) * dd.strides[2]});   // channels step by the source's stride
+                for (int k = 2; k < nd; ++k) lv.push_back({dd.strides[k], size_t(dd.dims[k + 1]) * dd.strides[k + 1]});
+            }
+            else
+                for (int k = 1; k < nd - 1; ++k)
+                    lv.push_back({dd.strides[k], size_t(dd.dims[k + 1]) * dd.strides[k + 1]});
+            for (const auto& l : lv)
+                if (l.first < l.second) return RPP_ERROR_INVALID_ARGUMENTS;
+            if (size_t(sd.dims[ch + 1]) * (layoutKind == 1 ? sd.strides[1] : 1) > size_t(UINT32_MAX))
+                return RPP_ERROR_INVALID_ARGUMENTS;
+        }
         a.anchor = static_cast<const int*>(h.device_view(anchorTensor, size_t(n) * nd * sizeof(int), aStage));
         a.shape = static_cast<const int*>(h.device_view(shapeTensor, size_t(n) * nd * sizeof(int), sStage));
         a.roi = static_cast<const uint32_t*>(h.device_view(roiTensor, size_t(n) * nd * 2 * sizeof(uint32_t), rStage));

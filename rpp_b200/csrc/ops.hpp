@@ -170,6 +170,10 @@ struct SliceArgs
     const uint32_t* roi;         // n * numDims * 2: begins (unused), then lengths
     bool enablePadding;
     int unitsPerSample;          // set by launch_slice
+    // 3-D and 4-D boxes
+    int layoutKind;              // 1: channel-first (NCHW, NCDHW), 2: channel-last (NHWC, NDHWC)
+    uint32_t srcStrides[5], dstStrides[5];   // the descriptors' strides[0 .. numDims]
+    uint32_t srcDims[4], dstDims[4];         // the descriptors' dims[1 .. numDims]
 };
 void launch_slice(Handle& h, const SliceArgs& a, const void* src, void* dst, const void* fill);
 

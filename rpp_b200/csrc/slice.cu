@@ -1,13 +1,18 @@
-// slice: copy each sample's box [anchor, anchor + shape) of a 1-D or 2-D tensor, clipped to the
+// slice: copy each sample's box [anchor, anchor + shape) of a 1-D to 4-D tensor, clipped to the
 // sample's roi lengths, with optional fill padding.
 //
-// Reference: src/modules/tensor/cpu/kernel/slice.cpp:40-60 and :197-228 (the host path the oracle
-// restates).  Per sample b with numDims d (the batch excluded):
+// Reference: src/modules/tensor/cpu/kernel/slice.cpp:40-60 and :197-228 (1-D, 2-D), :61-196 (3-D,
+// 4-D; the host path the oracle restates).  Per sample b with numDims d (the batch excluded):
 //   maxLen_k = min(shape_k, length_k - anchor_k), length_k = roi[b * 2d + d + k] (the roi begin
 //   values are not read);
 //   if any anchor_k + shape_k > length_k and padding is enabled, elements [0, dstStride0 - 1) of the
 //   sample are set to the fill value (the last element of the sample's stride is left as it was);
 //   the clipped box is copied to the start of the sample (rows of dstStride1 in 2-D).
+// 3-D / 4-D: the box is taken over the spatial dims only (H, W or D, H, W).  Channel-first layouts
+// (NCHW, NCDHW) copy every channel, the destination stepping by the source's channel stride between
+// channels as the reference does; channel-last layouts (NHWC, NDHWC) copy rows of width x channels
+// elements.  The padding test reads the spatial dims only.  Extents are also clipped to the
+// destination's dims, which the caller's descriptors must nest (checked by the dispatch).
 // Every destination element is written at most once: the kernel decides per element whether it
 // belongs to the box (source value), to the fill range (fill value) or to neither (untouched), so
 // the reference's fill-then-copy order needs no second pass.  A negative extent copies nothing (the
@@ -89,6 +94,73 @@ __global__ void __launch_bounds__(kThreads) slice_kernel(SliceArgs a, const T* _
                     for (int j = 0; j < 4; ++j)
                         if ((written >> j & 1) && i + j < iEnd) d[i + j] = v[j];
                 }
+            }
+        }
+        else if (a.numDims >= 3)
+        {
+            // the box as up to four nested levels (outermost first) of (count, source stride,
+            // destination stride); every destination element is decoded into level indices
+            const int sp = a.numDims - 1;                  // spatial dims
+            const bool first = a.layoutKind == 1;
+            const int o0 = first ? 1 : 0;
+            int cnt[4];
+            uint32_t ss[4], ds[4];
+            int nl = 0;
+            bool none = false, padS = false;
+            size_t base = 0;
+            int m[3];
+            for (int k = 0; k < sp; ++k)
+            {
+                const int d = o0 + k;
+                if (an[d] + sh[d] > len[d]) padS = true;
+                const int ext = min(len[d], int(a.srcDims[d]));
+                m[k] = an[d] < 0 ? 0 : min(max(min(sh[d], ext - an[d]), 0), int(a.dstDims[d]));
+                if (m[k] == 0) none = true;
+            }
+            const bool padN = padS && a.enablePadding;
+            if (first)
+            {
+                cnt[nl] = int(a.srcDims[0]);
+                ss[nl] = a.srcStrides[1];
+                ds[nl++] = a.srcStrides[1];   // the source's channel stride, as the reference steps
+                for (int k = 0; k < sp; ++k)
+                {
+                    const bool inner = k + 1 == sp;
+                    cnt[nl] = m[k];
+                    ss[nl] = inner ? 1u : a.srcStrides[o0 + k + 1];
+                    ds[nl++] = inner ? 1u : a.dstStrides[o0 + k + 1];
+                    if (!none) base += size_t(an[o0 + k]) * (inner ? 1u : a.srcStrides[o0 + k + 1]);
+                }
+            }
+            else
+            {
+                const int C = int(a.srcDims[a.numDims - 1]);
+                for (int k = 0; k < sp; ++k)
+                {
+                    const bool inner = k + 1 == sp;
+                    cnt[nl] = inner ? m[k] * C : m[k];
+                    ss[nl] = inner ? 1u : a.srcStrides[1 + k];
+                    ds[nl++] = inner ? 1u : a.dstStrides[1 + k];
+                    if (!none) base += size_t(an[k]) * (inner ? uint32_t(C) : a.srcStrides[1 + k]);
+                }
+            }
+            const long long writeEnd = padN ? (long long)a.dstStride0 - 1 : (long long)a.dstStride0;
+            if (none && !padN) continue;
+            const T* sb = s + base;
+            for (long long i = i0 + threadIdx.x; i < min(iEnd, writeEnd); i += kThreads)
+            {
+                uint32_t rem = uint32_t(i);
+                bool in = !none;
+                size_t off = 0;
+                for (int l = 0; l < nl; ++l)
+                {
+                    const uint32_t q = ds[l] == 1u ? rem : rem / ds[l];
+                    rem -= q * ds[l];
+                    in = in && q < uint32_t(cnt[l]);
+                    off += size_t(q) * ss[l];
+                }
+                if (in) d[i] = sb[off];
+                else if (padN) d[i] = fv;
             }
         }
         else

@@ -491,6 +491,44 @@ def test_slice_vs_oracle(gpu, oracle, num_dims, dtype, pad):
         np.testing.assert_array_equal(host(out), exp)
 
 
+SLICE_ND = [(0, (5, 3, 37, 53)), (0, (5, 1, 29, 64)), (1, (5, 31, 47, 3)), (1, (5, 17, 40, 4)),
+            (2, (4, 3, 9, 21, 33)), (2, (4, 1, 7, 16, 24)), (3, (4, 8, 19, 27, 3)), (3, (4, 6, 11, 13, 2))]
+
+
+@pytest.mark.parametrize("case", range(len(SLICE_ND)))
+@pytest.mark.parametrize("dtype", [np.float32, np.uint8])
+@pytest.mark.parametrize("pad", [False, True])
+def test_slice_nd_vs_oracle(gpu, oracle, case, dtype, pad):
+    """3-D (NCHW, NHWC) and 4-D (NCDHW, NDHWC) boxes: random anchors (some beyond the roi length:
+    nothing copied), shapes and roi lengths, bit for bit against the restatement of the
+    reference's host slice, the rest of the destination untouched."""
+    from rpp_b200.types import generic_desc, RpptDataType
+    layout, shp = SLICE_ND[case]
+    r = np.random.Generator(np.random.PCG64(177 + case))
+    n, ext = shp[0], np.array(shp[1:])
+    src = (r.integers(0, 255, shp).astype(np.uint8) if dtype == np.uint8
+           else r.standard_normal(shp).astype(np.float32))
+    length = np.stack([r.integers(1, e + 1, n) for e in ext], 1).astype(np.int32)
+    anchor = np.stack([r.integers(0, e, n) for e in ext], 1).astype(np.int32)
+    shape = np.stack([r.integers(1, e + 1, n) for e in ext], 1).astype(np.int32)
+    anchor[0] = 0
+    length[0] = ext
+    shape[0] = ext                                     # the whole first sample
+    roi = np.concatenate([np.zeros_like(length), length], 1).astype(np.uint32).ravel()
+    fill = np.array([5 if dtype == np.uint8 else -2.5], dtype)
+    dt = RpptDataType.U8 if dtype == np.uint8 else RpptDataType.F32
+    d = generic_desc(shp, dt, layout)
+    canvas_v = 9 if dtype == np.uint8 else 9.75
+    out = torch.from_numpy(np.full(shp, canvas_v, dtype)).cuda()
+    st = audio.slice(dev(src), d, out, d, anchor.ravel(), shape.ravel(), fill, pad, roi, gpu)
+    assert st == RppStatus.RPP_SUCCESS
+    exp = np.full(shp, canvas_v, dtype)
+    oracle.slice_nd(src, exp, anchor.ravel(), shape.ravel(), roi, fill[0], pad, layout)
+    got = host(out)
+    np.testing.assert_array_equal(got, exp)
+    np.testing.assert_array_equal(got[0], src[0])
+
+
 def test_slice_status_codes(gpu):
     from rpp_b200.types import generic_desc, RpptDataType, RpptLayout
     x = torch.zeros((2, 100), device="cuda")
@@ -504,8 +542,20 @@ def test_slice_status_codes(gpu):
     assert audio.slice(x, d, x, bad, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_INVALID_DST_DATATYPE
     other = generic_desc((2, 100), layout=RpptLayout.NHWC)
     assert audio.slice(x, d, x, other, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_LAYOUT_MISMATCH
-    d4 = generic_desc((2, 1, 10, 10))
+    # 3-D / 4-D tensors in layouts the reference does not slice
+    d4 = generic_desc((2, 1, 10, 10), layout=RpptLayout.NFT)
     assert audio.slice(x, d4, x, d4, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_NOT_IMPLEMENTED
+    d5 = generic_desc((2, 1, 2, 5, 10), layout=RpptLayout.NCHW)
+    assert audio.slice(x, d5, x, d5, a, s, f, True, roi, gpu) == RppStatus.RPP_ERROR_NOT_IMPLEMENTED
+    # channel counts must match; destination strides must nest
+    a3, s3 = np.zeros(6, np.int32), np.full(6, 2, np.int32)
+    roi3 = np.tile(np.array([0, 0, 0, 1, 10, 10], np.uint32), 2)
+    src3 = generic_desc((2, 1, 10, 10))
+    dst3 = generic_desc((2, 2, 10, 5))
+    assert audio.slice(x, src3, x, dst3, a3, s3, f, True, roi3, gpu) == RppStatus.RPP_ERROR_INVALID_ARGUMENTS
+    squeezed = generic_desc((2, 1, 10, 10))
+    squeezed.strides[2] = 5   # rows of 10 elements 5 apart
+    assert audio.slice(x, src3, x, squeezed, a3, s3, f, True, roi3, gpu) == RppStatus.RPP_ERROR_INVALID_ARGUMENTS
 
 
 # ---------------------------------------------------------------- normalize (api/rppt_tensor_statistical_operations.h:193)

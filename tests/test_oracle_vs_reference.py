@@ -180,6 +180,43 @@ def test_slice(oracle, reference, num_dims, dtype, pad):
     np.testing.assert_array_equal(a, b)
 
 
+SLICE_ND = [(RpptLayout.NCHW, (5, 3, 37, 53)), (RpptLayout.NCHW, (5, 1, 29, 64)), (RpptLayout.NHWC, (5, 31, 47, 3)),
+            (RpptLayout.NHWC, (5, 17, 40, 4)), (RpptLayout.NCDHW, (4, 3, 9, 21, 33)),
+            (RpptLayout.NCDHW, (4, 1, 7, 16, 24)), (RpptLayout.NDHWC, (4, 8, 19, 27, 3)),
+            (RpptLayout.NDHWC, (4, 6, 11, 13, 2))]
+
+
+def slice_nd_case(r, shp, layout):
+    """Random per-sample roi lengths, anchors below them (the reference turns a negative extent
+    into a huge unsigned size) and shapes, one sample reaching past its lengths (padding)."""
+    n, ext = shp[0], np.array(shp[1:])
+    length = np.stack([r.integers(max(e // 2, 1), e + 1, n) for e in ext], 1).astype(np.int32)
+    anchor = np.stack([r.integers(0, max(e // 2, 1), n) for e in ext], 1).astype(np.int32)
+    shape = np.stack([r.integers(1, e + 1, n) for e in ext], 1).astype(np.int32)
+    shape[1] = ext - anchor[1]
+    roi = np.concatenate([np.zeros_like(length), length], 1).astype(np.uint32)
+    return anchor.ravel(), shape.ravel(), roi.ravel()
+
+
+@pytest.mark.parametrize("case", range(len(SLICE_ND)))
+@pytest.mark.parametrize("dtype", [np.float32, np.uint8])
+@pytest.mark.parametrize("pad", [False, True])
+def test_slice_nd(oracle, reference, case, dtype, pad):
+    """3-D and 4-D boxes in the four layouts the reference slices (NCHW / NHWC, NCDHW / NDHWC)."""
+    layout, shp = SLICE_ND[case]
+    r = rng(70 + case)
+    src = (r.integers(0, 255, shp).astype(np.uint8) if dtype == np.uint8
+           else r.standard_normal(shp).astype(np.float32))
+    anchor, shape, roi = slice_nd_case(r, shp, layout)
+    fill = 7 if dtype == np.uint8 else -3.5
+    a = np.full_like(src, 9 if dtype == np.uint8 else 9.25)
+    b = a.copy()
+    oracle.slice_nd(src, a, anchor, shape, roi, fill, pad, int(layout))
+    reference.slice_nd(src, b, anchor, shape, roi, fill, pad, int(layout))
+    np.testing.assert_array_equal(a, b)
+    assert (a != (9 if dtype == np.uint8 else 9.25)).any()
+
+
 @pytest.mark.parametrize("axis_mask", [1, 2, 3])
 @pytest.mark.parametrize("compute", [0, 1, 2, 3])
 def test_normalize_2d(oracle, reference, axis_mask, compute):
