@@ -116,6 +116,9 @@ class Oracle:
         L.oracle_slice.argtypes = [ctypes.c_void_p, _L, _L, ctypes.c_void_p, _L, _L, _I, _I, _I32P, _I32P, _U32P,
                                    ctypes.c_void_p, _I, _I]
         _LP = ctypes.POINTER(_L)
+        L.oracle_normalize_nd.argtypes = [ctypes.c_void_p, _I, _LP, _I, _I32P, ctypes.c_void_p, _I, _LP, _I, _I, _I,
+                                          ctypes.c_uint, _F32P, _F32P, _I, _F, _F, _U32P]
+        L.oracle_normalize_nd.restype = _I
         L.oracle_slice_nd.argtypes = [ctypes.c_void_p, _LP, ctypes.c_void_p, _LP, _I32P, _I, _I, _I, _I32P, _I32P,
                                       _U32P, ctypes.c_void_p, _I, _I]
 
@@ -270,6 +273,25 @@ class Oracle:
                                  _p(np.ascontiguousarray(shape, np.int32), _I32P),
                                  _p(np.ascontiguousarray(roi, np.uint32), _U32P), f.ctypes.data, int(enable_padding),
                                  src.dtype.itemsize)
+        return dst
+
+    NORMALIZE_TYPES = {np.dtype(np.float32): 0, np.dtype(np.float16): 1, np.dtype(np.uint8): 2, np.dtype(np.int8): 3}
+
+    def normalize_nd(self, src, dst, axis_mask, mean, std, compute, scale, shift, roi, src_layout=0, dst_layout=0):
+        """rppt_normalize on dense [n][...] arrays of any rank and element type (float32, float16,
+        uint8, int8): the F32 3-D branch or the N-D branch of the reference host path (the F32 2-D
+        branch is normalize_2d).  mean / std are in-out arrays as in the reference; dst is updated in
+        place and returned."""
+        T = src.ndim - 1
+        def strides(a):
+            return (_L * (T + 1))(*[st // a.itemsize for st in a.strides])
+        dims = np.ascontiguousarray(src.shape[1:], np.int32)
+        st = self.lib.oracle_normalize_nd(src.ctypes.data, self.NORMALIZE_TYPES[src.dtype], strides(src), int(src_layout),
+                                          _p(dims, _I32P), dst.ctypes.data, self.NORMALIZE_TYPES[dst.dtype],
+                                          strides(dst), int(dst_layout), src.shape[0], T, int(axis_mask),
+                                          _p(mean, _F32P), _p(std, _F32P), int(compute), float(scale), float(shift),
+                                          _p(np.ascontiguousarray(roi, np.uint32), _U32P))
+        assert st == 0, st
         return dst
 
     def nsr(self, src, lengths, cutoff_db, window_length, ref_power, reset_interval, want_mms=False):
@@ -436,3 +458,24 @@ def _reference_normalize_2d(self, src, dst, axis_mask, mean, std, compute, scale
 
 
 Reference.normalize_2d = _reference_normalize_2d
+
+
+def _reference_normalize_nd(self, src, dst, axis_mask, mean, std, compute, scale, shift, roi, src_layout=0,
+                            dst_layout=0):
+    """The reference's host normalize (F32 any rank; U8; I8 through its unsigned destination) on
+    the same arrays as Oracle.normalize_nd."""
+    from rpp_b200.types import generic_desc, RpptDataType
+    dt = {np.dtype(np.float32): RpptDataType.F32, np.dtype(np.uint8): RpptDataType.U8,
+          np.dtype(np.int8): RpptDataType.I8}
+    sd, dd = generic_desc(src.shape, dt[src.dtype], src_layout), generic_desc(dst.shape, dt[dst.dtype], dst_layout)
+    L = self.lib
+    L.ref_normalize_nd.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint,
+                                   _F32P, _F32P, ctypes.c_ubyte, _F, _F, _U32P, ctypes.c_void_p]
+    st = L.ref_normalize_nd(src.ctypes.data, ctypes.addressof(sd), dst.ctypes.data, ctypes.addressof(dd),
+                            int(axis_mask), _p(mean, _F32P), _p(std, _F32P), int(compute), float(scale), float(shift),
+                            _p(np.ascontiguousarray(roi, np.uint32), _U32P), self.h)
+    assert st == 0, st
+    return dst
+
+
+Reference.normalize_nd = _reference_normalize_nd

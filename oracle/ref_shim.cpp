@@ -103,6 +103,39 @@ __attribute__((visibility("default"))) int ref_slice_nd_u8(unsigned char* src, R
 // The reference's host normalize for F32 (src/modules/tensor/cpu/kernel/normalize.cpp:507-767),
 // called at the kernel level for the same reason as slice; the 2-D branch reads no layout
 // parameters.
+// The layout parameters rppt_normalize_host derives (src/modules/tensor/rppt_tensor_statistical_operations.cpp:
+// 259-266) and the host normalize on them: F32 at any rank, and the generic path for U8 -> U8 and
+// I8 (written through an unsigned pointer, as the reference dispatch does).
+static RppLayoutParams normalize_layout(const RpptGenericDesc* s, const RpptGenericDesc* d)
+{
+    RppLayoutParams lp{};
+    const unsigned tensorDim = s->numDims - 1;
+    if (tensorDim == 3 && s->layout == RpptLayout::NHWC) lp = get_layout_params(s->layout, s->dims[3]);
+    else if (s->layout == RpptLayout::NCDHW && d->layout == RpptLayout::NCDHW) lp = get_layout_params(s->layout, s->dims[1]);
+    else if (s->layout == RpptLayout::NDHWC && d->layout == RpptLayout::NDHWC) lp = get_layout_params(s->layout, s->dims[4]);
+    else if (tensorDim == 2 && s->layout == RpptLayout::NHWC) lp = get_layout_params(s->layout, s->dims[2]);
+    return lp;
+}
+
+__attribute__((visibility("default"))) int ref_normalize_nd(void* src, RpptGenericDesc* srcDesc, void* dst,
+                                                            RpptGenericDesc* dstDesc, unsigned axisMask, float* mean,
+                                                            float* stdDev, unsigned char computeMeanStddev,
+                                                            float scale, float shift, unsigned* roi, void* h)
+{
+    rpp::Handle& handle = *static_cast<rpp::Handle*>(static_cast<rppHandle_t>(h));
+    const RppLayoutParams lp = normalize_layout(srcDesc, dstDesc);
+    if (srcDesc->dataType == RpptDataType::F32)
+        return normalize_f32_f32_host_tensor(static_cast<Rpp32f*>(src), srcDesc, static_cast<Rpp32f*>(dst), dstDesc,
+                                             axisMask, mean, stdDev, computeMeanStddev, scale, shift, roi, lp, handle);
+    if (srcDesc->dataType == RpptDataType::U8)
+        return normalize_generic_host_tensor(static_cast<Rpp8u*>(src), srcDesc, static_cast<Rpp8u*>(dst), dstDesc,
+                                             axisMask, mean, stdDev, computeMeanStddev, scale, shift, roi, lp, handle);
+    if (srcDesc->dataType == RpptDataType::I8)
+        return normalize_generic_host_tensor(static_cast<Rpp8s*>(src), srcDesc, static_cast<Rpp8u*>(dst), dstDesc,
+                                             axisMask, mean, stdDev, computeMeanStddev, scale, shift, roi, lp, handle);
+    return -1;
+}
+
 __attribute__((visibility("default"))) int ref_normalize_f32(float* src, RpptGenericDesc* srcDesc, float* dst,
                                                              RpptGenericDesc* dstDesc, unsigned axisMask, float* mean,
                                                              float* stdDev, unsigned char computeMeanStddev, float scale,

@@ -968,3 +968,382 @@ EXPORT int oracle_normalize_2d(const float *src, long srcStride0, long srcStride
     }
     return 0;
 }
+
+/* ---------------------------------------------------------------- normalize (N-D, all types; F32 3-D)
+ * src/modules/tensor/cpu/kernel/normalize.cpp:122-244 (3-D and N-D statistics), :244-415 (3-D and
+ * N-D normalization), :472-505 (collapse_axis), :507-767 (normalize_f32_f32_host_tensor's 3-D and
+ * N-D branches) and :768-868 (normalize_generic_host_tensor, used for U8 / F16 / I8 at every rank);
+ * rpp_rsqrt_avx of src/include/common/cpu/rpp_cpu_simd_math.hpp:936-986.
+ * Element types: 0 F32, 1 F16, 2 U8, 3 I8.  Deliberate differences from the host path, which this
+ * library follows instead of it: integer results are clamped to the type's range before the
+ * truncating conversion (the host's conversion of an out-of-range float is undefined; in range
+ * both truncate), I8 values are read and written as signed (the host reads them through an
+ * unsigned cast and writes unsigned bytes), and F16 results are rounded to nearest even. */
+static float h2f(unsigned short h)
+{
+    const unsigned sign = (unsigned)(h & 0x8000) << 16, e = (h >> 10) & 31, m = h & 1023;
+    unsigned u;
+    if (e == 31) u = sign | 0x7f800000u | (m << 13);
+    else if (e) u = sign | ((e + 112) << 23) | (m << 13);
+    else
+    {
+        float v = (float)m * (1.0f / 16777216.0f);   /* subnormal: m * 2^-24, exact */
+        memcpy(&u, &v, 4);
+        u |= sign;
+    }
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+static unsigned short f2h(float f)   /* round to nearest even */
+{
+    unsigned u;
+    memcpy(&u, &f, 4);
+    const unsigned sign = (u >> 16) & 0x8000, a = u & 0x7fffffffu;
+    if (a >= 0x7f800000u) return (unsigned short)(sign | (a > 0x7f800000u ? 0x7e00 : 0x7c00));
+    if (a >= 0x477ff000u) return (unsigned short)(sign | 0x7c00);   /* >= 65520: infinity */
+    if (a < 0x38800000u)                                             /* below 2^-14: subnormal */
+    {
+        float v;
+        memcpy(&v, &a, 4);
+        return (unsigned short)(sign | (unsigned)nearbyintf(v * 16777216.0f));
+    }
+    const unsigned mant = a & 0x7fffff, rem = mant & 0x1fff;
+    unsigned h = ((((a >> 23) - 112) << 10) | (mant >> 13));
+    if (rem > 0x1000 || (rem == 0x1000 && (h & 1))) h++;
+    return (unsigned short)(sign | h);
+}
+
+static float ld_t(const void *p, int t, long i)
+{
+    switch (t)
+    {
+    case 0: return ((const float *)p)[i];
+    case 1: return h2f(((const unsigned short *)p)[i]);
+    case 2: return (float)((const unsigned char *)p)[i];
+    default: return (float)((const signed char *)p)[i];
+    }
+}
+
+static void st_t(void *p, int t, long i, float v)
+{
+    switch (t)
+    {
+    case 0: ((float *)p)[i] = v; break;
+    case 1: ((unsigned short *)p)[i] = f2h(v); break;
+    case 2: ((unsigned char *)p)[i] = (unsigned char)(v > 255.f ? 255.f : v < 0.f ? 0.f : v); break;
+    default: ((signed char *)p)[i] = (signed char)(v > 127.f ? 127.f : v < -128.f ? -128.f : v); break;
+    }
+}
+
+static int esize_t(int t) { return t == 0 ? 4 : t == 1 ? 2 : 1; }
+
+static void t_sum(float *out, const char *in, int t, long stride, long n)
+{
+    if (n > 32)
+    {
+        long h = n >> 1;
+        float t1 = 0, t2 = 0;
+        t_sum(&t1, in, t, stride, h);
+        t_sum(&t2, in + h * stride * esize_t(t), t, stride, n - h);
+        t1 += t2;
+        *out += t1;
+    }
+    else
+    {
+        float tmp = 0;
+        for (long i = 0; i < n; i++) tmp += ld_t(in, t, i * stride);
+        *out += tmp;
+    }
+}
+
+static void t_dsq(float *out, const char *in, int t, long stride, long n, float mean)
+{
+    if (n > 32)
+    {
+        long h = n >> 1;
+        float t1 = 0, t2 = 0;
+        t_dsq(&t1, in, t, stride, h, mean);
+        t_dsq(&t2, in + h * stride * esize_t(t), t, stride, n - h, mean);
+        t1 += t2;
+        *out += t1;
+    }
+    else
+    {
+        float tmp = 0;
+        for (long i = 0; i < n; i++)
+        {
+            float c = ld_t(in, t, i * stride) - mean;
+            float c2 = c * c;
+            tmp += c2;
+        }
+        *out += tmp;
+    }
+}
+
+__attribute__((target("avx"))) static void n_rsqrt_avx(float *v, long n, float rdiv, float scale)
+{
+    long i = 0;
+    const __m256 r = _mm256_set1_ps(rdiv), m = _mm256_set1_ps(scale * 0.5f), three = _mm256_set1_ps(3.0f);
+    for (; i + 8 <= n; i += 8)
+    {
+        __m256 x = _mm256_mul_ps(_mm256_loadu_ps(v + i), r);
+        __m256 mask = _mm256_cmp_ps(x, _mm256_setzero_ps(), _CMP_NEQ_OQ);
+        __m256 y = _mm256_and_ps(_mm256_rsqrt_ps(x), mask);
+        __m256 xy2 = _mm256_mul_ps(x, _mm256_mul_ps(y, y));
+        y = _mm256_mul_ps(_mm256_mul_ps(y, _mm256_sub_ps(three, xy2)), m);
+        _mm256_storeu_ps(v + i, y);
+    }
+    for (; i < n; i++)
+    {
+        float x = v[i] * rdiv;
+        v[i] = x ? n_rsqrt_ps(x) * scale : 0;
+    }
+}
+
+/* compute_ND_mean / compute_ND_stddev (normalize.cpp:200-242), restated with the same recursion. */
+static void nd_stat(int sq, const char *src, int t, float *mean, float *std, const unsigned *dims, const unsigned *stride,
+                    const unsigned *axis, unsigned T, unsigned level, unsigned index, unsigned size, unsigned norm,
+                    unsigned last)
+{
+    const int es = esize_t(t);
+    if (level == T - 1 && axis[T - 1])
+    {
+        if (sq) t_dsq(&std[index], src, t, stride[level], dims[level], mean[index]);
+        else t_sum(&mean[index], src, t, stride[level], dims[level]);
+    }
+    else if (level == T)
+    {
+        if (sq) t_dsq(&std[index], src, t, stride[norm], dims[norm], mean[index]);
+        else t_sum(&mean[index], src, t, stride[norm], dims[norm]);
+    }
+    else if (!axis[level])
+    {
+        for (unsigned i = 0; i < dims[level]; i++)
+            nd_stat(sq, src + (long)i * stride[level] * es, t, mean, std, dims, stride, axis, T, level + 1,
+                    index + i * (size / dims[level]), size / dims[level], norm, last);
+    }
+    else if (level == last)
+        nd_stat(sq, src, t, mean, std, dims, stride, axis, T, level + 1, index, size, level, last);
+    else
+        for (unsigned i = 0; i < dims[level]; i++)
+            nd_stat(sq, src + (long)i * stride[level] * es, t, mean, std, dims, stride, axis, T, level + 1, index,
+                    size, level, last);
+}
+
+/* The 3-D statistics (normalize.cpp:122-198): dims/stride are the srcReductionDims / srcStride of
+ * the axis mask; params i * dims[1] + j (consecutive) or i. */
+static void stat3d(int sq, const float *src, float *mean, float *std, const unsigned *dims, const unsigned *stride,
+                   float scale, int consecutive)
+{
+    if (consecutive)
+    {
+        float nf = (float)(1.0 / dims[2]);
+        const float *p = src;
+        for (unsigned i = 0; i < dims[0]; i++)
+        {
+            const float *row = p;
+            for (unsigned j = 0; j < dims[1]; j++)
+            {
+                unsigned idx = i * dims[1] + j;
+                if (sq)
+                {
+                    std[idx] = 0;
+                    t_dsq(&std[idx], (const char *)row, 0, stride[0], dims[2], mean[idx]);
+                }
+                else
+                {
+                    mean[idx] = 0;
+                    t_sum(&mean[idx], (const char *)row, 0, stride[0], dims[2]);
+                    mean[idx] *= nf;
+                }
+                row += stride[1];
+            }
+            p += stride[2];
+        }
+        if (sq) n_rsqrt_avx(std, (long)dims[0] * dims[1], nf, scale);
+    }
+    else
+    {
+        float nf = (float)(1.0 / (dims[1] * dims[2]));
+        const float *p = src;
+        for (unsigned i = 0; i < dims[0]; i++)
+        {
+            if (sq) std[i] = 0;
+            else mean[i] = 0;
+            const float *row = p;
+            for (unsigned j = 0; j < dims[1]; j++)
+            {
+                if (sq) t_dsq(&std[i], (const char *)row, 0, stride[0], dims[2], mean[i]);
+                else t_sum(&mean[i], (const char *)row, 0, stride[0], dims[2]);
+                row += stride[1];
+            }
+            if (!sq) mean[i] *= nf;
+            p += stride[2];
+        }
+        if (sq) n_rsqrt_avx(std, dims[0], nf, scale);
+    }
+}
+
+/* srcStrides / dstStrides: the descriptors' strides[0 .. tensorDims]; layouts 0 NCHW, 1 NHWC. */
+EXPORT int oracle_normalize_nd(const void *src, int srcType, const long *srcStrides, int srcLayout, const int *srcDims,
+                               void *dst, int dstType, const long *dstStrides, int dstLayout, int n, int tensorDims,
+                               unsigned axisMask, float *mean, float *std, int compute, float scale, float shift,
+                               const unsigned *roi)
+{
+    const int T = tensorDims, ses = esize_t(srcType), des = esize_t(dstType);
+    unsigned maxSize = 1;
+    for (int b = 0; b < n; b++)
+    {
+        unsigned size = 1;
+        for (int i = 0; i < T; i++) size *= (axisMask & (1u << i)) ? 1 : roi[T * 2 * b + T + i];
+        if (size > maxSize) maxSize = size;
+    }
+    if (!compute)
+    {
+        for (unsigned i = 0; i < maxSize; i++) std[i] = !std[i] ? 1.0f : scale / std[i];
+        maxSize = 0;
+    }
+    for (int b = 0; b < n; b++)
+    {
+        const unsigned *begin = roi + b * T * 2, *length = begin + T;
+        const char *sb = (const char *)src + (long)b * srcStrides[0] * ses;
+        char *db = (char *)dst + (long)b * dstStrides[0] * des;
+        float *m = mean + (long)b * maxSize, *sd = std + (long)b * maxSize;
+        for (long c = 0; c < dstStrides[0]; c++) st_t(db, dstType, c, 0.0f);
+        if (srcType == 0 && T == 3)
+        {
+            unsigned rd[3] = {0, 0, 0}, rs[3] = {0, 0, 0}, ps[3] = {0, 0, 0};
+            const unsigned L0 = length[0], L1 = length[1], L2 = length[2];
+            const unsigned S1 = srcStrides[1], S2 = srcStrides[2], S3 = srcStrides[3];
+            int consecutive = 1;
+            switch (axisMask)
+            {
+            case 1: rd[0] = L1; rd[1] = L2; rd[2] = L0; rs[0] = S1; rs[1] = S3; rs[2] = S2; ps[1] = ps[2] = 1; break;
+            case 2: rd[0] = L0; rd[1] = L2; rd[2] = L1; rs[0] = S2; rs[1] = S3; rs[2] = S1; ps[0] = ps[2] = 1; break;
+            case 3: rd[0] = 1; rd[1] = L2; rd[2] = L0 * L1; rs[0] = S2; rs[1] = S3; rs[2] = S3; ps[2] = 1; break;
+            case 4: rd[0] = L0; rd[1] = L1; rd[2] = L2; rs[0] = S3; rs[1] = S2; rs[2] = S1; ps[0] = ps[1] = 1; break;
+            case 5: rd[0] = L1; rd[1] = L0; rd[2] = L2; rs[0] = S3; rs[1] = S1; rs[2] = S2; ps[1] = 1; consecutive = 0;
+                break;
+            case 6: rd[0] = 1; rd[1] = L0; rd[2] = L1 * L2; rs[0] = S3; rs[1] = S1; rs[2] = S3; ps[0] = 1; break;
+            case 7: rd[0] = 1; rd[1] = 1; rd[2] = L0 * L1 * L2; rs[0] = rs[1] = rs[2] = S3; break;
+            default: return -1;
+            }
+            const float *ch = (const float *)sb + (long)begin[0] * S1 + (long)begin[1] * S2;
+            if (compute & 1) stat3d(0, ch, m, sd, rd, rs, scale, consecutive);
+            if (compute & 2) stat3d(1, ch, m, sd, rd, rs, scale, consecutive);
+            float *d = (float *)db;
+            if (axisMask == 3 && srcLayout == 1 && dstLayout == 1 && srcDims[2] == 16)
+            {
+                /* normalize_3D_tensor_avx_axis3: 16 channel parameters over whole rows */
+                unsigned bl = L1 * 16, al = bl / 16 * 16;
+                for (unsigned i = 0; i < L0; i++)
+                    for (unsigned v = 0; v < al; v++)
+                        d[(long)i * dstStrides[1] + v] = ((ch[(long)i * S1 + v] - m[v % 16]) * sd[v % 16]) + shift;
+            }
+            else if (srcLayout == 1 && dstLayout == 1)
+            {
+                for (unsigned i = 0; i < L0; i++)
+                    for (unsigned j = 0; j < L1; j++)
+                        for (unsigned k = 0; k < L2; k++)
+                        {
+                            unsigned p = (ps[0] ? i : 0);
+                            p = p * (ps[1] ? L1 : 1) + (ps[1] ? j : 0);
+                            p = p * (ps[2] ? L2 : 1) + (ps[2] ? k : 0);
+                            d[(long)i * dstStrides[1] + (long)j * dstStrides[2] + k] =
+                                ((ch[(long)i * S1 + (long)j * S2 + k] - m[p]) * sd[p]) + shift;
+                        }
+            }
+            else if (axisMask == 3 && srcLayout == 1 && dstLayout == 0)
+            {
+                for (unsigned i = 0; i < L0; i++)
+                    for (unsigned j = 0; j < L1; j++)
+                        for (unsigned k = 0; k < L2; k++)
+                            d[(long)k * dstStrides[1] + (long)i * dstStrides[2] + (long)j * dstStrides[3]] =
+                                ((ch[(long)i * S1 + (long)j * S2 + k] - m[k]) * sd[k]) + shift;
+            }
+            continue;
+        }
+        /* N-D: normalize_generic_host_tensor / the N-D branch of normalize_f32_f32_host_tensor */
+        unsigned size = 1, total = 1, axis[16], newAxis[16], newDims[16], lastNorm = 0;
+        const char *ch = sb;
+        for (int i = 0; i < T; i++)
+        {
+            axis[i] = (axisMask & (1u << i)) ? 1 : 0;
+            size *= axis[i] ? 1 : length[i];
+            total *= axis[i] ? length[i] : 1;
+            ch += (long)begin[i] * srcStrides[i + 1] * ses;
+            newAxis[i] = newDims[i] = 0;
+        }
+        /* collapse_axis (normalize.cpp:472-505) */
+        int skipped = 0, prev = -2, k = 0;
+        unsigned nT = T;
+        for (int i = 0; i < T; i++)
+        {
+            if (axis[i])
+            {
+                int temp = i - skipped;
+                if (temp != prev + 1)
+                {
+                    newAxis[k] = 1;
+                    newDims[k] = length[i];
+                    prev = i;
+                    k++;
+                }
+                else if (prev >= 0)
+                {
+                    newDims[prev] *= length[i];
+                    skipped++;
+                }
+            }
+            else
+            {
+                newDims[k] = length[i];
+                k++;
+            }
+        }
+        nT -= skipped;
+        for (unsigned i = 0; i < nT; i++)
+            if (newAxis[i]) lastNorm = i;
+        unsigned dstr[16];
+        {
+            unsigned v = 1;
+            for (unsigned i = nT - 1; i > 0; i--)
+            {
+                dstr[i] = v;
+                v *= newDims[i];
+            }
+            dstr[0] = v;
+        }
+        if (compute & 1)
+        {
+            nd_stat(0, ch, srcType, m, sd, newDims, dstr, newAxis, nT, 0, 0, size, 0, lastNorm);
+            float nf = 1.0 / total;
+            for (unsigned i = 0; i < size; i++) m[i] *= nf;
+        }
+        if (compute & 2)
+        {
+            nd_stat(1, ch, srcType, m, sd, newDims, dstr, newAxis, nT, 0, 0, size, 0, lastNorm);
+            float nf = (float)(1.0 / total);
+            n_rsqrt_avx(sd, size, nf, scale);
+        }
+        /* normalize_ND_tensor_nontoggle: dense positions from the roi start (source) and the sample
+         * start (destination); the parameter is the row-major index over the unnormalized dims */
+        long count = 1;
+        for (unsigned i = 0; i < nT; i++) count *= newDims[i];
+        for (long e = 0; e < count; e++)
+        {
+            long rem = e;
+            unsigned p = 0;
+            for (unsigned l = 0; l < nT; l++)
+            {
+                unsigned c = (unsigned)(rem / dstr[l]);
+                rem -= (long)c * dstr[l];
+                if (!newAxis[l]) p = p * newDims[l] + c;
+            }
+            st_t(db, dstType, e, ((ld_t(ch, srcType, e) - m[p]) * sd[p]) + shift);
+        }
+    }
+    return 0;
+}

@@ -245,3 +245,125 @@ def test_normalize_2d(oracle, reference, axis_mask, compute):
     np.testing.assert_array_equal(outs[0][0], outs[1][0])
     np.testing.assert_array_equal(outs[0][1], outs[1][1])
     np.testing.assert_array_equal(outs[0][2], outs[1][2])
+
+
+def normalize_nd_case(r, shp, axis_mask, compute, dtype, begin_fits=False):
+    """Source, roi and in-out statistics for a normalize case; integer sources keep their results
+    inside the type's range (where the host path's float-to-integer conversion is defined)."""
+    n, ext = shp[0], np.array(shp[1:])
+    T = len(ext)
+    if dtype == np.float32:
+        src = (r.standard_normal(shp) * 3 + 1).astype(np.float32)
+    elif dtype == np.uint8:
+        src = r.integers(0, 256, shp).astype(np.uint8)
+    else:
+        src = r.integers(0, 128, shp).astype(np.int8)   # non-negative: the host path reads int8 as unsigned
+    roi = np.zeros((n, 2 * T), np.uint32)
+    roi[:, T:] = ext
+    if begin_fits:
+        # a dense region of the roi lengths from the begin offset, inside the sample
+        roi[1:, T:] = np.maximum(ext // 2, 1)
+        roi[1:, 0] = 1
+    size = max(int(np.prod([1 if axis_mask & (1 << i) else roi[b, T + i] for i in range(T)])) for b in range(n))
+    per = n * size
+    if compute == 0:
+        centre = {np.float32: 0.0, np.uint8: 128.0, np.int8: 64.0}[dtype]
+        mean = (r.uniform(-0.5, 0.5, per) + centre).astype(np.float32)
+        std = r.uniform(20.0, 40.0, per).astype(np.float32)
+    else:
+        mean = np.zeros(per, np.float32)
+        std = np.zeros(per, np.float32) if compute & 2 else np.full(per, 0.25, np.float32)
+        if compute == 2:
+            mean[:] = 60.0 if dtype != np.float32 else 0.5
+    return src, roi.ravel(), mean, std
+
+
+def run_normalize_nd(impls, src, dst_shape, dst_dtype, axis_mask, mean, std, compute, scale, shift, roi, sl, dl):
+    outs = []
+    for impl in impls:
+        m, s_ = mean.copy(), std.copy()
+        dst = np.full(dst_shape, 7, dst_dtype)
+        impl.normalize_nd(src, dst, axis_mask, m, s_, compute, scale, shift, roi, sl, dl)
+        outs.append((dst, m, s_))
+    return outs
+
+
+NORM3D = [(1, 1, m) for m in range(1, 8)] + [(1, 0, 3), (0, 0, 3)]
+
+
+@pytest.mark.parametrize("case", range(len(NORM3D)))
+@pytest.mark.parametrize("compute", [0, 1, 2, 3])
+def test_normalize_f32_3d(oracle, reference, case, compute):
+    """The F32 3-D branch: NHWC -> NHWC for every axis mask, NHWC -> NCHW (mask 3) and NCHW ->
+    NCHW (statistics only: the reference writes zeros), bit for bit with the in-out arrays."""
+    sl, dl, mask = NORM3D[case]
+    r = rng(200 + case * 4 + compute)
+    shp = (3, 19, 23, 3) if sl == 1 else (3, 3, 19, 23)
+    src, roi, mean, std = normalize_nd_case(r, shp, mask, compute, np.float32, begin_fits=mask in (1, 2, 4, 5))
+    dshape = shp if dl == sl else (3, 3, 19, 23)
+    a, b = run_normalize_nd((oracle, reference), src, dshape, np.float32, mask, mean, std, compute, 1.5, 0.25, roi,
+                            sl, dl)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_normalize_f32_3d_16_channels(oracle, reference):
+    """NHWC with 16 channels and mask 3 (the reference's vectorized row path)."""
+    r = rng(240)
+    src, roi, mean, std = normalize_nd_case(r, (2, 9, 11, 16), 3, 3, np.float32)
+    a, b = run_normalize_nd((oracle, reference), src, (2, 9, 11, 16), np.float32, 3, mean, std, 3, 2.0, -1.0, roi,
+                            1, 1)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+NORMND = [((4, 700), 1), ((3, 5, 6, 7, 40), 1), ((3, 5, 6, 7, 40), 8), ((3, 5, 6, 7, 40), 6),
+          ((3, 5, 6, 7, 40), 9), ((3, 5, 6, 7, 40), 15), ((3, 5, 6, 7, 40), 11), ((3, 5, 6, 7, 40), 13)]
+
+
+@pytest.mark.parametrize("case", range(len(NORMND)))
+@pytest.mark.parametrize("compute", [0, 1, 2, 3])
+def test_normalize_f32_nd(oracle, reference, case, compute):
+    """F32 at ranks 1, 4 and 5 (the N-D branch: collapsed axes, dense addressing from the roi begin)."""
+    shp, mask = NORMND[case]
+    r = rng(260 + case * 4 + compute)
+    src, roi, mean, std = normalize_nd_case(r, shp, mask, compute, np.float32, begin_fits=case == 2)
+    a, b = run_normalize_nd((oracle, reference), src, shp, np.float32, mask, mean, std, compute, 1.5, 0.25, roi, 0, 0)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+NORMINT = [((4, 37, 61), 1), ((4, 37, 61), 2), ((4, 37, 61), 3), ((3, 9, 11, 3), 4), ((3, 9, 11, 3), 3),
+           ((3, 9, 11, 3), 5), ((2, 4, 5, 6, 3), 8), ((2, 4, 5, 6, 3), 7)]
+
+
+@pytest.mark.parametrize("case", range(len(NORMINT)))
+@pytest.mark.parametrize("compute", [0, 3])
+@pytest.mark.parametrize("dtype", [np.uint8, np.int8])
+def test_normalize_integer(oracle, reference, case, compute, dtype):
+    """U8 and I8 (non-negative values, results in range) through the generic N-D path at ranks 2-4,
+    including the statistics accumulated onto the caller's arrays."""
+    shp, mask = NORMINT[case]
+    r = rng(300 + case * 4 + compute + (100 if dtype == np.int8 else 0))
+    src, roi, mean, std = normalize_nd_case(r, shp, mask, compute, dtype)
+    scale, shift = (15.0, 64.0) if dtype == np.int8 else (20.0, 128.0)
+    if compute == 0:
+        scale = 15.0   # scale / std dev <= 0.75: results stay in range
+    a, b = run_normalize_nd((oracle, reference), src, shp, dtype, mask, mean, std, compute, scale, shift, roi, 0, 0)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x.view(np.uint8) if x.dtype == np.int8 else x,
+                                      y.view(np.uint8) if y.dtype == np.int8 else y)
+    assert (a[0][0] != 7).any()
+
+
+def test_normalize_nd_accumulates_onto_caller_statistics(oracle, reference):
+    """The N-D branch adds its sums to the values already in the caller's mean / std-dev arrays
+    (normalize.cpp:200-242 never clears them); the restatement does the same."""
+    r = rng(330)
+    src, roi, _, _ = normalize_nd_case(r, (3, 5, 6, 7, 40), 8, 3, np.float32)
+    size = 3 * 5 * 6 * 7
+    mean = r.uniform(-1, 1, size).astype(np.float32)
+    std = r.uniform(0, 1, size).astype(np.float32)
+    a, b = run_normalize_nd((oracle, reference), src, src.shape, np.float32, 8, mean, std, 3, 1.0, 0.0, roi, 0, 0)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
