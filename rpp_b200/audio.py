@@ -150,7 +150,7 @@ def slice(src, src_desc, dst, dst_desc, anchor, shape, fill_value, enable_paddin
 
 
 def normalize(src, src_desc, dst, dst_desc, axis_mask, mean, std_dev, compute_mean_stddev, scale, shift, roi, handle):
-    """rppt_normalize_gpu (api/rppt_tensor_statistical_operations.h:193), 2-D F32."""
+    """rppt_normalize_gpu (api/rppt_tensor_statistical_operations.h:193): U8 / F16 / F32 / I8, ranks 1-4."""
     L = _lib.load()
     return _status(L.rppt_normalize_gpu(_addr(src), ctypes.byref(src_desc), _addr(dst), ctypes.byref(dst_desc),
                                         int(axis_mask), _addr(mean), _addr(std_dev), int(compute_mean_stddev),

@@ -982,6 +982,344 @@ extern "C" SHARED_PUBLIC RppStatus rppt_slice_gpu(RppPtr_t srcPtr, RpptGenericDe
     });
 }
 
+namespace {
+
+// The caller's roi tensor on the host (parameter counts and plans are built there).  Memory the
+// device can write (device, managed, pinned) may still be written by earlier work on the handle
+// stream, so the stream is synchronized before the host reads it; pageable memory is read as it is.
+std::vector<uint32_t> roi_to_host(Handle& h, const Rpp32u* roiTensor, size_t count)
+{
+    std::vector<uint32_t> roi(count);
+    cudaPointerAttributes attr{};
+    const bool known = cudaPointerGetAttributes(&attr, roiTensor) == cudaSuccess;
+    if (!known) cudaGetLastError();
+    const cudaMemoryType mt = known ? attr.type : cudaMemoryTypeUnregistered;
+    if (mt == cudaMemoryTypeDevice)
+    {
+        check_cuda(cudaMemcpyAsync(roi.data(), roiTensor, count * 4, cudaMemcpyDeviceToHost, h.stream()),
+                   "cudaMemcpyAsync(roi)");
+        check_cuda(cudaStreamSynchronize(h.stream()), "cudaStreamSynchronize(roi)");
+    }
+    else
+    {
+        if (mt == cudaMemoryTypeHost || mt == cudaMemoryTypeManaged)
+            check_cuda(cudaStreamSynchronize(h.stream()), "cudaStreamSynchronize(roi)");
+        std::memcpy(roi.data(), roiTensor, count * 4);
+    }
+    return roi;
+}
+
+int norm_type(RpptDataType t)
+{
+    return t == F32 ? kNormF32 : t == F16 ? kNormF16 : t == U8 ? kNormU8 : t == I8 ? kNormI8 : -1;
+}
+
+// Largest element offset a set of (count, stride) levels reaches; false if some count is 0.
+bool reach(const uint32_t* count, const uint32_t* stride, int levels, size_t& out)
+{
+    out = 0;
+    for (int l = 0; l < levels; ++l)
+    {
+        if (count[l] == 0) return false;
+        out += size_t(count[l] - 1) * stride[l];
+    }
+    return true;
+}
+
+// Plan of one sample for the F32 3-D branch (normalize.cpp:592-730).
+bool plan_3d(const RpptGenericDesc& sd, const RpptGenericDesc& dd, unsigned axisMask, const uint32_t* begin,
+             const uint32_t* length, NormNdSample& s, uint32_t& params)
+{
+    const uint32_t L0 = length[0], L1 = length[1], L2 = length[2];
+    const uint32_t S1 = sd.strides[1], S2 = sd.strides[2], S3 = sd.strides[3];
+    uint32_t rd[3], rs[3];
+    bool ps[3] = {false, false, false};
+    bool consecutive = true;
+    switch (axisMask)
+    {
+    case 1: rd[0] = L1; rd[1] = L2; rd[2] = L0; rs[0] = S1; rs[1] = S3; rs[2] = S2; ps[1] = ps[2] = true; break;
+    case 2: rd[0] = L0; rd[1] = L2; rd[2] = L1; rs[0] = S2; rs[1] = S3; rs[2] = S1; ps[0] = ps[2] = true; break;
+    case 3: rd[0] = 1; rd[1] = L2; rd[2] = L0 * L1; rs[0] = S2; rs[1] = S3; rs[2] = S3; ps[2] = true; break;
+    case 4: rd[0] = L0; rd[1] = L1; rd[2] = L2; rs[0] = S3; rs[1] = S2; rs[2] = S1; ps[0] = ps[1] = true; break;
+    case 5: rd[0] = L1; rd[1] = L0; rd[2] = L2; rs[0] = S3; rs[1] = S1; rs[2] = S2; ps[1] = true; consecutive = false;
+        break;
+    case 6: rd[0] = 1; rd[1] = L0; rd[2] = L1 * L2; rs[0] = S3; rs[1] = S1; rs[2] = S3; ps[0] = true; break;
+    default: rd[0] = 1; rd[1] = 1; rd[2] = L0 * L1 * L2; rs[0] = rs[1] = rs[2] = S3; break;
+    }
+    s.srcBase = size_t(begin[0]) * S1 + size_t(begin[1]) * S2;
+    s.accumulate = 0;
+    s.lineStride = rs[0];
+    s.lineCount = rd[2];
+    if (consecutive)
+    {
+        s.pLevels = 2;
+        s.pCount[0] = rd[0];
+        s.pStride[0] = rs[2];
+        s.pCount[1] = rd[1];
+        s.pStride[1] = rs[1];
+        s.oLevels = 0;
+        s.normFactor = float(1.0 / double(rd[2]));
+        params = rd[0] * rd[1];
+    }
+    else
+    {
+        s.pLevels = 1;
+        s.pCount[0] = rd[0];
+        s.pStride[0] = rs[2];
+        s.oLevels = 1;
+        s.oCount[0] = rd[1];
+        s.oStride[0] = rs[1];
+        s.normFactor = float(1.0 / double(rd[1] * rd[2]));
+        params = rd[0];
+    }
+    // output (normalize.cpp:717-723): NHWC -> NHWC (the 16-channel mask-3 case over whole rows of 16
+    // channels), NHWC -> NCHW for mask 3, otherwise nothing
+    s.levels = 0;
+    s.zeroFrom = 0;
+    if (axisMask == 3 && sd.layout == NHWC && dd.layout == NHWC && sd.dims[3] == 16)
+    {
+        if (L2 != 16) return false;   // the 16 channel parameters must all exist
+        s.lv[0] = {L0, S1, dd.strides[1], 0};
+        s.lv[1] = {L1, 16, 16, 0};
+        s.lv[2] = {16, 1, 1, 1};
+        s.levels = 3;
+    }
+    else if (sd.layout == NHWC && dd.layout == NHWC)
+    {
+        const uint32_t m2 = ps[2] ? 1 : 0, m1 = ps[1] ? (ps[2] ? L2 : 1) : 0;
+        const uint32_t m0 = ps[0] ? (ps[1] ? L1 : 1) * (ps[2] ? L2 : 1) : 0;
+        s.lv[0] = {L0, S1, dd.strides[1], m0};
+        s.lv[1] = {L1, S2, dd.strides[2], m1};
+        s.lv[2] = {L2, 1, 1, m2};
+        s.levels = 3;
+    }
+    else if (axisMask == 3 && sd.layout == NHWC && dd.layout == NCHW)
+    {
+        s.lv[0] = {L0, S1, dd.strides[2], 0};
+        s.lv[1] = {L1, S2, dd.strides[3], 0};
+        s.lv[2] = {L2, 1, dd.strides[1], 1};
+        s.levels = 3;
+    }
+    return true;
+}
+
+// Plan of one sample for the N-D branch (normalize.cpp:731-868): collapse_axis, dense addressing.
+bool plan_nd(const RpptGenericDesc& sd, int T, unsigned axisMask, const uint32_t* begin, const uint32_t* length,
+             NormNdSample& s, uint32_t& params)
+{
+    uint32_t axis[4], newAxis[4] = {0, 0, 0, 0}, newDims[4] = {0, 0, 0, 0}, size = 1, total = 1;
+    s.srcBase = 0;
+    for (int i = 0; i < T; ++i)
+    {
+        axis[i] = (axisMask >> i) & 1u;
+        size *= axis[i] ? 1 : length[i];
+        total *= axis[i] ? length[i] : 1;
+        s.srcBase += size_t(begin[i]) * sd.strides[i + 1];
+    }
+    // collapse_axis as the reference runs it: a normalized axis merges into the previous one only
+    // while no axis has been merged before it
+    int skipped = 0, prev = -2, k = 0;
+    for (int i = 0; i < T; ++i)
+    {
+        if (axis[i])
+        {
+            if (i - skipped != prev + 1)
+            {
+                newAxis[k] = 1;
+                newDims[k] = length[i];
+                prev = i;
+                ++k;
+            }
+            else if (prev >= 0)
+            {
+                newDims[prev] *= length[i];
+                ++skipped;
+            }
+        }
+        else
+            newDims[k++] = length[i];
+    }
+    const int nT = T - skipped;
+    int lastNorm = 0;
+    for (int i = 0; i < nT; ++i)
+        if (newAxis[i]) lastNorm = i;
+    uint32_t st[4];
+    uint32_t v = 1;
+    for (int i = nT - 1; i >= 0; --i)
+    {
+        st[i] = v;
+        v *= newDims[i];
+    }
+    s.accumulate = 1;
+    s.normFactor = float(1.0 / double(total));
+    s.pLevels = s.oLevels = 0;
+    for (int l = 0; l < nT; ++l)
+    {
+        if (!newAxis[l])
+        {
+            s.pCount[s.pLevels] = newDims[l];
+            s.pStride[s.pLevels++] = st[l];
+        }
+        else if (l != lastNorm)
+        {
+            s.oCount[s.oLevels] = newDims[l];
+            s.oStride[s.oLevels++] = st[l];
+        }
+    }
+    s.lineStride = st[lastNorm];
+    s.lineCount = newDims[lastNorm];
+    params = size;
+    s.levels = nT;
+    s.elems = 1;
+    for (int l = 0; l < nT; ++l)
+    {
+        uint32_t pm = 0;
+        if (!newAxis[l])
+        {
+            pm = 1;
+            for (int m = l + 1; m < nT; ++m)
+                if (!newAxis[m]) pm *= newDims[m];
+        }
+        s.lv[l] = {newDims[l], st[l], st[l], pm};
+        s.elems *= newDims[l];
+    }
+    return true;
+}
+
+// normalize for every type and rank but the 2-D F32 one.
+RppStatus normalize_nd(Handle& h, const void* srcPtr, const RpptGenericDesc& sd, void* dstPtr,
+                       const RpptGenericDesc& dd, Rpp32u axisMask, Rpp32f* meanTensor, Rpp32f* stdDevTensor,
+                       int compute, Rpp32f scale, Rpp32f shift, const Rpp32u* roiTensor)
+{
+    const int ts = norm_type(RpptDataType(sd.dataType)), td = norm_type(RpptDataType(dd.dataType));
+    if (ts < 0 || ts != td) return RPP_ERROR_NOT_IMPLEMENTED;   // U8, F16, F32, I8, source type = destination type
+    if (sd.numDims < 2 || sd.numDims > 5 || dd.numDims != sd.numDims) return RPP_ERROR_NOT_IMPLEMENTED;
+    const int T = int(sd.numDims) - 1;
+    if (axisMask == 0 || axisMask >= (1u << T)) return RPP_ERROR_INVALID_ARGUMENTS;
+    require(srcPtr && dstPtr && roiTensor && meanTensor && stdDevTensor, "null tensor");
+    const int n = int(dd.dims[0]);
+    if (n <= 0) return RPP_SUCCESS;
+    require(sd.dims[0] >= dd.dims[0], "source batch smaller than destination batch");
+    const std::vector<uint32_t> roi = roi_to_host(h, roiTensor, size_t(n) * T * 2);
+    int maxSize = 1;
+    for (int b = 0; b < n; ++b)
+    {
+        size_t size = 1;
+        for (int i = 0; i < T; ++i) size *= ((axisMask >> i) & 1u) ? 1 : roi[size_t(b) * 2 * T + T + i];
+        if (size > size_t(INT32_MAX)) return RPP_ERROR_INVALID_ARGUMENTS;
+        maxSize = std::max(maxSize, int(size));
+    }
+    const bool is3d = ts == kNormF32 && T == 3;
+    std::vector<NormNdSample> samples(n);
+    std::vector<int4> tasks;
+    size_t maxElems = 0, maxZero = 0;
+    for (int b = 0; b < n; ++b)
+    {
+        const uint32_t* begin = &roi[size_t(b) * 2 * T];
+        const uint32_t* length = begin + T;
+        NormNdSample& s = samples[b];
+        std::memset(&s, 0, sizeof s);
+        uint32_t params = 0;
+        if (!(is3d ? plan_3d(sd, dd, axisMask, begin, length, s, params)
+                   : plan_nd(sd, T, axisMask, begin, length, s, params)))
+            return RPP_ERROR_INVALID_ARGUMENTS;
+        // every read inside the source sample, every write inside the destination sample
+        uint32_t lc[4], lst[4], ld_[4];
+        for (int l = 0; l < s.levels; ++l)
+        {
+            lc[l] = s.lv[l].count;
+            lst[l] = s.lv[l].srcStride;
+            ld_[l] = s.lv[l].dstStride;
+        }
+        size_t r1 = 0, r2 = 0, r3 = 0, w = 0;
+        if (compute && params > 0 && s.lineCount > 0 && reach(s.pCount, s.pStride, s.pLevels, r1) &&
+            reach(s.oCount, s.oStride, s.oLevels, r2))
+        {
+            r3 = size_t(s.lineCount - 1) * s.lineStride;
+            if (s.srcBase + r1 + r2 + r3 >= sd.strides[0]) return RPP_ERROR_INVALID_ARGUMENTS;
+        }
+        if (s.levels > 0 && reach(lc, lst, s.levels, r1) && reach(lc, ld_, s.levels, w))
+        {
+            if (s.srcBase + r1 >= sd.strides[0] || w >= dd.strides[0]) return RPP_ERROR_INVALID_ARGUMENTS;
+        }
+        else
+            s.elems = 0;
+        if (!is3d) s.zeroFrom = std::min<size_t>(s.elems, dd.strides[0]);
+        else s.elems = s.levels > 0 ? size_t(s.lv[0].count) * s.lv[1].count * s.lv[2].count : 0;
+        if (s.levels == 0) s.elems = 0;
+        maxElems = std::max(maxElems, s.elems);
+        maxZero = std::max<size_t>(maxZero, dd.strides[0] - s.zeroFrom);
+        if (compute && params > 0)
+        {
+            if (s.lineCount >= uint32_t(kNormalizeWarpMinElems))
+                for (uint32_t p = 0; p < params; ++p) tasks.push_back(make_int4(b, int(p), 1, 1));
+            else
+                for (uint32_t p = 0; p < params; p += 32)
+                    tasks.push_back(make_int4(b, int(p), int(std::min<uint32_t>(32, params - p)), 0));
+        }
+    }
+    const size_t perAll = size_t(n) * maxSize;
+    const size_t meanInCount = compute == 0 ? size_t(maxSize) : perAll;
+    Carver m(nullptr);
+    m.take<NormNdSample>(n);
+    m.take<int4>(tasks.size());
+    m.take<float>(perAll);
+    m.take<float>(perAll);
+    m.take<float>(maxSize);
+    m.take<float>(meanInCount);
+    m.take<float>(meanInCount);
+    Carver cv(h.workspace(m.used()));
+    NormNdSample* dSamples = cv.take<NormNdSample>(n);
+    int4* dTasks = cv.take<int4>(tasks.size());
+    float* meanOut = cv.take<float>(perAll);
+    float* invOut = cv.take<float>(perAll);
+    float* inverted = cv.take<float>(maxSize);
+    float* meanStage = cv.take<float>(meanInCount);
+    float* stdStage = cv.take<float>(meanInCount);
+    h.upload(dSamples, samples.data(), samples.size() * sizeof(NormNdSample));
+    if (!tasks.empty()) h.upload(dTasks, tasks.data(), tasks.size() * sizeof(int4));
+    NormNdArgs a;
+    a.src = static_cast<const char*>(srcPtr) + sd.offsetInBytes;
+    a.dst = static_cast<char*>(dstPtr) + dd.offsetInBytes;
+    a.type = ts;
+    a.srcElem = a.dstElem = ts == kNormF32 ? 4 : ts == kNormF16 ? 2 : 1;
+    a.n = n;
+    a.srcStride0 = sd.strides[0];
+    a.dstStride0 = dd.strides[0];
+    a.compute = compute;
+    a.scale = scale;
+    a.shift = shift;
+    a.maxSize = maxSize;
+    a.samples = dSamples;
+    a.meanIn = (compute & 1) ? nullptr
+                             : static_cast<const float*>(h.device_view(meanTensor, meanInCount * 4, meanStage));
+    a.meanOut = meanOut;
+    a.invOut = invOut;
+    const float* stdIn =
+        (compute & 2) ? nullptr : static_cast<const float*>(h.device_view(stdDevTensor, meanInCount * 4, stdStage));
+    const float* meanEff = (compute & 1) ? meanOut : a.meanIn;
+    const float* invEff = (compute & 2) ? invOut : compute == 0 ? inverted : stdIn;
+    // the caller's values: where the N-D branch starts its sums, and what entries past a sample's
+    // parameter count keep
+    if (compute & 1)
+        check_cuda(cudaMemcpyAsync(meanOut, meanTensor, perAll * 4, cudaMemcpyDefault, h.stream()),
+                   "cudaMemcpyAsync(mean in)");
+    if (compute & 2)
+        check_cuda(cudaMemcpyAsync(invOut, stdDevTensor, perAll * 4, cudaMemcpyDefault, h.stream()),
+                   "cudaMemcpyAsync(stdDev in)");
+    launch_normalize_nd(h, a, dTasks, int(tasks.size()), meanEff, invEff, compute == 0 ? 0 : maxSize, maxElems,
+                        maxZero, stdIn, inverted, compute == 0 ? maxSize : 0);
+    if (compute & 1)
+        check_cuda(cudaMemcpyAsync(meanTensor, meanOut, perAll * 4, cudaMemcpyDefault, h.stream()),
+                   "cudaMemcpyAsync(mean)");
+    if (compute & 2)
+        check_cuda(cudaMemcpyAsync(stdDevTensor, invOut, perAll * 4, cudaMemcpyDefault, h.stream()),
+                   "cudaMemcpyAsync(stdDev)");
+    return RPP_SUCCESS;
+}
+
+}  // namespace
+
 extern "C" SHARED_PUBLIC RppStatus rppt_normalize_gpu(RppPtr_t srcPtr, RpptGenericDescPtr srcGenericDescPtr,
                                                       RppPtr_t dstPtr, RpptGenericDescPtr dstGenericDescPtr,
                                                       Rpp32u axisMask, Rpp32f* meanTensor, Rpp32f* stdDevTensor,
@@ -992,34 +1330,18 @@ extern "C" SHARED_PUBLIC RppStatus rppt_normalize_gpu(RppPtr_t srcPtr, RpptGener
         require(srcGenericDescPtr && dstGenericDescPtr, "null descriptor");
         const RpptGenericDesc& sd = *srcGenericDescPtr;
         const RpptGenericDesc& dd = *dstGenericDescPtr;
-        // built: the audio path's 2-D F32 tensors (normalize.cpp's tensorDims == 2 branch)
-        if (sd.dataType != F32 || dd.dataType != F32) return RPP_ERROR_NOT_IMPLEMENTED;
-        if (sd.numDims != 3 || dd.numDims != 3) return RPP_ERROR_NOT_IMPLEMENTED;
+        // the 2-D F32 tensors of the audio path (normalize.cpp's tensorDims == 2 branch) here; every
+        // other type and rank in normalize_nd
+        if (!(sd.dataType == F32 && dd.dataType == F32 && sd.numDims == 3 && dd.numDims == 3))
+            return normalize_nd(h, srcPtr, sd, dstPtr, dd, axisMask, meanTensor, stdDevTensor, computeMeanStddev & 3,
+                                scale, shift, roiTensor);
         if (axisMask < 1 || axisMask > 3) return RPP_ERROR_INVALID_ARGUMENTS;
         require(srcPtr && dstPtr && roiTensor && meanTensor && stdDevTensor, "null tensor");
         const int n = int(dd.dims[0]);
         if (n <= 0) return RPP_SUCCESS;
         const int compute = computeMeanStddev & 3;
-        // roi lengths are needed on the host (parameter counts, work list).  Memory the device can write
-        // (device, managed, pinned) may still be written by earlier work on the handle stream, so the
-        // stream is synchronized before the host reads it; pageable memory is read as it is.
-        std::vector<uint32_t> roi(size_t(n) * 4);
-        cudaPointerAttributes attr{};
-        const bool known = cudaPointerGetAttributes(&attr, roiTensor) == cudaSuccess;
-        if (!known) cudaGetLastError();
-        const cudaMemoryType mt = known ? attr.type : cudaMemoryTypeUnregistered;
-        if (mt == cudaMemoryTypeDevice)
-        {
-            check_cuda(cudaMemcpyAsync(roi.data(), roiTensor, roi.size() * 4, cudaMemcpyDeviceToHost, h.stream()),
-                       "cudaMemcpyAsync(roi)");
-            check_cuda(cudaStreamSynchronize(h.stream()), "cudaStreamSynchronize(roi)");
-        }
-        else
-        {
-            if (mt == cudaMemoryTypeHost || mt == cudaMemoryTypeManaged)
-                check_cuda(cudaStreamSynchronize(h.stream()), "cudaStreamSynchronize(roi)");
-            std::memcpy(roi.data(), roiTensor, roi.size() * 4);
-        }
+        // roi lengths are needed on the host (parameter counts, work list)
+        const std::vector<uint32_t> roi = roi_to_host(h, roiTensor, size_t(n) * 4);
         int maxSize = 1;
         std::vector<NormalizeSample> samples(n);
         std::vector<int4> tasks;

@@ -208,6 +208,47 @@ void launch_normalize(Handle& h, const NormalizeArgs& a, const int4* tasks, int 
                       const float* invEff, int paramOffsetPerSample, const float* stdToInvert, float* invertOut,
                       int invertCount);
 
+// normalize, every other type and rank (normalize_nd.cu): per-sample plans built by the dispatch.
+constexpr int kNormF32 = 0, kNormF16 = 1, kNormU8 = 2, kNormI8 = 3;
+struct NormNdLevel
+{
+    uint32_t count, srcStride, dstStride, paramMult;
+};
+struct NormNdSample
+{
+    // statistics: parameter p = row-major over pLevels (count, source stride); its lines row-major
+    // over oLevels; each line lineCount elements lineStride apart
+    int pLevels, oLevels;
+    uint32_t pCount[4], pStride[4], oCount[4], oStride[4];
+    uint32_t lineStride, lineCount;
+    float normFactor;
+    int accumulate;          // sums start from the caller's mean / std-dev value (the N-D branch)
+    // output: elems elements row-major over `levels`
+    int levels;
+    NormNdLevel lv[4];
+    size_t elems;
+    size_t srcBase;          // source element offset of the roi start within the sample
+    size_t zeroFrom;         // destination elements [zeroFrom, dstStride0) are cleared
+};
+struct NormNdArgs
+{
+    const void* src;
+    void* dst;
+    int type, srcElem, dstElem;   // kNorm*, element sizes in bytes
+    int n;
+    size_t srcStride0, dstStride0;
+    int compute;
+    float scale, shift;
+    int maxSize;
+    const NormNdSample* samples;  // device, n
+    const float* meanIn;
+    float* meanOut;
+    float* invOut;
+};
+void launch_normalize_nd(Handle& h, const NormNdArgs& a, const int4* tasks, int numTasks, const float* meanEff,
+                         const float* invEff, int paramOffsetPerSample, size_t maxElems, size_t maxZero,
+                         const float* stdToInvert, float* invertOut, int invertCount);
+
 // 16-bit PCM ingest (pcm.cu).
 void launch_pcm16(Handle& h, const short* src, uint32_t srcStride, float* dst, uint32_t dstStride, const int* len,
                   int channels, int n);
