@@ -49,7 +49,8 @@ def parse():
     p.add_argument("--precision", type=int, default=1, help="run the precision study on 1024 x 10 s clips (0: skip)")
     p.add_argument("--profile", action="store_true", help="run each entry point once for ncu captures, then exit")
     p.add_argument("--profile-repeat", type=int, default=1)
-    p.add_argument("--profile-only", default="", help="with --profile: only entry points whose name contains this")
+    p.add_argument("--profile-only", default="",
+                   help="with --profile: only entry points whose name contains this (=NAME: exactly this name)")
     p.add_argument("--serve-requests", type=int, default=5000,
                    help="requests per offered-load point of the serving measurement (0 skips it)")
     return p.parse_args()
@@ -1141,7 +1142,8 @@ def profile_ops(args):
             ctypes.c_void_p(stream))),
     ]
     for name, fn in ops:
-        if args.profile_only and args.profile_only not in name:
+        sel = args.profile_only
+        if sel and (name != sel[1:] if sel.startswith("=") else sel not in name):
             continue
         for _ in range(args.profile_repeat):
             st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
