@@ -62,6 +62,13 @@ inline bool resample_magic_ok(const ResampleWindowDev& w, bool pairs)
     return pairs && lo >= 0.0 && hi < 4194304.0;
 }
 
+// A power-of-two table scale (x * scale exact for every finite tap position).
+inline bool resample_scale_pow2(const ResampleWindowDev& w)
+{
+    int e = 0;
+    return w.scale > 0.f && std::isfinite(w.scale) && std::frexp(double(w.scale), &e) == 0.5;
+}
+
 inline void resample_pads(ResampleWindowDev& w)
 {
     const double reach = (double(w.lobes) + 1.0) * std::fabs(double(w.scale));
@@ -108,13 +115,18 @@ struct ResampleCount
 // floor(locRaw) in the low mantissa bits and float(floor(locRaw)) one subtraction away, instead of two
 // float <-> int conversions per tap (low-throughput instructions).  Used when the host has shown that
 // every locRaw a tap can produce lies in [0, 2^22): then trunc == floor, and both are exact this way.
-template <bool kPairs, bool kMagic = false>
+// The pair entry is then addressed as bias + 8 * bits(m): the shared address of entry 0 less 8 * bits of
+// 1.5 * 2^23 (mod 2^32), one shift-add per tap.
+// kFma: the table scale is a power of two, so x * scale is exact and x * scale + center rounds once
+// either way: one fused multiply-add gives the reference's value.
+template <bool kPairs, bool kMagic = false, bool kFma = false>
 struct Win
 {
     const float* lut;     // shared memory: the table (plain layout)
     const float2* pairs;  // shared memory: (value, next - value) at index 0 of the padded pair layout
     int lutSize;
     float scale, center;
+    uint32_t bias;        // kMagic with kPairs: shared address of pairs[0] - 8 * bits(1.5 * 2^23)
 
     __device__ __forceinline__ float interp(int idx, float weight) const
     {
@@ -136,12 +148,20 @@ struct Win
     {
         constexpr float kM = 12582912.0f;   // 1.5 * 2^23
         const float m = __fadd_rd(locRaw, kM);
-        return interp(__float_as_int(m) - __float_as_int(kM), __fsub_rn(locRaw, __fsub_rn(m, kM)));
+        const float w = __fsub_rn(locRaw, __fsub_rn(m, kM));
+        if constexpr (kPairs)
+        {
+            const uint32_t a = bias + (uint32_t(__float_as_int(m)) << 3);
+            float ex, ey;
+            asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(ex), "=f"(ey) : "r"(a));
+            return __fadd_rn(ex, __fmul_rn(w, ey));
+        }
+        return interp(__float_as_int(m) - __float_as_int(kM), w);
     }
     // rppdefs.h:771-782: truncating index (the SSE lanes)
     __device__ __forceinline__ float lane(float x) const
     {
-        const float locRaw = __fadd_rn(__fmul_rn(x, scale), center);
+        const float locRaw = kFma ? __fmaf_rn(x, scale, center) : __fadd_rn(__fmul_rn(x, scale), center);
         if constexpr (kMagic) return magic_floor(locRaw);
         const int idx = int(locRaw);
         return interp(idx, __fsub_rn(locRaw, float(idx)));
@@ -149,7 +169,7 @@ struct Win
     // rppdefs.h:760-769: floor, clamped index (the scalar tail and the multi-channel path)
     __device__ __forceinline__ float scalar(float x) const
     {
-        const float locRaw = __fadd_rn(__fmul_rn(x, scale), center);
+        const float locRaw = kFma ? __fmaf_rn(x, scale, center) : __fadd_rn(__fmul_rn(x, scale), center);
         if constexpr (kMagic) return magic_floor(locRaw);
         const int idx = int(floorf(locRaw));
         return interp(idx, __fsub_rn(locRaw, float(idx)));
@@ -168,7 +188,7 @@ struct UnitInfo
 
 // kMix: the input is interleaved multi-channel and is down-mixed to mono on the fly (MonoMix), so
 // the launch equals rppt_down_mixing_gpu followed by a mono rppt_resample_gpu.
-template <bool kMix, bool kTable, bool kPairs, bool kMagic = false>
+template <bool kMix, bool kTable, bool kPairs, bool kMagic = false, bool kFma = false>
 __global__ void __launch_bounds__(kThreads) resample_kernel(const float* __restrict__ src, uint32_t srcStride,
                                                             float* __restrict__ dst, uint32_t dstStride,
                                                             const float* __restrict__ inRateT,
@@ -190,8 +210,11 @@ __global__ void __launch_bounds__(kThreads) resample_kernel(const float* __restr
         }
     else
         for (int i = threadIdx.x; i < wd.lutSize; i += kThreads) s_lut[i] = wd.lut[i];
-    const Win<kPairs, kMagic> win{s_lut, reinterpret_cast<const float2*>(s_lut) + (kPairs ? wd.padLeft : 0),
-                                  wd.lutSize, wd.scale, wd.center};
+    const Win<kPairs, kMagic, kFma> win{s_lut, reinterpret_cast<const float2*>(s_lut) + (kPairs ? wd.padLeft : 0),
+                                        wd.lutSize, wd.scale, wd.center,
+                                        uint32_t(__cvta_generic_to_shared(reinterpret_cast<const float2*>(s_lut) +
+                                                                          (kPairs ? wd.padLeft : 0))) -
+                                            0x5A000000u};   // 8 * 0x4B400000 mod 2^32
     const int lobes = wd.lobes;
     __shared__ long long s_prefix[kPrefixCache];
     prefix = cache_prefix(prefix, n, s_prefix);   // ends with __syncthreads
@@ -375,9 +398,12 @@ void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStr
                                                      normalize, prefix, n, nullptr, 0.f);
     };
     const bool magic = resample_magic_ok(w, pairs);
-    if (downmix && magic) go(resample_kernel<true, false, true, true>);
+    const bool fma = resample_scale_pow2(w);
+    if (downmix && magic && fma) go(resample_kernel<true, false, true, true, true>);
+    else if (downmix && magic) go(resample_kernel<true, false, true, true>);
     else if (downmix && pairs) go(resample_kernel<true, false, true>);
     else if (downmix) go(resample_kernel<true, false, false>);
+    else if (magic && fma) go(resample_kernel<false, false, true, true, true>);
     else if (magic) go(resample_kernel<false, false, true, true>);
     else if (pairs) go(resample_kernel<false, false, true>);
     else go(resample_kernel<false, false, false>);
@@ -400,7 +426,8 @@ void launch_resample_clips(Handle& h, void* scratch, const RppbClip* clips, int 
         kernel<<<grid, kThreads, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, w, false,
                                                      prefix, n, clips, outRate);
     };
-    if (resample_magic_ok(w, pairs)) go(resample_kernel<false, true, true, true>);
+    if (resample_magic_ok(w, pairs) && resample_scale_pow2(w)) go(resample_kernel<false, true, true, true, true>);
+    else if (resample_magic_ok(w, pairs)) go(resample_kernel<false, true, true, true>);
     else if (pairs) go(resample_kernel<false, true, true>);
     else go(resample_kernel<false, true, false>);
     count_launch();
