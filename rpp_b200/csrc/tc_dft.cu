@@ -582,30 +582,99 @@ struct PrepArgs
     int n;
 };
 
-// BF16 (hi, and lo for the split format) or TF32 copy of the padded signal, [n][clipStride].
+// BF16 (hi, and lo for the split format) or TF32 copy of the padded signal, [n][clipStride].  Each
+// thread takes 8 consecutive positions: where they and the sample before them lie inside the clip
+// (the interior: no padding, no border sample), two 4-sample loads and one scalar give the
+// pre-emphasized values and the results leave as 16-byte stores (clipStride keeps rows 16-byte
+// aligned); at the clip's ends position by position.  Same values either way.
 template <int FMT>
 __global__ void tc_prep_kernel(PrepArgs p, void* __restrict__ outHi, void* __restrict__ outLo, uint32_t clipStride)
 {
+    const uint32_t groups = (clipStride + 7) / 8;
     for (int b = blockIdx.y; b < p.n; b += gridDim.y)
     {
         const PaddedSignal sig =
             padded_signal(p.src, p.srcStride, p.srcElems, p.len, p.coeff, p.border, p.reflect, p.centerOffset, b);
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < clipStride; i += gridDim.x * blockDim.x)
+        for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += gridDim.x * blockDim.x)
         {
-            const float v = sig(i);
-            const size_t o = size_t(b) * clipStride + i;
+            const uint32_t i0 = g * 8;
+            const long long t0 = (long long)i0 - sig.centerOffset;
+            const bool whole = i0 + 8 <= clipStride;
+            float v[8];
+            if (whole && t0 >= 1 && t0 + 8 <= sig.L)
+            {
+                const float* x = sig.x + t0;
+                float r[8];
+                if ((reinterpret_cast<uintptr_t>(x) & 15) == 0)
+                {
+                    const float4 a = __ldg(reinterpret_cast<const float4*>(x));
+                    const float4 c4 = __ldg(reinterpret_cast<const float4*>(x + 4));
+                    r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
+                    r[4] = c4.x; r[5] = c4.y; r[6] = c4.z; r[7] = c4.w;
+                }
+                else
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) r[k] = __ldg(x + k);
+                if (sig.preemph)
+                {
+                    float prev = __ldg(x - 1);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                    {
+                        v[k] = __fsub_rn(r[k], __fmul_rn(sig.c, prev));
+                        prev = r[k];
+                    }
+                }
+                else
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) v[k] = r[k];
+            }
+            else
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] = i0 + k < clipStride ? sig(i0 + k) : 0.f;
+            const size_t o = size_t(b) * clipStride + i0;
             if constexpr (FMT == kTcTf32)
             {
-                uint32_t t;
-                asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
-                static_cast<uint32_t*>(outHi)[o] = t;
+                uint32_t t[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t[k]) : "f"(v[k]));
+                uint32_t* out = static_cast<uint32_t*>(outHi) + o;
+                if (whole)
+                {
+                    reinterpret_cast<uint4*>(out)[0] = make_uint4(t[0], t[1], t[2], t[3]);
+                    reinterpret_cast<uint4*>(out)[1] = make_uint4(t[4], t[5], t[6], t[7]);
+                }
+                else
+                    for (int k = 0; k < 8 && i0 + k < clipStride; ++k) out[k] = t[k];
             }
             else
             {
-                const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-                static_cast<__nv_bfloat16*>(outHi)[o] = hi;
-                if constexpr (FMT == kTcBf16x3)
-                    static_cast<__nv_bfloat16*>(outLo)[o] = __float2bfloat16_rn(v - __bfloat162float(hi));
+                uint32_t hw[4], lw[4];
+#pragma unroll
+                for (int k = 0; k < 8; k += 2)
+                {
+                    const __nv_bfloat16 h0 = __float2bfloat16_rn(v[k]), h1 = __float2bfloat16_rn(v[k + 1]);
+                    hw[k / 2] = uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
+                    if constexpr (FMT == kTcBf16x3)
+                    {
+                        const __nv_bfloat16 l0 = __float2bfloat16_rn(v[k] - __bfloat162float(h0));
+                        const __nv_bfloat16 l1 = __float2bfloat16_rn(v[k + 1] - __bfloat162float(h1));
+                        lw[k / 2] = uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
+                    }
+                }
+                __nv_bfloat16* hi = static_cast<__nv_bfloat16*>(outHi) + o;
+                __nv_bfloat16* lo = FMT == kTcBf16x3 ? static_cast<__nv_bfloat16*>(outLo) + o : nullptr;
+                if (whole)
+                {
+                    *reinterpret_cast<uint4*>(hi) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    if constexpr (FMT == kTcBf16x3) *reinterpret_cast<uint4*>(lo) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                }
+                else
+                    for (int k = 0; k < 8 && i0 + k < clipStride; ++k)
+                    {
+                        hi[k] = __ushort_as_bfloat16(uint16_t(hw[k / 2] >> (16 * (k & 1))));
+                        if constexpr (FMT == kTcBf16x3) lo[k] = __ushort_as_bfloat16(uint16_t(lw[k / 2] >> (16 * (k & 1))));
+                    }
             }
         }
     }
@@ -1080,7 +1149,7 @@ void launch_tc_spectrogram(Handle& h, void* scratch, const TcSpectrogramArgs& s)
     }
     else
     {
-        dim3 pg(std::min<uint32_t>((s.geo.clipStride + 255) / 256, 64u), std::min(s.n, 65535));
+        dim3 pg(std::min<uint32_t>((s.geo.clipStride / 8 + 255) / 256 + 1, 64u), std::min(s.n, 65535));
         if (s.fmt == kTcTf32) tc_prep_kernel<kTcTf32><<<pg, 256, 0, h.stream()>>>(p, aHi, nullptr, s.geo.clipStride);
         else if (s.fmt == kTcBf16x3)
             tc_prep_kernel<kTcBf16x3><<<pg, 256, 0, h.stream()>>>(p, aHi, aLo, s.geo.clipStride);
