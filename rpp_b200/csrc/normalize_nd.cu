@@ -19,7 +19,7 @@
 //     clamped to their range, then truncated; half rounded to nearest even).
 // Kernels: zero_kernel (the sample's destination elements the output does not cover), stats_kernel
 // (one thread per parameter, or one warp per parameter for lines of >= 544 elements),
-// normalize_kernel (one sample per grid row, elements strided over its CTAs).
+// normalize_kernel (samples over the grid's rows, elements strided over its CTAs).
 #include <cuda_fp16.h>
 
 #include "common.cuh"
@@ -180,38 +180,42 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormNdArgs a, const int
 template <int TYPE>
 __global__ void __launch_bounds__(kThreads) zero_kernel(NormNdArgs a)
 {
-    const int b = blockIdx.y;
-    const NormNdSample s = a.samples[b];
-    void* dst = static_cast<char*>(a.dst) + size_t(b) * a.dstStride0 * a.dstElem;
-    for (size_t i = s.zeroFrom + size_t(blockIdx.x) * kThreads + threadIdx.x; i < a.dstStride0;
-         i += size_t(gridDim.x) * kThreads)
-        store_elem<TYPE>(dst, i, 0.f);
+    for (int b = blockIdx.y; b < a.n; b += gridDim.y)
+    {
+        const size_t zeroFrom = a.samples[b].zeroFrom;
+        void* dst = static_cast<char*>(a.dst) + size_t(b) * a.dstStride0 * a.dstElem;
+        for (size_t i = zeroFrom + size_t(blockIdx.x) * kThreads + threadIdx.x; i < a.dstStride0;
+             i += size_t(gridDim.x) * kThreads)
+            store_elem<TYPE>(dst, i, 0.f);
+    }
 }
 
 template <int TYPE>
 __global__ void __launch_bounds__(kThreads) normalize_kernel(NormNdArgs a, const float* __restrict__ mean,
                                                              const float* __restrict__ inv, int paramOffsetPerSample)
 {
-    const int b = blockIdx.y;
-    const NormNdSample s = a.samples[b];
-    const void* src = static_cast<const char*>(a.src) + size_t(b) * a.srcStride0 * a.srcElem;
-    void* dst = static_cast<char*>(a.dst) + size_t(b) * a.dstStride0 * a.dstElem;
-    const float* m = mean + size_t(b) * paramOffsetPerSample;
-    const float* iv = inv + size_t(b) * paramOffsetPerSample;
-    for (size_t e = size_t(blockIdx.x) * kThreads + threadIdx.x; e < s.elems; e += size_t(gridDim.x) * kThreads)
+    for (int b = blockIdx.y; b < a.n; b += gridDim.y)
     {
-        size_t so = s.srcBase, dof = 0, rem = e;
-        uint32_t p = 0;
-        for (int l = s.levels - 1; l >= 0; --l)
+        const NormNdSample s = a.samples[b];
+        const void* src = static_cast<const char*>(a.src) + size_t(b) * a.srcStride0 * a.srcElem;
+        void* dst = static_cast<char*>(a.dst) + size_t(b) * a.dstStride0 * a.dstElem;
+        const float* m = mean + size_t(b) * paramOffsetPerSample;
+        const float* iv = inv + size_t(b) * paramOffsetPerSample;
+        for (size_t e = size_t(blockIdx.x) * kThreads + threadIdx.x; e < s.elems; e += size_t(gridDim.x) * kThreads)
         {
-            const size_t c = rem % s.lv[l].count;
-            rem /= s.lv[l].count;
-            so += c * s.lv[l].srcStride;
-            dof += c * s.lv[l].dstStride;
-            p += uint32_t(c) * s.lv[l].paramMult;
+            size_t so = s.srcBase, dof = 0, rem = e;
+            uint32_t p = 0;
+            for (int l = s.levels - 1; l >= 0; --l)
+            {
+                const size_t c = rem % s.lv[l].count;
+                rem /= s.lv[l].count;
+                so += c * s.lv[l].srcStride;
+                dof += c * s.lv[l].dstStride;
+                p += uint32_t(c) * s.lv[l].paramMult;
+            }
+            const float x = load_elem<TYPE>(src, so);
+            store_elem<TYPE>(dst, dof, __fadd_rn(__fmul_rn(__fsub_rn(x, m[p]), iv[p]), a.shift));
         }
-        const float x = load_elem<TYPE>(src, so);
-        store_elem<TYPE>(dst, dof, __fadd_rn(__fmul_rn(__fsub_rn(x, m[p]), iv[p]), a.shift));
     }
 }
 
@@ -233,7 +237,7 @@ void launch_type(Handle& h, const NormNdArgs& a, const int4* tasks, int numTasks
     const dim3 block(kThreads);
     if (maxZero > 0)
     {
-        const dim3 grid(unsigned(std::min<size_t>((maxZero + kThreads - 1) / kThreads, 1024)), unsigned(a.n));
+        const dim3 grid(unsigned(std::min<size_t>((maxZero + kThreads - 1) / kThreads, 1024)), unsigned(std::min(a.n, 65535)));
         zero_kernel<TYPE><<<grid, block, 0, h.stream()>>>(a);
         count_launch(1);
     }
@@ -246,7 +250,7 @@ void launch_type(Handle& h, const NormNdArgs& a, const int4* tasks, int numTasks
     }
     if (maxElems > 0)
     {
-        const dim3 grid(unsigned(std::min<size_t>((maxElems + kThreads - 1) / kThreads, 1024)), unsigned(a.n));
+        const dim3 grid(unsigned(std::min<size_t>((maxElems + kThreads - 1) / kThreads, 1024)), unsigned(std::min(a.n, 65535)));
         normalize_kernel<TYPE><<<grid, block, 0, h.stream()>>>(a, meanEff, invEff, paramOffsetPerSample);
         count_launch(1);
     }
