@@ -1031,6 +1031,7 @@ bool plan_3d(const RpptGenericDesc& sd, const RpptGenericDesc& dd, unsigned axis
              const uint32_t* length, NormNdSample& s, uint32_t& params)
 {
     const uint32_t L0 = length[0], L1 = length[1], L2 = length[2];
+    if (uint64_t(L0) * L1 * L2 > UINT32_MAX) return false;   // the reduction counts stay 32-bit
     const uint32_t S1 = sd.strides[1], S2 = sd.strides[2], S3 = sd.strides[3];
     uint32_t rd[3], rs[3];
     bool ps[3] = {false, false, false};
@@ -1108,6 +1109,9 @@ bool plan_nd(const RpptGenericDesc& sd, int T, unsigned axisMask, const uint32_t
              NormNdSample& s, uint32_t& params)
 {
     uint32_t axis[4], newAxis[4] = {0, 0, 0, 0}, newDims[4] = {0, 0, 0, 0}, size = 1, total = 1;
+    uint64_t volume = 1;
+    for (int i = 0; i < T; ++i) volume *= length[i];
+    if (volume > UINT32_MAX) return false;   // dense strides and counts stay 32-bit
     s.srcBase = 0;
     for (int i = 0; i < T; ++i)
     {
