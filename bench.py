@@ -916,8 +916,42 @@ def run_b200(args, world, rank, local):
         out_host.copy_(fused.run(x_dev), non_blocking=True)
 
     full_ms = timed_host(e2e_full_step, e_steps)
+    # the link's bounds for the same byte counts: one contiguous copy-engine transfer each way, together
+    # (full duplex) and one after the other, pinned host memory on both ends
+    def link_ms(directions):
+        hin = x_host.view(-1)[:h2d // 4]
+        hout = out_host.view(-1)[:d2h // 4]
+        din = torch.empty(hin.numel(), device=x.device)
+        dout = torch.empty(hout.numel(), device=x.device)
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+        times = []
+        for _ in range(5):
+            st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            st.record()
+            s_in.wait_event(st)
+            s_out.wait_event(st)
+            if "in" in directions:
+                with torch.cuda.stream(s_in):
+                    din.copy_(hin, non_blocking=True)
+            if "out" in directions:
+                with torch.cuda.stream(s_out):
+                    hout.copy_(dout, non_blocking=True)
+            torch.cuda.current_stream().wait_stream(s_in)
+            torch.cuda.current_stream().wait_stream(s_out)
+            en.record()
+            torch.cuda.synchronize()
+            times.append(st.elapsed_time(en))
+        del din, dout
+        return float(np.median(times[1:]))
+
+    duplex_ms = link_ms(("in", "out"))
+    one_way_ms = link_ms(("in",)) + link_ms(("out",))
     e2e = {"value": replicas.job_throughput(clip_s, e2e_ms, world), "unit": "clip-s/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+           "pcie_duplex_bound_ms": duplex_ms, "frac_of_duplex_bound": duplex_ms / e2e_ms,
+           "pcie_sum_of_one_way_ms": one_way_ms,
+           "pcie_note": "bounds from contiguous copy-engine transfers of the same byte counts; the call moves ragged "
+                        "clips with SM-initiated copies, whose two directions only partly overlap on this link",
            "path": "pinned host tensors -> rppb_frontend_host_gpu (C ABI): valid samples copied in, valid decibel "
                    "rows copied out, %s chunks overlapping copy-in / kernels / copy-out" % (args.chunks or 16),
            "whole_tensor_copies": {"value": replicas.job_throughput(clip_s, full_ms, world), "ms_per_step": full_ms,
