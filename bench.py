@@ -395,7 +395,7 @@ def error_vs_fp64(chain, x_np, lens_np, clips=8, db_out=None):
             "note": "mel from the plain chain, dB from the fused call (bit-identical chains)"}
 
 
-def serving_measurement(torch, n_requests):
+def serving_measurement(torch, n_requests, link_gbs=None):
     """Serving: continuous-batching server (rpp_b200/serving.py) over a 40 GB device budget, with each step
     run by the fused front end and, for comparison on the same GPU, by the plain FP32 path (resample + the
     four rppt_*_gpu calls on a batch buffer); per mode the capacity from a closed burst, then open-loop
@@ -403,7 +403,12 @@ def serving_measurement(torch, n_requests):
     from rpp_b200 import serving
     rng = np.random.Generator(np.random.PCG64(20261203 + 4))
     pool = serving.ClipPool(torch, rng)
-    mean_cs = np.mean([serving.clip_seconds(pool.request(i, rng)) for i in range(2000)])
+    sample = [pool.request(i, rng) for i in range(2000)]
+    mean_cs = np.mean([serving.clip_seconds(r) for r in sample])
+    # PCIe bytes per clip-second of this request mix: float32 input at its own rate, 128 x 100 float32
+    # decibels per second out
+    in_bytes = sum(4 * c.numel() for r in sample for c in r.clips)
+    bytes_per_cs = in_bytes / sum(serving.clip_seconds(r) for r in sample) + 4 * 128 * 100
     modes = {}
     for mode, plain in (("fused", False), ("plain_fp32", True)):
         server = serving.FrontendServer(torch, budget_bytes=40 << 30, max_clips=256, tables=4, plain=plain)
@@ -418,7 +423,16 @@ def serving_measurement(torch, n_requests):
         server.close()
         modes[mode] = {"capacity_clip_s_per_s": cap, "loads": loads}
     f = modes["fused"]
+    bound = None
+    if link_gbs:
+        # the roofline of this loop is the host link: bytes per clip-second over the link rate measured by
+        # the e2e section (copy-engine transfers, both directions one after the other)
+        pb = link_gbs * 1e9 / bytes_per_cs
+        bound = {"bytes_per_clip_s": bytes_per_cs, "link_gbs_one_way": link_gbs, "pcie_bound_clip_s_per_s": pb,
+                 "frac_fused": f["capacity_clip_s_per_s"] / pb,
+                 "frac_plain_fp32": modes["plain_fp32"]["capacity_clip_s_per_s"] / pb}
     return {"capacity_clip_s_per_s": f["capacity_clip_s_per_s"], "loads": f["loads"], "modes": modes,
+            "roofline": bound,
             "mean_request_clip_s": float(mean_cs), "requests_per_point": n_requests, "budget_gb": 40,
             "chain": "resample (Kaiser sinc, 16 zero crossings) -> pre-emphasis -> STFT(512, 400, 160) -> mel(128) -> "
                      "dB, one captured graph per step over a device clip table; native scheduler thread "
@@ -1013,7 +1027,8 @@ def run_b200(args, world, rank, local):
         serve = None
         if args.serve_requests > 0:
             try:
-                serve = serving_measurement(torch, args.serve_requests)
+                link = (e2e["h2d_bytes_per_step"] + e2e["d2h_bytes_per_step"]) / (e2e["pcie_sum_of_one_way_ms"] * 1e6)
+                serve = serving_measurement(torch, args.serve_requests, link)
             except Exception as exc:   # report, do not lose the main line
                 serve = {"error": repr(exc)}
         try:
