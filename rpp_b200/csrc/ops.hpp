@@ -24,6 +24,9 @@ struct ResampleWindowDev
     float scale, center;
     int lobes;
     int padLeft = 0, padRight = 0;   // set by the resample launchers (shared-memory pair table padding)
+    // set by the resample launchers: outputs whose phase has a binary exponent in [exactMinE, exactMaxE]
+    // take the exact walk (every tap position exact in float; resample.cu)
+    int exactMinE = 1 << 30, exactMaxE = -(1 << 30);
 };
 // downmix: the input is interleaved {length, channels} and is down-mixed to mono while resampling
 // (equal to rppt_down_mixing_gpu followed by a mono rppt_resample_gpu).

@@ -12,12 +12,16 @@
 // summed per channel in order.  Every product and sum is explicitly rounded, so outputs are
 // bit-identical to the host path.
 //
-// One CTA of 8 + 1 warps walks the 256-output blocks: the ninth warp replays the next block's phase
-// sum into shared memory (double-buffered) while the eight compute this block, one output per
-// thread; when down-mixing, the block's input span is staged (down-mixed once per input sample) in
-// shared memory first.  The lookup table sits in shared memory as (value, next - value) pairs when
-// they fit, so a tap reads one 8-byte entry.  Compute-bound: 2 * lobes taps of ~10 float
-// operations per output.
+// One CTA of 8 + 1 warps takes its 256-output blocks in groups of eight.  The ninth warp decodes the
+// next group into shared memory: where each block lives, its output count and its phase sum, the
+// eight sums side by side, one per lane.  Meanwhile the eight compute warps work through the current
+// group, each taking one 32-output slice of every block of the group.  A block's first slice, the one
+// with the smallest phases, falls to a different warp for each block.  When down-mixing, each warp
+// stages its slice's input span (down-mixed once per input sample) in shared memory.  The lookup table
+// sits in shared memory as (value, next - value) pairs when they fit, so a tap reads one 8-byte entry.
+// Where a slice's phases allow it, the taps take the exact walk (resample_exact_range): each tap reads
+// the entry 32 positions past the previous one and uses the same weight.  That is 4 float operations
+// and 2 loads per tap, in place of ~10 operations.  Compute-bound.
 #include <algorithm>
 #include <cmath>
 
@@ -30,21 +34,20 @@ namespace {
 
 constexpr int kBlock = 256;        // outputs per block (the reference's block size)
 constexpr int kCopyChunk = 4096;   // floats per unit of an equal-rate copy
-constexpr int kSpan = 4096;        // input samples of one block staged in shared memory (mono paths)
 
 constexpr int kThreads = kBlock + 32;   // 8 warps compute outputs, the ninth replays the next unit's phases
 
 // Shared memory (floats): the table -- as padded (value, next - value) pairs when kPairs, else
-// plain -- then the staged input span.
+// plain -- then, when down-mixing, the staged input span.
 __host__ __device__ __forceinline__ size_t resample_pair_entries(int lutSize, int padLeft, int padRight)
 {
     return size_t(padLeft) + size_t(lutSize - 1) + size_t(padRight);
 }
-__host__ __device__ __forceinline__ size_t resample_smem_floats(const ResampleWindowDev& w, bool pairs)
+__host__ __device__ __forceinline__ size_t resample_smem_floats(const ResampleWindowDev& w, bool pairs, bool span)
 {
     return (pairs ? 2 * resample_pair_entries(w.lutSize, w.padLeft, w.padRight)
                   : ((size_t(w.lutSize) + 3) & ~size_t(3))) +
-           kSpan;
+           (span ? size_t(kBlock / 32) * 256 : 0);   // down-mixing: each compute warp's slice span
 }
 constexpr size_t kPairTableLimit = 200 * 1024;   // bytes of shared memory for the pair layout
 
@@ -67,6 +70,30 @@ inline bool resample_scale_pow2(const ResampleWindowDev& w)
 {
     int e = 0;
     return w.scale > 0.f && std::isfinite(w.scale) && std::frexp(double(w.scale), &e) == 0.5;
+}
+
+// The exact walk.  With table scale 32 and an integer center, take an output whose phase p has binary
+// exponent E (p in [2^E, 2^(E+1))).  A tap at input sample l has offset l - p, a multiple of 2^(E-23)
+// (l is an integer, E <= 23) with |l - p| <= lobes.  When lobes < 2^(E+1) that offset is a float, so the
+// reference's float subtraction and its lane increments by 1 and 4 are exact.  The tap's table position
+// 32 (l - p) + center is a multiple of 2^(E-18) (E <= 18) below center + 32 lobes; when that is below
+// 2^(E+6) the position is a float too, so the fused multiply-add is exact.  The positions of consecutive
+// taps then differ by exactly 32: their table indices are 32 apart and their interpolation weights equal.
+// The range is empty unless the kernel takes the round-down-add index (kMagic) and the FMA position
+// (kFma), whose values these are.
+inline void resample_exact_range(ResampleWindowDev& w, bool magic, bool fma)
+{
+    w.exactMinE = 1 << 30;
+    w.exactMaxE = -(1 << 30);
+    if (!magic || !fma || w.scale != 32.f || w.center != std::floor(w.center) || w.lobes < 1) return;
+    for (int e = -126; e <= 18; ++e)
+        if (double(w.lobes) < std::ldexp(1.0, e + 1) &&
+            double(w.center) + 32.0 * double(w.lobes) < std::ldexp(1.0, e + 6))
+        {
+            w.exactMinE = e;
+            w.exactMaxE = 18;
+            return;
+        }
 }
 
 inline void resample_pads(ResampleWindowDev& w)
@@ -176,32 +203,56 @@ struct Win
     }
 };
 
-// Where unit w of the flat work list lives and, for a resampling unit, its phases.
+// The exact walk (resample_exact_range): the pair entry at byte offset kOff from shared address a.
+template <int kOff>
+__device__ __forceinline__ float2 pair_at(uint32_t a)
+{
+    float2 v;
+    asm("ld.shared.v2.f32 {%0, %1}, [%2+%3];" : "=f"(v.x), "=f"(v.y) : "r"(a), "n"(kOff));
+    return v;
+}
+
+// A unit of the flat work list, decoded by the phase warp for the compute warps.
+constexpr int kUnitSkip = 0, kUnitCopy = 1, kUnitResample = 2;
 struct UnitInfo
 {
-    int b, unit, L, Csrc, C;
-    float inRate, outRate;
-    const float* x;
-    float* y;
+    const float* x;        // the sample's input
+    float* y;              // the sample's output
+    int L, Csrc, C;        // input length, input channels, channels of the resampled signal
+    int unit;              // the unit's index within its sample
     uint32_t dstStride;
+    int mode;              // kUnitSkip, kUnitCopy or kUnitResample
+    int outEnd;            // resampling: outputs of the sample that the destination takes
+    int inBlockRounded;    // resampling: the input sample the unit's phases count from
+    float wc;              // down-mixing: the weight of every channel
 };
+
+// A CTA takes its units (blockIdx.x + i * gridDim.x, i = 0, 1, ...) in groups of kGroup.  Lane j of the
+// phase warp decodes unit j of the next group (the eight phase sums run side by side) while the compute
+// warps work through the current group in kGroup steps: at step s, warp w takes outputs [32 s, 32 s + 32)
+// of unit (w + s) mod kGroup.  A unit's first outputs have the smallest phases and are the ones the exact
+// walk may not cover, so every warp takes one such slice per group and the group barrier waits for no
+// single slow warp.
+constexpr int kWarps = kBlock / 32;   // compute warps
+constexpr int kGroup = kWarps;
+constexpr int kSliceSpan = 256;       // down-mixing: input samples of one slice staged by its warp
+static_assert(kGroup == kWarps && kBlock == kWarps * 32, "one 32-output slice per compute warp and step");
 
 // kMix: the input is interleaved multi-channel and is down-mixed to mono on the fly (MonoMix), so
 // the launch equals rppt_down_mixing_gpu followed by a mono rppt_resample_gpu.
 template <bool kMix, bool kTable, bool kPairs, bool kMagic = false, bool kFma = false>
-__global__ void __launch_bounds__(kThreads) resample_kernel(const float* __restrict__ src, uint32_t srcStride,
-                                                            float* __restrict__ dst, uint32_t dstStride,
-                                                            const float* __restrict__ inRateT,
-                                                            const float* __restrict__ outRateT,
-                                                            const int* __restrict__ dims, ResampleWindowDev wd,
-                                                            bool normalize, const long long* __restrict__ prefix,
-                                                            int n, const RppbClip* __restrict__ clips,
-                                                            float outRateAll)
+__global__ void __launch_bounds__(kThreads, kMix ? 5 : 4)
+    resample_kernel(const float* __restrict__ src, uint32_t srcStride, float* __restrict__ dst, uint32_t dstStride,
+                    const float* __restrict__ inRateT, const float* __restrict__ outRateT,
+                    const int* __restrict__ dims, ResampleWindowDev wd, bool normalize,
+                    const long long* __restrict__ prefix, int n, const RppbClip* __restrict__ clips,
+                    float outRateAll)
 {
-    extern __shared__ float s_lut[];   // the table, then the staged input span
+    extern __shared__ float s_lut[];   // the table, then (down-mixing) each compute warp's staged slice span
     const int pairCount = kPairs ? int(resample_pair_entries(wd.lutSize, wd.padLeft, wd.padRight)) : 0;
-    float* s_in = s_lut + (kPairs ? 2 * pairCount : ((wd.lutSize + 3) & ~3));
-    __shared__ float s_phase[2][kBlock];
+    float* s_spans = s_lut + (kPairs ? 2 * pairCount : ((wd.lutSize + 3) & ~3));
+    __shared__ __align__(16) float s_phase[2][kGroup][kBlock];
+    __shared__ UnitInfo s_unit[2][kGroup];
     if (kPairs)
         for (int i = threadIdx.x; i < pairCount; i += kThreads)
         {
@@ -219,163 +270,218 @@ __global__ void __launch_bounds__(kThreads) resample_kernel(const float* __restr
     __shared__ long long s_prefix[kPrefixCache];
     prefix = cache_prefix(prefix, n, s_prefix);   // ends with __syncthreads
     const long long total = prefix[n];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    auto info = [&](long long w) {
+    // the CTA's unit j of group g
+    auto unit_of = [&](long long g, int j) {
+        return (long long)blockIdx.x + (g * kGroup + j) * (long long)gridDim.x;
+    };
+    // decodes unit w into s_unit[slot][j]: where it lives, what it does and, for a resampling unit, the
+    // reference's phase sum into s_phase[slot][j] (replayed in its float order)
+    auto decode = [&](long long w, int slot, int j) {
         UnitInfo u;
-        u.b = ragged_find(prefix, n, w);
-        u.unit = int(w - prefix[u.b]);
-        u.L = kTable ? clips[u.b].length : dims[2 * u.b];
-        u.Csrc = kTable ? 1 : dims[2 * u.b + 1];
-        u.C = kMix ? 1 : u.Csrc;   // channels of the resampled signal
-        u.inRate = kTable ? clips[u.b].inRate : inRateT[u.b];
-        u.outRate = kTable ? outRateAll : outRateT[u.b];
-        u.x = kTable ? clips[u.b].src : src + size_t(u.b) * srcStride;
-        u.y = kTable ? clips[u.b].work : dst + size_t(u.b) * dstStride;
-        u.dstStride = kTable ? 0x7fffffffu : dstStride;   // a clip's work buffer holds the whole resampled clip
-        return u;
-    };
-    // the reference's phase sum of a resampling unit (one thread; replayed in its float order)
-    auto phases = [&](long long w, float* out) {
-        if (w >= total) return;
-        const UnitInfo u = info(w);
-        if (u.inRate == u.outRate || (kMix && u.Csrc > 64)) return;
-        const double scale = __ddiv_rn(double(u.inRate), double(u.outRate));
-        const float fscale = __double2float_rn(scale);
-        const double inBlockRaw = __dmul_rn(double(u.unit * kBlock), scale);
-        float p = __double2float_rn(__dsub_rn(inBlockRaw, double(int(inBlockRaw))));
-        for (int k = 0; k < kBlock; ++k)
+        u.mode = kUnitSkip;
+        if (w < total)
         {
-            out[k] = p;
-            p = __fadd_rn(p, fscale);
+            const int b = ragged_find(prefix, n, w);
+            u.unit = int(w - prefix[b]);
+            u.L = kTable ? clips[b].length : dims[2 * b];
+            u.Csrc = kTable ? 1 : dims[2 * b + 1];
+            u.C = kMix ? 1 : u.Csrc;
+            const float inRate = kTable ? clips[b].inRate : inRateT[b];
+            const float outRate = kTable ? outRateAll : outRateT[b];
+            u.x = kTable ? clips[b].src : src + size_t(b) * srcStride;
+            u.y = kTable ? clips[b].work : dst + size_t(b) * dstStride;
+            u.dstStride = kTable ? 0x7fffffffu : dstStride;   // a clip's work buffer holds the whole resampled clip
+            u.wc = kMix ? MonoMix::weight(max(u.Csrc, 1), normalize) : 1.f;
+            u.mode = inRate == outRate ? kUnitCopy : (kMix && u.Csrc > 64) ? kUnitSkip : kUnitResample;
+            u.outEnd = 0;
+            u.inBlockRounded = 0;
+            if (u.mode == kUnitResample)
+            {
+                u.outEnd = min(out_length(u.L, inRate, outRate), int(u.dstStride / uint32_t(u.C)));
+                const double scale = __ddiv_rn(double(inRate), double(outRate));
+                const float fscale = __double2float_rn(scale);
+                const double inBlockRaw = __dmul_rn(double(u.unit * kBlock), scale);
+                u.inBlockRounded = int(inBlockRaw);
+                float p = __double2float_rn(__dsub_rn(inBlockRaw, double(int(inBlockRaw))));
+                float4* out = reinterpret_cast<float4*>(s_phase[slot][j]);
+#pragma unroll 8
+                for (int k = 0; k < kBlock / 4; ++k)
+                {
+                    float4 q;
+                    q.x = p;
+                    q.y = p = __fadd_rn(p, fscale);
+                    q.z = p = __fadd_rn(p, fscale);
+                    q.w = p = __fadd_rn(p, fscale);
+                    p = __fadd_rn(p, fscale);
+                    out[k] = q;
+                }
+            }
         }
+        s_unit[slot][j] = u;
     };
 
-    if (threadIdx.x == kBlock) phases(blockIdx.x, s_phase[0]);
+    if (warp == kWarps && lane < kGroup) decode(unit_of(0, lane), 0, lane);
     __syncthreads();
     int cur = 0;
-    for (long long w = blockIdx.x; w < total; w += gridDim.x, cur ^= 1)
+    for (long long g = 0; unit_of(g, 0) < total; ++g, cur ^= 1)
     {
-        if (threadIdx.x >= kBlock)
+        if (warp == kWarps)
         {
-            // the ninth warp: the next unit's phases while the others compute this one
-            if (threadIdx.x == kBlock) phases(w + gridDim.x, s_phase[cur ^ 1]);
+            // the phase warp: the next group while the others compute this one
+            if (lane < kGroup) decode(unit_of(g + 1, lane), cur ^ 1, lane);
         }
         else
         {
-            const UnitInfo u = info(w);
-            const float* x = u.x;
-            float* y = u.y;
-            const int L = u.L, Csrc = u.Csrc, C = u.C;
-            const MonoMix mix{x, kMix ? Csrc : 1, kMix ? MonoMix::weight(max(Csrc, 1), normalize) : 1.f};
-            if (kMix && Csrc > 64)
+            float* s_span = s_spans + warp * kSliceSpan;
+            for (int step = 0; step < kGroup; ++step)
             {
-                // not handled here (rejected by the caller)
-            }
-            else if (u.inRate == u.outRate)
-            {
-                if (kMix)
+                const int j = (warp + step) % kGroup;
+                const UnitInfo u = s_unit[cur][j];
+                const float* x = u.x;
+                float* y = u.y;
+                const int L = u.L, C = u.C;
+                const MonoMix mix{x, kMix ? u.Csrc : 1, u.wc};
+                if (u.mode == kUnitCopy)
                 {
-                    const long long count = min((long long)L, (long long)u.dstStride);
-                    for (long long i = (long long)u.unit * kCopyChunk + threadIdx.x;
-                         i < min(count, (long long)(u.unit + 1) * kCopyChunk); i += kBlock)
-                        y[i] = mix(i);
-                }
-                else
-                {
+                    constexpr int kPart = kCopyChunk / kGroup;
                     const long long count =
-                        kTable ? (long long)L : min((long long)L * C, (long long)min(srcStride, u.dstStride));
-                    for (long long i = (long long)u.unit * kCopyChunk + threadIdx.x;
-                         i < min(count, (long long)(u.unit + 1) * kCopyChunk); i += kBlock)
-                        y[i] = x[i];
+                        kMix ? min((long long)L, (long long)u.dstStride)
+                             : (kTable ? (long long)L : min((long long)L * C, (long long)min(srcStride, u.dstStride)));
+                    const long long i0 = (long long)u.unit * kCopyChunk + step * kPart;
+                    for (long long i = i0 + lane; i < min(count, i0 + kPart); i += 32) y[i] = kMix ? mix(i) : x[i];
                 }
-            }
-            else
-            {
-                const float* ph = s_phase[cur];
-                const int outEnd = min(out_length(L, u.inRate, u.outRate), int(u.dstStride / uint32_t(C)));
-                const double scale = __ddiv_rn(double(u.inRate), double(u.outRate));
-                const int outBlock = u.unit * kBlock;
-                const int inBlockRounded = int(__dmul_rn(double(outBlock), scale));
-                const float* in = x + (long long)inBlockRounded * C;
-                // down-mixing path: the unit's input span [lo, hi), down-mixed once per sample, goes to
-                // shared memory (every tap of the unit lies inside it because the phases increase);
-                // plain mono input is read through L1 directly, which measured faster than staging it
-                int lo = 0;
-                bool staged = false;
-                if (kMix)
+                else if (u.mode == kUnitResample)
                 {
-                    const int cnt = min(kBlock, outEnd - outBlock);
-                    if (cnt > 0)
+                    const float* ph = s_phase[cur][j];
+                    const int outBlock = u.unit * kBlock;
+                    const int cnt = min(kBlock, u.outEnd - outBlock);   // outputs of the unit
+                    const int k0 = step * 32;                           // the slice's first output
+                    if (k0 < cnt)
                     {
-                        lo = max(int(ceilf(ph[0])) - lobes, -inBlockRounded);
-                        const int hi = min(int(ceilf(ph[cnt - 1])) + lobes, L - inBlockRounded);
-                        staged = hi - lo <= kSpan;
-                        if (staged)
-                            for (int i = threadIdx.x; i < hi - lo; i += kBlock)
-                                s_in[i] = mix((long long)inBlockRounded + lo + i);
-                    }
-                    asm volatile("bar.sync 1, %0;" ::"n"(kBlock) : "memory");   // the compute warps only
-                }
-                const int outPos = outBlock + threadIdx.x;
-                if (outPos < outEnd)
-                {
-                    const float inPos = ph[threadIdx.x];
-                    const int xc = int(ceilf(inPos));
-                    int loc0 = xc - lobes, loc1 = xc + lobes;
-                    if (loc0 + inBlockRounded < 0) loc0 = -inBlockRounded;
-                    if (loc1 + inBlockRounded > L) loc1 = L - inBlockRounded;
-                    if (kMix || C == 1)
-                    {
-                        // mono input: 4 lanes, folded as (l0 + l2) + (l1 + l3), then a scalar tail
-                        auto taps = [&](auto at) {
-                            int l = loc0;
-                            const float locBegin = __fsub_rn(float(l), inPos);
-                            float lane[4] = {__fadd_rn(locBegin, 0.f), __fadd_rn(locBegin, 1.f),
-                                             __fadd_rn(locBegin, 2.f), __fadd_rn(locBegin, 3.f)};
-                            float acc4[4] = {0.f, 0.f, 0.f, 0.f};
-                            for (; l + 3 < loc1; l += 4)
-                            {
-#pragma unroll
-                                for (int j = 0; j < 4; ++j)
-                                {
-                                    acc4[j] = __fadd_rn(acc4[j], __fmul_rn(at(l + j), win.lane(lane[j])));
-                                    lane[j] = __fadd_rn(lane[j], 4.f);
-                                }
-                            }
-                            float accum = __fadd_rn(__fadd_rn(acc4[0], acc4[2]), __fadd_rn(acc4[1], acc4[3]));
-                            float xx = __fsub_rn(float(l), inPos);
-                            for (; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
-                                accum = __fadd_rn(accum, __fmul_rn(at(l), win.scalar(xx)));
-                            return accum;
-                        };
-                        float r;
-                        if (kMix && staged) r = taps([&](int l) { return s_in[l - lo]; });
-                        else if (kMix) r = taps([&](int l) { return mix((long long)inBlockRounded + l); });
-                        else r = taps([&](int l) { return __ldg(in + l); });
-                        y[outPos] = r;
-                    }
-                    else
-                    {
-                        constexpr int kMaxC = 16;
-                        float acc[kMaxC];
-#pragma unroll
-                        for (int c = 0; c < kMaxC; ++c) acc[c] = 0.f;
-                        float xx = __fsub_rn(float(loc0), inPos);
-                        for (int l = loc0; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
+                        const int inBlockRounded = u.inBlockRounded;
+                        const float* in = x + (long long)inBlockRounded * C;
+                        // down-mixing: the slice's input span [lo, hi), down-mixed once per sample, staged by
+                        // this warp (every tap of the slice lies inside it because the phases increase)
+                        int lo = 0;
+                        bool staged = false;
+                        if (kMix)
                         {
-                            const float wv = win.scalar(xx);
-#pragma unroll
-                            for (int c = 0; c < kMaxC; ++c)
-                                if (c < C) acc[c] = __fadd_rn(acc[c], __fmul_rn(__ldg(in + (long long)l * C + c), wv));
+                            lo = max(int(ceilf(ph[k0])) - lobes, -inBlockRounded);
+                            const int hi = min(int(ceilf(ph[min(k0 + 31, cnt - 1)])) + lobes, L - inBlockRounded);
+                            staged = hi - lo <= kSliceSpan;
+                            if (staged)
+                                for (int i = lane; i < hi - lo; i += 32)
+                                    s_span[i] = mix((long long)inBlockRounded + lo + i);
+                            __syncwarp();
                         }
+                        const int k = k0 + lane;
+                        const int outPos = outBlock + k;
+                        const float inPos = ph[k];
+                        // the exact walk (resample_exact_range) where every output of the slice allows it,
+                        // so a warp runs one of the two tap loops
+                        bool exact = false;
+                        if constexpr (kPairs && kMagic && kFma)
+                        {
+                            const int e = int((__float_as_uint(inPos) >> 23) & 0xffu) - 127;
+                            exact = __all_sync(0xffffffffu, k >= cnt || (e >= wd.exactMinE && e <= wd.exactMaxE));
+                        }
+                        if (k < cnt)
+                        {
+                            const int xc = int(ceilf(inPos));
+                            int loc0 = xc - lobes, loc1 = xc + lobes;
+                            if (loc0 + inBlockRounded < 0) loc0 = -inBlockRounded;
+                            if (loc1 + inBlockRounded > L) loc1 = L - inBlockRounded;
+                            if (kMix || C == 1)
+                            {
+                                // mono input: 4 lanes, folded as (l0 + l2) + (l1 + l3), then a scalar tail
+                                auto taps = [&](auto at) {
+                                    int l = loc0;
+                                    const float locBegin = __fsub_rn(float(l), inPos);
+                                    float lane4[4] = {__fadd_rn(locBegin, 0.f), __fadd_rn(locBegin, 1.f),
+                                                      __fadd_rn(locBegin, 2.f), __fadd_rn(locBegin, 3.f)};
+                                    float acc4[4] = {0.f, 0.f, 0.f, 0.f};
+                                    for (; l + 3 < loc1; l += 4)
+                                    {
 #pragma unroll
-                        for (int c = 0; c < kMaxC; ++c)
-                            if (c < C) y[(long long)outPos * C + c] = acc[c];
+                                        for (int q = 0; q < 4; ++q)
+                                        {
+                                            acc4[q] = __fadd_rn(acc4[q], __fmul_rn(at(l + q), win.lane(lane4[q])));
+                                            lane4[q] = __fadd_rn(lane4[q], 4.f);
+                                        }
+                                    }
+                                    float accum = __fadd_rn(__fadd_rn(acc4[0], acc4[2]), __fadd_rn(acc4[1], acc4[3]));
+                                    float xx = __fsub_rn(float(l), inPos);
+                                    for (; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
+                                        accum = __fadd_rn(accum, __fmul_rn(at(l), win.scalar(xx)));
+                                    return accum;
+                                };
+                                // the exact walk: the first tap's pair entry and weight by the same operations
+                                // as above, then each tap 32 entries (256 bytes) further on at that weight; the
+                                // same products and sums in the same order
+                                auto taps_exact = [&](auto at) {
+                                    constexpr float kM = 12582912.0f;   // 1.5 * 2^23
+                                    const float locRaw =
+                                        __fmaf_rn(__fsub_rn(float(loc0), inPos), win.scale, win.center);
+                                    const float m = __fadd_rd(locRaw, kM);
+                                    const float w = __fsub_rn(locRaw, __fsub_rn(m, kM));
+                                    uint32_t a = win.bias + (uint32_t(__float_as_int(m)) << 3);
+                                    auto tap = [&](int l, float2 e) {
+                                        return __fmul_rn(at(l), __fadd_rn(e.x, __fmul_rn(w, e.y)));
+                                    };
+                                    int l = loc0;
+                                    float acc4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+                                    for (; l + 3 < loc1; l += 4, a += 4 * 256)
+                                    {
+                                        acc4[0] = __fadd_rn(acc4[0], tap(l, pair_at<0>(a)));
+                                        acc4[1] = __fadd_rn(acc4[1], tap(l + 1, pair_at<256>(a)));
+                                        acc4[2] = __fadd_rn(acc4[2], tap(l + 2, pair_at<512>(a)));
+                                        acc4[3] = __fadd_rn(acc4[3], tap(l + 3, pair_at<768>(a)));
+                                    }
+                                    float accum = __fadd_rn(__fadd_rn(acc4[0], acc4[2]), __fadd_rn(acc4[1], acc4[3]));
+                                    for (; l < loc1; ++l, a += 256) accum = __fadd_rn(accum, tap(l, pair_at<0>(a)));
+                                    return accum;
+                                };
+                                auto run = [&](auto at) {
+                                    if constexpr (kPairs && kMagic && kFma)
+                                        if (exact) return taps_exact(at);
+                                    return taps(at);
+                                };
+                                float r;
+                                if (kMix && staged) r = run([&](int l) { return s_span[l - lo]; });
+                                else if (kMix) r = run([&](int l) { return mix((long long)inBlockRounded + l); });
+                                else r = run([&](int l) { return __ldg(in + l); });
+                                y[outPos] = r;
+                            }
+                            else
+                            {
+                                constexpr int kMaxC = 16;
+                                float acc[kMaxC];
+#pragma unroll
+                                for (int c = 0; c < kMaxC; ++c) acc[c] = 0.f;
+                                float xx = __fsub_rn(float(loc0), inPos);
+                                for (int l = loc0; l < loc1; ++l, xx = __fadd_rn(xx, 1.f))
+                                {
+                                    const float wv = win.scalar(xx);
+#pragma unroll
+                                    for (int c = 0; c < kMaxC; ++c)
+                                        if (c < C)
+                                            acc[c] = __fadd_rn(acc[c], __fmul_rn(__ldg(in + (long long)l * C + c), wv));
+                                }
+#pragma unroll
+                                for (int c = 0; c < kMaxC; ++c)
+                                    if (c < C) y[(long long)outPos * C + c] = acc[c];
+                            }
+                        }
+                        if (kMix) __syncwarp();   // the warp's span is restaged by its next slice
                     }
                 }
+                // kUnitSkip: no unit, or more than 64 channels to down-mix (rejected by the caller)
             }
         }
-        __syncthreads();   // s_phase[cur] is rewritten two units on; s_phase[cur ^ 1] is ready
+        __syncthreads();   // slot cur is rewritten by the next group's decode; slot cur ^ 1 is ready
     }
 }
 
@@ -390,15 +496,16 @@ void launch_resample(Handle& h, void* scratch, const float* src, uint32_t srcStr
     launch_ragged_prefix(ResampleCount{inRate, outRate, dims, downmix, nullptr, 0.f}, n, prefix, h.stream());
     ResampleWindowDev w = win;
     resample_pads(w);
-    const bool pairs = w.padLeft >= 0 && resample_smem_floats(w, true) * sizeof(float) <= kPairTableLimit;
-    const size_t smem = resample_smem_floats(w, pairs) * sizeof(float);
+    const bool pairs = w.padLeft >= 0 && resample_smem_floats(w, true, downmix) * sizeof(float) <= kPairTableLimit;
+    const size_t smem = resample_smem_floats(w, pairs, downmix) * sizeof(float);
+    const bool magic = resample_magic_ok(w, pairs);
+    const bool fma = resample_scale_pow2(w);
+    resample_exact_range(w, magic, fma);
     auto go = [&](auto kernel) {
         const int grid = persistent_grid(h, reinterpret_cast<const void*>(kernel), kThreads, smem);
         kernel<<<grid, kThreads, smem, h.stream()>>>(src, srcStride, dst, dstStride, inRate, outRate, dims, w,
                                                      normalize, prefix, n, nullptr, 0.f);
     };
-    const bool magic = resample_magic_ok(w, pairs);
-    const bool fma = resample_scale_pow2(w);
     if (downmix && magic && fma) go(resample_kernel<true, false, true, true, true>);
     else if (downmix && magic) go(resample_kernel<true, false, true, true>);
     else if (downmix && pairs) go(resample_kernel<true, false, true>);
@@ -419,15 +526,18 @@ void launch_resample_clips(Handle& h, void* scratch, const RppbClip* clips, int 
     launch_ragged_prefix(ResampleCount{nullptr, nullptr, nullptr, false, clips, outRate}, n, prefix, h.stream());
     ResampleWindowDev w = win;
     resample_pads(w);
-    const bool pairs = w.padLeft >= 0 && resample_smem_floats(w, true) * sizeof(float) <= kPairTableLimit;
-    const size_t smem = resample_smem_floats(w, pairs) * sizeof(float);
+    const bool pairs = w.padLeft >= 0 && resample_smem_floats(w, true, false) * sizeof(float) <= kPairTableLimit;
+    const size_t smem = resample_smem_floats(w, pairs, false) * sizeof(float);
+    const bool magic = resample_magic_ok(w, pairs);
+    const bool fma = resample_scale_pow2(w);
+    resample_exact_range(w, magic, fma);
     auto go = [&](auto kernel) {
         const int grid = persistent_grid(h, reinterpret_cast<const void*>(kernel), kThreads, smem);
         kernel<<<grid, kThreads, smem, h.stream()>>>(nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, w, false,
                                                      prefix, n, clips, outRate);
     };
-    if (resample_magic_ok(w, pairs) && resample_scale_pow2(w)) go(resample_kernel<false, true, true, true, true>);
-    else if (resample_magic_ok(w, pairs)) go(resample_kernel<false, true, true, true>);
+    if (magic && fma) go(resample_kernel<false, true, true, true, true>);
+    else if (magic) go(resample_kernel<false, true, true, true>);
     else if (pairs) go(resample_kernel<false, true, true>);
     else go(resample_kernel<false, true, false>);
     count_launch();

@@ -125,6 +125,42 @@ def test_resample(gpu, oracle, rates, channels):
     np.testing.assert_array_equal(host(out), ref)
 
 
+@pytest.mark.parametrize("coeffs,lobes", [(8 * 64 + 1, 8), (24 * 64 + 1, 24), (16 * 48 + 1, 16), (16 * 128 + 1, 16)])
+@pytest.mark.parametrize("rates", [(48000, 16000), (22050, 16000), (16000, 44100)])
+def test_resample_windows(gpu, oracle, coeffs, lobes, rates):
+    """Tables of scale 32 with 8 and 24 lobes take the exact walk from phase 16 and 32 on; scale 24 (not a
+    power of two) and scale 64 (a power of two other than 32) never do.  Bit-exact either way, on mono and
+    down-mixed stereo input."""
+    r = rng(23 + lobes)
+    n, L = 3, 12000
+    lens = np.array([L, 5003, 700], np.int32)
+    lut, scale, center, lobes = oracle.windowed_sinc(coeffs, lobes)
+    ir = np.full(n, rates[0], np.float32)
+    orr = np.full(n, rates[1], np.float32)
+    out_len = int(np.ceil(L * rates[1] / rates[0])) + 8
+    lut_d = dev(lut)
+    win = audio.resampling_window(lut_d, scale, center, lobes)
+    x = r.normal(0, 0.3, (n, L)).astype(np.float32)
+    dims = np.stack([lens, np.ones(n, np.int32)], 1).astype(np.int32)
+    ref = np.full((n, out_len), -12345.0, np.float32)
+    oracle.resample(x, ref, ir, orr, dims.ravel(), lut, scale, center, lobes)
+    out = canvas(ref.shape)
+    assert audio.resample(dev(x), audio_desc(n, L), out, audio_desc(n, out_len), dev(ir), dev(orr), dev(dims), win,
+                          gpu) == OK
+    np.testing.assert_array_equal(host(out), ref)
+    # the same mono signal as two equal channels, down-mixed on the fly: the channel mean is the signal
+    x2 = np.repeat(x, 2, axis=1)
+    dims2 = np.stack([lens, np.full(n, 2, np.int32)], 1).astype(np.int32)
+    mono = np.full((n, L), 0.0, np.float32)
+    oracle.down_mixing(x2, mono, dims2.ravel(), False)
+    ref2 = np.full((n, out_len), -12345.0, np.float32)
+    oracle.resample(mono, ref2, ir, orr, dims.ravel(), lut, scale, center, lobes)
+    out2 = canvas(ref2.shape)
+    assert audio.downmix_resample(dev(x2), audio_desc(n, L, channels=2, num_dims=3), out2, audio_desc(n, out_len),
+                                  dev(ir), dev(orr), dev(dims2), False, lut_d, scale, center, lobes, gpu) == OK
+    np.testing.assert_array_equal(host(out2), ref2)
+
+
 def test_resample_golden(gpu, oracle, golden):
     lens = golden["lengths"].astype(np.int32)
     d = audio_desc(3, int(lens.max()), pad_to_8=True)
