@@ -215,6 +215,19 @@ SHARED_PUBLIC RppStatus rppb_set_wait_fault_injection(rppHandle_t rppHandle, boo
  * the same bits), e.g. to test it.  Off by default; affects only this handle. */
 SHARED_PUBLIC RppStatus rppb_set_tc_materialized_frames(rppHandle_t rppHandle, bool materialize);
 
+/* Bounds-checked build (librppb_checked.so, built with `python -m rpp_b200.build --checked`); no
+ * counterpart in the reference.  In that library every global load and store of the kernels is checked
+ * against the device regions of the call that launched it: the caller's tensors as their descriptors
+ * describe them, the per-sample tensors, the handle's workspace and tables.  An access outside them is
+ * skipped (loads read a dummy, stores write one), and the call returns RPP_ERROR_OUT_OF_BOUND_SRC_ROI
+ * for a stray read or RPP_ERROR_INSUFFICIENT_DST_BUFFER_LENGTH for a stray write, with the file, line,
+ * address and count in rppbGetLastError().  Calls run one at a time and synchronize their stream at
+ * the end (a captured call's record is read by the next uncaptured one).  This test hook registers the
+ * next call's destination tensor `bytes` shorter than its descriptor says, so that the call's last
+ * in-bounds stores are reported (and skipped) as out of bounds.  It returns RPP_ERROR_NOT_IMPLEMENTED
+ * in the ordinary library. */
+SHARED_PUBLIC RppStatus rppb_check_shrink_next_destination(Rpp64u bytes);
+
 #ifdef __cplusplus
 }
 #endif

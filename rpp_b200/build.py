@@ -4,7 +4,12 @@ Each rpp_b200/csrc/*.cu file is compiled to an object in rpp_b200/_build/ (in pa
 it or a header changed) and linked into an in-tree shared library with the CUDA runtime linked
 statically, so the library loads next to any PyTorch/CUDA runtime in the process.
 
-    python -m rpp_b200.build [--verbose-ptxas]
+--checked builds rpp_b200/librppb_checked.so instead (objects in rpp_b200/_build_checked/): the same
+sources with -DRPPB_CHECKED and relocatable device code, in which every global access of the kernels
+is checked against the regions of the call that launched it (rpp_b200/csrc/check.cu).  Load it with
+RPPB_LIBRARY=checked (rpp_b200/lib.py).
+
+    python -m rpp_b200.build [--verbose-ptxas] [--checked]
 """
 import concurrent.futures as cf
 import glob
@@ -18,6 +23,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librppb.so")
+OBJ_CHECKED = os.path.join(HERE, "_build_checked")
+LIB_CHECKED = os.path.join(HERE, "librppb_checked.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -28,9 +35,11 @@ def nvcc():
     raise FileNotFoundError("nvcc not found")
 
 
-def _flags(ptxas_verbose=False):
+def _flags(ptxas_verbose=False, checked=False):
     f = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
                 "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "--expt-relaxed-constexpr"]
+    if checked:
+        f += ["-DRPPB_CHECKED", "-rdc=true"]
     if ptxas_verbose:
         f += ["-Xptxas", "-v"]
     return f
@@ -42,18 +51,21 @@ def _newest_header():
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 
-def build(force=False, ptxas_verbose=False, jobs=None):
-    os.makedirs(OBJ, exist_ok=True)
+def build(force=False, ptxas_verbose=False, jobs=None, checked=False):
+    objdir, lib = (OBJ_CHECKED, LIB_CHECKED) if checked else (OBJ, LIB)
+    os.makedirs(objdir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdr = _newest_header()
     cc = nvcc()
-    flags = _flags(ptxas_verbose)
+    flags = _flags(ptxas_verbose, checked)
 
     def one(src):
-        obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
         if not force and os.path.isfile(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr):
             return obj, ""
-        r = subprocess.run([cc] + flags + ["-c", src, "-o", obj], capture_output=True, text=True)
+        # the checked build's access check is called from kernels launched with as few as 32 registers
+        extra = ["-maxrregcount=32"] if checked and os.path.basename(src) == "check.cu" else []
+        r = subprocess.run([cc] + flags + extra + ["-c", src, "-o", obj], capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src}:\n{r.stderr}")
         return obj, r.stderr
@@ -62,18 +74,19 @@ def build(force=False, ptxas_verbose=False, jobs=None):
         results = list(ex.map(one, srcs))
     objs = [o for o, _ in results]
     logs = "".join(l for _, l in results)
-    if force or not os.path.isfile(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        r = subprocess.run([cc] + ARCH + ["-shared", "-cudart", "static", "-o", LIB + ".tmp"] + objs,
+    if force or not os.path.isfile(lib) or os.path.getmtime(lib) < max(os.path.getmtime(o) for o in objs):
+        link = ["-rdc=true"] if checked else []
+        r = subprocess.run([cc] + ARCH + link + ["-shared", "-cudart", "static", "-o", lib + ".tmp"] + objs,
                            capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
-        os.replace(LIB + ".tmp", LIB)
-    return LIB, logs
+        os.replace(lib + ".tmp", lib)
+    return lib, logs
 
 
 if __name__ == "__main__":
     v = "--verbose-ptxas" in sys.argv
-    lib, logs = build(force="--force" in sys.argv or v, ptxas_verbose=v)
+    lib, logs = build(force="--force" in sys.argv or v, ptxas_verbose=v, checked="--checked" in sys.argv)
     if v:
         print(logs)
     print(lib)

@@ -11,6 +11,47 @@ namespace rppb {
 void count_launch(int kernels);
 void check_cuda(cudaError_t err, const char* what);
 
+// ---------------------------------------------------------------- checked build
+// Every global load and store of the kernels names its address through RPPB_RD / RPPB_WR.  In the
+// library these expand to the address itself.  Built with -DRPPB_CHECKED (librppb_checked.so,
+// `python -m rpp_b200.build --checked`), each access is first compared with the device regions the
+// current call may touch (check.cu): the caller's tensors as their descriptors describe them, the
+// per-sample tensors, the workspace and the handle's tables.  An access outside them is recorded
+// (site, address, size; the first one of the call) and redirected to a dummy buffer, so it neither
+// reads nor writes out of bounds, and the call returns a status code for it.
+constexpr unsigned check_file_hash(const char* path)
+{
+    const char* base = path;
+    for (const char* q = path; *q; ++q)
+        if (*q == '/') base = q + 1;
+    unsigned h = 2166136261u;   // FNV-1a of the file's base name
+    for (; *base; ++base) h = (h ^ static_cast<unsigned char>(*base)) * 16777619u;
+    return h & 0xffffu;
+}
+template <unsigned kV>
+struct CheckConst
+{
+    static constexpr unsigned value = kV;
+};
+#define RPPB_SITE ((::rppb::CheckConst<::rppb::check_file_hash(__FILE__)>::value << 16) | (__LINE__ & 0xffff))
+#ifdef RPPB_CHECKED
+__device__ void* check_addr(const void* p, unsigned bytes, bool write, unsigned site);
+template <class T>
+__device__ __forceinline__ T* check_ptr(T* p, bool write, unsigned site)
+{
+    return static_cast<T*>(check_addr(p, unsigned(sizeof(T)), write, site));
+}
+// a range of `bytes` (bulk copies, prefetches): true when it lies inside one region
+__device__ bool check_range(const void* p, unsigned long long bytes, bool write, unsigned site);
+#define RPPB_RD(p) ::rppb::check_ptr((p), false, RPPB_SITE)
+#define RPPB_WR(p) ::rppb::check_ptr((p), true, RPPB_SITE)
+#define RPPB_RANGE_OK(p, bytes) ::rppb::check_range((p), (bytes), false, RPPB_SITE)
+#else
+#define RPPB_RD(p) (p)
+#define RPPB_WR(p) (p)
+#define RPPB_RANGE_OK(p, bytes) true
+#endif
+
 // ---------------------------------------------------------------- ragged batches
 // A batch of uneven samples is addressed as one flat list of work units (chunks, frame tiles,
 // reset blocks ...).  prefix[b] is the number of units of samples 0..b-1 (prefix[n] = total),
@@ -24,7 +65,7 @@ __device__ __forceinline__ int ragged_find(const long long* prefix, int n, long 
     while (lo < hi)
     {
         int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= w) lo = mid;
+        if (*RPPB_RD(prefix + mid) <= w) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -42,7 +83,7 @@ __device__ __forceinline__ const long long* cache_prefix(const long long* prefix
         __syncthreads();
         return prefix;
     }
-    for (int i = threadIdx.x; i <= n; i += blockDim.x) s_cache[i] = prefix[i];
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) s_cache[i] = *RPPB_RD(prefix + i);
     __syncthreads();
     return s_cache;
 }
@@ -56,7 +97,7 @@ __global__ void __launch_bounds__(1024) ragged_prefix_kernel(Count count, int n,
                                                              unsigned* __restrict__ zero, int zeroWords)
 {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    for (int i = threadIdx.x; i < zeroWords; i += 1024) zero[i] = 0u;
+    for (int i = threadIdx.x; i < zeroWords; i += 1024) *RPPB_WR(zero + i) = 0u;
     __shared__ long long part[1024];
     const int t = threadIdx.x;
     const int per = (n + 1023) / 1024;
@@ -75,10 +116,10 @@ __global__ void __launch_bounds__(1024) ragged_prefix_kernel(Count count, int n,
     long long run = t ? part[t - 1] : 0;
     for (int b = b0; b < b1; ++b)
     {
-        prefix[b] = run;
+        *RPPB_WR(prefix + b) = run;
         run += count(b);
     }
-    if (t == 1023) prefix[n] = part[1023];
+    if (t == 1023) *RPPB_WR(prefix + n) = part[1023];
 }
 
 template <class Count>
@@ -125,6 +166,7 @@ __device__ __forceinline__ void l2_prefetch(const float* begin, const float* end
     if (e <= b) return;
     const uintptr_t n = e - b;
     const uint32_t bytes = n < (uintptr_t(1) << 20) ? uint32_t(n) : (1u << 20);
+    if (!RPPB_RANGE_OK(reinterpret_cast<const void*>(b), bytes)) return;
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"(bytes) : "memory");
 }
 

@@ -21,6 +21,7 @@
 #include "../../include/rppt_tensor_audio_augmentations.h"
 #include "../../include/rppt_tensor_geometric_augmentations.h"
 #include "../../include/rppt_tensor_statistical_operations.h"
+#include "common.cuh"
 #include "handle.hpp"
 #include "ops.hpp"
 
@@ -32,31 +33,54 @@ namespace {
 
 thread_local std::string g_last_error;
 
+// Runs an entry point's body on its handle and turns exceptions into status codes.  In the checked build
+// (check.cu) calls run one at a time, and a call's end reads its access record.
 template <class F>
 RppStatus guarded(rppHandle_t handle, F&& body)
 {
+#ifdef RPPB_CHECKED
+    std::lock_guard<std::recursive_mutex> lk(check_mutex());
+#endif
+    Handle* hp = nullptr;
+    auto abandon = [&](RppStatus st) {
+#ifdef RPPB_CHECKED
+        if (hp)
+            try
+            {
+                hp->check_end(st);
+            }
+            catch (...)
+            {
+            }
+#endif
+        return st;
+    };
     try
     {
         Handle& h = deref(handle);
+        hp = &h;
         h.begin_call();
+        h.check_begin();
         RppStatus st = body(h);
+        hp = nullptr;
+        st = h.check_end(st);
         if (st == RPP_SUCCESS) h.end_call();
         return st;
     }
     catch (const Error& e)
     {
         g_last_error = e.what;
-        return e.status;
+        return abandon(e.status);
     }
     catch (const std::bad_alloc&)
     {
         g_last_error = "host allocation failed";
-        return RPP_ERROR_NOT_ENOUGH_MEMORY;
+        return abandon(RPP_ERROR_NOT_ENOUGH_MEMORY);
     }
     catch (...)
     {
         g_last_error = "unknown error";
-        return RPP_ERROR;
+        return abandon(RPP_ERROR);
     }
 }
 
@@ -65,6 +89,23 @@ inline bool is_f32(const RpptDesc* d) { return d->dataType == F32; }
 void require(bool cond, const char* what)
 {
     if (!cond) fail(RPP_ERROR_INVALID_ARGUMENTS, what);
+}
+
+// The bytes of a caller's tensor as its descriptor describes it (checked build: the regions of a call).
+size_t elem_bytes(int dataType) { return dataType == F32 ? 4 : (dataType == F16 || dataType == I16) ? 2 : 1; }
+size_t desc_bytes(const RpptDesc* d, int n)
+{
+    return size_t(d->offsetInBytes) + size_t(n) * d->strides.nStride * elem_bytes(d->dataType);
+}
+size_t desc_bytes(const RpptGenericDesc& d, int n)
+{
+    return size_t(d.offsetInBytes) + size_t(n) * d.strides[0] * elem_bytes(d.dataType);
+}
+template <class D>
+void check_tensors(Handle& h, const void* src, const D& sd, const void* dst, const D& dd, int n)
+{
+    h.check_add(src, desc_bytes(sd, n), false);
+    if (dst) h.check_dst(dst, desc_bytes(dd, n));
 }
 
 void build_hann(float* out, size_t count, const void*)
@@ -104,6 +145,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_pre_emphasis_filter_gpu(RppPtr_t srcPtr,
         void* scratch = cv.take<char>(prefix_bytes(n));
         const int* len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
         const float* coeff = static_cast<const float*>(h.device_view(coeffTensor, n * sizeof(float), coeffStage));
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_pre_emphasis(h, scratch, static_cast<const float*>(srcPtr), srcDescPtr->strides.nStride,
                             static_cast<float*>(dstPtr), dstDescPtr->strides.nStride, n, len, coeff, int(borderType),
                             size_t(n) * srcDescPtr->strides.nStride);
@@ -130,6 +172,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_down_mixing_gpu(RppPtr_t srcPtr, RpptDes
         int* dimsStage = cv.take<int>(2 * n);
         void* scratch = cv.take<char>(prefix_bytes(n));
         const int* dims = static_cast<const int*>(h.device_view(srcDimsTensor, 2 * n * sizeof(int), dimsStage));
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_down_mixing(h, scratch, static_cast<const float*>(srcPtr), srcDescPtr->strides.nStride,
                            static_cast<float*>(dstPtr), dstDescPtr->strides.nStride, n, dims, normalizeWeights);
         return RPP_SUCCESS;
@@ -173,6 +216,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_to_decibels_gpu(RppPtr_t srcPtr, RpptDes
         a.minRatio = minRatio;
         a.multiplier = multiplier;
         a.referenceMagnitude = referenceMagnitude;
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_to_decibels(h, scratch, a);
         return RPP_SUCCESS;
     });
@@ -220,6 +264,9 @@ extern "C" SHARED_PUBLIC RppStatus rppt_non_silent_region_detection_gpu(RppPtr_t
         a.windowLength = windowLength;
         a.referencePower = referencePower;
         a.resetInterval = resetInterval;
+        check_tensors(h, srcPtr, srcDescPtr, static_cast<const void*>(nullptr), srcDescPtr, n);
+        if (directBegin) h.check_dst(a.begin, n * sizeof(int));
+        if (directLength) h.check_dst(a.length, n * sizeof(int));
         launch_nsr(h, scratch, a);
         if (!directBegin)
             check_cuda(cudaMemcpyAsync(detectedIndexTensor, outStage, n * sizeof(int), cudaMemcpyDeviceToHost,
@@ -291,6 +338,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_spectrogram_gpu(RppPtr_t srcPtr, RpptDes
         a.windowLength = windowLength;
         a.windowStep = windowStep;
         a.maxFrames = int(a.nft ? dstDescPtr->w : dstDescPtr->h);
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_spectrogram(h, scratch, a);
         return RPP_SUCCESS;
     });
@@ -338,6 +386,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_mel_filter_bank_gpu(RppPtr_t srcPtr, Rpp
         a.numFilter = numFilter;
         a.sampleRate = sampleRate;
         a.normalize = normalize;
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_mel_filter_bank(h, scratch, a);
         return RPP_SUCCESS;
     });
@@ -378,6 +427,7 @@ RppStatus resample_common(Handle& h, RppPtr_t srcPtr, RpptDescPtr srcDescPtr, Rp
     win.scale = scale;
     win.center = center;
     win.lobes = lobes;
+    check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
     launch_resample(h, scratch, static_cast<const float*>(srcPtr), srcDescPtr->strides.nStride,
                     static_cast<float*>(dstPtr), dstDescPtr->strides.nStride, n,
                     static_cast<const float*>(h.device_view(inRateTensor, n * sizeof(float), inStage)),
@@ -522,6 +572,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_gpu(RppPtr_t srcPtr, RpptDescPt
         a.len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
         a.coeff = static_cast<const float*>(h.device_view(coeffTensor, n * sizeof(float), coeffStage));
         a.maxFrames = int(dstDescPtr->w);
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_frontend(h, scratch, a);
         return RPP_SUCCESS;
     });
@@ -631,6 +682,8 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost,
         const bool gatherK = h.device_writable(srcHost, &srcMapped);
         const bool scatterK = h.device_writable(dstHost, &dstMapped);
         if (gatherK || scatterK) a.reserveSms = kReservedSms;   // room for the movers next to the persistent kernel
+        if (gatherK) h.check_add(srcMapped, desc_bytes(srcDescPtr, n), false);
+        if (scatterK) h.check_dst(dstMapped, desc_bytes(dstDescPtr, n));
 
         cudaStream_t main = h.stream(), up = h.aux_stream(0), down = h.aux_stream(1);
         cudaEvent_t start = h.event(0);
@@ -735,6 +788,26 @@ RppStatus frontend_clips(Handle& h, const RppbClip* clips, int numClips, float o
         win.scale = scale;
         win.center = center;
         win.lobes = lobes;
+#ifdef RPPB_CHECKED
+        // the clips' buffers, as the table describes them (read back here; a captured call is not checked)
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        check_cuda(cudaStreamIsCapturing(h.stream(), &cap), "cudaStreamIsCapturing");
+        if (cap == cudaStreamCaptureStatusNone)
+        {
+            std::vector<RppbClip> hc(n);
+            check_cuda(cudaMemcpy(hc.data(), clips, n * sizeof(RppbClip), cudaMemcpyDefault), "read clip table");
+            for (const RppbClip& c : hc)
+            {
+                if (c.length <= 0) continue;
+                h.check_add(c.src, size_t(c.length) * sizeof(float), false);
+                h.check_add(c.work, size_t(std::max(resampled_length(c.length, c.inRate, outRate), 0)) * sizeof(float),
+                            true);
+                h.check_dst(c.dst, size_t(params->numFilter) * size_t(std::max(c.dstStride, 0)) * sizeof(float));
+            }
+        }
+        else
+            h.check_suspend();
+#endif
         launch_resample_clips(h, resampleScratch, dclips, n, outRate, win);
         a.src = nullptr;
         a.srcStride = 0;
@@ -880,6 +953,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_spectrogram_tc_gpu(RppPtr_t srcPtr, Rppt
         a.nft = nft;
         a.power = power;
         a.n = n;
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_tc_spectrogram(h, scratch, a);
         return RPP_SUCCESS;
     });
@@ -977,6 +1051,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_slice_gpu(RppPtr_t srcPtr, RpptGenericDe
         a.enablePadding = enablePadding;
         const void* fill = enablePadding ? h.device_view(fillValue, size_t(eb), fStage) : nullptr;
         const size_t off = sd.offsetInBytes, doff = dd.offsetInBytes;
+        check_tensors(h, srcPtr, sd, dstPtr, dd, n);
         launch_slice(h, a, static_cast<const char*>(srcPtr) + off, static_cast<char*>(dstPtr) + doff, fill);
         return RPP_SUCCESS;
     });
@@ -1311,6 +1386,7 @@ RppStatus normalize_nd(Handle& h, const void* srcPtr, const RpptGenericDesc& sd,
     if (compute & 2)
         check_cuda(cudaMemcpyAsync(invOut, stdDevTensor, perAll * 4, cudaMemcpyDefault, h.stream()),
                    "cudaMemcpyAsync(stdDev in)");
+    check_tensors(h, srcPtr, sd, dstPtr, dd, n);
     launch_normalize_nd(h, a, dTasks, int(tasks.size()), meanEff, invEff, compute == 0 ? 0 : maxSize, maxElems,
                         maxZero, stdIn, inverted, compute == 0 ? maxSize : 0);
     if (compute & 1)
@@ -1442,6 +1518,7 @@ extern "C" SHARED_PUBLIC RppStatus rppt_normalize_gpu(RppPtr_t srcPtr, RpptGener
         if (compute & 2)
             check_cuda(cudaMemcpyAsync(invOut, stdDevTensor, perAll * 4, cudaMemcpyDefault, h.stream()),
                        "cudaMemcpyAsync(stdDev in)");
+        check_tensors(h, srcPtr, sd, dstPtr, dd, n);
         launch_normalize(h, a, dTasks, int(tasks.size()), meanEff, invEff, compute == 0 ? 0 : maxSize, stdIn,
                          inverted, compute == 0 ? maxSize : 0);
         // computed statistics go back to the caller's arrays, as the reference writes them
@@ -1472,6 +1549,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_pcm16_to_f32_gpu(RppPtr_t srcPtr, RpptDe
         Carver cv(h.workspace(m.used()));
         int* lenStage = cv.take<int>(n);
         const int* len = static_cast<const int*>(h.device_view(srcLengthTensor, n * sizeof(int), lenStage));
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_pcm16(h, reinterpret_cast<const short*>(static_cast<const char*>(srcPtr) + srcDescPtr->offsetInBytes),
                      srcDescPtr->strides.nStride,
                      reinterpret_cast<float*>(static_cast<char*>(dstPtr) + dstDescPtr->offsetInBytes),
@@ -1530,6 +1608,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_mel_filter_bank_tc_gpu(RppPtr_t srcPtr, 
         a.dst = static_cast<float*>(dstPtr);
         a.dstNStride = dstDescPtr->strides.nStride;
         a.dstHStride = dstDescPtr->strides.hStride;
+        check_tensors(h, srcPtr, srcDescPtr, dstPtr, dstDescPtr, n);
         launch_tc_mel(h, scratch, a);
         return RPP_SUCCESS;
     });

@@ -26,7 +26,7 @@ struct DownmixCount
     const int* dims;
     __device__ long long operator()(int b) const
     {
-        int l = dims[2 * b];
+        int l = *RPPB_RD(dims + 2 * b);
         return l <= 0 ? 0 : (l + kChunk - 1) / kChunk;
     }
 };
@@ -43,13 +43,14 @@ __global__ void __launch_bounds__(kThreads) down_mixing_kernel(const float* __re
     {
         const int b = ragged_find(prefix, n, w);
         const int chunk = int(w - prefix[b]);
-        const int L = min(dims[2 * b], int(dstStride));   // stay inside dst
-        const int C = dims[2 * b + 1];
+        const int L = min(*RPPB_RD(dims + 2 * b), int(dstStride));   // stay inside dst
+        const int C = *RPPB_RD(dims + (2 * b + 1));
         const float* x = src + size_t(b) * srcStride;
         float* y = dst + size_t(b) * dstStride;
         if (C <= 1)
         {
-            for (int t = chunk * kChunk + threadIdx.x; t < min(L, (chunk + 1) * kChunk); t += kThreads) y[t] = x[t];
+            for (int t = chunk * kChunk + threadIdx.x; t < min(L, (chunk + 1) * kChunk); t += kThreads)
+                *RPPB_WR(y + t) = *RPPB_RD(x + t);
             continue;
         }
         if (C > kMaxChannels) continue;   // rejected by the dispatch layer when it can see the dims
@@ -57,7 +58,7 @@ __global__ void __launch_bounds__(kThreads) down_mixing_kernel(const float* __re
         for (int t = chunk * kChunk + threadIdx.x; t < min(L, (chunk + 1) * kChunk); t += kThreads)
         {
             const float acc = mix(t);
-            y[t] = acc;
+            *RPPB_WR(y + t) = acc;
         }
     }
 }

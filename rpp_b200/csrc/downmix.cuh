@@ -8,6 +8,8 @@
 
 #include <cuda_runtime.h>
 
+#include "common.cuh"
+
 namespace rppb {
 
 struct MonoMix
@@ -28,19 +30,19 @@ struct MonoMix
 
     __device__ __forceinline__ float operator()(long long t) const
     {
-        if (C == 1) return __ldg(x + t);
+        if (C == 1) return __ldg(RPPB_RD(x + t));
         const float* xs = x + t * C;
         if (C == 2)   // fewer than 4 channels: the SIMD part sums nothing
-            return __fadd_rn(__fadd_rn(0.f, __fmul_rn(__ldg(xs), wc)), __fmul_rn(__ldg(xs + 1), wc));
+            return __fadd_rn(__fadd_rn(0.f, __fmul_rn(__ldg(RPPB_RD(xs)), wc)), __fmul_rn(__ldg(RPPB_RD(xs + 1)), wc));
         const int lanes = C > 7 ? 8 : 4;
         const int aligned = (C / lanes) * lanes;
         float p[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         for (int g = 0; g < aligned; g += lanes)
-            for (int l = 0; l < lanes; ++l) p[l] = __fadd_rn(p[l], __fmul_rn(__ldg(xs + g + l), wc));
+            for (int l = 0; l < lanes; ++l) p[l] = __fadd_rn(p[l], __fmul_rn(__ldg(RPPB_RD(xs + g + l)), wc));
         float acc = lanes == 8 ? __fadd_rn(__fadd_rn(__fadd_rn(p[0], p[4]), __fadd_rn(p[2], p[6])),
                                            __fadd_rn(__fadd_rn(p[1], p[5]), __fadd_rn(p[3], p[7])))
                                : __fadd_rn(__fadd_rn(p[0], p[1]), __fadd_rn(p[2], p[3]));
-        for (int c = aligned; c < C; ++c) acc = __fadd_rn(acc, __fmul_rn(__ldg(xs + c), wc));
+        for (int c = aligned; c < C; ++c) acc = __fadd_rn(acc, __fmul_rn(__ldg(RPPB_RD(xs + c)), wc));
         return acc;
     }
 };

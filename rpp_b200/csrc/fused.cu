@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         if (melTables)
         {
             uint4* t = reinterpret_cast<uint4*>(smem + lay.melW);
-            for (int i = threadIdx.x; i < int((lay.total - lay.melW) / 16); i += kFusedThreads) t[i] = __ldg(melTables + i);
+            for (int i = threadIdx.x; i < int((lay.total - lay.melW) / 16); i += kFusedThreads) t[i] = __ldg(RPPB_RD(melTables + i));
             __syncthreads();
         }
         else
@@ -108,9 +108,9 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
     int cur = 0;
     if (threadIdx.x == 0)
     {
-        const long long w0 = (long long)atomicAdd(workCounter, 1ull);
-        const long long w1 = (long long)atomicAdd(workCounter, 1ull);
-        wAfter = w1 < total - 2ll * gridDim.x ? (long long)atomicAdd(workCounter, 1ull) : -1ll;
+        const long long w0 = (long long)atomicAdd(RPPB_WR(workCounter), 1ull);
+        const long long w1 = (long long)atomicAdd(RPPB_WR(workCounter), 1ull);
+        wAfter = w1 < total - 2ll * gridDim.x ? (long long)atomicAdd(RPPB_WR(workCounter), 1ull) : -1ll;
         s_it[0] = decode_item<TF>(a, cnt, prefix, nslots, total, w0);
         s_it[1] = decode_item<TF>(a, cnt, prefix, nslots, total, w1);
         prefetch_span(s_it[1]);
@@ -163,11 +163,11 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                         }
                         if (i > m0)
                         {
-                            yp[0] = fall.x;
+                            *RPPB_WR(yp) = fall.x;
                             tmax = fmaxf(tmax, fall.x);
                             if (second)
                             {
-                                yp[1] = fall.y;
+                                *RPPB_WR(yp + 1) = fall.y;
                                 tmax = fmaxf(tmax, fall.y);
                             }
                             yp += hs;
@@ -186,11 +186,11 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 const int need = cnt.tiles(b) + a.waitExtra;
                 const long long limit = a.waitLimit > 0 ? a.waitLimit : kWaitLimit;
                 long long spins = 0;
-                while (atomicAdd(done + b, 0) < need)
+                while (atomicAdd(RPPB_WR(done + b), 0) < need)
                 {
                     if (++spins > limit)
                     {
-                        atomicOr(errorWord, 1);
+                        atomicOr(RPPB_WR(errorWord), 1);
                         break;
                     }
                     __nanosleep(128);
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                 float ref = a.refMag;
                 if (a.refMag == 0.f)
                 {
-                    const unsigned k = __ldcg(maxKey + b);
+                    const unsigned k = __ldcg(RPPB_RD(maxKey + b));
                     ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
                 }
                 const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
@@ -222,20 +222,20 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
                     {
                         float v[kRows];
 #pragma unroll
-                        for (int r = 0; r < kRows; ++r) v[r] = __ldcg(p + r * step);
+                        for (int r = 0; r < kRows; ++r) v[r] = __ldcg(RPPB_RD(p + r * step));
 #pragma unroll
                         for (int r = 0; r < kRows; ++r)
                         {
                             float t = __fmul_rn(v[r], inv);
                             t = a.minRatio < t ? t : a.minRatio;
-                            p[r * step] = __fmul_rn(a.multiplier, __log2f(t));
+                            *RPPB_WR(p + r * step) = __fmul_rn(a.multiplier, __log2f(t));
                         }
                     }
                     for (; m < nmel; m += kDbGroups, p += step)
                     {
-                        float t = __fmul_rn(__ldcg(p), inv);
+                        float t = __fmul_rn(__ldcg(RPPB_RD(p)), inv);
                         t = a.minRatio < t ? t : a.minRatio;
-                        *p = __fmul_rn(a.multiplier, __log2f(t));
+                        *RPPB_WR(p) = __fmul_rn(a.multiplier, __log2f(t));
                     }
                 }
             }
@@ -251,8 +251,8 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
         {
             // the last 2 x grid items are claimed when needed, not reserved ahead, so that no CTA
             // holds work that an idle one could start (small batches: 0.039 -> 0.033 ms for one 1 s clip)
-            const long long w = wAfter >= 0 ? wAfter : (long long)atomicAdd(workCounter, 1ull);
-            wAfter = w < total - 2ll * gridDim.x ? (long long)atomicAdd(workCounter, 1ull) : -1ll;
+            const long long w = wAfter >= 0 ? wAfter : (long long)atomicAdd(RPPB_WR(workCounter), 1ull);
+            wAfter = w < total - 2ll * gridDim.x ? (long long)atomicAdd(RPPB_WR(workCounter), 1ull) : -1ll;
             const Item nx = decode_item<TF>(a, cnt, prefix, nslots, total, w);
             prefetch_span(nx);
             s_it[cur] = nx;
@@ -263,8 +263,8 @@ __global__ void __launch_bounds__(kFusedThreads, (NFFT <= 512 ? 3 : 2)) frontend
             // orders them (and the maximum) before the count
             float v = s_warpMax[0];
             for (int i = 1; i < kFusedThreads / 32; ++i) v = fmaxf(v, s_warpMax[i]);
-            atomicMax(maxKey + b, float_key(v));
-            asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(done + b) : "memory");
+            atomicMax(RPPB_WR(maxKey + b), float_key(v));
+            asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(RPPB_WR(done + b)) : "memory");
         }
         cur ^= 1;
     }

@@ -46,12 +46,12 @@ __device__ __forceinline__ ClipView clip_view(const FrontendArgs& a, int b)
 {
     if (a.clips)
     {
-        const RppbClip c = a.clips[b];
+        const RppbClip c = *RPPB_RD(a.clips + b);
         const int L = c.length <= 0 ? 0 : resampled_length(c.length, c.inRate, a.outRate);
         return {c.work, L, c.dst, uint32_t(c.dstStride), c.dstStride, a.coeffAll, L >= 2};
     }
-    return {a.src + size_t(b) * a.srcStride, a.len[b], a.dst + size_t(b) * a.dstNStride, a.dstHStride, a.maxFrames,
-            a.coeff[b], size_t(b) * a.srcStride + 1 < a.srcElems};
+    return {a.src + size_t(b) * a.srcStride, *RPPB_RD(a.len + b), a.dst + size_t(b) * a.dstNStride, a.dstHStride,
+            a.maxFrames, *RPPB_RD(a.coeff + b), size_t(b) * a.srcStride + 1 < a.srcElems};
 }
 
 template <int TF>
@@ -115,8 +115,8 @@ __device__ Item decode_item(const FrontendArgs& a, const SlotCount<TF>& cnt, con
     it.hs = cv.hStride;
     it.coeff = cv.coeff;
     it.bval = 0.f;
-    if (spectrumItem && a.border == 1) it.bval = cv.x[0];
-    else if (spectrumItem && a.border == 2 && cv.hasSecond) it.bval = cv.x[1];
+    if (spectrumItem && a.border == 1) it.bval = *RPPB_RD(cv.x);
+    else if (spectrumItem && a.border == 2 && cv.hasSecond) it.bval = *RPPB_RD(cv.x + 1);
     return it;
 }
 
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kFusedThreads) fused_mel_tables_kernel(Fronten
     const FusedLayout<NFFT, TFX> lay(a.mel.numFilter, a.W, a.hop);
     build_fused_mel<NFFT, TFX>(a, smem, lay);
     const uint4* src = reinterpret_cast<const uint4*>(smem + lay.melW);
-    for (int i = threadIdx.x; i < int((lay.total - lay.melW) / 16); i += kFusedThreads) out[i] = src[i];
+    for (int i = threadIdx.x; i < int((lay.total - lay.melW) / 16); i += kFusedThreads) *RPPB_WR(out + i) = src[i];
 }
 
 // The fused kernels' mel tables (the bytes [melW, total) of FusedLayout<NFFT, TFX>), built once per

@@ -71,6 +71,7 @@ Handle::Block Handle::block_alloc(size_t bytes)
 {
     Block b;
     b.p = dev_alloc(bytes);
+    b.bytes = bytes;
     b.custom = alloc_fn_ != nullptr;
     b.free_fn = free_fn_;
     b.ctx = alloc_ctx_;
@@ -104,6 +105,9 @@ void* Handle::workspace(size_t bytes)
     size_t grown = bytes + bytes / 4 + (1 << 20);
     ws_ = dev_alloc(grown);
     ws_bytes_ = grown;
+#ifdef RPPB_CHECKED
+    check_dirty_ = check_active_;
+#endif
     return ws_;
 }
 
@@ -169,9 +173,15 @@ const void* Handle::device_view(const void* p, size_t bytes, void* dst)
         attr.type = cudaMemoryTypeUnregistered;
     }
     if (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged)
+    {
+        check_add(p, bytes, false);
         return p;
+    }
     if (attr.type == cudaMemoryTypeHost && attr.devicePointer != nullptr)
+    {
+        check_add(attr.devicePointer, bytes, false);
         return attr.devicePointer;
+    }
     upload(dst, p, bytes);
     return dst;
 }
@@ -211,6 +221,9 @@ const float* Handle::table(const std::string& key, size_t count, void (*build)(f
     if (e != cudaSuccess) block_free(b);
     check_cuda(e, "cudaMemcpy(table)");
     tables_[key] = b;
+#ifdef RPPB_CHECKED
+    check_dirty_ = check_active_;
+#endif
     return static_cast<const float*>(b.p);
 }
 
@@ -225,6 +238,9 @@ void* Handle::device_table(const std::string& key, size_t bytes, bool* fresh)
     const Block b = block_alloc(bytes);
     tables_[key] = b;
     *fresh = true;
+#ifdef RPPB_CHECKED
+    check_dirty_ = check_active_;
+#endif
     return b.p;
 }
 
@@ -237,9 +253,71 @@ int* Handle::device_flags()
         if (e != cudaSuccess) block_free(b);
         check_cuda(e, "cudaMemset(flags)");
         flags_ = b;
+#ifdef RPPB_CHECKED
+        check_dirty_ = check_active_;
+#endif
     }
     return static_cast<int*>(flags_.p);
 }
+
+#ifdef RPPB_CHECKED
+void Handle::check_add(const void* p, size_t bytes, bool writable)
+{
+    if (!check_active_ || !p || !bytes) return;
+    check_spans_.push_back(CheckSpan{p, bytes, writable});
+    check_dirty_ = true;
+}
+
+void Handle::check_dst(const void* p, size_t bytes)
+{
+    const unsigned long long shrink = check_take_shrink();
+    check_add(p, shrink < bytes ? bytes - shrink : 0, true);
+}
+
+void Handle::check_flush() const
+{
+    std::vector<CheckSpan> spans = check_spans_;
+    if (ws_) spans.push_back(CheckSpan{ws_, ws_bytes_, true});
+    for (const auto& kv : tables_) spans.push_back(CheckSpan{kv.second.p, kv.second.bytes, true});
+    if (flags_.p) spans.push_back(CheckSpan{flags_.p, flags_.bytes, true});
+    check_dirty_ = false;
+    check_upload(stream_, true, spans);
+}
+
+void Handle::check_begin()
+{
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    check_cuda(cudaStreamIsCapturing(stream_, &cap), "cudaStreamIsCapturing");
+    if (cap == cudaStreamCaptureStatusNone)
+    {
+        // a record left by an earlier call that ended in an exception is not this call's
+        check_cuda(cudaStreamSynchronize(stream_), "cudaStreamSynchronize(check)");
+        check_reset();
+    }
+    check_spans_.clear();
+    check_active_ = true;
+    check_dirty_ = true;
+}
+
+void Handle::check_suspend()
+{
+    check_active_ = false;
+    check_dirty_ = false;
+    check_upload(stream_, false, {});
+}
+
+RppStatus Handle::check_end(RppStatus st)
+{
+    check_active_ = false;
+    check_dirty_ = false;
+    check_upload(stream_, false, {});
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    check_cuda(cudaStreamIsCapturing(stream_, &cap), "cudaStreamIsCapturing");
+    if (cap != cudaStreamCaptureStatusNone) return st;   // read by the next uncaptured call
+    check_cuda(cudaStreamSynchronize(stream_), "cudaStreamSynchronize(check)");
+    return check_collect(st);
+}
+#endif
 
 void Handle::set_allocator(rppAllocatorFunction a, rppDeallocatorFunction d, void* ctx)
 {

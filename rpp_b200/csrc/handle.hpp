@@ -32,6 +32,24 @@ struct Error
 void record_error(const std::string& what);
 void check_cuda(cudaError_t err, const char* what);
 
+// Checked build (RPPB_CHECKED, check.cu): a device region a call's kernels may touch.
+struct CheckSpan
+{
+    const void* p;
+    size_t bytes;
+    bool writable;
+};
+#ifdef RPPB_CHECKED
+std::recursive_mutex& check_mutex();
+// Uploads the table of `spans` (merged where they touch) on stream s; enabled = false switches checks off.
+void check_upload(cudaStream_t s, bool enabled, std::vector<CheckSpan> spans);
+// Reads and clears the violation record: st when there was none, else the violation's status code.
+RppStatus check_collect(RppStatus st);
+void check_reset();
+// The byte count rppb_check_shrink_next_destination set (0 when none), cleared by the read.
+unsigned long long check_take_shrink();
+#endif
+
 // Bump allocator over one workspace block: measure with base == nullptr, then carve.
 class Carver
 {
@@ -57,7 +75,16 @@ class Handle
     Handle(size_t batchSize, cudaStream_t stream);
     ~Handle();
 
+#ifdef RPPB_CHECKED
+    // uploads the call's region table first when it changed (check.cu)
+    cudaStream_t stream() const
+    {
+        if (check_dirty_) check_flush();
+        return stream_;
+    }
+#else
     cudaStream_t stream() const { return stream_; }
+#endif
     void set_stream(cudaStream_t s) { stream_ = s; }
     size_t batch_size() const { return batch_; }
     void set_batch_size(size_t b) { batch_ = b; }
@@ -105,6 +132,23 @@ class Handle
     void set_tc_materialize(bool on) { tc_materialize_ = on; }
     bool tc_materialize() const { return tc_materialize_; }
 
+    // Checked build: regions of the current call beyond the handle's own blocks (caller tensors,
+    // per-sample tensors, pinned host buffers); check_dst registers a caller's destination tensor.
+    // check_begin starts a call, check_end ends it and returns the status of any violation.
+#ifdef RPPB_CHECKED
+    void check_add(const void* p, size_t bytes, bool writable);
+    void check_dst(const void* p, size_t bytes);
+    void check_begin();
+    RppStatus check_end(RppStatus st);
+    // the rest of the call is not checked (its regions cannot be listed)
+    void check_suspend();
+#else
+    void check_add(const void*, size_t, bool) {}
+    void check_dst(const void*, size_t) {}
+    void check_begin() {}
+    RppStatus check_end(RppStatus st) { return st; }
+#endif
+
     // Extra streams of this handle (created on first use, non-blocking), for copies that overlap
     // the kernels on stream(); every call that uses them joins them back into stream() before it
     // returns, so stream order on stream() still covers all of the handle's work.
@@ -125,6 +169,7 @@ class Handle
         rppDeallocatorFunction free_fn = nullptr;
         void* ctx = nullptr;
         bool custom = false;
+        size_t bytes = 0;
     };
     void* dev_alloc(size_t bytes);
     void dev_free(void* p);
@@ -159,6 +204,13 @@ class Handle
     bool profiling_ = false;
     cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
     bool timed_ = false;
+
+#ifdef RPPB_CHECKED
+    void check_flush() const;
+    mutable std::vector<CheckSpan> check_spans_;
+    mutable bool check_dirty_ = false;
+    bool check_active_ = false;
+#endif
 };
 
 Handle& deref(rppHandle_t h);

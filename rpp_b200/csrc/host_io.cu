@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(kMoverThreads) host_gather_kernel(const float*
     for (long long u = blockIdx.x; u < units; u += gridDim.x)
     {
         const int b = int(u / segsPerClip), seg = int(u % segsPerClip);
-        const long long cnt = min(min((long long)nStride, (long long)max(len[b], 2)), (long long)dstStride);
+        const long long cnt = min(min((long long)nStride, (long long)max(*RPPB_RD(len + b), 2)), (long long)dstStride);
         const long long s0 = (long long)seg * kSegment;
         if (s0 >= cnt) continue;
         const int m = int(min((long long)kSegment, cnt - s0));
@@ -43,19 +43,19 @@ __global__ void __launch_bounds__(kMoverThreads) host_gather_kernel(const float*
             for (int k = 0; k < kUnroll; ++k)
             {
                 const int i = threadIdx.x + k * kMoverThreads;
-                if (i < q) v[k] = s4[i];
+                if (i < q) v[k] = *RPPB_RD(s4 + i);
             }
 #pragma unroll
             for (int k = 0; k < kUnroll; ++k)
             {
                 const int i = threadIdx.x + k * kMoverThreads;
-                if (i < q) d4[i] = v[k];
+                if (i < q) *RPPB_WR(d4 + i) = v[k];
             }
-            for (int i = (q << 2) + threadIdx.x; i < m; i += kMoverThreads) d[i] = s[i];
+            for (int i = (q << 2) + threadIdx.x; i < m; i += kMoverThreads) *RPPB_WR(d + i) = *RPPB_RD(s + i);
         }
         else
         {
-            for (int i = threadIdx.x; i < m; i += kMoverThreads) d[i] = s[i];
+            for (int i = threadIdx.x; i < m; i += kMoverThreads) *RPPB_WR(d + i) = *RPPB_RD(s + i);
         }
     }
 }
@@ -74,19 +74,20 @@ __global__ void __launch_bounds__(kMoverThreads) host_scatter_kernel(const float
     for (long long w = blockIdx.x * (long long)(kMoverThreads / 32) + (threadIdx.x >> 5); w < total; w += warps)
     {
         const int b = int(w / rows), r = int(w % rows);
-        const int F = frames[b];
+        const int F = *RPPB_RD(frames + b);
         const float* s = src + size_t(b) * srcNStride + size_t(r) * srcHStride;
         float* d = dst + size_t(b) * dstNStride + size_t(r) * dstHStride;
         int f = lane;
         for (; f + 96 < F; f += 128)
         {
-            const float v0 = s[f], v1 = s[f + 32], v2 = s[f + 64], v3 = s[f + 96];
-            d[f] = v0;
-            d[f + 32] = v1;
-            d[f + 64] = v2;
-            d[f + 96] = v3;
+            const float v0 = *RPPB_RD(s + f), v1 = *RPPB_RD(s + (f + 32)), v2 = *RPPB_RD(s + (f + 64)),
+                        v3 = *RPPB_RD(s + (f + 96));
+            *RPPB_WR(d + f) = v0;
+            *RPPB_WR(d + (f + 32)) = v1;
+            *RPPB_WR(d + (f + 64)) = v2;
+            *RPPB_WR(d + (f + 96)) = v3;
         }
-        for (; f < F; f += 32) d[f] = s[f];
+        for (; f < F; f += 32) *RPPB_WR(d + f) = *RPPB_RD(s + f);
     }
 }
 
@@ -104,10 +105,10 @@ __global__ void __launch_bounds__(kMoverThreads) copy_jobs_kernel(const CopyJob*
         while (lo < hi)
         {
             const int mid = (lo + hi + 1) >> 1;
-            if (jobs[mid].unit0 <= u) lo = mid;
+            if (RPPB_RD(jobs + mid)->unit0 <= u) lo = mid;
             else hi = mid - 1;
         }
-        const CopyJob jb = jobs[lo];
+        const CopyJob jb = *RPPB_RD(jobs + lo);
         const long long s0 = (u - jb.unit0) * kSegment;
         if (s0 >= jb.count) continue;
         const int m = int(min((long long)kSegment, jb.count - s0));
@@ -124,19 +125,19 @@ __global__ void __launch_bounds__(kMoverThreads) copy_jobs_kernel(const CopyJob*
             for (int k = 0; k < kUnroll; ++k)
             {
                 const int i = threadIdx.x + k * kMoverThreads;
-                if (i < q) v[k] = s4[i];
+                if (i < q) v[k] = *RPPB_RD(s4 + i);
             }
 #pragma unroll
             for (int k = 0; k < kUnroll; ++k)
             {
                 const int i = threadIdx.x + k * kMoverThreads;
-                if (i < q) d4[i] = v[k];
+                if (i < q) *RPPB_WR(d4 + i) = v[k];
             }
-            for (int i = (q << 2) + threadIdx.x; i < m; i += kMoverThreads) d[i] = s[i];
+            for (int i = (q << 2) + threadIdx.x; i < m; i += kMoverThreads) *RPPB_WR(d + i) = *RPPB_RD(s + i);
         }
         else
         {
-            for (int i = threadIdx.x; i < m; i += kMoverThreads) d[i] = s[i];
+            for (int i = threadIdx.x; i < m; i += kMoverThreads) *RPPB_WR(d + i) = *RPPB_RD(s + i);
         }
     }
 }

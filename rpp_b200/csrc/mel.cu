@@ -34,7 +34,7 @@ struct MelCount
     uint32_t dstHStride;
     __device__ long long operator()(int b) const
     {
-        long long frames = max(dims[2 * b + 1], 0);
+        long long frames = max(*RPPB_RD(dims + (2 * b + 1)), 0);
         long long cols = min(frames + 8, (long long)dstHStride);
         return (cols + kTile - 1) / kTile;
     }
@@ -156,8 +156,8 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
     {
         const int b = ragged_find(prefix, a.n, w);
         const int tile = int(w - prefix[b]);
-        const int bins = a.dims[2 * b];
-        const int frames = min(max(a.dims[2 * b + 1], 0), int(min(a.srcHStride, a.dstHStride)));
+        const int bins = *RPPB_RD(a.dims + 2 * b);
+        const int frames = min(max(*RPPB_RD(a.dims + (2 * b + 1)), 0), int(min(a.srcHStride, a.dstHStride)));
         const int nfft = (bins - 1) * 2;
         const bool ok = nfft >= 2 && bins <= maxBins && uint32_t(bins) <= a.srcRows;
         const int held = range[2];
@@ -188,11 +188,11 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
             {
                 float v[kBatch];
 #pragma unroll
-                for (int j = 0; j < kBatch; ++j, xs += rowStep) v[j] = colOk ? __ldg(xs) : 0.0f;
+                for (int j = 0; j < kBatch; ++j, xs += rowStep) v[j] = colOk ? __ldg(RPPB_RD(xs)) : 0.0f;
 #pragma unroll
                 for (int j = 0; j < kBatch; ++j, ss += kWarps * kLd) *ss = v[j];
             }
-            for (; r < rows; r += kWarps, xs += rowStep, ss += kWarps * kLd) *ss = colOk ? __ldg(xs) : 0.0f;
+            for (; r < rows; r += kWarps, xs += rowStep, ss += kWarps * kLd) *ss = colOk ? __ldg(RPPB_RD(xs)) : 0.0f;
         }
         __syncthreads();
         // one sweep over the group's intervals for frames t0 + t and t0 + t + 1; each power pair is
@@ -221,8 +221,8 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
                 }
                 if (i > m0)
                 {
-                    yp[0] = live0 ? fall.x : 0.0f;
-                    if (has1) yp[1] = live1 ? fall.y : 0.0f;
+                    *RPPB_WR(yp) = live0 ? fall.x : 0.0f;
+                    if (has1) *RPPB_WR(yp + 1) = live1 ? fall.y : 0.0f;
                     yp += a.dstHStride;
                 }
                 fall = rise;
@@ -231,8 +231,8 @@ __global__ void __launch_bounds__(kThreads) mel_kernel(MelArgs a, float maxFreq,
                 for (int m = g; m < a.numFilter; m += kGroups)
                 {
                     float* z = a.dst + size_t(b) * a.dstNStride + size_t(m) * a.dstHStride + col;
-                    z[0] = 0.0f;
-                    if (has1) z[1] = 0.0f;
+                    *RPPB_WR(z) = 0.0f;
+                    if (has1) *RPPB_WR(z + 1) = 0.0f;
                 }
         }
         __syncthreads();   // the next unit restages the tile and may rebuild the tables

@@ -47,7 +47,7 @@ __device__ float tree_sum(const float* in, int stride, int n, float mean)
     float t = 0.f;
     for (int i = 0; i < n; ++i)
     {
-        const float x = in[(long long)i * stride];
+        const float x = *RPPB_RD(in + (long long)i * stride);
         if (kSq)
         {
             const float c = __fsub_rn(x, mean);
@@ -96,9 +96,9 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormalizeArgs a, const 
     float* stage = s_stage[threadIdx.x >> 5];
     for (int t = (blockIdx.x * kThreads + threadIdx.x) >> 5; t < numTasks; t += warps)
     {
-        const int4 task = tasks[t];   // sample, first parameter, parameters, warp mode
+        const int4 task = *RPPB_RD(tasks + t);   // sample, first parameter, parameters, warp mode
         const int b = task.x;
-        const NormalizeSample s = a.samples[b];
+        const NormalizeSample s = *RPPB_RD(a.samples + b);
         const float* base = a.src + size_t(b) * a.srcStride0;
         auto one = [&](int p, bool warp) {
             const float* in = base + (long long)p * s.paramStride;
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormalizeArgs a, const 
             if (warp && es == 1 && s.count <= kStageElems)
             {
                 __syncwarp();   // the previous task's reads of the buffer are done
-                for (int k = lane; k < s.count; k += 32) stage[k] = __ldg(in + k);
+                for (int k = lane; k < s.count; k += 32) stage[k] = __ldg(RPPB_RD(in + k));
                 __syncwarp();
                 in = stage;
             }
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormalizeArgs a, const 
                 mean = __fmul_rn(sum, s.normFactor);
             }
             else
-                mean = a.meanIn[size_t(b) * a.maxSize + p];
+                mean = *RPPB_RD(a.meanIn + (size_t(b) * a.maxSize + p));
             float inv = 0.f;
             if (a.compute & 2)
             {
@@ -129,8 +129,8 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormalizeArgs a, const 
             }
             if (!warp || lane == 0)
             {
-                if (a.compute & 1) a.meanOut[size_t(b) * a.maxSize + p] = mean;
-                if (a.compute & 2) a.invOut[size_t(b) * a.maxSize + p] = inv;
+                if (a.compute & 1) *RPPB_WR(a.meanOut + (size_t(b) * a.maxSize + p)) = mean;
+                if (a.compute & 2) *RPPB_WR(a.invOut + (size_t(b) * a.maxSize + p)) = inv;
             }
         };
         if (task.w) one(task.y, true);
@@ -143,8 +143,8 @@ __global__ void __launch_bounds__(kThreads) invert_kernel(const float* __restric
 {
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < count; i += gridDim.x * kThreads)
     {
-        const float v = std[i];
-        inv[i] = v == 0.f ? 1.0f : __fdiv_rn(scale, v);
+        const float v = *RPPB_RD(std + i);
+        *RPPB_WR(inv + i) = v == 0.f ? 1.0f : __fdiv_rn(scale, v);
     }
 }
 
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(NormalizeArgs a, co
     {
         const int b = int(u / rowsPerSample);
         const uint32_t r = uint32_t(u - (long long)b * rowsPerSample);
-        const NormalizeSample s = a.samples[b];
+        const NormalizeSample s = *RPPB_RD(a.samples + b);
         const uint32_t rowBegin = r * a.dstStride1;
         const uint32_t rowLen = min(a.dstStride1, a.dstStride0 - rowBegin);
         float* d = a.dst + size_t(b) * a.dstStride0 + rowBegin;
@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(NormalizeArgs a, co
         if (rowIn && a.axisMask != 1)
         {
             const size_t q = q0 + (a.axisMask == 2 ? r : 0);
-            rowMean = mean[q];
-            rowInv = inv[q];
+            rowMean = *RPPB_RD(mean + q);
+            rowInv = *RPPB_RD(inv + q);
         }
         const uint32_t len1 = rowIn ? uint32_t(s.len1) : 0u;
         for (uint32_t c = 4 * threadIdx.x; c < rowLen; c += 4 * kThreads)
@@ -180,13 +180,13 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(NormalizeArgs a, co
             float xv[4] = {0.f, 0.f, 0.f, 0.f};
             if (c + 4 <= len1 && vecSrc)
             {
-                const float4 v = __ldg(reinterpret_cast<const float4*>(x + c));
+                const float4 v = __ldg(RPPB_RD(reinterpret_cast<const float4*>(x + c)));
                 xv[0] = v.x; xv[1] = v.y; xv[2] = v.z; xv[3] = v.w;
             }
             else
 #pragma unroll
                 for (int t = 0; t < 4; ++t)
-                    if (c + t < len1) xv[t] = __ldg(x + size_t(c + t) * a.srcStride2);
+                    if (c + t < len1) xv[t] = __ldg(RPPB_RD(x + size_t(c + t) * a.srcStride2));
             float ov[4];
 #pragma unroll
             for (int t = 0; t < 4; ++t)
@@ -194,17 +194,17 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(NormalizeArgs a, co
                 float m = rowMean, iv = rowInv;
                 if (a.axisMask == 1 && c + t < len1)
                 {
-                    m = mean[q0 + c + t];
-                    iv = inv[q0 + c + t];
+                    m = *RPPB_RD(mean + (q0 + c + t));
+                    iv = *RPPB_RD(inv + (q0 + c + t));
                 }
                 ov[t] = c + t < len1 ? __fadd_rn(__fmul_rn(__fsub_rn(xv[t], m), iv), a.shift) : 0.f;
             }
             if (c + 4 <= rowLen && vecDst)
-                *reinterpret_cast<float4*>(d + c) = make_float4(ov[0], ov[1], ov[2], ov[3]);
+                *RPPB_WR(reinterpret_cast<float4*>(d + c)) = make_float4(ov[0], ov[1], ov[2], ov[3]);
             else
 #pragma unroll
                 for (int t = 0; t < 4; ++t)
-                    if (c + t < rowLen) d[c + t] = ov[t];
+                    if (c + t < rowLen) *RPPB_WR(d + (c + t)) = ov[t];
         }
     }
 }

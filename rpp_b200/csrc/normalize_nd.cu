@@ -33,21 +33,23 @@ constexpr int kThreads = 256;
 template <int TYPE>
 __device__ __forceinline__ float load_elem(const void* p, size_t i)
 {
-    if constexpr (TYPE == kNormF32) return static_cast<const float*>(p)[i];
-    else if constexpr (TYPE == kNormF16) return __half2float(static_cast<const __half*>(p)[i]);
-    else if constexpr (TYPE == kNormU8) return float(static_cast<const unsigned char*>(p)[i]);
-    else return float(static_cast<const signed char*>(p)[i]);
+    if constexpr (TYPE == kNormF32) return *RPPB_RD(static_cast<const float*>(p) + i);
+    else if constexpr (TYPE == kNormF16) return __half2float(*RPPB_RD(static_cast<const __half*>(p) + i));
+    else if constexpr (TYPE == kNormU8) return float(*RPPB_RD(static_cast<const unsigned char*>(p) + i));
+    else return float(*RPPB_RD(static_cast<const signed char*>(p) + i));
 }
 
 template <int TYPE>
 __device__ __forceinline__ void store_elem(void* p, size_t i, float v)
 {
-    if constexpr (TYPE == kNormF32) static_cast<float*>(p)[i] = v;
-    else if constexpr (TYPE == kNormF16) static_cast<__half*>(p)[i] = __float2half_rn(v);
+    if constexpr (TYPE == kNormF32) *RPPB_WR(static_cast<float*>(p) + i) = v;
+    else if constexpr (TYPE == kNormF16) *RPPB_WR(static_cast<__half*>(p) + i) = __float2half_rn(v);
     else if constexpr (TYPE == kNormU8)
-        static_cast<unsigned char*>(p)[i] = static_cast<unsigned char>(__float2uint_rz(fmaxf(fminf(v, 255.f), 0.f)));
+        *RPPB_WR(static_cast<unsigned char*>(p) + i) =
+            static_cast<unsigned char>(__float2uint_rz(fmaxf(fminf(v, 255.f), 0.f)));
     else
-        static_cast<signed char*>(p)[i] = static_cast<signed char>(__float2int_rz(fmaxf(fminf(v, 127.f), -128.f)));
+        *RPPB_WR(static_cast<signed char*>(p) + i) =
+            static_cast<signed char>(__float2int_rz(fmaxf(fminf(v, 127.f), -128.f)));
 }
 
 // The reference's compute_sum / compute_diff_square_sum of one line (the value the "+=" adds).
@@ -144,31 +146,31 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(NormNdArgs a, const int
     const int warps = (gridDim.x * kThreads) >> 5;
     for (int t = (blockIdx.x * kThreads + threadIdx.x) >> 5; t < numTasks; t += warps)
     {
-        const int4 task = tasks[t];
+        const int4 task = *RPPB_RD(tasks + t);
         const int b = task.x;
-        const NormNdSample s = a.samples[b];
+        const NormNdSample s = *RPPB_RD(a.samples + b);
         const void* src = static_cast<const char*>(a.src) + size_t(b) * a.srcStride0 * a.srcElem;
         auto one = [&](uint32_t p, bool warp) {
             const size_t q = size_t(b) * a.maxSize + p;
             float mean;
             if (a.compute & 1)
             {
-                const float init = s.accumulate ? a.meanOut[q] : 0.f;
+                const float init = s.accumulate ? *RPPB_RD(a.meanOut + q) : 0.f;
                 mean = __fmul_rn(param_sum<TYPE, false>(a, s, src, p, init, 0.f, warp), s.normFactor);
             }
             else
-                mean = a.meanIn[q];
+                mean = *RPPB_RD(a.meanIn + q);
             float inv = 0.f;
             if (a.compute & 2)
             {
-                const float init = s.accumulate ? a.invOut[q] : 0.f;
+                const float init = s.accumulate ? *RPPB_RD(a.invOut + q) : 0.f;
                 const float x = __fmul_rn(param_sum<TYPE, true>(a, s, src, p, init, mean, warp), s.normFactor);
                 inv = x != 0.f ? __fmul_rn(__frsqrt_rn(x), a.scale) : 0.f;
             }
             if (!warp || lane == 0)
             {
-                if (a.compute & 1) a.meanOut[q] = mean;
-                if (a.compute & 2) a.invOut[q] = inv;
+                if (a.compute & 1) *RPPB_WR(a.meanOut + q) = mean;
+                if (a.compute & 2) *RPPB_WR(a.invOut + q) = inv;
             }
         };
         if (task.w) one(uint32_t(task.y), true);
@@ -182,7 +184,7 @@ __global__ void __launch_bounds__(kThreads) zero_kernel(NormNdArgs a)
 {
     for (int b = blockIdx.y; b < a.n; b += gridDim.y)
     {
-        const size_t zeroFrom = a.samples[b].zeroFrom;
+        const size_t zeroFrom = RPPB_RD(a.samples + b)->zeroFrom;
         void* dst = static_cast<char*>(a.dst) + size_t(b) * a.dstStride0 * a.dstElem;
         for (size_t i = zeroFrom + size_t(blockIdx.x) * kThreads + threadIdx.x; i < a.dstStride0;
              i += size_t(gridDim.x) * kThreads)
@@ -196,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(NormNdArgs a, const
 {
     for (int b = blockIdx.y; b < a.n; b += gridDim.y)
     {
-        const NormNdSample s = a.samples[b];
+        const NormNdSample s = *RPPB_RD(a.samples + b);
         const void* src = static_cast<const char*>(a.src) + size_t(b) * a.srcStride0 * a.srcElem;
         void* dst = static_cast<char*>(a.dst) + size_t(b) * a.dstStride0 * a.dstElem;
         const float* m = mean + size_t(b) * paramOffsetPerSample;
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(kThreads) normalize_kernel(NormNdArgs a, const
                 p += uint32_t(c) * s.lv[l].paramMult;
             }
             const float x = load_elem<TYPE>(src, so);
-            store_elem<TYPE>(dst, dof, __fadd_rn(__fmul_rn(__fsub_rn(x, m[p]), iv[p]), a.shift));
+            store_elem<TYPE>(dst, dof, __fadd_rn(__fmul_rn(__fsub_rn(x, *RPPB_RD(m + p)), *RPPB_RD(iv + p)), a.shift));
         }
     }
 }
@@ -225,8 +227,8 @@ __global__ void __launch_bounds__(kThreads) invert_kernel(const float* __restric
 {
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < count; i += gridDim.x * kThreads)
     {
-        const float v = std[i];
-        inv[i] = v == 0.f ? 1.0f : __fdiv_rn(scale, v);
+        const float v = *RPPB_RD(std + i);
+        *RPPB_WR(inv + i) = v == 0.f ? 1.0f : __fdiv_rn(scale, v);
     }
 }
 

@@ -37,7 +37,7 @@ struct NsrCount
     int reset;
     __device__ long long operator()(int b) const
     {
-        int L = min(len[b], int(stride));
+        int L = min(*RPPB_RD(len + b), int(stride));
         if (L <= 0) return 0;
         long long R = block_len(L, reset);
         return (L + R - 1) / R;
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kMmsThreads) mms_kernel(const float* __restric
             if (w < total)
             {
                 bb[j] = ragged_find(prefix, n, w);
-                const int L = min(len[bb[j]], int(stride));
+                const int L = min(*RPPB_RD(len + bb[j]), int(stride));
                 const long long R = block_len(L, reset);
                 st[j] = int((w - prefix[bb[j]]) * R);
                 en[j] = int(min((long long)L, st[j] + R));
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(kMmsThreads) mms_kernel(const float* __restric
                 for (int t = 0; t < kChunk / 32; ++t)
                 {
                     const int i = pre[j] + c + lane + 32 * t;
-                    r[j][t] = i < st[j] ? __ldg(x + i) : 0.0f;
+                    r[j][t] = i < st[j] ? __ldg(RPPB_RD(x + i)) : 0.0f;
                 }
             }
             if (lane < kBlocksPerWarp)   // the next steps' samples, from L2
@@ -155,8 +155,8 @@ __global__ void __launch_bounds__(kMmsThreads) mms_kernel(const float* __restric
                 {
                     const int i = st[j] + c + lane + 32 * t, o = i - windowLength + 1;
                     const bool live = i < en[j];
-                    ri[j][t] = live ? __ldg(x + i) : 0.0f;
-                    ro[j][t] = live && o >= 0 ? __ldg(x + o) : 0.0f;
+                    ri[j][t] = live ? __ldg(RPPB_RD(x + i)) : 0.0f;
+                    ro[j][t] = live && o >= 0 ? __ldg(RPPB_RD(x + o)) : 0.0f;
                 }
             }
             if (lane < kBlocksPerWarp)   // later steps' entering samples, from L2
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(kMmsThreads) mms_kernel(const float* __restric
                 float* m = mms + size_t(bb[j]) * stride;
 #pragma unroll
                 for (int k = lane; k < kChunk; k += 32)
-                    if (st[j] + c + k < en[j]) m[st[j] + c + k] = vv[j * kRowPitch + k];
+                    if (st[j] + c + k < en[j]) *RPPB_WR(m + (st[j] + c + k)) = vv[j * kRowPitch + k];
             }
             __syncwarp();
         }
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kMmsThreads) mms_kernel(const float* __restric
         {
             const float bm = __shfl_sync(0xffffffffu, bmax, kLaneGap * j);
             const long long w = g * kBlocksPerWarp + j;
-            if (lane == 0 && w < total) blockMax[w] = bm;
+            if (lane == 0 && w < total) *RPPB_WR(blockMax + w) = bm;
         }
     }
 }
@@ -238,10 +238,10 @@ __global__ void __launch_bounds__(kRegionThreads) region_kernel(const float* __r
     const int lane = threadIdx.x & 31;
     const int b = blockIdx.x * (kRegionThreads / 32) + (threadIdx.x >> 5);
     if (b >= n) return;
-    const int L = min(len[b], int(stride));
+    const int L = min(*RPPB_RD(len + b), int(stride));
     if (L <= 0)
     {
-        if (lane == 0) { outBegin[b] = 0; outLength[b] = 0; }
+        if (lane == 0) { *RPPB_WR(outBegin + b) = 0; *RPPB_WR(outLength + b) = 0; }
         return;
     }
     const long long R = block_len(L, reset);
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kRegionThreads) region_kernel(const float* __r
     if (referencePower == 0.0f)
     {
         float m = -FLT_MAX;
-        for (int k = lane; k < nb; k += 32) m = fmaxf(m, blockMax[u0 + k]);
+        for (int k = lane; k < nb; k += 32) m = fmaxf(m, *RPPB_RD(blockMax + (u0 + k)));
         base = warp_max(m);
     }
     const float cutOffMag = __fmul_rn(base, cutOff);
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kRegionThreads) region_kernel(const float* __r
     for (int k0 = 0; k0 < nb && firstBlock < 0; k0 += 32)
     {
         const int k = k0 + lane;
-        unsigned hit = __ballot_sync(0xffffffffu, k < nb && blockMax[u0 + k] >= cutOffMag);
+        unsigned hit = __ballot_sync(0xffffffffu, k < nb && *RPPB_RD(blockMax + (u0 + k)) >= cutOffMag);
         if (hit) firstBlock = k0 + __ffs(hit) - 1;
     }
     int detectBegin = 0, detectLength = 0;
@@ -273,14 +273,14 @@ __global__ void __launch_bounds__(kRegionThreads) region_kernel(const float* __r
         for (int i0 = s0; i0 < s1 && beginIdx < 0; i0 += 32)
         {
             const int i = i0 + lane;
-            unsigned hit = __ballot_sync(0xffffffffu, i < s1 && m[i] >= cutOffMag);
+            unsigned hit = __ballot_sync(0xffffffffu, i < s1 && *RPPB_RD(m + i) >= cutOffMag);
             if (hit) beginIdx = i0 + __ffs(hit) - 1;
         }
         int lastBlock = -1;
         for (int k1 = nb - 1; k1 >= 0 && lastBlock < 0; k1 -= 32)
         {
             const int k = k1 - lane;
-            unsigned hit = __ballot_sync(0xffffffffu, k >= 0 && blockMax[u0 + k] >= cutOffMag);
+            unsigned hit = __ballot_sync(0xffffffffu, k >= 0 && *RPPB_RD(blockMax + (u0 + k)) >= cutOffMag);
             if (hit) lastBlock = k1 - (__ffs(hit) - 1);
         }
         int endIdx = -1;
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kRegionThreads) region_kernel(const float* __r
         for (int i1 = e1 - 1; i1 >= e0 && endIdx < 0; i1 -= 32)
         {
             const int i = i1 - lane;
-            unsigned hit = __ballot_sync(0xffffffffu, i >= e0 && m[i] >= cutOffMag);
+            unsigned hit = __ballot_sync(0xffffffffu, i >= e0 && *RPPB_RD(m + i) >= cutOffMag);
             if (hit) endIdx = i1 - (__ffs(hit) - 1);
         }
         detectBegin = beginIdx;
@@ -302,8 +302,8 @@ __global__ void __launch_bounds__(kRegionThreads) region_kernel(const float* __r
     }
     if (lane == 0)
     {
-        outBegin[b] = detectBegin;
-        outLength[b] = detectLength;
+        *RPPB_WR(outBegin + b) = detectBegin;
+        *RPPB_WR(outLength + b) = detectLength;
     }
 }
 

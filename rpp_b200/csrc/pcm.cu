@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(kThreads) pcm16_kernel(const short* __restrict
     for (long long u = blockIdx.x; u < units; u += gridDim.x)
     {
         const int b = int(u / unitsPerSample);
-        const long long count = min((long long)max(len[b], 0) * channels, (long long)min(srcStride, dstStride));
+        const long long count = min((long long)max(*RPPB_RD(len + b), 0) * channels, (long long)min(srcStride, dstStride));
         const long long i0 = (u % unitsPerSample) * (long long)kChunk;
         if (i0 >= count) continue;
         const long long i1 = min(i0 + kChunk, count);
@@ -34,15 +34,15 @@ __global__ void __launch_bounds__(kThreads) pcm16_kernel(const short* __restrict
         {
             for (; i + 8 <= i1; i += 8 * kThreads)
             {
-                const int4 v = *reinterpret_cast<const int4*>(s + i);
+                const int4 v = *RPPB_RD(reinterpret_cast<const int4*>(s + i));
                 const short* p = reinterpret_cast<const short*>(&v);
                 const float k = 1.0f / 32768.0f;
-                *reinterpret_cast<float4*>(d + i) = make_float4(p[0] * k, p[1] * k, p[2] * k, p[3] * k);
-                *reinterpret_cast<float4*>(d + i + 4) = make_float4(p[4] * k, p[5] * k, p[6] * k, p[7] * k);
+                *RPPB_WR(reinterpret_cast<float4*>(d + i)) = make_float4(p[0] * k, p[1] * k, p[2] * k, p[3] * k);
+                *RPPB_WR(reinterpret_cast<float4*>(d + i + 4)) = make_float4(p[4] * k, p[5] * k, p[6] * k, p[7] * k);
             }
         }
         for (; i < i1; i += 8 * kThreads)
-            for (int j = 0; j < 8 && i + j < i1; ++j) d[i + j] = float(s[i + j]) * (1.0f / 32768.0f);
+            for (int j = 0; j < 8 && i + j < i1; ++j) *RPPB_WR(d + (i + j)) = float(*RPPB_RD(s + (i + j))) * (1.0f / 32768.0f);
     }
 }
 

@@ -23,7 +23,7 @@ struct PreemphCount
     const int* len;
     __device__ long long operator()(int b) const
     {
-        int l = len[b];
+        int l = *RPPB_RD(len + b);
         return l <= 0 ? 1 : (l + kChunk - 1) / kChunk;
     }
 };
@@ -46,8 +46,8 @@ __global__ void __launch_bounds__(kThreads) pre_emphasis_kernel(const float* __r
         const int chunk = int(w - prefix[b]);
         const float* x = src + size_t(b) * srcStride;
         float* y = dst + size_t(b) * dstStride;
-        const int L = len[b];
-        const float c = coeff[b];
+        const int L = *RPPB_RD(len + b);
+        const float c = *RPPB_RD(coeff + b);
 #pragma unroll
         for (int k = 0; k < kChunk / (kThreads * 4); ++k)
         {
@@ -56,25 +56,25 @@ __global__ void __launch_bounds__(kThreads) pre_emphasis_kernel(const float* __r
             bool full = kVec && (i + 3 < L);
             if (full)
             {
-                float4 q = *reinterpret_cast<const float4*>(x + i);
+                float4 q = *RPPB_RD(reinterpret_cast<const float4*>(x + i));
                 v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
             }
             else
             {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) v[j] = (i + j < L) ? x[i + j] : 0.f;
+                for (int j = 0; j < 4; ++j) v[j] = (i + j < L) ? *RPPB_RD(x + (i + j)) : 0.f;
             }
             // x[i-1] is the previous lane's last sample, except at lane 0 of each warp.
             float up = __shfl_up_sync(0xffffffffu, v[3], 1);
             if (i == 0)
             {
                 size_t base = size_t(b) * srcStride;
-                prev = border == 1 ? x[0] : border == 2 ? (base + 1 < srcElems ? x[1] : 0.f) : 0.f;
-                if (L <= 0) v[0] = base < srcElems ? x[0] : 0.f;
+                prev = border == 1 ? *RPPB_RD(x) : border == 2 ? (base + 1 < srcElems ? *RPPB_RD(x + 1) : 0.f) : 0.f;
+                if (L <= 0) v[0] = base < srcElems ? *RPPB_RD(x) : 0.f;
             }
             else
             {
-                prev = (lane == 0 && i - 1 < L) ? x[i - 1] : up;
+                prev = (lane == 0 && i - 1 < L) ? *RPPB_RD(x + (i - 1)) : up;
             }
             float out[4];
             out[0] = __fsub_rn(v[0], __fmul_rn(c, prev));
@@ -82,13 +82,13 @@ __global__ void __launch_bounds__(kThreads) pre_emphasis_kernel(const float* __r
             for (int j = 1; j < 4; ++j) out[j] = __fsub_rn(v[j], __fmul_rn(c, v[j - 1]));
             if (full)
             {
-                *reinterpret_cast<float4*>(y + i) = make_float4(out[0], out[1], out[2], out[3]);
+                *RPPB_WR(reinterpret_cast<float4*>(y + i)) = make_float4(out[0], out[1], out[2], out[3]);
             }
             else
             {
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    if (i + j < L || i + j == 0) y[i + j] = out[j];
+                    if (i + j < L || i + j == 0) *RPPB_WR(y + (i + j)) = out[j];
             }
         }
     }

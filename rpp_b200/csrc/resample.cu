@@ -125,11 +125,13 @@ struct ResampleCount
         float ir, orr;
         if (clips)
         {
-            L = clips[b].length, C = 1, Cs = 1, ir = clips[b].inRate, orr = outRateAll;
+            const RppbClip* c = RPPB_RD(clips + b);
+            L = c->length, C = 1, Cs = 1, ir = c->inRate, orr = outRateAll;
         }
         else
         {
-            L = dims[2 * b], Cs = dims[2 * b + 1], C = mix ? 1 : Cs, ir = inRate[b], orr = outRate[b];
+            L = *RPPB_RD(dims + 2 * b), Cs = *RPPB_RD(dims + (2 * b + 1)), C = mix ? 1 : Cs, ir = *RPPB_RD(inRate + b),
+            orr = *RPPB_RD(outRate + b);
         }
         if (L <= 0 || Cs <= 0) return 0;
         if (ir == orr) return ((long long)L * C + kCopyChunk - 1) / kCopyChunk;
@@ -257,10 +259,11 @@ __global__ void __launch_bounds__(kThreads, kMix ? 5 : 4)
         for (int i = threadIdx.x; i < pairCount; i += kThreads)
         {
             const int e = min(max(i - wd.padLeft, 0), wd.lutSize - 2);   // the clamped entry
-            reinterpret_cast<float2*>(s_lut)[i] = make_float2(wd.lut[e], __fsub_rn(wd.lut[e + 1], wd.lut[e]));
+            const float v0 = *RPPB_RD(wd.lut + e), v1 = *RPPB_RD(wd.lut + (e + 1));
+            reinterpret_cast<float2*>(s_lut)[i] = make_float2(v0, __fsub_rn(v1, v0));
         }
     else
-        for (int i = threadIdx.x; i < wd.lutSize; i += kThreads) s_lut[i] = wd.lut[i];
+        for (int i = threadIdx.x; i < wd.lutSize; i += kThreads) s_lut[i] = *RPPB_RD(wd.lut + i);
     const Win<kPairs, kMagic, kFma> win{s_lut, reinterpret_cast<const float2*>(s_lut) + (kPairs ? wd.padLeft : 0),
                                         wd.lutSize, wd.scale, wd.center,
                                         uint32_t(__cvta_generic_to_shared(reinterpret_cast<const float2*>(s_lut) +
@@ -285,13 +288,14 @@ __global__ void __launch_bounds__(kThreads, kMix ? 5 : 4)
         {
             const int b = ragged_find(prefix, n, w);
             u.unit = int(w - prefix[b]);
-            u.L = kTable ? clips[b].length : dims[2 * b];
-            u.Csrc = kTable ? 1 : dims[2 * b + 1];
+            const RppbClip* clip = kTable ? RPPB_RD(clips + b) : nullptr;
+            u.L = kTable ? clip->length : *RPPB_RD(dims + 2 * b);
+            u.Csrc = kTable ? 1 : *RPPB_RD(dims + (2 * b + 1));
             u.C = kMix ? 1 : u.Csrc;
-            const float inRate = kTable ? clips[b].inRate : inRateT[b];
-            const float outRate = kTable ? outRateAll : outRateT[b];
-            u.x = kTable ? clips[b].src : src + size_t(b) * srcStride;
-            u.y = kTable ? clips[b].work : dst + size_t(b) * dstStride;
+            const float inRate = kTable ? clip->inRate : *RPPB_RD(inRateT + b);
+            const float outRate = kTable ? outRateAll : *RPPB_RD(outRateT + b);
+            u.x = kTable ? clip->src : src + size_t(b) * srcStride;
+            u.y = kTable ? clip->work : dst + size_t(b) * dstStride;
             u.dstStride = kTable ? 0x7fffffffu : dstStride;   // a clip's work buffer holds the whole resampled clip
             u.wc = kMix ? MonoMix::weight(max(u.Csrc, 1), normalize) : 1.f;
             u.mode = inRate == outRate ? kUnitCopy : (kMix && u.Csrc > 64) ? kUnitSkip : kUnitResample;
@@ -350,7 +354,8 @@ __global__ void __launch_bounds__(kThreads, kMix ? 5 : 4)
                         kMix ? min((long long)L, (long long)u.dstStride)
                              : (kTable ? (long long)L : min((long long)L * C, (long long)min(srcStride, u.dstStride)));
                     const long long i0 = (long long)u.unit * kCopyChunk + step * kPart;
-                    for (long long i = i0 + lane; i < min(count, i0 + kPart); i += 32) y[i] = kMix ? mix(i) : x[i];
+                    for (long long i = i0 + lane; i < min(count, i0 + kPart); i += 32)
+                        *RPPB_WR(y + i) = kMix ? mix(i) : *RPPB_RD(x + i);
                 }
                 else if (u.mode == kUnitResample)
                 {
@@ -452,8 +457,8 @@ __global__ void __launch_bounds__(kThreads, kMix ? 5 : 4)
                                 float r;
                                 if (kMix && staged) r = run([&](int l) { return s_span[l - lo]; });
                                 else if (kMix) r = run([&](int l) { return mix((long long)inBlockRounded + l); });
-                                else r = run([&](int l) { return __ldg(in + l); });
-                                y[outPos] = r;
+                                else r = run([&](int l) { return __ldg(RPPB_RD(in + l)); });
+                                *RPPB_WR(y + outPos) = r;
                             }
                             else
                             {
@@ -468,11 +473,12 @@ __global__ void __launch_bounds__(kThreads, kMix ? 5 : 4)
 #pragma unroll
                                     for (int c = 0; c < kMaxC; ++c)
                                         if (c < C)
-                                            acc[c] = __fadd_rn(acc[c], __fmul_rn(__ldg(in + (long long)l * C + c), wv));
+                                            acc[c] = __fadd_rn(acc[c],
+                                                               __fmul_rn(__ldg(RPPB_RD(in + (long long)l * C + c)), wv));
                                 }
 #pragma unroll
                                 for (int c = 0; c < kMaxC; ++c)
-                                    if (c < C) y[(long long)outPos * C + c] = acc[c];
+                                    if (c < C) *RPPB_WR(y + ((long long)outPos * C + c)) = acc[c];
                             }
                         }
                         if (kMix) __syncwarp();   // the warp's span is restaged by its next slice

@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kThreads) slice_kernel(SliceArgs a, const T* _
                                                          const T* __restrict__ fill)
 {
     const long long units = (long long)a.n * a.unitsPerSample;
-    const T fv = a.enablePadding ? fill[0] : T(0);
+    const T fv = a.enablePadding ? *RPPB_RD(fill) : T(0);
     for (long long u = blockIdx.x; u < units; u += gridDim.x)
     {
         const int b = int(u / a.unitsPerSample);
@@ -40,6 +40,8 @@ __global__ void __launch_bounds__(kThreads) slice_kernel(SliceArgs a, const T* _
         const int* an = a.anchor + b * a.numDims;
         const int* sh = a.shape + b * a.numDims;
         const int* len = reinterpret_cast<const int*>(a.roi + b * a.numDims * 2 + a.numDims);
+        const unsigned rowBytes = unsigned(a.numDims) * sizeof(int);
+        if (!RPPB_RANGE_OK(an, rowBytes) || !RPPB_RANGE_OK(sh, rowBytes) || !RPPB_RANGE_OK(len, rowBytes)) continue;
         bool need = false;
         int m0 = 0, m1 = 1;
         for (int k = 0; k < a.numDims; ++k)
@@ -72,7 +74,7 @@ __global__ void __launch_bounds__(kThreads) slice_kernel(SliceArgs a, const T* _
                     const long long e = i + j;
                     if (e < m0)
                     {
-                        v[j] = sa[e];
+                        v[j] = *RPPB_RD(sa + e);
                         written |= 1 << j;
                     }
                     else if (pad && e < (long long)a.dstStride0 - 1)
@@ -84,15 +86,15 @@ __global__ void __launch_bounds__(kThreads) slice_kernel(SliceArgs a, const T* _
                 if (vec && written == 15 && i + 3 < iEnd)
                 {
                     if constexpr (sizeof(T) == 4)
-                        *reinterpret_cast<float4*>(d + i) = make_float4(v[0], v[1], v[2], v[3]);
+                        *RPPB_WR(reinterpret_cast<float4*>(d + i)) = make_float4(v[0], v[1], v[2], v[3]);
                     else
-                        *reinterpret_cast<uchar4*>(d + i) = make_uchar4(v[0], v[1], v[2], v[3]);
+                        *RPPB_WR(reinterpret_cast<uchar4*>(d + i)) = make_uchar4(v[0], v[1], v[2], v[3]);
                 }
                 else
                 {
 #pragma unroll
                     for (int j = 0; j < 4; ++j)
-                        if ((written >> j & 1) && i + j < iEnd) d[i + j] = v[j];
+                        if ((written >> j & 1) && i + j < iEnd) *RPPB_WR(d + (i + j)) = v[j];
                 }
             }
         }
@@ -159,8 +161,8 @@ __global__ void __launch_bounds__(kThreads) slice_kernel(SliceArgs a, const T* _
                     in = in && q < uint32_t(cnt[l]);
                     off += size_t(q) * ss[l];
                 }
-                if (in) d[i] = sb[off];
-                else if (padN) d[i] = fv;
+                if (in) *RPPB_WR(d + i) = *RPPB_RD(sb + off);
+                else if (padN) *RPPB_WR(d + i) = fv;
             }
         }
         else
@@ -168,8 +170,9 @@ __global__ void __launch_bounds__(kThreads) slice_kernel(SliceArgs a, const T* _
             for (long long i = i0 + threadIdx.x; i < iEnd; i += kThreads)
             {
                 const uint32_t r = uint32_t(i) / a.dstStride1, c = uint32_t(i) - r * a.dstStride1;
-                if (r < uint32_t(m0) && c < uint32_t(m1)) d[i] = s[(size_t)(an[0] + r) * a.srcStride1 + an[1] + c];
-                else if (pad && i < (long long)a.dstStride0 - 1) d[i] = fv;
+                if (r < uint32_t(m0) && c < uint32_t(m1))
+                    *RPPB_WR(d + i) = *RPPB_RD(s + ((size_t)(an[0] + r) * a.srcStride1 + an[1] + c));
+                else if (pad && i < (long long)a.dstStride0 - 1) *RPPB_WR(d + i) = fv;
             }
         }
     }

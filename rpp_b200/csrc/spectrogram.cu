@@ -37,7 +37,7 @@ struct SpecCount
     bool center;
     __device__ long long operator()(int b) const
     {
-        int F = min(num_windows(len[b], W, hop, center), maxFrames);
+        int F = min(num_windows(*RPPB_RD(len + b), W, hop, center), maxFrames);
         return F <= 0 ? 0 : (F + tile - 1) / tile;
     }
 };
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kThreads, (NFFT <= 512 ? 3 : 2)) spectrogram_f
     {
         const int b = ragged_find(prefix, a.n, w);
         const int f0 = int(w - prefix[b]) * TF;
-        const int L = a.len[b];
+        const int L = *RPPB_RD(a.len + b);
         const int F = min(num_windows(L, W, a.windowStep, a.center), a.maxFrames);
         const PlainSource src{a.src + size_t(b) * a.srcStride, L, a.reflect};
         stft_tile<NFFT, kThreads>(src, f0, F, W, a.windowStep, centerOffset, a.power, s_win, s_tw, s_tw1, s_span,
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kThreads, (NFFT <= 512 ? 3 : 2)) spectrogram_f
                 const float* sp = s_out + k * S::OUT_LD + f;
                 float* yp = y + size_t(k) * a.dstHStride + f0 + f;
                 const size_t ystep = size_t(KS) * a.dstHStride;
-                for (; k < BINS; k += KS, sp += KS * S::OUT_LD, yp += ystep) *yp = *sp;
+                for (; k < BINS; k += KS, sp += KS * S::OUT_LD, yp += ystep) *RPPB_WR(yp) = *sp;
             }
         }
         else
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(kThreads, (NFFT <= 512 ? 3 : 2)) spectrogram_f
             for (int idx = threadIdx.x; idx < BINS * TF; idx += kThreads)
             {
                 const int f = idx / BINS, k = idx % BINS;
-                if (f < Tv) y[size_t(f0 + f) * a.dstHStride + k] = s_out[k * S::OUT_LD + f];
+                if (f < Tv) *RPPB_WR(y + (size_t(f0 + f) * a.dstHStride + k)) = s_out[k * S::OUT_LD + f];
             }
         }
         __syncthreads();
@@ -130,7 +130,7 @@ struct FrameCount
     bool center;
     __device__ long long operator()(int b) const
     {
-        int F = min(num_windows(len[b], W, hop, center), maxFrames);
+        int F = min(num_windows(*RPPB_RD(len + b), W, hop, center), maxFrames);
         return F <= 0 ? 0 : F;
     }
 };
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kThreads) spectrogram_dft_kernel(SpectrogramAr
     const int N = a.nfft;
     float2* s_tw = reinterpret_cast<float2*>(smem);
     float* s_v = reinterpret_cast<float*>(smem + size_t(N) * 8);
-    for (int i = threadIdx.x; i < N; i += kThreads) s_tw[i] = twiddle[i];
+    for (int i = threadIdx.x; i < N; i += kThreads) s_tw[i] = *RPPB_RD(twiddle + i);
     const int W = a.windowLength;
     const int off = (W < N) ? (N - W) / 2 : 0;
     const int centerOffset = a.center ? W / 2 : 0;
@@ -154,14 +154,14 @@ __global__ void __launch_bounds__(kThreads) spectrogram_dft_kernel(SpectrogramAr
     {
         const int b = ragged_find(prefix, a.n, w);
         const int frame = int(w - prefix[b]);
-        const int L = a.len[b];
+        const int L = *RPPB_RD(a.len + b);
         const float* x = a.src + size_t(b) * a.srcStride;
         const int ws = frame * a.windowStep - centerOffset;
         __syncthreads();
         for (int t = threadIdx.x; t < N; t += kThreads)
         {
             const int u = t - off;
-            s_v[t] = (u >= 0 && u < W) ? a.window[u] * PlainSource{x, L, a.reflect}(ws + u) : 0.f;
+            s_v[t] = (u >= 0 && u < W) ? *RPPB_RD(a.window + u) * PlainSource{x, L, a.reflect}(ws + u) : 0.f;
         }
         __syncthreads();
         float* y = a.dst + size_t(b) * a.dstNStride;
@@ -180,8 +180,8 @@ __global__ void __launch_bounds__(kThreads) spectrogram_dft_kernel(SpectrogramAr
             }
             const float p = fmaf(re, re, im * im);
             const float o = (a.power == 1) ? sqrtf(p) : p;
-            if (a.nft) y[size_t(k) * a.dstHStride + frame] = o;
-            else y[size_t(frame) * a.dstHStride + k] = o;
+            if (a.nft) *RPPB_WR(y + (size_t(k) * a.dstHStride + frame)) = o;
+            else *RPPB_WR(y + (size_t(frame) * a.dstHStride + k)) = o;
         }
     }
 }

@@ -83,12 +83,15 @@ struct PlainSource
     bool reflect;
     __device__ __forceinline__ float operator()(int i) const
     {
-        if (i >= 0 && i < L) return __ldg(x + i);
+        if (i >= 0 && i < L) return __ldg(RPPB_RD(x + i));
         if (!reflect || L <= 0) return 0.f;
-        return __ldg(x + reflect_index(i, 0, L));
+        return __ldg(RPPB_RD(x + reflect_index(i, 0, L)));
     }
     // 4 consecutive in-range samples from 16-byte aligned x + i
-    __device__ __forceinline__ float4 quad(int i) const { return __ldg(reinterpret_cast<const float4*>(x + i)); }
+    __device__ __forceinline__ float4 quad(int i) const
+    {
+        return __ldg(RPPB_RD(reinterpret_cast<const float4*>(x + i)));
+    }
 };
 
 // The pre-emphasized signal y[0] = x[0] - c*border, y[i] = x[i] - c*x[i-1]
@@ -101,8 +104,8 @@ struct PreemphSource
     float c, border;
     __device__ __forceinline__ float at(int i) const
     {
-        const float prev = i == 0 ? border : __ldg(x + i - 1);
-        return __fsub_rn(__ldg(x + i), __fmul_rn(c, prev));
+        const float prev = i == 0 ? border : __ldg(RPPB_RD(x + i - 1));
+        return __fsub_rn(__ldg(RPPB_RD(x + i)), __fmul_rn(c, prev));
     }
     __device__ __forceinline__ float operator()(int i) const
     {
@@ -112,8 +115,8 @@ struct PreemphSource
     }
     __device__ __forceinline__ float4 quad(int i) const
     {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(x + i));
-        const float p = i == 0 ? border : __ldg(x + i - 1);
+        const float4 v = __ldg(RPPB_RD(reinterpret_cast<const float4*>(x + i)));
+        const float p = i == 0 ? border : __ldg(RPPB_RD(x + i - 1));
         return make_float4(__fsub_rn(v.x, __fmul_rn(c, p)), __fsub_rn(v.y, __fmul_rn(c, v.x)),
                            __fsub_rn(v.z, __fmul_rn(c, v.y)), __fsub_rn(v.w, __fmul_rn(c, v.z)));
     }
@@ -128,14 +131,15 @@ __device__ __forceinline__ void stft_tables(const float2* __restrict__ twiddle, 
                                             float2* s_tw, float2* s_tw1, float* s_win, float* s_span)
 {
     using S = StftShape<NFFT, THREADS>;
-    for (int i = threadIdx.x; i <= S::M / 2; i += THREADS) s_tw[i] = twiddle[i];
+    for (int i = threadIdx.x; i <= S::M / 2; i += THREADS) s_tw[i] = *RPPB_RD(twiddle + i);
     for (int i = threadIdx.x; i < S::R1 * S::R2; i += THREADS)
     {
         const int k1 = i / S::R2, j = i % S::R2;
-        s_tw1[i] = twiddle[(2 * j * k1) & (NFFT - 1)];
+        s_tw1[i] = *RPPB_RD(twiddle + ((2 * j * k1) & (NFFT - 1)));
     }
     const int off = S::window_offset(W);
-    for (int i = threadIdx.x; i < NFFT; i += THREADS) s_win[i] = (i >= off && i - off < W) ? window[i - off] : 0.f;
+    for (int i = threadIdx.x; i < NFFT; i += THREADS)
+        s_win[i] = (i >= off && i - off < W) ? *RPPB_RD(window + (i - off)) : 0.f;
     for (int i = threadIdx.x; i < S::span_pad(W); i += THREADS) s_span[i] = 0.f;
     __syncthreads();
 }

@@ -36,7 +36,7 @@ struct DecibelCount
     const uint32_t* dims;
     __device__ long long operator()(int b) const
     {
-        long long wdt = dims[2 * b], hgt = dims[2 * b + 1];
+        long long wdt = *RPPB_RD(dims + 2 * b), hgt = *RPPB_RD(dims + (2 * b + 1));
         if (wdt == 1) return (hgt + kChunk - 1) / kChunk;
         return ((hgt + kRowsPerUnit - 1) / kRowsPerUnit) * ((wdt + kChunk - 1) / kChunk);
     }
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(kThreads) decibel_max_kernel(const float* __re
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
     {
         const int b = ragged_find(prefix, n, w);
-        const uint32_t wdt = dims[2 * b], hgt = dims[2 * b + 1];
+        const uint32_t wdt = *RPPB_RD(dims + 2 * b), hgt = *RPPB_RD(dims + (2 * b + 1));
         const UnitSpan s = unit_span(wdt, hgt, w - prefix[b]);
         const float* base = src + size_t(b) * nStride + size_t(s.row) * hStride + s.col0;
         // a lane loads 4 column steps (16 values) before folding them, so the loads overlap
@@ -106,13 +106,13 @@ __global__ void __launch_bounds__(kThreads) decibel_max_kernel(const float* __re
                 {
                     const uint32_t c = c0 + k * step;
                     x[k] = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX);
-                    if (vec && c + 4 <= s.cols) x[k] = __ldg(reinterpret_cast<const float4*>(p + c));
+                    if (vec && c + 4 <= s.cols) x[k] = __ldg(RPPB_RD(reinterpret_cast<const float4*>(p + c)));
                     else
                     {
-                        if (c < s.cols) x[k].x = __ldg(p + c);
-                        if (c + 1 < s.cols) x[k].y = __ldg(p + c + 1);
-                        if (c + 2 < s.cols) x[k].z = __ldg(p + c + 2);
-                        if (c + 3 < s.cols) x[k].w = __ldg(p + c + 3);
+                        if (c < s.cols) x[k].x = __ldg(RPPB_RD(p + c));
+                        if (c + 1 < s.cols) x[k].y = __ldg(RPPB_RD(p + c + 1));
+                        if (c + 2 < s.cols) x[k].z = __ldg(RPPB_RD(p + c + 2));
+                        if (c + 3 < s.cols) x[k].w = __ldg(RPPB_RD(p + c + 3));
                     }
                 }
 #pragma unroll
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kThreads) decibel_max_kernel(const float* __re
         {
             float v = threadIdx.x < kThreads / 32 ? warpMax[threadIdx.x] : -FLT_MAX;
             v = warp_max(v);
-            if (threadIdx.x == 0) atomicMax(maxKey + b, float_key(v));
+            if (threadIdx.x == 0) atomicMax(RPPB_WR(maxKey + b), float_key(v));
         }
         __syncthreads();
     }
@@ -147,12 +147,12 @@ __global__ void __launch_bounds__(kThreads) decibel_kernel(const float* __restri
     for (long long w = blockIdx.x; w < total; w += gridDim.x)
     {
         const int b = ragged_find(prefix, n, w);
-        const uint32_t wdt = dims[2 * b], hgt = dims[2 * b + 1];
+        const uint32_t wdt = *RPPB_RD(dims + 2 * b), hgt = *RPPB_RD(dims + (2 * b + 1));
         const UnitSpan s = unit_span(wdt, hgt, w - prefix[b]);
         float ref = refMag;
         if (kUseMax)
         {
-            unsigned k = maxKey[b];
+            unsigned k = *RPPB_RD(maxKey + b);
             ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
         }
         const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
@@ -183,13 +183,13 @@ __global__ void __launch_bounds__(kThreads) decibel_kernel(const float* __restri
                 {
                     const uint32_t c = c0 + k * step;
                     x[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (vec && c + 4 <= s.cols) x[k] = *reinterpret_cast<const float4*>(p + c);
+                    if (vec && c + 4 <= s.cols) x[k] = *RPPB_RD(reinterpret_cast<const float4*>(p + c));
                     else
                     {
-                        if (c < s.cols) x[k].x = p[c];
-                        if (c + 1 < s.cols) x[k].y = p[c + 1];
-                        if (c + 2 < s.cols) x[k].z = p[c + 2];
-                        if (c + 3 < s.cols) x[k].w = p[c + 3];
+                        if (c < s.cols) x[k].x = *RPPB_RD(p + c);
+                        if (c + 1 < s.cols) x[k].y = *RPPB_RD(p + (c + 1));
+                        if (c + 2 < s.cols) x[k].z = *RPPB_RD(p + (c + 2));
+                        if (c + 3 < s.cols) x[k].w = *RPPB_RD(p + (c + 3));
                     }
                 }
 #pragma unroll
@@ -197,13 +197,13 @@ __global__ void __launch_bounds__(kThreads) decibel_kernel(const float* __restri
                 {
                     const uint32_t c = c0 + k * step;
                     const float4 y = make_float4(db(x[k].x), db(x[k].y), db(x[k].z), db(x[k].w));
-                    if (vec && c + 4 <= s.cols) *reinterpret_cast<float4*>(q + c) = y;
+                    if (vec && c + 4 <= s.cols) *RPPB_WR(reinterpret_cast<float4*>(q + c)) = y;
                     else
                     {
-                        if (c < s.cols) q[c] = y.x;
-                        if (c + 1 < s.cols) q[c + 1] = y.y;
-                        if (c + 2 < s.cols) q[c + 2] = y.z;
-                        if (c + 3 < s.cols) q[c + 3] = y.w;
+                        if (c < s.cols) *RPPB_WR(q + c) = y.x;
+                        if (c + 1 < s.cols) *RPPB_WR(q + (c + 1)) = y.y;
+                        if (c + 2 < s.cols) *RPPB_WR(q + (c + 2)) = y.z;
+                        if (c + 3 < s.cols) *RPPB_WR(q + (c + 3)) = y.w;
                     }
                 }
             }

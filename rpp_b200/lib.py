@@ -10,6 +10,9 @@ from .types import (RpptGenericDesc, RpptDesc, RpptImagePatch, RpptResamplingWin
                     RppbCompletion)
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "librppb.so")
+# The checked build (`python -m rpp_b200.build --checked`): every global access of the kernels checked against
+# the regions of its call.  RPPB_LIBRARY=checked loads it instead of LIB_PATH; RPPB_LIBRARY=<path> loads <path>.
+CHECKED_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "librppb_checked.so")
 
 # Every symbol the public headers (include/*.h) declare.
 EXPORTED = (
@@ -24,6 +27,7 @@ EXPORTED = (
     "rppb_server_create", "rppb_server_destroy", "rppb_server_frames", "rppb_server_submit", "rppb_server_poll",
     "rppb_server_arena_used",
     "rppt_slice_gpu", "rppt_normalize_gpu", "rppb_pcm16_to_f32_gpu", "rppb_mel_filter_bank_tc_gpu",
+    "rppb_check_shrink_next_destination",
 )
 
 _lib = None
@@ -40,7 +44,8 @@ def load(path=None):
     global _lib
     if _lib is not None:
         return _lib
-    p = path or LIB_PATH
+    env = os.environ.get("RPPB_LIBRARY", "")
+    p = path or (CHECKED_LIB_PATH if env == "checked" else env) or LIB_PATH
     if not os.path.isfile(p):
         raise FileNotFoundError(f"{p} is missing: build it with `python -m rpp_b200.build` (no CPU fallback)")
     L = ctypes.CDLL(p)
@@ -91,6 +96,8 @@ def load(path=None):
     L.rppb_pcm16_to_f32_gpu.restype = _I
     L.rppb_mel_filter_bank_tc_gpu.argtypes = [_V, _D, _V, _D, _V, _F, _F, _I, _I, _F, _B, _I, _V]
     L.rppb_mel_filter_bank_tc_gpu.restype = _I
+    L.rppb_check_shrink_next_destination.argtypes = [ctypes.c_uint64]
+    L.rppb_check_shrink_next_destination.restype = _I
     L.rppb_server_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(RppbServerConfig)]
     L.rppb_server_create.restype = _I
     L.rppb_server_destroy.argtypes = [_V]
