@@ -124,7 +124,7 @@ __device__ __forceinline__ void tc_tables(const float2* __restrict__ twiddle, un
         put(b2, r2, K, u);
     }
     // the twiddles of epilogue 1 by (n1, k2): W512^(n1 k2), 17 per n1
-    for (int e = threadIdx.x; e < 16 * 17; e += kFusedThreads) w512[e] = twiddle[(e / 17) * (e % 17)];
+    for (int e = threadIdx.x; e < 16 * 17; e += kFusedThreads) w512[e] = *RPPB_RD(twiddle + (e / 17) * (e % 17));
 }
 
 // Stage-1 operand: A1_j row (f, q) = q + 8 f, K index kk (hi 0..31 | lo 0..31) holding n2 = s1_n2(kk), value
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
             s_win[i] = (i >= off && i - off < a.W) ? a.window[i - off] : 0.f;
         for (int i = threadIdx.x; i < S::span_pad(a.W); i += kFusedThreads) s_span[i] = 0.f;
         uint4* t = reinterpret_cast<uint4*>(smem + lay.mel);
-        for (int i = threadIdx.x; i < int(lay.melBytes / 16); i += kFusedThreads) t[i] = __ldg(melTables + i);
+        for (int i = threadIdx.x; i < int(lay.melBytes / 16); i += kFusedThreads) t[i] = __ldg(RPPB_RD(melTables + i));
     }
     tc::fence_async_smem();   // the bases are read by the tensor core
     tc::fence_before();
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
             pending = 0;
         }
         tc::fence_after();
-        if (bad && threadIdx.x == 0) atomicOr(errorWord, 4);
+        if (bad && threadIdx.x == 0) atomicOr(RPPB_WR(errorWord), 4);
         return !bad;
     };
 
@@ -359,9 +359,9 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     int cur = 0;
     if (threadIdx.x == 0)
     {
-        const long long w0 = (long long)atomicAdd(workCounter, 1ull);
-        const long long w1 = (long long)atomicAdd(workCounter, 1ull);
-        wAfter = w1 < total - 2ll * gridDim.x ? (long long)atomicAdd(workCounter, 1ull) : -1ll;
+        const long long w0 = (long long)atomicAdd(RPPB_WR(workCounter), 1ull);
+        const long long w1 = (long long)atomicAdd(RPPB_WR(workCounter), 1ull);
+        wAfter = w1 < total - 2ll * gridDim.x ? (long long)atomicAdd(RPPB_WR(workCounter), 1ull) : -1ll;
         s_it[0] = decode_item<TF>(a, cnt, prefix, nslots, total, w0);
         s_it[1] = decode_item<TF>(a, cnt, prefix, nslots, total, w1);
         prefetch_span(s_it[1]);
@@ -481,11 +481,11 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                         }
                         if (i > m0)
                         {
-                            yp[0] = fall.x;
+                            *RPPB_WR(yp) = fall.x;
                             tmax = fmaxf(tmax, fall.x);
                             if (second)
                             {
-                                yp[1] = fall.y;
+                                *RPPB_WR(yp + 1) = fall.y;
                                 tmax = fmaxf(tmax, fall.y);
                             }
                             yp += hs;
@@ -505,11 +505,11 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                 const int need = cnt.tiles(b) + a.waitExtra;
                 const long long limit = a.waitLimit > 0 ? a.waitLimit : kWaitLimit;
                 long long spins = 0;
-                while (atomicAdd(done + b, 0) < need)
+                while (atomicAdd(RPPB_WR(done + b), 0) < need)
                 {
                     if (++spins > limit)
                     {
-                        atomicOr(errorWord, 1);
+                        atomicOr(RPPB_WR(errorWord), 1);
                         break;
                     }
                     __nanosleep(128);
@@ -523,7 +523,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                 float ref = a.refMag;
                 if (a.refMag == 0.f)
                 {
-                    const unsigned k = __ldcg(maxKey + b);
+                    const unsigned k = __ldcg(RPPB_RD(maxKey + b));
                     ref = k == 0u ? -FLT_MAX : fmaxf(-FLT_MAX, key_float(k));
                 }
                 const float inv = ref != 0.f ? __fdiv_rn(1.f, ref) : 1.0f;
@@ -540,20 +540,20 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                     {
                         float v[kRows];
 #pragma unroll
-                        for (int r = 0; r < kRows; ++r) v[r] = __ldcg(p + r * step);
+                        for (int r = 0; r < kRows; ++r) v[r] = __ldcg(RPPB_RD(p + r * step));
 #pragma unroll
                         for (int r = 0; r < kRows; ++r)
                         {
                             float t = __fmul_rn(v[r], inv);
                             t = a.minRatio < t ? t : a.minRatio;
-                            p[r * step] = __fmul_rn(a.multiplier, __log2f(t));
+                            *RPPB_WR(p + r * step) = __fmul_rn(a.multiplier, __log2f(t));
                         }
                     }
                     for (; m < nmel; m += kDbGroups, p += step)
                     {
-                        float t = __fmul_rn(__ldcg(p), inv);
+                        float t = __fmul_rn(__ldcg(RPPB_RD(p)), inv);
                         t = a.minRatio < t ? t : a.minRatio;
-                        *p = __fmul_rn(a.multiplier, __log2f(t));
+                        *RPPB_WR(p) = __fmul_rn(a.multiplier, __log2f(t));
                     }
                 }
             }
@@ -561,8 +561,8 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         __syncthreads();
         if (threadIdx.x == 0)
         {
-            const long long w = wAfter >= 0 ? wAfter : (long long)atomicAdd(workCounter, 1ull);
-            wAfter = w < total - 2ll * gridDim.x ? (long long)atomicAdd(workCounter, 1ull) : -1ll;
+            const long long w = wAfter >= 0 ? wAfter : (long long)atomicAdd(RPPB_WR(workCounter), 1ull);
+            wAfter = w < total - 2ll * gridDim.x ? (long long)atomicAdd(RPPB_WR(workCounter), 1ull) : -1ll;
             const Item nx = decode_item<TF>(a, cnt, prefix, nslots, total, w);
             prefetch_span(nx);
             s_it[cur] = nx;
@@ -571,8 +571,8 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         {
             float v = s_warpMax[0];
             for (int i = 1; i < kFusedThreads / 32; ++i) v = fmaxf(v, s_warpMax[i]);
-            atomicMax(maxKey + b, float_key(v));
-            asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(done + b) : "memory");
+            atomicMax(RPPB_WR(maxKey + b), float_key(v));
+            asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(RPPB_WR(done + b)) : "memory");
         }
         cur ^= 1;
     }

@@ -220,7 +220,7 @@ struct TcCount
     int chunks;
     __device__ long long operator()(int b) const
     {
-        const int F = max(frames[b], 0);
+        const int F = max(*RPPB_RD(frames + b), 0);
         return (long long)((F + kTileM - 1) / kTileM) * chunks;
     }
 };
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const lon
         if (!*abortFlag)
         {
             *abortFlag = 1;
-            atomicOr(a.errorWord, 2);
+            atomicOr(RPPB_WR(a.errorWord), 2);
         }
     };
 
@@ -442,12 +442,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const lon
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int F = a.frames[it.b];
+            const int F = *RPPB_RD(a.frames + it.b);
             const int frame = it.f0 + r;
             float* y = a.dst + size_t(it.b) * a.dstNStride;
             float sc = 1.f;
             if constexpr (FMT == kTcFp8)
-                if (frame < F) sc = a.invScale[size_t(it.b) * a.maxFrames + frame];
+                if (frame < F) sc = *RPPB_RD(a.invScale + (size_t(it.b) * a.maxFrames + frame));
 #pragma unroll 1
             for (int c0 = 0; c0 < kTileN; c0 += 32)
             {
@@ -472,8 +472,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const lon
                         const int col = n0 + k;
                         if (col >= a.validN) break;
                         const float o = __uint_as_float(v[k]) * sc;
-                        if (a.nft) y[size_t(col) * a.dstHStride + frame] = o;
-                        else y[size_t(frame) * a.dstHStride + col] = o;
+                        if (a.nft) *RPPB_WR(y + (size_t(col) * a.dstHStride + frame)) = o;
+                        else *RPPB_WR(y + (size_t(frame) * a.dstHStride + col)) = o;
                     }
                 }
                 if (EPI == kEpiPower && frame < F)
@@ -492,21 +492,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_dft_kernel(TcArgs a, const lon
                             const int nyq = a.nfft / 2;
                             if (a.nft)
                             {
-                                y[frame] = o0;
-                                y[size_t(nyq) * a.dstHStride + frame] = on;
+                                *RPPB_WR(y + frame) = o0;
+                                *RPPB_WR(y + (size_t(nyq) * a.dstHStride + frame)) = on;
                             }
                             else
                             {
-                                y[size_t(frame) * a.dstHStride] = o0;
-                                y[size_t(frame) * a.dstHStride + nyq] = on;
+                                *RPPB_WR(y + size_t(frame) * a.dstHStride) = o0;
+                                *RPPB_WR(y + (size_t(frame) * a.dstHStride + nyq)) = on;
                             }
                             continue;
                         }
                         const int bin = col >> 1;
                         const float p = fmaf(re, re, im * im);
                         const float o = a.power == 1 ? sqrtf(p) : p;
-                        if (a.nft) y[size_t(bin) * a.dstHStride + frame] = o;
-                        else y[size_t(frame) * a.dstHStride + bin] = o;
+                        if (a.nft) *RPPB_WR(y + (size_t(bin) * a.dstHStride + frame)) = o;
+                        else *RPPB_WR(y + (size_t(frame) * a.dstHStride + bin)) = o;
                     }
                 }
             }
@@ -548,8 +548,8 @@ struct PaddedSignal
             if (!reflect || L <= 0 || t > 0x3fffffff || t < -0x3fffffff) return 0.f;
             t = reflect_index(int(t), 0, L);
         }
-        if (!preemph) return x[t];
-        return __fsub_rn(x[t], __fmul_rn(c, t == 0 ? border : x[t - 1]));
+        if (!preemph) return *RPPB_RD(x + t);
+        return __fsub_rn(*RPPB_RD(x + t), __fmul_rn(c, t == 0 ? border : *RPPB_RD(x + (t - 1))));
     }
 };
 
@@ -559,11 +559,11 @@ __device__ __forceinline__ PaddedSignal padded_signal(const float* src, uint32_t
 {
     PaddedSignal p;
     p.x = src + size_t(b) * srcStride;
-    p.L = min(len[b], int(srcStride));
+    p.L = min(*RPPB_RD(len + b), int(srcStride));
     p.preemph = coeff != nullptr;
-    p.c = p.preemph ? coeff[b] : 0.f;
+    p.c = p.preemph ? *RPPB_RD(coeff + b) : 0.f;
     const size_t base = size_t(b) * srcStride;
-    p.border = border == 1 ? p.x[0] : border == 2 ? (base + 1 < srcElems ? p.x[1] : 0.f) : 0.f;
+    p.border = border == 1 ? *RPPB_RD(p.x) : border == 2 ? (base + 1 < srcElems ? *RPPB_RD(p.x + 1) : 0.f) : 0.f;
     p.reflect = reflect;
     p.centerOffset = centerOffset;
     return p;
@@ -607,17 +607,17 @@ __global__ void tc_prep_kernel(PrepArgs p, void* __restrict__ outHi, void* __res
                 float r[8];
                 if ((reinterpret_cast<uintptr_t>(x) & 15) == 0)
                 {
-                    const float4 a = __ldg(reinterpret_cast<const float4*>(x));
-                    const float4 c4 = __ldg(reinterpret_cast<const float4*>(x + 4));
+                    const float4 a = __ldg(RPPB_RD(reinterpret_cast<const float4*>(x)));
+                    const float4 c4 = __ldg(RPPB_RD(reinterpret_cast<const float4*>(x + 4)));
                     r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
                     r[4] = c4.x; r[5] = c4.y; r[6] = c4.z; r[7] = c4.w;
                 }
                 else
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) r[k] = __ldg(x + k);
+                    for (int k = 0; k < 8; ++k) r[k] = __ldg(RPPB_RD(x + k));
                 if (sig.preemph)
                 {
-                    float prev = __ldg(x - 1);
+                    float prev = __ldg(RPPB_RD(x - 1));
 #pragma unroll
                     for (int k = 0; k < 8; ++k)
                     {
@@ -641,11 +641,11 @@ __global__ void tc_prep_kernel(PrepArgs p, void* __restrict__ outHi, void* __res
                 uint32_t* out = static_cast<uint32_t*>(outHi) + o;
                 if (whole)
                 {
-                    reinterpret_cast<uint4*>(out)[0] = make_uint4(t[0], t[1], t[2], t[3]);
-                    reinterpret_cast<uint4*>(out)[1] = make_uint4(t[4], t[5], t[6], t[7]);
+                    *RPPB_WR(reinterpret_cast<uint4*>(out)) = make_uint4(t[0], t[1], t[2], t[3]);
+                    *RPPB_WR(reinterpret_cast<uint4*>(out) + 1) = make_uint4(t[4], t[5], t[6], t[7]);
                 }
                 else
-                    for (int k = 0; k < 8 && i0 + k < clipStride; ++k) out[k] = t[k];
+                    for (int k = 0; k < 8 && i0 + k < clipStride; ++k) *RPPB_WR(out + k) = t[k];
             }
             else
             {
@@ -666,14 +666,16 @@ __global__ void tc_prep_kernel(PrepArgs p, void* __restrict__ outHi, void* __res
                 __nv_bfloat16* lo = FMT == kTcBf16x3 ? static_cast<__nv_bfloat16*>(outLo) + o : nullptr;
                 if (whole)
                 {
-                    *reinterpret_cast<uint4*>(hi) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                    if constexpr (FMT == kTcBf16x3) *reinterpret_cast<uint4*>(lo) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                    *RPPB_WR(reinterpret_cast<uint4*>(hi)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    if constexpr (FMT == kTcBf16x3)
+                        *RPPB_WR(reinterpret_cast<uint4*>(lo)) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
                 }
                 else
                     for (int k = 0; k < 8 && i0 + k < clipStride; ++k)
                     {
-                        hi[k] = __ushort_as_bfloat16(uint16_t(hw[k / 2] >> (16 * (k & 1))));
-                        if constexpr (FMT == kTcBf16x3) lo[k] = __ushort_as_bfloat16(uint16_t(lw[k / 2] >> (16 * (k & 1))));
+                        *RPPB_WR(hi + k) = __ushort_as_bfloat16(uint16_t(hw[k / 2] >> (16 * (k & 1))));
+                        if constexpr (FMT == kTcBf16x3)
+                            *RPPB_WR(lo + k) = __ushort_as_bfloat16(uint16_t(lw[k / 2] >> (16 * (k & 1))));
                     }
             }
         }
@@ -690,7 +692,7 @@ __global__ void tc_prep_fp8_kernel(PrepArgs p, const int* __restrict__ frames, i
     {
         const PaddedSignal sig =
             padded_signal(p.src, p.srcStride, p.srcElems, p.len, p.coeff, p.border, p.reflect, p.centerOffset, b);
-        const int F = frames[b];
+        const int F = *RPPB_RD(frames + b);
         for (int f = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); f < F; f += gridDim.x * warpsPerBlock)
         {
             const long long s0 = (long long)f * hop;
@@ -699,8 +701,8 @@ __global__ void tc_prep_fp8_kernel(PrepArgs p, const int* __restrict__ frames, i
             m = warp_max(m);
             const float scale = m > 0.f ? kFp8Max / m : 1.f;
             __nv_fp8_e4m3* row = out + (size_t(b) * maxFrames + f) * kPad;
-            for (int t = lane; t < kPad; t += 32) row[t] = __nv_fp8_e4m3(t < W ? sig(s0 + t) * scale : 0.f);
-            if (lane == 0) invScale[size_t(b) * maxFrames + f] = 1.f / (scale * kFp8BasisScale);
+            for (int t = lane; t < kPad; t += 32) *RPPB_WR(row + t) = __nv_fp8_e4m3(t < W ? sig(s0 + t) * scale : 0.f);
+            if (lane == 0) *RPPB_WR(invScale + (size_t(b) * maxFrames + f)) = 1.f / (scale * kFp8BasisScale);
         }
     }
 }
@@ -717,7 +719,7 @@ __global__ void tc_prep_rows_kernel(PrepArgs p, const int* __restrict__ frames, 
     {
         const PaddedSignal sig =
             padded_signal(p.src, p.srcStride, p.srcElems, p.len, p.coeff, p.border, p.reflect, p.centerOffset, b);
-        const int F = frames[b];
+        const int F = *RPPB_RD(frames + b);
         for (int f = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); f < F; f += gridDim.x * warpsPerBlock)
         {
             const long long s0 = (long long)f * hop;
@@ -729,14 +731,15 @@ __global__ void tc_prep_rows_kernel(PrepArgs p, const int* __restrict__ frames, 
                 {
                     uint32_t u;
                     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(v));
-                    static_cast<uint32_t*>(outHi)[row + t] = u;
+                    *RPPB_WR(static_cast<uint32_t*>(outHi) + (row + t)) = u;
                 }
                 else
                 {
                     const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-                    static_cast<__nv_bfloat16*>(outHi)[row + t] = hi;
+                    *RPPB_WR(static_cast<__nv_bfloat16*>(outHi) + (row + t)) = hi;
                     if constexpr (FMT == kTcBf16x3)
-                        static_cast<__nv_bfloat16*>(outLo)[row + t] = __float2bfloat16_rn(v - __bfloat162float(hi));
+                        *RPPB_WR(static_cast<__nv_bfloat16*>(outLo) + (row + t)) =
+                            __float2bfloat16_rn(v - __bfloat162float(hi));
                 }
             }
         }
@@ -747,7 +750,7 @@ __global__ void tc_frames_kernel(const int* __restrict__ len, uint32_t srcStride
                                  int maxFrames, int* __restrict__ frames)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
-        frames[b] = min(num_windows(min(len[b], int(srcStride)), W, hop, center), maxFrames);
+        *RPPB_WR(frames + b) = min(num_windows(min(*RPPB_RD(len + b), int(srcStride)), W, hop, center), maxFrames);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver
@@ -952,13 +955,13 @@ __global__ void mel_frame_scale_kernel(MelPrepArgs a)
     for (int b = blockIdx.y; b < a.n; b += gridDim.y)
     {
         const float* x = a.src + size_t(b) * a.srcNStride;
-        const int F = a.frames[b];
+        const int F = *RPPB_RD(a.frames + b);
         for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < F; f += gridDim.x * blockDim.x)
         {
             float m = 0.f;
-            for (int k = 0; k < a.bins; ++k) m = fmaxf(m, fabsf(x[size_t(k) * a.srcHStride + f]));
+            for (int k = 0; k < a.bins; ++k) m = fmaxf(m, fabsf(*RPPB_RD(x + (size_t(k) * a.srcHStride + f))));
             const float sc = m > 0.f ? kFp8Max / m : 1.f;
-            a.invScale[size_t(b) * a.maxFrames + f] = 1.f / (sc * *a.bScale);
+            *RPPB_WR(a.invScale + (size_t(b) * a.maxFrames + f)) = 1.f / (sc * *RPPB_RD(a.bScale));
         }
     }
 }
@@ -971,14 +974,14 @@ __global__ void __launch_bounds__(256) mel_prep_kernel(MelPrepArgs a)
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
     for (int b = blockIdx.z; b < a.n; b += gridDim.z)
     {
-        const int F = a.frames[b];
+        const int F = *RPPB_RD(a.frames + b);
         const int f0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
         if (f0 >= F || k0 >= a.kPad) continue;
         const float* x = a.src + size_t(b) * a.srcNStride;
         for (int r = ty; r < 32; r += 8)
         {
             const int k = k0 + r, f = f0 + tx;
-            tile[r][tx] = (k < a.bins && f < F) ? x[size_t(k) * a.srcHStride + f] : 0.f;
+            tile[r][tx] = (k < a.bins && f < F) ? *RPPB_RD(x + (size_t(k) * a.srcHStride + f)) : 0.f;
         }
         __syncthreads();
         for (int r = ty; r < 32; r += 8)
@@ -992,19 +995,19 @@ __global__ void __launch_bounds__(256) mel_prep_kernel(MelPrepArgs a)
                 {
                     uint32_t t;
                     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
-                    reinterpret_cast<uint32_t*>(a.aHi)[o] = t;
+                    *RPPB_WR(reinterpret_cast<uint32_t*>(a.aHi) + o) = t;
                 }
                 else if (a.fmt == kTcFp8)
                 {
-                    const float sc = 1.f / (a.invScale[size_t(b) * a.maxFrames + f] * *a.bScale);
-                    reinterpret_cast<__nv_fp8_e4m3*>(a.aHi)[o] = __nv_fp8_e4m3(v * sc);
+                    const float sc = 1.f / (*RPPB_RD(a.invScale + (size_t(b) * a.maxFrames + f)) * *RPPB_RD(a.bScale));
+                    *RPPB_WR(reinterpret_cast<__nv_fp8_e4m3*>(a.aHi) + o) = __nv_fp8_e4m3(v * sc);
                 }
                 else
                 {
                     const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-                    reinterpret_cast<__nv_bfloat16*>(a.aHi)[o] = hi;
+                    *RPPB_WR(reinterpret_cast<__nv_bfloat16*>(a.aHi) + o) = hi;
                     if (a.fmt == kTcBf16x3)
-                        reinterpret_cast<__nv_bfloat16*>(a.aLo)[o] = __float2bfloat16_rn(v - __bfloat162float(hi));
+                        *RPPB_WR(reinterpret_cast<__nv_bfloat16*>(a.aLo) + o) = __float2bfloat16_rn(v - __bfloat162float(hi));
                 }
             }
         }
@@ -1015,7 +1018,7 @@ __global__ void __launch_bounds__(256) mel_prep_kernel(MelPrepArgs a)
 __global__ void mel_frames_kernel(const int* __restrict__ dims, int n, int maxFrames, int* __restrict__ frames)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
-        frames[b] = min(max(dims[2 * b + 1], 0), maxFrames);
+        *RPPB_WR(frames + b) = min(max(*RPPB_RD(dims + (2 * b + 1)), 0), maxFrames);
 }
 
 }  // namespace
