@@ -321,6 +321,17 @@ __global__ void __launch_bounds__(kThreads, kMix ? 5 : 4)
                     p = __fadd_rn(p, fscale);
                     out[k] = q;
                 }
+                // ask L2 for the unit's input span (a group ahead of its use): the taps of its outputs
+                // read samples [ceil(first phase) - lobes, ceil(last phase) + lobes) from inBlockRounded on
+                const int cnt = min(kBlock, u.outEnd - u.unit * kBlock);
+                if (cnt > 0)
+                {
+                    const float* ph = s_phase[slot][j];
+                    const long long lo = max((long long)u.inBlockRounded + int(ceilf(ph[0])) - lobes, 0ll);
+                    const long long hi =
+                        min((long long)u.inBlockRounded + int(ceilf(ph[cnt - 1])) + lobes, (long long)u.L);
+                    if (hi > lo) l2_prefetch(u.x + lo * u.Csrc, u.x + hi * u.Csrc);
+                }
             }
         }
         s_unit[slot][j] = u;
