@@ -134,23 +134,35 @@ void check_upload(cudaStream_t s, bool enabled, std::vector<CheckSpan> spans)
         return a.writable != b.writable ? a.writable < b.writable
                                         : reinterpret_cast<uintptr_t>(a.p) < reinterpret_cast<uintptr_t>(b.p);
     });
-    CheckTable t{};
-    t.enabled = enabled ? 1 : 0;
+    std::vector<CheckRegion> rs;
     for (const CheckSpan& x : keep)
     {
         const unsigned long long lo = reinterpret_cast<uintptr_t>(x.p), hi = lo + x.bytes;
-        if (t.count > 0)
-        {
-            CheckRegion& last = t.r[t.count - 1];
-            if (last.writable == int(x.writable) && lo <= last.hi)   // overlapping or adjacent: merge
-            {
-                last.hi = std::max(last.hi, hi);
-                continue;
-            }
-        }
-        if (t.count == kCheckRegions) fail(RPP_ERROR, "checked build: more device regions than the table holds");
-        t.r[t.count++] = CheckRegion{lo, hi, int(x.writable), 0};
+        if (!rs.empty() && rs.back().writable == int(x.writable) && lo <= rs.back().hi)   // overlapping or adjacent
+            rs.back().hi = std::max(rs.back().hi, hi);
+        else
+            rs.push_back(CheckRegion{lo, hi, int(x.writable), 0});
     }
+    // more regions than the table holds (a clip table of many separate buffers): merge the two neighbours
+    // of equal access with the smallest gap until they fit, so the checks only widen
+    while (rs.size() > size_t(kCheckRegions))
+    {
+        size_t best = rs.size();
+        unsigned long long gap = ~0ull;
+        for (size_t i = 0; i + 1 < rs.size(); ++i)
+            if (rs[i].writable == rs[i + 1].writable && rs[i + 1].lo - rs[i].hi < gap)
+            {
+                gap = rs[i + 1].lo - rs[i].hi;
+                best = i;
+            }
+        if (best == rs.size()) fail(RPP_ERROR, "checked build: more device regions than the table holds");
+        rs[best].hi = std::max(rs[best].hi, rs[best + 1].hi);
+        rs.erase(rs.begin() + best + 1);
+    }
+    CheckTable t{};
+    t.enabled = enabled ? 1 : 0;
+    t.count = int(rs.size());
+    std::copy(rs.begin(), rs.end(), t.r);
     check_table_kernel<<<1, 1, 0, s>>>(t);
     check_cuda(cudaGetLastError(), "check_table_kernel");
 }
