@@ -223,10 +223,10 @@ SHARED_PUBLIC RppStatus rppb_set_tc_materialized_frames(rppHandle_t rppHandle, b
  * for a stray read or RPP_ERROR_INSUFFICIENT_DST_BUFFER_LENGTH for a stray write, with the file, line,
  * address and count in rppbGetLastError().  Calls run one at a time and synchronize their stream at
  * the end (a captured call's record is read by the next uncaptured one).  This test hook registers the
- * next call's destination tensor `bytes` shorter than its descriptor says, so that the call's last
- * in-bounds stores are reported (and skipped) as out of bounds.  It returns RPP_ERROR_NOT_IMPLEMENTED
- * in the ordinary library. */
-SHARED_PUBLIC RppStatus rppb_check_shrink_next_destination(Rpp64u bytes);
+ * next call's source and destination tensors sourceBytes and destinationBytes shorter than their
+ * descriptors say (0: as described), so that the call's last in-bounds loads or stores are reported (and
+ * skipped) as out of bounds.  It returns RPP_ERROR_NOT_IMPLEMENTED in the ordinary library. */
+SHARED_PUBLIC RppStatus rppb_check_shrink_next_tensors(Rpp64u sourceBytes, Rpp64u destinationBytes);
 
 #ifdef __cplusplus
 }

@@ -9,8 +9,8 @@
 // capture) synchronizes, reads the record and turns a violation into a status code: a stray read into
 // RPP_ERROR_OUT_OF_BOUND_SRC_ROI, a stray write into RPP_ERROR_INSUFFICIENT_DST_BUFFER_LENGTH.
 //
-// In the library (no RPPB_CHECKED) this file only defines rppb_check_shrink_next_destination, which
-// returns RPP_ERROR_NOT_IMPLEMENTED there.
+// In the library (no RPPB_CHECKED) this file only defines rppb_check_shrink_next_tensors, which returns
+// RPP_ERROR_NOT_IMPLEMENTED there.
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
@@ -108,7 +108,7 @@ std::string site_name(unsigned site)
     return "file " + std::to_string(h) + ":" + std::to_string(site & 0xffffu);
 }
 
-unsigned long long g_shrink = 0;   // rppb_check_shrink_next_destination
+unsigned long long g_shrink[2] = {0, 0};   // rppb_check_shrink_next_tensors: source, destination
 
 }  // namespace
 
@@ -118,10 +118,10 @@ std::recursive_mutex& check_mutex()
     return m;
 }
 
-unsigned long long check_take_shrink()
+unsigned long long check_take_shrink(bool destination)
 {
-    const unsigned long long s = g_shrink;
-    g_shrink = 0;
+    const unsigned long long s = g_shrink[destination ? 1 : 0];
+    g_shrink[destination ? 1 : 0] = 0;
     return s;
 }
 
@@ -190,15 +190,16 @@ void check_reset()
 
 }  // namespace rppb
 
-extern "C" SHARED_PUBLIC RppStatus rppb_check_shrink_next_destination(Rpp64u bytes)
+extern "C" SHARED_PUBLIC RppStatus rppb_check_shrink_next_tensors(Rpp64u sourceBytes, Rpp64u destinationBytes)
 {
     std::lock_guard<std::recursive_mutex> lk(rppb::check_mutex());
-    rppb::g_shrink = bytes;
+    rppb::g_shrink[0] = sourceBytes;
+    rppb::g_shrink[1] = destinationBytes;
     return RPP_SUCCESS;
 }
 
 #else
 
-extern "C" SHARED_PUBLIC RppStatus rppb_check_shrink_next_destination(Rpp64u) { return RPP_ERROR_NOT_IMPLEMENTED; }
+extern "C" SHARED_PUBLIC RppStatus rppb_check_shrink_next_tensors(Rpp64u, Rpp64u) { return RPP_ERROR_NOT_IMPLEMENTED; }
 
 #endif

@@ -104,7 +104,7 @@ size_t desc_bytes(const RpptGenericDesc& d, int n)
 template <class D>
 void check_tensors(Handle& h, const void* src, const D& sd, const void* dst, const D& dd, int n)
 {
-    h.check_add(src, desc_bytes(sd, n), false);
+    h.check_src(src, desc_bytes(sd, n));
     if (dst) h.check_dst(dst, desc_bytes(dd, n));
 }
 
@@ -682,7 +682,7 @@ extern "C" SHARED_PUBLIC RppStatus rppb_frontend_host_gpu(const Rpp32f* srcHost,
         const bool gatherK = h.device_writable(srcHost, &srcMapped);
         const bool scatterK = h.device_writable(dstHost, &dstMapped);
         if (gatherK || scatterK) a.reserveSms = kReservedSms;   // room for the movers next to the persistent kernel
-        if (gatherK) h.check_add(srcMapped, desc_bytes(srcDescPtr, n), false);
+        if (gatherK) h.check_src(srcMapped, desc_bytes(srcDescPtr, n));
         if (scatterK) h.check_dst(dstMapped, desc_bytes(dstDescPtr, n));
 
         cudaStream_t main = h.stream(), up = h.aux_stream(0), down = h.aux_stream(1);

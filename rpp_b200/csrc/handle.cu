@@ -268,9 +268,15 @@ void Handle::check_add(const void* p, size_t bytes, bool writable)
     check_dirty_ = true;
 }
 
+void Handle::check_src(const void* p, size_t bytes)
+{
+    const unsigned long long shrink = check_take_shrink(false);
+    check_add(p, shrink < bytes ? bytes - shrink : 0, false);
+}
+
 void Handle::check_dst(const void* p, size_t bytes)
 {
-    const unsigned long long shrink = check_take_shrink();
+    const unsigned long long shrink = check_take_shrink(true);
     check_add(p, shrink < bytes ? bytes - shrink : 0, true);
 }
 

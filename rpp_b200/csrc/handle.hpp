@@ -46,8 +46,9 @@ void check_upload(cudaStream_t s, bool enabled, std::vector<CheckSpan> spans);
 // Reads and clears the violation record: st when there was none, else the violation's status code.
 RppStatus check_collect(RppStatus st);
 void check_reset();
-// The byte count rppb_check_shrink_next_destination set (0 when none), cleared by the read.
-unsigned long long check_take_shrink();
+// The byte count rppb_check_shrink_next_tensors set for the next source or destination tensor (0 when
+// none), cleared by the read.
+unsigned long long check_take_shrink(bool destination);
 #endif
 
 // Bump allocator over one workspace block: measure with base == nullptr, then carve.
@@ -133,10 +134,12 @@ class Handle
     bool tc_materialize() const { return tc_materialize_; }
 
     // Checked build: regions of the current call beyond the handle's own blocks (caller tensors,
-    // per-sample tensors, pinned host buffers); check_dst registers a caller's destination tensor.
+    // per-sample tensors, pinned host buffers); check_src / check_dst register a caller's source /
+    // destination tensor.
     // check_begin starts a call, check_end ends it and returns the status of any violation.
 #ifdef RPPB_CHECKED
     void check_add(const void* p, size_t bytes, bool writable);
+    void check_src(const void* p, size_t bytes);
     void check_dst(const void* p, size_t bytes);
     void check_begin();
     RppStatus check_end(RppStatus st);
@@ -144,6 +147,7 @@ class Handle
     void check_suspend();
 #else
     void check_add(const void*, size_t, bool) {}
+    void check_src(const void*, size_t) {}
     void check_dst(const void*, size_t) {}
     void check_begin() {}
     RppStatus check_end(RppStatus st) { return st; }

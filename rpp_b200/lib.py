@@ -27,7 +27,7 @@ EXPORTED = (
     "rppb_server_create", "rppb_server_destroy", "rppb_server_frames", "rppb_server_submit", "rppb_server_poll",
     "rppb_server_arena_used",
     "rppt_slice_gpu", "rppt_normalize_gpu", "rppb_pcm16_to_f32_gpu", "rppb_mel_filter_bank_tc_gpu",
-    "rppb_check_shrink_next_destination",
+    "rppb_check_shrink_next_tensors",
 )
 
 _lib = None
@@ -96,8 +96,8 @@ def load(path=None):
     L.rppb_pcm16_to_f32_gpu.restype = _I
     L.rppb_mel_filter_bank_tc_gpu.argtypes = [_V, _D, _V, _D, _V, _F, _F, _I, _I, _F, _B, _I, _V]
     L.rppb_mel_filter_bank_tc_gpu.restype = _I
-    L.rppb_check_shrink_next_destination.argtypes = [ctypes.c_uint64]
-    L.rppb_check_shrink_next_destination.restype = _I
+    L.rppb_check_shrink_next_tensors.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+    L.rppb_check_shrink_next_tensors.restype = _I
     L.rppb_server_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(RppbServerConfig)]
     L.rppb_server_create.restype = _I
     L.rppb_server_destroy.argtypes = [_V]
