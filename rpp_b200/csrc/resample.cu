@@ -35,7 +35,7 @@ namespace {
 constexpr int kBlock = 256;        // outputs per block (the reference's block size)
 constexpr int kCopyChunk = 4096;   // floats per unit of an equal-rate copy
 
-constexpr int kThreads = kBlock + 32;   // 8 warps compute outputs, the ninth replays the next unit's phases
+constexpr int kThreads = kBlock + 32;   // 8 warps compute outputs, the ninth decodes the next group of blocks
 
 // Shared memory (floats): the table -- as padded (value, next - value) pairs when kPairs, else
 // plain -- then, when down-mixing, the staged input span.
