@@ -17,8 +17,10 @@
  * intermediate pre-emphasized signal, spectrum and mel tensors never reach memory except the mel
  * power, which is written into dst and converted to decibels in place once the clip's maximum is
  * known.  dst is NFT [numFilter][frames] per sample (hStride >= frames); only the valid frames
- * are written.  nfft must be a power of two from 128 to 2048.  Asynchronous on the handle stream;
- * capturable in a CUDA graph after one uncaptured call has sized the handle workspace.
+ * are written.  nfft must be a power of two from 128 to 2048.  The tables, a frame tile's span and its
+ * power tile sit in shared memory: a window, step or numFilter too large for a CTA's share returns
+ * RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE.  Asynchronous on the handle stream; capturable in a CUDA
+ * graph after one uncaptured call has sized the handle workspace.
  */
 #ifndef RPPB_FRONTEND_H
 #define RPPB_FRONTEND_H

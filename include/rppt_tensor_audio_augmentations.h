@@ -87,7 +87,10 @@ SHARED_PUBLIC RppStatus rppt_down_mixing_gpu(RppPtr_t srcPtr, RpptDescPtr srcDes
  * centerWindows (reflect or zero padding at the edges), multiplied by windowFunction (host
  * pointer; nullptr = Hann), placed in the middle of an nfft-point buffer (nfft 0 = windowLength)
  * and transformed.  dst is NFT [nfft/2+1][frames] or NTF [frames][nfft/2+1] per sample.
- * srcDesc numDims = 2, dstDesc numDims = 3.  Replaces api/rppt_tensor_audio_augmentations.h:232. */
+ * srcDesc numDims = 2, dstDesc numDims = 3.  A CTA stages a tile of frames with their input span in
+ * shared memory: for nfft 2048 with a window and step of over ~1000 samples the tile does not fit, and
+ * the call returns RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE.  Replaces
+ * api/rppt_tensor_audio_augmentations.h:232. */
 SHARED_PUBLIC RppStatus rppt_spectrogram_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr, RpptDescPtr dstDescPtr,
                                              Rpp32s *srcLengthTensor, bool centerWindows, bool reflectPadding,
                                              Rpp32f *windowFunction, Rpp32s nfft, Rpp32s power, Rpp32s windowLength,
@@ -96,7 +99,9 @@ SHARED_PUBLIC RppStatus rppt_spectrogram_gpu(RppPtr_t srcPtr, RpptDescPtr srcDes
 /* Mel filter bank over an NFT spectrum: numFilter triangular filters evenly spaced on the
  * mel scale between minFreq and maxFreq (0 = sampleRate/2), optionally area-normalized.
  * srcDimsTensor = {bins, frames} per sample; nfft is derived per sample as (bins-1)*2.
- * src/dst layout NFT, numDims = 3.  Replaces api/rppt_tensor_audio_augmentations.h:274. */
+ * src/dst layout NFT, numDims = 3.  The filter tables and a spectrum tile sit in shared memory: bins and
+ * filters whose tables exceed a CTA's share return RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE.
+ * Replaces api/rppt_tensor_audio_augmentations.h:274. */
 SHARED_PUBLIC RppStatus rppt_mel_filter_bank_gpu(RppPtr_t srcPtr, RpptDescPtr srcDescPtr, RppPtr_t dstPtr, RpptDescPtr dstDescPtr,
                                                  Rpp32s *srcDimsTensor, Rpp32f maxFreq, Rpp32f minFreq,
                                                  RpptMelScaleFormula melFormula, Rpp32s numFilter, Rpp32f sampleRate,

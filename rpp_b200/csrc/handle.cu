@@ -397,6 +397,10 @@ int persistent_grid(const Handle& h, const void* kernel, int threads, size_t sme
     // without the opt-in attribute, static + dynamic shared memory must stay within 48 KB
     cudaFuncAttributes fa{};
     check_cuda(cudaFuncGetAttributes(&fa, kernel), "cudaFuncGetAttributes");
+    int optin = 0;
+    check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h.device()), "smem limit");
+    if (smem + fa.sharedSizeBytes > size_t(optin))
+        fail(RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, "the call's tile needs more shared memory than a CTA has");
     if (smem + fa.sharedSizeBytes > 48 * 1024 && smem > limit)
     {
         check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem attr");

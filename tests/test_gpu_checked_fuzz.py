@@ -23,7 +23,7 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(os.environ.get("RPPB_LIBRARY") != "checked",
                                  reason="runs against librppb_checked.so (tests/test_gpu_checked.py)")]
 
-SEEDS = range(16)
+SEEDS = range(40)
 OK = RppStatus.RPP_SUCCESS
 
 
@@ -49,8 +49,13 @@ def case(r):
     return n, L, pad
 
 
-def run(st):
+def run(st, tile_limit=False):
+    """tile_limit: a call whose frame tile does not fit a CTA's shared memory may return the documented
+    RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE (large nfft with a long window and step, many filters)."""
+    if tile_limit and st == RppStatus.RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE:
+        return False
     assert st == OK, (st, lib.last_error())
+    return True
 
 
 @pytest.mark.parametrize("seed", SEEDS)
@@ -120,8 +125,9 @@ def test_spectrogram_mel_decibels(gpu, seed):
     layout = RpptLayout.NFT if nft else RpptLayout.NTF
     spec = torch.zeros((n, bins, mf) if nft else (n, mf, bins), device="cuda")
     dd = spectra_desc(n, bins, mf, layout) if nft else spectra_desc(n, mf, bins, layout)
-    run(audio.spectrogram(signal(r, n, L + pad), audio_desc(n, L + pad), spec, dd, dev(lens), center, reflect, None,
-                          nfft, int(r.integers(1, 3)), W, hop, gpu))
+    if not run(audio.spectrogram(signal(r, n, L + pad), audio_desc(n, L + pad), spec, dd, dev(lens), center, reflect,
+                                 None, nfft, int(r.integers(1, 3)), W, hop, gpu), tile_limit=True):
+        return
     if not nft:
         return
     nmel = int(min(r.choice([16, 40, 80, 128]), bins - 1))
@@ -130,7 +136,7 @@ def test_spectrogram_mel_decibels(gpu, seed):
     mel = torch.zeros((n, nmel, mf), device="cuda")
     run(audio.mel_filter_bank(spec.abs() + 1e-6, spectra_desc(n, bins, mf), mel, spectra_desc(n, nmel, mf), dev(dims),
                               fmax if fmax else 8000.0, float(r.choice([0.0, 20.0])), int(r.integers(0, 2)), nmel,
-                              16000.0, bool(r.integers(0, 2)), gpu))
+                              16000.0, bool(r.integers(0, 2)), gpu), tile_limit=True)
     patches = audio.image_patches(F, [nmel] * n)
     run(audio.to_decibels(mel.abs() + 1e-6, spectra_desc(n, nmel, mf), torch.zeros((n, nmel, mf), device="cuda"),
                           spectra_desc(n, nmel, mf), patches, -80.0, 10.0, float(r.choice([0.0, 1.0])), gpu))
@@ -154,9 +160,9 @@ def test_frontend(gpu, seed):
                         lookahead=int(r.choice([0, 1, 8])), db_frames=int(r.choice([0, 16, 64])))
     x = signal(r, n, L + pad)
     coeff = dev(r.uniform(0.5, 0.99, n).astype(np.float32))
-    run(audio.frontend(x, audio_desc(n, L + pad), torch.zeros((n, nmel, mf), device="cuda"),
-                       spectra_desc(n, nmel, mf), dev(lens), coeff, p, gpu))
-    if engine == 0 and seed % 4 == 0:
+    fits = run(audio.frontend(x, audio_desc(n, L + pad), torch.zeros((n, nmel, mf), device="cuda"),
+                              spectra_desc(n, nmel, mf), dev(lens), coeff, p, gpu), tile_limit=True)
+    if fits and engine == 0 and seed % 4 == 0:
         xh = torch.from_numpy(r.uniform(-0.5, 0.5, (n, L + pad)).astype(np.float32)).pin_memory()
         out = torch.zeros((n, nmel, mf)).pin_memory()
         run(audio.frontend_host(xh, audio_desc(n, L + pad), out, spectra_desc(n, nmel, mf), lens,

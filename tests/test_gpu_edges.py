@@ -98,3 +98,16 @@ def test_full_size_decibel_range(gpu, full_batch):
         v = out[b, :, :F[b]]
         assert abs(float(v.max())) <= 1e-5
         assert float(v.min()) >= -80.0 - 1e-3
+
+
+def test_frame_tile_too_large_for_shared_memory(gpu):
+    """nfft 2048 with a 1512-sample window every 1031 samples: the frame tile and its span do not fit a CTA's
+    shared memory, and the call says so with the documented status instead of failing to launch."""
+    n, L = 2, 6000
+    x = torch.zeros((n, L), device="cuda")
+    lens = torch.full((n,), L, dtype=torch.int32, device="cuda")
+    F = L // 1031 + 1
+    out = torch.zeros((n, 1025, F), device="cuda")
+    st = audio.spectrogram(x, audio_desc(n, L), out, spectra_desc(n, 1025, F), lens, True, True, None, 2048, 2, 1512,
+                           1031, gpu)
+    assert st == RppStatus.RPP_ERROR_OUT_OF_BOUND_SHARED_MEMORY_SIZE, st
