@@ -22,7 +22,8 @@ from rpp_b200 import lib
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SUITES = ["tests/test_gpu_ops.py", "tests/test_gpu_normalize_nd.py", "tests/test_gpu_frontend.py",
           "tests/test_gpu_frontend_tc.py", "tests/test_gpu_tc.py", "tests/test_gpu_parity_reference.py",
-          "tests/test_gpu_edges.py", "tests/test_gpu_checked_hooks.py", "tests/test_gpu_checked_fuzz.py"]
+          "tests/test_gpu_edges.py", "tests/test_gpu_parity_fuzz.py", "tests/test_gpu_checked_hooks.py",
+          "tests/test_gpu_checked_fuzz.py"]
 
 
 @pytest.mark.gpu
