@@ -243,7 +243,7 @@ static_assert(kGroup == kWarps && kBlock == kWarps * 32, "one 32-output slice pe
 // kMix: the input is interleaved multi-channel and is down-mixed to mono on the fly (MonoMix), so
 // the launch equals rppt_down_mixing_gpu followed by a mono rppt_resample_gpu.
 template <bool kMix, bool kTable, bool kPairs, bool kMagic = false, bool kFma = false>
-__global__ void __launch_bounds__(kThreads, kMix ? 5 : 4)
+__global__ void __launch_bounds__(kThreads, 4)
     resample_kernel(const float* __restrict__ src, uint32_t srcStride, float* __restrict__ dst, uint32_t dstStride,
                     const float* __restrict__ inRateT, const float* __restrict__ outRateT,
                     const int* __restrict__ dims, ResampleWindowDev wd, bool normalize,
