@@ -219,14 +219,14 @@ void launch_to_decibels(Handle& h, void* scratch, const DecibelArgs& a)
     Carver cv(scratch);
     long long* prefix = cv.take<long long>(a.n + 1);
     unsigned* maxKey = cv.take<unsigned>(a.n);
-    launch_ragged_prefix(DecibelCount{a.dims}, a.n, prefix, h.stream());
     const bool useMax = (a.referenceMagnitude == 0.f);
+    // the maxima accumulate with atomicMax from zero keys: the prefix kernel zeroes them
+    launch_ragged_prefix(DecibelCount{a.dims}, a.n, prefix, h.stream(), maxKey, useMax ? a.n : 0);
     auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
     const bool vecSrc = aligned(a.src) && (a.srcNStride & 3) == 0 && (a.srcHStride & 3) == 0;
     const bool vec = vecSrc && aligned(a.dst) && (a.dstNStride & 3) == 0 && (a.dstHStride & 3) == 0;
     if (useMax)
     {
-        check_cuda(cudaMemsetAsync(maxKey, 0, size_t(a.n) * sizeof(unsigned), h.stream()), "memset(max)");
         int grid = persistent_grid(h, reinterpret_cast<const void*>(decibel_max_kernel), kThreads, 0);
         decibel_max_kernel<<<grid, kThreads, 0, h.stream()>>>(a.src, a.srcNStride, a.srcHStride, a.dims, maxKey,
                                                               prefix, a.n, vecSrc);
