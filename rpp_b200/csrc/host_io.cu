@@ -33,9 +33,17 @@ __global__ void __launch_bounds__(kMoverThreads) host_gather_kernel(const float*
         float* d = dst + size_t(b) * dstStride + s0;
         if (((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(d)) & 15) == 0)
         {
-            const int q = m >> 2;
-            const float4* s4 = reinterpret_cast<const float4*>(s);
-            float4* d4 = reinterpret_cast<float4*>(d);
+            // the warps' loads follow the 128-byte lines of the host row: the samples before the first
+            // line boundary (a multiple of 4, at most 28) go one per thread, the rest 16 bytes per
+            // thread from the boundary on, so each warp load reads 4 whole lines rather than parts of 5
+            const int head = min(m, int(((128u - unsigned(reinterpret_cast<uintptr_t>(s) & 127u)) & 127u) >> 2));
+            if (int(threadIdx.x) < head) *RPPB_WR(d + threadIdx.x) = *RPPB_RD(s + threadIdx.x);
+            const float* sa = s + head;
+            float* da = d + head;
+            const int ma = m - head;
+            const int q = ma >> 2;
+            const float4* s4 = reinterpret_cast<const float4*>(sa);
+            float4* d4 = reinterpret_cast<float4*>(da);
             // 8 loads in flight per thread before the stores
             constexpr int kUnroll = kSegment / 4 / kMoverThreads;
             float4 v[kUnroll];
@@ -51,7 +59,7 @@ __global__ void __launch_bounds__(kMoverThreads) host_gather_kernel(const float*
                 const int i = threadIdx.x + k * kMoverThreads;
                 if (i < q) *RPPB_WR(d4 + i) = v[k];
             }
-            for (int i = (q << 2) + threadIdx.x; i < m; i += kMoverThreads) *RPPB_WR(d + i) = *RPPB_RD(s + i);
+            for (int i = (q << 2) + threadIdx.x; i < ma; i += kMoverThreads) *RPPB_WR(da + i) = *RPPB_RD(sa + i);
         }
         else
         {
@@ -61,7 +69,7 @@ __global__ void __launch_bounds__(kMoverThreads) host_gather_kernel(const float*
 }
 
 // dst[(c0 + b) * dstNStride + r * dstHStride + f] = src[b * srcNStride + r * srcHStride + f] for
-// rows r < rows and frames f < frames_b: one warp per row, coalesced 128-byte writes.
+// rows r < rows and frames f < frames_b: one warp per row, each store one 128-byte line of dst.
 __global__ void __launch_bounds__(kMoverThreads) host_scatter_kernel(const float* __restrict__ src, uint32_t srcNStride,
                                                                      uint32_t srcHStride,
                                                                      const int* __restrict__ frames, int clips,
@@ -77,7 +85,13 @@ __global__ void __launch_bounds__(kMoverThreads) host_scatter_kernel(const float
         const int F = *RPPB_RD(frames + b);
         const float* s = src + size_t(b) * srcNStride + size_t(r) * srcHStride;
         float* d = dst + size_t(b) * dstNStride + size_t(r) * dstHStride;
-        int f = lane;
+        // the warp's stores follow the 128-byte lines of the destination row: lane l first takes frame
+        // l - head (when that is >= 0), the rest of the line that d[0] lies in, so every later store
+        // of the warp fills one whole line (one PCIe write rather than two partial ones)
+        const int head = int((reinterpret_cast<uintptr_t>(d) >> 2) & 31);
+        int f = lane - head;
+        if (f >= 0 && f < F) *RPPB_WR(d + f) = *RPPB_RD(s + f);
+        f += 32;
         for (; f + 96 < F; f += 128)
         {
             const float v0 = *RPPB_RD(s + f), v1 = *RPPB_RD(s + (f + 32)), v2 = *RPPB_RD(s + (f + 64)),
