@@ -887,8 +887,9 @@ def run_b200(args, world, rank, local):
     if sampler:
         sampler.start()
     # The timed steps last a few ms, shorter than the sampler's period: keep the same call running
-    # (untimed) for about 0.4 s first, so the samples show the clocks under this load.
-    load_steps = max(1, int(400.0 / max(plain_ms, 0.05)))
+    # (untimed) for about 0.4 s first, so the samples show the clocks under this load (the fused call
+    # takes about half the plain chain's time, so 800 ms worth of plain steps).
+    load_steps = max(1, int(800.0 / max(plain_ms, 0.05)))
     for _ in range(load_steps):
         fused.run(x)
     torch.cuda.synchronize()
